@@ -1,0 +1,53 @@
+/*
+ * ORACLE -- test infrastructure only. A plain-C restatement of ExaHyPE's
+ * generic nonlinear ADER-DG kernels, limiter kernels and FV MUSCL-Hancock
+ * update, plus a uniform-mesh harness that sequences them the way the
+ * reference solver does. It is the checker for the CUDA path: only the test
+ * suite, the smoke check and the bench's CPU-baseline leg may call it.
+ *
+ * Parity pins: tests/golden/ (the reference's own kernel-test vectors) and the
+ * reference kernels themselves compiled from source into oracle/_ref/.
+ */
+#ifndef EXA_ORACLE_H
+#define EXA_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* PDE ids: 0 = Euler as in the EulerADERDG demonstrator (outflow boundary),
+ *          1 = the "2.5D" Euler mock of the reference kernel tests (nPar = 1). */
+typedef struct {
+  int dim;   /* 2 or 3 */
+  int order; /* N, basis size N+1 */
+  int pde;
+} orc_solver;
+
+int orc_nvar(const orc_solver* s);
+int orc_npar(const orc_solver* s);
+
+/* spaceTimePredictorNonlinear (+ volumeIntegralNonlinear when lduh != 0).
+ * Optional temporaries in the reference layouts (may be 0):
+ *   lQi[z][y][x][t][nD], lFi[t][z][y][x][d+1][nV], lQhi[z][y][x][nD],
+ *   lFhi[d+1][..][nV] (per-direction transposed blocks).
+ * Returns the number of Picard sweeps executed. */
+int orc_predictor(const orc_solver* s, const double* luh, const double* dx, double dt, double* lQhbnd,
+                  double* lFhbnd, double* lduh, double* lQi, double* lFi, double* lQhi, double* lFhi);
+void orc_volume_integral(const orc_solver* s, double* lduh, const double* lFhi, const double* dx);
+void orc_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, const double* QR, int dir);
+void orc_boundary_face(const orc_solver* s, double* FIn, const double* QIn, const double* centre,
+                       const double* size, double t, double dt, int faceIndex);
+void orc_surface_integral(const orc_solver* s, double* lduh, const double* lFhbnd, const double* dx);
+void orc_solution_update(const orc_solver* s, double* luh, const double* lduh, double dt);
+double orc_stable_dt(const orc_solver* s, const double* luh, const double* dx);
+
+/* PDE hooks */
+void orc_flux(const orc_solver* s, const double* Q, double* F /* [dim][nV] */);
+void orc_eigenvalues(const orc_solver* s, const double* Q, int d, double* lambda);
+
+/* table access (generated dg_tables.h) */
+const double* orc_table(const char* name, int order);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,158 @@
+"""ORACLE -- test infrastructure only. ctypes access to
+
+* ``oracle/lib/liboracle.so``: the plain-C restatement of the reference
+  kernels and the uniform-mesh harness (oracle.c, harness.c), and
+* ``oracle/_ref/libexaref{2d,3d}.so``: the reference's own generic kernels
+  compiled from its sources (oracle/ref/Makefile), when present.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_D)
+
+
+def _pi(a):
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_I)
+
+
+class _Solver(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("order", ctypes.c_int), ("pde", ctypes.c_int)]
+
+
+def build():
+    """Builds liboracle.so (and oracle/_ref when the reference checkout exists)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+    ref = os.environ.get("EXAHYPE_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "ExaHyPE", "kernels")):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "lib", "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _lib = ctypes.CDLL(path)
+        _lib.orc_stable_dt.restype = ctypes.c_double
+        _lib.orc_predictor.restype = ctypes.c_int
+        _lib.orc_table.restype = _D
+        if hasattr(_lib, "orc_mesh_time"):
+            _lib.orc_mesh_time.restype = ctypes.c_double
+            _lib.orc_mesh_dt.restype = ctypes.c_double
+    return _lib
+
+
+_ref = {}
+
+
+def ref_available(dim=2):
+    return os.path.exists(os.path.join(HERE, "_ref", "libexaref%dd.so" % dim))
+
+
+def reflib(dim):
+    if dim not in _ref:
+        l = ctypes.CDLL(os.path.join(HERE, "_ref", "libexaref%dd.so" % dim))
+        getattr(l, "ref%dd_stable_dt" % dim).restype = ctypes.c_double
+        _ref[dim] = l
+    return _ref[dim]
+
+
+class Kernels:
+    """Per-cell / per-face kernels of one (dim, order, pde), either the C
+    restatement (impl='oracle') or the compiled reference (impl='ref')."""
+
+    def __init__(self, dim, order, pde=0, impl="oracle"):
+        self.dim, self.order, self.pde, self.impl = dim, order, pde, impl
+        self.b = order + 1
+        self.nvar = 5
+        self.ndata = 5 + (1 if pde == 1 else 0)
+        self.P = self.b ** dim
+        self.F = self.b ** (dim - 1)
+        self._s = _Solver(dim, order, pde)
+        self._l = lib() if impl == "oracle" else reflib(dim)
+        self._pre = "orc_" if impl == "oracle" else "ref%dd_" % dim
+
+    def _call(self, name, *args):
+        f = getattr(self._l, self._pre + name)
+        if self.impl == "oracle":
+            return f(ctypes.byref(self._s), *args)
+        return f(self.pde, self.order, *args)
+
+    def predictor(self, luh, dx, dt, temps=False):
+        b, P, F, d, nV, nD = self.b, self.P, self.F, self.dim, self.nvar, self.ndata
+        luh = np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        qb = np.zeros(2 * d * F * nD)
+        fb = np.zeros(2 * d * F * nV)
+        du = np.zeros(P * nV)
+        t = [np.zeros(P * b * nD), np.zeros(P * b * (d + 1) * nV), np.zeros(P * nD), np.zeros(P * (d + 1) * nV)]
+        it = self._call("predictor", _p(luh), _p(dx), ctypes.c_double(dt), _p(qb), _p(fb), _p(du),
+                        *[_p(x) for x in t])
+        out = dict(lQhbnd=qb, lFhbnd=fb, lduh=du, iterations=it)
+        if temps:
+            out.update(lQi=t[0], lFi=t[1], lQhi=t[2], lFhi=t[3])
+        return out
+
+    def riemann(self, FL, FR, QL, QR, direction):
+        FL = np.array(FL, dtype=np.float64).reshape(-1)
+        FR = np.array(FR, dtype=np.float64).reshape(-1)
+        QL = np.ascontiguousarray(QL, dtype=np.float64).reshape(-1)
+        QR = np.ascontiguousarray(QR, dtype=np.float64).reshape(-1)
+        if self.impl == "oracle":
+            self._call("riemann", _p(FL), _p(FR), _p(QL), _p(QR), ctypes.c_int(direction))
+        else:
+            self._call("riemann", _p(FL), _p(FR), _p(QL), _p(QR), ctypes.c_double(0.0), ctypes.c_int(direction))
+        return FL, FR
+
+    def surface_integral(self, lduh, lFhbnd, dx):
+        lduh = np.array(lduh, dtype=np.float64).reshape(-1)
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        self._call("surface_integral", _p(lduh), _p(np.ascontiguousarray(lFhbnd, dtype=np.float64).reshape(-1)),
+                   _p(dx))
+        return lduh
+
+    def solution_update(self, luh, lduh, dt):
+        luh = np.array(luh, dtype=np.float64).reshape(-1)
+        self._call("solution_update", _p(luh), _p(np.ascontiguousarray(lduh, dtype=np.float64).reshape(-1)),
+                   ctypes.c_double(dt))
+        return luh
+
+    def stable_dt(self, luh, dx):
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        return self._call("stable_dt", _p(np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)), _p(dx))
+
+    def boundary_face(self, FIn, QIn, face_index, centre=(0.5, 0.5, 0.5), size=(0.1, 0.1, 0.1), t=0.0, dt=0.0):
+        FIn = np.array(FIn, dtype=np.float64).reshape(-1)
+        c = np.ascontiguousarray(np.resize(np.asarray(centre, dtype=np.float64), 3))
+        s = np.ascontiguousarray(np.resize(np.asarray(size, dtype=np.float64), 3))
+        self._call("boundary_face", _p(FIn), _p(np.ascontiguousarray(QIn, dtype=np.float64).reshape(-1)), _p(c),
+                   _p(s), ctypes.c_double(t), ctypes.c_double(dt), ctypes.c_int(face_index))
+        return FIn
+
+
+def table(name, order):
+    """Generated operator table (the same numbers the CUDA path uses)."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(HERE), "exahype_b200", "csrc"))
+    import gen_tables
+    return np.array(gen_tables.build(order)[name])

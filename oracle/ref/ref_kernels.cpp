@@ -1,0 +1,329 @@
+// Oracle-only wrapper: exposes the reference's own generic C++ kernels
+// (ExaHyPE/kernels/...) behind plain C entry points so that the test suite and
+// the CPU baseline can call them. This file is test infrastructure; it is
+// compiled once per dimension (-DDIMENSIONS=2/3) against the unmodified
+// reference sources by oracle/ref/Makefile and never ships with the product.
+//
+// The PDE classes below restate the two PDEs the reference uses for this
+// path:
+//   * EulerDemo  -- Demonstrators/EulerADERDG/MyEulerSolver_ADERDG.cpp:102-160
+//                   (5 variables, gamma 1.4, 3 momentum components in 2D too)
+//   * EulerTest  -- exahype/tests/kernels/c/GenericEulerKernelTest{2D,3D}.cpp:28-77
+//                   ("2.5D" Euler in 2D, one material parameter)
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <set>
+#include <algorithm>
+
+// g++ 13 no longer provides std::abs<double> as a function template that
+// std::transform can take; riemannSolverNonlinear.cpph:70-71 relies on it.
+namespace std {
+template <typename T> inline T abs(T x) { return x < 0 ? -x : x; }
+}
+
+#include "kernels/aderdg/generic/Kernels.h"
+#include "kernels/GaussLegendreQuadrature.h"
+#include "kernels/GaussLobattoQuadrature.h"
+#include "kernels/DGMatrices.h"
+#include "kernels/LimiterProjectionMatrices.h"
+#include "kernels/limiter/generic/Limiter.h"
+#include "kernels/finitevolumes/riemannsolvers/c/riemannsolvers.h"
+#include "kernels/finitevolumes/musclhancock/c/musclhancock.h"
+#include "kernels/finitevolumes/commons/c/commons.h"
+#include "exahype/solvers/ADERDGSolver.h"
+
+#if DIMENSIONS == 2
+#define REFNAME(x) ref2d_##x
+#else
+#define REFNAME(x) ref3d_##x
+#endif
+
+namespace {
+
+// Base for both PDEs: counts flux calls so the driver can report how many
+// Picard sweeps the reference predictor ran (b^(d+1) flux calls per sweep).
+template <int N_, int nPar_>
+struct PDEBase : public exahype::solvers::ADERDGSolver {
+  static constexpr int NumberOfVariables = 5;
+  static constexpr int NumberOfParameters = nPar_;
+  static constexpr int Order = N_;
+  static constexpr double CFL = 0.9;
+  static constexpr int PatchSize = 2 * N_ + 1;
+  static constexpr int GhostLayerWidth = 2;
+  long fluxCalls = 0;
+  int getDMPObservables() const override { return NumberOfVariables; }
+  int getNodesPerCoordinateAxis() const override { return N_ + 1; }
+  int getNumberOfVariables() const override { return NumberOfVariables; }
+  void mapDiscreteMaximumPrincipleObservables(double* obs, const int n, const double* const Q) const override {
+    for (int i = 0; i < NumberOfVariables; ++i) obs[i] = Q[i];
+  }
+  void algebraicSource(const double* const, double* S) { for (int i = 0; i < 5; i++) S[i] = 0.0; }
+  void nonConservativeProduct(const double* const, const double* const, double* B) { for (int i = 0; i < 5; i++) B[i] = 0.0; }
+  void adjustPointSolution(const double* const, const double, const double, double*) {}
+  bool isPhysicallyAdmissible(const double* const, const double* const obsMin, const double* const,
+                              const int, const tarch::la::Vector<DIMENSIONS, double>&,
+                              const tarch::la::Vector<DIMENSIONS, double>&, const double, const double) const {
+    if (obsMin[0] <= 0.0) return false;
+    if (obsMin[4] <= 0.0) return false;
+    return true;
+  }
+};
+
+// Euler as in the demonstrator (pressure from all three momentum components).
+template <int N_>
+struct EulerDemo : public PDEBase<N_, 0> {
+  void flux(const double* const Q, double** F) {
+    this->fluxCalls++;
+    const double GAMMA = 1.4;
+    const double irho = 1. / Q[0];
+    const double jj = Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3];
+    const double p = (GAMMA - 1) * (Q[4] - 0.5 * irho * jj);
+    for (int d = 0; d < DIMENSIONS; d++) {
+      F[d][0] = Q[1 + d];
+      for (int a = 0; a < 3; a++) F[d][1 + a] = irho * (Q[1 + d] * Q[1 + a]) + (d == a ? p : 0.0);
+      F[d][4] = (irho * (Q[4] + p)) * Q[1 + d];
+    }
+  }
+  void eigenvalues(const double* const Q, const int d, double* lambda) {
+    const double GAMMA = 1.4;
+    const double irho = 1. / Q[0];
+    const double jj = Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3];
+    const double p = (GAMMA - 1) * (Q[4] - 0.5 * irho * jj);
+    const double u_n = Q[d + 1] * irho;
+    const double c = std::sqrt(GAMMA * p * irho);
+    lambda[0] = u_n - c;
+    lambda[1] = u_n;
+    lambda[2] = u_n;
+    lambda[3] = u_n;
+    lambda[4] = u_n + c;
+  }
+  // outflow: copy the inside state and flux (ADER-DG hook)
+  void boundaryValues(const double* const, const double, const double, const int, const int,
+                      const double* const fluxIn, const double* const stateIn, double* fluxOut, double* stateOut) {
+    std::copy_n(stateIn, 5, stateOut);
+    std::copy_n(fluxIn, 5, fluxOut);
+  }
+  // outflow (FV hook)
+  void boundaryValues(const double* const, const double, const double, const int, const int,
+                      const double* const stateIn, double* stateOut) {
+    std::copy_n(stateIn, 5, stateOut);
+  }
+  double riemannSolver(double* fL, double* fR, const double* qL, const double* qR, int normalNonZero) {
+    return kernels::finitevolumes::riemannsolvers::c::rusanov<false, true, EulerDemo<N_>>(*this, fL, fR, qL, qR, normalNonZero);
+  }
+};
+
+// The kernel-test mock PDE (2.5D in 2D; one material parameter).
+template <int N_>
+struct EulerTest : public PDEBase<N_, 1> {
+  void flux(const double* const Q, double** F) {
+    this->fluxCalls++;
+    const double GAMMA = 1.4;
+    const double irho = 1.0 / Q[0];
+#if DIMENSIONS == 2
+    const double p = (GAMMA - 1) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2]) * irho);
+#else
+    const double p = (GAMMA - 1) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) * irho);
+#endif
+    for (int d = 0; d < DIMENSIONS; d++) {
+      double* f = F[d];
+      f[0] = Q[1 + d];
+      for (int a = 0; a < 3; a++) f[1 + a] = irho * Q[1 + d] * Q[1 + a] + (d == a ? p : 0.0);
+      f[4] = irho * Q[1 + d] * (Q[4] + p);
+    }
+  }
+  void eigenvalues(const double* const Q, const int d, double* lambda) {
+    const double GAMMA = 1.4;
+    double irho = 1.0 / Q[0];
+#if DIMENSIONS == 2
+    double p = (GAMMA - 1) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2]) * irho);
+#else
+    double p = (GAMMA - 1) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) * irho);
+#endif
+    double u_n = Q[d + 1] * irho;
+    double c = std::sqrt(GAMMA * p * irho);
+    lambda[0] = u_n - c;
+    lambda[1] = u_n;
+    lambda[2] = u_n;
+    lambda[3] = u_n;
+    lambda[4] = u_n + c;
+  }
+  void boundaryValues(const double* const, const double, const double, const int, const int,
+                      const double* const fluxIn, const double* const stateIn, double* fluxOut, double* stateOut) {
+    std::copy_n(stateIn, 6, stateOut);
+    std::copy_n(fluxIn, 5, fluxOut);
+  }
+};
+
+template <int D> using Vec = tarch::la::Vector<D, double>;
+
+Vec<DIMENSIONS> vec(const double* a) {
+  Vec<DIMENSIONS> v;
+  for (int d = 0; d < DIMENSIONS; d++) v[d] = a[d];
+  return v;
+}
+
+constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+// ---- per-cell kernel drivers ------------------------------------------------
+template <class S>
+int predictor(const double* luh, const double* dxa, double dt, double* lQhbnd, double* lFhbnd, double* lduh,
+              double* lQi_out, double* lFi_out, double* lQhi_out, double* lFhi_out) {
+  constexpr int b = S::Order + 1;
+  constexpr int nV = S::NumberOfVariables, nD = nV + S::NumberOfParameters;
+  constexpr int st = ipow(b, DIMENSIONS + 1);
+  constexpr int sp = ipow(b, DIMENSIONS);
+  static thread_local double lQi[st * nD], rhs[st * nD], lFi[st * (DIMENSIONS + 1) * nV], gradQ[st * DIMENSIONS * nV];
+  static thread_local double lQhi[sp * nD], lFhi[sp * (DIMENSIONS + 1) * nV];
+  double* stu[2] = {lQi, rhs};
+  double* stf[2] = {lFi, gradQ};
+  std::fill_n(lFi, st * (DIMENSIONS + 1) * nV, 0.0);
+  S s;
+  kernels::aderdg::generic::c::spaceTimePredictorNonlinear<false, true, false, false, S>(
+      s, lQhbnd, lFhbnd, stu, stf, lQhi, lFhi, luh, vec(dxa), dt);
+  if (lduh) kernels::aderdg::generic::c::volumeIntegralNonlinear<false, true, false, nV, b>(lduh, lFi, lFhi, vec(dxa));
+  if (lQi_out) std::copy_n(lQi, st * nD, lQi_out);
+  if (lFi_out) std::copy_n(lFi, st * (DIMENSIONS + 1) * nV, lFi_out);
+  if (lQhi_out) std::copy_n(lQhi, sp * nD, lQhi_out);
+  if (lFhi_out) std::copy_n(lFhi, sp * (DIMENSIONS + 1) * nV, lFhi_out);
+  return (int)(s.fluxCalls / st);
+}
+
+template <class S>
+void riemann(double* FL, double* FR, const double* QL, const double* QR, double dt, int dir) {
+  S s;
+  kernels::aderdg::generic::c::riemannSolverNonlinear<false, S>(s, FL, FR, QL, QR, dt, dir);
+}
+
+// ADERDGSolver::applyBoundaryConditions (exahype/solvers/ADERDGSolver.cpp:2893-2962)
+template <class S>
+void boundary_face(double* FIn, const double* QIn, const double* centre, const double* size, double t, double dt,
+                   int faceIndex) {
+  constexpr int b = S::Order + 1;
+  constexpr int nV = S::NumberOfVariables, nD = nV + S::NumberOfParameters;
+  constexpr int nf = ipow(b, DIMENSIONS - 1);
+  double QOut[nf * nD], FOut[nf * nV];
+  S s;
+  const int dir = (faceIndex - faceIndex % 2) / 2;
+  kernels::aderdg::generic::c::boundaryConditions<S>(s, FOut, QOut, FIn, QIn, vec(centre), vec(size), t, dt,
+                                                      faceIndex, dir);
+  if (faceIndex % 2 == 0)
+    kernels::aderdg::generic::c::riemannSolverNonlinear<false, S>(s, FOut, FIn, QOut, QIn, dt, dir);
+  else
+    kernels::aderdg::generic::c::riemannSolverNonlinear<false, S>(s, FIn, FOut, QIn, QOut, dt, dir);
+}
+
+template <class S>
+void surface(double* lduh, const double* lFhbnd, const double* dxa) {
+  kernels::aderdg::generic::c::surfaceIntegralNonlinear<S::NumberOfVariables, S::Order + 1>(lduh, lFhbnd, vec(dxa));
+}
+
+template <class S>
+void update(double* luh, const double* lduh, double dt) {
+  S s;
+  kernels::aderdg::generic::c::solutionUpdate<S>(s, luh, lduh, dt);
+}
+
+template <class S>
+double stable_dt(const double* luh, const double* dxa) {
+  S s;
+  return kernels::aderdg::generic::c::stableTimeStepSize<S>(s, luh, vec(dxa));
+}
+
+}  // namespace
+
+#define DISPATCH(pde, N, call)                                              \
+  do {                                                                      \
+    if (pde == 0) {                                                         \
+      switch (N) {                                                          \
+        case 3: { typedef EulerDemo<3> S; call; } break;                    \
+        case 4: { typedef EulerDemo<4> S; call; } break;                    \
+        case 5: { typedef EulerDemo<5> S; call; } break;                    \
+        case 7: { typedef EulerDemo<7> S; call; } break;                    \
+        default: std::fprintf(stderr, "ref: order %d not built\n", N);     \
+      }                                                                     \
+    } else {                                                                \
+      switch (N) {                                                          \
+        case 3: { typedef EulerTest<3> S; call; } break;                    \
+        case 5: { typedef EulerTest<5> S; call; } break;                    \
+        default: std::fprintf(stderr, "ref: order %d not built\n", N);     \
+      }                                                                     \
+    }                                                                       \
+  } while (0)
+
+extern "C" {
+
+void REFNAME(init)() {
+  static bool done = false;
+  if (done) return;
+  std::set<int> orders;
+  kernels::initGaussLegendreNodesAndWeights(orders);
+  kernels::initGaussLobattoNodesAndWeights(orders);
+  kernels::initDGMatrices(orders);
+  kernels::initLimiterProjectionMatrices(orders);
+  done = true;
+}
+
+// Copies one of the reference's operator tables for order N into out.
+// Returns the number of doubles written, or -1 for an unknown name.
+int REFNAME(table)(const char* name, int N, double* out) {
+  REFNAME(init)();
+  const int b = N + 1, bl = 2 * N + 1;
+  int k = 0;
+  if (!std::strcmp(name, "weights")) { for (int i = 0; i < b; i++) out[k++] = kernels::gaussLegendreWeights[N][i]; }
+  else if (!std::strcmp(name, "nodes")) { for (int i = 0; i < b; i++) out[k++] = kernels::gaussLegendreNodes[N][i]; }
+  else if (!std::strcmp(name, "lobatto_nodes")) { for (int i = 0; i < b; i++) out[k++] = kernels::gaussLobattoNodes[N][i]; }
+  else if (!std::strcmp(name, "lobatto_weights")) { for (int i = 0; i < b; i++) out[k++] = kernels::gaussLobattoWeights[N][i]; }
+  else if (!std::strcmp(name, "FLCoeff")) { for (int i = 0; i < b; i++) out[k++] = kernels::FLCoeff[N][i]; }
+  else if (!std::strcmp(name, "FRCoeff")) { for (int i = 0; i < b; i++) out[k++] = kernels::FRCoeff[N][i]; }
+  else if (!std::strcmp(name, "FCoeff")) { for (int s = 0; s < 2; s++) for (int i = 0; i < b; i++) out[k++] = kernels::FCoeff[N][s][i]; }
+  else if (!std::strcmp(name, "Kxi")) { for (int i = 0; i < b; i++) for (int j = 0; j < b; j++) out[k++] = kernels::Kxi[N][i][j]; }
+  else if (!std::strcmp(name, "iK1")) { for (int i = 0; i < b; i++) for (int j = 0; j < b; j++) out[k++] = kernels::iK1[N][i][j]; }
+  else if (!std::strcmp(name, "dudx")) { for (int i = 0; i < b; i++) for (int j = 0; j < b; j++) out[k++] = kernels::dudx[N][i][j]; }
+  else if (!std::strcmp(name, "uh2lim")) { for (int i = 0; i < b * bl; i++) out[k++] = kernels::uh2lim[N][i]; }
+  else if (!std::strcmp(name, "lim2uh")) { for (int i = 0; i < b * bl; i++) out[k++] = kernels::lim2uh[N][i]; }
+  else if (!std::strcmp(name, "uh2lob")) { for (int i = 0; i < b * b; i++) out[k++] = kernels::uh2lob[N][i]; }
+  else return -1;
+  return k;
+}
+
+int REFNAME(predictor)(int pde, int N, const double* luh, const double* dx, double dt, double* lQhbnd,
+                       double* lFhbnd, double* lduh, double* lQi, double* lFi, double* lQhi, double* lFhi) {
+  REFNAME(init)();
+  int it = -1;
+  DISPATCH(pde, N, it = predictor<S>(luh, dx, dt, lQhbnd, lFhbnd, lduh, lQi, lFi, lQhi, lFhi));
+  return it;
+}
+
+void REFNAME(riemann)(int pde, int N, double* FL, double* FR, const double* QL, const double* QR, double dt,
+                      int dir) {
+  REFNAME(init)();
+  DISPATCH(pde, N, riemann<S>(FL, FR, QL, QR, dt, dir));
+}
+
+void REFNAME(boundary_face)(int pde, int N, double* FIn, const double* QIn, const double* centre,
+                            const double* size, double t, double dt, int faceIndex) {
+  REFNAME(init)();
+  DISPATCH(pde, N, boundary_face<S>(FIn, QIn, centre, size, t, dt, faceIndex));
+}
+
+void REFNAME(surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx) {
+  REFNAME(init)();
+  DISPATCH(pde, N, surface<S>(lduh, lFhbnd, dx));
+}
+
+void REFNAME(solution_update)(int pde, int N, double* luh, const double* lduh, double dt) {
+  REFNAME(init)();
+  DISPATCH(pde, N, update<S>(luh, lduh, dt));
+}
+
+double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx) {
+  REFNAME(init)();
+  double r = -1;
+  DISPATCH(pde, N, r = stable_dt<S>(luh, dx));
+  return r;
+}
+
+}  // extern "C"
