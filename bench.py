@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the ADER-DG hot path on B200.
+
+Workload: 3D compressible Euler, ADER-DG order N=5 (6^3 Gauss-Legendre nodes
+per cell), uniform 27^3 cells on the periodic unit cube, four seeded Gaussian
+density pulses on rho = 1, one seeded velocity, p = 1 (seed 0). One bench step
+is one non-fused ADER-DG time step over the whole mesh: Rusanov fluxes on all
+faces, surface integral + solution update + admissible step (min-reduced on
+the device), space-time predictor + volume integral with the new step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). Under torchrun every rank runs an independent
+replica of the workload (the solver is single-GPU; replicas only).
+Metric: DoF-updates/s, one DoF-update = one (cell, node, conserved variable)
+advanced by one step (ncells * 216 * 5 per step).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+DIM, ORDER, CELLS, SEED = 3, 5, (27, 27, 27), 0
+NVAR = 5
+WORKLOAD = "euler3d_N5_27^3_periodic_4pulses"
+METRIC = "ADER-DG DoF-updates/s (FP64, 3D Euler N=5, 27^3 periodic)"
+
+
+def dof_per_step():
+    return int(np.prod(CELLS)) * (ORDER + 1) ** DIM * NVAR
+
+
+def flux_flops(dim):
+    # Euler flux at one node (pde.cuh EulerPDE::flux): 1/rho, |j|^2, p, (E+p)/rho,
+    # and per direction 1 + 3*2 (+1 on the diagonal) + 1 products/sums
+    return 1 + 5 + 4 + 2 + dim * 9
+
+
+def predictor_flops(dim, N, sweeps, ncells, nV=NVAR):
+    """Algorithmic FLOPs of spaceTimePredictor + volumeIntegral (padding and
+    idle lanes not counted): per Picard sweep per cell
+    2 d nV b^(d+2) (derivatives) + 2 nV b^(d+2) (iK1) + 2 nV b^(d+1) (rhs0)
+    + b^(d+1) flux evaluations; per cell once: time averaging +
+    extrapolation 2(d+2) nV b^(d+1) + 8 d nV b^d, volume integral 2 d nV b^(d+1)."""
+    b = N + 1
+    per_sweep = 2 * dim * nV * b ** (dim + 2) + 2 * nV * b ** (dim + 2) + 2 * nV * b ** (dim + 1) \
+        + b ** (dim + 1) * flux_flops(dim)
+    per_cell = 2 * (dim + 2) * nV * b ** (dim + 1) + 8 * dim * nV * b ** dim + 2 * dim * nV * b ** (dim + 1)
+    return per_sweep * sweeps + per_cell * ncells
+
+
+def bytes_per_step(dim, N, ncells, nV=NVAR, nD=NVAR):
+    """compulsory HBM bytes of each phase per step (FP64)"""
+    b = N + 1
+    P, F = b ** dim, b ** (dim - 1)
+    pred = 8 * ncells * (P * nD + 2 * dim * F * (nD + nV) + P * nV)
+    riem = 8 * ncells * dim * (2 * F * nD + 4 * F * nV)
+    corr = 8 * ncells * (2 * P * nD + P * nV + 2 * dim * F * nV)
+    return dict(predictor=pred, riemann=riem, corrector=corr)
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return dict(hbm_gbs=j.get("hbm_gbs", 6650.0), src="measured")
+    return dict(hbm_gbs=6650.0, src="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (median SM clock, reasons)."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return dict(sm_mhz=float(np.median(sm)), sm_max_mhz=mx, reasons=sorted(reasons), samples=len(sm))
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def cpu_reference_run(steps, warmup, nthreads, cells=CELLS):
+    """The reference's own generic kernels (compiled from its sources into
+    oracle/_ref) driven by the oracle harness on the host cores."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle
+    from exahype_b200 import problems
+    if not pyoracle.ref_available(DIM):
+        return None
+    u, _ = problems.gaussian_pulses_3d(ORDER, cells, seed=SEED)
+    m = pyoracle.Mesh(DIM, ORDER, cells, [1.0] * DIM, -1, impl="ref", nthreads=nthreads)
+    m.set_solution(u)
+    m.init(0.0)
+    if warmup:
+        m.step(warmup)
+    t0 = time.perf_counter()
+    m.step(steps)
+    el = time.perf_counter() - t0
+    dof = int(np.prod(cells)) * (ORDER + 1) ** DIM * NVAR * steps
+    return dict(value=dof / el, seconds=el, steps=steps, cells=list(cells))
+
+
+def run_reference_arm(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    r = cpu_reference_run(a.steps, a.warmup, nthreads)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference kernels built from the "
+                          "reference sources) is not present in this tree"}))
+        return 0
+    ms = 1000.0 * r["seconds"] / a.steps
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "DoF-updates/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian pulses)",
+        "config": {"workload": WORKLOAD, "dim": DIM, "order": ORDER, "cells": list(CELLS),
+                   "dof_per_step": dof_per_step(), "l2": "inputs larger than L2 (170 MB solution)"},
+        "cpu_baseline": {"value": r["value"], "unit": "DoF-updates/s", "cores": nthreads, "kind": "reference",
+                         "sample": "%d full time steps of the 27^3 mesh after %d warm-up steps" % (a.steps,
+                                                                                                  a.warmup)},
+        "e2e": {"value": r["value"], "unit": "DoF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(a):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    import exahype_b200 as eb
+    from exahype_b200 import problems
+
+    u0, _ = problems.gaussian_pulses_3d(ORDER, CELLS, seed=SEED + rank)
+    s = eb.Solver(DIM, ORDER, eb.PDE_EULER)
+    m = eb.Mesh(s, CELLS, [0.0] * DIM, [1.0] * DIM, eb.BC_PERIODIC)
+    m.set_solution(u0)
+    m.init(0.0)
+    stream = torch.cuda.ExternalStream(m.stream_handle, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    # warm-up
+    m.step(a.warmup)
+    m.synchronize()
+    st0 = m.state()
+    m.phase_times(reset=True)
+    m.set_profiling(True)
+    clk = ClockSampler(local)
+    barrier()
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(a.steps)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clocks = clk.stop()
+    m.set_profiling(False)
+    ms_total = e0.elapsed_time(e1)
+    ph = m.phase_times(reset=True)
+    st1 = m.state()
+    sweeps = st1["picard_sweeps"] - st0["picard_sweeps"]
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+    dof = dof_per_step() * a.steps * world
+    value = dof / (ms_total / 1000.0)
+
+    # roofline of the dominant kernel (predictor + volume integral, FP64 pipe)
+    ncells = int(np.prod(CELLS))
+    pred_ms = ph["predictor"][0] / a.steps
+    pflops = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells)
+    fp64_peak = measure_fp64_peak() if not a.no_fp64_probe else None
+    peaks = load_peaks()
+    byt = bytes_per_step(DIM, ORDER, ncells)
+    kernels = {}
+    for name, bound in (("predictor", "fp64"), ("riemann", "hbm"), ("corrector", "hbm")):
+        t_ms = ph[name][0] / a.steps
+        if bound == "fp64":
+            ach = pflops / (t_ms / 1e3) / 1e12
+            kernels[name] = dict(bound="fp64", achieved=ach, unit="TFLOP/s", ms=t_ms,
+                                 peak=fp64_peak, frac=(ach / fp64_peak) if fp64_peak else None)
+        else:
+            ach = byt[name] / (t_ms / 1e3) / 1e9
+            kernels[name] = dict(bound="hbm", achieved=ach, unit="GB/s", ms=t_ms, peak=peaks["hbm_gbs"],
+                                 frac=ach / peaks["hbm_gbs"])
+    roof = dict(kernels["predictor"])
+    roof.update(traffic=None, peak_source="fp64 DFMA probe measured in this run (exa_fp64_peak_probe); "
+                "MEASURED_PEAKS.json has no FP64 figure",
+                algorithmic_flops_per_launch=pflops, picard_sweeps_per_cell=sweeps / a.steps / ncells)
+
+    # end to end through the C ABI: per step, H2D of the solution from pinned
+    # host memory, one time step, D2H of the solution
+    e2e = None
+    if not a.no_e2e:
+        nbytes = int(np.prod(m.solution_shape)) * 8
+        pin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+        pin.numpy()[:] = m.get_solution().reshape(-1)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ke = max(1, min(a.steps, 10))
+        f0.record(stream)
+        for _ in range(ke):
+            m.upload_solution_async(pin.data_ptr(), nbytes)
+            m.step(1)
+            m.download_solution_async(pin.data_ptr(), nbytes)
+        f1.record(stream)
+        f1.synchronize()
+        e2e_ms = f0.elapsed_time(f1)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": dof_per_step() * ke * world / (e2e_ms / 1e3), "unit": "DoF-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ke,
+               "api": "exa_mesh_copy_solution(H2D) + exa_mesh_step(1) + exa_mesh_copy_solution(D2H)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        r = cpu_reference_run(1, 0, nthreads)
+        if r is not None:
+            cpu = {"value": r["value"], "unit": "DoF-updates/s", "cores": nthreads, "kind": "reference",
+                   "sample": "1 full time step of the 27^3 mesh (after the initial predictor) on the "
+                             "reference's generic kernels, %.1f s" % r["seconds"]}
+    launches = sum(v[1] for v in ph.values())
+    line = {
+        "metric": METRIC, "value": value, "unit": "DoF-updates/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian pulses)",
+        "config": {"workload": WORKLOAD, "dim": DIM, "order": ORDER, "cells": list(CELLS),
+                   "dof_per_step": dof_per_step(), "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
+        "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
+        "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def measure_fp64_peak():
+    import ctypes
+    import exahype_b200 as eb
+    out = ctypes.c_double()
+    lib = eb.load()
+    if not hasattr(lib, "exa_fp64_peak_probe"):
+        return None
+    if lib.exa_fp64_peak_probe(ctypes.byref(out)) != 0:
+        return None
+    return out.value
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-probe", action="store_true")
+    a = ap.parse_args()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

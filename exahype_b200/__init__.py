@@ -1,0 +1,236 @@
+"""exahype_b200: B200 (sm_100a) ADER-DG hot path of ExaHyPE behind a C ABI.
+
+This module is a thin ctypes binding of ``include/exahype_b200.h``; every call
+runs the CUDA kernels of ``lib/libexahype_b200.so``. There is no CPU path: if
+the library is missing or fails to load, :func:`load` raises.
+
+Two levels, mirroring the reference:
+
+* :class:`Solver` -- the kernel calls of the reference's generated solver glue
+  (``spaceTimePredictor``, ``riemannSolver``, ``boundaryConditions``,
+  ``surfaceIntegral`` + ``solutionUpdate`` + ``stableTimeStepSize``), batched
+  over many cells/faces, on device buffers (torch CUDA tensors or raw device
+  pointers).
+* :class:`Mesh` -- a uniform Cartesian mesh with device-resident state driven
+  by the reference's non-fused time step (Riemann, corrector + dt, predictor).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libexahype_b200.so")
+
+PDE_EULER = 0
+PDE_EULER_TEST = 1
+BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE = -1, 0, 1
+
+_lib = None
+
+
+class ExaError(RuntimeError):
+    pass
+
+
+def load():
+    """Loads the CUDA library (building it first if this is a source tree
+    without one). Raises if it cannot be loaded -- there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    try:
+        lib = ctypes.CDLL(LIB_PATH)
+    except OSError as e:
+        raise ExaError("exahype_b200: cannot load %s: %s" % (LIB_PATH, e))
+    lib.exa_last_error.restype = ctypes.c_char_p
+    lib.exa_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise ExaError("%s failed (%d): %s" % (what, rc, load().exa_last_error().decode()))
+
+
+def _ptr(x):
+    """device pointer of a torch tensor / int / None"""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    return ctypes.c_void_p(x.data_ptr())
+
+
+def _dbl3(v):
+    a = (ctypes.c_double * 3)()
+    for i, x in enumerate(v):
+        a[i] = float(x)
+    return a
+
+
+def _stream(stream):
+    if stream is None:
+        try:
+            import torch
+            return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            return None
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Solver:
+    """Kernel set for one (dim, order, pde) -- the ADERDGSolver of the reference."""
+
+    def __init__(self, dim, order, pde=PDE_EULER):
+        lib = load()
+        h = ctypes.c_void_p()
+        _check(lib.exa_solver_create(int(dim), int(order), int(pde), ctypes.byref(h)), "exa_solver_create")
+        self._h = h
+        self.dim, self.order, self.pde = dim, order, pde
+        z = (ctypes.c_int * 4)()
+        _check(lib.exa_solver_sizes(h, z), "exa_solver_sizes")
+        self.unknowns_per_cell, self.data_per_cell, self.data_per_face, self.fluxes_per_face = list(z)
+        self.nvar = 5
+        self.ndata = self.data_per_cell // (order + 1) ** dim
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().exa_solver_destroy(self._h)
+        except Exception:
+            pass
+
+    # -- reference kernel calls, batched over cells/faces (device buffers) --
+    def space_time_predictor(self, luh, lQhbnd, lFhbnd, lduh, dt_dev, dx, ncells, cell_list=None, iterations=None,
+                             stream=None):
+        _check(load().exa_space_time_predictor_nonlinear(
+            self._h, _ptr(luh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(lduh), _ptr(dt_dev), _dbl3(dx), int(ncells),
+            _ptr(cell_list), _ptr(iterations), _stream(stream)), "exa_space_time_predictor_nonlinear")
+
+    def space_time_predictor_temps(self, luh, lQhbnd, lFhbnd, lduh, dt_dev, dx, ncells, iterations, lQi, lFi, lQhi,
+                                   lFhi, stream=None):
+        _check(load().exa_space_time_predictor_nonlinear_temps(
+            self._h, _ptr(luh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(lduh), _ptr(dt_dev), _dbl3(dx), int(ncells),
+            _ptr(iterations), _ptr(lQi), _ptr(lFi), _ptr(lQhi), _ptr(lFhi), _stream(stream)),
+            "exa_space_time_predictor_nonlinear_temps")
+
+    def riemann_solver(self, lQhbnd, lFhbnd, face_left, face_right, face_dir, nfaces, stream=None):
+        _check(load().exa_riemann_solver_nonlinear(self._h, _ptr(lQhbnd), _ptr(lFhbnd), _ptr(face_left),
+                                                   _ptr(face_right), _ptr(face_dir), int(nfaces), _stream(stream)),
+               "exa_riemann_solver_nonlinear")
+
+    def boundary_conditions(self, lQhbnd, lFhbnd, bcell, bface, nb, kind=BC_OUTFLOW, stream=None):
+        _check(load().exa_boundary_conditions(self._h, _ptr(lQhbnd), _ptr(lFhbnd), _ptr(bcell), _ptr(bface), int(nb),
+                                              int(kind), _stream(stream)), "exa_boundary_conditions")
+
+    def corrector(self, luh, lduh, lFhbnd, dt_dev, dt_min_dev, dx, ncells, cell_list=None, update=True, stream=None):
+        _check(load().exa_corrector(self._h, _ptr(luh), _ptr(lduh), _ptr(lFhbnd), _ptr(dt_dev), _ptr(dt_min_dev),
+                                    _dbl3(dx), int(ncells), _ptr(cell_list), int(bool(update)), _stream(stream)),
+               "exa_corrector")
+
+    @staticmethod
+    def reset_min(dev, stream=None):
+        _check(load().exa_reset_min(_ptr(dev), _stream(stream)), "exa_reset_min")
+
+
+class Mesh:
+    """Uniform Cartesian mesh with device-resident ADER-DG state."""
+
+    def __init__(self, solver, cells, offset, size, bc):
+        lib = load()
+        d = solver.dim
+        c = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        o = _dbl3(list(offset) + [0.0] * (3 - len(offset)))
+        s = _dbl3(list(size) + [1.0] * (3 - len(size)))
+        if isinstance(bc, int):
+            bc = [bc] * (2 * d)
+        b = (ctypes.c_int * 6)(*(list(bc) + [0] * (6 - len(bc))))
+        h = ctypes.c_void_p()
+        _check(lib.exa_mesh_create(solver._h, c, o, s, b, ctypes.byref(h)), "exa_mesh_create")
+        self._h = h
+        self.solver = solver
+        self.cells = tuple(cells)
+        n = ctypes.c_int()
+        _check(lib.exa_mesh_num_cells(h, ctypes.byref(n)), "exa_mesh_num_cells")
+        self.ncells = n.value
+        self.dx = [size[i] / cells[i] for i in range(d)]
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().exa_mesh_destroy(self._h)
+        except Exception:
+            pass
+
+    @property
+    def solution_shape(self):
+        s = self.solver
+        return (self.ncells, (s.order + 1) ** s.dim, s.ndata)
+
+    def set_solution(self, luh):
+        a = np.ascontiguousarray(luh, dtype=np.float64)
+        assert a.size == int(np.prod(self.solution_shape))
+        _check(load().exa_mesh_set_solution(self._h, a.ctypes.data_as(ctypes.c_void_p)), "exa_mesh_set_solution")
+
+    def get_solution(self):
+        a = np.empty(self.solution_shape, dtype=np.float64)
+        _check(load().exa_mesh_get_solution(self._h, a.ctypes.data_as(ctypes.c_void_p)), "exa_mesh_get_solution")
+        return a
+
+    def init(self, t0=0.0):
+        _check(load().exa_mesh_init(self._h, ctypes.c_double(t0)), "exa_mesh_init")
+
+    def step(self, nsteps=1):
+        _check(load().exa_mesh_step(self._h, int(nsteps)), "exa_mesh_step")
+
+    def run_until(self, t_end, max_steps=10 ** 9):
+        n = ctypes.c_int()
+        _check(load().exa_mesh_run_until(self._h, ctypes.c_double(t_end), int(max_steps), ctypes.byref(n)),
+               "exa_mesh_run_until")
+        return n.value
+
+    def state(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        st, sw = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(load().exa_mesh_state(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st), ctypes.byref(sw)),
+               "exa_mesh_state")
+        return dict(t=t.value, dt=dt.value, steps=st.value, picard_sweeps=sw.value)
+
+    def synchronize(self):
+        _check(load().exa_mesh_synchronize(self._h), "exa_mesh_synchronize")
+
+    @property
+    def stream_handle(self):
+        """cudaStream_t of the mesh (for torch.cuda.ExternalStream / events)."""
+        h = ctypes.c_void_p()
+        _check(load().exa_mesh_stream(self._h, ctypes.byref(h)), "exa_mesh_stream")
+        return h.value or 0
+
+    def set_profiling(self, on=True):
+        _check(load().exa_mesh_set_profiling(self._h, int(bool(on))), "exa_mesh_set_profiling")
+
+    PHASES = ("predictor", "riemann", "corrector", "bookkeeping")
+
+    def phase_times(self, reset=False):
+        """{phase: (milliseconds, launches)} accumulated while profiling was on."""
+        ms = (ctypes.c_double * 4)()
+        n = (ctypes.c_longlong * 4)()
+        _check(load().exa_mesh_phase_times(self._h, ms, n, int(bool(reset))), "exa_mesh_phase_times")
+        return {p: (ms[i], n[i]) for i, p in enumerate(self.PHASES)}
+
+    def upload_solution_async(self, host_ptr, nbytes):
+        """H2D copy of the solution from a (pinned) host pointer, ordered on the mesh stream."""
+        _check(load().exa_mesh_copy_solution(self._h, ctypes.c_void_p(host_ptr), ctypes.c_size_t(nbytes), 1),
+               "exa_mesh_copy_solution")
+
+    def download_solution_async(self, host_ptr, nbytes):
+        """D2H copy of the solution into a (pinned) host pointer, ordered on the mesh stream."""
+        _check(load().exa_mesh_copy_solution(self._h, ctypes.c_void_p(host_ptr), ctypes.c_size_t(nbytes), 0),
+               "exa_mesh_copy_solution")

@@ -1,0 +1,536 @@
+// ADER-DG cell and face kernels (FP64), one template per (DIM, N, PDE).
+//
+// Layouts in HBM are the reference's per-cell layouts (kernels/KernelUtils.h
+// idx helpers, last index fastest), cells stored back to back:
+//   luh    [cell][z][y][x][nD]          lduh   [cell][z][y][x][nV]
+//   lQhbnd [cell][2*DIM][face node][nD] lFhbnd [cell][2*DIM][face node][nV]
+// Face order 0:-x 1:+x 2:-y 3:+y 4:-z 5:+z; face nodes run over the two other
+// coordinates in (z,y,x) order (kernels/aderdg/generic/Kernels.h:69-74).
+#pragma once
+#include "common.cuh"
+#include "pde.cuh"
+
+namespace exa {
+
+template <int DIM, int N, class PDE>
+struct Shape {
+  static constexpr int b = N + 1;
+  static constexpr int P = ipow(b, DIM);      // nodes per cell
+  static constexpr int F = ipow(b, DIM - 1);  // nodes per face
+  static constexpr int nV = PDE::nVar;
+  static constexpr int nP = PDE::nPar;
+  static constexpr int nD = nV + nP;
+  static constexpr int maxIter = 2 * (N + 1);  // spaceTimePredictorNonlinear.cpph:85
+};
+
+// Cells per block for the one-thread-per-node cell kernels.
+template <int P>
+constexpr int cells_per_block() { return P >= 256 ? 1 : 256 / P; }
+constexpr int pow2ceil(int v) { return v <= 1 ? 1 : 2 * pow2ceil((v + 1) / 2); }
+
+struct Geometry {
+  double dx[3];
+};
+
+// ---------------------------------------------------------------------------
+// Space-time predictor: the discrete Picard iteration of
+// aderPicardLoopNonlinear (3d/spaceTimePredictorNonlinear.cpph:42-329) with
+// the time averaging (:337-409), the boundary extrapolation (:411-528) and
+// volumeIntegralNonlinear (3d/volumeIntegralNonlinear.cpph:135-225) fused into
+// one kernel. One thread owns one spatial node of one cell. Per Picard sweep
+// the time slices are processed one at a time: the slice's fluxes go to shared
+// memory, every thread forms its node's rhs and folds it into its registers
+// through iK1, so only lQi ([P][b][nD]) and one flux slice ([DIM][P][nV]) are
+// resident in shared memory.
+template <int DIM, int N, class PDE>
+struct PredictorCfg : Shape<DIM, N, PDE> {
+  using S = Shape<DIM, N, PDE>;
+  static constexpr int CPB = cells_per_block<S::P>();
+  static constexpr int THREADS = CPB * S::P;
+  static constexpr int SQ = S::P * S::b * S::nD;  // lQi per cell
+  static constexpr int SF = DIM * S::P * S::nV;   // one flux slice per cell
+  static constexpr int SR = pow2ceil(S::P);       // residual reduction per cell
+  static constexpr int SK = S::b * S::b;          // Kxi copy (per block)
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR) + SK);
+};
+
+struct PredictorTemps {  // optional reference-layout temporaries (golden replay)
+  double *lQi, *lFi, *lQhi, *lFhi;
+};
+
+template <int DIM, int N, class PDE, bool TEMPS>
+__global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE>::THREADS)
+    predictor_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
+                     double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
+                     Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp) {
+  using C = PredictorCfg<DIM, N, PDE>;
+  constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD;
+  extern __shared__ double smem[];
+  const OrderTables& T = c_tab[N];
+
+  const int lc = threadIdx.x / P;
+  const int p = threadIdx.x - lc * P;
+  const int slot = blockIdx.x * C::CPB + lc;
+  const bool active = slot < ncells;
+  const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
+
+  double* sQ = smem + lc * C::SQ;
+  double* sF = smem + C::CPB * C::SQ + lc * C::SF;
+  double* sR = smem + C::CPB * (C::SQ + C::SF) + lc * C::SR;
+  double* sK = smem + C::CPB * (C::SQ + C::SF + C::SR);
+  for (int i = threadIdx.x; i < C::SK; i += blockDim.x) sK[i] = T.Kxi[i];
+
+  const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
+  const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
+  const double wpt = wz * wy * wx;  // reference order (w_z w_y) w_x
+  const double iw = 1.0 / wpt;
+  const double dt = *dt_ptr;
+  const double invDx0 = 1.0 / geo.dx[0], invDx1 = 1.0 / geo.dx[1], invDx2 = DIM == 3 ? 1.0 / geo.dx[2] : 0.0;
+
+  double lu[nD];
+  {
+    const double* src = luh + ((size_t)cell * P + p) * nD;
+#pragma unroll
+    for (int v = 0; v < nD; v++) lu[v] = active ? __ldg(src + v) : (v == 0 ? 1.0 : (v == nD - 1 && nD == 5 ? 2.5 : 0.0));
+  }
+  // trivial initial guess lQi(:,t) = luh (:66-82)
+#pragma unroll
+  for (int t = 0; t < b; t++)
+#pragma unroll
+    for (int v = 0; v < nD; v++) sQ[(p * b + t) * nD + v] = lu[v];
+
+  double fh[DIM][nV];
+  bool done = !active;
+  int it_done = 0;
+  for (int iter = 0; iter < C::maxIter; iter++) {
+    double qn[b][nV];
+#pragma unroll
+    for (int l = 0; l < b; l++)
+#pragma unroll
+      for (int v = 0; v < nV; v++) qn[l][v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+#pragma unroll
+      for (int v = 0; v < nV; v++) fh[d][v] = 0.0;
+
+    for (int t = 0; t < b; t++) {
+      __syncthreads();  // previous slice's readers are done with sF
+      if (!done) {
+        double Q[nD];
+#pragma unroll
+        for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+        double Fl[DIM][nV];
+        PDE::template flux<DIM>(Q, Fl);
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int v = 0; v < nV; v++) {
+            sF[(d * P + p) * nV + v] = Fl[d][v];
+            fh[d][v] += Fl[d][v] * T.w[t];
+          }
+        if (TEMPS) {
+          double* dst = tmp.lFi + (((size_t)cell * b + t) * P + p) * (DIM + 1) * nV;
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int v = 0; v < nV; v++) dst[d * nV + v] = Fl[d][v];
+        }
+      }
+      __syncthreads();
+      if (!done) {
+        double rhs[nV];
+        const double r0 = wpt * T.FL[t];
+#pragma unroll
+        for (int v = 0; v < nV; v++) rhs[v] = r0 * lu[v];
+        {  // x derivative (:151-178)
+          const double us = (T.w[t] * wz) * wy * dt * invDx0;
+          const double* Fx = sF + (0 * P + (z * b + y) * b) * nV;
+#pragma unroll
+          for (int v = 0; v < nV; v++)
+#pragma unroll
+            for (int n = 0; n < b; n++) rhs[v] -= us * Fx[n * nV + v] * sK[n * b + x];
+        }
+        {  // y derivative (:180-207)
+          const double us = (T.w[t] * wz) * wx * dt * invDx1;
+          const double* Fy = sF + (1 * P + z * b * b + x) * nV;
+#pragma unroll
+          for (int v = 0; v < nV; v++)
+#pragma unroll
+            for (int n = 0; n < b; n++) rhs[v] -= us * Fy[n * b * nV + v] * sK[n * b + y];
+        }
+        if (DIM == 3) {  // z derivative (:209-236)
+          const double us = (T.w[t] * wy) * wx * dt * invDx2;
+          const double* Fz = sF + (2 * P + y * b + x) * nV;
+#pragma unroll
+          for (int v = 0; v < nV; v++)
+#pragma unroll
+            for (int n = 0; n < b; n++) rhs[v] -= us * Fz[n * b * b * nV + v] * sK[n * b + z];
+        }
+        // discrete time integral (:280-311): lQi_new[l] = sum_t iw rhs[t] iK1[l][t]
+#pragma unroll
+        for (int l = 0; l < b; l++) {
+          const double k1 = T.iK1[l * b + t];
+#pragma unroll
+          for (int v = 0; v < nV; v++) qn[l][v] += iw * rhs[v] * k1;
+        }
+      }
+    }
+    // residual and update of lQi (:282-311)
+    double part = 0.0;
+    if (!done) {
+#pragma unroll
+      for (int l = 0; l < b; l++)
+#pragma unroll
+        for (int v = 0; v < nV; v++) {
+          const double dq = qn[l][v] - sQ[(p * b + l) * nD + v];
+          part += dq * dq;
+          sQ[(p * b + l) * nD + v] = qn[l][v];
+        }
+    }
+    sR[p] = part;
+    if (p < C::SR - P) sR[P + p] = 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int s = C::SR / 2; s > 0; s >>= 1) {
+      if (p < s) sR[p] += sR[p + s];
+      __syncthreads();
+    }
+    const double sq_res = sR[0];
+    if (!done) {
+      it_done = iter + 1;
+      if (sq_res < 1e-7 * 1e-7) done = true;  // exit condition (:315-318)
+    }
+    if (!__syncthreads_or(!done)) break;
+  }
+  if (iters && active && p == 0) iters[cell] = it_done;
+
+  // time averages (:337-409). lQhi from the final lQi, lFhi from the fluxes of
+  // the last sweep (the reference does not re-evaluate F after the last update).
+  double qh[nD];
+#pragma unroll
+  for (int v = 0; v < nD; v++) {
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < b; m++) s += sQ[(p * b + m) * nD + v] * T.w[m];
+    qh[v] = s;
+  }
+  if (TEMPS && active) {
+    double* dq = tmp.lQi + ((size_t)cell * P + p) * b * nD;
+    for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * b * nD + i];
+    for (int v = 0; v < nD; v++) tmp.lQhi[((size_t)cell * P + p) * nD + v] = qh[v];
+    // reference lFhi blocks: x (z,y,x), y (z,x,y), z (y,x,z), then the source block
+    double* fhd = tmp.lFhi + (size_t)cell * (DIM + 1) * P * nV;
+    const int py = DIM == 3 ? (z * b + x) * b + y : x * b + y;
+    const int pz = (y * b + x) * b + z;
+    for (int v = 0; v < nV; v++) {
+      fhd[(0 * P + p) * nV + v] = fh[0][v];
+      fhd[(1 * P + py) * nV + v] = fh[1][v];
+      if (DIM == 3) fhd[(2 * P + pz) * nV + v] = fh[DIM - 1][v];
+      fhd[(DIM * P + p) * nV + v] = 0.0;
+    }
+  }
+  __syncthreads();  // everyone has read its lQi row
+  double* sQh = sQ;  // lQhi [P][nD] reuses the lQi buffer
+#pragma unroll
+  for (int v = 0; v < nD; v++) sQh[p * nD + v] = qh[v];
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+#pragma unroll
+    for (int v = 0; v < nV; v++) sF[(d * P + p) * nV + v] = fh[d][v];
+  __syncthreads();
+  if (!active) return;
+
+  // volume integral at this node (3d/volumeIntegralNonlinear.cpph:135-225)
+  if (lduh) {
+    double du[nV];
+#pragma unroll
+    for (int v = 0; v < nV; v++) du[v] = 0.0;
+    {
+      const double us = (wz * wy) * invDx0;
+      const double* Fx = sF + (0 * P + (z * b + y) * b) * nV;
+#pragma unroll
+      for (int v = 0; v < nV; v++)
+#pragma unroll
+        for (int m = 0; m < b; m++) du[v] += sK[x * b + m] * Fx[m * nV + v] * us;
+    }
+    {
+      const double us = (wz * wx) * invDx1;
+      const double* Fy = sF + (1 * P + z * b * b + x) * nV;
+#pragma unroll
+      for (int v = 0; v < nV; v++)
+#pragma unroll
+        for (int m = 0; m < b; m++) du[v] += sK[y * b + m] * Fy[m * b * nV + v] * us;
+    }
+    if (DIM == 3) {
+      const double us = (wy * wx) * invDx2;
+      const double* Fz = sF + (2 * P + y * b + x) * nV;
+#pragma unroll
+      for (int v = 0; v < nV; v++)
+#pragma unroll
+        for (int m = 0; m < b; m++) du[v] += sK[z * b + m] * Fz[m * b * b * nV + v] * us;
+    }
+    double* dst = lduh + ((size_t)cell * P + p) * nV;
+#pragma unroll
+    for (int v = 0; v < nV; v++) dst[v] = du[v];
+  }
+
+  // boundary extrapolation (3d/spaceTimePredictorNonlinear.cpph:411-528)
+  for (int k = p; k < DIM * F; k += P) {
+    const int dir = k / F, fn = k - dir * F;
+    const int a = DIM == 3 ? fn / b : 0, c = DIM == 3 ? fn % b : fn;
+    // node index of position l along dir on this face line
+    const int base = dir == 0 ? (a * b + c) * b : dir == 1 ? a * b * b + c : a * b + c;
+    const int stride = dir == 0 ? 1 : dir == 1 ? b : b * b;
+    double* qL = lQhbnd + (((size_t)cell * 2 * DIM + 2 * dir) * F + fn) * nD;
+    double* qR = lQhbnd + (((size_t)cell * 2 * DIM + 2 * dir + 1) * F + fn) * nD;
+    double* fL = lFhbnd + (((size_t)cell * 2 * DIM + 2 * dir) * F + fn) * nV;
+    double* fR = lFhbnd + (((size_t)cell * 2 * DIM + 2 * dir + 1) * F + fn) * nV;
+#pragma unroll
+    for (int v = 0; v < nV; v++) {
+      double sl = 0.0, sr = 0.0;
+#pragma unroll
+      for (int l = 0; l < b; l++) {
+        const double f = sF[(dir * P + base + l * stride) * nV + v];
+        sl += f * T.FL[l];
+        sr += f * T.FR[l];
+      }
+      fL[v] = sl;
+      fR[v] = sr;
+    }
+#pragma unroll
+    for (int v = 0; v < nD; v++) {
+      double sl = 0.0, sr = 0.0;
+#pragma unroll
+      for (int l = 0; l < b; l++) {
+        const double q = sQh[(base + l * stride) * nD + v];
+        sl += q * T.FL[l];
+        sr += q * T.FR[l];
+      }
+      qL[v] = sl;
+      qR[v] = sr;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Rusanov flux on interior faces: riemannSolverNonlinear<useNCP=false>
+// (3d/riemannSolverNonlinear.cpph:37-117). One warp per face: weighted face
+// averages of both states by warp-shuffle reduction, one smax per face from
+// the averaged states, then F = (FL+FR)/2 - smax (QR-QL)/2 written to both
+// sides. The face joins cell `left` (its face 2*dir+1) and cell `right` (its
+// face 2*dir).
+template <int DIM, int N, class PDE>
+__device__ __forceinline__ void face_average(const double* Q, int lane, double* avg) {
+  using S = Shape<DIM, N, PDE>;
+  const OrderTables& T = c_tab[N];
+#pragma unroll
+  for (int k = 0; k < S::nD; k++) avg[k] = 0.0;
+  for (int fn = lane; fn < S::F; fn += 32) {
+    const double wf = DIM == 3 ? T.w[fn / S::b] * T.w[fn % S::b] : T.w[fn];
+#pragma unroll
+    for (int k = 0; k < S::nD; k++) avg[k] += wf * Q[fn * S::nD + k];
+  }
+#pragma unroll
+  for (int k = 0; k < S::nD; k++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) avg[k] += __shfl_xor_sync(0xffffffffu, avg[k], o);
+}
+
+template <int DIM, class PDE>
+__device__ __forceinline__ double face_smax(const double* aL, const double* aR, int dir) {
+  double LL[PDE::nVar], LR[PDE::nVar];
+  Hooks<PDE, DIM>::eigenvalues(aL, dir, LL);
+  Hooks<PDE, DIM>::eigenvalues(aR, dir, LR);
+  double sL = fabs(LL[0]), sR = fabs(LR[0]);
+#pragma unroll
+  for (int k = 1; k < PDE::nVar; k++) {
+    if (sL < fabs(LL[k])) sL = fabs(LL[k]);
+    if (sR < fabs(LR[k])) sR = fabs(LR[k]);
+  }
+  return (sL < sR) ? sR : sL;
+}
+
+template <int DIM, int N, class PDE>
+__global__ void __launch_bounds__(128) riemann_kernel(const double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
+                                                      const int* __restrict__ face_left,
+                                                      const int* __restrict__ face_right,
+                                                      const int* __restrict__ face_dir, int nfaces) {
+  using S = Shape<DIM, N, PDE>;
+  constexpr int F = S::F, nV = S::nV, nD = S::nD;
+  const int lane = threadIdx.x & 31;
+  const int f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (f >= nfaces) return;
+  const int cl = face_left[f], cr = face_right[f], dir = face_dir[f];
+  const double* QL = lQhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nD;
+  const double* QR = lQhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nD;
+  double* FL = lFhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nV;
+  double* FR = lFhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nV;
+  double aL[nD], aR[nD];
+  face_average<DIM, N, PDE>(QL, lane, aL);
+  face_average<DIM, N, PDE>(QR, lane, aR);
+  const double smax = face_smax<DIM, PDE>(aL, aR, dir);
+  for (int e = lane; e < F * nV; e += 32) {
+    const int fn = e / nV, k = e - fn * nV;
+    const double r = 0.5 * (FR[e] + FL[e]) - 0.5 * smax * (QR[fn * nD + k] - QL[fn * nD + k]);
+    FL[e] = r;
+    FR[e] = r;
+  }
+}
+
+// Boundary faces: ADERDGSolver::applyBoundaryConditions
+// (exahype/solvers/ADERDGSolver.cpp:2893-2962) -- user boundaryValues at every
+// face node, then the Rusanov flux with the outside state on the outer side
+// (argument order by faceIndex parity). Only the cell's own flux is kept.
+template <int DIM, int N, class PDE>
+__global__ void __launch_bounds__(128) boundary_kernel(const double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
+                                                       const int* __restrict__ bcell, const int* __restrict__ bface,
+                                                       int nb, int kind) {
+  using S = Shape<DIM, N, PDE>;
+  constexpr int F = S::F, nV = S::nV, nD = S::nD;
+  const int lane = threadIdx.x & 31;
+  const int f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (f >= nb) return;
+  const int c = bcell[f], face = bface[f], dir = face >> 1;
+  const double* QIn = lQhbnd + ((size_t)c * 2 * DIM + face) * F * nD;
+  double* FIn = lFhbnd + ((size_t)c * 2 * DIM + face) * F * nV;
+  const OrderTables& T = c_tab[N];
+  double aIn[nD], aOut[nD];
+#pragma unroll
+  for (int k = 0; k < nD; k++) aIn[k] = aOut[k] = 0.0;
+  for (int fn = lane; fn < F; fn += 32) {
+    const double wf = DIM == 3 ? T.w[fn / S::b] * T.w[fn % S::b] : T.w[fn];
+    double qo[nD], fo[nV];
+    PDE::template boundaryValues<DIM>(kind, dir, FIn + fn * nV, QIn + fn * nD, fo, qo);
+#pragma unroll
+    for (int k = 0; k < nD; k++) {
+      aIn[k] += wf * QIn[fn * nD + k];
+      aOut[k] += wf * qo[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < nD; k++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      aIn[k] += __shfl_xor_sync(0xffffffffu, aIn[k], o);
+      aOut[k] += __shfl_xor_sync(0xffffffffu, aOut[k], o);
+    }
+  // riemannSolver(FOut, FIn, QOut, QIn) for even faces, (FIn, FOut, QIn, QOut) for odd
+  const bool even = (face & 1) == 0;
+  const double smax = even ? face_smax<DIM, PDE>(aOut, aIn, dir) : face_smax<DIM, PDE>(aIn, aOut, dir);
+  __syncwarp();
+  for (int fn = lane; fn < F; fn += 32) {
+    double qo[nD], fo[nV];
+    PDE::template boundaryValues<DIM>(kind, dir, FIn + fn * nV, QIn + fn * nD, fo, qo);
+#pragma unroll
+    for (int k = 0; k < nV; k++) {
+      const double fi = FIn[fn * nV + k], qi = QIn[fn * nD + k];
+      FIn[fn * nV + k] = even ? 0.5 * (fi + fo[k]) - 0.5 * smax * (qi - qo[k])
+                              : 0.5 * (fo[k] + fi) - 0.5 * smax * (qo[k] - qi);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Corrector: surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90),
+// solutionUpdate (3d/solutionUpdate.cpph:23-47) and stableTimeStepSize
+// (3d/stableTimeStepSize.cpph:21-63) fused, one thread per node. The new
+// admissible step is min-reduced over the whole launch into *dt_out; the
+// time-step arithmetic uses explicit round-to-nearest operations so that it
+// reproduces the reference's unfused evaluation bit for bit.
+template <int DIM, int N, class PDE>
+struct CorrectorCfg : Shape<DIM, N, PDE> {
+  static constexpr int CPB = cells_per_block<Shape<DIM, N, PDE>::P>();
+  static constexpr int THREADS = CPB * Shape<DIM, N, PDE>::P;
+};
+
+template <int DIM, int N, class PDE>
+__global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
+    corrector_kernel(double* __restrict__ luh, const double* __restrict__ lduh, const double* __restrict__ lFhbnd,
+                     const double* __restrict__ dt_ptr, double* __restrict__ dt_out, Geometry geo, int ncells,
+                     const int* __restrict__ cell_list, int do_update) {
+  using C = CorrectorCfg<DIM, N, PDE>;
+  constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD;
+  const OrderTables& T = c_tab[N];
+  __shared__ double red[32];
+  const int lc = threadIdx.x / P;
+  const int p = threadIdx.x - lc * P;
+  const int slot = blockIdx.x * C::CPB + lc;
+  const bool active = slot < ncells;
+  double dtmin = __longlong_as_double(0x7fefffffffffffffll);  // DBL_MAX
+  if (active) {
+    const int cell = cell_list ? cell_list[slot] : slot;
+    const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
+    const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
+    const double invDx0 = __ddiv_rn(1.0, geo.dx[0]), invDx1 = __ddiv_rn(1.0, geo.dx[1]);
+    const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, geo.dx[2]) : 0.0;
+    double* u = luh + ((size_t)cell * P + p) * nD;
+    double q[nD];
+#pragma unroll
+    for (int v = 0; v < nD; v++) q[v] = u[v];
+    if (do_update) {
+      const double* du_in = lduh + ((size_t)cell * P + p) * nV;
+      const double* Fb = lFhbnd + (size_t)cell * 2 * DIM * F * nV;
+      double du[nV];
+#pragma unroll
+      for (int v = 0; v < nV; v++) du[v] = du_in[v];
+      {
+        const double us = (wz * wy) * invDx0;
+        const int fn = DIM == 3 ? z * b + y : y;
+#pragma unroll
+        for (int v = 0; v < nV; v++)
+          du[v] -= (Fb[(1 * F + fn) * nV + v] * T.FR[x] - Fb[(0 * F + fn) * nV + v] * T.FL[x]) * us;
+      }
+      {
+        const double us = (wz * wx) * invDx1;
+        const int fn = DIM == 3 ? z * b + x : x;
+#pragma unroll
+        for (int v = 0; v < nV; v++)
+          du[v] -= (Fb[(3 * F + fn) * nV + v] * T.FR[y] - Fb[(2 * F + fn) * nV + v] * T.FL[y]) * us;
+      }
+      if (DIM == 3) {
+        const double us = (wy * wx) * invDx2;
+        const int fn = y * b + x;
+#pragma unroll
+        for (int v = 0; v < nV; v++)
+          du[v] -= (Fb[(5 * F + fn) * nV + v] * T.FR[z] - Fb[(4 * F + fn) * nV + v] * T.FL[z]) * us;
+      }
+      const double us = *dt_ptr / (wz * wy * wx);
+#pragma unroll
+      for (int v = 0; v < nV; v++) {
+        q[v] += du[v] * us;
+        u[v] = q[v];
+      }
+    }
+    double den = 0.0;
+    den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 0), invDx0));
+    den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 1), invDx1));
+    if (DIM == 3) den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 2), invDx2));
+    const double dtp = __ddiv_rn(__dmul_rn(0.9, pnpm(N)), den);
+    dtmin = (dtp < dtmin) ? dtp : dtmin;
+  }
+  // block min, then one atomic per block
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, dtmin, o);
+    dtmin = (other < dtmin) ? other : dtmin;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dtmin;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double m = threadIdx.x < nw ? red[threadIdx.x] : __longlong_as_double(0x7fefffffffffffffll);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, m, o);
+      m = (other < m) ? other : m;
+    }
+    if (threadIdx.x == 0 && dt_out) atomic_min_pos_double(dt_out, m);
+  }
+}
+
+// Sets *a = DBL_MAX (start of a min-reduction) and optionally advances the
+// time-stepping scalars on the device so that no host round trip is needed
+// between steps.
+__global__ void reset_min_kernel(double* a) { *a = __longlong_as_double(0x7fefffffffffffffll); }
+
+}  // namespace exa

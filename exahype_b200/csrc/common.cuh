@@ -1,0 +1,44 @@
+// Shared device-side definitions: operator tables in constant memory,
+// compile-time basis sizes and small helpers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dg_tables.h"
+
+namespace exa {
+
+constexpr int kMaxOrder = 9;
+constexpr int kMaxB = kMaxOrder + 1;
+
+// One order's 1-D operators, in constant memory. Layouts follow the reference
+// (kernels/DGMatrices.h:47-80): Kxi[k][l], iK1[l][n] row-major. (dudx is only
+// needed by non-conservative products, which no PDE here uses.)
+struct OrderTables {
+  double w[kMaxB], x[kMaxB], FL[kMaxB], FR[kMaxB];
+  double Kxi[kMaxB * kMaxB], iK1[kMaxB * kMaxB];
+  double lobatto[kMaxB];
+  double uh2lim[kMaxB * (2 * kMaxOrder + 1)];  // [k][i]: DG basis k -> subcell i
+  double lim2uh[(2 * kMaxOrder + 1) * kMaxB];  // [i][j]: subcell i -> DG basis j
+  double uh2lob[kMaxB * kMaxB];                // [j][i]: DG basis j at Lobatto node i
+};
+
+// Filled by upload_tables() (capi.cu) when the first solver is created on a
+// device. The library is one translation unit, so this is the only definition.
+__constant__ OrderTables c_tab[kMaxOrder + 1];
+
+constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+// Minimum-stability constants of stableTimeStepSize (kernels/aderdg/generic/c/3d/stableTimeStepSize.cpph:33-34).
+__host__ __device__ constexpr double pnpm(int N) {
+  return N == 0 ? 1.0 : N == 1 ? 0.33 : N == 2 ? 0.17 : N == 3 ? 0.1 : N == 4 ? 0.069 : N == 5 ? 0.045
+       : N == 6 ? 0.038 : N == 7 ? 0.03 : N == 8 ? 0.02 : 0.015;
+}
+
+// positive doubles order like their bit patterns: a min-reduction over
+// time-step sizes can use an integer atomicMin on the bits.
+__device__ __forceinline__ void atomic_min_pos_double(double* addr, double v) {
+  atomicMin(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+}  // namespace exa

@@ -1,0 +1,104 @@
+"""Seeded synthetic initial conditions for the Euler workloads, evaluated at
+the Gauss-Legendre nodes of every cell (what the reference's
+adjustPointSolution does at t = 0, kernels/aderdg/generic/c/*/solutionAdjustment.cpph).
+
+All workloads are analytic: no dataset is involved. Densities/pressures are
+turned into conserved variables (rho, rho u, E) with gamma = 1.4.
+"""
+import os
+import sys
+
+import numpy as np
+
+GAMMA = 1.4
+_CSRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc")
+
+
+def gl_nodes(order):
+    sys.path.insert(0, _CSRC)
+    try:
+        import gen_tables
+    finally:
+        sys.path.pop(0)
+    return np.array(gen_tables.build(order)["nodes"])
+
+
+def node_coordinates(dim, order, cells, offset=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0)):
+    """(ncells, b^dim, dim) coordinates of every node, cells in x-fastest order,
+    nodes in (z, y, x) order with x fastest."""
+    x = gl_nodes(order)
+    b = order + 1
+    dx = [size[d] / cells[d] for d in range(dim)]
+    if dim == 2:
+        j, i = np.meshgrid(np.arange(cells[1]), np.arange(cells[0]), indexing="ij")
+        cy, cx = j.ravel(), i.ravel()
+        ny, nx = np.meshgrid(x, x, indexing="ij")
+        X = offset[0] + (cx[:, None] + nx.ravel()[None, :]) * dx[0]
+        Y = offset[1] + (cy[:, None] + ny.ravel()[None, :]) * dx[1]
+        return np.stack([X, Y], axis=-1)
+    k, j, i = np.meshgrid(np.arange(cells[2]), np.arange(cells[1]), np.arange(cells[0]), indexing="ij")
+    cz, cy, cx = k.ravel(), j.ravel(), i.ravel()
+    nz, ny, nx = np.meshgrid(x, x, x, indexing="ij")
+    X = offset[0] + (cx[:, None] + nx.ravel()[None, :]) * dx[0]
+    Y = offset[1] + (cy[:, None] + ny.ravel()[None, :]) * dx[1]
+    Z = offset[2] + (cz[:, None] + nz.ravel()[None, :]) * dx[2]
+    assert X.shape[1] == b ** 3
+    return np.stack([X, Y, Z], axis=-1)
+
+
+def conserved(rho, vel, p):
+    """rho: (...), vel: (..., 3), p: (...) -> Q (..., 5)"""
+    Q = np.empty(rho.shape + (5,))
+    Q[..., 0] = rho
+    Q[..., 1:4] = rho[..., None] * vel
+    Q[..., 4] = p / (GAMMA - 1) + 0.5 * rho * np.sum(vel * vel, axis=-1)
+    return Q
+
+
+def _periodic_d2(X, c):
+    d = X - c
+    d -= np.round(d)
+    return np.sum(d * d, axis=-1)
+
+
+def gaussian_pulse_2d(order, cells=(27, 27), seed=0):
+    """rho = 1 + 0.5 exp(-|x - x0|^2 / 0.01), x0 ~ U[0.3, 0.7]^2, u = (1, 1, 0),
+    p = 1 on the periodic unit square (minimum-image distance)."""
+    rng = np.random.default_rng(seed)
+    x0 = rng.uniform(0.3, 0.7, size=2)
+    X = node_coordinates(2, order, cells)
+    rho = 1.0 + 0.5 * np.exp(-_periodic_d2(X, x0) / 0.01)
+    vel = np.broadcast_to(np.array([1.0, 1.0, 0.0]), rho.shape + (3,))
+    return conserved(rho, vel, np.ones_like(rho)), dict(x0=x0.tolist())
+
+
+def gaussian_pulses_3d(order, cells=(27, 27, 27), seed=0, npulses=4):
+    """rho = 1 + sum_k a_k exp(-|x - c_k|^2 / w_k^2), a_k ~ U[0.1, 0.5],
+    w_k ~ U[0.05, 0.15], c_k ~ U[0, 1]^3; one velocity with components
+    U[-0.5, 0.5]; p = 1; periodic unit cube."""
+    rng = np.random.default_rng(seed)
+    amps = rng.uniform(0.1, 0.5, size=npulses)
+    widths = rng.uniform(0.05, 0.15, size=npulses)
+    centres = rng.uniform(0.0, 1.0, size=(npulses, 3))
+    vel0 = rng.uniform(-0.5, 0.5, size=3)
+    X = node_coordinates(3, order, cells)
+    rho = np.ones(X.shape[:-1])
+    for a, w, c in zip(amps, widths, centres):
+        rho += a * np.exp(-_periodic_d2(X, c) / (w * w))
+    vel = np.broadcast_to(vel0, rho.shape + (3,))
+    return conserved(rho, vel, np.ones_like(rho)), dict(amps=amps.tolist(), widths=widths.tolist(),
+                                                        centres=centres.tolist(), velocity=vel0.tolist())
+
+
+def explosion_2d(order, cells=(81, 81), seed=0, radius=0.2):
+    """Circular explosion: inside |x - c| < radius rho = 1, p = 1, outside
+    rho = 0.125, p = 0.1, zero velocity; c ~ U[0.4, 0.6]^2."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.4, 0.6, size=2)
+    X = node_coordinates(2, order, cells)
+    r2 = np.sum((X - c) ** 2, axis=-1)
+    inside = r2 < radius * radius
+    rho = np.where(inside, 1.0, 0.125)
+    p = np.where(inside, 1.0, 0.1)
+    vel = np.zeros(rho.shape + (3,))
+    return conserved(rho, vel, p), dict(centre=c.tolist())

@@ -1,0 +1,148 @@
+/*
+ * exahype_b200 -- C ABI of the B200 ADER-DG hot path.
+ *
+ * Two layers:
+ *  1. Kernel entry points that replace, batched over many cells or faces, the
+ *     calls the reference's generated solver glue makes into its generic
+ *     kernels (Toolkit/src/eu/exahype/solvers/templates/
+ *     AbstractGenericADERDGSolverImplementation.template:46-149, virtuals in
+ *     ExaHyPE/exahype/solvers/ADERDGSolver.h:961-1085). Buffers are device
+ *     pointers in the reference's per-cell layouts (kernels/KernelUtils.h),
+ *     cells stored back to back; calls are ordered on `stream` and never
+ *     allocate.
+ *  2. A uniform-mesh solver (exa_mesh_*) that owns device-resident state and
+ *     sequences the kernels the way the reference's non-fused time step does
+ *     (exahype/runners/Runner.cpp:1116-1162).
+ *
+ * Layouts (N = order, b = N+1, d = dimension, nV = variables, nD = nV + parameters):
+ *   luh    [cell][b^d][nD]            lduh   [cell][b^d][nV]
+ *   lQhbnd [cell][2d][b^(d-1)][nD]    lFhbnd [cell][2d][b^(d-1)][nV]
+ * Face index 0:-x 1:+x 2:-y 3:+y 4:-z 5:+z.
+ *
+ * Every function returns EXA_OK (0) or a negative EXA_ERR_* code; the text of
+ * the last error of the calling thread is available from exa_last_error().
+ */
+#ifndef EXAHYPE_B200_H
+#define EXAHYPE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EXA_OK 0
+#define EXA_ERR_ARG (-1)         /* bad argument (null pointer, size, unsupported order/dimension) */
+#define EXA_ERR_UNSUPPORTED (-2) /* this build has no kernels for the requested combination */
+#define EXA_ERR_CUDA (-3)        /* a CUDA call failed; see exa_last_error() */
+#define EXA_ERR_NOMEM (-4)       /* device allocation failed (mesh creation only) */
+#define EXA_ERR_STATE (-5)       /* call out of order (e.g. step before init) */
+
+/* PDE identifiers. */
+#define EXA_PDE_EULER 0      /* compressible Euler, 5 variables (EulerADERDG demonstrator) */
+#define EXA_PDE_EULER_TEST 1 /* the reference kernel tests' mock Euler with one parameter */
+
+/* Boundary kinds for exa_boundary_conditions / exa_mesh_create. */
+#define EXA_BC_PERIODIC (-1)
+#define EXA_BC_OUTFLOW 0
+#define EXA_BC_REFLECTIVE 1
+
+typedef struct exa_solver exa_solver;
+typedef struct exa_mesh exa_mesh;
+
+const char* exa_last_error(void);
+const char* exa_version(void);
+
+/* Kernel set for one (dimension, order, PDE): ADERDGSolver's constructor
+ * arguments (exahype/solvers/ADERDGSolver.cpp:~430). */
+int exa_solver_create(int dim, int order, int pde, exa_solver** out);
+int exa_solver_destroy(exa_solver* s);
+/* sizes in doubles: [0] unknowns per cell (b^d nV), [1] data per cell (b^d nD),
+ * [2] data per face (b^(d-1) nD), [3] fluxes per face (b^(d-1) nV)
+ * (ADERDGSolver::get{UnknownsPerCell,DataPerCell,BndFaceSize,BndFluxSize}). */
+int exa_solver_sizes(const exa_solver* s, int* sizes4);
+
+/* spaceTimePredictor (Kernels.h:85-95) + volumeIntegral (Kernels.h:104-106)
+ * for ncells cells: reads luh, writes lQhbnd, lFhbnd and, when lduh is not
+ * NULL, the volume integral lduh. dt_dev: device pointer to the predictor
+ * step size. dx: host array of d cell widths. iterations_dev (optional):
+ * per-cell Picard sweep counts. cell_list (optional, device): indices of the
+ * cells to process (ncells entries); NULL processes cells 0..ncells-1. */
+int exa_space_time_predictor_nonlinear(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
+                                       double* lduh, const double* dt_dev, const double* dx, int ncells,
+                                       const int* cell_list, int* iterations_dev, void* stream);
+/* As above, also writing the reference's temporaries per cell (golden-vector
+ * replay): lQi [b^d][b][nD], lFi [b][b^d][d+1][nV] (flux slots only; the
+ * source slot is left untouched), lQhi [b^d][nD], lFhi [d+1][b^d][nV]. */
+int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* luh, double* lQhbnd,
+                                             double* lFhbnd, double* lduh, const double* dt_dev, const double* dx,
+                                             int ncells, int* iterations_dev, double* lQi, double* lFi,
+                                             double* lQhi, double* lFhi, void* stream);
+/* riemannSolver (Kernels.h:136-142) for nfaces interior faces: face f joins
+ * cell face_left[f] (its face 2*dir+1) and face_right[f] (its face 2*dir),
+ * dir = face_dir[f]; the Rusanov flux is written to both cells' lFhbnd slots
+ * (ADERDGSolver::solveRiemannProblemAtInterface, ADERDGSolver.cpp:2789-2866). */
+int exa_riemann_solver_nonlinear(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* face_left,
+                                 const int* face_right, const int* face_dir, int nfaces, void* stream);
+/* boundaryConditions + riemannSolver on boundary faces (ADERDGSolver::
+ * applyBoundaryConditions, ADERDGSolver.cpp:2893-2962): face f is face
+ * bface[f] of cell bcell[f]; kind is EXA_BC_OUTFLOW or EXA_BC_REFLECTIVE. */
+int exa_boundary_conditions(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* bcell,
+                            const int* bface, int nb, int kind, void* stream);
+/* surfaceIntegral (Kernels.h:110-112) + solutionUpdate (Kernels.h:97-98) +
+ * stableTimeStepSize (Kernels.h:155-157) for ncells cells, fused: luh is
+ * advanced by *dt_dev and the minimum admissible step over the cells is
+ * min-combined into *dt_min_dev (initialise it with exa_reset_min). With
+ * update == 0 only the time step of the current luh is computed. */
+int exa_corrector(const exa_solver* s, double* luh, const double* lduh, const double* lFhbnd, const double* dt_dev,
+                  double* dt_min_dev, const double* dx, int ncells, const int* cell_list, int update, void* stream);
+/* *dev = DBL_MAX, ordered on stream. */
+int exa_reset_min(double* dev, void* stream);
+
+/* ---- uniform-mesh solver ------------------------------------------------ */
+/* cells[d]: cells per axis; offset/size[d]: domain; bc[2d]: per domain face
+ * EXA_BC_PERIODIC / EXA_BC_OUTFLOW / EXA_BC_REFLECTIVE (periodic must be set
+ * on both faces of an axis). Allocates all device state. */
+int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset, const double* size, const int* bc,
+                    exa_mesh** out);
+int exa_mesh_destroy(exa_mesh* m);
+int exa_mesh_num_cells(const exa_mesh* m, int* ncells);
+/* host <-> device solution, luh layout above, cells in x-fastest order */
+int exa_mesh_set_solution(exa_mesh* m, const double* luh_host);
+int exa_mesh_get_solution(exa_mesh* m, double* luh_host);
+/* Asynchronous solution copy ordered on the mesh stream: to_device != 0 copies
+ * host -> device, else device -> host. nbytes must equal the solution size;
+ * use page-locked host memory for overlap. */
+int exa_mesh_copy_solution(exa_mesh* m, void* host, size_t nbytes, int to_device);
+/* Sets t = t0, computes the first admissible step from the current solution
+ * and runs the first predictor (Runner::runAsMaster, Runner.cpp:681-700). */
+int exa_mesh_init(exa_mesh* m, double t0);
+/* nsteps non-fused time steps (Riemann, corrector + dt, predictor) without
+ * host synchronisation. */
+int exa_mesh_step(exa_mesh* m, int nsteps);
+/* Steps while t < t_end and dt > 0 (Runner.cpp:708-709; no clamp of the last
+ * step), at most max_steps; returns the steps taken in *steps. */
+int exa_mesh_run_until(exa_mesh* m, double t_end, int max_steps, int* steps);
+/* current time, current (predictor) step size, steps taken, and the total
+ * number of Picard sweeps executed by the predictor so far */
+int exa_mesh_state(exa_mesh* m, double* t, double* dt, long long* steps, long long* picard_sweeps);
+int exa_mesh_synchronize(exa_mesh* m);
+/* the CUDA stream (cudaStream_t) all of the mesh's work is ordered on */
+int exa_mesh_stream(exa_mesh* m, void** stream);
+/* Per-phase device timing with CUDA events recorded on the mesh stream around
+ * every phase of every step (0 disables). exa_mesh_phase_times returns the
+ * accumulated milliseconds and launch counts of phases
+ * 0 predictor+volume, 1 Riemann (interior + boundary), 2 corrector+dt,
+ * 3 bookkeeping, since the last reset (synchronises the stream). */
+int exa_mesh_set_profiling(exa_mesh* m, int on);
+int exa_mesh_phase_times(exa_mesh* m, double* ms4, long long* launches4, int reset);
+
+/* Measurement helper (no counterpart in the reference): sustained FP64 FMA
+ * throughput of the current GPU in TFLOP/s, from independent DFMA chains on
+ * every SM timed with CUDA events -- the FP64 roofline of the predictor. */
+int exa_fp64_peak_probe(double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

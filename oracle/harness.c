@@ -1,1 +1,212 @@
-#include "harness.h"
+/*
+ * ORACLE harness -- test infrastructure only. A uniform Cartesian mesh driven
+ * by the reference's non-fused, globally time-stepped ADER-DG step
+ * (exahype/runners/Runner.cpp:681-709, 1116-1162):
+ *   init:   dt = min over cells of stableTimeStepSize(u0); predictor(u0, dt)
+ *   step:   1. riemannSolver on every interior face, boundaryConditions +
+ *              riemannSolver on every boundary face   (mappings/Merging.cpp)
+ *           2. per cell: surfaceIntegral, solutionUpdate(dt), new admissible
+ *              step from the updated solution           (mappings/SolutionUpdate.cpp)
+ *           3. t += dt; dt = min over cells              (ADERDGSolver.cpp:560-592)
+ *           4. per cell: predictor + volume integral with the new dt
+ *                                                        (mappings/Prediction.cpp)
+ *   loop:   while t < t_end && dt > 0 (no clamp of the last step).
+ * The per-cell / per-face kernels come from a backend table, so the same
+ * sequencing drives both the C restatement and the reference kernels.
+ * Cells run in parallel on `nthreads` POSIX threads.
+ *
+ * This file is #included by the translation unit that defines the backend.
+ */
+#include <float.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+  void* ctx;
+  int dim, order, nvar, ndata;
+  int (*predictor)(void* ctx, const double* luh, const double* dx, double dt, double* lQhbnd, double* lFhbnd,
+                   double* lduh);
+  void (*riemann)(void* ctx, double* FL, double* FR, const double* QL, const double* QR, int dir);
+  void (*boundary_face)(void* ctx, double* FIn, const double* QIn, int faceIndex);
+  void (*surface_integral)(void* ctx, double* lduh, const double* lFhbnd, const double* dx);
+  void (*solution_update)(void* ctx, double* luh, const double* lduh, double dt);
+  double (*stable_dt)(void* ctx, const double* luh, const double* dx);
+} hrn_backend;
+
+typedef struct {
+  hrn_backend k;
+  int dim, cells[3], ncells, P, F, nthreads;
+  double dx[3];
+  int bc[6]; /* -1 periodic, 0 outflow, 1 reflective */
+  double *luh, *lduh, *lQhbnd, *lFhbnd;
+  int *fl, *fr, *fd, nfaces, *bcell, *bface, nb;
+  int* iters;
+  double t, dt;
+  long steps, sweeps;
+} hrn_mesh;
+
+static int hrn_cid(const hrn_mesh* m, int i, int j, int k) { return (k * m->cells[1] + j) * m->cells[0] + i; }
+
+static hrn_mesh* hrn_create(const hrn_backend* k, const int* cells, const double* size, const int* bc, int nthreads) {
+  hrn_mesh* m = (hrn_mesh*)calloc(1, sizeof(hrn_mesh));
+  m->k = *k;
+  m->dim = k->dim;
+  m->nthreads = nthreads < 1 ? 1 : nthreads;
+  int b = k->order + 1;
+  m->P = m->dim == 3 ? b * b * b : b * b;
+  m->F = m->dim == 3 ? b * b : b;
+  m->ncells = 1;
+  for (int d = 0; d < 3; d++) {
+    m->cells[d] = d < m->dim ? cells[d] : 1;
+    m->dx[d] = d < m->dim ? size[d] / cells[d] : 1.0;
+    m->ncells *= m->cells[d];
+  }
+  for (int f = 0; f < 2 * m->dim; f++) m->bc[f] = bc[f];
+  const size_t n = m->ncells;
+  m->luh = (double*)calloc(n * m->P * k->ndata, sizeof(double));
+  m->lduh = (double*)calloc(n * m->P * k->nvar, sizeof(double));
+  m->lQhbnd = (double*)calloc(n * 2 * m->dim * m->F * k->ndata, sizeof(double));
+  m->lFhbnd = (double*)calloc(n * 2 * m->dim * m->F * k->nvar, sizeof(double));
+  m->iters = (int*)calloc(n, sizeof(int));
+  /* face lists in the order the GPU mesh builds them */
+  m->fl = (int*)malloc(sizeof(int) * n * 3);
+  m->fr = (int*)malloc(sizeof(int) * n * 3);
+  m->fd = (int*)malloc(sizeof(int) * n * 3);
+  m->bcell = (int*)malloc(sizeof(int) * n * 6);
+  m->bface = (int*)malloc(sizeof(int) * n * 6);
+  for (int kk = 0; kk < m->cells[2]; kk++)
+    for (int j = 0; j < m->cells[1]; j++)
+      for (int i = 0; i < m->cells[0]; i++) {
+        const int c = hrn_cid(m, i, j, kk);
+        int ijk[3] = {i, j, kk};
+        for (int d = 0; d < m->dim; d++) {
+          int nb[3] = {i, j, kk};
+          nb[d] = ijk[d] + 1;
+          if (nb[d] < m->cells[d] || m->bc[2 * d + 1] == -1) {
+            if (nb[d] >= m->cells[d]) nb[d] = 0;
+            m->fl[m->nfaces] = c;
+            m->fr[m->nfaces] = hrn_cid(m, nb[0], nb[1], nb[2]);
+            m->fd[m->nfaces] = d;
+            m->nfaces++;
+          } else {
+            m->bcell[m->nb] = c;
+            m->bface[m->nb] = 2 * d + 1;
+            m->nb++;
+          }
+          if (ijk[d] == 0 && m->bc[2 * d] != -1) {
+            m->bcell[m->nb] = c;
+            m->bface[m->nb] = 2 * d;
+            m->nb++;
+          }
+        }
+      }
+  return m;
+}
+
+static void hrn_destroy(hrn_mesh* m) {
+  if (!m) return;
+  free(m->luh); free(m->lduh); free(m->lQhbnd); free(m->lFhbnd); free(m->iters);
+  free(m->fl); free(m->fr); free(m->fd); free(m->bcell); free(m->bface);
+  free(m);
+}
+
+/* ---- parallel loops over cells / faces ---- */
+typedef struct {
+  hrn_mesh* m;
+  int phase, lo, hi;
+  double dtmin;
+} hrn_job;
+
+static void hrn_run_range(hrn_job* j) {
+  hrn_mesh* m = j->m;
+  const hrn_backend* k = &m->k;
+  const int P = m->P, F = m->F, nV = k->nvar, nD = k->ndata, D2 = 2 * m->dim;
+  j->dtmin = DBL_MAX;
+  for (int i = j->lo; i < j->hi; i++) {
+    if (j->phase == 0) { /* predictor + volume integral */
+      m->iters[i] = k->predictor(k->ctx, m->luh + (size_t)i * P * nD, m->dx, m->dt, m->lQhbnd + (size_t)i * D2 * F * nD,
+                                 m->lFhbnd + (size_t)i * D2 * F * nV, m->lduh + (size_t)i * P * nV);
+    } else if (j->phase == 1) { /* interior face */
+      const int cl = m->fl[i], cr = m->fr[i], d = m->fd[i];
+      k->riemann(k->ctx, m->lFhbnd + ((size_t)cl * D2 + 2 * d + 1) * F * nV, m->lFhbnd + ((size_t)cr * D2 + 2 * d) * F * nV,
+                 m->lQhbnd + ((size_t)cl * D2 + 2 * d + 1) * F * nD, m->lQhbnd + ((size_t)cr * D2 + 2 * d) * F * nD, d);
+    } else if (j->phase == 2) { /* boundary face */
+      const int c = m->bcell[i], f = m->bface[i];
+      k->boundary_face(k->ctx, m->lFhbnd + ((size_t)c * D2 + f) * F * nV, m->lQhbnd + ((size_t)c * D2 + f) * F * nD, f);
+    } else if (j->phase == 3) { /* corrector + admissible step */
+      double* u = m->luh + (size_t)i * P * nD;
+      double* du = m->lduh + (size_t)i * P * nV;
+      k->surface_integral(k->ctx, du, m->lFhbnd + (size_t)i * D2 * F * nV, m->dx);
+      k->solution_update(k->ctx, u, du, m->dt);
+      const double d = k->stable_dt(k->ctx, u, m->dx);
+      j->dtmin = (d < j->dtmin) ? d : j->dtmin;
+    } else { /* admissible step only */
+      const double d = k->stable_dt(k->ctx, m->luh + (size_t)i * P * nD, m->dx);
+      j->dtmin = (d < j->dtmin) ? d : j->dtmin;
+    }
+  }
+}
+
+static void* hrn_thread(void* a) {
+  hrn_run_range((hrn_job*)a);
+  return 0;
+}
+
+/* runs `phase` over [0, n); returns the min of the per-item step sizes */
+static double hrn_parallel(hrn_mesh* m, int phase, int n) {
+  const int T = m->nthreads < n ? m->nthreads : (n > 0 ? n : 1);
+  hrn_job jobs[256];
+  pthread_t th[256];
+  const int nt = T > 256 ? 256 : T;
+  for (int t = 0; t < nt; t++) {
+    jobs[t].m = m;
+    jobs[t].phase = phase;
+    jobs[t].lo = (int)((long)n * t / nt);
+    jobs[t].hi = (int)((long)n * (t + 1) / nt);
+  }
+  if (nt == 1) {
+    hrn_run_range(&jobs[0]);
+  } else {
+    for (int t = 1; t < nt; t++) pthread_create(&th[t], 0, hrn_thread, &jobs[t]);
+    hrn_run_range(&jobs[0]);
+    for (int t = 1; t < nt; t++) pthread_join(th[t], 0);
+  }
+  double r = DBL_MAX;
+  for (int t = 0; t < nt; t++) r = (jobs[t].dtmin < r) ? jobs[t].dtmin : r;
+  return r;
+}
+
+static void hrn_predict(hrn_mesh* m) {
+  hrn_parallel(m, 0, m->ncells);
+  for (int i = 0; i < m->ncells; i++) m->sweeps += m->iters[i];
+}
+
+static void hrn_init(hrn_mesh* m, double t0) {
+  m->t = t0;
+  m->steps = 0;
+  m->sweeps = 0;
+  m->dt = hrn_parallel(m, 4, m->ncells);
+  hrn_predict(m);
+}
+
+static void hrn_step(hrn_mesh* m, int n) {
+  for (int s = 0; s < n; s++) {
+    hrn_parallel(m, 1, m->nfaces);
+    hrn_parallel(m, 2, m->nb);
+    const double dtn = hrn_parallel(m, 3, m->ncells);
+    m->t += m->dt;
+    m->dt = dtn;
+    m->steps++;
+    hrn_predict(m);
+  }
+}
+
+static int hrn_run_until(hrn_mesh* m, double t_end, int max_steps) {
+  int n = 0;
+  while (n < max_steps && m->t < t_end && m->dt > 0.0) {
+    hrn_step(m, 1);
+    n++;
+  }
+  return n;
+}

@@ -156,3 +156,65 @@ def table(name, order):
     sys.path.insert(0, os.path.join(os.path.dirname(HERE), "exahype_b200", "csrc"))
     import gen_tables
     return np.array(gen_tables.build(order)[name])
+
+
+class Mesh:
+    """Uniform mesh run by the oracle harness (oracle/harness.c) over the C
+    restatement (impl='oracle') or the compiled reference kernels (impl='ref')."""
+
+    def __init__(self, dim, order, cells, size, bc, pde=0, impl="oracle", nthreads=1):
+        self.dim, self.order, self.pde, self.impl = dim, order, pde, impl
+        ci = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        sz = (ctypes.c_double * 3)(*(list(size) + [1.0] * (3 - len(size))))
+        if isinstance(bc, int):
+            bc = [bc] * (2 * dim)
+        b = (ctypes.c_int * 6)(*(list(bc) + [0] * (6 - len(bc))))
+        if impl == "oracle":
+            self._l = lib()
+            self._pre = "orc_mesh_"
+            create = self._l.orc_mesh_create
+            create.restype = ctypes.c_void_p
+            self._h = ctypes.c_void_p(create(dim, order, pde, ci, sz, b, nthreads))
+        else:
+            self._l = reflib(dim)
+            self._pre = "ref%dd_mesh_" % dim
+            create = getattr(self._l, self._pre + "create")
+            create.restype = ctypes.c_void_p
+            self._h = ctypes.c_void_p(create(order, pde, ci, sz, b, nthreads))
+        for nm, rt in (("time", ctypes.c_double), ("dt", ctypes.c_double), ("steps", ctypes.c_long),
+                       ("sweeps", ctypes.c_long), ("run_until", ctypes.c_int)):
+            getattr(self._l, self._pre + nm).restype = rt
+        self.ncells = int(np.prod(cells))
+        self.shape = (self.ncells, (order + 1) ** dim, 5 + (1 if pde == 1 else 0))
+
+    def _f(self, nm):
+        return getattr(self._l, self._pre + nm)
+
+    def __del__(self):
+        try:
+            self._f("destroy")(self._h)
+        except Exception:
+            pass
+
+    def set_solution(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.size == int(np.prod(self.shape))
+        self._f("set_solution")(self._h, _p(u.reshape(-1)))
+
+    def get_solution(self):
+        u = np.empty(self.shape)
+        self._f("get_solution")(self._h, _p(u.reshape(-1)))
+        return u
+
+    def init(self, t0=0.0):
+        self._f("init")(self._h, ctypes.c_double(t0))
+
+    def step(self, n=1):
+        self._f("step")(self._h, int(n))
+
+    def run_until(self, t_end, max_steps=10 ** 9):
+        return self._f("run_until")(self._h, ctypes.c_double(t_end), int(max_steps))
+
+    def state(self):
+        return dict(t=self._f("time")(self._h), dt=self._f("dt")(self._h), steps=self._f("steps")(self._h),
+                    picard_sweeps=self._f("sweeps")(self._h))

@@ -1,0 +1,251 @@
+"""GPU parity of the ADER-DG kernels against the oracle, through the C ABI.
+
+Tolerances: FP64 path, 1e-12 relative (max-norm per array, or relative L2
+for mesh runs) against the C oracle; the reference kernel tests' absolute
+eps 1e-10 against their golden vectors; time-step sizes computed from the
+same solution must be bit-identical; Picard sweep counts must be equal.
+"""
+import numpy as np
+import pytest
+
+import pyoracle
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def eb():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    import exahype_b200
+    exahype_b200.load()
+    return exahype_b200
+
+
+def dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def random_states(rng, n, P, ndata, spread=1.0):
+    u = np.zeros((n, P, ndata))
+    u[..., 0] = 1.0 + 0.3 * spread * rng.random((n, P))
+    u[..., 1:4] = 0.4 * spread * (rng.random((n, P, 3)) - 0.5)
+    u[..., 4] = 2.5 + 0.5 * spread * rng.random((n, P))
+    return u
+
+
+def widen(a, nvar, ndata):
+    a = a.reshape(-1, nvar)
+    out = np.zeros((a.shape[0], ndata))
+    out[:, :nvar] = a
+    return out
+
+
+@pytest.mark.parametrize("dim,dt", [(2, 1.686854344081342e-3), (3, 1.083937460199773e-3)])
+def test_predictor_golden_gpu(eb, golden, dim, dt):
+    """GenericEulerKernelTest{2D,3D}::testSpaceTimePredictorNonlinear replayed on the GPU."""
+    s = eb.Solver(dim, 3, eb.PDE_EULER_TEST)
+    b, nV, nD = 4, 5, 6
+    P, F = b ** dim, b ** (dim - 1)
+    g = "%dd/generic_euler/testSpaceTimePredictorNonlinear/" % dim
+    luh = dev(widen(golden[g + "luh"], 5, 6))
+    qb = torch.zeros(2 * dim * F * nD, device="cuda", dtype=torch.float64)
+    fb = torch.zeros(2 * dim * F * nV, device="cuda", dtype=torch.float64)
+    du = torch.zeros(P * nV, device="cuda", dtype=torch.float64)
+    it = torch.zeros(1, device="cuda", dtype=torch.int32)
+    lQi = torch.zeros(P * b * nD, device="cuda", dtype=torch.float64)
+    lFi = torch.zeros(P * b * (dim + 1) * nV, device="cuda", dtype=torch.float64)
+    lQhi = torch.zeros(P * nD, device="cuda", dtype=torch.float64)
+    lFhi = torch.zeros(P * (dim + 1) * nV, device="cuda", dtype=torch.float64)
+    dtd = dev([dt])
+    s.space_time_predictor_temps(luh, qb, fb, du, dtd, [0.05] * dim, 1, it, lQi, lFi, lQhi, lFhi)
+    eps = 1e-10
+    np.testing.assert_allclose(host(lQi).reshape(-1, nD)[:, :nV].ravel(), golden[g + "lQi"], rtol=0, atol=eps)
+    np.testing.assert_allclose(host(lFi).reshape(-1, dim + 1, nV)[:, :dim].ravel(), golden[g + "lFi"], rtol=0,
+                               atol=eps)
+    np.testing.assert_allclose(host(lQhi).reshape(-1, nD)[:, :nV].ravel(), golden[g + "lQhi"], rtol=0, atol=eps)
+    nflux = dim * nV * P
+    np.testing.assert_allclose(host(lFhi)[:nflux], golden[g + "lFhi"][:nflux], rtol=0, atol=eps)
+    np.testing.assert_allclose(host(qb).reshape(-1, nD)[:, :nV].ravel(), golden[g + "lQhbnd"], rtol=0, atol=eps)
+    np.testing.assert_allclose(host(fb), golden[g + "lFhbnd"], rtol=0, atol=eps)
+    # and against the oracle, tightly
+    o = pyoracle.Kernels(dim, 3, pde=1).predictor(widen(golden[g + "luh"], 5, 6), [0.05] * dim, dt, temps=True)
+    assert host(it)[0] == o["iterations"]
+    assert rel(host(lQi), o["lQi"]) < RTOL
+    assert rel(host(qb), o["lQhbnd"]) < RTOL
+    assert rel(host(fb), o["lFhbnd"]) < RTOL
+    assert rel(host(du), o["lduh"]) < RTOL
+
+
+@pytest.mark.parametrize("dim,order", [(2, 3), (2, 5), (2, 7), (3, 3), (3, 5), (3, 7), (2, 4), (3, 4)])
+def test_predictor_batch_vs_oracle(eb, dim, order):
+    rng = np.random.default_rng(10 * dim + order)
+    s = eb.Solver(dim, order, eb.PDE_EULER)
+    k = pyoracle.Kernels(dim, order, pde=0)
+    b = order + 1
+    P, F, nV, nD = b ** dim, b ** (dim - 1), 5, 5
+    n = 37 if dim == 3 else 101  # not a multiple of the cells-per-block
+    u = random_states(rng, n, P, nD)
+    dx = [0.05, 0.04, 0.03][:dim]
+    dt = 4e-4 if dim == 3 else 1e-3
+    qb = torch.zeros(n * 2 * dim * F * nD, device="cuda", dtype=torch.float64)
+    fb = torch.zeros(n * 2 * dim * F * nV, device="cuda", dtype=torch.float64)
+    du = torch.zeros(n * P * nV, device="cuda", dtype=torch.float64)
+    it = torch.zeros(n, device="cuda", dtype=torch.int32)
+    s.space_time_predictor(dev(u), qb, fb, du, dev([dt]), dx, n, iterations=it)
+    qb, fb, du, it = host(qb).reshape(n, -1), host(fb).reshape(n, -1), host(du).reshape(n, -1), host(it)
+    for c in range(0, n, 7 if dim == 3 else 13):
+        o = k.predictor(u[c], dx, dt)
+        assert it[c] == o["iterations"], (c, it[c], o["iterations"])
+        assert rel(qb[c], o["lQhbnd"]) < RTOL
+        assert rel(fb[c], o["lFhbnd"]) < RTOL
+        assert rel(du[c], o["lduh"]) < RTOL
+
+
+def test_predictor_cell_list(eb):
+    """only the listed cells are processed (the limiter's gating of troubled cells)"""
+    rng = np.random.default_rng(3)
+    s = eb.Solver(2, 3, eb.PDE_EULER)
+    n, P, F = 20, 16, 4
+    u = random_states(rng, n, P, 5)
+    lst = np.array([3, 7, 8, 19], dtype=np.int32)
+    qb = torch.full((n * 4 * F * 5,), -7.0, device="cuda", dtype=torch.float64)
+    fb = torch.zeros(n * 4 * F * 5, device="cuda", dtype=torch.float64)
+    du = torch.zeros(n * P * 5, device="cuda", dtype=torch.float64)
+    s.space_time_predictor(dev(u), qb, fb, du, dev([1e-3]), [0.05, 0.05], len(lst), cell_list=dev(lst, torch.int32))
+    qb = host(qb).reshape(n, -1)
+    k = pyoracle.Kernels(2, 3, pde=0)
+    for c in range(n):
+        if c in lst:
+            assert rel(qb[c], k.predictor(u[c], [0.05, 0.05], 1e-3)["lQhbnd"]) < RTOL
+        else:
+            assert np.all(qb[c] == -7.0)
+
+
+@pytest.mark.parametrize("dim,order", [(2, 3), (2, 5), (3, 3), (3, 5), (3, 7)])
+def test_riemann_and_boundary_vs_oracle(eb, dim, order):
+    rng = np.random.default_rng(dim * 100 + order)
+    s = eb.Solver(dim, order, eb.PDE_EULER)
+    k = pyoracle.Kernels(dim, order, pde=0)
+    b = order + 1
+    F, nV, nD, D2 = b ** (dim - 1), 5, 5, 2 * dim
+    n = 11
+    qb = random_states(rng, n * D2, F, nD).reshape(n, D2, F, nD)
+    fb = rng.standard_normal((n, D2, F, nV))
+    fl = np.array([0, 1, 2, 5, 9], dtype=np.int32)
+    fr = np.array([1, 2, 3, 6, 0], dtype=np.int32)
+    fd = np.array([0, 1, dim - 1, 0, 1], dtype=np.int32)
+    fbd = dev(fb)
+    s.riemann_solver(dev(qb), fbd, dev(fl, torch.int32), dev(fr, torch.int32), dev(fd, torch.int32), len(fl))
+    # boundary faces on cells that no interior face touches
+    bc = np.array([4, 7, 8], dtype=np.int32)
+    bf = np.array([0, 2 * dim - 1, 3], dtype=np.int32)
+    s.boundary_conditions(dev(qb), fbd, dev(bc, torch.int32), dev(bf, torch.int32), len(bc), eb.BC_OUTFLOW)
+    got = host(fbd).reshape(n, D2, F, nV)
+    exp = fb.copy()
+    for l, r, d in zip(fl, fr, fd):
+        FL, FR = k.riemann(exp[l, 2 * d + 1], exp[r, 2 * d], qb[l, 2 * d + 1], qb[r, 2 * d], int(d))
+        exp[l, 2 * d + 1] = FL.reshape(F, nV)
+        exp[r, 2 * d] = FR.reshape(F, nV)
+    for c, f in zip(bc, bf):
+        exp[c, f] = k.boundary_face(exp[c, f], qb[c, f], int(f)).reshape(F, nV)
+    assert rel(got, exp) < RTOL
+
+
+@pytest.mark.parametrize("dim,order", [(2, 3), (2, 5), (3, 5), (3, 7)])
+def test_corrector_and_dt_vs_oracle(eb, dim, order):
+    rng = np.random.default_rng(7 * dim + order)
+    s = eb.Solver(dim, order, eb.PDE_EULER)
+    k = pyoracle.Kernels(dim, order, pde=0)
+    b = order + 1
+    P, F, nV, nD, D2 = b ** dim, b ** (dim - 1), 5, 5, 2 * dim
+    n = 23
+    u = random_states(rng, n, P, nD)
+    du = 0.1 * rng.standard_normal((n, P, nV))
+    fb = 0.1 * rng.standard_normal((n, D2, F, nV))
+    dx = [0.05, 0.04, 0.03][:dim]
+    dt = 1e-3
+    ud = dev(u)
+    dmin = torch.zeros(1, device="cuda", dtype=torch.float64)
+    # (a) time step of the unchanged solution: bit-identical to the reference's
+    s.reset_min(dmin)
+    s.corrector(ud, None, None, None, dmin, dx, n, update=False)
+    assert host(dmin)[0] == min(k.stable_dt(u[c], dx) for c in range(n))
+    # (b) surface integral + update + dt
+    s.reset_min(dmin)
+    s.corrector(ud, dev(du), dev(fb), dev([dt]), dmin, dx, n, update=True)
+    got = host(ud)
+    exp = np.empty_like(u)
+    for c in range(n):
+        d2 = k.surface_integral(du[c], fb[c], dx)
+        exp[c] = k.solution_update(u[c], d2, dt).reshape(P, nD)
+    assert rel(got, exp) < RTOL
+    dt_new = host(dmin)[0]
+    dt_ref = min(k.stable_dt(got[c], dx) for c in range(n))
+    assert dt_new == dt_ref  # bit-identical from the same (GPU) solution
+
+
+def _mesh_pair(eb, dim, order, cells, bc, u):
+    s = eb.Solver(dim, order, eb.PDE_EULER)
+    m = eb.Mesh(s, cells, [0.0] * dim, [1.0] * dim, bc)
+    m.set_solution(u)
+    m.init(0.0)
+    o = pyoracle.Mesh(dim, order, cells, [1.0] * dim, bc, nthreads=8)
+    o.set_solution(u)
+    o.init(0.0)
+    return s, m, o
+
+
+@pytest.mark.parametrize("dim,order,cells,steps", [(2, 3, (27, 27), 10), (2, 5, (9, 9), 6), (3, 5, (5, 5, 5), 3),
+                                                   (3, 3, (6, 5, 4), 4), (2, 7, (5, 6), 3)])
+def test_mesh_periodic_vs_oracle(eb, dim, order, cells, steps):
+    from exahype_b200 import problems
+    if dim == 2:
+        u, _ = problems.gaussian_pulse_2d(order, cells, seed=5)
+    else:
+        u, _ = problems.gaussian_pulses_3d(order, cells, seed=5)
+    s, m, o = _mesh_pair(eb, dim, order, cells, eb.BC_PERIODIC, u)
+    m.step(steps)
+    o.step(steps)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < RTOL
+    sm, so = m.state(), o.state()
+    assert sm["steps"] == so["steps"] == steps
+    assert sm["picard_sweeps"] == so["picard_sweeps"]
+    assert abs(sm["t"] - so["t"]) <= 1e-13 * so["t"]
+
+
+def test_mesh_outflow_vs_oracle(eb):
+    from exahype_b200 import problems
+    u, _ = problems.gaussian_pulse_2d(3, (12, 12), seed=2)
+    s, m, o = _mesh_pair(eb, 2, 3, (12, 12), eb.BC_OUTFLOW, u)
+    m.step(5)
+    o.step(5)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < RTOL
+
+
+def test_config0_full_run_step_count(eb):
+    """2D Euler N=3 on 27^2 periodic cells to t = 0.1: same number of steps
+    as the oracle, fields within 1e-12 relative L2."""
+    from exahype_b200 import problems
+    u, _ = problems.gaussian_pulse_2d(3, (27, 27), seed=0)
+    s, m, o = _mesh_pair(eb, 2, 3, (27, 27), eb.BC_PERIODIC, u)
+    n_gpu = m.run_until(0.1)
+    n_orc = o.run_until(0.1)
+    assert n_gpu == n_orc
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < RTOL
+    assert m.state()["t"] >= 0.1

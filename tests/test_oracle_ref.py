@@ -1,0 +1,53 @@
+"""The C oracle against the reference's own kernels compiled from source
+(oracle/_ref): per-kernel and over whole uniform-mesh runs. Skipped where the
+reference build is absent."""
+import numpy as np
+import pytest
+
+import pyoracle
+from exahype_b200 import problems
+
+pytestmark = pytest.mark.skipif(not (pyoracle.ref_available(2) and pyoracle.ref_available(3)),
+                                reason="oracle/_ref not built")
+
+
+def rand_cell(rng, P, nD):
+    u = np.zeros((P, nD))
+    u[:, 0] = 1 + 0.3 * rng.random(P)
+    u[:, 1:4] = 0.4 * (rng.random((P, 3)) - 0.5)
+    u[:, 4] = 2.5 + 0.5 * rng.random(P)
+    return u
+
+
+@pytest.mark.parametrize("dim,N,pde", [(2, 3, 0), (2, 5, 0), (2, 7, 0), (3, 3, 0), (3, 5, 0), (3, 7, 0), (2, 3, 1),
+                                       (3, 3, 1)])
+def test_kernels_vs_reference(dim, N, pde):
+    rng = np.random.default_rng(dim * 10 + N + 100 * pde)
+    o, r = pyoracle.Kernels(dim, N, pde), pyoracle.Kernels(dim, N, pde, impl="ref")
+    u = rand_cell(rng, (N + 1) ** dim, 5 + pde)
+    dx = [0.05] * dim
+    a, b = o.predictor(u, dx, 1e-3, temps=True), r.predictor(u, dx, 1e-3, temps=True)
+    assert a["iterations"] == b["iterations"]
+    for k in ("lQhbnd", "lFhbnd", "lduh", "lQi", "lFi", "lQhi", "lFhi"):
+        assert np.max(np.abs(a[k] - b[k])) <= 1e-13 * max(np.max(np.abs(b[k])), 1.0), k
+    assert o.stable_dt(u, dx) == r.stable_dt(u, dx)  # bit-identical time step
+
+
+@pytest.mark.parametrize("dim,N,cells,steps,bc", [(2, 3, (9, 9), 8, -1), (3, 3, (4, 4, 4), 3, -1),
+                                                  (2, 5, (6, 6), 4, 0), (3, 5, (3, 3, 3), 2, -1)])
+def test_mesh_vs_reference(dim, N, cells, steps, bc):
+    if dim == 2:
+        u, _ = problems.gaussian_pulse_2d(N, cells, seed=3)
+    else:
+        u, _ = problems.gaussian_pulses_3d(N, cells, seed=3)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.Mesh(dim, N, cells, [1.0] * dim, bc, impl=impl, nthreads=4)
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(steps)
+        res.append((m.get_solution(), m.state()))
+    (a, sa), (b, sb) = res
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-13
+    assert sa["picard_sweeps"] == sb["picard_sweeps"]
+    assert sa["steps"] == sb["steps"] == steps
