@@ -194,6 +194,13 @@ def run_ours(a):
 
     u0, _ = problems.gaussian_pulses_3d(ORDER, CELLS, seed=SEED + rank)
     s = eb.Solver(DIM, ORDER, eb.PDE_EULER)
+    tune = None
+    if a.variant is None:
+        chosen, vms = s.autotune(4096)
+        tune = {"chosen": chosen, "variant_ms_4096_cells": vms}
+    else:
+        s.variant = a.variant
+        tune = {"chosen": a.variant, "forced": True}
     m = eb.Mesh(s, CELLS, [0.0] * DIM, [1.0] * DIM, eb.BC_PERIODIC)
     m.set_solution(u0)
     m.init(0.0)
@@ -299,7 +306,7 @@ def run_ours(a):
                    "dof_per_step": dof_per_step(), "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
-        "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps,
+        "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -329,6 +336,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-probe", action="store_true")
+    ap.add_argument("--variant", type=int, default=None, help="predictor variant (default: autotune)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)

@@ -135,6 +135,25 @@ class Solver:
                                     _dbl3(dx), int(ncells), _ptr(cell_list), int(bool(update)), _stream(stream)),
                "exa_corrector")
 
+    @property
+    def variant(self):
+        v = ctypes.c_int()
+        _check(load().exa_solver_get_variant(self._h, ctypes.byref(v)), "exa_solver_get_variant")
+        return v.value
+
+    @variant.setter
+    def variant(self, v):
+        _check(load().exa_solver_set_variant(self._h, int(v)), "exa_solver_set_variant")
+
+    def autotune(self, ncells=4096):
+        """Times every predictor variant on `ncells` synthetic cells, keeps the
+        fastest; returns (chosen, [ms per variant])."""
+        n = load().exa_solver_variants() if hasattr(load(), "exa_solver_variants") else 4
+        ms = (ctypes.c_double * n)()
+        ch = ctypes.c_int()
+        _check(load().exa_solver_autotune(self._h, int(ncells), ms, ctypes.byref(ch)), "exa_solver_autotune")
+        return ch.value, list(ms)
+
     @staticmethod
     def reset_min(dev, stream=None):
         _check(load().exa_reset_min(_ptr(dev), _stream(stream)), "exa_reset_min")

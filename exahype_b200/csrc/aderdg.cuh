@@ -37,20 +37,27 @@ struct Geometry {
 // aderPicardLoopNonlinear (3d/spaceTimePredictorNonlinear.cpph:42-329) with
 // the time averaging (:337-409), the boundary extrapolation (:411-528) and
 // volumeIntegralNonlinear (3d/volumeIntegralNonlinear.cpph:135-225) fused into
-// one kernel. One thread owns one spatial node of one cell. Per Picard sweep
-// the time slices are processed one at a time: the slice's fluxes go to shared
-// memory, every thread forms its node's rhs and folds it into its registers
-// through iK1, so only lQi ([P][b][nD]) and one flux slice ([DIM][P][nV]) are
-// resident in shared memory.
-template <int DIM, int N, class PDE>
+// one kernel.
+//
+// Work split: VSPLIT threads own one spatial node of one cell, each a slice of
+// the nV conserved variables. Per Picard sweep the time slices are processed
+// one at a time: the slice's fluxes go to shared memory, every thread forms
+// its (node, variables) rhs from the three derivative contractions and folds
+// it into its registers through iK1. Resident in shared memory per cell: the
+// space-time iterate lQi [P][b][nD] and one flux slice [DIM][P][nV].
+// MINB is the number of blocks per SM the register budget is sized for.
+template <int DIM, int N, class PDE, int VSPLIT = 1, int MINB = 1>
 struct PredictorCfg : Shape<DIM, N, PDE> {
   using S = Shape<DIM, N, PDE>;
   static constexpr int CPB = cells_per_block<S::P>();
-  static constexpr int THREADS = CPB * S::P;
-  static constexpr int SQ = S::P * S::b * S::nD;  // lQi per cell
-  static constexpr int SF = DIM * S::P * S::nV;   // one flux slice per cell
-  static constexpr int SR = pow2ceil(S::P);       // residual reduction per cell
-  static constexpr int SK = S::b * S::b;          // Kxi copy (per block)
+  static constexpr int TPC = CPB * S::P;                     // threads per variable slice
+  static constexpr int THREADS = VSPLIT * TPC;
+  static constexpr int MIN_BLOCKS = MINB;
+  static constexpr int NVT = (S::nV + VSPLIT - 1) / VSPLIT;  // variables per thread
+  static constexpr int SQ = S::P * S::b * S::nD;            // lQi per cell
+  static constexpr int SF = DIM * S::P * S::nV;             // one flux slice per cell
+  static constexpr int SR = VSPLIT * S::P + 1;              // residual partials + the cell's sum
+  static constexpr int SK = S::b * S::b;                    // Kxi copy (per block)
   static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR) + SK);
 };
 
@@ -58,18 +65,22 @@ struct PredictorTemps {  // optional reference-layout temporaries (golden replay
   double *lQi, *lFi, *lQhi, *lFhi;
 };
 
-template <int DIM, int N, class PDE, bool TEMPS>
-__global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE>::THREADS)
+template <int DIM, int N, class PDE, bool TEMPS, int VSPLIT, int MINB>
+__global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREADS, MINB)
     predictor_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                      double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
                      Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp) {
-  using C = PredictorCfg<DIM, N, PDE>;
-  constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD;
+  using C = PredictorCfg<DIM, N, PDE, VSPLIT, MINB>;
+  constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD, NVT = C::NVT;
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
 
-  const int lc = threadIdx.x / P;
-  const int p = threadIdx.x - lc * P;
+  const int part_id = threadIdx.x / C::TPC;  // which variable slice
+  const int r = threadIdx.x - part_id * C::TPC;
+  const int lc = r / P;
+  const int p = r - lc * P;
+  const int v0 = part_id * NVT;
+  const bool lead = part_id == 0;  // evaluates fluxes and owns the parameters
   const int slot = blockIdx.x * C::CPB + lc;
   const bool active = slot < ncells;
   const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
@@ -87,35 +98,37 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE>::THREADS)
   const double dt = *dt_ptr;
   const double invDx0 = 1.0 / geo.dx[0], invDx1 = 1.0 / geo.dx[1], invDx2 = DIM == 3 ? 1.0 / geo.dx[2] : 0.0;
 
-  double lu[nD];
+  // own variables of luh (for the rhs0 term); the lead thread also seeds the
+  // whole trivial initial guess lQi(:,t) = luh (:66-82)
+  double lu[NVT];
   {
     const double* src = luh + ((size_t)cell * P + p) * nD;
 #pragma unroll
-    for (int v = 0; v < nD; v++) lu[v] = active ? __ldg(src + v) : (v == 0 ? 1.0 : (v == nD - 1 && nD == 5 ? 2.5 : 0.0));
+    for (int j = 0; j < NVT; j++) lu[j] = (active && v0 + j < nV) ? __ldg(src + v0 + j) : 0.0;
+    if (lead) {
+      double q[nD];
+#pragma unroll
+      for (int v = 0; v < nD; v++) q[v] = active ? __ldg(src + v) : 0.0;
+#pragma unroll
+      for (int t = 0; t < b; t++)
+#pragma unroll
+        for (int v = 0; v < nD; v++) sQ[(p * b + t) * nD + v] = q[v];
+    }
   }
-  // trivial initial guess lQi(:,t) = luh (:66-82)
-#pragma unroll
-  for (int t = 0; t < b; t++)
-#pragma unroll
-    for (int v = 0; v < nD; v++) sQ[(p * b + t) * nD + v] = lu[v];
 
-  double fh[DIM][nV];
+  double fh[DIM][nV];  // lead threads: time-averaged fluxes of the last sweep
   bool done = !active;
   int it_done = 0;
   for (int iter = 0; iter < C::maxIter; iter++) {
-    double qn[b][nV];
+    double qn[b][NVT];
 #pragma unroll
     for (int l = 0; l < b; l++)
 #pragma unroll
-      for (int v = 0; v < nV; v++) qn[l][v] = 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; d++)
-#pragma unroll
-      for (int v = 0; v < nV; v++) fh[d][v] = 0.0;
+      for (int j = 0; j < NVT; j++) qn[l][j] = 0.0;
 
     for (int t = 0; t < b; t++) {
-      __syncthreads();  // previous slice's readers are done with sF
-      if (!done) {
+      __syncthreads();  // previous slice's readers are done with sF (and lQi is seeded)
+      if (!done && lead) {
         double Q[nD];
 #pragma unroll
         for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
@@ -124,97 +137,150 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE>::THREADS)
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int v = 0; v < nV; v++) {
-            sF[(d * P + p) * nV + v] = Fl[d][v];
-            fh[d][v] += Fl[d][v] * T.w[t];
-          }
-        if (TEMPS) {
-          double* dst = tmp.lFi + (((size_t)cell * b + t) * P + p) * (DIM + 1) * nV;
-#pragma unroll
-          for (int d = 0; d < DIM; d++)
-#pragma unroll
-            for (int v = 0; v < nV; v++) dst[d * nV + v] = Fl[d][v];
-        }
+          for (int v = 0; v < nV; v++) sF[(d * P + p) * nV + v] = Fl[d][v];
       }
       __syncthreads();
       if (!done) {
-        double rhs[nV];
+        // derivative contractions (:151-236); the quadrature factor of each
+        // direction is applied once per node instead of once per term
+        double ax[NVT], ay[NVT], az[NVT];
+#pragma unroll
+        for (int j = 0; j < NVT; j++) ax[j] = ay[j] = az[j] = 0.0;
+        {
+          const double* Fx = sF + (0 * P + (z * b + y) * b) * nV + v0;
+#pragma unroll
+          for (int n = 0; n < b; n++) {
+            const double k = sK[n * b + x];
+#pragma unroll
+            for (int j = 0; j < NVT; j++)
+              if (v0 + j < nV) ax[j] = fma(Fx[n * nV + j], k, ax[j]);
+          }
+        }
+        {
+          const double* Fy = sF + (1 * P + z * b * b + x) * nV + v0;
+#pragma unroll
+          for (int n = 0; n < b; n++) {
+            const double k = sK[n * b + y];
+#pragma unroll
+            for (int j = 0; j < NVT; j++)
+              if (v0 + j < nV) ay[j] = fma(Fy[n * b * nV + j], k, ay[j]);
+          }
+        }
+        if (DIM == 3) {
+          const double* Fz = sF + (2 * P + y * b + x) * nV + v0;
+#pragma unroll
+          for (int n = 0; n < b; n++) {
+            const double k = sK[n * b + z];
+#pragma unroll
+            for (int j = 0; j < NVT; j++)
+              if (v0 + j < nV) az[j] = fma(Fz[n * b * b * nV + j], k, az[j]);
+          }
+        }
+        const double usx = (T.w[t] * wz) * wy * dt * invDx0;
+        const double usy = (T.w[t] * wz) * wx * dt * invDx1;
+        const double usz = DIM == 3 ? (T.w[t] * wy) * wx * dt * invDx2 : 0.0;
         const double r0 = wpt * T.FL[t];
+        // discrete time integral (:280-311): lQi_new[l] += iw rhs[t] iK1[l][t]
 #pragma unroll
-        for (int v = 0; v < nV; v++) rhs[v] = r0 * lu[v];
-        {  // x derivative (:151-178)
-          const double us = (T.w[t] * wz) * wy * dt * invDx0;
-          const double* Fx = sF + (0 * P + (z * b + y) * b) * nV;
+        for (int j = 0; j < NVT; j++) {
+          double rhs = r0 * lu[j] - usx * ax[j] - usy * ay[j];
+          if (DIM == 3) rhs -= usz * az[j];
+          const double ir = iw * rhs;
 #pragma unroll
-          for (int v = 0; v < nV; v++)
-#pragma unroll
-            for (int n = 0; n < b; n++) rhs[v] -= us * Fx[n * nV + v] * sK[n * b + x];
-        }
-        {  // y derivative (:180-207)
-          const double us = (T.w[t] * wz) * wx * dt * invDx1;
-          const double* Fy = sF + (1 * P + z * b * b + x) * nV;
-#pragma unroll
-          for (int v = 0; v < nV; v++)
-#pragma unroll
-            for (int n = 0; n < b; n++) rhs[v] -= us * Fy[n * b * nV + v] * sK[n * b + y];
-        }
-        if (DIM == 3) {  // z derivative (:209-236)
-          const double us = (T.w[t] * wy) * wx * dt * invDx2;
-          const double* Fz = sF + (2 * P + y * b + x) * nV;
-#pragma unroll
-          for (int v = 0; v < nV; v++)
-#pragma unroll
-            for (int n = 0; n < b; n++) rhs[v] -= us * Fz[n * b * b * nV + v] * sK[n * b + z];
-        }
-        // discrete time integral (:280-311): lQi_new[l] = sum_t iw rhs[t] iK1[l][t]
-#pragma unroll
-        for (int l = 0; l < b; l++) {
-          const double k1 = T.iK1[l * b + t];
-#pragma unroll
-          for (int v = 0; v < nV; v++) qn[l][v] += iw * rhs[v] * k1;
+          for (int l = 0; l < b; l++) qn[l][j] = fma(ir, T.iK1[l * b + t], qn[l][j]);
         }
       }
     }
-    // residual and update of lQi (:282-311)
+    // residual (:282-311): partial sums per (node, slice), reduced per cell by a warp
     double part = 0.0;
     if (!done) {
 #pragma unroll
       for (int l = 0; l < b; l++)
 #pragma unroll
-        for (int v = 0; v < nV; v++) {
-          const double dq = qn[l][v] - sQ[(p * b + l) * nD + v];
-          part += dq * dq;
-          sQ[(p * b + l) * nD + v] = qn[l][v];
-        }
+        for (int j = 0; j < NVT; j++)
+          if (v0 + j < nV) {
+            const double dq = qn[l][j] - sQ[(p * b + l) * nD + v0 + j];
+            part = fma(dq, dq, part);
+          }
     }
-    sR[p] = part;
-    if (p < C::SR - P) sR[P + p] = 0.0;
+    sR[part_id * P + p] = part;
     __syncthreads();
+    {
+      constexpr int kFullWarps = C::THREADS / 32;
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      if (warp < kFullWarps) {
+        for (int c = warp; c < C::CPB; c += kFullWarps) {
+          double* rr = smem + C::CPB * (C::SQ + C::SF) + c * C::SR;
+          double acc = 0.0;
+          for (int i = lane; i < VSPLIT * P; i += 32) acc += rr[i];
 #pragma unroll
-    for (int s = C::SR / 2; s > 0; s >>= 1) {
-      if (p < s) sR[p] += sR[p + s];
-      __syncthreads();
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (lane == 0) rr[VSPLIT * P] = acc;
+        }
+      }
     }
-    const double sq_res = sR[0];
+    __syncthreads();
+    const double sq_res = sR[VSPLIT * P];
     if (!done) {
       it_done = iter + 1;
-      if (sq_res < 1e-7 * 1e-7) done = true;  // exit condition (:315-318)
+      const bool conv = sq_res < 1e-7 * 1e-7;  // exit condition (:315-318)
+      if (conv || iter + 1 == C::maxIter) {
+        // lFhi is the time average of the fluxes this sweep evaluated, i.e. of
+        // the iterate before the update (:337-409): the lead thread re-evaluates
+        // them from its node's old lQi row before the row is overwritten.
+        if (lead) {
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int v = 0; v < nV; v++) fh[d][v] = 0.0;
+          for (int t = 0; t < b; t++) {
+            double Q[nD];
+#pragma unroll
+            for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+            double Fl[DIM][nV];
+            PDE::template flux<DIM>(Q, Fl);
+#pragma unroll
+            for (int d = 0; d < DIM; d++)
+#pragma unroll
+              for (int v = 0; v < nV; v++) fh[d][v] += Fl[d][v] * T.w[t];
+            if (TEMPS) {
+              double* dst = tmp.lFi + (((size_t)cell * b + t) * P + p) * (DIM + 1) * nV;
+#pragma unroll
+              for (int d = 0; d < DIM; d++)
+#pragma unroll
+                for (int v = 0; v < nV; v++) dst[d * nV + v] = Fl[d][v];
+            }
+          }
+        }
+        done = true;
+      }
+    }
+    // the lead thread of a node may still read the old row above; every
+    // thread overwrites its own variables only after the barrier
+    __syncthreads();
+    if (it_done == iter + 1) {
+#pragma unroll
+      for (int l = 0; l < b; l++)
+#pragma unroll
+        for (int j = 0; j < NVT; j++)
+          if (v0 + j < nV) sQ[(p * b + l) * nD + v0 + j] = qn[l][j];
     }
     if (!__syncthreads_or(!done)) break;
   }
-  if (iters && active && p == 0) iters[cell] = it_done;
+  if (iters && active && lead && p == 0) iters[cell] = it_done;
 
-  // time averages (:337-409). lQhi from the final lQi, lFhi from the fluxes of
-  // the last sweep (the reference does not re-evaluate F after the last update).
+  // time averages (:337-409). lQhi from the final lQi (lead threads).
   double qh[nD];
+  if (lead) {
 #pragma unroll
-  for (int v = 0; v < nD; v++) {
-    double s = 0.0;
+    for (int v = 0; v < nD; v++) {
+      double s = 0.0;
 #pragma unroll
-    for (int m = 0; m < b; m++) s += sQ[(p * b + m) * nD + v] * T.w[m];
-    qh[v] = s;
+      for (int m = 0; m < b; m++) s += sQ[(p * b + m) * nD + v] * T.w[m];
+      qh[v] = s;
+    }
   }
-  if (TEMPS && active) {
+  if (TEMPS && active && lead) {
     double* dq = tmp.lQi + ((size_t)cell * P + p) * b * nD;
     for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * b * nD + i];
     for (int v = 0; v < nD; v++) tmp.lQhi[((size_t)cell * P + p) * nD + v] = qh[v];
@@ -231,51 +297,46 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE>::THREADS)
   }
   __syncthreads();  // everyone has read its lQi row
   double* sQh = sQ;  // lQhi [P][nD] reuses the lQi buffer
+  if (lead) {
 #pragma unroll
-  for (int v = 0; v < nD; v++) sQh[p * nD + v] = qh[v];
+    for (int v = 0; v < nD; v++) sQh[p * nD + v] = qh[v];
 #pragma unroll
-  for (int d = 0; d < DIM; d++)
+    for (int d = 0; d < DIM; d++)
 #pragma unroll
-    for (int v = 0; v < nV; v++) sF[(d * P + p) * nV + v] = fh[d][v];
+      for (int v = 0; v < nV; v++) sF[(d * P + p) * nV + v] = fh[d][v];
+  }
   __syncthreads();
   if (!active) return;
 
-  // volume integral at this node (3d/volumeIntegralNonlinear.cpph:135-225)
+  // volume integral at this node, own variables (3d/volumeIntegralNonlinear.cpph:135-225)
   if (lduh) {
-    double du[nV];
-#pragma unroll
-    for (int v = 0; v < nV; v++) du[v] = 0.0;
-    {
-      const double us = (wz * wy) * invDx0;
-      const double* Fx = sF + (0 * P + (z * b + y) * b) * nV;
-#pragma unroll
-      for (int v = 0; v < nV; v++)
-#pragma unroll
-        for (int m = 0; m < b; m++) du[v] += sK[x * b + m] * Fx[m * nV + v] * us;
-    }
-    {
-      const double us = (wz * wx) * invDx1;
-      const double* Fy = sF + (1 * P + z * b * b + x) * nV;
-#pragma unroll
-      for (int v = 0; v < nV; v++)
-#pragma unroll
-        for (int m = 0; m < b; m++) du[v] += sK[y * b + m] * Fy[m * b * nV + v] * us;
-    }
-    if (DIM == 3) {
-      const double us = (wy * wx) * invDx2;
-      const double* Fz = sF + (2 * P + y * b + x) * nV;
-#pragma unroll
-      for (int v = 0; v < nV; v++)
-#pragma unroll
-        for (int m = 0; m < b; m++) du[v] += sK[z * b + m] * Fz[m * b * b * nV + v] * us;
-    }
     double* dst = lduh + ((size_t)cell * P + p) * nV;
+    const double usx = (wz * wy) * invDx0, usy = (wz * wx) * invDx1, usz = (wy * wx) * invDx2;
 #pragma unroll
-    for (int v = 0; v < nV; v++) dst[v] = du[v];
+    for (int j = 0; j < NVT; j++) {
+      const int v = v0 + j;
+      if (v >= nV) break;
+      double sx = 0.0, sy = 0.0, sz = 0.0;
+      const double* Fx = sF + (0 * P + (z * b + y) * b) * nV + v;
+      const double* Fy = sF + (1 * P + z * b * b + x) * nV + v;
+#pragma unroll
+      for (int m = 0; m < b; m++) {
+        sx = fma(sK[x * b + m], Fx[m * nV], sx);
+        sy = fma(sK[y * b + m], Fy[m * b * nV], sy);
+      }
+      double du = sx * usx + sy * usy;
+      if (DIM == 3) {
+        const double* Fz = sF + (2 * P + y * b + x) * nV + v;
+#pragma unroll
+        for (int m = 0; m < b; m++) sz = fma(sK[z * b + m], Fz[m * b * b * nV], sz);
+        du += sz * usz;
+      }
+      dst[v] = du;
+    }
   }
 
   // boundary extrapolation (3d/spaceTimePredictorNonlinear.cpph:411-528)
-  for (int k = p; k < DIM * F; k += P) {
+  for (int k = part_id * P + p; k < DIM * F; k += VSPLIT * P) {
     const int dir = k / F, fn = k - dir * F;
     const int a = DIM == 3 ? fn / b : 0, c = DIM == 3 ? fn % b : fn;
     // node index of position l along dir on this face line
@@ -440,7 +501,8 @@ __global__ void __launch_bounds__(128) boundary_kernel(const double* __restrict_
 template <int DIM, int N, class PDE>
 struct CorrectorCfg : Shape<DIM, N, PDE> {
   static constexpr int CPB = cells_per_block<Shape<DIM, N, PDE>::P>();
-  static constexpr int THREADS = CPB * Shape<DIM, N, PDE>::P;
+  // whole warps: the block min-reduction shuffles across full warps
+  static constexpr int THREADS = (CPB * Shape<DIM, N, PDE>::P + 31) / 32 * 32;
 };
 
 template <int DIM, int N, class PDE>
@@ -455,7 +517,7 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
   const int lc = threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
   const int slot = blockIdx.x * C::CPB + lc;
-  const bool active = slot < ncells;
+  const bool active = lc < C::CPB && slot < ncells;  // padding threads only join the reduction
   double dtmin = __longlong_as_double(0x7fefffffffffffffll);  // DBL_MAX
   if (active) {
     const int cell = cell_list ? cell_list[slot] : slot;

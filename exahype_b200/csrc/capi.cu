@@ -75,7 +75,7 @@ static int upload_tables() {
 struct KernelSet {
   int dim, order, pde, nvar, npar, P, F;
   int (*predictor)(const double*, double*, double*, double*, int*, const double*, Geometry, int, const int*,
-                   PredictorTemps, bool, unsigned long long*, cudaStream_t);
+                   PredictorTemps, bool, unsigned long long*, int, cudaStream_t);
   int (*riemann)(const double*, double*, const int*, const int*, const int*, int, cudaStream_t);
   int (*boundary)(const double*, double*, const int*, const int*, int, int, cudaStream_t);
   int (*corrector)(double*, const double*, const double*, const double*, double*, Geometry, int, const int*, int,
@@ -91,31 +91,48 @@ __global__ void sweep_count_kernel(const int* iters, const int* cell_list, int n
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
 }
 
+// Predictor variants (work split, blocks per SM) the autotuner chooses from.
+constexpr int kPredictorVariants = 4;
+__host__ __device__ constexpr int variant_vsplit(int v) { return v == 0 || v == 3 ? 1 : 2; }
+__host__ __device__ constexpr int variant_minb(int v) { return v == 2 || v == 3 ? 2 : 1; }
+
 template <int DIM, int N, class PDE>
 struct Launch {
-  using PC = PredictorCfg<DIM, N, PDE>;
   using CC = CorrectorCfg<DIM, N, PDE>;
 
-  static int predictor(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
-                       Geometry g, int n, const int* list, PredictorTemps tmp, bool temps, unsigned long long* acc,
-                       cudaStream_t st) {
-    if (n <= 0) return EXA_OK;
+  template <bool TEMPS, int VS, int MB>
+  static int launch_pred(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
+                         Geometry g, int n, const int* list, PredictorTemps tmp, cudaStream_t st) {
+    using PC = PredictorCfg<DIM, N, PDE, VS, MB>;
     static bool attr = false;
     if (!attr) {
-      EXA_CUDA(cudaFuncSetAttribute(predictor_kernel<DIM, N, PDE, false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PC::SMEM));
-      EXA_CUDA(cudaFuncSetAttribute(predictor_kernel<DIM, N, PDE, true>,
+      EXA_CUDA(cudaFuncSetAttribute(predictor_kernel<DIM, N, PDE, TEMPS, VS, MB>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PC::SMEM));
       attr = true;
     }
     const int grid = (n + PC::CPB - 1) / PC::CPB;
-    if (temps)
-      predictor_kernel<DIM, N, PDE, true><<<grid, PC::THREADS, PC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g, n, list,
-                                                                              tmp);
-    else
-      predictor_kernel<DIM, N, PDE, false><<<grid, PC::THREADS, PC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g, n,
-                                                                               list, tmp);
+    predictor_kernel<DIM, N, PDE, TEMPS, VS, MB><<<grid, PC::THREADS, PC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
+                                                                                     n, list, tmp);
     EXA_LAUNCHED();
+    return EXA_OK;
+  }
+
+  static int predictor(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
+                       Geometry g, int n, const int* list, PredictorTemps tmp, bool temps, unsigned long long* acc,
+                       int variant, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    int rc;
+    if (temps)
+      rc = launch_pred<true, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+    else if (variant == 1)
+      rc = launch_pred<false, 2, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+    else if (variant == 2)
+      rc = launch_pred<false, 2, 2>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+    else if (variant == 3)
+      rc = launch_pred<false, 1, 2>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+    else
+      rc = launch_pred<false, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+    if (rc) return rc;
     if (acc && iters) {
       sweep_count_kernel<DIM, N, PDE><<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(iters, list, n, acc);
       EXA_LAUNCHED();
@@ -207,6 +224,7 @@ using namespace exa;
 
 struct exa_solver {
   KernelSet k;
+  int variant = 0;  // predictor variant (set by exa_solver_autotune / exa_solver_set_variant)
 };
 
 struct exa_mesh {
@@ -295,7 +313,7 @@ int exa_space_time_predictor_nonlinear(const exa_solver* s, const double* luh, d
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_nonlinear: null argument or negative count");
   return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, cell_list,
-                        PredictorTemps{}, false, nullptr, (cudaStream_t)stream);
+                        PredictorTemps{}, false, nullptr, s->variant, (cudaStream_t)stream);
 }
 
 int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* luh, double* lQhbnd,
@@ -305,7 +323,7 @@ int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* 
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0 || !lQi || !lFi || !lQhi || !lFhi)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_nonlinear_temps: null argument or negative count");
   return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, nullptr,
-                        PredictorTemps{lQi, lFi, lQhi, lFhi}, true, nullptr, (cudaStream_t)stream);
+                        PredictorTemps{lQi, lFi, lQhi, lFhi}, true, nullptr, 0, (cudaStream_t)stream);
 }
 
 int exa_riemann_solver_nonlinear(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* face_left,
@@ -336,6 +354,82 @@ int exa_reset_min(double* dev, void* stream) {
   if (!dev) return fail(EXA_ERR_ARG, "exa_reset_min: null pointer");
   reset_min_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(dev);
   EXA_LAUNCHED();
+  return EXA_OK;
+}
+
+// smooth synthetic states for the autotuner: rho, j, E with O(10%) variation
+__global__ void autotune_fill_kernel(double* luh, long long n, int nD) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long node = i / nD;
+    const int v = (int)(i - node * nD);
+    const double s = sin(0.37 * (double)node) * cos(0.011 * (double)node);
+    luh[i] = v == 0 ? 1.0 + 0.1 * s : v == 4 ? 2.5 + 0.2 * s : v < 4 ? 0.3 * s * (v - 2) : 0.0;
+  }
+}
+
+int exa_solver_set_variant(exa_solver* s, int variant) {
+  if (!s || variant < 0 || variant >= kPredictorVariants) return fail(EXA_ERR_ARG, "exa_solver_set_variant: bad argument");
+  s->variant = variant;
+  return EXA_OK;
+}
+
+int exa_solver_get_variant(const exa_solver* s, int* variant) {
+  if (!s || !variant) return fail(EXA_ERR_ARG, "exa_solver_get_variant: null argument");
+  *variant = s->variant;
+  return EXA_OK;
+}
+
+int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chosen) {
+  if (!s || ncells < 1) return fail(EXA_ERR_ARG, "exa_solver_autotune: bad argument");
+  const KernelSet& k = s->k;
+  const size_t P = k.P, F = k.F, nV = k.nvar, nD = k.nvar + k.npar, D2 = 2 * k.dim, n = ncells;
+  double *luh = nullptr, *qb = nullptr, *fb = nullptr, *du = nullptr, *dt = nullptr;
+  int* it = nullptr;
+  auto cleanup = [&]() { cudaFree(luh); cudaFree(qb); cudaFree(fb); cudaFree(du); cudaFree(dt); cudaFree(it); };
+  if (cudaMalloc(&luh, n * P * nD * 8) != cudaSuccess || cudaMalloc(&qb, n * D2 * F * nD * 8) != cudaSuccess ||
+      cudaMalloc(&fb, n * D2 * F * nV * 8) != cudaSuccess || cudaMalloc(&du, n * P * nV * 8) != cudaSuccess ||
+      cudaMalloc(&dt, 8) != cudaSuccess || cudaMalloc(&it, n * 4) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return fail(EXA_ERR_NOMEM, "exa_solver_autotune: device allocation failed");
+  }
+  cudaStream_t st;
+  EXA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  autotune_fill_kernel<<<1024, 256, 0, st>>>(luh, (long long)(n * P * nD), (int)nD);
+  Geometry g{};
+  for (int d = 0; d < 3; d++) g.dx[d] = 1.0 / 27.0;
+  reset_min_kernel<<<1, 1, 0, st>>>(dt);
+  int rc = k.corrector(luh, nullptr, nullptr, nullptr, dt, g, (int)n, nullptr, 0, st);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int best = 0;
+  double best_ms = 1e300;
+  for (int v = 0; v < kPredictorVariants && rc == EXA_OK; v++) {
+    float ms = 0.f, tot = 0.f;
+    for (int r = 0; r < 4 && rc == EXA_OK; r++) {
+      cudaEventRecord(a, st);
+      rc = k.predictor(luh, qb, fb, du, it, dt, g, (int)n, nullptr, PredictorTemps{}, false, nullptr, v, st);
+      cudaEventRecord(b, st);
+      cudaEventSynchronize(b);
+      cudaEventElapsedTime(&ms, a, b);
+      if (r > 0) tot += ms;  // first launch is a warm-up
+    }
+    const double avg = tot / 3.0;
+    if (variant_ms) variant_ms[v] = avg;
+    if (avg < best_ms) {
+      best_ms = avg;
+      best = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cleanup();
+  if (rc) return rc;
+  s->variant = best;
+  if (chosen) *chosen = best;
   return EXA_OK;
 }
 
@@ -501,7 +595,7 @@ static int mesh_predict(exa_mesh* m) {
   PhaseTimer pt(m, 0);
   m->phase_launches[0] += 2;
   return k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->scal + 0, m->geo, m->ncells, nullptr,
-                     PredictorTemps{}, false, m->sweeps, m->stream);
+                     PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
 }
 
 int exa_mesh_init(exa_mesh* m, double t0) {

@@ -62,6 +62,18 @@ int exa_solver_destroy(exa_solver* s);
  * (ADERDGSolver::get{UnknownsPerCell,DataPerCell,BndFaceSize,BndFluxSize}). */
 int exa_solver_sizes(const exa_solver* s, int* sizes4);
 
+/* Predictor variants: how a cell's nodes and variables are spread over
+ * threads and how many blocks per SM the register budget targets. The
+ * autotuner (no counterpart in the reference, whose generic kernels have one
+ * shape per order) times every variant on `ncells` synthetic cells of this
+ * solver's order and keeps the fastest; variant_ms[EXA_PREDICTOR_VARIANTS]
+ * (optional) receives the per-variant milliseconds. It allocates and frees
+ * its own device buffers and synchronises the device. */
+#define EXA_PREDICTOR_VARIANTS 4
+int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chosen);
+int exa_solver_set_variant(exa_solver* s, int variant);
+int exa_solver_get_variant(const exa_solver* s, int* variant);
+
 /* spaceTimePredictor (Kernels.h:85-95) + volumeIntegral (Kernels.h:104-106)
  * for ncells cells: reads luh, writes lQhbnd, lFhbnd and, when lduh is not
  * NULL, the volume integral lduh. dt_dev: device pointer to the predictor
