@@ -13,6 +13,7 @@
 
 #include "../../include/exahype_b200.h"
 #include "aderdg.cuh"
+#include "predictor_lines.cuh"
 
 namespace exa {
 
@@ -91,10 +92,10 @@ __global__ void sweep_count_kernel(const int* iters, const int* cell_list, int n
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
 }
 
-// Predictor variants (work split, blocks per SM) the autotuner chooses from.
+// Predictor variants the autotuner chooses from:
+//   0 node form, 1 block/SM budget    1 line form, 1 block/SM
+//   2 line form, 2 blocks/SM          3 node form, 2 blocks/SM
 constexpr int kPredictorVariants = 4;
-__host__ __device__ constexpr int variant_vsplit(int v) { return v == 0 || v == 3 ? 1 : 2; }
-__host__ __device__ constexpr int variant_minb(int v) { return v == 2 || v == 3 ? 2 : 1; }
 
 template <int DIM, int N, class PDE>
 struct Launch {
@@ -117,17 +118,37 @@ struct Launch {
     return EXA_OK;
   }
 
+  template <bool TEMPS, int MB>
+  static int launch_lines(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
+                          Geometry g, int n, const int* list, PredictorTemps tmp, cudaStream_t st) {
+    using LC = LinesCfg<DIM, N, PDE, MB>;
+    static bool attr = false;
+    if (!attr) {
+      EXA_CUDA(cudaFuncSetAttribute(predictor_lines_kernel<DIM, N, PDE, TEMPS, MB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LC::SMEM));
+      attr = true;
+    }
+    const int grid = (n + LC::CPB - 1) / LC::CPB;
+    predictor_lines_kernel<DIM, N, PDE, TEMPS, MB><<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
+                                                                                       n, list, tmp);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  // two blocks of the line form only fit when their shared memory does
+  static constexpr bool kLines2 = 2 * LinesCfg<DIM, N, PDE, 2>::SMEM <= 227 * 1024;
+
   static int predictor(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
                        Geometry g, int n, const int* list, PredictorTemps tmp, bool temps, unsigned long long* acc,
                        int variant, cudaStream_t st) {
     if (n <= 0) return EXA_OK;
     int rc;
     if (temps)
-      rc = launch_pred<true, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
-    else if (variant == 1)
-      rc = launch_pred<false, 2, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+      rc = variant == 1 || variant == 2 ? launch_lines<true, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st)
+                                        : launch_pred<true, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+    else if (variant == 1 || (variant == 2 && !kLines2))
+      rc = launch_lines<false, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
     else if (variant == 2)
-      rc = launch_pred<false, 2, 2>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+      rc = launch_lines<false, kLines2 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
     else if (variant == 3)
       rc = launch_pred<false, 1, 2>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
     else
@@ -323,7 +344,7 @@ int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* 
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0 || !lQi || !lFi || !lQhi || !lFhi)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_nonlinear_temps: null argument or negative count");
   return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, nullptr,
-                        PredictorTemps{lQi, lFi, lQhi, lFhi}, true, nullptr, 0, (cudaStream_t)stream);
+                        PredictorTemps{lQi, lFi, lQhi, lFhi}, true, nullptr, s->variant, (cudaStream_t)stream);
 }
 
 int exa_riemann_solver_nonlinear(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* face_left,

@@ -1,0 +1,335 @@
+// Space-time predictor, "line" form.
+//
+// Same algorithm and outputs as predictor_kernel (aderdg.cuh): the Picard
+// iteration of aderPicardLoopNonlinear (3d/spaceTimePredictorNonlinear.cpph:
+// 42-329), time averaging (:337-409), extrapolation (:411-528) and
+// volumeIntegralNonlinear (3d/volumeIntegralNonlinear.cpph:135-225).
+//
+// The derivative contractions are organised around 1-D lines instead of
+// nodes, which is what bounds the node form (every derivative term reloads a
+// flux value from shared memory). Per time slice:
+//   A  one thread per node evaluates the flux and stores it line-major,
+//      sF[d][n][L][v]: d direction, n position along d, L the line (the other
+//      coordinates in (z,y,x) order), v the variable;
+//   B  one thread per (d, L, v) loads its line once, forms all b outputs
+//      sum_n F[n] Kxi[n][l] with the stiffness entries as compile-time-indexed
+//      constant-bank operands, scales by the line's quadrature factor and
+//      writes them back in place;
+//   C  one thread per node adds its three directional contributions to the
+//      rhs and folds the rhs into its Picard accumulators through iK1.
+// Shared memory per cell: lQi [P][b][nD], one line-major slice, residuals.
+#pragma once
+#include "aderdg.cuh"
+
+namespace exa {
+
+template <int DIM, int N, class PDE, int MINB>
+struct LinesCfg : Shape<DIM, N, PDE> {
+  using S = Shape<DIM, N, PDE>;
+  static constexpr int CPB = cells_per_block<S::P>();
+  static constexpr int THREADS = CPB * S::P;
+  static constexpr int LINES = S::P / S::b;  // lines per direction = face nodes
+  static constexpr int SLAB = LINES * S::nV + 1;  // one n-slab of one direction (odd stride)
+  static constexpr int SQ = S::P * S::b * S::nD;
+  static constexpr int SF = DIM * S::b * SLAB;
+  static constexpr int SR = S::P + 1;
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR));
+  static constexpr int ITEMS = CPB * DIM * LINES * S::nV;  // phase-B work items per block
+};
+
+// node p = (z, y, x) -> position n along direction d and line index L
+template <int DIM, int b>
+__device__ __forceinline__ void node_line(int d, int z, int y, int x, int& n, int& L) {
+  if (d == 0) { n = x; L = z * b + y; }
+  else if (d == 1) { n = y; L = z * b + x; }
+  else { n = z; L = y * b + x; }
+}
+
+template <int DIM, int N, class PDE, bool TEMPS, int MINB>
+__global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
+    predictor_lines_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
+                           double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
+                           Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp) {
+  using C = LinesCfg<DIM, N, PDE, MINB>;
+  constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, SLAB = C::SLAB;
+  extern __shared__ double smem[];
+  const OrderTables& T = c_tab[N];
+
+  const int lc = threadIdx.x / P;
+  const int p = threadIdx.x - lc * P;
+  const int slot = blockIdx.x * C::CPB + lc;
+  const bool active = slot < ncells;
+  const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
+  double* sQ = smem + lc * C::SQ;
+  double* sF = smem + C::CPB * C::SQ + lc * C::SF;
+  double* sR = smem + C::CPB * (C::SQ + C::SF) + lc * C::SR;
+  double* sFall = smem + C::CPB * C::SQ;
+
+  // quadrature weights in shared memory: phase-B threads index them by line,
+  // which would serialise on the constant cache
+  __shared__ double s_w[b];
+  if (threadIdx.x < b) s_w[threadIdx.x] = T.w[threadIdx.x];
+  const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
+  const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
+  const double wpt = wz * wy * wx;
+  const double iw = 1.0 / wpt;
+  const double dt = *dt_ptr;
+  const double invDx0 = 1.0 / geo.dx[0], invDx1 = 1.0 / geo.dx[1], invDx2 = DIM == 3 ? 1.0 / geo.dx[2] : 0.0;
+  int nd[DIM], Ld[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) node_line<DIM, b>(d, z, y, x, nd[d], Ld[d]);
+
+  double lu[nV];
+  {
+    const double* src = luh + ((size_t)cell * P + p) * nD;
+    double q[nD];
+#pragma unroll
+    for (int v = 0; v < nD; v++) q[v] = active ? __ldg(src + v) : 0.0;
+#pragma unroll
+    for (int v = 0; v < nV; v++) lu[v] = q[v];
+#pragma unroll
+    for (int t = 0; t < b; t++)
+#pragma unroll
+      for (int v = 0; v < nD; v++) sQ[(p * b + t) * nD + v] = q[v];
+  }
+
+  // Which cells of the block still iterate; phase B skips converged cells.
+  __shared__ int s_done[C::CPB];
+  if (p == 0) s_done[lc] = !active;
+
+  double fh[DIM][nV];
+  bool done = !active;
+  int it_done = 0;
+  for (int iter = 0; iter < C::maxIter; iter++) {
+    double qn[b][nV];
+#pragma unroll
+    for (int l = 0; l < b; l++)
+#pragma unroll
+      for (int v = 0; v < nV; v++) qn[l][v] = 0.0;
+
+    for (int t = 0; t < b; t++) {
+      __syncthreads();  // phase C of the previous slice is done with sF
+      // A: fluxes of slice t, line-major
+      if (!done) {
+        double Q[nD];
+#pragma unroll
+        for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+        double Fl[DIM][nV];
+        PDE::template flux<DIM>(Q, Fl);
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int v = 0; v < nV; v++) sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = Fl[d][v];
+      }
+      __syncthreads();
+      // B: line contractions, in place
+      for (int it = threadIdx.x; it < C::ITEMS; it += C::THREADS) {
+        const int v = it % nV;
+        const int L = (it / nV) % LINES;
+        const int d = (it / (nV * LINES)) % DIM;
+        const int c = it / (nV * LINES * DIM);
+        if (s_done[c]) continue;
+        double* base = sFall + c * C::SF + d * b * SLAB + L * nV + v;
+        double f[b];
+#pragma unroll
+        for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
+        // quadrature factor of the line: w_t times the two transverse weights
+        const int a0 = L / b, a1 = L % b;
+        const double wa = DIM == 3 ? s_w[a0] : 1.0;
+        const double idx = d == 0 ? invDx0 : d == 1 ? invDx1 : invDx2;
+        const double us = (T.w[t] * wa) * s_w[a1] * dt * idx;
+#pragma unroll
+        for (int l = 0; l < b; l++) {
+          double s = 0.0;
+#pragma unroll
+          for (int n = 0; n < b; n++) s = fma(f[n], T.Kxi[n * b + l], s);
+          base[l * SLAB] = us * s;
+        }
+      }
+      __syncthreads();
+      // C: rhs at this node, folded into the Picard accumulators
+      if (!done) {
+        const double r0 = wpt * T.FL[t];
+#pragma unroll
+        for (int v = 0; v < nV; v++) {
+          double rhs = r0 * lu[v];
+#pragma unroll
+          for (int d = 0; d < DIM; d++) rhs -= sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+          const double ir = iw * rhs;
+#pragma unroll
+          for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
+        }
+      }
+    }
+    // residual, reduced per cell by one warp
+    double part = 0.0;
+    if (!done) {
+#pragma unroll
+      for (int l = 0; l < b; l++)
+#pragma unroll
+        for (int v = 0; v < nV; v++) {
+          const double dq = qn[l][v] - sQ[(p * b + l) * nD + v];
+          part = fma(dq, dq, part);
+        }
+    }
+    sR[p] = part;
+    __syncthreads();
+    {
+      constexpr int kFullWarps = C::THREADS / 32;
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      if (warp < kFullWarps) {
+        for (int c = warp; c < C::CPB; c += kFullWarps) {
+          double* rr = smem + C::CPB * (C::SQ + C::SF) + c * C::SR;
+          double acc = 0.0;
+          for (int i = lane; i < P; i += 32) acc += rr[i];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (lane == 0) rr[P] = acc;
+        }
+      }
+    }
+    __syncthreads();
+    const double sq_res = sR[P];
+    if (!done) {
+      it_done = iter + 1;
+      if (sq_res < 1e-7 * 1e-7 || iter + 1 == C::maxIter) {
+        // time-averaged fluxes of this sweep = of the iterate before the update
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int v = 0; v < nV; v++) fh[d][v] = 0.0;
+        for (int t = 0; t < b; t++) {
+          double Q[nD];
+#pragma unroll
+          for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+          double Fl[DIM][nV];
+          PDE::template flux<DIM>(Q, Fl);
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int v = 0; v < nV; v++) fh[d][v] += Fl[d][v] * T.w[t];
+          if (TEMPS) {
+            double* dst = tmp.lFi + (((size_t)cell * b + t) * P + p) * (DIM + 1) * nV;
+#pragma unroll
+            for (int d = 0; d < DIM; d++)
+#pragma unroll
+              for (int v = 0; v < nV; v++) dst[d * nV + v] = Fl[d][v];
+          }
+        }
+        done = true;
+      }
+#pragma unroll
+      for (int l = 0; l < b; l++)
+#pragma unroll
+        for (int v = 0; v < nV; v++) sQ[(p * b + l) * nD + v] = qn[l][v];
+    }
+    if (p == 0) s_done[lc] = done;
+    if (!__syncthreads_or(!done)) break;
+  }
+  if (iters && active && p == 0) iters[cell] = it_done;
+
+  // time average of lQi (lQhi)
+  double qh[nD];
+#pragma unroll
+  for (int v = 0; v < nD; v++) {
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < b; m++) s += sQ[(p * b + m) * nD + v] * T.w[m];
+    qh[v] = s;
+  }
+  if (TEMPS && active) {
+    double* dq = tmp.lQi + ((size_t)cell * P + p) * b * nD;
+    for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * b * nD + i];
+    for (int v = 0; v < nD; v++) tmp.lQhi[((size_t)cell * P + p) * nD + v] = qh[v];
+    double* fhd = tmp.lFhi + (size_t)cell * (DIM + 1) * P * nV;
+    const int py = DIM == 3 ? (z * b + x) * b + y : x * b + y;
+    const int pz = (y * b + x) * b + z;
+    for (int v = 0; v < nV; v++) {
+      fhd[(0 * P + p) * nV + v] = fh[0][v];
+      fhd[(1 * P + py) * nV + v] = fh[1][v];
+      if (DIM == 3) fhd[(2 * P + pz) * nV + v] = fh[DIM - 1][v];
+      fhd[(DIM * P + p) * nV + v] = 0.0;
+    }
+  }
+  __syncthreads();
+  double* sQh = sQ;  // lQhi [P][nD]
+#pragma unroll
+  for (int v = 0; v < nD; v++) sQh[p * nD + v] = qh[v];
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+#pragma unroll
+    for (int v = 0; v < nV; v++) sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = fh[d][v];
+  if (p == 0) s_done[lc] = !active;
+  __syncthreads();
+
+  // extrapolated fluxes and the volume-integral line contractions
+  // (transposed stiffness, quadrature factor w_a w_c / dx), in place
+  for (int it = threadIdx.x; it < C::ITEMS; it += C::THREADS) {
+    const int v = it % nV;
+    const int L = (it / nV) % LINES;
+    const int d = (it / (nV * LINES)) % DIM;
+    const int c = it / (nV * LINES * DIM);
+    if (s_done[c]) continue;
+    const int slot_c = blockIdx.x * C::CPB + c;
+    const int cell_c = cell_list ? cell_list[slot_c] : slot_c;
+    double* base = sFall + c * C::SF + d * b * SLAB + L * nV + v;
+    double f[b];
+#pragma unroll
+    for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
+    double sl = 0.0, sr = 0.0;
+#pragma unroll
+    for (int l = 0; l < b; l++) {
+      sl += f[l] * T.FL[l];
+      sr += f[l] * T.FR[l];
+    }
+    lFhbnd[(((size_t)cell_c * 2 * DIM + 2 * d) * LINES + L) * nV + v] = sl;
+    lFhbnd[(((size_t)cell_c * 2 * DIM + 2 * d + 1) * LINES + L) * nV + v] = sr;
+    const int a0 = L / b, a1 = L % b;
+    const double idx = d == 0 ? invDx0 : d == 1 ? invDx1 : invDx2;
+    const double us = (DIM == 3 ? s_w[a0] : 1.0) * s_w[a1] * idx;
+#pragma unroll
+    for (int k = 0; k < b; k++) {
+      double s = 0.0;
+#pragma unroll
+      for (int m = 0; m < b; m++) s = fma(T.Kxi[k * b + m], f[m], s);
+      base[k * SLAB] = s * us;
+    }
+  }
+  // extrapolated states from lQhi lines
+  constexpr int QITEMS = C::CPB * DIM * LINES * nD;
+  for (int it = threadIdx.x; it < QITEMS; it += C::THREADS) {
+    const int v = it % nD;
+    const int L = (it / nD) % LINES;
+    const int d = (it / (nD * LINES)) % DIM;
+    const int c = it / (nD * LINES * DIM);
+    if (s_done[c]) continue;
+    const int slot_c = blockIdx.x * C::CPB + c;
+    const int cell_c = cell_list ? cell_list[slot_c] : slot_c;
+    const double* qh_c = smem + c * C::SQ;
+    const int a0 = L / b, a1 = L % b;
+    const int base = d == 0 ? (a0 * b + a1) * b : d == 1 ? a0 * b * b + a1 : a0 * b + a1;
+    const int stride = d == 0 ? 1 : d == 1 ? b : b * b;
+    const int bs = DIM == 3 ? base : (d == 0 ? a1 * b : a1);
+    double sl = 0.0, sr = 0.0;
+#pragma unroll
+    for (int l = 0; l < b; l++) {
+      const double q = qh_c[(bs + l * stride) * nD + v];
+      sl += q * T.FL[l];
+      sr += q * T.FR[l];
+    }
+    lQhbnd[(((size_t)cell_c * 2 * DIM + 2 * d) * LINES + L) * nD + v] = sl;
+    lQhbnd[(((size_t)cell_c * 2 * DIM + 2 * d + 1) * LINES + L) * nD + v] = sr;
+  }
+  __syncthreads();
+  if (!active || !lduh) return;
+  double* dst = lduh + ((size_t)cell * P + p) * nV;
+#pragma unroll
+  for (int v = 0; v < nV; v++) {
+    double du = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) du += sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+    dst[v] = du;
+  }
+}
+
+}  // namespace exa

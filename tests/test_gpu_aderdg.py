@@ -53,10 +53,13 @@ def widen(a, nvar, ndata):
     return out
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("dim,dt", [(2, 1.686854344081342e-3), (3, 1.083937460199773e-3)])
-def test_predictor_golden_gpu(eb, golden, dim, dt):
-    """GenericEulerKernelTest{2D,3D}::testSpaceTimePredictorNonlinear replayed on the GPU."""
+def test_predictor_golden_gpu(eb, golden, dim, dt, variant):
+    """GenericEulerKernelTest{2D,3D}::testSpaceTimePredictorNonlinear replayed on
+    the GPU, node form (variant 0) and line form (variant 1)."""
     s = eb.Solver(dim, 3, eb.PDE_EULER_TEST)
+    s.variant = variant
     b, nV, nD = 4, 5, 6
     P, F = b ** dim, b ** (dim - 1)
     g = "%dd/generic_euler/testSpaceTimePredictorNonlinear/" % dim
