@@ -54,10 +54,13 @@ struct PredictorCfg : Shape<DIM, N, PDE> {
   static constexpr int THREADS = VSPLIT * TPC;
   static constexpr int MIN_BLOCKS = MINB;
   static constexpr int NVT = (S::nV + VSPLIT - 1) / VSPLIT;  // variables per thread
-  static constexpr int SQ = S::P * S::b * S::nD;            // lQi per cell
   static constexpr int SF = DIM * S::P * S::nV;             // one flux slice per cell
   static constexpr int SR = VSPLIT * S::P + 1;              // residual partials + the cell's sum
   static constexpr int SK = S::b * S::b;                    // Kxi copy (per block)
+  // lQi node stride: odd (no bank conflicts across nodes) when that still fits
+  static constexpr int QS = sizeof(double) * (CPB * (S::P * (S::b * S::nD + 1) + SF + SR) + SK) <= 227 * 1024
+                                ? S::b * S::nD + 1 : S::b * S::nD;
+  static constexpr int SQ = S::P * QS;                      // lQi per cell
   static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR) + SK);
 };
 
@@ -71,7 +74,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
                      double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
                      Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp) {
   using C = PredictorCfg<DIM, N, PDE, VSPLIT, MINB>;
-  constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD, NVT = C::NVT;
+  constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD, NVT = C::NVT, QS = C::QS;
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
 
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
 #pragma unroll
       for (int t = 0; t < b; t++)
 #pragma unroll
-        for (int v = 0; v < nD; v++) sQ[(p * b + t) * nD + v] = q[v];
+        for (int v = 0; v < nD; v++) sQ[p * QS + t * nD + v] = q[v];
     }
   }
 
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
       if (!done && lead) {
         double Q[nD];
 #pragma unroll
-        for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+        for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
         double Fl[DIM][nV];
         PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
 #pragma unroll
         for (int j = 0; j < NVT; j++)
           if (v0 + j < nV) {
-            const double dq = qn[l][j] - sQ[(p * b + l) * nD + v0 + j];
+            const double dq = qn[l][j] - sQ[p * QS + l * nD + v0 + j];
             part = fma(dq, dq, part);
           }
     }
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
           for (int t = 0; t < b; t++) {
             double Q[nD];
 #pragma unroll
-            for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+            for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
             double Fl[DIM][nV];
             PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
       for (int l = 0; l < b; l++)
 #pragma unroll
         for (int j = 0; j < NVT; j++)
-          if (v0 + j < nV) sQ[(p * b + l) * nD + v0 + j] = qn[l][j];
+          if (v0 + j < nV) sQ[p * QS + l * nD + v0 + j] = qn[l][j];
     }
     if (!__syncthreads_or(!done)) break;
   }
@@ -276,13 +279,13 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
     for (int v = 0; v < nD; v++) {
       double s = 0.0;
 #pragma unroll
-      for (int m = 0; m < b; m++) s += sQ[(p * b + m) * nD + v] * T.w[m];
+      for (int m = 0; m < b; m++) s += sQ[p * QS + m * nD + v] * T.w[m];
       qh[v] = s;
     }
   }
   if (TEMPS && active && lead) {
     double* dq = tmp.lQi + ((size_t)cell * P + p) * b * nD;
-    for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * b * nD + i];
+    for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * QS + i];
     for (int v = 0; v < nD; v++) tmp.lQhi[((size_t)cell * P + p) * nD + v] = qh[v];
     // reference lFhi blocks: x (z,y,x), y (z,x,y), z (y,x,z), then the source block
     double* fhd = tmp.lFhi + (size_t)cell * (DIM + 1) * P * nV;

@@ -23,18 +23,32 @@
 
 namespace exa {
 
+// Stride of one n-slab of the line-major flux slice, chosen per (b, DIM) with
+// a shared-memory bank model (64-bit accesses, 16 bank pairs per half-warp)
+// over the three access patterns of a slice; the fallback is odd.
+constexpr int line_slab(int b, int dim, int lines5) {
+  return dim == 3 ? (b == 6 ? 190 : b == 4 ? 84 : b == 8 ? 322 : b == 5 ? 137 : lines5 + 1)
+                  : (b == 6 ? 30 : b == 4 ? 20 : b == 8 ? 42 : b == 5 ? 25 : lines5 + 1);
+}
+
 template <int DIM, int N, class PDE, int MINB>
 struct LinesCfg : Shape<DIM, N, PDE> {
   using S = Shape<DIM, N, PDE>;
   static constexpr int CPB = cells_per_block<S::P>();
   static constexpr int THREADS = CPB * S::P;
   static constexpr int LINES = S::P / S::b;  // lines per direction = face nodes
-  static constexpr int SLAB = LINES * S::nV + 1;  // one n-slab of one direction (odd stride)
-  static constexpr int SQ = S::P * S::b * S::nD;
-  static constexpr int SF = DIM * S::b * SLAB;
   static constexpr int SR = S::P + 1;
+  static constexpr int SLAB0 = S::nV == 5 ? line_slab(S::b, DIM, LINES * 5) : LINES * S::nV + 1;
+  // padded strides (bank-conflict-free) where they fit in 227 KB, packed otherwise
+  static constexpr bool kPad =
+      sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + DIM * S::b * SLAB0 + SR)) <= 227 * 1024;
+  static constexpr int SLAB = kPad ? SLAB0 : LINES * S::nV;
+  static constexpr int QS = kPad ? S::b * S::nD + 1 : S::b * S::nD;  // lQi node stride
+  static constexpr int SQ = S::P * QS;
+  static constexpr int SF = DIM * S::b * SLAB;
   static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR));
   static constexpr int ITEMS = CPB * DIM * LINES * S::nV;  // phase-B work items per block
+  static constexpr int IPT = (ITEMS + THREADS - 1) / THREADS;  // items per thread
 };
 
 // node p = (z, y, x) -> position n along direction d and line index L
@@ -51,7 +65,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
                            double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
                            Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp) {
   using C = LinesCfg<DIM, N, PDE, MINB>;
-  constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, SLAB = C::SLAB;
+  constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, SLAB = C::SLAB, QS = C::QS;
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
 
@@ -90,12 +104,35 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
 #pragma unroll
     for (int t = 0; t < b; t++)
 #pragma unroll
-      for (int v = 0; v < nD; v++) sQ[(p * b + t) * nD + v] = q[v];
+      for (int v = 0; v < nD; v++) sQ[p * QS + t * nD + v] = q[v];
   }
 
   // Which cells of the block still iterate; phase B skips converged cells.
   __shared__ int s_done[C::CPB];
   if (p == 0) s_done[lc] = !active;
+  __syncthreads();  // s_w
+  // this thread's phase-B items (direction, line, variable): slice offset,
+  // cell, and the line's quadrature factor w_a w_c dt / dx_d (times w_t later)
+  int it_off[C::IPT], it_cell[C::IPT];
+  double it_us[C::IPT];
+#pragma unroll
+  for (int k = 0; k < C::IPT; k++) {
+    const int it = threadIdx.x + k * C::THREADS;
+    it_off[k] = -1;
+    it_cell[k] = 0;
+    it_us[k] = 0.0;
+    if (it < C::ITEMS) {
+      const int v = it % nV;
+      const int L = (it / nV) % LINES;
+      const int d = (it / (nV * LINES)) % DIM;
+      const int c = it / (nV * LINES * DIM);
+      it_off[k] = c * C::SF + d * b * SLAB + L * nV + v;
+      it_cell[k] = c;
+      const int a0 = L / b, a1 = L % b;
+      const double idx = d == 0 ? invDx0 : d == 1 ? invDx1 : invDx2;
+      it_us[k] = (DIM == 3 ? s_w[a0] : 1.0) * s_w[a1] * dt * idx;
+    }
+  }
 
   double fh[DIM][nV];
   bool done = !active;
@@ -113,7 +150,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
       if (!done) {
         double Q[nD];
 #pragma unroll
-        for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+        for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
         double Fl[DIM][nV];
         PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -123,21 +160,14 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
       }
       __syncthreads();
       // B: line contractions, in place
-      for (int it = threadIdx.x; it < C::ITEMS; it += C::THREADS) {
-        const int v = it % nV;
-        const int L = (it / nV) % LINES;
-        const int d = (it / (nV * LINES)) % DIM;
-        const int c = it / (nV * LINES * DIM);
-        if (s_done[c]) continue;
-        double* base = sFall + c * C::SF + d * b * SLAB + L * nV + v;
+#pragma unroll
+      for (int k = 0; k < C::IPT; k++) {
+        if (it_off[k] < 0 || s_done[it_cell[k]]) continue;
+        double* base = sFall + it_off[k];
         double f[b];
 #pragma unroll
         for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
-        // quadrature factor of the line: w_t times the two transverse weights
-        const int a0 = L / b, a1 = L % b;
-        const double wa = DIM == 3 ? s_w[a0] : 1.0;
-        const double idx = d == 0 ? invDx0 : d == 1 ? invDx1 : invDx2;
-        const double us = (T.w[t] * wa) * s_w[a1] * dt * idx;
+        const double us = T.w[t] * it_us[k];
 #pragma unroll
         for (int l = 0; l < b; l++) {
           double s = 0.0;
@@ -168,7 +198,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
       for (int l = 0; l < b; l++)
 #pragma unroll
         for (int v = 0; v < nV; v++) {
-          const double dq = qn[l][v] - sQ[(p * b + l) * nD + v];
+          const double dq = qn[l][v] - sQ[p * QS + l * nD + v];
           part = fma(dq, dq, part);
         }
     }
@@ -201,7 +231,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
         for (int t = 0; t < b; t++) {
           double Q[nD];
 #pragma unroll
-          for (int v = 0; v < nD; v++) Q[v] = sQ[(p * b + t) * nD + v];
+          for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
           double Fl[DIM][nV];
           PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -221,7 +251,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
 #pragma unroll
       for (int l = 0; l < b; l++)
 #pragma unroll
-        for (int v = 0; v < nV; v++) sQ[(p * b + l) * nD + v] = qn[l][v];
+        for (int v = 0; v < nV; v++) sQ[p * QS + l * nD + v] = qn[l][v];
     }
     if (p == 0) s_done[lc] = done;
     if (!__syncthreads_or(!done)) break;
@@ -234,12 +264,12 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
   for (int v = 0; v < nD; v++) {
     double s = 0.0;
 #pragma unroll
-    for (int m = 0; m < b; m++) s += sQ[(p * b + m) * nD + v] * T.w[m];
+    for (int m = 0; m < b; m++) s += sQ[p * QS + m * nD + v] * T.w[m];
     qh[v] = s;
   }
   if (TEMPS && active) {
     double* dq = tmp.lQi + ((size_t)cell * P + p) * b * nD;
-    for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * b * nD + i];
+    for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * QS + i];
     for (int v = 0; v < nD; v++) tmp.lQhi[((size_t)cell * P + p) * nD + v] = qh[v];
     double* fhd = tmp.lFhi + (size_t)cell * (DIM + 1) * P * nV;
     const int py = DIM == 3 ? (z * b + x) * b + y : x * b + y;
