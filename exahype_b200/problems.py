@@ -102,3 +102,40 @@ def explosion_2d(order, cells=(81, 81), seed=0, radius=0.2):
     p = np.where(inside, 1.0, 0.1)
     vel = np.zeros(rho.shape + (3,))
     return conserved(rho, vel, p), dict(centre=c.tolist())
+
+
+def subcell_coordinates(dim, order, cells, offset=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0)):
+    """(ncells, (2N+1)^dim, dim) centres of the FV subcells of every cell (the
+    limiter's (2N+1)^d patch), subcells in (z, y, x) order with x fastest."""
+    B = 2 * order + 1
+    xs = (np.arange(B) + 0.5) / B
+    dx = [size[d] / cells[d] for d in range(dim)]
+    if dim == 2:
+        j, i = np.meshgrid(np.arange(cells[1]), np.arange(cells[0]), indexing="ij")
+        ny, nx = np.meshgrid(xs, xs, indexing="ij")
+        X = offset[0] + (i.ravel()[:, None] + nx.ravel()[None, :]) * dx[0]
+        Y = offset[1] + (j.ravel()[:, None] + ny.ravel()[None, :]) * dx[1]
+        return np.stack([X, Y], axis=-1)
+    k, j, i = np.meshgrid(np.arange(cells[2]), np.arange(cells[1]), np.arange(cells[0]), indexing="ij")
+    nz, ny, nx = np.meshgrid(xs, xs, xs, indexing="ij")
+    X = offset[0] + (i.ravel()[:, None] + nx.ravel()[None, :]) * dx[0]
+    Y = offset[1] + (j.ravel()[:, None] + ny.ravel()[None, :]) * dx[1]
+    Z = offset[2] + (k.ravel()[:, None] + nz.ravel()[None, :]) * dx[2]
+    return np.stack([X, Y, Z], axis=-1)
+
+
+def explosion(dim, order, cells, seed=0, radius=0.2):
+    """Circular/spherical explosion at the GL nodes and at the FV subcell
+    centres: inside |x - c| < radius rho = 1, p = 1, outside rho = 0.125,
+    p = 0.1, zero velocity; c ~ U[0.4, 0.6]^dim. Returns (luh, fv, params)."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.4, 0.6, size=dim)
+
+    def state(X):
+        inside = np.sum((X - c) ** 2, axis=-1) < radius * radius
+        rho = np.where(inside, 1.0, 0.125)
+        p = np.where(inside, 1.0, 0.1)
+        return conserved(rho, np.zeros(rho.shape + (3,)), p)
+
+    return (state(node_coordinates(dim, order, cells)), state(subcell_coordinates(dim, order, cells)),
+            dict(centre=c.tolist()))

@@ -2,6 +2,7 @@
  * over the C restatement of the kernels (oracle.c). */
 #include "oracle.h"
 #include "harness.c"
+#include "limiting_harness.c"
 
 static int be_pred(void* c, const double* luh, const double* dx, double dt, double* qb, double* fb, double* du) {
   return orc_predictor((const orc_solver*)c, luh, dx, dt, qb, fb, du, 0, 0, 0, 0);
@@ -43,3 +44,63 @@ double orc_mesh_time(void* h) { return ((orc_mesh*)h)->m->t; }
 double orc_mesh_dt(void* h) { return ((orc_mesh*)h)->m->dt; }
 long orc_mesh_steps(void* h) { return ((orc_mesh*)h)->m->steps; }
 long orc_mesh_sweeps(void* h) { return ((orc_mesh*)h)->m->sweeps; }
+
+/* ---- limiting mesh over the C restatement ---- */
+void orc_project_fv(const orc_solver* s, const double* luh, double* lim);
+void orc_project_dg(const orc_solver* s, const double* lim, double* luh);
+void orc_local_minmax(const orc_solver* s, const double* luh, double* mn, double* mx);
+void orc_limiter_minmax(const orc_solver* s, const double* lim, double* mn, double* mx);
+int orc_dmp(const orc_solver* s, const double* luh, double relax, double scale, double* minB, double* maxB);
+int orc_admissible(const orc_solver* s, const double* obsMin);
+double orc_musclhancock(const orc_solver* s, double* lnew, const double* lold, const double* dx, double dt);
+void orc_fv_ghost_fill(const orc_solver* s, double* lim, const double* nb, int face);
+void orc_fv_boundary_fill(const orc_solver* s, double* lim, int face);
+int orc_fv_patch_size(const orc_solver* s);
+
+static void lb_pfv(void* c, const double* u, double* l) { orc_project_fv((const orc_solver*)c, u, l); }
+static void lb_pdg(void* c, const double* l, double* u) { orc_project_dg((const orc_solver*)c, l, u); }
+static void lb_lmm(void* c, const double* l, double* a, double* b) { orc_limiter_minmax((const orc_solver*)c, l, a, b); }
+static void lb_smm(void* c, const double* u, double* a, double* b) { orc_local_minmax((const orc_solver*)c, u, a, b); }
+static int lb_dmp(void* c, const double* u, double r, double sc, double* a, double* b) { return orc_dmp((const orc_solver*)c, u, r, sc, a, b); }
+static int lb_adm(void* c, const double* m) { return orc_admissible((const orc_solver*)c, m); }
+static void lb_fvu(void* c, double* ln, const double* lo, const double* dx, double dt) { orc_musclhancock((const orc_solver*)c, ln, lo, dx, dt); }
+static void lb_fvg(void* c, double* l, const double* nb, int f) { orc_fv_ghost_fill((const orc_solver*)c, l, nb, f); }
+static void lb_fvb(void* c, double* l, int f) { orc_fv_boundary_fill((const orc_solver*)c, l, f); }
+
+typedef struct {
+  orc_solver s;
+  lhrn* r;
+} orc_lmesh;
+
+void* orc_lmesh_create(int dim, int order, const int* cells, const double* size, const int* bc, int nthreads,
+                       int helper_layers, int cure_steps, double relax, double scale) {
+  orc_lmesh* om = (orc_lmesh*)calloc(1, sizeof(orc_lmesh));
+  om->s.dim = dim;
+  om->s.order = order;
+  om->s.pde = 0;
+  hrn_backend k = {&om->s, dim, order, 5, 5, be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  lhrn_backend L = {lb_pfv, lb_pdg, lb_lmm, lb_smm, lb_dmp, lb_adm, lb_fvu, lb_fvg, lb_fvb, orc_fv_patch_size(&om->s)};
+  om->r = lhrn_create(&k, &L, cells, size, bc, nthreads, helper_layers, cure_steps, relax, scale);
+  return om;
+}
+void orc_lmesh_destroy(void* h) { orc_lmesh* om = (orc_lmesh*)h; lhrn_destroy(om->r); free(om); }
+void orc_lmesh_set_solution(void* h, const double* u) { hrn_mesh* m = ((orc_lmesh*)h)->r->m; memcpy(m->luh, u, nsol(m) * 8); }
+void orc_lmesh_get_solution(void* h, double* u) { hrn_mesh* m = ((orc_lmesh*)h)->r->m; memcpy(u, m->luh, nsol(m) * 8); }
+void orc_lmesh_init(void* h, double t0) { lhrn_init(((orc_lmesh*)h)->r, t0); }
+/* FV initial condition for cells that are limited at t0: [cell][(2N+1)^d][nV] */
+void orc_lmesh_set_fv_initial(void* h, const double* v) {
+  lhrn* r = ((orc_lmesh*)h)->r;
+  const int B = 2 * r->m->k.order + 1, Bd = r->m->dim == 3 ? B * B * B : B * B;
+  const size_t n = (size_t)r->m->ncells * Bd * r->m->k.nvar;
+  free(r->fv_ic);
+  r->fv_ic = (double*)malloc(sizeof(double) * n);
+  memcpy(r->fv_ic, v, sizeof(double) * n);
+}
+void orc_lmesh_step(void* h, int n) { for (int i = 0; i < n; i++) lhrn_step(((orc_lmesh*)h)->r); }
+int orc_lmesh_run_until(void* h, double t_end, int max_steps) { return lhrn_run_until(((orc_lmesh*)h)->r, t_end, max_steps); }
+double orc_lmesh_time(void* h) { return ((orc_lmesh*)h)->r->m->t; }
+double orc_lmesh_dt(void* h) { return ((orc_lmesh*)h)->r->m->dt; }
+long orc_lmesh_steps(void* h) { return ((orc_lmesh*)h)->r->m->steps; }
+long orc_lmesh_sweeps(void* h) { return ((orc_lmesh*)h)->r->m->sweeps; }
+void orc_lmesh_status(void* h, int* s) { lhrn* r = ((orc_lmesh*)h)->r; memcpy(s, r->s, sizeof(int) * r->m->ncells); }
+long orc_lmesh_irregular_steps(void* h) { return ((orc_lmesh*)h)->r->irregular_steps; }

@@ -218,3 +218,99 @@ class Mesh:
     def state(self):
         return dict(t=self._f("time")(self._h), dt=self._f("dt")(self._h), steps=self._f("steps")(self._h),
                     picard_sweeps=self._f("sweeps")(self._h))
+
+
+class LimitingMesh:
+    """Uniform mesh with the a-posteriori subcell limiter, run by the oracle's
+    limiting harness (oracle/limiting_harness.c) over the C restatement."""
+
+    def __init__(self, dim, order, cells, size, bc, helper_layers=1, cure_steps=0, relax=1e-4, scale=1e-3,
+                 nthreads=1):
+        self.dim, self.order = dim, order
+        l = lib()
+        ci = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        sz = (ctypes.c_double * 3)(*(list(size) + [1.0] * (3 - len(size))))
+        if isinstance(bc, int):
+            bc = [bc] * (2 * dim)
+        b = (ctypes.c_int * 6)(*(list(bc) + [0] * (6 - len(bc))))
+        l.orc_lmesh_create.restype = ctypes.c_void_p
+        for nm, rt in (("time", ctypes.c_double), ("dt", ctypes.c_double), ("steps", ctypes.c_long),
+                       ("sweeps", ctypes.c_long), ("run_until", ctypes.c_int), ("irregular_steps", ctypes.c_long)):
+            getattr(l, "orc_lmesh_" + nm).restype = rt
+        self._l = l
+        self._h = ctypes.c_void_p(l.orc_lmesh_create(dim, order, ci, sz, b, nthreads, helper_layers, cure_steps,
+                                                     ctypes.c_double(relax), ctypes.c_double(scale)))
+        self.ncells = int(np.prod(cells))
+        self.shape = (self.ncells, (order + 1) ** dim, 5)
+
+    def __del__(self):
+        try:
+            self._l.orc_lmesh_destroy(self._h)
+        except Exception:
+            pass
+
+    def set_solution(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self._l.orc_lmesh_set_solution(self._h, _p(u.reshape(-1)))
+
+    def get_solution(self):
+        u = np.empty(self.shape)
+        self._l.orc_lmesh_get_solution(self._h, _p(u.reshape(-1)))
+        return u
+
+    def set_fv_initial(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        self._l.orc_lmesh_set_fv_initial(self._h, _p(v.reshape(-1)))
+
+    def init(self, t0=0.0):
+        self._l.orc_lmesh_init(self._h, ctypes.c_double(t0))
+
+    def step(self, n=1):
+        self._l.orc_lmesh_step(self._h, int(n))
+
+    def run_until(self, t_end, max_steps=10 ** 9):
+        return self._l.orc_lmesh_run_until(self._h, ctypes.c_double(t_end), int(max_steps))
+
+    def status(self):
+        s = np.empty(self.ncells, dtype=np.int32)
+        self._l.orc_lmesh_status(self._h, _pi(s))
+        return s
+
+    def state(self):
+        f = self._l
+        return dict(t=f.orc_lmesh_time(self._h), dt=f.orc_lmesh_dt(self._h), steps=f.orc_lmesh_steps(self._h),
+                    picard_sweeps=f.orc_lmesh_sweeps(self._h), irregular_steps=f.orc_lmesh_irregular_steps(self._h))
+
+
+class RefLimitingMesh(LimitingMesh):
+    """The limiting harness over the reference's own kernels (oracle/_ref)."""
+
+    def __init__(self, dim, order, cells, size, bc, helper_layers=1, cure_steps=0, relax=1e-4, scale=1e-3,
+                 nthreads=1):
+        self.dim, self.order = dim, order
+        l = reflib(dim)
+        pre = "ref%dd_lmesh_" % dim
+        ci = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        sz = (ctypes.c_double * 3)(*(list(size) + [1.0] * (3 - len(size))))
+        if isinstance(bc, int):
+            bc = [bc] * (2 * dim)
+        b = (ctypes.c_int * 6)(*(list(bc) + [0] * (6 - len(bc))))
+        getattr(l, pre + "create").restype = ctypes.c_void_p
+        for nm, rt in (("time", ctypes.c_double), ("dt", ctypes.c_double), ("steps", ctypes.c_long),
+                       ("sweeps", ctypes.c_long), ("run_until", ctypes.c_int), ("irregular_steps", ctypes.c_long)):
+            getattr(l, pre + nm).restype = rt
+        self._l = _Prefixed(l, pre)
+        self._h = ctypes.c_void_p(getattr(l, pre + "create")(order, ci, sz, b, nthreads, helper_layers, cure_steps,
+                                                           ctypes.c_double(relax), ctypes.c_double(scale)))
+        self.ncells = int(np.prod(cells))
+        self.shape = (self.ncells, (order + 1) ** dim, 5)
+
+
+class _Prefixed:
+    """maps orc_lmesh_<name> to <prefix><name> of another library"""
+
+    def __init__(self, lib, prefix):
+        self._lib, self._pre = lib, prefix
+
+    def __getattr__(self, name):
+        return getattr(self._lib, self._pre + name.replace("orc_lmesh_", ""))

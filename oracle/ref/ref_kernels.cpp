@@ -232,6 +232,55 @@ double stable_dt(const double* luh, const double* dxa) {
   return kernels::aderdg::generic::c::stableTimeStepSize<S>(s, luh, vec(dxa));
 }
 
+// ---- limiter and FV kernels (Euler demonstrator PDE) ------------------------
+template <class S>
+void project_fv(const double* luh, double* lim) {
+  kernels::limiter::generic::c::projectOnFVLimiterSpace(luh, 5, S::Order + 1, S::GhostLayerWidth, lim);
+}
+template <class S>
+void project_dg(const double* lim, double* luh) {
+  kernels::limiter::generic::c::projectOnDGSpace(lim, 5, S::Order + 1, S::GhostLayerWidth, luh);
+}
+template <class S>
+void local_minmax(const double* luh, double* mn, double* mx) {
+  S s;
+  kernels::limiter::generic::c::findCellLocalMinAndMax(luh, &s, mn, mx);
+}
+template <class S>
+void limiter_minmax(const double* lim, double* mn, double* mx) {
+  S s;
+  kernels::limiter::generic::c::findCellLocalLimiterMinAndMax(lim, &s, S::GhostLayerWidth, mn, mx);
+}
+template <class S>
+int dmp(const double* luh, double relax, double scale, double* mn, double* mx) {
+  S s;
+  return kernels::limiter::generic::c::discreteMaximumPrincipleAndMinAndMaxSearch(luh, &s, relax, scale, mn, mx);
+}
+template <class S>
+double muscl(double* lnew, const double* lold, const double* dxa, double dt) {
+  S s;
+  return kernels::finitevolumes::musclhancock::c::solutionUpdate<false, false, true, S>(s, lnew, lold, vec(dxa), dt);
+}
+template <class S>
+void fv_ghost(double* lim, const double* nb, int face) {
+  S s;
+  tarch::la::Vector<DIMENSIONS, int> pos(0);
+  pos[face / 2] = (face % 2) ? 1 : -1;
+  kernels::finitevolumes::commons::c::ghostLayerFilling<S>(s, lim, nb, pos);
+}
+template <class S>
+void fv_boundary(double* lim, int face) {
+  S s;
+  constexpr int P = S::PatchSize, g = S::GhostLayerWidth;
+  double in[ipow(P, DIMENSIONS - 1) * g * 5], out[ipow(P, DIMENSIONS - 1) * g * 5];
+  tarch::la::Vector<DIMENSIONS, int> pos(0);
+  pos[face / 2] = (face % 2) ? 1 : -1;
+  Vec<DIMENSIONS> c(0.5), h(0.1);
+  kernels::finitevolumes::commons::c::boundaryLayerExtraction<S>(s, in, lim, pos);
+  kernels::finitevolumes::commons::c::boundaryConditions<S>(s, out, in, c, h, 0.0, 0.0, face, face / 2);
+  kernels::finitevolumes::commons::c::ghostLayerFillingAtBoundary<S>(s, lim, out, pos);
+}
+
 }  // namespace
 
 #define DISPATCH(pde, N, call)                                              \
@@ -251,6 +300,18 @@ double stable_dt(const double* luh, const double* dxa) {
         default: std::fprintf(stderr, "ref: order %d not built\n", N);     \
       }                                                                     \
     }                                                                       \
+  } while (0)
+
+// limiter / FV kernels exist for the demonstrator PDE only
+#define DISPATCH_EULER(N, call)                                          \
+  do {                                                                  \
+    switch (N) {                                                        \
+      case 3: { typedef EulerDemo<3> S; call; } break;                  \
+      case 4: { typedef EulerDemo<4> S; call; } break;                  \
+      case 5: { typedef EulerDemo<5> S; call; } break;                  \
+      case 7: { typedef EulerDemo<7> S; call; } break;                  \
+      default: std::fprintf(stderr, "ref: order %d not built\n", N);   \
+    }                                                                   \
   } while (0)
 
 extern "C" {
@@ -318,6 +379,31 @@ void REFNAME(solution_update)(int pde, int N, double* luh, const double* lduh, d
   REFNAME(init)();
   DISPATCH(pde, N, update<S>(luh, lduh, dt));
 }
+
+void REFNAME(project_fv)(int N, const double* luh, double* lim) { REFNAME(init)(); DISPATCH_EULER(N, project_fv<S>(luh, lim)); }
+void REFNAME(project_dg)(int N, const double* lim, double* luh) { REFNAME(init)(); DISPATCH_EULER(N, project_dg<S>(lim, luh)); }
+void REFNAME(local_minmax)(int N, const double* luh, double* mn, double* mx) {
+  REFNAME(init)();
+  DISPATCH_EULER(N, local_minmax<S>(luh, mn, mx));
+}
+void REFNAME(limiter_minmax)(int N, const double* lim, double* mn, double* mx) {
+  REFNAME(init)();
+  DISPATCH_EULER(N, limiter_minmax<S>(lim, mn, mx));
+}
+int REFNAME(dmp)(int N, const double* luh, double relax, double scale, double* mn, double* mx) {
+  REFNAME(init)();
+  int r = -1;
+  DISPATCH_EULER(N, r = dmp<S>(luh, relax, scale, mn, mx));
+  return r;
+}
+double REFNAME(musclhancock)(int N, double* lnew, const double* lold, const double* dx, double dt) {
+  REFNAME(init)();
+  double r = 0;
+  DISPATCH_EULER(N, r = muscl<S>(lnew, lold, dx, dt));
+  return r;
+}
+void REFNAME(fv_ghost)(int N, double* lim, const double* nb, int face) { DISPATCH_EULER(N, fv_ghost<S>(lim, nb, face)); }
+void REFNAME(fv_boundary)(int N, double* lim, int face) { DISPATCH_EULER(N, fv_boundary<S>(lim, face)); }
 
 double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx) {
   REFNAME(init)();

@@ -7,6 +7,7 @@
 
 extern "C" {
 #include "../harness.c"
+#include "../limiting_harness.c"
 }
 
 #if DIMENSIONS == 2
@@ -25,6 +26,14 @@ void REFNAME(surface_integral)(int pde, int N, double* lduh, const double* lFhbn
 void REFNAME(solution_update)(int pde, int N, double* luh, const double* lduh, double dt);
 double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx);
 void REFNAME(init)();
+void REFNAME(project_fv)(int N, const double* luh, double* lim);
+void REFNAME(project_dg)(int N, const double* lim, double* luh);
+void REFNAME(local_minmax)(int N, const double* luh, double* mn, double* mx);
+void REFNAME(limiter_minmax)(int N, const double* lim, double* mn, double* mx);
+int REFNAME(dmp)(int N, const double* luh, double relax, double scale, double* mn, double* mx);
+double REFNAME(musclhancock)(int N, double* lnew, const double* lold, const double* dx, double dt);
+void REFNAME(fv_ghost)(int N, double* lim, const double* nb, int face);
+void REFNAME(fv_boundary)(int N, double* lim, int face);
 }
 
 namespace {
@@ -69,4 +78,53 @@ double REFNAME(mesh_time)(void* h) { return ((RefMesh*)h)->m->t; }
 double REFNAME(mesh_dt)(void* h) { return ((RefMesh*)h)->m->dt; }
 long REFNAME(mesh_steps)(void* h) { return ((RefMesh*)h)->m->steps; }
 long REFNAME(mesh_sweeps)(void* h) { return ((RefMesh*)h)->m->sweeps; }
+}
+
+namespace {
+void lb_pfv(void* c, const double* u, double* l) { REFNAME(project_fv)(((Ctx*)c)->N, u, l); }
+void lb_pdg(void* c, const double* l, double* u) { REFNAME(project_dg)(((Ctx*)c)->N, l, u); }
+void lb_lmm(void* c, const double* l, double* a, double* b) { REFNAME(limiter_minmax)(((Ctx*)c)->N, l, a, b); }
+void lb_smm(void* c, const double* u, double* a, double* b) { REFNAME(local_minmax)(((Ctx*)c)->N, u, a, b); }
+int lb_dmp(void* c, const double* u, double r, double sc, double* a, double* b) { return REFNAME(dmp)(((Ctx*)c)->N, u, r, sc, a, b); }
+int lb_adm(void* c, const double* m) { return !(m[0] <= 0.0) && !(m[4] <= 0.0); }
+void lb_fvu(void* c, double* ln, const double* lo, const double* dx, double dt) { REFNAME(musclhancock)(((Ctx*)c)->N, ln, lo, dx, dt); }
+void lb_fvg(void* c, double* l, const double* nb, int f) { REFNAME(fv_ghost)(((Ctx*)c)->N, l, nb, f); }
+void lb_fvb(void* c, double* l, int f) { REFNAME(fv_boundary)(((Ctx*)c)->N, l, f); }
+struct RefLMesh { Ctx c; lhrn* r; };
+}
+
+extern "C" {
+void* REFNAME(lmesh_create)(int order, const int* cells, const double* size, const int* bc, int nthreads,
+                            int helper_layers, int cure_steps, double relax, double scale) {
+  REFNAME(init)();
+  RefLMesh* r = new RefLMesh();
+  r->c.pde = 0;
+  r->c.N = order;
+  const int B = 2 * order + 1, E = B + 4;
+  const int fv = (DIMENSIONS == 3 ? E * E * E : E * E) * 5;
+  hrn_backend k = {&r->c, DIMENSIONS, order, 5, 5, be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  lhrn_backend L = {lb_pfv, lb_pdg, lb_lmm, lb_smm, lb_dmp, lb_adm, lb_fvu, lb_fvg, lb_fvb, fv};
+  r->r = lhrn_create(&k, &L, cells, size, bc, nthreads, helper_layers, cure_steps, relax, scale);
+  return r;
+}
+void REFNAME(lmesh_destroy)(void* h) { RefLMesh* r = (RefLMesh*)h; lhrn_destroy(r->r); delete r; }
+void REFNAME(lmesh_set_solution)(void* h, const double* u) { hrn_mesh* m = ((RefLMesh*)h)->r->m; memcpy(m->luh, u, nsol(m) * 8); }
+void REFNAME(lmesh_get_solution)(void* h, double* u) { hrn_mesh* m = ((RefLMesh*)h)->r->m; memcpy(u, m->luh, nsol(m) * 8); }
+void REFNAME(lmesh_set_fv_initial)(void* h, const double* v) {
+  lhrn* r = ((RefLMesh*)h)->r;
+  const int B = 2 * r->m->k.order + 1, Bd = r->m->dim == 3 ? B * B * B : B * B;
+  const size_t n = (size_t)r->m->ncells * Bd * 5;
+  free(r->fv_ic);
+  r->fv_ic = (double*)malloc(sizeof(double) * n);
+  memcpy(r->fv_ic, v, sizeof(double) * n);
+}
+void REFNAME(lmesh_init)(void* h, double t0) { lhrn_init(((RefLMesh*)h)->r, t0); }
+void REFNAME(lmesh_step)(void* h, int n) { for (int i = 0; i < n; i++) lhrn_step(((RefLMesh*)h)->r); }
+int REFNAME(lmesh_run_until)(void* h, double t_end, int max_steps) { return lhrn_run_until(((RefLMesh*)h)->r, t_end, max_steps); }
+double REFNAME(lmesh_time)(void* h) { return ((RefLMesh*)h)->r->m->t; }
+double REFNAME(lmesh_dt)(void* h) { return ((RefLMesh*)h)->r->m->dt; }
+long REFNAME(lmesh_steps)(void* h) { return ((RefLMesh*)h)->r->m->steps; }
+long REFNAME(lmesh_sweeps)(void* h) { return ((RefLMesh*)h)->r->m->sweeps; }
+void REFNAME(lmesh_status)(void* h, int* s) { lhrn* r = ((RefLMesh*)h)->r; memcpy(s, r->s, sizeof(int) * r->m->ncells); }
+long REFNAME(lmesh_irregular_steps)(void* h) { return ((RefLMesh*)h)->r->irregular_steps; }
 }

@@ -107,3 +107,30 @@ def test_pde_fluxes_golden(golden):
         for d, name in enumerate("fgh"[:dim]):
             np.testing.assert_allclose(F[5 * d:5 * d + 5], golden["%dd/generic_euler/testPDEFluxes/%s" % (dim, name)],
                                        rtol=0, atol=EPS)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_limiter_projections_golden(golden, dim):
+    """limiter_testdata.cpp (LimiterKernelTest, N = 3, nVar = 5, no ghost
+    layers): luh -> subcell averages, luh -> Lobatto values, subcells -> luh."""
+    import ctypes
+    N, b, B, E, nV = 3, 4, 7, 11, 5
+    s = pyoracle._Solver(dim, N, 0)
+    g = "%dd/limiter/" % dim
+    luh = np.ascontiguousarray(golden[g + "testFromLuhConversion/luh_in"])
+    lim = np.zeros((E,) * dim + (nV,))
+    pyoracle.lib().orc_project_fv(ctypes.byref(s), pyoracle._p(luh), pyoracle._p(lim.reshape(-1)))
+    inner = lim[(slice(2, -2),) * dim].reshape(-1)
+    np.testing.assert_allclose(inner, golden[g + "testFromLuhConversion/lim_out"], rtol=0, atol=1e-10)
+    # Lobatto values with the generated uh2lob table ([j][i]: basis j at node i)
+    L = pyoracle.table("uh2lob", N).reshape(b, b)
+    u = luh.reshape((b,) * dim + (nV,))
+    lob = np.einsum("yxv,ya,xb->abv", u, L, L) if dim == 2 else np.einsum("zyxv,zc,ya,xb->cabv", u, L, L, L)
+    np.testing.assert_allclose(lob.reshape(-1), golden[g + "testFromLuhConversion/lob_out"], rtol=0, atol=1e-10)
+    lim2 = np.zeros((E,) * dim + (nV,))
+    lim2[(slice(2, -2),) * dim] = golden[g + "testToLuhConversion/lim_in"].reshape((B,) * dim + (nV,))
+    out = np.zeros(b ** dim * nV)
+    pyoracle.lib().orc_project_dg(ctypes.byref(s), pyoracle._p(np.ascontiguousarray(lim2.reshape(-1))),
+                                  pyoracle._p(out))
+    np.testing.assert_allclose(out, golden[g + "testToLuhConversion/luh_out"], rtol=0, atol=1e-10)
+
