@@ -253,3 +253,104 @@ class Mesh:
         """D2H copy of the solution into a (pinned) host pointer, ordered on the mesh stream."""
         _check(load().exa_mesh_copy_solution(self._h, ctypes.c_void_p(host_ptr), ctypes.c_size_t(nbytes), 0),
                "exa_mesh_copy_solution")
+
+
+class LimitingMesh:
+    """Uniform Cartesian mesh with the a-posteriori subcell limiter
+    (LimitingADERDGSolver): DG cells, FV-limited cells with MUSCL-Hancock
+    patches of (2N+1)^d subcells, limiter status spreading and local
+    recomputation, all device-resident. Euler PDE; periodic or outflow faces.
+
+    helper_layers, cure_steps, relax and scale are the reference's
+    helper-layers, steps-till-cured, DMP relaxation parameter (delta0) and
+    DMP difference scaling (epsilon)."""
+
+    def __init__(self, solver, cells, offset, size, bc, helper_layers=1, cure_steps=0, relax=1e-4, scale=1e-3):
+        lib = load()
+        d = solver.dim
+        c = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        o = _dbl3(list(offset) + [0.0] * (3 - len(offset)))
+        s = _dbl3(list(size) + [1.0] * (3 - len(size)))
+        if isinstance(bc, int):
+            bc = [bc] * (2 * d)
+        b = (ctypes.c_int * 6)(*(list(bc) + [0] * (6 - len(bc))))
+        h = ctypes.c_void_p()
+        _check(lib.exa_lmesh_create(solver._h, c, o, s, b, int(helper_layers), int(cure_steps), ctypes.c_double(relax),
+                                    ctypes.c_double(scale), ctypes.byref(h)), "exa_lmesh_create")
+        self._h = h
+        self.solver = solver
+        self.cells = tuple(cells)
+        self.ncells = int(np.prod(cells[:d]))
+        self.dx = [size[i] / cells[i] for i in range(d)]
+        B = 2 * solver.order + 1
+        self.patch_shape = ((B + 4) ** d, 5)
+        self.subcells = B ** d
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().exa_lmesh_destroy(self._h)
+        except Exception:
+            pass
+
+    @property
+    def solution_shape(self):
+        s = self.solver
+        return (self.ncells, (s.order + 1) ** s.dim, s.ndata)
+
+    def set_solution(self, luh):
+        a = np.ascontiguousarray(luh, dtype=np.float64)
+        assert a.size == int(np.prod(self.solution_shape))
+        _check(load().exa_lmesh_set_solution(self._h, a.ctypes.data_as(ctypes.c_void_p)), "exa_lmesh_set_solution")
+
+    def get_solution(self):
+        a = np.empty(self.solution_shape, dtype=np.float64)
+        _check(load().exa_lmesh_get_solution(self._h, a.ctypes.data_as(ctypes.c_void_p)), "exa_lmesh_get_solution")
+        return a
+
+    def set_fv_initial(self, fv):
+        """FV initial condition at the subcell centres, (ncells, (2N+1)^d, 5)."""
+        a = np.ascontiguousarray(fv, dtype=np.float64)
+        assert a.size == self.ncells * self.subcells * 5
+        _check(load().exa_lmesh_set_fv_initial(self._h, a.ctypes.data_as(ctypes.c_void_p)), "exa_lmesh_set_fv_initial")
+
+    def init(self, t0=0.0):
+        _check(load().exa_lmesh_init(self._h, ctypes.c_double(t0)), "exa_lmesh_init")
+
+    def step(self, nsteps=1):
+        _check(load().exa_lmesh_step(self._h, int(nsteps)), "exa_lmesh_step")
+
+    def run_until(self, t_end, max_steps=10 ** 9):
+        n = ctypes.c_int()
+        _check(load().exa_lmesh_run_until(self._h, ctypes.c_double(t_end), int(max_steps), ctypes.byref(n)),
+               "exa_lmesh_run_until")
+        return n.value
+
+    def state(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        st, sw, irr = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        _check(load().exa_lmesh_state(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st), ctypes.byref(sw),
+                                      ctypes.byref(irr)), "exa_lmesh_state")
+        return dict(t=t.value, dt=dt.value, steps=st.value, picard_sweeps=sw.value, irregular_steps=irr.value)
+
+    def status(self):
+        s = np.empty(self.ncells, dtype=np.int32)
+        _check(load().exa_lmesh_get_status(self._h, s.ctypes.data_as(ctypes.c_void_p)), "exa_lmesh_get_status")
+        return s
+
+    def limiter(self):
+        """(FV patches (ncells, E^d, 5) incl. ghost layers, allocated flags)"""
+        lim = np.empty((self.ncells,) + self.patch_shape, dtype=np.float64)
+        al = np.empty(self.ncells, dtype=np.int32)
+        _check(load().exa_lmesh_get_limiter(self._h, lim.ctypes.data_as(ctypes.c_void_p),
+                                            al.ctypes.data_as(ctypes.c_void_p)), "exa_lmesh_get_limiter")
+        return lim, al
+
+    def synchronize(self):
+        _check(load().exa_lmesh_synchronize(self._h), "exa_lmesh_synchronize")
+
+    @property
+    def stream_handle(self):
+        h = ctypes.c_void_p()
+        _check(load().exa_lmesh_stream(self._h, ctypes.byref(h)), "exa_lmesh_stream")
+        return h.value or 0

@@ -72,7 +72,8 @@ template <int DIM, int N, class PDE, bool TEMPS, int VSPLIT, int MINB>
 __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREADS, MINB)
     predictor_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                      double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
-                     Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp) {
+                     Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp,
+                     const int* __restrict__ count) {
   using C = PredictorCfg<DIM, N, PDE, VSPLIT, MINB>;
   constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD, NVT = C::NVT, QS = C::QS;
   extern __shared__ double smem[];
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
   const int v0 = part_id * NVT;
   const bool lead = part_id == 0;  // evaluates fluxes and owns the parameters
   const int slot = blockIdx.x * C::CPB + lc;
-  const bool active = slot < ncells;
+  const bool active = slot < (count ? min(*count, ncells) : ncells);  // count: optional device-side list length
   const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
 
   double* sQ = smem + lc * C::SQ;
@@ -512,7 +513,7 @@ template <int DIM, int N, class PDE>
 __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
     corrector_kernel(double* __restrict__ luh, const double* __restrict__ lduh, const double* __restrict__ lFhbnd,
                      const double* __restrict__ dt_ptr, double* __restrict__ dt_out, Geometry geo, int ncells,
-                     const int* __restrict__ cell_list, int do_update) {
+                     const int* __restrict__ cell_list, int do_update, const int* __restrict__ count) {
   using C = CorrectorCfg<DIM, N, PDE>;
   constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD;
   const OrderTables& T = c_tab[N];
@@ -520,7 +521,8 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
   const int lc = threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
   const int slot = blockIdx.x * C::CPB + lc;
-  const bool active = lc < C::CPB && slot < ncells;  // padding threads only join the reduction
+  // padding threads only join the reduction; count: optional device-side list length
+  const bool active = lc < C::CPB && slot < (count ? min(*count, ncells) : ncells);
   double dtmin = __longlong_as_double(0x7fefffffffffffffll);  // DBL_MAX
   if (active) {
     const int cell = cell_list ? cell_list[slot] : slot;

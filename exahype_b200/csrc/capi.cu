@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -14,6 +15,7 @@
 #include "../../include/exahype_b200.h"
 #include "aderdg.cuh"
 #include "predictor_lines.cuh"
+#include "limiter.cuh"
 
 namespace exa {
 
@@ -75,16 +77,20 @@ static int upload_tables() {
 // ---- per-(DIM, N, PDE) launchers ------------------------------------------
 struct KernelSet {
   int dim, order, pde, nvar, npar, P, F;
+  // (luh, lQhbnd, lFhbnd, lduh, iters, dt, geo, n, list, count, temps, with_temps, sweeps, variant, stream);
+  // count (optional, device) caps the list length at launch time
   int (*predictor)(const double*, double*, double*, double*, int*, const double*, Geometry, int, const int*,
-                   PredictorTemps, bool, unsigned long long*, int, cudaStream_t);
+                   const int*, PredictorTemps, bool, unsigned long long*, int, cudaStream_t);
   int (*riemann)(const double*, double*, const int*, const int*, const int*, int, cudaStream_t);
   int (*boundary)(const double*, double*, const int*, const int*, int, int, cudaStream_t);
   int (*corrector)(double*, const double*, const double*, const double*, double*, Geometry, int, const int*, int,
-                   cudaStream_t);
+                   const int*, cudaStream_t);
 };
 
 template <int DIM, int N, class PDE>
-__global__ void sweep_count_kernel(const int* iters, const int* cell_list, int n, unsigned long long* acc) {
+__global__ void sweep_count_kernel(const int* iters, const int* cell_list, int n, const int* count,
+                                   unsigned long long* acc) {
+  if (count) n = min(n, *count);
   unsigned long long s = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     s += (unsigned long long)iters[cell_list ? cell_list[i] : i];
@@ -103,7 +109,7 @@ struct Launch {
 
   template <bool TEMPS, int VS, int MB>
   static int launch_pred(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
-                         Geometry g, int n, const int* list, PredictorTemps tmp, cudaStream_t st) {
+                         Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, cudaStream_t st) {
     using PC = PredictorCfg<DIM, N, PDE, VS, MB>;
     static bool attr = false;
     if (!attr) {
@@ -113,14 +119,14 @@ struct Launch {
     }
     const int grid = (n + PC::CPB - 1) / PC::CPB;
     predictor_kernel<DIM, N, PDE, TEMPS, VS, MB><<<grid, PC::THREADS, PC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
-                                                                                     n, list, tmp);
+                                                                                     n, list, tmp, cnt);
     EXA_LAUNCHED();
     return EXA_OK;
   }
 
   template <bool TEMPS, int MB>
   static int launch_lines(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
-                          Geometry g, int n, const int* list, PredictorTemps tmp, cudaStream_t st) {
+                          Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, cudaStream_t st) {
     using LC = LinesCfg<DIM, N, PDE, MB>;
     static bool attr = false;
     if (!attr) {
@@ -130,7 +136,7 @@ struct Launch {
     }
     const int grid = (n + LC::CPB - 1) / LC::CPB;
     predictor_lines_kernel<DIM, N, PDE, TEMPS, MB><<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
-                                                                                       n, list, tmp);
+                                                                                       n, list, tmp, cnt);
     EXA_LAUNCHED();
     return EXA_OK;
   }
@@ -138,24 +144,24 @@ struct Launch {
   static constexpr bool kLines2 = 2 * LinesCfg<DIM, N, PDE, 2>::SMEM <= 227 * 1024;
 
   static int predictor(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
-                       Geometry g, int n, const int* list, PredictorTemps tmp, bool temps, unsigned long long* acc,
-                       int variant, cudaStream_t st) {
+                       Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, bool temps,
+                       unsigned long long* acc, int variant, cudaStream_t st) {
     if (n <= 0) return EXA_OK;
     int rc;
     if (temps)
-      rc = variant == 1 || variant == 2 ? launch_lines<true, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st)
-                                        : launch_pred<true, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+      rc = variant == 1 || variant == 2 ? launch_lines<true, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st)
+                                        : launch_pred<true, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else if (variant == 1 || (variant == 2 && !kLines2))
-      rc = launch_lines<false, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+      rc = launch_lines<false, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else if (variant == 2)
-      rc = launch_lines<false, kLines2 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+      rc = launch_lines<false, kLines2 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else if (variant == 3)
-      rc = launch_pred<false, 1, 2>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+      rc = launch_pred<false, 1, 2>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else
-      rc = launch_pred<false, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, tmp, st);
+      rc = launch_pred<false, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     if (rc) return rc;
     if (acc && iters) {
-      sweep_count_kernel<DIM, N, PDE><<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(iters, list, n, acc);
+      sweep_count_kernel<DIM, N, PDE><<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(iters, list, n, cnt, acc);
       EXA_LAUNCHED();
     }
     return EXA_OK;
@@ -173,10 +179,10 @@ struct Launch {
     return EXA_OK;
   }
   static int corrector(double* luh, const double* du, const double* fb, const double* dt, double* dtout, Geometry g,
-                       int n, const int* list, int upd, cudaStream_t st) {
+                       int n, const int* list, int upd, const int* cnt, cudaStream_t st) {
     if (n <= 0) return EXA_OK;
     corrector_kernel<DIM, N, PDE><<<(n + CC::CPB - 1) / CC::CPB, CC::THREADS, 0, st>>>(luh, du, fb, dt, dtout, g, n,
-                                                                                      list, upd);
+                                                                                      list, upd, cnt);
     EXA_LAUNCHED();
     return EXA_OK;
   }
@@ -333,7 +339,7 @@ int exa_space_time_predictor_nonlinear(const exa_solver* s, const double* luh, d
                                        const int* cell_list, int* iterations_dev, void* stream) {
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_nonlinear: null argument or negative count");
-  return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, cell_list,
+  return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, cell_list, nullptr,
                         PredictorTemps{}, false, nullptr, s->variant, (cudaStream_t)stream);
 }
 
@@ -343,7 +349,7 @@ int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* 
                                              double* lQhi, double* lFhi, void* stream) {
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0 || !lQi || !lFi || !lQhi || !lFhi)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_nonlinear_temps: null argument or negative count");
-  return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, nullptr,
+  return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, nullptr, nullptr,
                         PredictorTemps{lQi, lFi, lQhi, lFhi}, true, nullptr, s->variant, (cudaStream_t)stream);
 }
 
@@ -367,7 +373,7 @@ int exa_corrector(const exa_solver* s, double* luh, const double* lduh, const do
                   double* dt_min_dev, const double* dx, int ncells, const int* cell_list, int update, void* stream) {
   if (!s || !luh || !dx || ncells < 0 || (update && (!lduh || !lFhbnd || !dt_dev)))
     return fail(EXA_ERR_ARG, "exa_corrector: null argument or negative count");
-  return s->k.corrector(luh, lduh, lFhbnd, dt_dev, dt_min_dev, geom(s, dx), ncells, cell_list, update,
+  return s->k.corrector(luh, lduh, lFhbnd, dt_dev, dt_min_dev, geom(s, dx), ncells, cell_list, update, nullptr,
                         (cudaStream_t)stream);
 }
 
@@ -420,7 +426,7 @@ int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chos
   Geometry g{};
   for (int d = 0; d < 3; d++) g.dx[d] = 1.0 / 27.0;
   reset_min_kernel<<<1, 1, 0, st>>>(dt);
-  int rc = k.corrector(luh, nullptr, nullptr, nullptr, dt, g, (int)n, nullptr, 0, st);
+  int rc = k.corrector(luh, nullptr, nullptr, nullptr, dt, g, (int)n, nullptr, 0, nullptr, st);
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
@@ -430,7 +436,7 @@ int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chos
     float ms = 0.f, tot = 0.f;
     for (int r = 0; r < 4 && rc == EXA_OK; r++) {
       cudaEventRecord(a, st);
-      rc = k.predictor(luh, qb, fb, du, it, dt, g, (int)n, nullptr, PredictorTemps{}, false, nullptr, v, st);
+      rc = k.predictor(luh, qb, fb, du, it, dt, g, (int)n, nullptr, nullptr, PredictorTemps{}, false, nullptr, v, st);
       cudaEventRecord(b, st);
       cudaEventSynchronize(b);
       cudaEventElapsedTime(&ms, a, b);
@@ -616,7 +622,7 @@ static int mesh_predict(exa_mesh* m) {
   PhaseTimer pt(m, 0);
   m->phase_launches[0] += 2;
   return k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->scal + 0, m->geo, m->ncells, nullptr,
-                     PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
+                     nullptr, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
 }
 
 int exa_mesh_init(exa_mesh* m, double t0) {
@@ -626,7 +632,8 @@ int exa_mesh_init(exa_mesh* m, double t0) {
   EXA_LAUNCHED();
   EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, m->stream));
   // first admissible step from the initial data, then the first predictor
-  int rc = k.corrector(m->luh, nullptr, nullptr, nullptr, m->scal + 1, m->geo, m->ncells, nullptr, 0, m->stream);
+  int rc = k.corrector(m->luh, nullptr, nullptr, nullptr, m->scal + 1, m->geo, m->ncells, nullptr, 0, nullptr,
+                       m->stream);
   if (rc) return rc;
   take_dt_kernel<<<1, 1, 0, m->stream>>>(m->scal);
   EXA_LAUNCHED();
@@ -653,7 +660,8 @@ static int mesh_one_step(exa_mesh* m) {
   }
   {
     PhaseTimer pt(m, 2);
-    rc = k.corrector(m->luh, m->lduh, m->lFhbnd, m->scal + 0, m->scal + 1, m->geo, m->ncells, nullptr, 1, m->stream);
+    rc = k.corrector(m->luh, m->lduh, m->lFhbnd, m->scal + 0, m->scal + 1, m->geo, m->ncells, nullptr, 1, nullptr,
+                     m->stream);
     if (rc) return rc;
     m->phase_launches[2] += 1;
   }
@@ -780,6 +788,436 @@ int exa_mesh_synchronize(exa_mesh* m) {
   if (!m) return fail(EXA_ERR_ARG, "exa_mesh_synchronize: null mesh");
   EXA_CUDA(cudaStreamSynchronize(m->stream));
   return EXA_OK;
+}
+
+}  // extern "C"
+
+// ---- limiting mesh ------------------------------------------------------------
+struct exa_lmesh {
+  exa_mesh* m = nullptr;  // DG state, faces, stream and time scalars
+  int A = 2, T = 3, cure_steps = 0;
+  double relax = 1e-4, scale = 1e-3;
+  // s: limiter status; flags: [0] irregular change this step, [1] DG list
+  // length, [2] FV list length, [3] predictor list length
+  int *s = nullptr, *s_prev = nullptr, *cure = nullptr, *fs = nullptr, *has_lim = nullptr, *flags = nullptr;
+  int *listA = nullptr, *listF = nullptr, *listP = nullptr;
+  double *minB = nullptr, *maxB = nullptr, *lim = nullptr, *lim_prev = nullptr, *luh_prev = nullptr;
+  double *fv_ic = nullptr, *gscratch = nullptr;
+  int muscl_grid = 1;
+  size_t LS = 0, PB = 0;  // doubles per FV patch (ghosts included), subcells per cell
+  int (*init)(exa_lmesh*, double) = nullptr;
+  int (*step)(exa_lmesh*) = nullptr;
+  bool initialised = false;
+};
+
+namespace exa {
+
+// scal: [0] dt, [1] min target after the update, [2] t, [3] steps,
+//       [4] min target after a local recomputation, [5] irregular steps
+__global__ void lim_scalars_kernel(double* scal, double t0) {
+  scal[0] = 0.0;
+  scal[1] = __longlong_as_double(0x7fefffffffffffffll);
+  scal[2] = t0;
+  scal[3] = 0.0;
+  scal[4] = __longlong_as_double(0x7fefffffffffffffll);
+  scal[5] = 0.0;
+}
+
+// Time bookkeeping of a limiting step: on an irregular step the reference's
+// LocalRecomputation::endIteration runs startNewTimeStep() once more
+// (mappings/LocalRecomputation.cpp:193-207 after SolutionUpdate.cpp:308-322),
+// so the time stamp also advances by the step found after the update, and the
+// next step uses the one found after the recomputation.
+__global__ void lim_advance_kernel(double* scal, const int* flags) {
+  const bool irr = flags[0] != 0;
+  scal[2] += scal[0];
+  if (irr) scal[2] += scal[1];
+  scal[0] = irr ? scal[4] : scal[1];
+  scal[1] = __longlong_as_double(0x7fefffffffffffffll);
+  scal[4] = __longlong_as_double(0x7fefffffffffffffll);
+  scal[3] += 1.0;
+  if (irr) scal[5] += 1.0;
+}
+
+template <int DIM, int N>
+struct LimLaunch {
+  using PDE = EulerPDE;
+  using L = LimShape<DIM, N>;
+  using MC = MusclCfg<DIM, N>;
+  using PC = PostCfg<DIM, N>;
+  static constexpr int PROJ_TMP = tensor_tmp<DIM, L::b, L::B>() > tensor_tmp<DIM, L::B, L::b>()
+                                      ? tensor_tmp<DIM, L::b, L::B>() : tensor_tmp<DIM, L::B, L::b>();
+  static constexpr size_t PROJ_SMEM = sizeof(double) * PROJ_TMP;
+  static_assert(MC::SMEM <= 227 * 1024 && PC::SMEM <= 227 * 1024 && PROJ_SMEM <= 227 * 1024, "shared memory");
+
+  static int attrs() {
+    static bool done = false;
+    if (done) return EXA_OK;
+    EXA_CUDA(cudaFuncSetAttribute(lim_muscl_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)MC::SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_post_update_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)PC::SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_init_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)PC::SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_seed_kernel<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)PROJ_SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_reinit_kernel<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)PROJ_SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_recompute_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)PROJ_SMEM));
+    done = true;
+    return EXA_OK;
+  }
+  // MUSCL blocks resident on the device at once (grid-stride over the FV list)
+  static int muscl_grid(int ncells, int* grid) {
+    EXA_CUDA(cudaFuncSetAttribute(lim_muscl_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)MC::SMEM));
+    int dev = 0, sms = 0, per_sm = 0;
+    EXA_CUDA(cudaGetDevice(&dev));
+    EXA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    EXA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lim_muscl_kernel<DIM, N, PDE>, MC::THREADS,
+                                                           MC::SMEM));
+    *grid = std::max(1, std::min(ncells, sms * std::max(1, per_sm)));
+    return EXA_OK;
+  }
+  static size_t scratch_doubles() { return MC::kShared ? 0 : (size_t)MC::SCR; }
+  static LimParams params(const exa_lmesh* lm) { return LimParams{lm->A, lm->T, lm->cure_steps, lm->relax, lm->scale}; }
+
+  static int select(exa_lmesh* lm, int lo, int hi, int* list, int* count, const int* gate) {
+    exa_mesh* m = lm->m;
+    EXA_CUDA(cudaMemsetAsync(count, 0, sizeof(int), m->stream));
+    lim_select_kernel<<<(m->ncells + 255) / 256, 256, 0, m->stream>>>(m->ncells, lm->s, lo, hi, list, count, gate);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int merge(exa_lmesh* lm, int minmax, const int* gate) {
+    exa_mesh* m = lm->m;
+    if (m->nfaces <= 0) return EXA_OK;
+    lim_merge_faces_kernel<DIM><<<(m->nfaces + 127) / 128, 128, 0, m->stream>>>(
+        m->fl, m->fr, m->fd, m->nfaces, lm->s, lm->minB, lm->maxB, lm->fs, lm->T, minmax, gate);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int spread(exa_lmesh* lm, const int* gate) {  // T sweeps of limiter status spreading
+    exa_mesh* m = lm->m;
+    for (int it = 0; it < lm->T; it++) {
+      int rc = merge(lm, 0, gate);
+      if (rc) return rc;
+      lim_spread_cells_kernel<DIM, N><<<(m->ncells + 127) / 128, 128, 0, m->stream>>>(
+          m->ncells, lm->s, lm->cure, lm->fs, lm->has_lim, lm->lim, lm->lim_prev, params(lm), gate);
+      EXA_LAUNCHED();
+    }
+    return EXA_OK;
+  }
+  static int halo(exa_lmesh* lm, const int* gate) {
+    exa_mesh* m = lm->m;
+    const int nb = m->nbfaces[EXA_BC_OUTFLOW], total = m->nfaces + nb;
+    if (total <= 0) return EXA_OK;
+    lim_fv_halo_kernel<DIM, N><<<(total + 3) / 4, 128, 0, m->stream>>>(
+        m->fl, m->fr, m->fd, m->nfaces, m->bcell + m->boff[EXA_BC_OUTFLOW], m->bface + m->boff[EXA_BC_OUTFLOW], nb,
+        lm->s, lm->has_lim, lm->lim, lm->A, gate);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int muscl(exa_lmesh* lm, const int* gate) {
+    exa_mesh* m = lm->m;
+    lim_muscl_kernel<DIM, N, PDE><<<lm->muscl_grid, MC::THREADS, MC::SMEM, m->stream>>>(
+        lm->listF, lm->flags + 2, lm->lim, lm->lim_prev, m->luh, m->geo, m->scal + 0, lm->gscratch, gate);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int predict(exa_lmesh* lm) {  // cells with status < T (mappings/Prediction.cpp:176-178)
+    exa_mesh* m = lm->m;
+    int rc = select(lm, INT_MIN, lm->T, lm->listP, lm->flags + 3, nullptr);
+    if (rc) return rc;
+    return m->s->k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->scal + 0, m->geo, m->ncells,
+                             lm->listP, lm->flags + 3, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
+  }
+
+  static int init(exa_lmesh* lm, double t0) {
+    exa_mesh* m = lm->m;
+    const int n = m->ncells;
+    int rc = attrs();
+    if (rc) return rc;
+    lim_scalars_kernel<<<1, 1, 0, m->stream>>>(m->scal, t0);
+    EXA_LAUNCHED();
+    EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, m->stream));
+    EXA_CUDA(cudaMemsetAsync(lm->flags, 0, 4 * sizeof(int), m->stream));
+    lim_init_kernel<DIM, N, PDE><<<n, PC::THREADS, PC::SMEM, m->stream>>>(
+        n, m->luh, lm->s, lm->s_prev, lm->cure, lm->fs, lm->has_lim, lm->minB, lm->maxB, params(lm));
+    EXA_LAUNCHED();
+    if ((rc = spread(lm, nullptr))) return rc;
+    lim_seed_kernel<DIM, N><<<n, 128, PROJ_SMEM, m->stream>>>(n, lm->s, m->luh, lm->fv_ic, lm->lim);
+    EXA_LAUNCHED();
+    if ((rc = m->s->k.corrector(m->luh, nullptr, nullptr, nullptr, m->scal + 1, m->geo, n, nullptr, 0, nullptr,
+                                m->stream)))
+      return rc;
+    take_dt_kernel<<<1, 1, 0, m->stream>>>(m->scal);
+    EXA_LAUNCHED();
+    return predict(lm);
+  }
+
+  static int step(exa_lmesh* lm) {
+    exa_mesh* m = lm->m;
+    const KernelSet& k = m->s->k;
+    const int n = m->ncells;
+    const LimParams prm = params(lm);
+    cudaStream_t st = m->stream;
+    int rc;
+    EXA_CUDA(cudaMemsetAsync(lm->flags, 0, sizeof(int), st));
+    // merge: DMP min/max and facewise statuses; DG Riemann problems (the
+    // fluxes of faces between two FV-active cells are computed but never
+    // read); FV halo exchange and FV boundary on FV-active faces
+    if ((rc = merge(lm, 1, nullptr))) return rc;
+    if ((rc = k.riemann(m->lQhbnd, m->lFhbnd, m->fl, m->fr, m->fd, m->nfaces, st))) return rc;
+    if ((rc = k.boundary(m->lQhbnd, m->lFhbnd, m->bcell + m->boff[EXA_BC_OUTFLOW], m->bface + m->boff[EXA_BC_OUTFLOW],
+                         m->nbfaces[EXA_BC_OUTFLOW], EXA_BC_OUTFLOW, st)))
+      return rc;
+    if ((rc = halo(lm, nullptr))) return rc;
+    // update: DG cells (s < A) by the corrector, FV-active cells by MUSCL-Hancock
+    EXA_CUDA(cudaMemcpyAsync(lm->luh_prev, m->luh, (size_t)n * L::P * L::nV * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st));
+    if ((rc = select(lm, INT_MIN, lm->A, lm->listA, lm->flags + 1, nullptr))) return rc;
+    if ((rc = k.corrector(m->luh, m->lduh, m->lFhbnd, m->scal + 0, nullptr, m->geo, n, lm->listA, 1, lm->flags + 1,
+                          st)))
+      return rc;
+    if ((rc = select(lm, lm->A, INT_MAX, lm->listF, lm->flags + 2, nullptr))) return rc;
+    if ((rc = muscl(lm, nullptr))) return rc;
+    lim_post_update_kernel<DIM, N, PDE><<<n, PC::THREADS, PC::SMEM, st>>>(
+        n, m->luh, lm->s, lm->s_prev, lm->cure, lm->fs, lm->has_lim, lm->minB, lm->maxB, lm->lim, lm->lim_prev,
+        m->geo, prm, m->scal + 1, lm->flags);
+    EXA_LAUNCHED();
+    // irregular limiter domain change: every launch below returns at once
+    // unless the post-update kernel raised flags[0]
+    const int* g = lm->flags;
+    if ((rc = spread(lm, g))) return rc;
+    lim_reinit_kernel<DIM, N><<<n, 128, PROJ_SMEM, st>>>(n, m->luh, lm->luh_prev, lm->s, lm->s_prev, lm->cure,
+                                                          lm->has_lim, lm->lim, lm->lim_prev, prm, g);
+    EXA_LAUNCHED();
+    if ((rc = halo(lm, g))) return rc;
+    if ((rc = select(lm, lm->A, INT_MAX, lm->listF, lm->flags + 2, g))) return rc;
+    if ((rc = muscl(lm, g))) return rc;
+    lim_recompute_kernel<DIM, N, PDE><<<n, 128, PROJ_SMEM, st>>>(n, m->luh, lm->luh_prev, lm->s, lm->s_prev,
+                                                                  lm->lim, lm->lim_prev, m->geo, prm, m->scal + 4, g);
+    EXA_LAUNCHED();
+    lim_advance_kernel<<<1, 1, 0, st>>>(m->scal, lm->flags);
+    EXA_LAUNCHED();
+    return predict(lm);
+  }
+};
+
+struct LimOps {
+  int (*init)(exa_lmesh*, double);
+  int (*step)(exa_lmesh*);
+  int (*grid)(int, int*);
+  size_t (*scratch)();
+  size_t LS, PB;
+};
+
+static bool find_lim_ops(int dim, int order, LimOps* out) {
+#define X(D, NN, PDE_, ID)                                                                              \
+  if (dim == D && order == NN) {                                                                        \
+    using LL = LimLaunch<D, NN>;                                                                        \
+    *out = LimOps{&LL::init, &LL::step, &LL::muscl_grid, &LL::scratch_doubles, (size_t)LimShape<D, NN>::LS, \
+                  (size_t)LimShape<D, NN>::PB};                                                         \
+    return true;                                                                                        \
+  }
+  EXA_ORDERS_EULER(X, 2)
+  EXA_ORDERS_EULER(X, 3)
+#undef X
+  return false;
+}
+
+}  // namespace exa
+
+extern "C" {
+
+static void lmesh_free(exa_lmesh* lm) {
+  cudaFree(lm->s);
+  cudaFree(lm->s_prev);
+  cudaFree(lm->cure);
+  cudaFree(lm->fs);
+  cudaFree(lm->has_lim);
+  cudaFree(lm->flags);
+  cudaFree(lm->listA);
+  cudaFree(lm->listF);
+  cudaFree(lm->listP);
+  cudaFree(lm->minB);
+  cudaFree(lm->maxB);
+  cudaFree(lm->lim);
+  cudaFree(lm->lim_prev);
+  cudaFree(lm->luh_prev);
+  cudaFree(lm->fv_ic);
+  cudaFree(lm->gscratch);
+  if (lm->m) exa_mesh_destroy(lm->m);
+  lm->m = nullptr;
+}
+
+int exa_lmesh_create(const exa_solver* s, const int* cells, const double* offset, const double* size, const int* bc,
+                     int helper_layers, int cure_steps, double relax, double scale, exa_lmesh** out) {
+  if (!s || !cells || !offset || !size || !bc || !out) return fail(EXA_ERR_ARG, "exa_lmesh_create: null argument");
+  if (s->k.pde != EXA_PDE_EULER) return fail(EXA_ERR_UNSUPPORTED, "exa_lmesh_create: the limiter supports EXA_PDE_EULER");
+  if (helper_layers < 1 || helper_layers > 8 || cure_steps < 0 || !(relax >= 0) || !(scale >= 0))
+    return fail(EXA_ERR_ARG, "exa_lmesh_create: helper_layers 1..8, cure_steps >= 0, relax/scale >= 0");
+  for (int f = 0; f < 2 * s->k.dim; f++)
+    if (bc[f] != EXA_BC_PERIODIC && bc[f] != EXA_BC_OUTFLOW)
+      return fail(EXA_ERR_UNSUPPORTED, "exa_lmesh_create: boundary faces must be periodic or outflow");
+  LimOps ops{};
+  if (!find_lim_ops(s->k.dim, s->k.order, &ops))
+    return fail(EXA_ERR_UNSUPPORTED, "exa_lmesh_create: no limiter kernels for this order");
+  std::unique_ptr<exa_lmesh> lm(new exa_lmesh());
+  int rc = exa_mesh_create(s, cells, offset, size, bc, &lm->m);
+  if (rc) return rc;
+  lm->A = helper_layers + 1;
+  lm->T = 2 * helper_layers + 1;
+  lm->cure_steps = cure_steps;
+  lm->relax = relax;
+  lm->scale = scale;
+  lm->LS = ops.LS;
+  lm->PB = ops.PB;
+  lm->init = ops.init;
+  lm->step = ops.step;
+  const size_t n = lm->m->ncells, D2 = 2 * s->k.dim, P = s->k.P;
+  rc = ops.grid((int)n, &lm->muscl_grid);
+  if (rc) {
+    lmesh_free(lm.get());
+    return rc;
+  }
+  const size_t scr = ops.scratch();
+  bool ok = cudaMalloc(&lm->s, n * 4) == cudaSuccess && cudaMalloc(&lm->s_prev, n * 4) == cudaSuccess &&
+            cudaMalloc(&lm->cure, n * 4) == cudaSuccess && cudaMalloc(&lm->fs, n * D2 * 4) == cudaSuccess &&
+            cudaMalloc(&lm->has_lim, n * 4) == cudaSuccess && cudaMalloc(&lm->flags, 4 * 4) == cudaSuccess &&
+            cudaMalloc(&lm->listA, n * 4) == cudaSuccess && cudaMalloc(&lm->listF, n * 4) == cudaSuccess &&
+            cudaMalloc(&lm->listP, n * 4) == cudaSuccess && cudaMalloc(&lm->minB, n * D2 * 5 * 8) == cudaSuccess &&
+            cudaMalloc(&lm->maxB, n * D2 * 5 * 8) == cudaSuccess && cudaMalloc(&lm->lim, n * lm->LS * 8) == cudaSuccess &&
+            cudaMalloc(&lm->lim_prev, n * lm->LS * 8) == cudaSuccess &&
+            cudaMalloc(&lm->luh_prev, n * P * 5 * 8) == cudaSuccess &&
+            (scr == 0 || cudaMalloc(&lm->gscratch, (size_t)lm->muscl_grid * scr * 8) == cudaSuccess);
+  if (!ok) {
+    cudaGetLastError();
+    lmesh_free(lm.get());
+    return fail(EXA_ERR_NOMEM, "exa_lmesh_create: device allocation failed");
+  }
+  cudaStream_t st = lm->m->stream;
+  EXA_CUDA(cudaMemsetAsync(lm->s, 0, n * 4, st));
+  EXA_CUDA(cudaMemsetAsync(lm->s_prev, 0, n * 4, st));
+  EXA_CUDA(cudaMemsetAsync(lm->cure, 0, n * 4, st));
+  EXA_CUDA(cudaMemsetAsync(lm->fs, 0, n * D2 * 4, st));
+  EXA_CUDA(cudaMemsetAsync(lm->has_lim, 0, n * 4, st));
+  EXA_CUDA(cudaMemsetAsync(lm->flags, 0, 16, st));
+  EXA_CUDA(cudaMemsetAsync(lm->lim, 0, n * lm->LS * 8, st));
+  EXA_CUDA(cudaMemsetAsync(lm->lim_prev, 0, n * lm->LS * 8, st));
+  EXA_CUDA(cudaMemsetAsync(lm->luh_prev, 0, n * P * 5 * 8, st));
+  EXA_CUDA(cudaStreamSynchronize(st));
+  *out = lm.release();
+  return EXA_OK;
+}
+
+int exa_lmesh_destroy(exa_lmesh* lm) {
+  if (!lm) return EXA_OK;
+  lmesh_free(lm);
+  delete lm;
+  return EXA_OK;
+}
+
+int exa_lmesh_set_solution(exa_lmesh* lm, const double* h) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_set_solution: null mesh");
+  return exa_mesh_set_solution(lm->m, h);
+}
+
+int exa_lmesh_get_solution(exa_lmesh* lm, double* h) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_get_solution: null mesh");
+  return exa_mesh_get_solution(lm->m, h);
+}
+
+int exa_lmesh_set_fv_initial(exa_lmesh* lm, const double* h) {
+  if (!lm || !h) return fail(EXA_ERR_ARG, "exa_lmesh_set_fv_initial: null argument");
+  const size_t bytes = (size_t)lm->m->ncells * lm->PB * 5 * 8;
+  if (!lm->fv_ic && cudaMalloc(&lm->fv_ic, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    lm->fv_ic = nullptr;
+    return fail(EXA_ERR_NOMEM, "exa_lmesh_set_fv_initial: device allocation failed");
+  }
+  EXA_CUDA(cudaMemcpyAsync(lm->fv_ic, h, bytes, cudaMemcpyHostToDevice, lm->m->stream));
+  EXA_CUDA(cudaStreamSynchronize(lm->m->stream));
+  return EXA_OK;
+}
+
+int exa_lmesh_init(exa_lmesh* lm, double t0) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_init: null mesh");
+  int rc = lm->init(lm, t0);
+  if (rc) return rc;
+  lm->initialised = true;
+  return EXA_OK;
+}
+
+int exa_lmesh_step(exa_lmesh* lm, int nsteps) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_step: null mesh");
+  if (!lm->initialised) return fail(EXA_ERR_STATE, "exa_lmesh_step: call exa_lmesh_init first");
+  for (int i = 0; i < nsteps; i++) {
+    int rc = lm->step(lm);
+    if (rc) return rc;
+  }
+  return EXA_OK;
+}
+
+int exa_lmesh_state(exa_lmesh* lm, double* t, double* dt, long long* steps, long long* sweeps, long long* irregular) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_state: null mesh");
+  exa_mesh* m = lm->m;
+  double h[6];
+  unsigned long long sw = 0;
+  EXA_CUDA(cudaMemcpyAsync(h, m->scal, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+  EXA_CUDA(cudaMemcpyAsync(&sw, m->sweeps, 8, cudaMemcpyDeviceToHost, m->stream));
+  EXA_CUDA(cudaStreamSynchronize(m->stream));
+  if (t) *t = h[2];
+  if (dt) *dt = h[0];
+  if (steps) *steps = (long long)h[3];
+  if (sweeps) *sweeps = (long long)sw;
+  if (irregular) *irregular = (long long)h[5];
+  return EXA_OK;
+}
+
+int exa_lmesh_run_until(exa_lmesh* lm, double t_end, int max_steps, int* steps) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_run_until: null mesh");
+  if (!lm->initialised) return fail(EXA_ERR_STATE, "exa_lmesh_run_until: call exa_lmesh_init first");
+  int n = 0;
+  while (n < max_steps) {
+    double t, dt;
+    int rc = exa_lmesh_state(lm, &t, &dt, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    if (!(t < t_end && dt > 0.0)) break;
+    rc = lm->step(lm);
+    if (rc) return rc;
+    n++;
+  }
+  if (steps) *steps = n;
+  return EXA_OK;
+}
+
+int exa_lmesh_get_status(exa_lmesh* lm, int* h) {
+  if (!lm || !h) return fail(EXA_ERR_ARG, "exa_lmesh_get_status: null argument");
+  EXA_CUDA(cudaMemcpyAsync(h, lm->s, (size_t)lm->m->ncells * 4, cudaMemcpyDeviceToHost, lm->m->stream));
+  EXA_CUDA(cudaStreamSynchronize(lm->m->stream));
+  return EXA_OK;
+}
+
+int exa_lmesh_get_limiter(exa_lmesh* lm, double* lim, int* allocated) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_get_limiter: null mesh");
+  const size_t n = lm->m->ncells;
+  if (lim) EXA_CUDA(cudaMemcpyAsync(lim, lm->lim, n * lm->LS * 8, cudaMemcpyDeviceToHost, lm->m->stream));
+  if (allocated) EXA_CUDA(cudaMemcpyAsync(allocated, lm->has_lim, n * 4, cudaMemcpyDeviceToHost, lm->m->stream));
+  EXA_CUDA(cudaStreamSynchronize(lm->m->stream));
+  return EXA_OK;
+}
+
+int exa_lmesh_synchronize(exa_lmesh* lm) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_synchronize: null mesh");
+  return exa_mesh_synchronize(lm->m);
+}
+
+int exa_lmesh_stream(exa_lmesh* lm, void** stream) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_stream: null mesh");
+  return exa_mesh_stream(lm->m, stream);
 }
 
 }  // extern "C"

@@ -63,7 +63,8 @@ template <int DIM, int N, class PDE, bool TEMPS, int MINB>
 __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
     predictor_lines_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                            double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
-                           Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp) {
+                           Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp,
+                           const int* __restrict__ count) {
   using C = LinesCfg<DIM, N, PDE, MINB>;
   constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, SLAB = C::SLAB, QS = C::QS;
   extern __shared__ double smem[];
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
   const int lc = threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
   const int slot = blockIdx.x * C::CPB + lc;
-  const bool active = slot < ncells;
+  const bool active = slot < (count ? min(*count, ncells) : ncells);  // count: optional device-side list length
   const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
   double* sQ = smem + lc * C::SQ;
   double* sF = smem + C::CPB * C::SQ + lc * C::SF;

@@ -149,6 +149,54 @@ int exa_mesh_stream(exa_mesh* m, void** stream);
 int exa_mesh_set_profiling(exa_mesh* m, int on);
 int exa_mesh_phase_times(exa_mesh* m, double* ms4, long long* launches4, int reset);
 
+/* ---- uniform mesh with the a-posteriori subcell limiter ------------------- */
+/* The LimitingADERDGSolver (exahype/solvers/LimitingADERDGSolver.h:82-1508)
+ * over the uniform mesh: every cell carries a limiter status, DMP min/max
+ * blocks per face and, while its status is > 0, an FV patch of (2N+1)^d
+ * subcells with 2 ghost layers (MUSCL-Hancock, minmod, Rusanov;
+ * GenericFiniteVolumesMUSCLHancockInC). Euler PDE only (EXA_PDE_EULER);
+ * boundary faces must be periodic or outflow.
+ *   helper_layers h: activeFV status A = h+1, troubled status T = 2h+1
+ *     (LimitingADERDGSolver.h:452-458 and the generated solver's constructor);
+ *   cure_steps: iterationsToCureTroubledCell (:452-458), the specification
+ *     file's steps-till-cured (EulerADERDG.exahype:62 uses 10);
+ *   relax / scale: DMPRelaxationParameter (delta0) and DMPDifferenceScaling
+ *     (epsilon) of the discrete maximum principle, 1e-4 / 1e-3 by default.
+ * The step follows the reference's non-fused limiting sequence
+ * (mergeNeighboursBasedOnLimiterStatus :1146, updateSolution :873,
+ * determineLimiterStatusAfterSolutionUpdate :304, then on an irregular limiter
+ * domain change limiter status spreading, reinitialiseSolversLocally :1006 and
+ * recomputeSolutionLocally :1029, and the prediction of every cell with
+ * status < T) without host synchronisation. */
+typedef struct exa_lmesh exa_lmesh;
+int exa_lmesh_create(const exa_solver* s, const int* cells, const double* offset, const double* size, const int* bc,
+                     int helper_layers, int cure_steps, double relax, double scale, exa_lmesh** out);
+int exa_lmesh_destroy(exa_lmesh* m);
+/* host <-> device DG solution (layout and cell order of exa_mesh) */
+int exa_lmesh_set_solution(exa_lmesh* m, const double* luh_host);
+int exa_lmesh_get_solution(exa_lmesh* m, double* luh_host);
+/* Optional FV initial condition at the subcell centres, [cell][(2N+1)^d][5]
+ * (the FV solver's adjustSolution at t = 0); limiter patches allocated at
+ * initialisation start from it instead of from the DG projection. */
+int exa_lmesh_set_fv_initial(exa_lmesh* m, const double* fv_host);
+/* Initial limiter status from the physical admissibility of the initial data,
+ * status spreading, first admissible step and first predictor
+ * (LimitingADERDGSolver::setInitialConditions :849, Runner.cpp:681-700). */
+int exa_lmesh_init(exa_lmesh* m, double t0);
+int exa_lmesh_step(exa_lmesh* m, int nsteps);
+int exa_lmesh_run_until(exa_lmesh* m, double t_end, int max_steps, int* steps);
+/* time, current step size, steps, Picard sweeps, steps with an irregular
+ * limiter domain change (local recomputation) */
+int exa_lmesh_state(exa_lmesh* m, double* t, double* dt, long long* steps, long long* picard_sweeps,
+                    long long* irregular_steps);
+/* limiter status per cell (0 DG, 1..h helper, A..T-1 FV-active, T troubled) */
+int exa_lmesh_get_status(exa_lmesh* m, int* status_host);
+/* FV patches [cell][E^d][5], E = 2N+5 (ghost layers included; cells whose
+ * patch is not allocated hold stale values) and per-cell allocation flags */
+int exa_lmesh_get_limiter(exa_lmesh* m, double* lim_host, int* allocated_host);
+int exa_lmesh_synchronize(exa_lmesh* m);
+int exa_lmesh_stream(exa_lmesh* m, void** stream);
+
 /* Measurement helper (no counterpart in the reference): sustained FP64 FMA
  * throughput of the current GPU in TFLOP/s, from independent DFMA chains on
  * every SM timed with CUDA events -- the FP64 roofline of the predictor. */

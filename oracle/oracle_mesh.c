@@ -104,3 +104,9 @@ long orc_lmesh_steps(void* h) { return ((orc_lmesh*)h)->r->m->steps; }
 long orc_lmesh_sweeps(void* h) { return ((orc_lmesh*)h)->r->m->sweeps; }
 void orc_lmesh_status(void* h, int* s) { lhrn* r = ((orc_lmesh*)h)->r; memcpy(s, r->s, sizeof(int) * r->m->ncells); }
 long orc_lmesh_irregular_steps(void* h) { return ((orc_lmesh*)h)->r->irregular_steps; }
+/* FV patches [cell][E^d][nV] (ghost layers included) and allocation flags */
+void orc_lmesh_limiter(void* h, double* lim, int* allocated) {
+  lhrn* r = ((orc_lmesh*)h)->r;
+  if (lim) memcpy(lim, r->lim, sizeof(double) * (size_t)r->m->ncells * r->L.fv_size);
+  if (allocated) memcpy(allocated, r->has_lim, sizeof(int) * r->m->ncells);
+}

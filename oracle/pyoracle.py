@@ -276,6 +276,14 @@ class LimitingMesh:
         self._l.orc_lmesh_status(self._h, _pi(s))
         return s
 
+    def limiter(self):
+        """(FV patches (ncells, E^d, 5) incl. ghost layers, allocated flags)"""
+        B = 2 * self.order + 1
+        lim = np.empty((self.ncells, (B + 4) ** self.dim, 5))
+        al = np.empty(self.ncells, dtype=np.int32)
+        self._l.orc_lmesh_limiter(self._h, _p(lim.reshape(-1)), _pi(al))
+        return lim, al
+
     def state(self):
         f = self._l
         return dict(t=f.orc_lmesh_time(self._h), dt=f.orc_lmesh_dt(self._h), steps=f.orc_lmesh_steps(self._h),

@@ -127,4 +127,9 @@ long REFNAME(lmesh_steps)(void* h) { return ((RefLMesh*)h)->r->m->steps; }
 long REFNAME(lmesh_sweeps)(void* h) { return ((RefLMesh*)h)->r->m->sweeps; }
 void REFNAME(lmesh_status)(void* h, int* s) { lhrn* r = ((RefLMesh*)h)->r; memcpy(s, r->s, sizeof(int) * r->m->ncells); }
 long REFNAME(lmesh_irregular_steps)(void* h) { return ((RefLMesh*)h)->r->irregular_steps; }
+void REFNAME(lmesh_limiter)(void* h, double* lim, int* allocated) {
+  lhrn* r = ((RefLMesh*)h)->r;
+  if (lim) memcpy(lim, r->lim, sizeof(double) * (size_t)r->m->ncells * r->L.fv_size);
+  if (allocated) memcpy(allocated, r->has_lim, sizeof(int) * r->m->ncells);
+}
 }
