@@ -14,6 +14,11 @@ Prints one JSON line (rank 0). Under torchrun every rank runs an independent
 replica of the workload (the solver is single-GPU; replicas only).
 Metric: DoF-updates/s, one DoF-update = one (cell, node, conserved variable)
 advanced by one step (ncells * 216 * 5 per step).
+
+Besides the headline line's own keys, "limiter" reports the a-posteriori
+limiter workload measured in the same run: 2D Euler N=5 circular explosion on
+81x81 outflow cells, 11x11 MUSCL-Hancock subcells, DMP delta0 1e-4 and
+epsilon 1e-3, run to t = 0.2 (--workload limiter prints it as its own line).
 """
 import argparse
 import json
@@ -31,7 +36,12 @@ sys.path.insert(0, REPO)
 DIM, ORDER, CELLS, SEED = 3, 5, (27, 27, 27), 0
 NVAR = 5
 WORKLOAD = "euler3d_N5_27^3_periodic_4pulses"
-METRIC = "ADER-DG DoF-updates/s (FP64, 3D Euler N=5, 27^3 periodic)"
+METRIC = "ADER-DG DoF-updates/s on 1 B200, mixed vs FP64 at \u22641e-9 L2; p99 solve latency"
+LIM_DIM, LIM_ORDER, LIM_CELLS, LIM_TEND = 2, 5, (81, 81), 0.2
+LIM_WORKLOAD = "euler2d_N5_81^2_explosion_limiter_outflow_t0.2"
+# per-launch DRAM traffic of the predictor from the committed ncu capture
+PROFILE_PREDICTOR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                                 "predictor_euler3d_N5_27cubed.md")
 
 
 def dof_per_step():
@@ -127,6 +137,31 @@ class ClockSampler:
         if not sm:
             return None
         return dict(sm_mhz=float(np.median(sm)), sm_max_mhz=mx, reasons=sorted(reasons), samples=len(sm))
+
+
+def predictor_traffic_bytes():
+    """dram__bytes_read.sum + dram__bytes_write.sum of one predictor launch on
+    the 27^3 N=5 mesh, from the line 'traffic_bytes_per_launch: <n>' of the
+    committed ncu summary (None if absent)."""
+    try:
+        with open(PROFILE_PREDICTOR) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip().split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def reduce_max(x, world, device=None):
+    """max over ranks of a scalar (identity for one rank)"""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def dist_env():
@@ -233,10 +268,7 @@ def run_ours(a):
     ph = m.phase_times(reset=True)
     st1 = m.state()
     sweeps = st1["picard_sweeps"] - st0["picard_sweeps"]
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = reduce_max(ms_total, world, dev)
     dof = dof_per_step() * a.steps * world
     value = dof / (ms_total / 1000.0)
 
@@ -259,7 +291,7 @@ def run_ours(a):
             kernels[name] = dict(bound="hbm", achieved=ach, unit="GB/s", ms=t_ms, peak=peaks["hbm_gbs"],
                                  frac=ach / peaks["hbm_gbs"])
     roof = dict(kernels["predictor"])
-    roof.update(traffic=None, peak_source="fp64 DFMA probe measured in this run (exa_fp64_peak_probe); "
+    roof.update(traffic=predictor_traffic_bytes(), peak_source="fp64 DFMA probe measured in this run (exa_fp64_peak_probe); "
                 "MEASURED_PEAKS.json has no FP64 figure",
                 algorithmic_flops_per_launch=pflops, picard_sweeps_per_cell=sweeps / a.steps / ncells)
 
@@ -281,10 +313,7 @@ def run_ours(a):
         f1.record(stream)
         f1.synchronize()
         e2e_ms = f0.elapsed_time(f1)
-        if world > 1:
-            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = reduce_max(e2e_ms, world, dev)
         e2e = {"value": dof_per_step() * ke * world / (e2e_ms / 1e3), "unit": "DoF-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ke,
                "api": "exa_mesh_copy_solution(H2D) + exa_mesh_step(1) + exa_mesh_copy_solution(D2H)"}
@@ -298,6 +327,7 @@ def run_ours(a):
                    "sample": "1 full time step of the 27^3 mesh (after the initial predictor) on the "
                              "reference's generic kernels, %.1f s" % r["seconds"]}
     launches = sum(v[1] for v in ph.values())
+    lim = None if a.no_limiter else run_limiter_workload(a, world, dev, rank)
     line = {
         "metric": METRIC, "value": value, "unit": "DoF-updates/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -307,12 +337,67 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
+        "limiter": lim,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def run_limiter_workload(a, world, dev, rank):
+    """The limiter workload to t = 0.2 (after init), timed with CUDA events on
+    the mesh stream; max over ranks. DoF-updates/s counts every cell (DG or
+    FV-limited) as (N+1)^2 nodes x 5 variables per step."""
+    import torch
+    import exahype_b200 as eb
+    from exahype_b200 import problems
+    luh, fv, _ = problems.explosion(LIM_DIM, LIM_ORDER, LIM_CELLS, seed=SEED + rank)
+    s = eb.Solver(LIM_DIM, LIM_ORDER, eb.PDE_EULER)
+    s.autotune(int(np.prod(LIM_CELLS)))
+    m = eb.LimitingMesh(s, LIM_CELLS, [0.0] * LIM_DIM, [1.0] * LIM_DIM, eb.BC_OUTFLOW, helper_layers=1, cure_steps=0)
+    m.set_solution(luh)
+    m.set_fv_initial(fv)
+    m.init(0.0)
+    m.synchronize()
+    stream = torch.cuda.ExternalStream(m.stream_handle, device=dev)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    if a.limiter_steps:
+        m.step(a.limiter_steps)
+        n = a.limiter_steps
+    else:
+        n = m.run_until(LIM_TEND)
+    e1.record(stream)
+    e1.synchronize()
+    ms = reduce_max(e0.elapsed_time(e1), world, dev)
+    st = m.state()
+    status = m.status()
+    dof_step = int(np.prod(LIM_CELLS)) * (LIM_ORDER + 1) ** LIM_DIM * NVAR
+    out = {"workload": LIM_WORKLOAD, "value": dof_step * n * world / (ms / 1e3), "unit": "DoF-updates/s",
+           "steps": n, "ms_per_step": ms / max(n, 1), "t_end": st["t"], "irregular_steps": st["irregular_steps"],
+           "picard_sweeps": st["picard_sweeps"], "final_status_counts": np.bincount(status, minlength=4).tolist(),
+           "timing": "exa_lmesh_run_until(0.2) incl. its per-step host check of t and dt, CUDA events"}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import pyoracle
+        if pyoracle.ref_available(LIM_DIM):
+            nthreads = os.cpu_count() or 1
+            r = pyoracle.RefLimitingMesh(LIM_DIM, LIM_ORDER, LIM_CELLS, [1.0] * LIM_DIM, 0, nthreads=nthreads)
+            r.set_solution(luh)
+            r.set_fv_initial(fv)
+            r.init(0.0)
+            k = 8
+            t0 = time.perf_counter()
+            r.step(k)
+            el = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": dof_step * k / el, "unit": "DoF-updates/s", "cores": nthreads,
+                                   "kind": "reference",
+                                   "sample": "the first %d steps of the same workload on the reference's "
+                                             "limiter/MUSCL-Hancock/ADER-DG kernels, %.1f s" % (k, el)}
+    return out
 
 
 def measure_fp64_peak():
@@ -337,10 +422,32 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-probe", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="predictor variant (default: autotune)")
+    ap.add_argument("--no-limiter", action="store_true", help="skip the limiter workload")
+    ap.add_argument("--limiter-steps", type=int, default=0, help="limiter workload: K steps instead of t = 0.2")
+    ap.add_argument("--workload", default="headline", choices=["headline", "limiter"],
+                    help="limiter: only the limiter workload, as its own JSON line")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
+    if a.workload == "limiter":
+        return run_limiter_only(a)
     return run_ours(a)
+
+
+def run_limiter_only(a):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    r = run_limiter_workload(a, world, torch.device("cuda", local), rank)
+    if rank == 0:
+        print(json.dumps(dict(r, metric=METRIC, n_gpus=world, dtype="f64", data="synthetic (seeded explosion)")),
+              flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
 
 
 if __name__ == "__main__":
