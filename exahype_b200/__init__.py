@@ -135,6 +135,28 @@ class Solver:
                                     _dbl3(dx), int(ncells), _ptr(cell_list), int(bool(update)), _stream(stream)),
                "exa_corrector")
 
+    # -- limiter kernels (Euler); FV patches lim[cell][(2N+5)^d][5] --
+    def project_on_fv_limiter_space(self, luh, lim, ncells, cell_list=None, stream=None):
+        _check(load().exa_project_on_fv_limiter_space(self._h, _ptr(luh), _ptr(lim), int(ncells), _ptr(cell_list),
+                                                      _stream(stream)), "exa_project_on_fv_limiter_space")
+
+    def project_on_dg_space(self, lim, luh, ncells, cell_list=None, stream=None):
+        _check(load().exa_project_on_dg_space(self._h, _ptr(lim), _ptr(luh), int(ncells), _ptr(cell_list),
+                                              _stream(stream)), "exa_project_on_dg_space")
+
+    def fv_musclhancock_scratch_bytes(self, ncells):
+        b = ctypes.c_size_t()
+        _check(load().exa_fv_musclhancock_scratch_bytes(self._h, int(ncells), ctypes.byref(b)),
+               "exa_fv_musclhancock_scratch_bytes")
+        return b.value
+
+    def fv_musclhancock_update(self, lim, lim_old, luh, dt_dev, dx, ncells, cell_list=None, scratch=None,
+                               scratch_bytes=0, stream=None):
+        _check(load().exa_fv_musclhancock_update(self._h, _ptr(lim), _ptr(lim_old), _ptr(luh), _ptr(dt_dev),
+                                                 _dbl3(dx), int(ncells), _ptr(cell_list), _ptr(scratch),
+                                                 ctypes.c_size_t(int(scratch_bytes)), _stream(stream)),
+               "exa_fv_musclhancock_update")
+
     @property
     def variant(self):
         v = ctypes.c_int()

@@ -865,6 +865,8 @@ struct LimLaunch {
                                   (int)PROJ_SMEM));
     EXA_CUDA(cudaFuncSetAttribute(lim_recompute_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)PROJ_SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_project_kernel<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)PROJ_SMEM));
     done = true;
     return EXA_OK;
   }
@@ -881,6 +883,48 @@ struct LimLaunch {
     return EXA_OK;
   }
   static size_t scratch_doubles() { return MC::kShared ? 0 : (size_t)MC::SCR; }
+
+  // kernel-level entry points (no mesh): MUSCL-Hancock over a cell list with
+  // caller-provided scratch, and the two projections
+  static int muscl_call(double* lim, double* lim_old, double* luh, const double* dt, Geometry g, int n,
+                        const int* list, double* scratch, size_t scratch_doubles_avail, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    int rc = attrs();
+    if (rc) return rc;
+    int grid = 0;
+    if ((rc = muscl_grid(n, &grid))) return rc;
+    if (!MC::kShared) {
+      const size_t fit = scratch_doubles_avail / (size_t)MC::SCR;
+      if (fit < 1 || !scratch)
+        return fail(EXA_ERR_ARG, "exa_fv_musclhancock_update: scratch holds " +
+                                     std::to_string(scratch_doubles_avail * 8) + " bytes, one block needs " +
+                                     std::to_string((size_t)MC::SCR * 8));
+      grid = (int)std::min<size_t>((size_t)grid, fit);
+    }
+    lim_muscl_kernel<DIM, N, PDE><<<grid, MC::THREADS, MC::SMEM, st>>>(list, nullptr, n, lim, lim_old, luh, g, dt,
+                                                                       scratch, nullptr);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int scratch_bytes_for(int n, size_t* bytes) {
+    if (MC::kShared || n <= 0) {
+      *bytes = 0;
+      return EXA_OK;
+    }
+    int grid = 0;
+    int rc = muscl_grid(n, &grid);
+    if (rc) return rc;
+    *bytes = (size_t)grid * MC::SCR * sizeof(double);
+    return EXA_OK;
+  }
+  static int project_call(double* luh, double* lim, int n, const int* list, int to_fv, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    int rc = attrs();
+    if (rc) return rc;
+    lim_project_kernel<DIM, N><<<n, 128, PROJ_SMEM, st>>>(list, n, luh, lim, to_fv);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
   static LimParams params(const exa_lmesh* lm) { return LimParams{lm->A, lm->T, lm->cure_steps, lm->relax, lm->scale}; }
 
   static int select(exa_lmesh* lm, int lo, int hi, int* list, int* count, const int* gate) {
@@ -922,7 +966,7 @@ struct LimLaunch {
   static int muscl(exa_lmesh* lm, const int* gate) {
     exa_mesh* m = lm->m;
     lim_muscl_kernel<DIM, N, PDE><<<lm->muscl_grid, MC::THREADS, MC::SMEM, m->stream>>>(
-        lm->listF, lm->flags + 2, lm->lim, lm->lim_prev, m->luh, m->geo, m->scal + 0, lm->gscratch, gate);
+        lm->listF, lm->flags + 2, 0, lm->lim, lm->lim_prev, m->luh, m->geo, m->scal + 0, lm->gscratch, gate);
     EXA_LAUNCHED();
     return EXA_OK;
   }
@@ -1012,6 +1056,9 @@ struct LimOps {
   int (*grid)(int, int*);
   size_t (*scratch)();
   size_t LS, PB;
+  int (*muscl)(double*, double*, double*, const double*, Geometry, int, const int*, double*, size_t, cudaStream_t);
+  int (*scratch_bytes)(int, size_t*);
+  int (*project)(double*, double*, int, const int*, int, cudaStream_t);
 };
 
 static bool find_lim_ops(int dim, int order, LimOps* out) {
@@ -1019,7 +1066,7 @@ static bool find_lim_ops(int dim, int order, LimOps* out) {
   if (dim == D && order == NN) {                                                                        \
     using LL = LimLaunch<D, NN>;                                                                        \
     *out = LimOps{&LL::init, &LL::step, &LL::muscl_grid, &LL::scratch_doubles, (size_t)LimShape<D, NN>::LS, \
-                  (size_t)LimShape<D, NN>::PB};                                                         \
+                  (size_t)LimShape<D, NN>::PB, &LL::muscl_call, &LL::scratch_bytes_for, &LL::project_call};   \
     return true;                                                                                        \
   }
   EXA_ORDERS_EULER(X, 2)
@@ -1031,6 +1078,52 @@ static bool find_lim_ops(int dim, int order, LimOps* out) {
 }  // namespace exa
 
 extern "C" {
+
+static int lim_ops_of(const exa_solver* s, const char* fn, LimOps* ops) {
+  if (!s) return fail(EXA_ERR_ARG, std::string(fn) + ": null solver");
+  if (s->k.pde != EXA_PDE_EULER) return fail(EXA_ERR_UNSUPPORTED, std::string(fn) + ": the limiter supports EXA_PDE_EULER");
+  if (!find_lim_ops(s->k.dim, s->k.order, ops))
+    return fail(EXA_ERR_UNSUPPORTED, std::string(fn) + ": no limiter kernels for this order");
+  return EXA_OK;
+}
+
+int exa_project_on_fv_limiter_space(const exa_solver* s, const double* luh, double* lim, int ncells,
+                                    const int* cell_list, void* stream) {
+  LimOps ops;
+  int rc = lim_ops_of(s, "exa_project_on_fv_limiter_space", &ops);
+  if (rc) return rc;
+  if (!luh || !lim || ncells < 0) return fail(EXA_ERR_ARG, "exa_project_on_fv_limiter_space: bad argument");
+  return ops.project(const_cast<double*>(luh), lim, ncells, cell_list, 1, (cudaStream_t)stream);
+}
+
+int exa_project_on_dg_space(const exa_solver* s, const double* lim, double* luh, int ncells, const int* cell_list,
+                            void* stream) {
+  LimOps ops;
+  int rc = lim_ops_of(s, "exa_project_on_dg_space", &ops);
+  if (rc) return rc;
+  if (!luh || !lim || ncells < 0) return fail(EXA_ERR_ARG, "exa_project_on_dg_space: bad argument");
+  return ops.project(luh, const_cast<double*>(lim), ncells, cell_list, 0, (cudaStream_t)stream);
+}
+
+int exa_fv_musclhancock_scratch_bytes(const exa_solver* s, int ncells, size_t* bytes) {
+  LimOps ops;
+  int rc = lim_ops_of(s, "exa_fv_musclhancock_scratch_bytes", &ops);
+  if (rc) return rc;
+  if (!bytes || ncells < 0) return fail(EXA_ERR_ARG, "exa_fv_musclhancock_scratch_bytes: bad argument");
+  return ops.scratch_bytes(ncells, bytes);
+}
+
+int exa_fv_musclhancock_update(const exa_solver* s, double* lim, double* lim_old, double* luh, const double* dt_dev,
+                               const double* dx, int ncells, const int* cell_list, void* scratch, size_t scratch_bytes,
+                               void* stream) {
+  LimOps ops;
+  int rc = lim_ops_of(s, "exa_fv_musclhancock_update", &ops);
+  if (rc) return rc;
+  if (!lim || !lim_old || !dt_dev || !dx || ncells < 0)
+    return fail(EXA_ERR_ARG, "exa_fv_musclhancock_update: bad argument");
+  return ops.muscl(lim, lim_old, luh, dt_dev, geom(s, dx), ncells, cell_list, (double*)scratch,
+                   scratch_bytes / sizeof(double), (cudaStream_t)stream);
+}
 
 static void lmesh_free(exa_lmesh* lm) {
   cudaFree(lm->s);

@@ -255,7 +255,8 @@ __global__ void __launch_bounds__(128) lim_fv_halo_kernel(const int* __restrict_
 
 // ---------------------------------------------------------------------------
 // MUSCL-Hancock (2d/musclhancock.cpph:50-276, 3d/musclhancock.cpph) on the
-// FV-active cells of `list`, then projectOnDGSpace of the result. Before the
+// cells of `list` (length *count when count is given, else nlist; list NULL:
+// cells 0..n-1), then projectOnDGSpace of the result into luh (unless NULL). Before the
 // update lim_prev <- lim (FiniteVolumesSolver::updateSolution,
 // FiniteVolumesSolver.cpp:662-715). Work arrays (evolved boundary states and
 // edge fluxes) live in shared memory when they fit, else in a per-block slice
@@ -291,7 +292,7 @@ __device__ __forceinline__ void dir_flux(const double* q, int d, double* f) {
 
 template <int DIM, int N, class PDE>
 __global__ void __launch_bounds__(256) lim_muscl_kernel(const int* __restrict__ list, const int* __restrict__ count,
-                                                       double* __restrict__ lim, double* __restrict__ lim_prev,
+                                                       int nlist, double* __restrict__ lim, double* __restrict__ lim_prev,
                                                        double* __restrict__ luh, Geometry geo,
                                                        const double* __restrict__ dt_ptr, double* __restrict__ gscratch,
                                                        const int* __restrict__ gate) {
@@ -311,9 +312,9 @@ __global__ void __launch_bounds__(256) lim_muscl_kernel(const int* __restrict__ 
     ics[d] = 1. / cs[d];
     icsdt[d] = dt * ics[d];
   }
-  const int n = *count;
+  const int n = count ? *count : nlist;
   for (int li = blockIdx.x; li < n; li += gridDim.x) {
-    const int cell = list[li];
+    const int cell = list ? list[li] : li;
     double* l = lim + (size_t)cell * L::LS;
     double* lp = lim_prev + (size_t)cell * L::LS;
     for (int i = threadIdx.x; i < L::LS; i += blockDim.x) lp[i] = l[i];
@@ -439,7 +440,7 @@ __global__ void __launch_bounds__(256) lim_muscl_kernel(const int* __restrict__ 
         l[idx * nV + v] -= icsdt[d] * f;
     }
     __syncthreads();
-    project_dg_block<DIM, N>(l, luh + (size_t)cell * L::P * nV, tmp);
+    if (luh) project_dg_block<DIM, N>(l, luh + (size_t)cell * L::P * nV, tmp);
   }
 }
 
@@ -817,6 +818,25 @@ __global__ void __launch_bounds__(128) lim_recompute_kernel(int ncells, double* 
     dtm = (x < dtm) ? x : dtm;
   }
   if ((threadIdx.x & 31) == 0) atomic_min_pos_double(dt_min, dtm);
+}
+
+// Batched projections for the kernel-level entry points: one block per listed
+// cell (list NULL: cells 0..n-1). to_fv: luh -> interior subcells of lim,
+// else interior subcells of lim -> luh.
+template <int DIM, int N>
+__global__ void __launch_bounds__(128) lim_project_kernel(const int* __restrict__ list, int n,
+                                                          double* __restrict__ luh, double* __restrict__ lim,
+                                                          int to_fv) {
+  using L = LimShape<DIM, N>;
+  extern __shared__ double tmp[];
+  if ((int)blockIdx.x >= n) return;
+  const int c = list ? list[blockIdx.x] : (int)blockIdx.x;
+  double* u = luh + (size_t)c * L::P * L::nV;
+  double* l = lim + (size_t)c * L::LS;
+  if (to_fv)
+    project_fv_block<DIM, N>(u, l, tmp);
+  else
+    project_dg_block<DIM, N>(l, u, tmp);
 }
 
 // Compacts the cells whose status satisfies lo <= s < hi into list/count

@@ -149,6 +149,31 @@ int exa_mesh_stream(exa_mesh* m, void** stream);
 int exa_mesh_set_profiling(exa_mesh* m, int on);
 int exa_mesh_phase_times(exa_mesh* m, double* ms4, long long* launches4, int reset);
 
+/* ---- limiter kernels (batched, stream-ordered, EXA_PDE_EULER) ------------- */
+/* FV patches: lim[cell][(2N+5)^d][5] (2N+1 subcells plus 2 ghost layers per
+ * side, (z,y,x) order). cell_list (optional, device): the cells to process. */
+/* projectOnFVLimiterSpace (kernels/limiter/generic/Limiter.h:48,
+ * Limiter.cpp:23-66): interior subcells of lim from luh. */
+int exa_project_on_fv_limiter_space(const exa_solver* s, const double* luh, double* lim, int ncells,
+                                    const int* cell_list, void* stream);
+/* projectOnDGSpace (Limiter.h:58, Limiter.cpp:69-112): luh from the interior
+ * subcells of lim. */
+int exa_project_on_dg_space(const exa_solver* s, const double* lim, double* luh, int ncells, const int* cell_list,
+                            void* stream);
+/* FiniteVolumesSolver::updateSolution's kernel call (FiniteVolumesSolver.cpp:662-715;
+ * musclhancock::c::solutionUpdate, musclhancock.h:38-41, generated glue
+ * AbstractGenericFiniteVolumesSolverInCImplementation.template:48-51): for every
+ * listed cell lim_old <- lim (ghost layers included; the caller has filled
+ * them), then lim <- the MUSCL-Hancock update of lim_old by *dt_dev, and, when
+ * luh is not NULL, luh <- projectOnDGSpace(lim). 3D patches need device
+ * scratch of at least exa_fv_musclhancock_scratch_bytes(s, ncells) bytes (less
+ * runs with fewer blocks; less than one block's share is an error); 2D needs
+ * none (scratch may be NULL). */
+int exa_fv_musclhancock_scratch_bytes(const exa_solver* s, int ncells, size_t* bytes);
+int exa_fv_musclhancock_update(const exa_solver* s, double* lim, double* lim_old, double* luh, const double* dt_dev,
+                               const double* dx, int ncells, const int* cell_list, void* scratch, size_t scratch_bytes,
+                               void* stream);
+
 /* ---- uniform mesh with the a-posteriori subcell limiter ------------------- */
 /* The LimitingADERDGSolver (exahype/solvers/LimitingADERDGSolver.h:82-1508)
  * over the uniform mesh: every cell carries a limiter status, DMP min/max

@@ -141,6 +141,32 @@ class Kernels:
         dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
         return self._call("stable_dt", _p(np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)), _p(dx))
 
+    # limiter kernels of the C restatement (oracle/limiter.c); Euler only
+    def fv_patch_size(self):
+        E = 2 * self.order + 5
+        return E ** self.dim * 5
+
+    def project_fv(self, luh, lim=None):
+        lim = np.zeros(self.fv_patch_size()) if lim is None else np.array(lim, dtype=np.float64).reshape(-1)
+        self._l.orc_project_fv(ctypes.byref(self._s), _p(np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)),
+                               _p(lim))
+        return lim
+
+    def project_dg(self, lim):
+        luh = np.zeros(self.P * 5)
+        self._l.orc_project_dg(ctypes.byref(self._s), _p(np.ascontiguousarray(lim, dtype=np.float64).reshape(-1)),
+                               _p(luh))
+        return luh
+
+    def musclhancock(self, lim_old, dx, dt):
+        """MUSCL-Hancock update of one patch (ghost layers filled by the caller)"""
+        old = np.ascontiguousarray(lim_old, dtype=np.float64).reshape(-1)
+        new = old.copy()
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        self._l.orc_musclhancock.restype = ctypes.c_double
+        self._l.orc_musclhancock(ctypes.byref(self._s), _p(new), _p(old), _p(dx), ctypes.c_double(dt))
+        return new
+
     def boundary_face(self, FIn, QIn, face_index, centre=(0.5, 0.5, 0.5), size=(0.1, 0.1, 0.1), t=0.0, dt=0.0):
         FIn = np.array(FIn, dtype=np.float64).reshape(-1)
         c = np.ascontiguousarray(np.resize(np.asarray(centre, dtype=np.float64), 3))
