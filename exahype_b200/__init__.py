@@ -157,6 +157,13 @@ class Solver:
                                                  ctypes.c_size_t(int(scratch_bytes)), _stream(stream)),
                "exa_fv_musclhancock_update")
 
+    def fv_musclhancock_update_noalloc(self, lim, lim_old, luh, dt_dev, dx, ncells, cell_list=None, stream=None):
+        """fv_musclhancock_update with the library's static scratch: no device
+        allocation; overlapping calls race on the shared scratch."""
+        _check(load().exa_fv_musclhancock_update_noalloc(self._h, _ptr(lim), _ptr(lim_old), _ptr(luh), _ptr(dt_dev),
+                                                         _dbl3(dx), int(ncells), _ptr(cell_list), _stream(stream)),
+               "exa_fv_musclhancock_update_noalloc")
+
     @property
     def variant(self):
         v = ctypes.c_int()

@@ -1125,6 +1125,56 @@ int exa_fv_musclhancock_update(const exa_solver* s, double* lim, double* lim_old
                    scratch_bytes / sizeof(double), (cudaStream_t)stream);
 }
 
+// ---- MUSCL-Hancock without device allocation ---------------------------------
+// exa_fv_musclhancock_update_noalloc runs the same kernel as
+// exa_fv_musclhancock_update with the library's own scratch: a file-scope
+// __device__ array of kNoAllocScratchBytes, found once per device by
+// cudaGetSymbolAddress. The call allocates nothing. Nothing in the array needs
+// to start at zero (every slot a block reads was written by that block for the
+// same cell). Calls that overlap in time share the array and race.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
+
+static int noalloc_scratch(double** out) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, double*>> per_device;
+  int dev = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto& e : per_device)
+    if (e.first == dev) {
+      *out = e.second;
+      return EXA_OK;
+    }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(EXA_ERR_CUDA, std::string("exa_fv_musclhancock_update_noalloc: cudaGetSymbolAddress: ") +
+                                  cudaGetErrorString(e));
+  per_device.emplace_back(dev, static_cast<double*>(p));
+  *out = static_cast<double*>(p);
+  return EXA_OK;
+}
+
+int exa_fv_musclhancock_update_noalloc(const exa_solver* s, double* lim, double* lim_old, double* luh,
+                                       const double* dt_dev, const double* dx, int ncells, const int* cell_list,
+                                       void* stream) {
+  LimOps ops;
+  int rc = lim_ops_of(s, "exa_fv_musclhancock_update_noalloc", &ops);
+  if (rc) return rc;
+  if (!lim || !lim_old || !dt_dev || !dx || ncells < 0)
+    return fail(EXA_ERR_ARG, "exa_fv_musclhancock_update_noalloc: bad argument");
+  const size_t per_block = ops.scratch() * sizeof(double);
+  if (per_block > kNoAllocScratchBytes)
+    return fail(EXA_ERR_UNSUPPORTED, "exa_fv_musclhancock_update_noalloc: one block of this order needs " +
+                                         std::to_string(per_block) + " bytes of scratch, the static scratch holds " +
+                                         std::to_string(kNoAllocScratchBytes));
+  double* scratch = nullptr;
+  if (per_block > 0 && (rc = noalloc_scratch(&scratch))) return rc;
+  return ops.muscl(lim, lim_old, luh, dt_dev, geom(s, dx), ncells, cell_list, scratch,
+                   kNoAllocScratchBytes / sizeof(double), (cudaStream_t)stream);
+}
+
 static void lmesh_free(exa_lmesh* lm) {
   cudaFree(lm->s);
   cudaFree(lm->s_prev);

@@ -173,6 +173,22 @@ int exa_fv_musclhancock_scratch_bytes(const exa_solver* s, int ncells, size_t* b
 int exa_fv_musclhancock_update(const exa_solver* s, double* lim, double* lim_old, double* luh, const double* dt_dev,
                                const double* dx, int ncells, const int* cell_list, void* scratch, size_t scratch_bytes,
                                void* stream);
+/* The same update without any device allocation and without caller scratch
+ * (no counterpart in the reference, whose kernels take their scratch from the
+ * caller's per-thread temporaries, TemporaryVariables.cpp:68-111). For callers
+ * that cannot hand out device memory: code inside a framework traversal that
+ * owns no device allocator, or a host thread that must not call cudaMalloc or
+ * cudaFree because they can synchronise the device. The scratch is a 32 MiB
+ * array inside the library; a call runs as many blocks as fit in it (3D N=3:
+ * 151, N=5: 47, N=7: 20; 2D needs none), and an order whose one-block share
+ * exceeds it is rejected with EXA_ERR_UNSUPPORTED. Nothing in it has to start
+ * at zero. All calls share the array: calls that overlap in time (on
+ * different streams or threads) race on it and must be serialised. The first
+ * call on a device looks the array up and sets kernel attributes; make it
+ * before any stream capture begins. */
+int exa_fv_musclhancock_update_noalloc(const exa_solver* s, double* lim, double* lim_old, double* luh,
+                                       const double* dt_dev, const double* dx, int ncells, const int* cell_list,
+                                       void* stream);
 
 /* ---- uniform mesh with the a-posteriori subcell limiter ------------------- */
 /* The LimitingADERDGSolver (exahype/solvers/LimitingADERDGSolver.h:82-1508)
