@@ -328,6 +328,8 @@ def run_ours(a):
                              "reference's generic kernels, %.1f s" % r["seconds"]}
     launches = sum(v[1] for v in ph.values())
     lim = None if a.no_limiter else run_limiter_workload(a, world, dev, rank)
+    ens = None if a.no_ensemble else run_ensemble_workload(a, world, dev, rank)
+    srv = None if a.no_serving else run_serving_workload(a, world, dev, rank)
     line = {
         "metric": METRIC, "value": value, "unit": "DoF-updates/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -337,7 +339,7 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
-        "limiter": lim,
+        "limiter": lim, "ensemble": ens, "serving": srv,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -400,6 +402,112 @@ def run_limiter_workload(a, world, dev, rank):
     return out
 
 
+def run_ensemble_workload(a, world, dev, rank, steps=50):
+    """The ragged ensemble: 256 independent 2D periodic pulse solves (sides
+    {9,27,81}, N {3,5,7}, per-instance seeded centre and amplitude
+    U[0.1,0.5]), `steps` steps each, as one exa_batch (one CUDA graph launch
+    per step) and, for comparison, one instance at a time on its own Mesh.
+    Initialisation is outside both timed regions."""
+    import torch
+    import exahype_b200 as eb
+    from exahype_b200 import problems
+    ens = problems.pulse_ensemble(256, seed=SEED + rank)
+    dofs = sum(int(np.prod(p["cells"])) * (p["order"] + 1) ** 2 * NVAR for p in ens)
+    bt = eb.Batch()
+    for p in ens:
+        bt.add(2, p["order"], p["cells"], [1.0, 1.0], eb.BC_PERIODIC, p["luh"])
+    bt.commit()
+    bt.step(1)  # captures the graph
+    bt.synchronize()
+    stream = torch.cuda.ExternalStream(bt.stream_handle, device=dev)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    bt.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms_b = reduce_max(e0.elapsed_time(e1), world, dev)
+    # one at a time: the same problems, each on its own Mesh (same variants)
+    solvers = {}
+    ms_s = 0.0
+    for p in ens:
+        o = p["order"]
+        if o not in solvers:
+            solvers[o] = eb.Solver(2, o)
+            solvers[o].variant = bt.variant(2, o)
+        m = eb.Mesh(solvers[o], p["cells"], [0.0, 0.0], [1.0, 1.0], eb.BC_PERIODIC)
+        m.set_solution(p["luh"])
+        m.init(0.0)
+        m.step(1)
+        m.synchronize()
+        st = torch.cuda.ExternalStream(m.stream_handle, device=dev)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(st)
+        m.step(steps)
+        f1.record(st)
+        f1.synchronize()
+        ms_s += f0.elapsed_time(f1)
+        del m
+    ms_s = reduce_max(ms_s, world, dev)
+    counts = {}
+    for p in ens:
+        k = "N%d_%dx%d" % (p["order"], p["cells"][0], p["cells"][1])
+        counts[k] = counts.get(k, 0) + 1
+    return {"workload": "euler2d_pulse_ensemble_256_sides9-27-81_N3-5-7_periodic", "steps": steps,
+            "instances": len(ens), "dof_per_step": dofs, "value": dofs * steps * world / (ms_b / 1e3),
+            "unit": "DoF-updates/s", "ms_per_step": ms_b / steps,
+            "one_at_a_time": {"value": dofs * steps * world / (ms_s / 1e3), "ms_per_step": ms_s / steps},
+            "speedup_vs_one_at_a_time": ms_s / ms_b, "path": "fp64", "instance_mix": counts,
+            "timing": "CUDA events on the batch stream (one graph launch per step) vs the sum over instances "
+                      "of each Mesh's own stepping time"}
+
+
+def run_serving_workload(a, world, dev, rank):
+    """Continuous-batching serving of a seeded Poisson stream of independent
+    Euler solves (exahype_b200.serving) against the same requests served one
+    at a time on the plain FP64 path. Default mix (scaled so both arms take
+    seconds): 48 requests at 40/s, 70 % 2D with 27..243 cells per side, 30 %
+    3D with 9..27, N in {3,5,7}, 20 % limiter explosions, 10..100 steps,
+    8 GB device budget; --serving-full uses 3D sides 9..81, 10..200 steps and
+    a 120 GB budget."""
+    from exahype_b200 import serving
+    import exahype_b200 as eb
+    full = a.serving_full
+    kw = dict(sides_2d=(27, 243), sides_3d=(9, 81) if full else (9, 27), steps=(10, 200) if full else (10, 100))
+    n, rate, budget = (96, 10.0, 120e9) if full else (48, 40.0, 8e9)
+    variants = {}
+    for dim in (2, 3):
+        for o in (3, 5, 7):
+            variants[(dim, o)] = eb.Solver(dim, o).autotune(4096)[0]
+    reqs = serving.request_stream(n, rate, seed=SEED + rank, **kw)
+    for r in reqs:
+        r.build_initial()
+    srv = serving.Server(budget, variants)
+    t0 = time.perf_counter()
+    done, rejected = srv.run(reqs, keep_results=False)
+    wall = time.perf_counter() - t0
+    res = serving.summarise(done, wall)
+    rej = {r.rid for r in rejected}
+    base = [r for r in serving.request_stream(n, rate, seed=SEED + rank, **kw) if r.rid not in rej]
+    for r in base:
+        r.build_initial()
+    t0 = time.perf_counter()
+    serving.run_one_at_a_time(base, variants, keep_results=False)
+    wall_b = time.perf_counter() - t0
+    res_b = serving.summarise(base, wall_b)
+    kinds = {}
+    for r in reqs:
+        k = "%dD_%s" % (r.dim, r.kind)
+        kinds[k] = kinds.get(k, 0) + 1
+    return {"workload": "serving_poisson_%d_requests" % n, "full_size": bool(full), "rate_per_s": rate,
+            "budget_bytes": budget, "rejected_over_budget": len(rejected), "mix": kinds,
+            "p50_time_to_solution_s": res["p50_s"], "p99_time_to_solution_s": res["p99_s"],
+            "value": res["value"], "unit": "DoF-updates/s", "wall_s": wall,
+            "one_at_a_time": {"p50_time_to_solution_s": res_b["p50_s"], "p99_time_to_solution_s": res_b["p99_s"],
+                              "value": res_b["value"], "wall_s": wall_b},
+            "timing": "host wall clock from the first arrival to the last result on the host"}
+
+
 def measure_fp64_peak():
     import ctypes
     import exahype_b200 as eb
@@ -424,27 +532,31 @@ def main():
     ap.add_argument("--variant", type=int, default=None, help="predictor variant (default: autotune)")
     ap.add_argument("--no-limiter", action="store_true", help="skip the limiter workload")
     ap.add_argument("--limiter-steps", type=int, default=0, help="limiter workload: K steps instead of t = 0.2")
-    ap.add_argument("--workload", default="headline", choices=["headline", "limiter"],
-                    help="limiter: only the limiter workload, as its own JSON line")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble workload")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
+    ap.add_argument("--serving-full", action="store_true", help="serving: the full-size request mix")
+    ap.add_argument("--workload", default="headline", choices=["headline", "limiter", "ensemble", "serving"],
+                    help="limiter / ensemble / serving: only that workload, as its own JSON line")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
-    if a.workload == "limiter":
-        return run_limiter_only(a)
+    if a.workload in ("limiter", "ensemble", "serving"):
+        return run_secondary_only(a)
     return run_ours(a)
 
 
-def run_limiter_only(a):
+def run_secondary_only(a):
     import torch
     rank, world, local = dist_env()
     if world > 1:
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    r = run_limiter_workload(a, world, torch.device("cuda", local), rank)
+    run = {"limiter": run_limiter_workload, "ensemble": run_ensemble_workload,
+           "serving": run_serving_workload}[a.workload]
+    r = run(a, world, torch.device("cuda", local), rank)
     if rank == 0:
-        print(json.dumps(dict(r, metric=METRIC, n_gpus=world, dtype="f64", data="synthetic (seeded explosion)")),
-              flush=True)
+        print(json.dumps(dict(r, metric=METRIC, n_gpus=world, dtype="f64", data="synthetic (seeded)")), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0

@@ -383,3 +383,97 @@ class LimitingMesh:
         h = ctypes.c_void_p()
         _check(load().exa_lmesh_stream(self._h, ctypes.byref(h)), "exa_lmesh_stream")
         return h.value or 0
+
+
+class Batch:
+    """Batched ragged ensemble of independent uniform-mesh solves (exa_batch_*):
+    instances of one (dim, order) share device arrays, a step is one CUDA graph
+    launch, and every instance computes what a Mesh of the same problem would."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        _check(load().exa_batch_create(ctypes.byref(h)), "exa_batch_create")
+        self._h = h
+        self._shape = {}
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().exa_batch_destroy(self._h)
+        except Exception:
+            pass
+
+    def add(self, dim, order, cells, size, bc, luh, pde=PDE_EULER):
+        c = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        s = _dbl3(list(size) + [1.0] * (3 - len(size)))
+        if isinstance(bc, int):
+            bc = [bc] * (2 * dim)
+        b = (ctypes.c_int * 6)(*(list(bc) + [0] * (6 - len(bc))))
+        a = np.ascontiguousarray(luh, dtype=np.float64)
+        i = ctypes.c_int()
+        _check(load().exa_batch_add(self._h, int(dim), int(order), int(pde), c, s, b,
+                                    a.ctypes.data_as(ctypes.c_void_p), ctypes.byref(i)), "exa_batch_add")
+        ndata = 5 + (1 if pde == PDE_EULER_TEST else 0)
+        self._shape[i.value] = (int(np.prod(cells[:dim])), (order + 1) ** dim, ndata)
+        return i.value
+
+    def remove(self, iid):
+        _check(load().exa_batch_remove(self._h, int(iid)), "exa_batch_remove")
+
+    def commit(self):
+        _check(load().exa_batch_commit(self._h), "exa_batch_commit")
+
+    def step(self, nsteps=1):
+        _check(load().exa_batch_step(self._h, int(nsteps)), "exa_batch_step")
+
+    def set_graph(self, on=True):
+        _check(load().exa_batch_set_graph(self._h, int(bool(on))), "exa_batch_set_graph")
+
+    def variant(self, dim, order, pde=PDE_EULER):
+        v = ctypes.c_int()
+        _check(load().exa_batch_get_variant(self._h, int(dim), int(order), int(pde), ctypes.byref(v)),
+               "exa_batch_get_variant")
+        return v.value
+
+    def set_variant(self, dim, order, variant, pde=PDE_EULER):
+        _check(load().exa_batch_set_variant(self._h, int(dim), int(order), int(pde), int(variant)),
+               "exa_batch_set_variant")
+
+    def state(self, iid):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+        _check(load().exa_batch_state(self._h, int(iid), ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)),
+               "exa_batch_state")
+        return dict(t=t.value, dt=dt.value, steps=st.value)
+
+    def get_solution(self, iid):
+        a = np.empty(self._shape[iid], dtype=np.float64)
+        _check(load().exa_batch_get_solution(self._h, int(iid), a.ctypes.data_as(ctypes.c_void_p)),
+               "exa_batch_get_solution")
+        return a
+
+    @staticmethod
+    def instance_bytes(dim, order, cells, pde=PDE_EULER):
+        c = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        b = ctypes.c_size_t()
+        _check(load().exa_batch_instance_bytes(int(dim), int(order), int(pde), c, ctypes.byref(b)),
+               "exa_batch_instance_bytes")
+        return b.value
+
+    def device_bytes(self):
+        b = ctypes.c_size_t()
+        _check(load().exa_batch_device_bytes(self._h, ctypes.byref(b)), "exa_batch_device_bytes")
+        return b.value
+
+    def sweeps(self):
+        v = ctypes.c_longlong()
+        _check(load().exa_batch_sweeps(self._h, ctypes.byref(v)), "exa_batch_sweeps")
+        return v.value
+
+    def synchronize(self):
+        _check(load().exa_batch_synchronize(self._h), "exa_batch_synchronize")
+
+    @property
+    def stream_handle(self):
+        h = ctypes.c_void_p()
+        _check(load().exa_batch_stream(self._h, ctypes.byref(h)), "exa_batch_stream")
+        return h.value or 0

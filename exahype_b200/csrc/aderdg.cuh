@@ -28,9 +28,19 @@ template <int P>
 constexpr int cells_per_block() { return P >= 256 ? 1 : 256 / P; }
 constexpr int pow2ceil(int v) { return v <= 1 ? 1 : 2 * pow2ceil((v + 1) / 2); }
 
+// Cell widths of one mesh, or of a batch of independent instances: with
+// inst != NULL cell c belongs to instance inst[c], whose widths are
+// inst_dx[3 inst + d] and whose step size is dt[inst[c]] (the kernels' dt
+// pointer then points at the per-instance array).
 struct Geometry {
   double dx[3];
+  const int* inst;
+  const double* inst_dx;
 };
+__device__ __forceinline__ int cell_instance(const Geometry& g, int cell) { return g.inst ? g.inst[cell] : 0; }
+__device__ __forceinline__ double cell_width(const Geometry& g, int inst, int d) {
+  return g.inst ? g.inst_dx[3 * inst + d] : g.dx[d];
+}
 
 // ---------------------------------------------------------------------------
 // Space-time predictor: the discrete Picard iteration of
@@ -99,8 +109,10 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
   const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
   const double wpt = wz * wy * wx;  // reference order (w_z w_y) w_x
   const double iw = 1.0 / wpt;
-  const double dt = *dt_ptr;
-  const double invDx0 = 1.0 / geo.dx[0], invDx1 = 1.0 / geo.dx[1], invDx2 = DIM == 3 ? 1.0 / geo.dx[2] : 0.0;
+  const int inst = cell_instance(geo, cell);
+  const double dt = dt_ptr[inst];
+  const double invDx0 = 1.0 / cell_width(geo, inst, 0), invDx1 = 1.0 / cell_width(geo, inst, 1);
+  const double invDx2 = DIM == 3 ? 1.0 / cell_width(geo, inst, 2) : 0.0;
 
   // own variables of luh (for the rhs0 term); the lead thread also seeds the
   // whole trivial initial guess lQi(:,t) = luh (:66-82)
@@ -524,12 +536,14 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
   // padding threads only join the reduction; count: optional device-side list length
   const bool active = lc < C::CPB && slot < (count ? min(*count, ncells) : ncells);
   double dtmin = __longlong_as_double(0x7fefffffffffffffll);  // DBL_MAX
+  int inst = 0;
   if (active) {
     const int cell = cell_list ? cell_list[slot] : slot;
+    inst = cell_instance(geo, cell);
     const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
     const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
-    const double invDx0 = __ddiv_rn(1.0, geo.dx[0]), invDx1 = __ddiv_rn(1.0, geo.dx[1]);
-    const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, geo.dx[2]) : 0.0;
+    const double invDx0 = __ddiv_rn(1.0, cell_width(geo, inst, 0)), invDx1 = __ddiv_rn(1.0, cell_width(geo, inst, 1));
+    const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, cell_width(geo, inst, 2)) : 0.0;
     double* u = luh + ((size_t)cell * P + p) * nD;
     double q[nD];
 #pragma unroll
@@ -561,7 +575,7 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
         for (int v = 0; v < nV; v++)
           du[v] -= (Fb[(5 * F + fn) * nV + v] * T.FR[z] - Fb[(4 * F + fn) * nV + v] * T.FL[z]) * us;
       }
-      const double us = *dt_ptr / (wz * wy * wx);
+      const double us = dt_ptr[inst] / (wz * wy * wx);
 #pragma unroll
       for (int v = 0; v < nV; v++) {
         q[v] += du[v] * us;
@@ -574,6 +588,23 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
     if (DIM == 3) den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 2), invDx2));
     const double dtp = __ddiv_rn(__dmul_rn(0.9, pnpm(N)), den);
     dtmin = (dtp < dtmin) ? dtp : dtmin;
+  }
+  // A batch block may hold cells of two instances (instances are contiguous
+  // cell ranges): then every thread min-combines into its own instance.
+  __shared__ int s_inst[2];
+  if (geo.inst) {
+    if (threadIdx.x == 0) s_inst[0] = INT_MAX, s_inst[1] = INT_MIN;
+    __syncthreads();
+    if (active) {
+      atomicMin(&s_inst[0], inst);
+      atomicMax(&s_inst[1], inst);
+    }
+    __syncthreads();
+    if (s_inst[0] != s_inst[1] && s_inst[0] != INT_MAX) {
+      if (active && dt_out) atomic_min_pos_double(dt_out + inst, dtmin);
+      return;
+    }
+    inst = s_inst[0] == INT_MAX ? 0 : s_inst[0];
   }
   // block min, then one atomic per block
 #pragma unroll
@@ -591,7 +622,7 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
       const double other = __shfl_xor_sync(0xffffffffu, m, o);
       m = (other < m) ? other : m;
     }
-    if (threadIdx.x == 0 && dt_out) atomic_min_pos_double(dt_out, m);
+    if (threadIdx.x == 0 && dt_out) atomic_min_pos_double(dt_out + inst, m);
   }
 }
 

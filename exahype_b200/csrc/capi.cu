@@ -1364,3 +1364,5 @@ int exa_lmesh_stream(exa_lmesh* lm, void** stream) {
 }
 
 }  // extern "C"
+
+#include "batch.cuh"

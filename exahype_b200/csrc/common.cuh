@@ -1,6 +1,7 @@
 // Shared device-side definitions: operator tables in constant memory,
 // compile-time basis sizes and small helpers.
 #pragma once
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 

@@ -88,8 +88,19 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
   const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
   const double wpt = wz * wy * wx;
   const double iw = 1.0 / wpt;
-  const double dt = *dt_ptr;
-  const double invDx0 = 1.0 / geo.dx[0], invDx1 = 1.0 / geo.dx[1], invDx2 = DIM == 3 ? 1.0 / geo.dx[2] : 0.0;
+  const int inst = cell_instance(geo, cell);
+  const double dt = dt_ptr[inst];
+  const double invDx0 = 1.0 / cell_width(geo, inst, 0), invDx1 = 1.0 / cell_width(geo, inst, 1);
+  const double invDx2 = DIM == 3 ? 1.0 / cell_width(geo, inst, 2) : 0.0;
+  // step size and inverse widths of every cell of the block (phase-B items
+  // and the epilogue work on other cells of the block than their thread's)
+  __shared__ double s_dt[C::CPB], s_idx[C::CPB][3];
+  if (p == 0) {
+    s_dt[lc] = dt;
+    s_idx[lc][0] = invDx0;
+    s_idx[lc][1] = invDx1;
+    s_idx[lc][2] = invDx2;
+  }
   int nd[DIM], Ld[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; d++) node_line<DIM, b>(d, z, y, x, nd[d], Ld[d]);
@@ -130,8 +141,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
       it_off[k] = c * C::SF + d * b * SLAB + L * nV + v;
       it_cell[k] = c;
       const int a0 = L / b, a1 = L % b;
-      const double idx = d == 0 ? invDx0 : d == 1 ? invDx1 : invDx2;
-      it_us[k] = (DIM == 3 ? s_w[a0] : 1.0) * s_w[a1] * dt * idx;
+      it_us[k] = (DIM == 3 ? s_w[a0] : 1.0) * s_w[a1] * s_dt[c] * s_idx[c][d];
     }
   }
 
@@ -316,8 +326,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
     lFhbnd[(((size_t)cell_c * 2 * DIM + 2 * d) * LINES + L) * nV + v] = sl;
     lFhbnd[(((size_t)cell_c * 2 * DIM + 2 * d + 1) * LINES + L) * nV + v] = sr;
     const int a0 = L / b, a1 = L % b;
-    const double idx = d == 0 ? invDx0 : d == 1 ? invDx1 : invDx2;
-    const double us = (DIM == 3 ? s_w[a0] : 1.0) * s_w[a1] * idx;
+    const double us = (DIM == 3 ? s_w[a0] : 1.0) * s_w[a1] * s_idx[c][d];
 #pragma unroll
     for (int k = 0; k < b; k++) {
       double s = 0.0;

@@ -5,6 +5,7 @@ adjustPointSolution does at t = 0, kernels/aderdg/generic/c/*/solutionAdjustment
 All workloads are analytic: no dataset is involved. Densities/pressures are
 turned into conserved variables (rho, rho u, E) with gamma = 1.4.
 """
+import functools
 import os
 import sys
 
@@ -14,13 +15,18 @@ GAMMA = 1.4
 _CSRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc")
 
 
-def gl_nodes(order):
+@functools.lru_cache(maxsize=None)
+def _gl_nodes(order):
     sys.path.insert(0, _CSRC)
     try:
         import gen_tables
     finally:
         sys.path.pop(0)
-    return np.array(gen_tables.build(order)["nodes"])
+    return tuple(gen_tables.build(order)["nodes"])
+
+
+def gl_nodes(order):
+    return np.array(_gl_nodes(order))
 
 
 def node_coordinates(dim, order, cells, offset=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0)):
@@ -61,15 +67,33 @@ def _periodic_d2(X, c):
     return np.sum(d * d, axis=-1)
 
 
-def gaussian_pulse_2d(order, cells=(27, 27), seed=0):
-    """rho = 1 + 0.5 exp(-|x - x0|^2 / 0.01), x0 ~ U[0.3, 0.7]^2, u = (1, 1, 0),
-    p = 1 on the periodic unit square (minimum-image distance)."""
+def gaussian_pulse_2d(order, cells=(27, 27), seed=0, amplitude=0.5):
+    """rho = 1 + a exp(-|x - x0|^2 / 0.01), x0 ~ U[0.3, 0.7]^2, u = (1, 1, 0),
+    p = 1 on the periodic unit square (minimum-image distance); a = 0.5 unless
+    given."""
     rng = np.random.default_rng(seed)
     x0 = rng.uniform(0.3, 0.7, size=2)
     X = node_coordinates(2, order, cells)
-    rho = 1.0 + 0.5 * np.exp(-_periodic_d2(X, x0) / 0.01)
+    rho = 1.0 + amplitude * np.exp(-_periodic_d2(X, x0) / 0.01)
     vel = np.broadcast_to(np.array([1.0, 1.0, 0.0]), rho.shape + (3,))
-    return conserved(rho, vel, np.ones_like(rho)), dict(x0=x0.tolist())
+    return conserved(rho, vel, np.ones_like(rho)), dict(x0=x0.tolist(), amplitude=amplitude)
+
+
+def pulse_ensemble(n=256, seed=0, sides=(9, 27, 81), orders=(3, 5, 7)):
+    """The ragged ensemble: n independent 2D periodic pulse problems, each with
+    cells per side drawn from `sides`, order from `orders`, its own seeded
+    centre and amplitude U[0.1, 0.5]. Returns a list of dicts (order, cells,
+    seed, amplitude, luh)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        side = int(rng.choice(sides))
+        order = int(rng.choice(orders))
+        amp = float(rng.uniform(0.1, 0.5))
+        iseed = int(rng.integers(0, 2 ** 31 - 1))
+        luh, _ = gaussian_pulse_2d(order, (side, side), seed=iseed, amplitude=amp)
+        out.append(dict(order=order, cells=(side, side), seed=iseed, amplitude=amp, luh=luh))
+    return out
 
 
 def gaussian_pulses_3d(order, cells=(27, 27, 27), seed=0, npulses=4):

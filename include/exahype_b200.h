@@ -238,6 +238,42 @@ int exa_lmesh_get_limiter(exa_lmesh* m, double* lim_host, int* allocated_host);
 int exa_lmesh_synchronize(exa_lmesh* m);
 int exa_lmesh_stream(exa_lmesh* m, void** stream);
 
+/* ---- batched ragged ensemble (no counterpart in the reference) ------------ */
+/* Many independent uniform-mesh solves (any mix of dimension, order, size and
+ * boundary kinds, each with its own global time step as one exa_mesh would
+ * have) advanced together: instances of one (dim, order, pde) share device
+ * arrays, so each phase of a step is one launch per order, and the whole step
+ * is replayed as one CUDA graph. Every instance computes exactly what an
+ * exa_mesh of the same problem computes (same predictor variant), whatever
+ * else is in the batch.
+ * exa_batch_add copies the initial solution (exa_mesh layout) and returns an
+ * instance id; adds and removes take effect at the next exa_batch_commit or
+ * exa_batch_step (new instances get exa_mesh_init's first step size and
+ * predictor, t = 0). The first instance of an order runs the predictor
+ * autotuner for that order. */
+typedef struct exa_batch exa_batch;
+int exa_batch_create(exa_batch** out);
+int exa_batch_destroy(exa_batch* b);
+int exa_batch_add(exa_batch* b, int dim, int order, int pde, const int* cells, const double* size, const int* bc,
+                  const double* luh_host, int* id);
+int exa_batch_remove(exa_batch* b, int id);
+int exa_batch_commit(exa_batch* b);
+/* nsteps steps of every live instance (one graph launch per step unless
+ * exa_batch_set_graph(b, 0)); no host synchronisation */
+int exa_batch_step(exa_batch* b, int nsteps);
+int exa_batch_set_graph(exa_batch* b, int on);
+int exa_batch_set_variant(exa_batch* b, int dim, int order, int pde, int variant);
+int exa_batch_get_variant(const exa_batch* b, int dim, int order, int pde, int* variant);
+int exa_batch_state(exa_batch* b, int id, double* t, double* dt, long long* steps);
+int exa_batch_get_solution(exa_batch* b, int id, double* luh_host);
+/* device bytes an instance of that shape adds, and the batch's current total
+ * (for admission by memory budget) */
+int exa_batch_instance_bytes(int dim, int order, int pde, const int* cells, size_t* bytes);
+int exa_batch_device_bytes(const exa_batch* b, size_t* bytes);
+int exa_batch_sweeps(exa_batch* b, long long* picard_sweeps);
+int exa_batch_synchronize(exa_batch* b);
+int exa_batch_stream(exa_batch* b, void** stream);
+
 /* Measurement helper (no counterpart in the reference): sustained FP64 FMA
  * throughput of the current GPU in TFLOP/s, from independent DFMA chains on
  * every SM timed with CUDA events -- the FP64 roofline of the predictor. */
