@@ -30,6 +30,10 @@ import time
 
 import numpy as np
 
+# every mesh of the serving workload has its own stream: let CUDA map up to 32
+# of them to separate hardware queues (the default 8 makes unrelated streams
+# queue behind each other); read when the CUDA context is created
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
@@ -468,13 +472,13 @@ def run_serving_workload(a, world, dev, rank):
     at a time on the plain FP64 path. Default mix (scaled so both arms take
     seconds): 48 requests at 40/s, 70 % 2D with 27..243 cells per side, 30 %
     3D with 9..27, N in {3,5,7}, 20 % limiter explosions, 10..100 steps,
-    8 GB device budget; --serving-full uses 3D sides 9..81, 10..200 steps and
+    64 GB device budget; --serving-full uses 3D sides 9..81, 10..200 steps and
     a 120 GB budget."""
     from exahype_b200 import serving
     import exahype_b200 as eb
     full = a.serving_full
     kw = dict(sides_2d=(27, 243), sides_3d=(9, 81) if full else (9, 27), steps=(10, 200) if full else (10, 100))
-    n, rate, budget = (96, 10.0, 120e9) if full else (48, 40.0, 8e9)
+    n, rate, budget = (96, 10.0, 120e9) if full else (48, 40.0, 64e9)
     variants = {}
     for dim in (2, 3):
         for o in (3, 5, 7):

@@ -264,6 +264,11 @@ class Mesh:
     def set_profiling(self, on=True):
         _check(load().exa_mesh_set_profiling(self._h, int(bool(on))), "exa_mesh_set_profiling")
 
+    def set_priority(self, level):
+        """stream priority level (0 default; higher levels run first when
+        kernels of several streams wait for SMs); call between steps"""
+        _check(load().exa_mesh_set_priority(self._h, int(level)), "exa_mesh_set_priority")
+
     PHASES = ("predictor", "riemann", "corrector", "bookkeeping")
 
     def phase_times(self, reset=False):
@@ -377,6 +382,9 @@ class LimitingMesh:
 
     def synchronize(self):
         _check(load().exa_lmesh_synchronize(self._h), "exa_lmesh_synchronize")
+
+    def set_priority(self, level):
+        _check(load().exa_lmesh_set_priority(self._h, int(level)), "exa_lmesh_set_priority")
 
     @property
     def stream_handle(self):

@@ -67,6 +67,7 @@ struct BatchGroup {
       *bface = nullptr;
   std::vector<int> members;  // instance ids in layout order
   bool dirty = false;
+  bool warmed = false;  // its kernels have run (and set their attributes) outside a capture
 };
 
 struct exa_batch {
@@ -85,18 +86,10 @@ struct exa_batch {
 
 namespace exa {
 
-static void batch_group_free(BatchGroup& g) {
-  cudaFree(g.luh);
-  cudaFree(g.lduh);
-  cudaFree(g.lQhbnd);
-  cudaFree(g.lFhbnd);
-  cudaFree(g.iters);
-  cudaFree(g.cell_inst);
-  cudaFree(g.fl);
-  cudaFree(g.fr);
-  cudaFree(g.fd);
-  cudaFree(g.bcell);
-  cudaFree(g.bface);
+static void batch_group_free(BatchGroup& g, cudaStream_t st) {
+  for (void* p : {(void*)g.luh, (void*)g.lduh, (void*)g.lQhbnd, (void*)g.lFhbnd, (void*)g.iters, (void*)g.cell_inst,
+                  (void*)g.fl, (void*)g.fr, (void*)g.fd, (void*)g.bcell, (void*)g.bface})
+    sfree(p, st);
   g.luh = g.lduh = g.lQhbnd = g.lFhbnd = nullptr;
   g.iters = g.cell_inst = g.fl = g.fr = g.fd = g.bcell = g.bface = nullptr;
 }
@@ -113,8 +106,9 @@ static int batch_grow_slots(exa_batch* b, int need) {
   const int cap = std::max(need, std::max(16, 2 * b->slot_cap));
   double *dt, *dtn, *t, *st, *dx;
   int* live;
-  if (cudaMalloc(&dt, cap * 8) || cudaMalloc(&dtn, cap * 8) || cudaMalloc(&t, cap * 8) || cudaMalloc(&st, cap * 8) ||
-      cudaMalloc(&dx, cap * 24) || cudaMalloc(&live, cap * 4)) {
+  cudaStream_t bs = b->stream;
+  if (!salloc(&dt, cap * 8, bs) || !salloc(&dtn, cap * 8, bs) || !salloc(&t, cap * 8, bs) ||
+      !salloc(&st, cap * 8, bs) || !salloc(&dx, cap * 24, bs) || !salloc(&live, cap * 4, bs)) {
     cudaGetLastError();
     return fail(EXA_ERR_NOMEM, "exa_batch: slot allocation failed");
   }
@@ -128,13 +122,9 @@ static int batch_grow_slots(exa_batch* b, int need) {
     EXA_CUDA(cudaMemcpyAsync(dx, b->dx, b->slot_cap * 24, cudaMemcpyDeviceToDevice, b->stream));
     EXA_CUDA(cudaMemcpyAsync(live, b->live, b->slot_cap * 4, cudaMemcpyDeviceToDevice, b->stream));
   }
-  EXA_CUDA(cudaStreamSynchronize(b->stream));
-  cudaFree(b->dt);
-  cudaFree(b->dtn);
-  cudaFree(b->t);
-  cudaFree(b->steps);
-  cudaFree(b->dx);
-  cudaFree(b->live);
+  for (void* p : {(void*)b->dt, (void*)b->dtn, (void*)b->t, (void*)b->steps, (void*)b->dx, (void*)b->live})
+    sfree(p, bs);
+  EXA_CUDA(cudaStreamSynchronize(bs));
   b->dt = dt;
   b->dtn = dtn;
   b->t = t;
@@ -165,7 +155,7 @@ static int batch_init_fresh(exa_batch* b, BatchGroup& ng, const std::vector<int>
   EXA_CUDA(cudaMemsetAsync(ng.lQhbnd + c0 * D2 * F * nD, 0, nc * D2 * F * nD * 8, st));
   EXA_CUDA(cudaMemsetAsync(ng.lFhbnd + c0 * D2 * F * nV, 0, nc * D2 * F * nV * 8, st));
   int* dslots = nullptr;
-  if (cudaMalloc(&dslots, slots.size() * 4) != cudaSuccess) {
+  if (!salloc(&dslots, slots.size() * 4, st)) {
     cudaGetLastError();
     return fail(EXA_ERR_NOMEM, "exa_batch: device allocation failed");
   }
@@ -189,8 +179,8 @@ static int batch_init_fresh(exa_batch* b, BatchGroup& ng, const std::vector<int>
     rc = ng.k.predictor(ng.luh + c0 * P * nD, ng.lQhbnd + c0 * D2 * F * nD, ng.lFhbnd + c0 * D2 * F * nV,
                         ng.lduh + c0 * P * nV, ng.iters + c0, b->dt, geo, (int)nc, nullptr, nullptr, PredictorTemps{},
                         false, b->sweeps, ng.variant, st);
+  sfree(dslots, st);
   cudaStreamSynchronize(st);
-  cudaFree(dslots);
   return rc;
 }
 
@@ -268,18 +258,16 @@ static int batch_relayout(exa_batch* b, BatchGroup& g) {
     bface.insert(bface.end(), bfc[kd].begin(), bfc[kd].end());
   }
   const size_t nn = std::max<long long>(n, 1);
-  bool ok = cudaMalloc(&ng.luh, nn * P * nD * 8) == cudaSuccess && cudaMalloc(&ng.lduh, nn * P * nV * 8) == cudaSuccess &&
-            cudaMalloc(&ng.lQhbnd, nn * D2 * F * nD * 8) == cudaSuccess &&
-            cudaMalloc(&ng.lFhbnd, nn * D2 * F * nV * 8) == cudaSuccess && cudaMalloc(&ng.iters, nn * 4) == cudaSuccess &&
-            cudaMalloc(&ng.cell_inst, nn * 4) == cudaSuccess &&
-            cudaMalloc(&ng.fl, std::max<size_t>(1, fl.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&ng.fr, std::max<size_t>(1, fl.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&ng.fd, std::max<size_t>(1, fl.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&ng.bcell, std::max<size_t>(1, bcell.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&ng.bface, std::max<size_t>(1, bcell.size()) * 4) == cudaSuccess;
+  bool ok = salloc(&ng.luh, nn * P * nD * 8, st) && salloc(&ng.lduh, nn * P * nV * 8, st) &&
+            salloc(&ng.lQhbnd, nn * D2 * F * nD * 8, st) && salloc(&ng.lFhbnd, nn * D2 * F * nV * 8, st) &&
+            salloc(&ng.iters, nn * 4, st) && salloc(&ng.cell_inst, nn * 4, st) &&
+            salloc(&ng.fl, std::max<size_t>(1, fl.size()) * 4, st) && salloc(&ng.fr, std::max<size_t>(1, fl.size()) * 4, st) &&
+            salloc(&ng.fd, std::max<size_t>(1, fl.size()) * 4, st) &&
+            salloc(&ng.bcell, std::max<size_t>(1, bcell.size()) * 4, st) &&
+            salloc(&ng.bface, std::max<size_t>(1, bcell.size()) * 4, st);
   if (!ok) {
     cudaGetLastError();
-    batch_group_free(ng);
+    batch_group_free(ng, st);
     return fail(EXA_ERR_NOMEM, "exa_batch: device allocation failed");
   }
   if (n) EXA_CUDA(cudaMemcpyAsync(ng.cell_inst, cinst.data(), n * 4, cudaMemcpyHostToDevice, st));
@@ -304,9 +292,12 @@ static int batch_relayout(exa_batch* b, BatchGroup& g) {
     EXA_CUDA(cudaMemcpyAsync(ng.iters + dst, g.iters + src, nc * 4, cudaMemcpyDeviceToDevice, st));
   }
   int rc = EXA_OK;
-  if (!fresh.empty()) rc = batch_init_fresh(b, ng, fresh, new_off);
+  if (!fresh.empty()) {
+    rc = batch_init_fresh(b, ng, fresh, new_off);
+    ng.warmed = true;  // the first predictor of the new instances ran the group's variant
+  }
   if (rc) {
-    batch_group_free(ng);
+    batch_group_free(ng, st);
     return rc;
   }
   EXA_CUDA(cudaStreamSynchronize(st));
@@ -315,7 +306,7 @@ static int batch_relayout(exa_batch* b, BatchGroup& g) {
     b->inst[id].live = true;
     std::vector<double>().swap(b->inst[id].init);
   }
-  batch_group_free(g);
+  batch_group_free(g, st);
   ng.dirty = false;
   g = ng;
   return EXA_OK;
@@ -385,8 +376,12 @@ int exa_batch_create(exa_batch** out) {
   int rc = upload_tables();
   if (rc) return rc;
   std::unique_ptr<exa_batch> b(new exa_batch());
-  EXA_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  if (cudaMalloc(&b->sweeps, 8) != cudaSuccess) {
+  // the batch holds the many small solves: its blocks are scheduled ahead of
+  // those of other streams (large single meshes) when both wait for SMs
+  int lo = 0, hi = 0;
+  EXA_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  EXA_CUDA(cudaStreamCreateWithPriority(&b->stream, cudaStreamNonBlocking, hi));
+  if (!salloc(&b->sweeps, 8, b->stream)) {
     cudaGetLastError();
     cudaStreamDestroy(b->stream);
     return fail(EXA_ERR_NOMEM, "exa_batch_create: device allocation failed");
@@ -402,14 +397,10 @@ int exa_batch_destroy(exa_batch* b) {
   if (!b) return EXA_OK;
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  for (BatchGroup& g : b->groups) batch_group_free(g);
-  cudaFree(b->dt);
-  cudaFree(b->dtn);
-  cudaFree(b->t);
-  cudaFree(b->steps);
-  cudaFree(b->dx);
-  cudaFree(b->live);
-  cudaFree(b->sweeps);
+  for (BatchGroup& g : b->groups) batch_group_free(g, b->stream);
+  for (void* p : {(void*)b->dt, (void*)b->dtn, (void*)b->t, (void*)b->steps, (void*)b->dx, (void*)b->live,
+                  (void*)b->sweeps})
+    sfree(p, b->stream);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return EXA_OK;
@@ -419,11 +410,23 @@ int exa_batch_set_variant(exa_batch* b, int dim, int order, int pde, int variant
   if (!b || variant < 0 || variant >= kPredictorVariants) return fail(EXA_ERR_ARG, "exa_batch_set_variant: bad argument");
   for (BatchGroup& g : b->groups)
     if (g.dim == dim && g.order == order && g.pde == pde) {
+      if (g.variant != variant) g.warmed = false;
       g.variant = variant;
       b->graph_valid = false;
       return EXA_OK;
     }
-  return fail(EXA_ERR_ARG, "exa_batch_set_variant: no instance of that dimension/order/PDE was added");
+  // no instance of this order yet: its group starts with the given variant
+  KernelSet k{};
+  if (!find_kernels(dim, order, pde, &k))
+    return fail(EXA_ERR_UNSUPPORTED, "exa_batch_set_variant: no kernels built for that dimension/order/PDE");
+  BatchGroup g;
+  g.dim = dim;
+  g.order = order;
+  g.pde = pde;
+  g.k = k;
+  g.variant = variant;
+  b->groups.push_back(g);
+  return EXA_OK;
 }
 
 int exa_batch_get_variant(const exa_batch* b, int dim, int order, int pde, int* variant) {
@@ -546,10 +549,13 @@ int exa_batch_step(exa_batch* b, int nsteps) {
       cudaGraphExecDestroy(b->graph);
       b->graph = nullptr;
     }
-    // this step runs eagerly (it also sets the kernels' attributes outside any
-    // capture); the same launch sequence is then captured for the next steps
-    if ((rc = batch_launch_step(b))) return rc;
-    EXA_CUDA(cudaStreamSynchronize(b->stream));
+    bool warm = true;
+    for (const BatchGroup& g : b->groups) warm = warm && (g.ncells == 0 || g.warmed);
+    if (!warm) {  // run this step eagerly: kernels set their attributes outside any capture
+      if ((rc = batch_launch_step(b))) return rc;
+      for (BatchGroup& g : b->groups) g.warmed = true;
+      continue;
+    }
     cudaGraph_t g = nullptr;
     EXA_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     rc = batch_launch_step(b);
@@ -564,6 +570,7 @@ int exa_batch_step(exa_batch* b, int nsteps) {
     if (e2 != cudaSuccess)
       return fail(EXA_ERR_CUDA, std::string("exa_batch_step: instantiate: ") + cudaGetErrorString(e2));
     b->graph_valid = true;
+    EXA_CUDA(cudaGraphLaunch(b->graph, b->stream));
   }
   return EXA_OK;
 }

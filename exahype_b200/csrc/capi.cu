@@ -38,6 +38,42 @@ static int fail(int code, const std::string& msg) {
     if (e_ != cudaSuccess) return fail(EXA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
   } while (0)
 
+// Stream-ordered device allocation for the meshes: cudaMallocAsync and
+// cudaFreeAsync on the owner's stream never wait for other streams (cudaFree
+// synchronises the whole device), so creating or destroying one mesh does
+// not stall the work queued for others.
+// The memory comes from a pool of the library's own per device that keeps
+// freed memory for reuse instead of returning it to the driver, so a server
+// that creates and destroys meshes continuously does not pay for it each time.
+static cudaMemPool_t library_pool() {
+  static std::mutex mu;
+  static std::vector<std::pair<int, cudaMemPool_t>> pools;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto& e : pools)
+    if (e.first == dev) return e.second;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools.emplace_back(dev, pool);
+  return pool;
+}
+template <class T>
+static bool salloc(T** p, size_t bytes, cudaStream_t st) {
+  cudaMemPool_t pool = library_pool();
+  if (!pool) return false;
+  return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, st) == cudaSuccess;
+}
+static void sfree(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
 // ---- tables ---------------------------------------------------------------
 static int upload_tables() {
   static std::mutex mu;
@@ -464,18 +500,9 @@ int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chos
 static void mesh_free(exa_mesh* m) {
   for (cudaEvent_t e : m->ev) cudaEventDestroy(e);
   m->ev.clear();
-  cudaFree(m->luh);
-  cudaFree(m->lduh);
-  cudaFree(m->lQhbnd);
-  cudaFree(m->lFhbnd);
-  cudaFree(m->scal);
-  cudaFree(m->iters);
-  cudaFree(m->fl);
-  cudaFree(m->fr);
-  cudaFree(m->fd);
-  cudaFree(m->bcell);
-  cudaFree(m->bface);
-  cudaFree(m->sweeps);
+  for (void* p : {(void*)m->luh, (void*)m->lduh, (void*)m->lQhbnd, (void*)m->lFhbnd, (void*)m->scal, (void*)m->iters,
+                  (void*)m->fl, (void*)m->fr, (void*)m->fd, (void*)m->bcell, (void*)m->bface, (void*)m->sweeps})
+    sfree(p, m->stream);
   if (m->stream) cudaStreamDestroy(m->stream);
 }
 
@@ -545,34 +572,35 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
   }
   const size_t P = s->k.P, F = s->k.F, nV = s->k.nvar, nD = s->k.nvar + s->k.npar, D2 = 2 * m->dim;
   const size_t n = m->ncells;
-  bool ok = cudaMalloc(&m->luh, n * P * nD * 8) == cudaSuccess && cudaMalloc(&m->lduh, n * P * nV * 8) == cudaSuccess &&
-            cudaMalloc(&m->lQhbnd, n * D2 * F * nD * 8) == cudaSuccess &&
-            cudaMalloc(&m->lFhbnd, n * D2 * F * nV * 8) == cudaSuccess && cudaMalloc(&m->scal, 8 * 8) == cudaSuccess &&
-            cudaMalloc(&m->iters, n * 4) == cudaSuccess &&
-            cudaMalloc(&m->fl, std::max<size_t>(1, fl.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&m->fr, std::max<size_t>(1, fl.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&m->fd, std::max<size_t>(1, fl.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&m->bcell, std::max<size_t>(1, bcell.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&m->bface, std::max<size_t>(1, bcell.size()) * 4) == cudaSuccess &&
-            cudaMalloc(&m->sweeps, 8) == cudaSuccess;
+  EXA_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  cudaStream_t st = m->stream;
+  bool ok = salloc(&m->luh, n * P * nD * 8, st) && salloc(&m->lduh, n * P * nV * 8, st) &&
+            salloc(&m->lQhbnd, n * D2 * F * nD * 8, st) && salloc(&m->lFhbnd, n * D2 * F * nV * 8, st) &&
+            salloc(&m->scal, 8 * 8, st) && salloc(&m->iters, n * 4, st) &&
+            salloc(&m->fl, std::max<size_t>(1, fl.size()) * 4, st) && salloc(&m->fr, std::max<size_t>(1, fl.size()) * 4, st) &&
+            salloc(&m->fd, std::max<size_t>(1, fl.size()) * 4, st) &&
+            salloc(&m->bcell, std::max<size_t>(1, bcell.size()) * 4, st) &&
+            salloc(&m->bface, std::max<size_t>(1, bcell.size()) * 4, st) && salloc(&m->sweeps, 8, st);
   if (!ok) {
     cudaGetLastError();
     mesh_free(m.get());
     return fail(EXA_ERR_NOMEM, "exa_mesh_create: device allocation failed");
   }
-  EXA_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
-  EXA_CUDA(cudaMemcpy(m->fl, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice));
-  EXA_CUDA(cudaMemcpy(m->fr, fr.data(), fr.size() * 4, cudaMemcpyHostToDevice));
-  EXA_CUDA(cudaMemcpy(m->fd, fd.data(), fd.size() * 4, cudaMemcpyHostToDevice));
-  if (!bcell.empty()) {
-    EXA_CUDA(cudaMemcpy(m->bcell, bcell.data(), bcell.size() * 4, cudaMemcpyHostToDevice));
-    EXA_CUDA(cudaMemcpy(m->bface, bface.data(), bface.size() * 4, cudaMemcpyHostToDevice));
+  if (!fl.empty()) {
+    EXA_CUDA(cudaMemcpyAsync(m->fl, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, st));
+    EXA_CUDA(cudaMemcpyAsync(m->fr, fr.data(), fr.size() * 4, cudaMemcpyHostToDevice, st));
+    EXA_CUDA(cudaMemcpyAsync(m->fd, fd.data(), fd.size() * 4, cudaMemcpyHostToDevice, st));
   }
-  EXA_CUDA(cudaMemset(m->luh, 0, n * P * nD * 8));
-  EXA_CUDA(cudaMemset(m->lduh, 0, n * P * nV * 8));
-  EXA_CUDA(cudaMemset(m->lQhbnd, 0, n * D2 * F * nD * 8));
-  EXA_CUDA(cudaMemset(m->lFhbnd, 0, n * D2 * F * nV * 8));
-  EXA_CUDA(cudaMemset(m->sweeps, 0, 8));
+  if (!bcell.empty()) {
+    EXA_CUDA(cudaMemcpyAsync(m->bcell, bcell.data(), bcell.size() * 4, cudaMemcpyHostToDevice, st));
+    EXA_CUDA(cudaMemcpyAsync(m->bface, bface.data(), bface.size() * 4, cudaMemcpyHostToDevice, st));
+  }
+  EXA_CUDA(cudaMemsetAsync(m->luh, 0, n * P * nD * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->lduh, 0, n * P * nV * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->lQhbnd, 0, n * D2 * F * nD * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->lFhbnd, 0, n * D2 * F * nV * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, st));
+  EXA_CUDA(cudaStreamSynchronize(st));
   *out = m.release();
   return EXA_OK;
 }
@@ -781,6 +809,20 @@ int exa_fp64_peak_probe(double* tflops) {
   cudaFree(out);
   if (e != cudaSuccess) return fail(EXA_ERR_CUDA, std::string("exa_fp64_peak_probe: ") + cudaGetErrorString(e));
   *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
+  return EXA_OK;
+}
+
+int exa_mesh_set_priority(exa_mesh* m, int level) {
+  if (!m || level < 0) return fail(EXA_ERR_ARG, "exa_mesh_set_priority: bad argument");
+  int lo = 0, hi = 0;
+  EXA_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  // level 0 is the default (least) priority; greater levels are more urgent
+  const int prio = std::max(hi, lo - level);
+  cudaStream_t st = nullptr;
+  EXA_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio));
+  EXA_CUDA(cudaStreamSynchronize(m->stream));  // all work and allocations so far are done
+  cudaStreamDestroy(m->stream);
+  m->stream = st;
   return EXA_OK;
 }
 
@@ -1176,22 +1218,12 @@ int exa_fv_musclhancock_update_noalloc(const exa_solver* s, double* lim, double*
 }
 
 static void lmesh_free(exa_lmesh* lm) {
-  cudaFree(lm->s);
-  cudaFree(lm->s_prev);
-  cudaFree(lm->cure);
-  cudaFree(lm->fs);
-  cudaFree(lm->has_lim);
-  cudaFree(lm->flags);
-  cudaFree(lm->listA);
-  cudaFree(lm->listF);
-  cudaFree(lm->listP);
-  cudaFree(lm->minB);
-  cudaFree(lm->maxB);
-  cudaFree(lm->lim);
-  cudaFree(lm->lim_prev);
-  cudaFree(lm->luh_prev);
-  cudaFree(lm->fv_ic);
-  cudaFree(lm->gscratch);
+  cudaStream_t st = lm->m ? lm->m->stream : nullptr;
+  for (void* p : {(void*)lm->s, (void*)lm->s_prev, (void*)lm->cure, (void*)lm->fs, (void*)lm->has_lim,
+                  (void*)lm->flags, (void*)lm->listA, (void*)lm->listF, (void*)lm->listP, (void*)lm->minB,
+                  (void*)lm->maxB, (void*)lm->lim, (void*)lm->lim_prev, (void*)lm->luh_prev, (void*)lm->fv_ic,
+                  (void*)lm->gscratch})
+    sfree(p, st);
   if (lm->m) exa_mesh_destroy(lm->m);
   lm->m = nullptr;
 }
@@ -1227,15 +1259,14 @@ int exa_lmesh_create(const exa_solver* s, const int* cells, const double* offset
     return rc;
   }
   const size_t scr = ops.scratch();
-  bool ok = cudaMalloc(&lm->s, n * 4) == cudaSuccess && cudaMalloc(&lm->s_prev, n * 4) == cudaSuccess &&
-            cudaMalloc(&lm->cure, n * 4) == cudaSuccess && cudaMalloc(&lm->fs, n * D2 * 4) == cudaSuccess &&
-            cudaMalloc(&lm->has_lim, n * 4) == cudaSuccess && cudaMalloc(&lm->flags, 4 * 4) == cudaSuccess &&
-            cudaMalloc(&lm->listA, n * 4) == cudaSuccess && cudaMalloc(&lm->listF, n * 4) == cudaSuccess &&
-            cudaMalloc(&lm->listP, n * 4) == cudaSuccess && cudaMalloc(&lm->minB, n * D2 * 5 * 8) == cudaSuccess &&
-            cudaMalloc(&lm->maxB, n * D2 * 5 * 8) == cudaSuccess && cudaMalloc(&lm->lim, n * lm->LS * 8) == cudaSuccess &&
-            cudaMalloc(&lm->lim_prev, n * lm->LS * 8) == cudaSuccess &&
-            cudaMalloc(&lm->luh_prev, n * P * 5 * 8) == cudaSuccess &&
-            (scr == 0 || cudaMalloc(&lm->gscratch, (size_t)lm->muscl_grid * scr * 8) == cudaSuccess);
+  cudaStream_t lst = lm->m->stream;
+  bool ok = salloc(&lm->s, n * 4, lst) && salloc(&lm->s_prev, n * 4, lst) && salloc(&lm->cure, n * 4, lst) &&
+            salloc(&lm->fs, n * D2 * 4, lst) && salloc(&lm->has_lim, n * 4, lst) && salloc(&lm->flags, 4 * 4, lst) &&
+            salloc(&lm->listA, n * 4, lst) && salloc(&lm->listF, n * 4, lst) && salloc(&lm->listP, n * 4, lst) &&
+            salloc(&lm->minB, n * D2 * 5 * 8, lst) && salloc(&lm->maxB, n * D2 * 5 * 8, lst) &&
+            salloc(&lm->lim, n * lm->LS * 8, lst) && salloc(&lm->lim_prev, n * lm->LS * 8, lst) &&
+            salloc(&lm->luh_prev, n * P * 5 * 8, lst) &&
+            (scr == 0 || salloc(&lm->gscratch, (size_t)lm->muscl_grid * scr * 8, lst));
   if (!ok) {
     cudaGetLastError();
     lmesh_free(lm.get());
@@ -1276,7 +1307,7 @@ int exa_lmesh_get_solution(exa_lmesh* lm, double* h) {
 int exa_lmesh_set_fv_initial(exa_lmesh* lm, const double* h) {
   if (!lm || !h) return fail(EXA_ERR_ARG, "exa_lmesh_set_fv_initial: null argument");
   const size_t bytes = (size_t)lm->m->ncells * lm->PB * 5 * 8;
-  if (!lm->fv_ic && cudaMalloc(&lm->fv_ic, bytes) != cudaSuccess) {
+  if (!lm->fv_ic && !salloc(&lm->fv_ic, bytes, lm->m->stream)) {
     cudaGetLastError();
     lm->fv_ic = nullptr;
     return fail(EXA_ERR_NOMEM, "exa_lmesh_set_fv_initial: device allocation failed");
@@ -1351,6 +1382,11 @@ int exa_lmesh_get_limiter(exa_lmesh* lm, double* lim, int* allocated) {
   if (allocated) EXA_CUDA(cudaMemcpyAsync(allocated, lm->has_lim, n * 4, cudaMemcpyDeviceToHost, lm->m->stream));
   EXA_CUDA(cudaStreamSynchronize(lm->m->stream));
   return EXA_OK;
+}
+
+int exa_lmesh_set_priority(exa_lmesh* lm, int level) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_set_priority: null mesh");
+  return exa_mesh_set_priority(lm->m, level);
 }
 
 int exa_lmesh_synchronize(exa_lmesh* lm) {

@@ -139,6 +139,11 @@ int exa_mesh_run_until(exa_mesh* m, double t_end, int max_steps, int* steps);
  * number of Picard sweeps executed by the predictor so far */
 int exa_mesh_state(exa_mesh* m, double* t, double* dt, long long* steps, long long* picard_sweeps);
 int exa_mesh_synchronize(exa_mesh* m);
+/* Moves the mesh's work to a new stream of stream priority `level` (0: the
+ * default, least urgent; each level up is more urgent, capped at the device's
+ * range): where several streams' kernels wait for SMs, the higher priority's
+ * go first. Synchronises the mesh's stream; call it between steps. */
+int exa_mesh_set_priority(exa_mesh* m, int level);
 /* the CUDA stream (cudaStream_t) all of the mesh's work is ordered on */
 int exa_mesh_stream(exa_mesh* m, void** stream);
 /* Per-phase device timing with CUDA events recorded on the mesh stream around
@@ -236,6 +241,7 @@ int exa_lmesh_get_status(exa_lmesh* m, int* status_host);
  * patch is not allocated hold stale values) and per-cell allocation flags */
 int exa_lmesh_get_limiter(exa_lmesh* m, double* lim_host, int* allocated_host);
 int exa_lmesh_synchronize(exa_lmesh* m);
+int exa_lmesh_set_priority(exa_lmesh* m, int level);  /* as exa_mesh_set_priority */
 int exa_lmesh_stream(exa_lmesh* m, void** stream);
 
 /* ---- batched ragged ensemble (no counterpart in the reference) ------------ */
@@ -250,7 +256,9 @@ int exa_lmesh_stream(exa_lmesh* m, void** stream);
  * instance id; adds and removes take effect at the next exa_batch_commit or
  * exa_batch_step (new instances get exa_mesh_init's first step size and
  * predictor, t = 0). The first instance of an order runs the predictor
- * autotuner for that order. */
+ * autotuner for that order unless exa_batch_set_variant set its variant
+ * before. The batch's stream has the highest stream
+ * priority, so its kernels go ahead of other streams' when both wait for SMs. */
 typedef struct exa_batch exa_batch;
 int exa_batch_create(exa_batch** out);
 int exa_batch_destroy(exa_batch* b);
