@@ -331,6 +331,7 @@ def run_ours(a):
                    "sample": "1 full time step of the 27^3 mesh (after the initial predictor) on the "
                              "reference's generic kernels, %.1f s" % r["seconds"]}
     launches = sum(v[1] for v in ph.values())
+    mixed = None if a.no_mixed else run_mixed_arm(a, u0, s.variant, dev)
     lim = None if a.no_limiter else run_limiter_workload(a, world, dev, rank)
     ens = None if a.no_ensemble else run_ensemble_workload(a, world, dev, rank)
     srv = None if a.no_serving else run_serving_workload(a, world, dev, rank)
@@ -343,7 +344,7 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
-        "limiter": lim, "ensemble": ens, "serving": srv,
+        "mixed": mixed, "limiter": lim, "ensemble": ens, "serving": srv,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -512,6 +513,40 @@ def run_serving_workload(a, world, dev, rank):
             "timing": "host wall clock from the first arrival to the last result on the host"}
 
 
+def run_mixed_arm(a, u0, fp64_variant, dev):
+    """The same workload with the mixed-precision predictor (EXA_PREDICTOR_MIXED):
+    DoF-updates/s over the same timed steps, and the relative L2 difference of
+    its solution from the FP64 path's after warm-up + timed steps."""
+    import torch
+    import exahype_b200 as eb
+    out = {}
+    sols = {}
+    for name, variant in (("mixed", eb.PREDICTOR_MIXED), ("fp64", fp64_variant)):
+        s = eb.Solver(DIM, ORDER, eb.PDE_EULER)
+        s.variant = variant
+        m = eb.Mesh(s, CELLS, [0.0] * DIM, [1.0] * DIM, eb.BC_PERIODIC)
+        m.set_solution(u0)
+        m.init(0.0)
+        m.step(a.warmup)
+        m.synchronize()
+        stream = torch.cuda.ExternalStream(m.stream_handle, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.step(a.steps)
+        e1.record(stream)
+        e1.synchronize()
+        sols[name] = m.get_solution()
+        if name == "mixed":
+            ms = e0.elapsed_time(e1)
+            out = {"value": dof_per_step() * a.steps / (ms / 1e3), "unit": "DoF-updates/s",
+                   "ms_per_step": ms / a.steps, "variant": variant,
+                   "picard_sweeps_per_step": m.state()["picard_sweeps"] / (a.steps + a.warmup + 1)}
+    err = float(np.linalg.norm(sols["mixed"] - sols["fp64"]) / np.linalg.norm(sols["fp64"]))
+    out["rel_l2_vs_fp64"] = err
+    out["within_1e-9"] = err <= 1e-9
+    return out
+
+
 def measure_fp64_peak():
     import ctypes
     import exahype_b200 as eb
@@ -535,6 +570,7 @@ def main():
     ap.add_argument("--no-fp64-probe", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="predictor variant (default: autotune)")
     ap.add_argument("--no-limiter", action="store_true", help="skip the limiter workload")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     ap.add_argument("--limiter-steps", type=int, default=0, help="limiter workload: K steps instead of t = 0.2")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")

@@ -25,6 +25,8 @@ LIB_PATH = os.path.join(HERE, "lib", "libexahype_b200.so")
 PDE_EULER = 0
 PDE_EULER_TEST = 1
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE = -1, 0, 1
+# predictor variants beyond the autotuned 0..3: the mixed-precision predictor
+PREDICTOR_MIXED, PREDICTOR_MIXED_2 = 4, 5
 
 _lib = None
 

@@ -407,7 +407,7 @@ int exa_batch_destroy(exa_batch* b) {
 }
 
 int exa_batch_set_variant(exa_batch* b, int dim, int order, int pde, int variant) {
-  if (!b || variant < 0 || variant >= kPredictorVariants) return fail(EXA_ERR_ARG, "exa_batch_set_variant: bad argument");
+  if (!b || variant < 0 || variant >= kAllVariants) return fail(EXA_ERR_ARG, "exa_batch_set_variant: bad argument");
   for (BatchGroup& g : b->groups)
     if (g.dim == dim && g.order == order && g.pde == pde) {
       if (g.variant != variant) g.warmed = false;

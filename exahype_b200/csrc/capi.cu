@@ -84,10 +84,13 @@ static int upload_tables() {
   for (int d : done_dev)
     if (d == dev) return EXA_OK;
   std::vector<OrderTables> h(kMaxOrder + 1);
+  std::vector<LimiterTables> hl(kMaxOrder + 1);
   std::memset(h.data(), 0, sizeof(OrderTables) * h.size());
+  std::memset(hl.data(), 0, sizeof(LimiterTables) * hl.size());
   for (int N = 1; N <= kMaxOrder; N++) {
     const int b = N + 1, bl = 2 * N + 1;
     OrderTables& t = h[N];
+    LimiterTables& l = hl[N];
     for (int i = 0; i < b; i++) {
       t.w[i] = exa_tab_weights[exa_tab_weights_off[N] + i];
       t.x[i] = exa_tab_nodes[exa_tab_nodes_off[N] + i];
@@ -98,14 +101,16 @@ static int upload_tables() {
     for (int i = 0; i < b * b; i++) {
       t.Kxi[i] = exa_tab_Kxi[exa_tab_Kxi_off[N] + i];
       t.iK1[i] = exa_tab_iK1[exa_tab_iK1_off[N] + i];
-      t.uh2lob[i] = exa_tab_uh2lob[exa_tab_uh2lob_off[N] + i];
+      t.Kxi_f[i] = (float)t.Kxi[i];
+      l.uh2lob[i] = exa_tab_uh2lob[exa_tab_uh2lob_off[N] + i];
     }
     for (int i = 0; i < b * bl; i++) {
-      t.uh2lim[i] = exa_tab_uh2lim[exa_tab_uh2lim_off[N] + i];
-      t.lim2uh[i] = exa_tab_lim2uh[exa_tab_lim2uh_off[N] + i];
+      l.uh2lim[i] = exa_tab_uh2lim[exa_tab_uh2lim_off[N] + i];
+      l.lim2uh[i] = exa_tab_lim2uh[exa_tab_lim2uh_off[N] + i];
     }
   }
   EXA_CUDA(cudaMemcpyToSymbol(c_tab, h.data(), sizeof(OrderTables) * h.size()));
+  EXA_CUDA(cudaMemcpyToSymbol(g_lim_tab, hl.data(), sizeof(LimiterTables) * hl.size()));
   done_dev.push_back(dev);
   return EXA_OK;
 }
@@ -134,10 +139,14 @@ __global__ void sweep_count_kernel(const int* iters, const int* cell_list, int n
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
 }
 
-// Predictor variants the autotuner chooses from:
+// Predictor variants the autotuner chooses from (all FP64):
 //   0 node form, 1 block/SM budget    1 line form, 1 block/SM
 //   2 line form, 2 blocks/SM          3 node form, 2 blocks/SM
+// and the mixed-precision line form (FP32 increment sweeps after the first
+// FP64 sweep), selected explicitly:
+//   4 mixed line form, 1 block/SM     5 mixed line form, 2 blocks/SM
 constexpr int kPredictorVariants = 4;
+constexpr int kAllVariants = 6;
 
 template <int DIM, int N, class PDE>
 struct Launch {
@@ -160,24 +169,25 @@ struct Launch {
     return EXA_OK;
   }
 
-  template <bool TEMPS, int MB>
+  template <bool TEMPS, int MB, bool MIXED = false>
   static int launch_lines(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
                           Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, cudaStream_t st) {
-    using LC = LinesCfg<DIM, N, PDE, MB>;
+    using LC = LinesCfg<DIM, N, PDE, MB, MIXED>;
     static bool attr = false;
     if (!attr) {
-      EXA_CUDA(cudaFuncSetAttribute(predictor_lines_kernel<DIM, N, PDE, TEMPS, MB>,
+      EXA_CUDA(cudaFuncSetAttribute(predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LC::SMEM));
       attr = true;
     }
     const int grid = (n + LC::CPB - 1) / LC::CPB;
-    predictor_lines_kernel<DIM, N, PDE, TEMPS, MB><<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
+    predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED><<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
                                                                                        n, list, tmp, cnt);
     EXA_LAUNCHED();
     return EXA_OK;
   }
   // two blocks of the line form only fit when their shared memory does
   static constexpr bool kLines2 = 2 * LinesCfg<DIM, N, PDE, 2>::SMEM <= 227 * 1024;
+  static constexpr bool kMixed2 = 2 * LinesCfg<DIM, N, PDE, 2, true>::SMEM <= 227 * 1024;
 
   static int predictor(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
                        Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, bool temps,
@@ -193,6 +203,10 @@ struct Launch {
       rc = launch_lines<false, kLines2 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else if (variant == 3)
       rc = launch_pred<false, 1, 2>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
+    else if (variant == 4 || (variant == 5 && !kMixed2))
+      rc = launch_lines<false, 1, true>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
+    else if (variant == 5)
+      rc = launch_lines<false, kMixed2 ? 2 : 1, true>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else
       rc = launch_pred<false, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     if (rc) return rc;
@@ -431,7 +445,7 @@ __global__ void autotune_fill_kernel(double* luh, long long n, int nD) {
 }
 
 int exa_solver_set_variant(exa_solver* s, int variant) {
-  if (!s || variant < 0 || variant >= kPredictorVariants) return fail(EXA_ERR_ARG, "exa_solver_set_variant: bad argument");
+  if (!s || variant < 0 || variant >= kAllVariants) return fail(EXA_ERR_ARG, "exa_solver_set_variant: bad argument");
   s->variant = variant;
   return EXA_OK;
 }

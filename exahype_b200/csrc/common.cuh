@@ -19,6 +19,14 @@ struct OrderTables {
   double w[kMaxB], x[kMaxB], FL[kMaxB], FR[kMaxB];
   double Kxi[kMaxB * kMaxB], iK1[kMaxB * kMaxB];
   double lobatto[kMaxB];
+  // FP32 copy of Kxi for the mixed-precision Picard sweeps
+  float Kxi_f[kMaxB * kMaxB];
+};
+
+// Limiter projections of one order, in global memory (they are read by
+// whole blocks through shared-memory staging, and the constant bank is kept
+// for the predictor's operands).
+struct LimiterTables {
   double uh2lim[kMaxB * (2 * kMaxOrder + 1)];  // [k][i]: DG basis k -> subcell i
   double lim2uh[(2 * kMaxOrder + 1) * kMaxB];  // [i][j]: subcell i -> DG basis j
   double uh2lob[kMaxB * kMaxB];                // [j][i]: DG basis j at Lobatto node i
@@ -27,6 +35,7 @@ struct OrderTables {
 // Filled by upload_tables() (capi.cu) when the first solver is created on a
 // device. The library is one translation unit, so this is the only definition.
 __constant__ OrderTables c_tab[kMaxOrder + 1];
+__device__ LimiterTables g_lim_tab[kMaxOrder + 1];
 
 constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
 

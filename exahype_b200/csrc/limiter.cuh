@@ -109,7 +109,7 @@ __device__ void project_fv_block(const double* luh, double* lim, double* tmp) {
   tensor_map<DIM, L::b, L::B>(
       [&](int z, int y, int x, int v) { return luh[(((DIM == 3 ? z * L::b : 0) + y) * L::b + x) * L::nV + v]; },
       [&](int z, int y, int x, int v, double s) { lim[lim_index<DIM, N>(z, y, x) * L::nV + v] = s; },
-      c_tab[N].uh2lim, tmp);
+      g_lim_tab[N].uh2lim, tmp);
 }
 // projectOnDGSpace (Limiter.cpp:69-112): interior subcells -> DG nodes
 template <int DIM, int N>
@@ -118,7 +118,7 @@ __device__ void project_dg_block(const double* lim, double* luh, double* tmp) {
   tensor_map<DIM, L::B, L::b>(
       [&](int z, int y, int x, int v) { return lim[lim_index<DIM, N>(z, y, x) * L::nV + v]; },
       [&](int z, int y, int x, int v, double s) { luh[(((DIM == 3 ? z * L::b : 0) + y) * L::b + x) * L::nV + v] = s; },
-      c_tab[N].lim2uh, tmp);
+      g_lim_tab[N].lim2uh, tmp);
 }
 
 // block-wide min/max of 5 variables: each thread passes its partial values
@@ -481,8 +481,8 @@ __device__ void local_minmax_block(const double* u, double* mn, double* mx, doub
     mx[v] = (mx[v] < val) ? val : mx[v];
   };
   auto src = [&](int z, int y, int x, int v) { return u[(((DIM == 3 ? z * L::b : 0) + y) * L::b + x) * nV + v]; };
-  tensor_map<DIM, L::b, L::b>(src, fold, c_tab[N].uh2lob, tmp);
-  tensor_map<DIM, L::b, L::B>(src, fold, c_tab[N].uh2lim, tmp);
+  tensor_map<DIM, L::b, L::b>(src, fold, g_lim_tab[N].uh2lob, tmp);
+  tensor_map<DIM, L::b, L::B>(src, fold, g_lim_tab[N].uh2lim, tmp);
   block_minmax5(mn, mx, red);
 }
 

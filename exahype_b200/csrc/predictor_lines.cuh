@@ -31,22 +31,25 @@ constexpr int line_slab(int b, int dim, int lines5) {
                   : (b == 6 ? 30 : b == 4 ? 20 : b == 8 ? 42 : b == 5 ? 25 : lines5 + 1);
 }
 
-template <int DIM, int N, class PDE, int MINB>
+// MIXED: the mixed-precision form (see predictor_lines_kernel) keeps each
+// node's last FP32 update in shared memory, SD doubles per cell.
+template <int DIM, int N, class PDE, int MINB, bool MIXED = false>
 struct LinesCfg : Shape<DIM, N, PDE> {
   using S = Shape<DIM, N, PDE>;
   static constexpr int CPB = cells_per_block<S::P>();
   static constexpr int THREADS = CPB * S::P;
   static constexpr int LINES = S::P / S::b;  // lines per direction = face nodes
   static constexpr int SR = S::P + 1;
+  static constexpr int SD = MIXED ? (S::P * S::b * S::nV + 1) / 2 : 0;
   static constexpr int SLAB0 = S::nV == 5 ? line_slab(S::b, DIM, LINES * 5) : LINES * S::nV + 1;
   // padded strides (bank-conflict-free) where they fit in 227 KB, packed otherwise
   static constexpr bool kPad =
-      sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + DIM * S::b * SLAB0 + SR)) <= 227 * 1024;
+      sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + DIM * S::b * SLAB0 + SR + SD)) <= 227 * 1024;
   static constexpr int SLAB = kPad ? SLAB0 : LINES * S::nV;
   static constexpr int QS = kPad ? S::b * S::nD + 1 : S::b * S::nD;  // lQi node stride
   static constexpr int SQ = S::P * QS;
   static constexpr int SF = DIM * S::b * SLAB;
-  static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR));
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR + SD));
   static constexpr int ITEMS = CPB * DIM * LINES * S::nV;  // phase-B work items per block
   static constexpr int IPT = (ITEMS + THREADS - 1) / THREADS;  // items per thread
 };
@@ -59,13 +62,22 @@ __device__ __forceinline__ void node_line(int d, int z, int y, int x, int& n, in
   else { n = z; L = y * b + x; }
 }
 
-template <int DIM, int N, class PDE, bool TEMPS, int MINB>
-__global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
+// MIXED: the first sweep is the FP64 sweep above; every later sweep k works
+// on increments. Its flux increment dF = F(q^k) - F(q^k - d^k) (d^k the
+// node's last update, kept in FP32) is formed in FP64 and stored in FP32; the
+// line contractions of dF run in FP32 (half the shared-memory bytes, FP32
+// arithmetic); the iK1 fold accumulates in FP64 and the update d^(k+1) is
+// added to the FP64 iterate. The rhs0 term
+// cancels in the difference, so FP32 only ever carries the increments, whose
+// rounding (relative 6e-8 of the update) is far below the stop test's scale.
+// The stop test and the outputs are as in the FP64 form.
+template <int DIM, int N, class PDE, bool TEMPS, int MINB, bool MIXED = false>
+__global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED>::THREADS, MINB)
     predictor_lines_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                            double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
                            Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp,
                            const int* __restrict__ count) {
-  using C = LinesCfg<DIM, N, PDE, MINB>;
+  using C = LinesCfg<DIM, N, PDE, MINB, MIXED>;
   constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, SLAB = C::SLAB, QS = C::QS;
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
@@ -79,6 +91,11 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
   double* sF = smem + C::CPB * C::SQ + lc * C::SF;
   double* sR = smem + C::CPB * (C::SQ + C::SF) + lc * C::SR;
   double* sFall = smem + C::CPB * C::SQ;
+  // FP32 views (mixed sweeps): the slices at the same offsets in float units
+  // (a cell's float slice is its double slice's first half), the updates
+  float* sF32 = reinterpret_cast<float*>(sF);
+  float* sFall32 = reinterpret_cast<float*>(sFall);
+  float* sD = reinterpret_cast<float*>(smem + C::CPB * (C::SQ + C::SF + C::SR) + lc * C::SD);
 
   // quadrature weights in shared memory: phase-B threads index them by line,
   // which would serialise on the constant cache
@@ -149,7 +166,8 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
   bool done = !active;
   int it_done = 0;
   for (int iter = 0; iter < C::maxIter; iter++) {
-    double qn[b][nV];
+    const bool low = MIXED && iter > 0;  // an FP32 increment sweep
+    double qn[b][nV];  // the new iterate (FP64 sweep) or the update (increment sweep)
 #pragma unroll
     for (int l = 0; l < b; l++)
 #pragma unroll
@@ -158,7 +176,21 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
     for (int t = 0; t < b; t++) {
       __syncthreads();  // phase C of the previous slice is done with sF
       // A: fluxes of slice t, line-major
-      if (!done) {
+      if (!done && low) {  // flux increments in FP64, stored as FP32
+        double Q[nD], Qp[nD];
+#pragma unroll
+        for (int v = 0; v < nD; v++) Q[v] = Qp[v] = sQ[p * QS + t * nD + v];
+#pragma unroll
+        for (int v = 0; v < nV; v++) Qp[v] -= (double)sD[(p * b + t) * nV + v];
+        double Fl[DIM][nV], Fp[DIM][nV];
+        PDE::template flux<DIM>(Q, Fl);
+        PDE::template flux<DIM>(Qp, Fp);
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int v = 0; v < nV; v++)
+            sF32[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = (float)(Fl[d][v] - Fp[d][v]);
+      } else if (!done) {
         double Q[nD];
 #pragma unroll
         for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
@@ -174,6 +206,21 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
 #pragma unroll
       for (int k = 0; k < C::IPT; k++) {
         if (it_off[k] < 0 || s_done[it_cell[k]]) continue;
+        if (low) {
+          float* base = sFall32 + it_off[k] + it_cell[k] * C::SF;
+          float f[b];
+#pragma unroll
+          for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
+          const float us = (float)(T.w[t] * it_us[k]);
+#pragma unroll
+          for (int l = 0; l < b; l++) {
+            float s = 0.0f;
+#pragma unroll
+            for (int n = 0; n < b; n++) s = fmaf(f[n], T.Kxi_f[n * b + l], s);
+            base[l * SLAB] = us * s;
+          }
+          continue;
+        }
         double* base = sFall + it_off[k];
         double f[b];
 #pragma unroll
@@ -189,7 +236,17 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
       }
       __syncthreads();
       // C: rhs at this node, folded into the Picard accumulators
-      if (!done) {
+      if (!done && low) {  // increment: the rhs0 term cancels
+#pragma unroll
+        for (int v = 0; v < nV; v++) {
+          double rhs = 0.0;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) rhs -= (double)sF32[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+          const double ir = iw * rhs;
+#pragma unroll
+          for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
+        }
+      } else if (!done) {
         const double r0 = wpt * T.FL[t];
 #pragma unroll
         for (int v = 0; v < nV; v++) {
@@ -209,8 +266,9 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
       for (int l = 0; l < b; l++)
 #pragma unroll
         for (int v = 0; v < nV; v++) {
-          const double dq = qn[l][v] - sQ[p * QS + l * nD + v];
+          const double dq = low ? qn[l][v] : qn[l][v] - sQ[p * QS + l * nD + v];
           part = fma(dq, dq, part);
+          if (MIXED) sD[(p * b + l) * nV + v] = (float)dq;  // own node only: no barrier needed
         }
     }
     sR[p] = part;
@@ -262,7 +320,12 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB>::THREADS, MINB)
 #pragma unroll
       for (int l = 0; l < b; l++)
 #pragma unroll
-        for (int v = 0; v < nV; v++) sQ[p * QS + l * nD + v] = qn[l][v];
+        for (int v = 0; v < nV; v++) {
+          if (low)
+            sQ[p * QS + l * nD + v] += qn[l][v];
+          else
+            sQ[p * QS + l * nD + v] = qn[l][v];
+        }
     }
     if (p == 0) s_done[lc] = done;
     if (!__syncthreads_or(!done)) break;

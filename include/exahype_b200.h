@@ -70,6 +70,15 @@ int exa_solver_sizes(const exa_solver* s, int* sizes4);
  * (optional) receives the per-variant milliseconds. It allocates and frees
  * its own device buffers and synchronises the device. */
 #define EXA_PREDICTOR_VARIANTS 4
+/* Variants beyond the autotuned ones (exa_solver_set_variant only): the
+ * mixed-precision predictor. Its first Picard sweep is the FP64 sweep; every
+ * later sweep forms the flux increment F(q^k) - F(q^(k-1)) in FP64 and runs
+ * the stiffness contractions and the iK1 fold of that increment in FP32,
+ * adding the FP32 update to the FP64 iterate (no counterpart in the
+ * reference, whose predictor is FP64 throughout). Results differ from the
+ * FP64 predictor at the level of FP32 rounding of the later updates. */
+#define EXA_PREDICTOR_MIXED 4    /* mixed line form, 1 block per SM */
+#define EXA_PREDICTOR_MIXED_2 5  /* mixed line form, 2 blocks per SM where they fit */
 int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chosen);
 int exa_solver_set_variant(exa_solver* s, int variant);
 int exa_solver_get_variant(const exa_solver* s, int* variant);
