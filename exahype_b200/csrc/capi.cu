@@ -142,11 +142,13 @@ __global__ void sweep_count_kernel(const int* iters, const int* cell_list, int n
 // Predictor variants the autotuner chooses from (all FP64):
 //   0 node form, 1 block/SM budget    1 line form, 1 block/SM
 //   2 line form, 2 blocks/SM          3 node form, 2 blocks/SM
+//   6 line form, two time slices per phase, 2 blocks/SM
+//   7 line form, two time slices per phase, 1 block/SM
 // and the mixed-precision line form (FP32 increment sweeps after the first
-// FP64 sweep), selected explicitly:
+// FP64 sweep), selected explicitly, never by the autotuner:
 //   4 mixed line form, 1 block/SM     5 mixed line form, 2 blocks/SM
-constexpr int kPredictorVariants = 4;
-constexpr int kAllVariants = 6;
+constexpr int kAllVariants = 8;
+constexpr bool variant_is_mixed(int v) { return v == 4 || v == 5; }
 
 template <int DIM, int N, class PDE>
 struct Launch {
@@ -169,18 +171,18 @@ struct Launch {
     return EXA_OK;
   }
 
-  template <bool TEMPS, int MB, bool MIXED = false>
+  template <bool TEMPS, int MB, bool MIXED = false, int TS = 1>
   static int launch_lines(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
                           Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, cudaStream_t st) {
-    using LC = LinesCfg<DIM, N, PDE, MB, MIXED>;
+    using LC = LinesCfg<DIM, N, PDE, MB, MIXED, TS>;
     static bool attr = false;
     if (!attr) {
-      EXA_CUDA(cudaFuncSetAttribute(predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED>,
+      EXA_CUDA(cudaFuncSetAttribute(predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED, TS>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LC::SMEM));
       attr = true;
     }
     const int grid = (n + LC::CPB - 1) / LC::CPB;
-    predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED><<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
+    predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED, TS><<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
                                                                                        n, list, tmp, cnt);
     EXA_LAUNCHED();
     return EXA_OK;
@@ -188,6 +190,8 @@ struct Launch {
   // two blocks of the line form only fit when their shared memory does
   static constexpr bool kLines2 = 2 * LinesCfg<DIM, N, PDE, 2>::SMEM <= 227 * 1024;
   static constexpr bool kMixed2 = 2 * LinesCfg<DIM, N, PDE, 2, true>::SMEM <= 227 * 1024;
+  static constexpr bool kSlices2 = 2 * LinesCfg<DIM, N, PDE, 2, false, 2>::SMEM <= 227 * 1024;
+  static constexpr bool kSlices1 = LinesCfg<DIM, N, PDE, 1, false, 2>::SMEM <= 227 * 1024;
 
   static int predictor(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
                        Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, bool temps,
@@ -207,6 +211,10 @@ struct Launch {
       rc = launch_lines<false, 1, true>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else if (variant == 5)
       rc = launch_lines<false, kMixed2 ? 2 : 1, true>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
+    else if (variant == 6 && kSlices2)
+      rc = launch_lines<false, 2, false, kSlices2 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
+    else if (variant == 6 || variant == 7)
+      rc = launch_lines<false, 1, false, kSlices1 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else
       rc = launch_pred<false, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     if (rc) return rc;
@@ -482,7 +490,11 @@ int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chos
   cudaEventCreate(&b);
   int best = 0;
   double best_ms = 1e300;
-  for (int v = 0; v < kPredictorVariants && rc == EXA_OK; v++) {
+  for (int v = 0; v < kAllVariants && rc == EXA_OK; v++) {
+    if (variant_is_mixed(v)) {  // changes the results: never chosen for the user
+      if (variant_ms) variant_ms[v] = -1.0;
+      continue;
+    }
     float ms = 0.f, tot = 0.f;
     for (int r = 0; r < 4 && rc == EXA_OK; r++) {
       cudaEventRecord(a, st);

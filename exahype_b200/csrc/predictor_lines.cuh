@@ -33,7 +33,9 @@ constexpr int line_slab(int b, int dim, int lines5) {
 
 // MIXED: the mixed-precision form (see predictor_lines_kernel) keeps each
 // node's last FP32 update in shared memory, SD doubles per cell.
-template <int DIM, int N, class PDE, int MINB, bool MIXED = false>
+// TS: time slices per phase (each phase of a Picard sweep handles TS slices
+// between two barriers; TS slice buffers per cell).
+template <int DIM, int N, class PDE, int MINB, bool MIXED = false, int TS = 1>
 struct LinesCfg : Shape<DIM, N, PDE> {
   using S = Shape<DIM, N, PDE>;
   static constexpr int CPB = cells_per_block<S::P>();
@@ -44,11 +46,12 @@ struct LinesCfg : Shape<DIM, N, PDE> {
   static constexpr int SLAB0 = S::nV == 5 ? line_slab(S::b, DIM, LINES * 5) : LINES * S::nV + 1;
   // padded strides (bank-conflict-free) where they fit in 227 KB, packed otherwise
   static constexpr bool kPad =
-      sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + DIM * S::b * SLAB0 + SR + SD)) <= 227 * 1024;
+      sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + TS * DIM * S::b * SLAB0 + SR + SD)) <= 227 * 1024;
   static constexpr int SLAB = kPad ? SLAB0 : LINES * S::nV;
   static constexpr int QS = kPad ? S::b * S::nD + 1 : S::b * S::nD;  // lQi node stride
   static constexpr int SQ = S::P * QS;
-  static constexpr int SF = DIM * S::b * SLAB;
+  static constexpr int SFJ = DIM * S::b * SLAB;  // one slice
+  static constexpr int SF = TS * SFJ;
   static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR + SD));
   static constexpr int ITEMS = CPB * DIM * LINES * S::nV;  // phase-B work items per block
   static constexpr int IPT = (ITEMS + THREADS - 1) / THREADS;  // items per thread
@@ -71,13 +74,14 @@ __device__ __forceinline__ void node_line(int d, int z, int y, int x, int& n, in
 // cancels in the difference, so FP32 only ever carries the increments, whose
 // rounding (relative 6e-8 of the update) is far below the stop test's scale.
 // The stop test and the outputs are as in the FP64 form.
-template <int DIM, int N, class PDE, bool TEMPS, int MINB, bool MIXED = false>
-__global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED>::THREADS, MINB)
+template <int DIM, int N, class PDE, bool TEMPS, int MINB, bool MIXED = false, int TS = 1>
+__global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREADS, MINB)
     predictor_lines_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                            double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
                            Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp,
                            const int* __restrict__ count) {
-  using C = LinesCfg<DIM, N, PDE, MINB, MIXED>;
+  using C = LinesCfg<DIM, N, PDE, MINB, MIXED, TS>;
+  static_assert(!MIXED || TS == 1, "the mixed form works one slice at a time");
   constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, SLAB = C::SLAB, QS = C::QS;
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
@@ -173,10 +177,11 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED>::THREADS, M
 #pragma unroll
       for (int v = 0; v < nV; v++) qn[l][v] = 0.0;
 
-    for (int t = 0; t < b; t++) {
-      __syncthreads();  // phase C of the previous slice is done with sF
-      // A: fluxes of slice t, line-major
+    for (int t0 = 0; t0 < b; t0 += TS) {
+      __syncthreads();  // phase C of the previous slices is done with sF
+      // A: fluxes of slices t0 .. t0+TS-1, line-major, slice j in buffer j
       if (!done && low) {  // flux increments in FP64, stored as FP32
+        const int t = t0;
         double Q[nD], Qp[nD];
 #pragma unroll
         for (int v = 0; v < nD; v++) Q[v] = Qp[v] = sQ[p * QS + t * nD + v];
@@ -191,15 +196,21 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED>::THREADS, M
           for (int v = 0; v < nV; v++)
             sF32[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = (float)(Fl[d][v] - Fp[d][v]);
       } else if (!done) {
-        double Q[nD];
 #pragma unroll
-        for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
-        double Fl[DIM][nV];
-        PDE::template flux<DIM>(Q, Fl);
+        for (int j = 0; j < TS; j++) {
+          const int t = t0 + j;
+          if (t < b) {
+            double Q[nD];
 #pragma unroll
-        for (int d = 0; d < DIM; d++)
+            for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
+            double Fl[DIM][nV];
+            PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
-          for (int v = 0; v < nV; v++) sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = Fl[d][v];
+            for (int d = 0; d < DIM; d++)
+#pragma unroll
+              for (int v = 0; v < nV; v++) sF[j * C::SFJ + (d * b + nd[d]) * SLAB + Ld[d] * nV + v] = Fl[d][v];
+          }
+        }
       }
       __syncthreads();
       // B: line contractions, in place
@@ -207,6 +218,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED>::THREADS, M
       for (int k = 0; k < C::IPT; k++) {
         if (it_off[k] < 0 || s_done[it_cell[k]]) continue;
         if (low) {
+          const int t = t0;
           float* base = sFall32 + it_off[k] + it_cell[k] * C::SF;
           float f[b];
 #pragma unroll
@@ -221,22 +233,28 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED>::THREADS, M
           }
           continue;
         }
-        double* base = sFall + it_off[k];
-        double f[b];
 #pragma unroll
-        for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
-        const double us = T.w[t] * it_us[k];
+        for (int j = 0; j < TS; j++) {
+          const int t = t0 + j;
+          if (t >= b) break;
+          double* base = sFall + it_off[k] + j * C::SFJ;
+          double f[b];
 #pragma unroll
-        for (int l = 0; l < b; l++) {
-          double s = 0.0;
+          for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
+          const double us = T.w[t] * it_us[k];
 #pragma unroll
-          for (int n = 0; n < b; n++) s = fma(f[n], T.Kxi[n * b + l], s);
-          base[l * SLAB] = us * s;
+          for (int l = 0; l < b; l++) {
+            double s = 0.0;
+#pragma unroll
+            for (int n = 0; n < b; n++) s = fma(f[n], T.Kxi[n * b + l], s);
+            base[l * SLAB] = us * s;
+          }
         }
       }
       __syncthreads();
       // C: rhs at this node, folded into the Picard accumulators
       if (!done && low) {  // increment: the rhs0 term cancels
+        const int t = t0;
 #pragma unroll
         for (int v = 0; v < nV; v++) {
           double rhs = 0.0;
@@ -247,15 +265,21 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED>::THREADS, M
           for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
         }
       } else if (!done) {
-        const double r0 = wpt * T.FL[t];
 #pragma unroll
-        for (int v = 0; v < nV; v++) {
-          double rhs = r0 * lu[v];
+        for (int j = 0; j < TS; j++) {
+          const int t = t0 + j;
+          if (t < b) {
+            const double r0 = wpt * T.FL[t];
 #pragma unroll
-          for (int d = 0; d < DIM; d++) rhs -= sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
-          const double ir = iw * rhs;
+            for (int v = 0; v < nV; v++) {
+              double rhs = r0 * lu[v];
 #pragma unroll
-          for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
+              for (int d = 0; d < DIM; d++) rhs -= sF[j * C::SFJ + (d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+              const double ir = iw * rhs;
+#pragma unroll
+              for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
+            }
+          }
         }
       }
     }
