@@ -923,8 +923,8 @@ struct LimLaunch {
     if (done) return EXA_OK;
     EXA_CUDA(cudaFuncSetAttribute(lim_muscl_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)MC::SMEM));
-    EXA_CUDA(cudaFuncSetAttribute(lim_post_update_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)PC::SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_post_update_kernel<DIM, N, PDE, typename PC::Group>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PC::POST_SMEM));
     EXA_CUDA(cudaFuncSetAttribute(lim_init_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)PC::SMEM));
     EXA_CUDA(cudaFuncSetAttribute(lim_seed_kernel<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1095,7 +1095,8 @@ struct LimLaunch {
       return rc;
     if ((rc = select(lm, lm->A, INT_MAX, lm->listF, lm->flags + 2, nullptr))) return rc;
     if ((rc = muscl(lm, nullptr))) return rc;
-    lim_post_update_kernel<DIM, N, PDE><<<n, PC::THREADS, PC::SMEM, st>>>(
+    lim_post_update_kernel<DIM, N, PDE, typename PC::Group>
+        <<<(n + PC::CELLS - 1) / PC::CELLS, PC::THREADS, PC::POST_SMEM, st>>>(
         n, m->luh, lm->s, lm->s_prev, lm->cure, lm->fs, lm->has_lim, lm->minB, lm->maxB, lm->lim, lm->lim_prev,
         m->geo, prm, m->scal + 1, lm->flags);
     EXA_LAUNCHED();

@@ -12,6 +12,8 @@
 // Per-cell status data: s (limiter status), s_prev, cure counter, facewise
 // statuses fs[2d], has_lim (patch allocated), DMP blocks minB/maxB[2d][nV].
 #pragma once
+#include <type_traits>
+
 #include "aderdg.cuh"
 
 namespace exa {
@@ -43,24 +45,40 @@ __device__ __forceinline__ int lim_index(int z, int y, int x) {
 }
 
 // ---------------------------------------------------------------------------
-// Separable tensor-product maps for one cell, executed by a whole block.
+// The threads that process one cell: a whole block, or one warp of a block
+// that holds several cells (small 2D cells, where block-wide barriers would
+// dominate the little work per cell).
+struct BlockGroup {
+  __device__ static int tid() { return threadIdx.x; }
+  __device__ static int size() { return blockDim.x; }
+  __device__ static int index() { return 0; }
+  __device__ static void sync() { __syncthreads(); }
+};
+struct WarpGroup {
+  __device__ static int tid() { return threadIdx.x & 31; }
+  __device__ static int size() { return 32; }
+  __device__ static int index() { return threadIdx.x >> 5; }
+  __device__ static void sync() { __syncwarp(); }
+};
+
+// Separable tensor-product maps for one cell, executed by one thread group.
 // out[o1..][v] = sum_in src[in..][v] prod_d M[in_d][o_d], M row-major [IN][OUT].
 // Summation is per axis (x, then y, then z) rather than the reference's single
 // triple loop; the difference is at round-off level.
-template <int DIM, int IN, int OUT, class Src, class Dst>
+template <int DIM, int IN, int OUT, class G = BlockGroup, class Src, class Dst>
 __device__ void tensor_map(Src src, Dst dst, const double* M, double* tmp) {
   constexpr int nV = 5;
   if (DIM == 2) {
     // t[y][xo][v] = sum_x src(y,x,v) M[x][xo]
-    for (int i = threadIdx.x; i < IN * OUT * nV; i += blockDim.x) {
+    for (int i = G::tid(); i < IN * OUT * nV; i += G::size()) {
       const int v = i % nV, xo = (i / nV) % OUT, y = i / (nV * OUT);
       double s = 0.0;
 #pragma unroll
       for (int x = 0; x < IN; x++) s += src(0, y, x, v) * M[x * OUT + xo];
       tmp[i] = s;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < OUT * OUT * nV; i += blockDim.x) {
+    G::sync();
+    for (int i = G::tid(); i < OUT * OUT * nV; i += G::size()) {
       const int v = i % nV, xo = (i / nV) % OUT, yo = i / (nV * OUT);
       double s = 0.0;
 #pragma unroll
@@ -70,23 +88,23 @@ __device__ void tensor_map(Src src, Dst dst, const double* M, double* tmp) {
   } else {
     double* t1 = tmp;                      // [z][y][xo]
     double* t2 = tmp + IN * IN * OUT * nV;  // [z][yo][xo]
-    for (int i = threadIdx.x; i < IN * IN * OUT * nV; i += blockDim.x) {
+    for (int i = G::tid(); i < IN * IN * OUT * nV; i += G::size()) {
       const int v = i % nV, xo = (i / nV) % OUT, y = (i / (nV * OUT)) % IN, z = i / (nV * OUT * IN);
       double s = 0.0;
 #pragma unroll
       for (int x = 0; x < IN; x++) s += src(z, y, x, v) * M[x * OUT + xo];
       t1[i] = s;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < IN * OUT * OUT * nV; i += blockDim.x) {
+    G::sync();
+    for (int i = G::tid(); i < IN * OUT * OUT * nV; i += G::size()) {
       const int v = i % nV, xo = (i / nV) % OUT, yo = (i / (nV * OUT)) % OUT, z = i / (nV * OUT * OUT);
       double s = 0.0;
 #pragma unroll
       for (int y = 0; y < IN; y++) s += t1[((z * IN + y) * OUT + xo) * nV + v] * M[y * OUT + yo];
       t2[i] = s;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < OUT * OUT * OUT * nV; i += blockDim.x) {
+    G::sync();
+    for (int i = G::tid(); i < OUT * OUT * OUT * nV; i += G::size()) {
       const int v = i % nV, xo = (i / nV) % OUT, yo = (i / (nV * OUT)) % OUT, zo = i / (nV * OUT * OUT);
       double s = 0.0;
 #pragma unroll
@@ -94,7 +112,7 @@ __device__ void tensor_map(Src src, Dst dst, const double* M, double* tmp) {
       dst(zo, yo, xo, v, s);
     }
   }
-  __syncthreads();
+  G::sync();
 }
 
 template <int DIM, int IN, int OUT>
@@ -103,19 +121,19 @@ constexpr int tensor_tmp() {
 }
 
 // projectOnFVLimiterSpace (Limiter.cpp:23-66): DG nodes -> interior subcells
-template <int DIM, int N>
-__device__ void project_fv_block(const double* luh, double* lim, double* tmp) {
+template <int DIM, int N, class G = BlockGroup>
+__device__ void project_fv_block(const double* luh, double* lim, double* tmp, const double* uh2lim = nullptr) {
   using L = LimShape<DIM, N>;
-  tensor_map<DIM, L::b, L::B>(
+  tensor_map<DIM, L::b, L::B, G>(
       [&](int z, int y, int x, int v) { return luh[(((DIM == 3 ? z * L::b : 0) + y) * L::b + x) * L::nV + v]; },
       [&](int z, int y, int x, int v, double s) { lim[lim_index<DIM, N>(z, y, x) * L::nV + v] = s; },
-      g_lim_tab[N].uh2lim, tmp);
+      uh2lim ? uh2lim : g_lim_tab[N].uh2lim, tmp);
 }
 // projectOnDGSpace (Limiter.cpp:69-112): interior subcells -> DG nodes
-template <int DIM, int N>
+template <int DIM, int N, class G = BlockGroup>
 __device__ void project_dg_block(const double* lim, double* luh, double* tmp) {
   using L = LimShape<DIM, N>;
-  tensor_map<DIM, L::B, L::b>(
+  tensor_map<DIM, L::B, L::b, G>(
       [&](int z, int y, int x, int v) { return lim[lim_index<DIM, N>(z, y, x) * L::nV + v]; },
       [&](int z, int y, int x, int v, double s) { luh[(((DIM == 3 ? z * L::b : 0) + y) * L::b + x) * L::nV + v] = s; },
       g_lim_tab[N].lim2uh, tmp);
@@ -165,6 +183,28 @@ __device__ __forceinline__ void block_minmax5(double* mn, double* mx, double* re
   }
   __syncthreads();
 }
+
+// the same for one warp: shuffles only, every lane ends with the result
+__device__ __forceinline__ void warp_minmax5(double* mn, double* mx) {
+#pragma unroll
+  for (int v = 0; v < 5; v++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double a = __shfl_xor_sync(0xffffffffu, mn[v], o);
+      const double c = __shfl_xor_sync(0xffffffffu, mx[v], o);
+      mn[v] = (a < mn[v]) ? a : mn[v];
+      mx[v] = (mx[v] < c) ? c : mx[v];
+    }
+}
+
+template <class G>
+struct GroupReduce {  // a whole block: through shared memory
+  __device__ static void minmax5(double* mn, double* mx, double* red) { block_minmax5(mn, mx, red); }
+};
+template <>
+struct GroupReduce<WarpGroup> {  // one warp: shuffles
+  __device__ static void minmax5(double* mn, double* mx, double*) { warp_minmax5(mn, mx); }
+};
 
 // ---------------------------------------------------------------------------
 // Face merge (mergeSolutionMinMaxOnFace :1654-1690, mergeNeighboursLimiterStatus
@@ -454,6 +494,15 @@ struct PostCfg {
                                  ? tensor_tmp<DIM, L::b, L::B>() : tensor_tmp<DIM, L::b, L::b>();
   static constexpr int THREADS = 128;
   static constexpr size_t SMEM = sizeof(double) * (TMP + 320);
+  // the post-update kernel of 2D meshes runs one warp per cell, 4 per block
+  static constexpr bool kWarp = DIM == 2;
+  using Group = typename std::conditional<kWarp, WarpGroup, BlockGroup>::type;
+  static constexpr int CELLS = kWarp ? THREADS / 32 : 1;
+  // per cell: tensor-map scratch, reduction slots, the staged DG solution and
+  // the two projection tables
+  static constexpr int STAGE = L::P * L::nV + L::b * L::b + L::b * L::B;
+  static constexpr int PER = TMP + 320 + STAGE;
+  static constexpr size_t POST_SMEM = sizeof(double) * CELLS * PER;
 };
 
 // Min/max of the observables (the conserved variables) over the
@@ -461,8 +510,9 @@ struct PostCfg {
 // cell (findCellLocalMinAndMax + compareWithADERDGSolutionAtGaussLobattoNodes +
 // compareWithADERDGSolutionAtFVSubcellCenters, Limiter.cpp:210-368). Block-wide;
 // every thread ends with the cell's values in mn/mx.
-template <int DIM, int N>
-__device__ void local_minmax_block(const double* u, double* mn, double* mx, double* tmp, double* red) {
+template <int DIM, int N, class G = BlockGroup>
+__device__ void local_minmax_block(const double* u, double* mn, double* mx, double* tmp, double* red,
+                                   const double* uh2lob, const double* uh2lim) {
   using L = LimShape<DIM, N>;
   constexpr int nV = L::nV;
 #pragma unroll
@@ -470,20 +520,29 @@ __device__ void local_minmax_block(const double* u, double* mn, double* mx, doub
     mn[v] = __longlong_as_double(0x7fefffffffffffffll);
     mx[v] = -mn[v];
   }
-  for (int i = threadIdx.x; i < L::P * nV; i += blockDim.x) {
-    const int v = i % nV;
-    mn[v] = (u[i] < mn[v]) ? u[i] : mn[v];
-    mx[v] = (mx[v] < u[i]) ? u[i] : mx[v];
+  for (int p = G::tid(); p < L::P; p += G::size()) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const double q = u[p * nV + v];
+      mn[v] = (q < mn[v]) ? q : mn[v];
+      mx[v] = (mx[v] < q) ? q : mx[v];
+    }
   }
-  // the projected values are folded into the running min/max as they are produced
+  // the projected values are folded into the running min/max as they are
+  // produced; the variable is selected with compile-time indices so that
+  // mn/mx stay in registers
   auto fold = [&](int, int, int, int v, double val) {
-    mn[v] = (val < mn[v]) ? val : mn[v];
-    mx[v] = (mx[v] < val) ? val : mx[v];
+#pragma unroll
+    for (int w = 0; w < 5; w++)
+      if (w == v) {
+        mn[w] = (val < mn[w]) ? val : mn[w];
+        mx[w] = (mx[w] < val) ? val : mx[w];
+      }
   };
   auto src = [&](int z, int y, int x, int v) { return u[(((DIM == 3 ? z * L::b : 0) + y) * L::b + x) * nV + v]; };
-  tensor_map<DIM, L::b, L::b>(src, fold, g_lim_tab[N].uh2lob, tmp);
-  tensor_map<DIM, L::b, L::B>(src, fold, g_lim_tab[N].uh2lim, tmp);
-  block_minmax5(mn, mx, red);
+  tensor_map<DIM, L::b, L::b, G>(src, fold, uh2lob, tmp);
+  tensor_map<DIM, L::b, L::B, G>(src, fold, uh2lim, tmp);
+  GroupReduce<G>::minmax5(mn, mx, red);
 }
 
 // Initial limiter status (updateLimiterStatusAndMinAndMaxAfterSetInitialConditions,
@@ -503,7 +562,8 @@ __global__ void __launch_bounds__(128) lim_init_kernel(int ncells, const double*
   const int cell = blockIdx.x;
   if (cell >= ncells) return;
   double mn[5], mx[5];
-  local_minmax_block<DIM, N>(luh + (size_t)cell * L::P * L::nV, mn, mx, smem, smem + C::TMP);
+  local_minmax_block<DIM, N>(luh + (size_t)cell * L::P * L::nV, mn, mx, smem, smem + C::TMP, g_lim_tab[N].uh2lob,
+                             g_lim_tab[N].uh2lim);
   if (threadIdx.x == 0) {
     double* mnB = minB + (size_t)cell * D2 * 5;
     double* mxB = maxB + (size_t)cell * D2 * 5;
@@ -556,7 +616,9 @@ __global__ void __launch_bounds__(128) lim_seed_kernel(int ncells, const int* __
 //   - DMP over GL, Gauss-Lobatto and subcell values, admissibility, the
 //     FV-subcell min/max for FV-active cells, the status machine
 //   - an irregular change (a cell with s <= A became troubled) sets *irregular.
-template <int DIM, int N, class PDE>
+// G: one block per cell (BlockGroup) or one warp per cell, 4 cells per block
+// (WarpGroup; 2D).
+template <int DIM, int N, class PDE, class G = BlockGroup>
 __global__ void __launch_bounds__(128) lim_post_update_kernel(
     int ncells, double* __restrict__ luh, int* __restrict__ s, int* __restrict__ s_prev, int* __restrict__ cure,
     int* __restrict__ fs, int* __restrict__ has_lim, double* __restrict__ minB, double* __restrict__ maxB,
@@ -566,41 +628,49 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
   using C = PostCfg<DIM, N>;
   constexpr int nV = L::nV, D2 = 2 * DIM;
   extern __shared__ double smem[];
-  double* tmp = smem;
-  double* red = smem + C::TMP;
-  __shared__ int s_flags[4];
-  const int cell = blockIdx.x;
+  double* tmp = smem + G::index() * C::PER;
+  double* red = tmp + C::TMP;
+  double* su = red + 320;                  // the cell's DG solution after the update
+  double* slob = su + L::P * L::nV;        // uh2lob
+  double* slim = slob + L::b * L::b;       // uh2lim
+  __shared__ int s_flags_all[4][4];
+  int* s_flags = s_flags_all[G::index()];
+  const int cell = blockIdx.x * (blockDim.x / G::size()) + G::index();
   if (cell >= ncells) return;
   const int st = s[cell];  // status before the update
   double* u = luh + (size_t)cell * L::P * nV;
   double* l = lim + (size_t)cell * L::LS;
   double* lp = lim_prev + (size_t)cell * L::LS;
-  if (threadIdx.x == 0) {
+  if (G::tid() == 0) {
     s_prev[cell] = st;
     s_flags[0] = has_lim[cell];
   }
-  __syncthreads();
+  G::sync();
   if (st > 0 && st < prm.A) {
     if (!s_flags[0])
-      for (int i = threadIdx.x; i < L::LS; i += blockDim.x) l[i] = lp[i] = 0.0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < L::LS; i += blockDim.x) {
+      for (int i = G::tid(); i < L::LS; i += G::size()) l[i] = lp[i] = 0.0;
+    G::sync();
+    for (int i = G::tid(); i < L::LS; i += G::size()) {
       const double a = l[i];
       l[i] = lp[i];
       lp[i] = a;
     }
-    __syncthreads();
-    project_fv_block<DIM, N>(u, l, tmp);
-    if (threadIdx.x == 0) has_lim[cell] = 1;
+    G::sync();
+    project_fv_block<DIM, N, G>(u, l, tmp, g_lim_tab[N].uh2lim);
+    if (G::tid() == 0) has_lim[cell] = 1;
   }
-  if (st == 0 && threadIdx.x == 0) has_lim[cell] = 0;  // ensureNoUnrequiredLimiterPatchIsAllocatedOnComputeCell
+  if (st == 0 && G::tid() == 0) has_lim[cell] = 0;  // ensureNoUnrequiredLimiterPatchIsAllocatedOnComputeCell
   // admissible step of the new solution
   const double invDx0 = __ddiv_rn(1.0, geo.dx[0]), invDx1 = __ddiv_rn(1.0, geo.dx[1]);
   const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, geo.dx[2]) : 0.0;
-  __syncthreads();  // projections above wrote u's patch; u itself is final
+  // stage the (final) DG solution and the projection tables of this order
+  for (int i = G::tid(); i < L::P * nV; i += G::size()) su[i] = u[i];
+  for (int i = G::tid(); i < L::b * L::b; i += G::size()) slob[i] = g_lim_tab[N].uh2lob[i];
+  for (int i = G::tid(); i < L::b * L::B; i += G::size()) slim[i] = g_lim_tab[N].uh2lim[i];
+  G::sync();
   double dtm = __longlong_as_double(0x7fefffffffffffffll);
-  for (int p = threadIdx.x; p < L::P; p += blockDim.x) {
-    const double* q = u + p * nV;
+  for (int p = G::tid(); p < L::P; p += G::size()) {
+    const double* q = su + p * nV;
     double den = 0.0;
     den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 0), invDx0));
     den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 1), invDx1));
@@ -618,7 +688,7 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
     if ((threadIdx.x & 31) == 0) atomic_min_pos_double(dt_min, m);
   }
   double mn[5], mx[5];
-  local_minmax_block<DIM, N>(u, mn, mx, tmp, red);
+  local_minmax_block<DIM, N, G>(su, mn, mx, tmp, red, slob, slim);
   // FV-subcell min/max of FV-active cells (findCellLocalLimiterMinAndMax, :167-205)
   double fmn[5], fmx[5];
   if (st >= prm.A) {
@@ -627,7 +697,7 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
       fmn[v] = __longlong_as_double(0x7fefffffffffffffll);
       fmx[v] = -fmn[v];
     }
-    for (int i = threadIdx.x; i < L::PB; i += blockDim.x) {
+    for (int i = G::tid(); i < L::PB; i += G::size()) {
       const int x = i % L::B, y = (i / L::B) % L::B, z = DIM == 3 ? i / (L::B * L::B) : 0;
       const double* q = l + lim_index<DIM, N>(z, y, x) * nV;
 #pragma unroll
@@ -636,9 +706,9 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
         fmx[v] = (fmx[v] < q[v]) ? q[v] : fmx[v];
       }
     }
-    block_minmax5(fmn, fmx, red);
+    GroupReduce<G>::minmax5(fmn, fmx, red);
   }
-  if (threadIdx.x == 0) {
+  if (G::tid() == 0) {
     double* mnB = minB + (size_t)cell * D2 * 5;
     double* mxB = maxB + (size_t)cell * D2 * 5;
     // discreteMaximumPrincipleAndMinAndMaxSearch (Limiter.cpp:114-165)
@@ -685,11 +755,11 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
     s_flags[2] = (ns > 0 && !had);
     if (s_flags[2]) has_lim[cell] = 1;
   }
-  __syncthreads();
+  G::sync();
   if (s_flags[2]) {  // newly allocated patch: zeroed; projection for helper cells
-    for (int i = threadIdx.x; i < L::LS; i += blockDim.x) l[i] = lp[i] = 0.0;
-    __syncthreads();
-    if (s_flags[1] < prm.A) project_fv_block<DIM, N>(u, l, tmp);
+    for (int i = G::tid(); i < L::LS; i += G::size()) l[i] = lp[i] = 0.0;
+    G::sync();
+    if (s_flags[1] < prm.A) project_fv_block<DIM, N, G>(su, l, tmp, slim);
   }
 }
 
