@@ -386,7 +386,8 @@ def run_limiter_workload(a, world, dev, rank):
     out = {"workload": LIM_WORKLOAD, "value": dof_step * n * world / (ms / 1e3), "unit": "DoF-updates/s",
            "steps": n, "ms_per_step": ms / max(n, 1), "t_end": st["t"], "irregular_steps": st["irregular_steps"],
            "picard_sweeps": st["picard_sweeps"], "final_status_counts": np.bincount(status, minlength=4).tolist(),
-           "timing": "exa_lmesh_run_until(0.2) incl. its per-step host check of t and dt, CUDA events"}
+           "timing": "exa_lmesh_run_until(0.2): the step captured once as a CUDA graph (capture inside the "
+                     "timed region), replayed 16 steps per host check of t, CUDA events"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         sys.path.insert(0, os.path.join(REPO, "oracle"))
         import pyoracle

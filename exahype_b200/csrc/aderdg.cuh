@@ -431,11 +431,13 @@ template <int DIM, int N, class PDE>
 __global__ void __launch_bounds__(128) riemann_kernel(const double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                                                       const int* __restrict__ face_left,
                                                       const int* __restrict__ face_right,
-                                                      const int* __restrict__ face_dir, int nfaces) {
+                                                      const int* __restrict__ face_dir, int nfaces,
+                                                      const int* __restrict__ gate = nullptr) {
   using S = Shape<DIM, N, PDE>;
   constexpr int F = S::F, nV = S::nV, nD = S::nD;
   const int lane = threadIdx.x & 31;
   const int f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (gate && !*gate) return;  // gate (optional, device): 0 skips the launch's work
   if (f >= nfaces) return;
   const int cl = face_left[f], cr = face_right[f], dir = face_dir[f];
   const double* QL = lQhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nD;
@@ -461,12 +463,12 @@ __global__ void __launch_bounds__(128) riemann_kernel(const double* __restrict__
 template <int DIM, int N, class PDE>
 __global__ void __launch_bounds__(128) boundary_kernel(const double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                                                        const int* __restrict__ bcell, const int* __restrict__ bface,
-                                                       int nb, int kind) {
+                                                       int nb, int kind, const int* __restrict__ gate = nullptr) {
   using S = Shape<DIM, N, PDE>;
   constexpr int F = S::F, nV = S::nV, nD = S::nD;
   const int lane = threadIdx.x & 31;
   const int f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (f >= nb) return;
+  if (f >= nb || (gate && !*gate)) return;
   const int c = bcell[f], face = bface[f], dir = face >> 1;
   const double* QIn = lQhbnd + ((size_t)c * 2 * DIM + face) * F * nD;
   double* FIn = lFhbnd + ((size_t)c * 2 * DIM + face) * F * nV;

@@ -344,9 +344,10 @@ static int batch_launch_step(exa_batch* b) {
   int rc;
   for (BatchGroup& g : b->groups) {
     if (g.ncells == 0) continue;
-    if ((rc = g.k.riemann(g.lQhbnd, g.lFhbnd, g.fl, g.fr, g.fd, g.nfaces, st))) return rc;
+    if ((rc = g.k.riemann(g.lQhbnd, g.lFhbnd, g.fl, g.fr, g.fd, g.nfaces, nullptr, st))) return rc;
     for (int kd = 0; kd < 2; kd++)
-      if ((rc = g.k.boundary(g.lQhbnd, g.lFhbnd, g.bcell + g.boff[kd], g.bface + g.boff[kd], g.nb[kd], kd, st)))
+      if ((rc = g.k.boundary(g.lQhbnd, g.lFhbnd, g.bcell + g.boff[kd], g.bface + g.boff[kd], g.nb[kd], kd, nullptr,
+                             st)))
         return rc;
     Geometry geo{};
     geo.inst = g.cell_inst;

@@ -122,8 +122,9 @@ struct KernelSet {
   // count (optional, device) caps the list length at launch time
   int (*predictor)(const double*, double*, double*, double*, int*, const double*, Geometry, int, const int*,
                    const int*, PredictorTemps, bool, unsigned long long*, int, cudaStream_t);
-  int (*riemann)(const double*, double*, const int*, const int*, const int*, int, cudaStream_t);
-  int (*boundary)(const double*, double*, const int*, const int*, int, int, cudaStream_t);
+  // the last pointer before the stream: optional device gate (0 skips the work)
+  int (*riemann)(const double*, double*, const int*, const int*, const int*, int, const int*, cudaStream_t);
+  int (*boundary)(const double*, double*, const int*, const int*, int, int, const int*, cudaStream_t);
   int (*corrector)(double*, const double*, const double*, const double*, double*, Geometry, int, const int*, int,
                    const int*, cudaStream_t);
 };
@@ -224,15 +225,17 @@ struct Launch {
     }
     return EXA_OK;
   }
-  static int riemann(const double* qb, double* fb, const int* l, const int* r, const int* d, int n, cudaStream_t st) {
+  static int riemann(const double* qb, double* fb, const int* l, const int* r, const int* d, int n, const int* gate,
+                     cudaStream_t st) {
     if (n <= 0) return EXA_OK;
-    riemann_kernel<DIM, N, PDE><<<(n + 3) / 4, 128, 0, st>>>(qb, fb, l, r, d, n);
+    riemann_kernel<DIM, N, PDE><<<(n + 3) / 4, 128, 0, st>>>(qb, fb, l, r, d, n, gate);
     EXA_LAUNCHED();
     return EXA_OK;
   }
-  static int boundary(const double* qb, double* fb, const int* c, const int* f, int n, int kind, cudaStream_t st) {
+  static int boundary(const double* qb, double* fb, const int* c, const int* f, int n, int kind, const int* gate,
+                      cudaStream_t st) {
     if (n <= 0) return EXA_OK;
-    boundary_kernel<DIM, N, PDE><<<(n + 3) / 4, 128, 0, st>>>(qb, fb, c, f, n, kind);
+    boundary_kernel<DIM, N, PDE><<<(n + 3) / 4, 128, 0, st>>>(qb, fb, c, f, n, kind, gate);
     EXA_LAUNCHED();
     return EXA_OK;
   }
@@ -415,7 +418,7 @@ int exa_riemann_solver_nonlinear(const exa_solver* s, const double* lQhbnd, doub
                                  const int* face_right, const int* face_dir, int nfaces, void* stream) {
   if (!s || !lQhbnd || !lFhbnd || nfaces < 0 || (nfaces > 0 && (!face_left || !face_right || !face_dir)))
     return fail(EXA_ERR_ARG, "exa_riemann_solver_nonlinear: null argument or negative count");
-  return s->k.riemann(lQhbnd, lFhbnd, face_left, face_right, face_dir, nfaces, (cudaStream_t)stream);
+  return s->k.riemann(lQhbnd, lFhbnd, face_left, face_right, face_dir, nfaces, nullptr, (cudaStream_t)stream);
 }
 
 int exa_boundary_conditions(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* bcell,
@@ -424,7 +427,7 @@ int exa_boundary_conditions(const exa_solver* s, const double* lQhbnd, double* l
     return fail(EXA_ERR_ARG, "exa_boundary_conditions: null argument or negative count");
   if (kind != EXA_BC_OUTFLOW && kind != EXA_BC_REFLECTIVE)
     return fail(EXA_ERR_ARG, "exa_boundary_conditions: kind must be outflow or reflective");
-  return s->k.boundary(lQhbnd, lFhbnd, bcell, bface, nb, kind, (cudaStream_t)stream);
+  return s->k.boundary(lQhbnd, lFhbnd, bcell, bface, nb, kind, nullptr, (cudaStream_t)stream);
 }
 
 int exa_corrector(const exa_solver* s, double* luh, const double* lduh, const double* lFhbnd, const double* dt_dev,
@@ -702,12 +705,12 @@ static int mesh_one_step(exa_mesh* m) {
   int rc;
   {
     PhaseTimer pt(m, 1);
-    rc = k.riemann(m->lQhbnd, m->lFhbnd, m->fl, m->fr, m->fd, m->nfaces, m->stream);
+    rc = k.riemann(m->lQhbnd, m->lFhbnd, m->fl, m->fr, m->fd, m->nfaces, nullptr, m->stream);
     if (rc) return rc;
     m->phase_launches[1] += m->nfaces > 0;
     for (int kd = 0; kd < 2; kd++) {
       rc = k.boundary(m->lQhbnd, m->lFhbnd, m->bcell + m->boff[kd], m->bface + m->boff[kd], m->nbfaces[kd], kd,
-                      m->stream);
+                      nullptr, m->stream);
       if (rc) return rc;
       m->phase_launches[1] += m->nbfaces[kd] > 0;
     }
@@ -866,7 +869,8 @@ struct exa_lmesh {
   int A = 2, T = 3, cure_steps = 0;
   double relax = 1e-4, scale = 1e-3;
   // s: limiter status; flags: [0] irregular change this step, [1] DG list
-  // length, [2] FV list length, [3] predictor list length
+  // length, [2] FV list length, [3] predictor list length, [4] run flag of
+  // run_until's captured step
   int *s = nullptr, *s_prev = nullptr, *cure = nullptr, *fs = nullptr, *has_lim = nullptr, *flags = nullptr;
   int *listA = nullptr, *listF = nullptr, *listP = nullptr;
   double *minB = nullptr, *maxB = nullptr, *lim = nullptr, *lim_prev = nullptr, *luh_prev = nullptr;
@@ -875,13 +879,17 @@ struct exa_lmesh {
   size_t LS = 0, PB = 0;  // doubles per FV patch (ghosts included), subcells per cell
   int (*init)(exa_lmesh*, double) = nullptr;
   int (*step)(exa_lmesh*) = nullptr;
+  int (*chunk)(exa_lmesh*, int) = nullptr;
+  cudaGraphExec_t graph = nullptr;  // captured gated step of run_until
+  int graph_variant = -1;
   bool initialised = false;
 };
 
 namespace exa {
 
 // scal: [0] dt, [1] min target after the update, [2] t, [3] steps,
-//       [4] min target after a local recomputation, [5] irregular steps
+//       [4] min target after a local recomputation, [5] irregular steps,
+//       [6] end time of run_until
 __global__ void lim_scalars_kernel(double* scal, double t0) {
   scal[0] = 0.0;
   scal[1] = __longlong_as_double(0x7fefffffffffffffll);
@@ -896,7 +904,8 @@ __global__ void lim_scalars_kernel(double* scal, double t0) {
 // (mappings/LocalRecomputation.cpp:193-207 after SolutionUpdate.cpp:308-322),
 // so the time stamp also advances by the step found after the update, and the
 // next step uses the one found after the recomputation.
-__global__ void lim_advance_kernel(double* scal, const int* flags) {
+__global__ void lim_advance_kernel(double* scal, const int* flags, const int* run) {
+  if (run && !*run) return;
   const bool irr = flags[0] != 0;
   scal[2] += scal[0];
   if (irr) scal[2] += scal[1];
@@ -906,6 +915,9 @@ __global__ void lim_advance_kernel(double* scal, const int* flags) {
   scal[3] += 1.0;
   if (irr) scal[5] += 1.0;
 }
+
+// run flag of the next step of run_until: t < t_end (scal[6]) and dt > 0
+__global__ void lim_run_gate_kernel(const double* scal, int* run) { *run = scal[2] < scal[6] && scal[0] > 0.0; }
 
 template <int DIM, int N>
 struct LimLaunch {
@@ -1038,9 +1050,9 @@ struct LimLaunch {
     EXA_LAUNCHED();
     return EXA_OK;
   }
-  static int predict(exa_lmesh* lm) {  // cells with status < T (mappings/Prediction.cpp:176-178)
+  static int predict(exa_lmesh* lm, const int* run = nullptr) {  // status < T (mappings/Prediction.cpp:176-178)
     exa_mesh* m = lm->m;
-    int rc = select(lm, INT_MIN, lm->T, lm->listP, lm->flags + 3, nullptr);
+    int rc = select(lm, INT_MIN, lm->T, lm->listP, lm->flags + 3, run);
     if (rc) return rc;
     return m->s->k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->scal + 0, m->geo, m->ncells,
                              lm->listP, lm->flags + 3, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
@@ -1069,7 +1081,9 @@ struct LimLaunch {
     return predict(lm);
   }
 
-  static int step(exa_lmesh* lm) {
+  // One limiting step. run (optional, device): when it holds 0 every launch
+  // of the step returns at once (run_until replays captured steps past t_end).
+  static int step_launch(exa_lmesh* lm, const int* run) {
     exa_mesh* m = lm->m;
     const KernelSet& k = m->s->k;
     const int n = m->ncells;
@@ -1080,28 +1094,30 @@ struct LimLaunch {
     // merge: DMP min/max and facewise statuses; DG Riemann problems (the
     // fluxes of faces between two FV-active cells are computed but never
     // read); FV halo exchange and FV boundary on FV-active faces
-    if ((rc = merge(lm, 1, nullptr))) return rc;
-    if ((rc = k.riemann(m->lQhbnd, m->lFhbnd, m->fl, m->fr, m->fd, m->nfaces, st))) return rc;
+    if ((rc = merge(lm, 1, run))) return rc;
+    if ((rc = k.riemann(m->lQhbnd, m->lFhbnd, m->fl, m->fr, m->fd, m->nfaces, run, st))) return rc;
     if ((rc = k.boundary(m->lQhbnd, m->lFhbnd, m->bcell + m->boff[EXA_BC_OUTFLOW], m->bface + m->boff[EXA_BC_OUTFLOW],
-                         m->nbfaces[EXA_BC_OUTFLOW], EXA_BC_OUTFLOW, st)))
+                         m->nbfaces[EXA_BC_OUTFLOW], EXA_BC_OUTFLOW, run, st)))
       return rc;
-    if ((rc = halo(lm, nullptr))) return rc;
-    // update: DG cells (s < A) by the corrector, FV-active cells by MUSCL-Hancock
+    if ((rc = halo(lm, run))) return rc;
+    // update: DG cells (s < A) by the corrector, FV-active cells by
+    // MUSCL-Hancock (lists come out empty when run holds 0)
     EXA_CUDA(cudaMemcpyAsync(lm->luh_prev, m->luh, (size_t)n * L::P * L::nV * sizeof(double),
                              cudaMemcpyDeviceToDevice, st));
-    if ((rc = select(lm, INT_MIN, lm->A, lm->listA, lm->flags + 1, nullptr))) return rc;
+    if ((rc = select(lm, INT_MIN, lm->A, lm->listA, lm->flags + 1, run))) return rc;
     if ((rc = k.corrector(m->luh, m->lduh, m->lFhbnd, m->scal + 0, nullptr, m->geo, n, lm->listA, 1, lm->flags + 1,
                           st)))
       return rc;
-    if ((rc = select(lm, lm->A, INT_MAX, lm->listF, lm->flags + 2, nullptr))) return rc;
-    if ((rc = muscl(lm, nullptr))) return rc;
+    if ((rc = select(lm, lm->A, INT_MAX, lm->listF, lm->flags + 2, run))) return rc;
+    if ((rc = muscl(lm, run))) return rc;
     lim_post_update_kernel<DIM, N, PDE, typename PC::Group>
         <<<(n + PC::CELLS - 1) / PC::CELLS, PC::THREADS, PC::POST_SMEM, st>>>(
         n, m->luh, lm->s, lm->s_prev, lm->cure, lm->fs, lm->has_lim, lm->minB, lm->maxB, lm->lim, lm->lim_prev,
-        m->geo, prm, m->scal + 1, lm->flags);
+        m->geo, prm, m->scal + 1, lm->flags, run);
     EXA_LAUNCHED();
     // irregular limiter domain change: every launch below returns at once
-    // unless the post-update kernel raised flags[0]
+    // unless the post-update kernel raised flags[0] (it never does on a step
+    // that run skips)
     const int* g = lm->flags;
     if ((rc = spread(lm, g))) return rc;
     lim_reinit_kernel<DIM, N><<<n, 128, PROJ_SMEM, st>>>(n, m->luh, lm->luh_prev, lm->s, lm->s_prev, lm->cure,
@@ -1113,15 +1129,50 @@ struct LimLaunch {
     lim_recompute_kernel<DIM, N, PDE><<<n, 128, PROJ_SMEM, st>>>(n, m->luh, lm->luh_prev, lm->s, lm->s_prev,
                                                                   lm->lim, lm->lim_prev, m->geo, prm, m->scal + 4, g);
     EXA_LAUNCHED();
-    lim_advance_kernel<<<1, 1, 0, st>>>(m->scal, lm->flags);
+    lim_advance_kernel<<<1, 1, 0, st>>>(m->scal, lm->flags, run);
     EXA_LAUNCHED();
-    return predict(lm);
+    return predict(lm, run);
+  }
+  static int step(exa_lmesh* lm) { return step_launch(lm, nullptr); }
+
+  // k steps of run_until: the step is captured once as a CUDA graph whose
+  // first node sets the run flag (t < t_end && dt > 0, t_end in scal[6]) and
+  // is replayed k times; replays past t_end change nothing.
+  static int chunk(exa_lmesh* lm, int k) {
+    cudaStream_t st = lm->m->stream;
+    if (!lm->graph || lm->graph_variant != lm->m->s->variant) {
+      if (lm->graph) {
+        EXA_CUDA(cudaStreamSynchronize(st));
+        cudaGraphExecDestroy(lm->graph);
+      }
+      lm->graph = nullptr;
+      cudaGraph_t g = nullptr;
+      EXA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      lim_run_gate_kernel<<<1, 1, 0, st>>>(lm->m->scal, lm->flags + 4);
+      const int rc = step_launch(lm, lm->flags + 4);
+      const cudaError_t e = cudaStreamEndCapture(st, &g);
+      if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc ? rc : fail(EXA_ERR_CUDA, std::string("exa_lmesh_run_until: capture: ") + cudaGetErrorString(e));
+      }
+      const cudaError_t e2 = cudaGraphInstantiate(&lm->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e2 != cudaSuccess) {
+        lm->graph = nullptr;
+        return fail(EXA_ERR_CUDA, std::string("exa_lmesh_run_until: instantiate: ") + cudaGetErrorString(e2));
+      }
+      lm->graph_variant = lm->m->s->variant;
+    }
+    for (int i = 0; i < k; i++) EXA_CUDA(cudaGraphLaunch(lm->graph, st));
+    return EXA_OK;
   }
 };
 
 struct LimOps {
   int (*init)(exa_lmesh*, double);
   int (*step)(exa_lmesh*);
+  int (*chunk)(exa_lmesh*, int);
   int (*grid)(int, int*);
   size_t (*scratch)();
   size_t LS, PB;
@@ -1134,7 +1185,7 @@ static bool find_lim_ops(int dim, int order, LimOps* out) {
 #define X(D, NN, PDE_, ID)                                                                              \
   if (dim == D && order == NN) {                                                                        \
     using LL = LimLaunch<D, NN>;                                                                        \
-    *out = LimOps{&LL::init, &LL::step, &LL::muscl_grid, &LL::scratch_doubles, (size_t)LimShape<D, NN>::LS, \
+    *out = LimOps{&LL::init, &LL::step, &LL::chunk, &LL::muscl_grid, &LL::scratch_doubles, (size_t)LimShape<D, NN>::LS, \
                   (size_t)LimShape<D, NN>::PB, &LL::muscl_call, &LL::scratch_bytes_for, &LL::project_call};   \
     return true;                                                                                        \
   }
@@ -1246,6 +1297,8 @@ int exa_fv_musclhancock_update_noalloc(const exa_solver* s, double* lim, double*
 
 static void lmesh_free(exa_lmesh* lm) {
   cudaStream_t st = lm->m ? lm->m->stream : nullptr;
+  if (lm->graph) cudaGraphExecDestroy(lm->graph);
+  lm->graph = nullptr;
   for (void* p : {(void*)lm->s, (void*)lm->s_prev, (void*)lm->cure, (void*)lm->fs, (void*)lm->has_lim,
                   (void*)lm->flags, (void*)lm->listA, (void*)lm->listF, (void*)lm->listP, (void*)lm->minB,
                   (void*)lm->maxB, (void*)lm->lim, (void*)lm->lim_prev, (void*)lm->luh_prev, (void*)lm->fv_ic,
@@ -1279,6 +1332,7 @@ int exa_lmesh_create(const exa_solver* s, const int* cells, const double* offset
   lm->PB = ops.PB;
   lm->init = ops.init;
   lm->step = ops.step;
+  lm->chunk = ops.chunk;
   const size_t n = lm->m->ncells, D2 = 2 * s->k.dim, P = s->k.P;
   rc = ops.grid((int)n, &lm->muscl_grid);
   if (rc) {
@@ -1288,7 +1342,7 @@ int exa_lmesh_create(const exa_solver* s, const int* cells, const double* offset
   const size_t scr = ops.scratch();
   cudaStream_t lst = lm->m->stream;
   bool ok = salloc(&lm->s, n * 4, lst) && salloc(&lm->s_prev, n * 4, lst) && salloc(&lm->cure, n * 4, lst) &&
-            salloc(&lm->fs, n * D2 * 4, lst) && salloc(&lm->has_lim, n * 4, lst) && salloc(&lm->flags, 4 * 4, lst) &&
+            salloc(&lm->fs, n * D2 * 4, lst) && salloc(&lm->has_lim, n * 4, lst) && salloc(&lm->flags, 8 * 4, lst) &&
             salloc(&lm->listA, n * 4, lst) && salloc(&lm->listF, n * 4, lst) && salloc(&lm->listP, n * 4, lst) &&
             salloc(&lm->minB, n * D2 * 5 * 8, lst) && salloc(&lm->maxB, n * D2 * 5 * 8, lst) &&
             salloc(&lm->lim, n * lm->LS * 8, lst) && salloc(&lm->lim_prev, n * lm->LS * 8, lst) &&
@@ -1305,7 +1359,7 @@ int exa_lmesh_create(const exa_solver* s, const int* cells, const double* offset
   EXA_CUDA(cudaMemsetAsync(lm->cure, 0, n * 4, st));
   EXA_CUDA(cudaMemsetAsync(lm->fs, 0, n * D2 * 4, st));
   EXA_CUDA(cudaMemsetAsync(lm->has_lim, 0, n * 4, st));
-  EXA_CUDA(cudaMemsetAsync(lm->flags, 0, 16, st));
+  EXA_CUDA(cudaMemsetAsync(lm->flags, 0, 32, st));
   EXA_CUDA(cudaMemsetAsync(lm->lim, 0, n * lm->LS * 8, st));
   EXA_CUDA(cudaMemsetAsync(lm->lim_prev, 0, n * lm->LS * 8, st));
   EXA_CUDA(cudaMemsetAsync(lm->luh_prev, 0, n * P * 5 * 8, st));
@@ -1381,15 +1435,21 @@ int exa_lmesh_state(exa_lmesh* lm, double* t, double* dt, long long* steps, long
 int exa_lmesh_run_until(exa_lmesh* lm, double t_end, int max_steps, int* steps) {
   if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_run_until: null mesh");
   if (!lm->initialised) return fail(EXA_ERR_STATE, "exa_lmesh_run_until: call exa_lmesh_init first");
+  // Steps are replayed from a captured graph in chunks of up to 16; each
+  // replay runs a step only while t < t_end and dt > 0 hold on the device, so
+  // the steps taken are the ones a step-by-step loop checking t on the host
+  // would take. The host reads the time once per chunk.
+  constexpr int kChunk = 16;
+  double t = 0.0, dt = 0.0;
+  long long s0 = 0, s1 = 0;
+  int rc = exa_lmesh_state(lm, &t, &dt, &s0, nullptr, nullptr);
+  if (rc) return rc;
+  EXA_CUDA(cudaMemcpyAsync(lm->m->scal + 6, &t_end, sizeof(double), cudaMemcpyHostToDevice, lm->m->stream));
   int n = 0;
-  while (n < max_steps) {
-    double t, dt;
-    int rc = exa_lmesh_state(lm, &t, &dt, nullptr, nullptr, nullptr);
-    if (rc) return rc;
-    if (!(t < t_end && dt > 0.0)) break;
-    rc = lm->step(lm);
-    if (rc) return rc;
-    n++;
+  while (n < max_steps && t < t_end && dt > 0.0) {
+    if ((rc = lm->chunk(lm, std::min(kChunk, max_steps - n)))) return rc;
+    if ((rc = exa_lmesh_state(lm, &t, &dt, &s1, nullptr, nullptr))) return rc;
+    n = (int)(s1 - s0);
   }
   if (steps) *steps = n;
   return EXA_OK;
@@ -1413,6 +1473,11 @@ int exa_lmesh_get_limiter(exa_lmesh* lm, double* lim, int* allocated) {
 
 int exa_lmesh_set_priority(exa_lmesh* lm, int level) {
   if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_set_priority: null mesh");
+  if (lm->graph) {  // captured on the old stream's priority
+    cudaStreamSynchronize(lm->m->stream);
+    cudaGraphExecDestroy(lm->graph);
+    lm->graph = nullptr;
+  }
   return exa_mesh_set_priority(lm->m, level);
 }
 

@@ -616,6 +616,7 @@ __global__ void __launch_bounds__(128) lim_seed_kernel(int ncells, const int* __
 //   - DMP over GL, Gauss-Lobatto and subcell values, admissibility, the
 //     FV-subcell min/max for FV-active cells, the status machine
 //   - an irregular change (a cell with s <= A became troubled) sets *irregular.
+// run (optional): the kernel does nothing when it holds 0.
 // G: one block per cell (BlockGroup) or one warp per cell, 4 cells per block
 // (WarpGroup; 2D).
 template <int DIM, int N, class PDE, class G = BlockGroup>
@@ -623,9 +624,10 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
     int ncells, double* __restrict__ luh, int* __restrict__ s, int* __restrict__ s_prev, int* __restrict__ cure,
     int* __restrict__ fs, int* __restrict__ has_lim, double* __restrict__ minB, double* __restrict__ maxB,
     double* __restrict__ lim, double* __restrict__ lim_prev, Geometry geo, LimParams prm,
-    double* __restrict__ dt_min, int* __restrict__ irregular) {
+    double* __restrict__ dt_min, int* __restrict__ irregular, const int* __restrict__ run = nullptr) {
   using L = LimShape<DIM, N>;
   using C = PostCfg<DIM, N>;
+  if (run && !*run) return;
   constexpr int nV = L::nV, D2 = 2 * DIM;
   extern __shared__ double smem[];
   double* tmp = smem + G::index() * C::PER;

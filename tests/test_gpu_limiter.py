@@ -185,3 +185,46 @@ def test_limiting_explosion_81x81_to_t02(eb):
     rho = dg[..., 0]
     p = 0.4 * (dg[..., 4] - 0.5 * np.sum(dg[..., 1:4] ** 2, axis=-1) / rho)
     assert rho.min() > 0 and p.min() > 0
+
+
+@pytest.mark.parametrize("dim,order,cells", [(2, 5, (24, 24)), (3, 3, (8, 8, 8))])
+def test_run_until_graph_matches_eager_steps(eb, dim, order, cells):
+    """run_until replays a captured, device-gated step in chunks; it takes
+    exactly the steps an eager loop with a host check of t and dt takes, with
+    bit-identical solution, statuses and FV patches, also when max_steps ends
+    a chunk early and when the predictor variant changes between calls"""
+    from exahype_b200 import problems
+    luh, fv, _ = problems.explosion(dim, order, cells, seed=3)
+    s = eb.Solver(dim, order)
+    meshes = []
+    for _ in range(2):
+        m = eb.LimitingMesh(s, cells, [0.0] * dim, [1.0] * dim, 0, helper_layers=1, cure_steps=0)
+        m.set_solution(luh)
+        m.set_fv_initial(fv)
+        m.init(0.0)
+        meshes.append(m)
+    graph, eager = meshes
+
+    def eager_until(t_end, max_steps=10 ** 9):
+        n = 0
+        while n < max_steps:
+            st = eager.state()
+            if not (st["t"] < t_end and st["dt"] > 0):
+                break
+            eager.step(1)
+            n += 1
+        return n
+
+    assert graph.run_until(0.05, max_steps=5) == eager_until(0.05, max_steps=5) == 5
+    s.variant = 1 if s.variant != 1 else 0
+    t_end = 0.03 if dim == 2 else 0.06
+    n_g, n_e = graph.run_until(t_end), eager_until(t_end)
+    assert n_g == n_e > 5
+    assert graph.run_until(t_end) == 0  # already there: no replay changes anything
+    a, b = graph.state(), eager.state()
+    assert a == b and a["irregular_steps"] > 0
+    assert np.array_equal(graph.get_solution(), eager.get_solution())
+    assert np.array_equal(graph.status(), eager.status())
+    la, ma = graph.limiter()
+    lb, mb = eager.limiter()
+    assert np.array_equal(ma, mb) and np.array_equal(la[ma != 0], lb[mb != 0])
