@@ -163,3 +163,25 @@ def explosion(dim, order, cells, seed=0, radius=0.2):
 
     return (state(node_coordinates(dim, order, cells)), state(subcell_coordinates(dim, order, cells)),
             dict(centre=c.tolist()))
+
+
+def elastic_pulse(dim, order, cells, seed=0):
+    """Linear elastic waves on the periodic unit square/cube: a Gaussian
+    velocity pulse (width 0.1, direction ~ U[-1, 1]^3, centre ~ U[0.3, 0.7]^d)
+    with zero initial stress in a smoothly heterogeneous medium,
+    rho = 1 + 0.3 s, lambda = 2 + 0.5 s, mu = 1 + 0.2 s with
+    s = sin(2 pi (x + phase_x)) sin(2 pi (y + phase_y)), phases ~ U[0, 1].
+    Returns luh (ncells, b^d, 12): sxx syy szz sxy syz sxz u v w lambda mu rho."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.3, 0.7, size=dim)
+    direction = rng.uniform(-1.0, 1.0, size=3)
+    phase = rng.uniform(0.0, 1.0, size=2)
+    X = node_coordinates(dim, order, cells)
+    g = np.exp(-_periodic_d2(X, c) / 0.01)
+    s = np.sin(2 * np.pi * (X[..., 0] + phase[0])) * np.sin(2 * np.pi * (X[..., 1] + phase[1]))
+    Q = np.zeros(X.shape[:-1] + (12,))
+    Q[..., 6:9] = g[..., None] * direction
+    Q[..., 9] = 2.0 + 0.5 * s
+    Q[..., 10] = 1.0 + 0.2 * s
+    Q[..., 11] = 1.0 + 0.3 * s
+    return Q, dict(centre=c.tolist(), direction=direction.tolist(), phase=phase.tolist())

@@ -29,8 +29,8 @@ const double* orc_table(const char* name, int N) {
   return 0;
 }
 
-int orc_nvar(const orc_solver* s) { (void)s; return 5; }
-int orc_npar(const orc_solver* s) { return s->pde == 1 ? 1 : 0; }
+int orc_nvar(const orc_solver* s) { return s->pde == 2 ? 9 : 5; }
+int orc_npar(const orc_solver* s) { return s->pde == 1 ? 1 : s->pde == 2 ? 3 : 0; }
 
 /* ---- PDE hooks ----------------------------------------------------------
  * pde 0: Demonstrators/EulerADERDG/MyEulerSolver_ADERDG.cpp:102-135
@@ -67,6 +67,21 @@ void orc_flux(const orc_solver* s, const double* Q, double* F) {
 }
 
 void orc_eigenvalues(const orc_solver* s, const double* Q, int d, double* lambda) {
+  if (s->pde == 2) { /* elastic waves: ElasticityKernelTest2D.cpp:99-125 */
+    const double lam = Q[9], mu = Q[10], rho0 = Q[11];
+    const double cp = sqrt((lam + 2 * mu) / rho0);
+    const double cs = sqrt(mu / rho0);
+    lambda[0] = -cp;
+    lambda[1] = -cs;
+    lambda[2] = -cs;
+    lambda[3] = 0.0;
+    lambda[4] = 0.0;
+    lambda[5] = 0.0;
+    lambda[6] = +cs;
+    lambda[7] = +cs;
+    lambda[8] = +cp;
+    return;
+  }
   const double GAMMA = 1.4;
   const double irho = 1.0 / Q[0];
   const double p = pressure(s, Q, irho);
@@ -416,7 +431,7 @@ double orc_stable_dt(const orc_solver* s, const double* luh, const double* dx) {
   for (int p = 0; p < g.P; p++) {
     double den = 0.0;
     for (int d = 0; d < g.d; d++) {
-      double lam[5];
+      double lam[16];
       orc_eigenvalues(s, luh + p * g.nD, d, lam);
       double me = 0.0;
       for (int k = 0; k < g.nV; k++) me = dmax(fabs(lam[k]), me);

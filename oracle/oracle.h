@@ -15,7 +15,9 @@ extern "C" {
 #endif
 
 /* PDE ids: 0 = Euler as in the EulerADERDG demonstrator (outflow boundary),
- *          1 = the "2.5D" Euler mock of the reference kernel tests (nPar = 1). */
+ *          1 = the "2.5D" Euler mock of the reference kernel tests (nPar = 1),
+ *          2 = linear elastic waves of the reference kernel tests (nVar = 9,
+ *              nPar = 3: lambda, mu, rho; linear kernels only). */
 typedef struct {
   int dim;   /* 2 or 3 */
   int order; /* N, basis size N+1 */
@@ -43,6 +45,17 @@ double orc_stable_dt(const orc_solver* s, const double* luh, const double* dx);
 /* PDE hooks */
 void orc_flux(const orc_solver* s, const double* Q, double* F /* [dim][nV] */);
 void orc_eigenvalues(const orc_solver* s, const double* Q, int d, double* lambda);
+void orc_ncp(const orc_solver* s, const double* Q, const double* gradQ /* [dim][nV] */, double* BgradQ);
+void orc_coefficient_matrix(const orc_solver* s, const double* Q, int d, double* Bn /* [nV][nV] */);
+
+/* Linear kernels (linear.c): spaceTimePredictorLinear (Cauchy-Kovalevski,
+ * non-conservative product) + volumeIntegralLinear when lduh != 0; lQhi
+ * [b^d][nD] and lFhi [d][b^d][nV] optional. */
+void orc_lin_predictor(const orc_solver* s, const double* luh, const double* dx, double dt, double* lQhbnd,
+                       double* lFhbnd, double* lduh, double* lQhi, double* lFhi);
+void orc_lin_volume_integral(const orc_solver* s, double* lduh, const double* lFhi, const double* dx);
+void orc_lin_surface_integral(const orc_solver* s, double* lduh, const double* lFhbnd, const double* dx);
+void orc_lin_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, const double* QR, int dir);
 
 /* table access (generated dg_tables.h) */
 const double* orc_table(const char* name, int order);

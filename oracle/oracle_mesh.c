@@ -18,6 +18,19 @@ static void be_surf(void* c, double* du, const double* fb, const double* dx) { o
 static void be_upd(void* c, double* u, const double* du, double dt) { orc_solution_update((const orc_solver*)c, u, du, dt); }
 static double be_dt(void* c, const double* u, const double* dx) { return orc_stable_dt((const orc_solver*)c, u, dx); }
 
+/* linear PDEs (pde 2): Cauchy-Kovalevski predictor, linear Riemann solver and
+ * surface integral; periodic meshes only (no boundary kernels) */
+static int be_lpred(void* c, const double* luh, const double* dx, double dt, double* qb, double* fb, double* du) {
+  orc_lin_predictor((const orc_solver*)c, luh, dx, dt, qb, fb, du, 0, 0);
+  return 0;
+}
+static void be_lriem(void* c, double* FL, double* FR, const double* QL, const double* QR, int d) {
+  orc_lin_riemann((const orc_solver*)c, FL, FR, QL, QR, d);
+}
+static void be_lsurf(void* c, double* du, const double* fb, const double* dx) {
+  orc_lin_surface_integral((const orc_solver*)c, du, fb, dx);
+}
+
 typedef struct {
   orc_solver s;
   hrn_mesh* m;
@@ -30,6 +43,11 @@ void* orc_mesh_create(int dim, int order, int pde, const int* cells, const doubl
   om->s.pde = pde;
   hrn_backend k = {&om->s, dim, order, orc_nvar(&om->s), orc_nvar(&om->s) + orc_npar(&om->s),
                    be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  if (pde == 2) {
+    k.predictor = be_lpred;
+    k.riemann = be_lriem;
+    k.surface_integral = be_lsurf;
+  }
   om->m = hrn_create(&k, cells, size, bc, nthreads);
   return om;
 }

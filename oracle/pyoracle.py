@@ -84,8 +84,8 @@ class Kernels:
     def __init__(self, dim, order, pde=0, impl="oracle"):
         self.dim, self.order, self.pde, self.impl = dim, order, pde, impl
         self.b = order + 1
-        self.nvar = 5
-        self.ndata = 5 + (1 if pde == 1 else 0)
+        self.nvar = 9 if pde == 2 else 5
+        self.ndata = self.nvar + {1: 1, 2: 3}.get(pde, 0)
         self.P = self.b ** dim
         self.F = self.b ** (dim - 1)
         self._s = _Solver(dim, order, pde)
@@ -140,6 +140,42 @@ class Kernels:
     def stable_dt(self, luh, dx):
         dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
         return self._call("stable_dt", _p(np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)), _p(dx))
+
+    # linear kernels (oracle/linear.c; the reference's spaceTimePredictorLinear,
+    # riemannSolverLinear, surfaceIntegralLinear, volumeIntegralLinear)
+    def lin_predictor(self, luh, dx, dt):
+        P, F, d, nV, nD = self.P, self.F, self.dim, self.nvar, self.ndata
+        luh = np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        qb, fb = np.zeros(2 * d * F * nD), np.zeros(2 * d * F * nV)
+        du, qh, fh = np.zeros(P * nV), np.zeros(P * nD), np.zeros(d * P * nV)
+        self._call("lin_predictor", _p(luh), _p(dx), ctypes.c_double(dt), _p(qb), _p(fb), _p(du), _p(qh), _p(fh))
+        return dict(lQhbnd=qb, lFhbnd=fb, lduh=du, lQhi=qh, lFhi=fh)
+
+    def lin_riemann(self, QL, QR, direction):
+        n = self.F * self.nvar
+        FL, FR = np.zeros(n), np.zeros(n)
+        QL = np.ascontiguousarray(QL, dtype=np.float64).reshape(-1)
+        QR = np.ascontiguousarray(QR, dtype=np.float64).reshape(-1)
+        if self.impl == "oracle":
+            self._call("lin_riemann", _p(FL), _p(FR), _p(QL), _p(QR), ctypes.c_int(direction))
+        else:
+            self._call("lin_riemann", _p(FL), _p(FR), _p(QL), _p(QR), ctypes.c_double(0.0), ctypes.c_int(direction))
+        return FL, FR
+
+    def lin_surface_integral(self, lduh, lFhbnd, dx):
+        lduh = np.array(lduh, dtype=np.float64).reshape(-1)
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        self._call("lin_surface_integral", _p(lduh),
+                   _p(np.ascontiguousarray(lFhbnd, dtype=np.float64).reshape(-1)), _p(dx))
+        return lduh
+
+    def lin_volume_integral(self, lFhi, dx):
+        lduh = np.zeros(self.P * self.nvar)
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        self._call("lin_volume_integral", _p(lduh), _p(np.ascontiguousarray(lFhi, dtype=np.float64).reshape(-1)),
+                   _p(dx))
+        return lduh
 
     # limiter kernels of the C restatement (oracle/limiter.c); Euler only
     def fv_patch_size(self):
@@ -211,7 +247,7 @@ class Mesh:
                        ("sweeps", ctypes.c_long), ("run_until", ctypes.c_int)):
             getattr(self._l, self._pre + nm).restype = rt
         self.ncells = int(np.prod(cells))
-        self.shape = (self.ncells, (order + 1) ** dim, 5 + (1 if pde == 1 else 0))
+        self.shape = (self.ncells, (order + 1) ** dim, {1: 6, 2: 12}.get(pde, 5))
 
     def _f(self, nm):
         return getattr(self._l, self._pre + nm)

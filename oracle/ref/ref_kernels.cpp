@@ -155,6 +155,98 @@ struct EulerTest : public PDEBase<N_, 1> {
     std::copy_n(stateIn, 6, stateOut);
     std::copy_n(fluxIn, 5, fluxOut);
   }
+  // GenericEulerKernelTest{2D,3D}.cpp: the zero system matrix of the mock
+  void coefficientMatrix(const double* const, const int, double* Bn) { std::fill_n(Bn, 25, 0.0); }
+};
+
+// The kernel tests' linear elastic-wave PDE (exahype/tests/kernels/c/
+// ElasticityKernelTest2D.cpp:31-235: 9 variables, parameters lambda, mu, rho),
+// restated for the linear kernels; the z parts are the ones written out
+// (commented) beside the x and y parts there.
+template <int N_>
+struct Elastic {
+  static constexpr int NumberOfVariables = 9;
+  static constexpr int NumberOfParameters = 3;
+  static constexpr int Order = N_;
+  static constexpr double CFL = 0.9;
+  void flux(const double* const, double** F) {
+    for (int d = 0; d < DIMENSIONS; d++) std::fill_n(F[d], 9, 0.0);
+  }
+  void algebraicSource(const double* const, double* S) { std::fill_n(S, 9, 0.0); }
+  void eigenvalues(const double* const Q, const int, double* lambda) {
+    std::fill_n(lambda, 9, 0.0);
+    const double lam = Q[9], mu = Q[10], rho0 = Q[11];
+    const double cp = std::sqrt((lam + 2 * mu) / rho0);
+    const double cs = std::sqrt(mu / rho0);
+    lambda[0] = -cp;
+    lambda[1] = -cs;
+    lambda[2] = -cs;
+    lambda[3] = 0.0;
+    lambda[4] = 0.0;
+    lambda[5] = 0.0;
+    lambda[6] = +cs;
+    lambda[7] = +cs;
+    lambda[8] = +cp;
+  }
+  void nonConservativeProduct(const double* const Q, const double* const gradQ, double* BgradQ) {
+    std::fill_n(BgradQ, 9 * DIMENSIONS, 0.0);
+    const double lam = Q[9], mu = Q[10], irho = 1.0 / Q[11];
+    const double* gx = gradQ;
+    const double* gy = gradQ + 9;
+    double* bx = BgradQ;
+    double* by = BgradQ + 9;
+    bx[0] = -(lam + 2 * mu) * gx[6];
+    bx[1] = -lam * gx[6];
+    bx[2] = -lam * gx[6];
+    bx[3] = -mu * gx[7];
+    bx[4] = 0.0;
+    bx[5] = -mu * gx[8];
+    bx[6] = -irho * gx[0];
+    bx[7] = -irho * gx[3];
+    bx[8] = -irho * gx[5];
+    by[0] = -lam * gy[7];
+    by[1] = -(lam + 2 * mu) * gy[7];
+    by[2] = -lam * gy[7];
+    by[3] = -mu * gy[6];
+    by[4] = -mu * gy[8];
+    by[5] = 0.0;
+    by[6] = -irho * gy[3];
+    by[7] = -irho * gy[1];
+    by[8] = -irho * gy[4];
+#if DIMENSIONS == 3
+    const double* gz = gradQ + 18;
+    double* bz = BgradQ + 18;
+    bz[0] = -lam * gz[8];
+    bz[1] = -lam * gz[8];
+    bz[2] = -(lam + 2 * mu) * gz[8];
+    bz[3] = 0.0;
+    bz[4] = -mu * gz[7];
+    bz[5] = -mu * gz[6];
+    bz[6] = -irho * gz[5];
+    bz[7] = -irho * gz[4];
+    bz[8] = -irho * gz[2];
+#endif
+  }
+  void coefficientMatrix(const double* const Q, const int normalNonZero, double* Bn) {
+    std::fill_n(Bn, 81, 0.0);
+    const double lam = Q[9], mu = Q[10], irho = 1.0 / Q[11];
+#define B(r, c) Bn[(r - 1) * 9 + (c - 1)]
+    switch (normalNonZero) {
+      case 0:
+        B(7, 1) = -(lam + 2 * mu); B(7, 2) = -lam; B(7, 3) = -lam; B(8, 4) = -mu; B(9, 6) = -mu;
+        B(1, 7) = -irho; B(4, 8) = -irho; B(6, 9) = -irho;
+        break;
+      case 1:
+        B(8, 1) = -lam; B(8, 2) = -(lam + 2 * mu); B(8, 3) = -lam; B(7, 4) = -mu; B(9, 5) = -mu;
+        B(4, 7) = -irho; B(2, 8) = -irho; B(5, 9) = -irho;
+        break;
+      default:
+        B(9, 1) = -lam; B(9, 2) = -lam; B(9, 3) = -(lam + 2 * mu); B(8, 5) = -mu; B(7, 6) = -mu;
+        B(6, 7) = -irho; B(5, 8) = -irho; B(3, 9) = -irho;
+        break;
+    }
+#undef B
+  }
 };
 
 template <int D> using Vec = tarch::la::Vector<D, double>;
@@ -232,6 +324,43 @@ double stable_dt(const double* luh, const double* dxa) {
   return kernels::aderdg::generic::c::stableTimeStepSize<S>(s, luh, vec(dxa));
 }
 
+// ---- linear kernels ----------------------------------------------------------
+// spaceTimePredictorLinear<usePointSource=false, useSource=false,
+// useFlux=false, useNCP=true> + volumeIntegralLinear (Toolkit/src/eu/exahype/
+// solvers/templates/AbstractGenericADERDGSolverImplementation.template:53-54,85-86)
+template <class S>
+void lin_predictor(const double* luh, const double* dxa, double dt, double* lQhbnd, double* lFhbnd, double* lduh,
+                   double* lQhi_out, double* lFhi_out) {
+  constexpr int b = S::Order + 1;
+  constexpr int nV = S::NumberOfVariables, nD = nV + S::NumberOfParameters;
+  constexpr int sp = ipow(b, DIMENSIONS);
+  constexpr int st = sp * b;
+  static thread_local double lQi[(st + sp) * nD], lFi[st * (2 * DIMENSIONS + 1) * nV], gradQ[st * DIMENSIONS * nV];
+  static thread_local double lQh[sp * nD], lFh[sp * (DIMENSIONS + 1) * nV];
+  double* stu[2] = {lQi, nullptr};
+  double* stf[2] = {lFi, gradQ};
+  S s;
+  kernels::aderdg::generic::c::spaceTimePredictorLinear<false, false, false, true, S>(
+      s, lQhbnd, lFhbnd, stu, stf, lQh, lFh, luh, vec(dxa), dt, nullptr);
+  if (lduh) kernels::aderdg::generic::c::volumeIntegralLinear<false, false, nV, b>(lduh, lFh, vec(dxa));
+  if (lQhi_out) std::copy_n(lQh, sp * nD, lQhi_out);
+  if (lFhi_out) std::copy_n(lFh, sp * DIMENSIONS * nV, lFhi_out);
+}
+template <class S>
+void lin_riemann(double* FL, double* FR, const double* QL, const double* QR, double dt, int dir) {
+  S s;
+  kernels::aderdg::generic::c::riemannSolverLinear<true, S>(s, FL, FR, QL, QR, dt, dir);
+}
+template <class S>
+void lin_surface(double* lduh, const double* lFhbnd, const double* dxa) {
+  kernels::aderdg::generic::c::surfaceIntegralLinear<S::NumberOfVariables, S::Order + 1>(lduh, lFhbnd, vec(dxa));
+}
+template <class S>
+void lin_volume(double* lduh, const double* lFhi, const double* dxa) {
+  kernels::aderdg::generic::c::volumeIntegralLinear<false, false, S::NumberOfVariables, S::Order + 1>(lduh, lFhi,
+                                                                                                    vec(dxa));
+}
+
 // ---- limiter and FV kernels (Euler demonstrator PDE) ------------------------
 template <class S>
 void project_fv(const double* luh, double* lim) {
@@ -282,6 +411,30 @@ void fv_boundary(double* lim, int face) {
 }
 
 }  // namespace
+
+#define DISPATCH_ELASTIC(N, call)                                        \
+  do {                                                                  \
+    switch (N) {                                                        \
+      case 3: { typedef Elastic<3> S; call; } break;                    \
+      case 4: { typedef Elastic<4> S; call; } break;                    \
+      case 5: { typedef Elastic<5> S; call; } break;                    \
+      default: std::fprintf(stderr, "ref: order %d not built\n", N);   \
+    }                                                                   \
+  } while (0)
+
+// linear kernels: the elastic-wave PDE, or (pde 1) the Euler mock
+#define DISPATCH_LIN(pde, N, call)                                       \
+  do {                                                                  \
+    if (pde == 2) {                                                     \
+      DISPATCH_ELASTIC(N, call);                                        \
+    } else {                                                            \
+      switch (N) {                                                      \
+        case 3: { typedef EulerTest<3> S; call; } break;                \
+        case 5: { typedef EulerTest<5> S; call; } break;                \
+        default: std::fprintf(stderr, "ref: order %d not built\n", N); \
+      }                                                                 \
+    }                                                                   \
+  } while (0)
 
 #define DISPATCH(pde, N, call)                                              \
   do {                                                                      \
@@ -377,7 +530,8 @@ void REFNAME(surface_integral)(int pde, int N, double* lduh, const double* lFhbn
 
 void REFNAME(solution_update)(int pde, int N, double* luh, const double* lduh, double dt) {
   REFNAME(init)();
-  DISPATCH(pde, N, update<S>(luh, lduh, dt));
+  if (pde == 2) DISPATCH_ELASTIC(N, update<S>(luh, lduh, dt));
+  else DISPATCH(pde, N, update<S>(luh, lduh, dt));
 }
 
 void REFNAME(project_fv)(int N, const double* luh, double* lim) { REFNAME(init)(); DISPATCH_EULER(N, project_fv<S>(luh, lim)); }
@@ -408,8 +562,29 @@ void REFNAME(fv_boundary)(int N, double* lim, int face) { DISPATCH_EULER(N, fv_b
 double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx) {
   REFNAME(init)();
   double r = -1;
-  DISPATCH(pde, N, r = stable_dt<S>(luh, dx));
+  if (pde == 2) DISPATCH_ELASTIC(N, r = stable_dt<S>(luh, dx));
+  else DISPATCH(pde, N, r = stable_dt<S>(luh, dx));
   return r;
+}
+
+void REFNAME(lin_predictor)(int pde, int N, const double* luh, const double* dx, double dt, double* lQhbnd,
+                            double* lFhbnd, double* lduh, double* lQhi, double* lFhi) {
+  REFNAME(init)();
+  DISPATCH_ELASTIC(N, lin_predictor<S>(luh, dx, dt, lQhbnd, lFhbnd, lduh, lQhi, lFhi));
+  (void)pde;
+}
+void REFNAME(lin_riemann)(int pde, int N, double* FL, double* FR, const double* QL, const double* QR, double dt,
+                          int dir) {
+  REFNAME(init)();
+  DISPATCH_LIN(pde, N, lin_riemann<S>(FL, FR, QL, QR, dt, dir));
+}
+void REFNAME(lin_surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx) {
+  REFNAME(init)();
+  DISPATCH_LIN(pde, N, lin_surface<S>(lduh, lFhbnd, dx));
+}
+void REFNAME(lin_volume_integral)(int pde, int N, double* lduh, const double* lFhi, const double* dx) {
+  REFNAME(init)();
+  DISPATCH_LIN(pde, N, lin_volume<S>(lduh, lFhi, dx));
 }
 
 }  // extern "C"

@@ -25,6 +25,11 @@ void REFNAME(boundary_face)(int pde, int N, double* FIn, const double* QIn, cons
 void REFNAME(surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx);
 void REFNAME(solution_update)(int pde, int N, double* luh, const double* lduh, double dt);
 double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx);
+void REFNAME(lin_predictor)(int pde, int N, const double* luh, const double* dx, double dt, double* lQhbnd,
+                            double* lFhbnd, double* lduh, double* lQhi, double* lFhi);
+void REFNAME(lin_riemann)(int pde, int N, double* FL, double* FR, const double* QL, const double* QR, double dt,
+                          int dir);
+void REFNAME(lin_surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx);
 void REFNAME(init)();
 void REFNAME(project_fv)(int N, const double* luh, double* lim);
 void REFNAME(project_dg)(int N, const double* lim, double* luh);
@@ -54,6 +59,21 @@ void be_bnd(void* c, double* FIn, const double* QIn, int f) {
 void be_surf(void* c, double* du, const double* fb, const double* dx) { Ctx* x = (Ctx*)c; REFNAME(surface_integral)(x->pde, x->N, du, fb, dx); }
 void be_upd(void* c, double* u, const double* du, double dt) { Ctx* x = (Ctx*)c; REFNAME(solution_update)(x->pde, x->N, u, du, dt); }
 double be_dt(void* c, const double* u, const double* dx) { Ctx* x = (Ctx*)c; return REFNAME(stable_dt)(x->pde, x->N, u, dx); }
+// linear PDE (elastic waves): Cauchy-Kovalevski predictor, linear Riemann
+// solver and surface integral; periodic meshes only
+int be_lpred(void* c, const double* luh, const double* dx, double dt, double* qb, double* fb, double* du) {
+  Ctx* x = (Ctx*)c;
+  REFNAME(lin_predictor)(x->pde, x->N, luh, dx, dt, qb, fb, du, nullptr, nullptr);
+  return 0;
+}
+void be_lriem(void* c, double* FL, double* FR, const double* QL, const double* QR, int d) {
+  Ctx* x = (Ctx*)c;
+  REFNAME(lin_riemann)(x->pde, x->N, FL, FR, QL, QR, 0.0, d);
+}
+void be_lsurf(void* c, double* du, const double* fb, const double* dx) {
+  Ctx* x = (Ctx*)c;
+  REFNAME(lin_surface_integral)(x->pde, x->N, du, fb, dx);
+}
 struct RefMesh { Ctx c; hrn_mesh* m; };
 size_t nsol(hrn_mesh* m) { return (size_t)m->ncells * m->P * m->k.ndata; }
 }
@@ -65,6 +85,13 @@ void* REFNAME(mesh_create)(int order, int pde, const int* cells, const double* s
   r->c.pde = pde;
   r->c.N = order;
   hrn_backend k = {&r->c, DIMENSIONS, order, 5, 5 + (pde == 1 ? 1 : 0), be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  if (pde == 2) {
+    k.nvar = 9;
+    k.ndata = 12;
+    k.predictor = be_lpred;
+    k.riemann = be_lriem;
+    k.surface_integral = be_lsurf;
+  }
   r->m = hrn_create(&k, cells, size, bc, nthreads);
   return r;
 }

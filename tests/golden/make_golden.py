@@ -7,8 +7,8 @@ committed and nothing at test time reads the reference.
 Writes
   kernel_vectors.npz  every array of the reference's kernel-test data files
                       (ExaHyPE/exahype/tests/kernels/testdata/
-                      {generic_euler,limiter}_testdata.cpp), read as text and
-                      keyed "<dim>/<file>/<namespace>/<array>".
+                      {generic_euler,limiter,elasticity}_testdata.cpp), read
+                      as text and keyed "<dim>/<file>/<namespace>/<array>".
   ref_tables.npz      the reference's operator tables, dumped by its own init
                       code compiled into oracle/_ref (key "<name>/<N>").
   ref_mesh_*.npz      uniform-mesh runs of the reference kernels through the
@@ -26,7 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 
-ARRAY_RE = re.compile(r"const\s+double\s+(\w+)\s*\[\s*(\d+)\s*\]\s*=?\s*\{(.*?)\}\s*;", re.S)
+ARRAY_RE = re.compile(r"const\s+double\s+(\w+)\s*\[\s*([\d\s*]+?)\s*\]\s*=?\s*\{(.*?)\}\s*;", re.S)
 
 
 def parse_testdata(path):
@@ -52,7 +52,8 @@ def parse_testdata(path):
             am = ARRAY_RE.match(sec, tok.start())
             if not am:
                 continue
-            name, n, body = am.group(1), int(am.group(2)), am.group(3)
+            name, body = am.group(1), am.group(3)
+            n = int(np.prod([int(f) for f in am.group(2).split("*")]))  # sizes like "9 * 5 * 4"
             vals = [float(v) for v in re.split(r"[,\s]+", body.strip()) if v]
             if not vals:
                 continue
@@ -65,7 +66,7 @@ def parse_testdata(path):
 def make_kernel_vectors(ref):
     td = os.path.join(ref, "ExaHyPE", "exahype", "tests", "kernels", "testdata")
     out = {}
-    for fname in ("generic_euler_testdata.cpp", "limiter_testdata.cpp"):
+    for fname in ("generic_euler_testdata.cpp", "limiter_testdata.cpp", "elasticity_testdata.cpp"):
         for k, v in parse_testdata(os.path.join(td, fname)).items():
             dim, rest = k.split("/", 1)
             out["%s/%s/%s" % (dim, fname.split("_testdata")[0], rest)] = v
