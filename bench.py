@@ -42,6 +42,9 @@ NVAR = 5
 WORKLOAD = "euler3d_N5_27^3_periodic_4pulses"
 METRIC = "ADER-DG DoF-updates/s on 1 B200, mixed vs FP64 at \u22641e-9 L2; p99 solve latency"
 LIM_DIM, LIM_ORDER, LIM_CELLS, LIM_TEND = 2, 5, (81, 81), 0.2
+# linear-kernel workload: elastic waves, 9 variables + 3 material parameters
+EL_DIM, EL_ORDER, EL_CELLS, EL_NVAR, EL_NDATA = 3, 5, (27, 27, 27), 9, 12
+EL_WORKLOAD = "elastic3d_N5_27^3_periodic_pulse_linear"
 LIM_WORKLOAD = "euler2d_N5_81^2_explosion_limiter_outflow_t0.2"
 # per-launch DRAM traffic of the predictor from the committed ncu capture
 PROFILE_PREDICTOR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
@@ -79,6 +82,20 @@ def bytes_per_step(dim, N, ncells, nV=NVAR, nD=NVAR):
     riem = 8 * ncells * dim * (2 * F * nD + 4 * F * nV)
     corr = 8 * ncells * (2 * P * nD + P * nV + 2 * dim * F * nV)
     return dict(predictor=pred, riemann=riem, corrector=corr)
+
+
+def linear_predictor_flops(dim, N, ncells, nV=EL_NVAR, nD=EL_NDATA):
+    """Algorithmic FLOPs of the linear predictor (Cauchy-Kovalevski) + volume
+    integral per launch: per derivative level (b of them) 2 d nV b^(d+1)
+    (line gradients) + per node the elastic non-conservative product (3 per
+    direction: 2 products for the moduli, 9 products) and the level update and
+    both time averages (d nV + 2 nV + 2 d nV); per cell once the boundary
+    extrapolation 4 d b^(d-1) b (nD + nV) and the volume integral 2 d nV b^d."""
+    b = N + 1
+    P = b ** dim
+    per_level = 2 * dim * nV * b ** (dim + 1) + P * (dim * (2 + nV) + dim * nV + 2 * nV + 2 * dim * nV)
+    per_cell = b * per_level + 4 * dim * b ** (dim - 1) * b * (nD + nV) + 2 * dim * nV * P
+    return per_cell * ncells
 
 
 def load_peaks():
@@ -334,6 +351,7 @@ def run_ours(a):
     mixed = None if a.no_mixed else run_mixed_arm(a, u0, s.variant, dev)
     lim = None if a.no_limiter else run_limiter_workload(a, world, dev, rank)
     ens = None if a.no_ensemble else run_ensemble_workload(a, world, dev, rank)
+    ela = None if a.no_elastic else run_elastic_workload(a, world, dev, rank, fp64_peak)
     srv = None if a.no_serving else run_serving_workload(a, world, dev, rank)
     line = {
         "metric": METRIC, "value": value, "unit": "DoF-updates/s", "n_gpus": world, "steps": a.steps,
@@ -344,13 +362,80 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
-        "mixed": mixed, "limiter": lim, "ensemble": ens, "serving": srv,
+        "mixed": mixed, "limiter": lim, "ensemble": ens, "serving": srv, "elastic": ela,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def run_elastic_workload(a, world, dev, rank, fp64_peak=None):
+    """The linear-kernel workload: 3D elastic waves (velocity pulse in a
+    smoothly heterogeneous medium), N = 5 on 27^3 periodic cells; warm-up
+    steps, then min(steps, 20) timed steps with CUDA events on the mesh
+    stream, per-phase events for the kernel split; max over ranks."""
+    import torch
+    import exahype_b200 as eb
+    from exahype_b200 import problems
+    u0, _ = problems.elastic_pulse(EL_DIM, EL_ORDER, EL_CELLS, seed=SEED + rank)
+    ncells = int(np.prod(EL_CELLS))
+    s = eb.Solver(EL_DIM, EL_ORDER, eb.PDE_ELASTIC)
+    chosen, vms = s.autotune(ncells)
+    m = eb.Mesh(s, EL_CELLS, [0.0] * EL_DIM, [1.0] * EL_DIM, eb.BC_PERIODIC)
+    m.set_solution(u0)
+    m.init(0.0)
+    stream = torch.cuda.ExternalStream(m.stream_handle, device=dev)
+    m.step(max(3, a.warmup))
+    m.synchronize()
+    k = max(1, min(a.steps, 20))
+    m.phase_times(reset=True)
+    m.set_profiling(True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(k)
+    e1.record(stream)
+    e1.synchronize()
+    m.set_profiling(False)
+    ph = m.phase_times(reset=True)
+    ms = reduce_max(e0.elapsed_time(e1), world, dev)
+    dof_step = ncells * (EL_ORDER + 1) ** EL_DIM * EL_NVAR
+    pred_ms = ph["predictor"][0] / k
+    pfl = linear_predictor_flops(EL_DIM, EL_ORDER, ncells)
+    ach = pfl / (pred_ms / 1e3) / 1e12
+    peaks = load_peaks()
+    byt = bytes_per_step(EL_DIM, EL_ORDER, ncells, nV=EL_NVAR, nD=EL_NDATA)
+    # the linear Riemann solver reads both sides' states and writes both fluctuations
+    F = (EL_ORDER + 1) ** (EL_DIM - 1)
+    byt["riemann"] = 8 * ncells * EL_DIM * (2 * F * EL_NDATA + 2 * F * EL_NVAR)
+    kern = {"predictor": dict(bound="fp64", achieved=ach, unit="TFLOP/s", ms=pred_ms, peak=fp64_peak,
+                              frac=(ach / fp64_peak) if fp64_peak else None, algorithmic_flops_per_launch=pfl)}
+    for name in ("riemann", "corrector"):
+        t_ms = ph[name][0] / k
+        gbs = byt[name] / (t_ms / 1e3) / 1e9
+        kern[name] = dict(bound="hbm", achieved=gbs, unit="GB/s", ms=t_ms, peak=peaks["hbm_gbs"],
+                          frac=gbs / peaks["hbm_gbs"])
+    out = {"workload": EL_WORKLOAD, "value": dof_step * k * world / (ms / 1e3), "unit": "DoF-updates/s",
+           "steps": k, "ms_per_step": ms / k, "dof_per_step": dof_step, "kernels": kern,
+           "predictor_variant": {"chosen": chosen, "variant_ms_full_mesh": vms[:2]},
+           "dt": m.state()["dt"], "timing": "exa_mesh_step(k), CUDA events on the mesh stream"}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import pyoracle
+        if pyoracle.ref_available(EL_DIM):
+            nthreads = os.cpu_count() or 1
+            r = pyoracle.Mesh(EL_DIM, EL_ORDER, EL_CELLS, [1.0] * EL_DIM, -1, pde=2, impl="ref", nthreads=nthreads)
+            r.set_solution(u0)
+            r.init(0.0)
+            t0 = time.perf_counter()
+            r.step(1)
+            el = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": dof_step / el, "unit": "DoF-updates/s", "cores": nthreads,
+                                   "kind": "reference", "sample": "1 full time step of the 27^3 elastic mesh on the "
+                                   "reference's linear kernels, %.1f s" % el}
+    return out
 
 
 def run_limiter_workload(a, world, dev, rank):
@@ -576,12 +661,14 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--serving-full", action="store_true", help="serving: the full-size request mix")
-    ap.add_argument("--workload", default="headline", choices=["headline", "limiter", "ensemble", "serving"],
-                    help="limiter / ensemble / serving: only that workload, as its own JSON line")
+    ap.add_argument("--no-elastic", action="store_true", help="skip the linear-kernel (elastic waves) workload")
+    ap.add_argument("--workload", default="headline",
+                    choices=["headline", "limiter", "ensemble", "serving", "elastic"],
+                    help="limiter / ensemble / serving / elastic: only that workload, as its own JSON line")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
-    if a.workload in ("limiter", "ensemble", "serving"):
+    if a.workload in ("limiter", "ensemble", "serving", "elastic"):
         return run_secondary_only(a)
     return run_ours(a)
 
@@ -594,8 +681,11 @@ def run_secondary_only(a):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     run = {"limiter": run_limiter_workload, "ensemble": run_ensemble_workload,
-           "serving": run_serving_workload}[a.workload]
-    r = run(a, world, torch.device("cuda", local), rank)
+           "serving": run_serving_workload, "elastic": run_elastic_workload}[a.workload]
+    if a.workload == "elastic":
+        r = run(a, world, torch.device("cuda", local), rank, None if a.no_fp64_probe else measure_fp64_peak())
+    else:
+        r = run(a, world, torch.device("cuda", local), rank)
     if rank == 0:
         print(json.dumps(dict(r, metric=METRIC, n_gpus=world, dtype="f64", data="synthetic (seeded)")), flush=True)
     if world > 1:

@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libexahype_b200.so")
 
 PDE_EULER = 0
 PDE_EULER_TEST = 1
+PDE_ELASTIC = 2  # linear elastic waves: 9 variables + lambda, mu, rho; linear kernels
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE = -1, 0, 1
 # predictor variants beyond the autotuned 0..3: the mixed-precision predictor
 PREDICTOR_MIXED, PREDICTOR_MIXED_2 = 4, 5
@@ -99,8 +100,9 @@ class Solver:
         z = (ctypes.c_int * 4)()
         _check(lib.exa_solver_sizes(h, z), "exa_solver_sizes")
         self.unknowns_per_cell, self.data_per_cell, self.data_per_face, self.fluxes_per_face = list(z)
-        self.nvar = 5
+        self.nvar = self.unknowns_per_cell // (order + 1) ** dim
         self.ndata = self.data_per_cell // (order + 1) ** dim
+        self.linear = pde == PDE_ELASTIC
 
     def __del__(self):
         try:
@@ -127,6 +129,28 @@ class Solver:
         _check(load().exa_riemann_solver_nonlinear(self._h, _ptr(lQhbnd), _ptr(lFhbnd), _ptr(face_left),
                                                    _ptr(face_right), _ptr(face_dir), int(nfaces), _stream(stream)),
                "exa_riemann_solver_nonlinear")
+
+    # -- linear kernels (solvers of a linear PDE, e.g. PDE_ELASTIC) --
+    def space_time_predictor_linear(self, luh, lQhbnd, lFhbnd, lduh, dt_dev, dx, ncells, cell_list=None,
+                                    stream=None):
+        _check(load().exa_space_time_predictor_linear(
+            self._h, _ptr(luh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(lduh), _ptr(dt_dev), _dbl3(dx), int(ncells),
+            _ptr(cell_list), _stream(stream)), "exa_space_time_predictor_linear")
+
+    def space_time_predictor_linear_temps(self, luh, lQhbnd, lFhbnd, lduh, dt_dev, dx, ncells, lQhi, lFhi,
+                                          stream=None):
+        _check(load().exa_space_time_predictor_linear_temps(
+            self._h, _ptr(luh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(lduh), _ptr(dt_dev), _dbl3(dx), int(ncells),
+            _ptr(lQhi), _ptr(lFhi), _stream(stream)), "exa_space_time_predictor_linear_temps")
+
+    def riemann_solver_linear(self, lQhbnd, lFhbnd, face_left, face_right, face_dir, nfaces, stream=None):
+        _check(load().exa_riemann_solver_linear(self._h, _ptr(lQhbnd), _ptr(lFhbnd), _ptr(face_left),
+                                                _ptr(face_right), _ptr(face_dir), int(nfaces), _stream(stream)),
+               "exa_riemann_solver_linear")
+
+    def volume_integral_linear(self, lduh, lFhi, ncells, stream=None):
+        _check(load().exa_volume_integral_linear(self._h, _ptr(lduh), _ptr(lFhi), int(ncells), _stream(stream)),
+               "exa_volume_integral_linear")
 
     def boundary_conditions(self, lQhbnd, lFhbnd, bcell, bface, nb, kind=BC_OUTFLOW, stream=None):
         _check(load().exa_boundary_conditions(self._h, _ptr(lQhbnd), _ptr(lFhbnd), _ptr(bcell), _ptr(bface), int(nb),

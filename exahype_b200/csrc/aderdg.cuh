@@ -510,7 +510,8 @@ __global__ void __launch_bounds__(128) boundary_kernel(const double* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// Corrector: surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90),
+// Corrector: surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90)
+// or, for a linear PDE, surfaceIntegralLinear,
 // solutionUpdate (3d/solutionUpdate.cpph:23-47) and stableTimeStepSize
 // (3d/stableTimeStepSize.cpph:21-63) fused, one thread per node. The new
 // admissible step is min-reduced over the whole launch into *dt_out; the
@@ -556,26 +557,33 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
       double du[nV];
 #pragma unroll
       for (int v = 0; v < nV; v++) du[v] = du_in[v];
+      // nonlinear: surfaceIntegralNonlinear, flux difference times w / dx;
+      // linear (surfaceIntegralLinear, 3d/surfaceIntegralLinear.cpph:24-91):
+      // the two faces' fluctuations are added, scaled by w divided by dx
+      constexpr bool LIN = PDE::kLinear;
       {
-        const double us = (wz * wy) * invDx0;
+        const double us = LIN ? (wz * wy) / cell_width(geo, inst, 0) : (wz * wy) * invDx0;
         const int fn = DIM == 3 ? z * b + y : y;
 #pragma unroll
         for (int v = 0; v < nV; v++)
-          du[v] -= (Fb[(1 * F + fn) * nV + v] * T.FR[x] - Fb[(0 * F + fn) * nV + v] * T.FL[x]) * us;
+          du[v] -= (LIN ? Fb[(1 * F + fn) * nV + v] * T.FR[x] + Fb[(0 * F + fn) * nV + v] * T.FL[x]
+                        : Fb[(1 * F + fn) * nV + v] * T.FR[x] - Fb[(0 * F + fn) * nV + v] * T.FL[x]) * us;
       }
       {
-        const double us = (wz * wx) * invDx1;
+        const double us = LIN ? (wz * wx) / cell_width(geo, inst, 1) : (wz * wx) * invDx1;
         const int fn = DIM == 3 ? z * b + x : x;
 #pragma unroll
         for (int v = 0; v < nV; v++)
-          du[v] -= (Fb[(3 * F + fn) * nV + v] * T.FR[y] - Fb[(2 * F + fn) * nV + v] * T.FL[y]) * us;
+          du[v] -= (LIN ? Fb[(3 * F + fn) * nV + v] * T.FR[y] + Fb[(2 * F + fn) * nV + v] * T.FL[y]
+                        : Fb[(3 * F + fn) * nV + v] * T.FR[y] - Fb[(2 * F + fn) * nV + v] * T.FL[y]) * us;
       }
       if (DIM == 3) {
-        const double us = (wy * wx) * invDx2;
+        const double us = LIN ? (wy * wx) / cell_width(geo, inst, 2) : (wy * wx) * invDx2;
         const int fn = y * b + x;
 #pragma unroll
         for (int v = 0; v < nV; v++)
-          du[v] -= (Fb[(5 * F + fn) * nV + v] * T.FR[z] - Fb[(4 * F + fn) * nV + v] * T.FL[z]) * us;
+          du[v] -= (LIN ? Fb[(5 * F + fn) * nV + v] * T.FR[z] + Fb[(4 * F + fn) * nV + v] * T.FL[z]
+                        : Fb[(5 * F + fn) * nV + v] * T.FR[z] - Fb[(4 * F + fn) * nV + v] * T.FL[z]) * us;
       }
       const double us = dt_ptr[inst] / (wz * wy * wx);
 #pragma unroll

@@ -448,6 +448,7 @@ int exa_batch_add(exa_batch* b, int dim, int order, int pde, const int* cells, c
   if (!find_kernels(dim, order, pde, &k))
     return fail(EXA_ERR_UNSUPPORTED, "exa_batch_add: no kernels built for dim=" + std::to_string(dim) +
                                          " order=" + std::to_string(order) + " pde=" + std::to_string(pde));
+  if (k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_batch_add: linear PDEs are stepped by exa_mesh only");
   BatchInst in;
   in.dim = dim;
   in.order = order;

@@ -16,6 +16,7 @@
 #include "aderdg.cuh"
 #include "predictor_lines.cuh"
 #include "limiter.cuh"
+#include "linear.cuh"
 
 namespace exa {
 
@@ -101,6 +102,7 @@ static int upload_tables() {
     for (int i = 0; i < b * b; i++) {
       t.Kxi[i] = exa_tab_Kxi[exa_tab_Kxi_off[N] + i];
       t.iK1[i] = exa_tab_iK1[exa_tab_iK1_off[N] + i];
+      t.dudx[i] = exa_tab_dudx[exa_tab_dudx_off[N] + i];
       t.Kxi_f[i] = (float)t.Kxi[i];
       l.uh2lob[i] = exa_tab_uh2lob[exa_tab_uh2lob_off[N] + i];
     }
@@ -118,6 +120,7 @@ static int upload_tables() {
 // ---- per-(DIM, N, PDE) launchers ------------------------------------------
 struct KernelSet {
   int dim, order, pde, nvar, npar, P, F;
+  bool linear;  // linear PDE: Cauchy-Kovalevski predictor, linear Riemann solver and surface integral
   // (luh, lQhbnd, lFhbnd, lduh, iters, dt, geo, n, list, count, temps, with_temps, sweeps, variant, stream);
   // count (optional, device) caps the list length at launch time
   int (*predictor)(const double*, double*, double*, double*, int*, const double*, Geometry, int, const int*,
@@ -127,6 +130,8 @@ struct KernelSet {
   int (*boundary)(const double*, double*, const int*, const int*, int, int, const int*, cudaStream_t);
   int (*corrector)(double*, const double*, const double*, const double*, double*, Geometry, int, const int*, int,
                    const int*, cudaStream_t);
+  // volumeIntegralLinear on its own (lduh, lFhi, ncells, stream); linear PDEs only
+  int (*volume)(double*, const double*, int, cudaStream_t);
 };
 
 template <int DIM, int N, class PDE>
@@ -249,12 +254,83 @@ struct Launch {
   }
   static KernelSet make(int pde) {
     using S = Shape<DIM, N, PDE>;
-    return KernelSet{DIM, N, pde, S::nV, S::nP, S::P, S::F, &predictor, &riemann, &boundary, &corrector};
+    return KernelSet{DIM, N, pde, S::nV, S::nP, S::P, S::F, false, &predictor, &riemann, &boundary, &corrector,
+                     nullptr};
+  }
+};
+
+// Launchers of a linear PDE (PDE::kLinear): the Cauchy-Kovalevski predictor
+// with the linear volume integral, the linear Riemann solver, and the
+// corrector with the linear surface integral. The predictor has one shape, so
+// the variant is ignored; there are no Picard sweeps to count. Boundary
+// conditions are not provided for linear PDEs (periodic meshes only).
+template <int DIM, int N, class PDE>
+struct LinearLaunch {
+  using CC = CorrectorCfg<DIM, N, PDE>;
+  using KC = CKCfg<DIM, N, PDE>;
+  static_assert(KC::SMEM <= 227 * 1024, "shared memory");
+  template <int MINB>
+  static int launch_ck(const double* luh, double* qb, double* fb, double* du, const double* dt, Geometry g, int n,
+                       const int* list, const int* cnt, double* qhi, double* fhi, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+      EXA_CUDA(cudaFuncSetAttribute(ck_predictor_kernel<DIM, N, PDE, MINB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KC::SMEM));
+      attr = true;
+    }
+    ck_predictor_kernel<DIM, N, PDE, MINB><<<(n + KC::CPB - 1) / KC::CPB, KC::THREADS, KC::SMEM, st>>>(
+        luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  // variant 0: register budget of one block per SM; 1: of two blocks per SM
+  // (where their shared memory fits); the autotuner picks between them
+  static constexpr bool kTwo = 2 * KC::SMEM <= 227 * 1024;
+  static int predictor(const double* luh, double* qb, double* fb, double* du, int*, const double* dt, Geometry g,
+                       int n, const int* list, const int* cnt, PredictorTemps tmp, bool temps, unsigned long long*,
+                       int variant, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    double* qhi = temps ? tmp.lQhi : nullptr;
+    double* fhi = temps ? tmp.lFhi : nullptr;
+    if (variant == 1 && kTwo) return launch_ck<kTwo ? 2 : 1>(luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi, st);
+    return launch_ck<1>(luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi, st);
+  }
+  static int riemann(const double* qb, double* fb, const int* l, const int* r, const int* d, int n, const int* gate,
+                     cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    riemann_linear_kernel<DIM, N, PDE><<<(n + 3) / 4, 128, 0, st>>>(qb, fb, l, r, d, n, gate);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int boundary(const double*, double*, const int*, const int*, int n, int, const int*, cudaStream_t) {
+    if (n <= 0) return EXA_OK;
+    return fail(EXA_ERR_UNSUPPORTED, "boundary conditions: the linear kernels support periodic meshes only");
+  }
+  static int corrector(double* luh, const double* du, const double* fb, const double* dt, double* dtout, Geometry g,
+                       int n, const int* list, int upd, const int* cnt, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    corrector_kernel<DIM, N, PDE><<<(n + CC::CPB - 1) / CC::CPB, CC::THREADS, 0, st>>>(luh, du, fb, dt, dtout, g, n,
+                                                                                      list, upd, cnt);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int volume(double* du, const double* fhi, int n, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    const long long total = (long long)n * Shape<DIM, N, PDE>::P;
+    volume_linear_kernel<DIM, N, PDE><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(du, fhi, n);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static KernelSet make(int pde) {
+    using S = Shape<DIM, N, PDE>;
+    return KernelSet{DIM, N, pde, S::nV, S::nP, S::P, S::F, true, &predictor, &riemann, &boundary, &corrector,
+                     &volume};
   }
 };
 
 #define EXA_ORDERS_EULER(X, D) X(D, 3, EulerPDE, 0) X(D, 4, EulerPDE, 0) X(D, 5, EulerPDE, 0) X(D, 7, EulerPDE, 0)
 #define EXA_ORDERS_TEST(X, D) X(D, 3, EulerTestPDE, 1) X(D, 5, EulerTestPDE, 1)
+#define EXA_ORDERS_ELASTIC(X, D) X(D, 3, ElasticPDE, 2) X(D, 4, ElasticPDE, 2) X(D, 5, ElasticPDE, 2)
 
 static bool find_kernels(int dim, int order, int pde, KernelSet* out) {
 #define X(D, NN, PDE_, ID)                                     \
@@ -266,6 +342,14 @@ static bool find_kernels(int dim, int order, int pde, KernelSet* out) {
   EXA_ORDERS_EULER(X, 3)
   EXA_ORDERS_TEST(X, 2)
   EXA_ORDERS_TEST(X, 3)
+#undef X
+#define X(D, NN, PDE_, ID)                                     \
+  if (dim == D && order == NN && pde == ID) {                 \
+    *out = LinearLaunch<D, NN, PDE_>::make(ID);               \
+    return true;                                               \
+  }
+  EXA_ORDERS_ELASTIC(X, 2)
+  EXA_ORDERS_ELASTIC(X, 3)
 #undef X
   return false;
 }
@@ -400,6 +484,7 @@ int exa_space_time_predictor_nonlinear(const exa_solver* s, const double* luh, d
                                        const int* cell_list, int* iterations_dev, void* stream) {
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_nonlinear: null argument or negative count");
+  if (s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_nonlinear: linear PDE, use _linear");
   return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, cell_list, nullptr,
                         PredictorTemps{}, false, nullptr, s->variant, (cudaStream_t)stream);
 }
@@ -410,6 +495,8 @@ int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* 
                                              double* lQhi, double* lFhi, void* stream) {
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0 || !lQi || !lFi || !lQhi || !lFhi)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_nonlinear_temps: null argument or negative count");
+  if (s->k.linear)
+    return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_nonlinear_temps: linear PDE, use _linear_temps");
   return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, iterations_dev, dt_dev, geom(s, dx), ncells, nullptr, nullptr,
                         PredictorTemps{lQi, lFi, lQhi, lFhi}, true, nullptr, s->variant, (cudaStream_t)stream);
 }
@@ -418,7 +505,44 @@ int exa_riemann_solver_nonlinear(const exa_solver* s, const double* lQhbnd, doub
                                  const int* face_right, const int* face_dir, int nfaces, void* stream) {
   if (!s || !lQhbnd || !lFhbnd || nfaces < 0 || (nfaces > 0 && (!face_left || !face_right || !face_dir)))
     return fail(EXA_ERR_ARG, "exa_riemann_solver_nonlinear: null argument or negative count");
+  if (s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_riemann_solver_nonlinear: linear PDE, use _linear");
   return s->k.riemann(lQhbnd, lFhbnd, face_left, face_right, face_dir, nfaces, nullptr, (cudaStream_t)stream);
+}
+
+int exa_space_time_predictor_linear(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
+                                    double* lduh, const double* dt_dev, const double* dx, int ncells,
+                                    const int* cell_list, void* stream) {
+  if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0)
+    return fail(EXA_ERR_ARG, "exa_space_time_predictor_linear: null argument or negative count");
+  if (!s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_linear: nonlinear PDE");
+  return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, nullptr, dt_dev, geom(s, dx), ncells, cell_list, nullptr,
+                        PredictorTemps{}, false, nullptr, s->variant, (cudaStream_t)stream);
+}
+
+int exa_space_time_predictor_linear_temps(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
+                                          double* lduh, const double* dt_dev, const double* dx, int ncells,
+                                          double* lQhi, double* lFhi, void* stream) {
+  if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0 || !lQhi || !lFhi)
+    return fail(EXA_ERR_ARG, "exa_space_time_predictor_linear_temps: null argument or negative count");
+  if (!s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_linear_temps: nonlinear PDE");
+  return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, nullptr, dt_dev, geom(s, dx), ncells, nullptr, nullptr,
+                        PredictorTemps{nullptr, nullptr, lQhi, lFhi}, true, nullptr, s->variant,
+                        (cudaStream_t)stream);
+}
+
+int exa_riemann_solver_linear(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* face_left,
+                              const int* face_right, const int* face_dir, int nfaces, void* stream) {
+  if (!s || !lQhbnd || !lFhbnd || nfaces < 0 || (nfaces > 0 && (!face_left || !face_right || !face_dir)))
+    return fail(EXA_ERR_ARG, "exa_riemann_solver_linear: null argument or negative count");
+  if (!s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_riemann_solver_linear: nonlinear PDE");
+  return s->k.riemann(lQhbnd, lFhbnd, face_left, face_right, face_dir, nfaces, nullptr, (cudaStream_t)stream);
+}
+
+int exa_volume_integral_linear(const exa_solver* s, double* lduh, const double* lFhi, int ncells, void* stream) {
+  if (!s || !lduh || !lFhi || ncells < 0)
+    return fail(EXA_ERR_ARG, "exa_volume_integral_linear: null argument or negative count");
+  if (!s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_volume_integral_linear: nonlinear PDE");
+  return s->k.volume(lduh, lFhi, ncells, (cudaStream_t)stream);
 }
 
 int exa_boundary_conditions(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* bcell,
@@ -446,12 +570,13 @@ int exa_reset_min(double* dev, void* stream) {
 }
 
 // smooth synthetic states for the autotuner: rho, j, E with O(10%) variation
-__global__ void autotune_fill_kernel(double* luh, long long n, int nD) {
+// (parameters, v >= nV, positive: the elastic PDE divides by rho)
+__global__ void autotune_fill_kernel(double* luh, long long n, int nD, int nV) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long node = i / nD;
     const int v = (int)(i - node * nD);
     const double s = sin(0.37 * (double)node) * cos(0.011 * (double)node);
-    luh[i] = v == 0 ? 1.0 + 0.1 * s : v == 4 ? 2.5 + 0.2 * s : v < 4 ? 0.3 * s * (v - 2) : 0.0;
+    luh[i] = v >= nV ? 1.5 + 0.2 * s : v == 0 ? 1.0 + 0.1 * s : v == 4 ? 2.5 + 0.2 * s : v < 4 ? 0.3 * s * (v - 2) : 0.0;
   }
 }
 
@@ -483,7 +608,7 @@ int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chos
   }
   cudaStream_t st;
   EXA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  autotune_fill_kernel<<<1024, 256, 0, st>>>(luh, (long long)(n * P * nD), (int)nD);
+  autotune_fill_kernel<<<1024, 256, 0, st>>>(luh, (long long)(n * P * nD), (int)nD, (int)nV);
   Geometry g{};
   for (int d = 0; d < 3; d++) g.dx[d] = 1.0 / 27.0;
   reset_min_kernel<<<1, 1, 0, st>>>(dt);
@@ -494,7 +619,7 @@ int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chos
   int best = 0;
   double best_ms = 1e300;
   for (int v = 0; v < kAllVariants && rc == EXA_OK; v++) {
-    if (variant_is_mixed(v)) {  // changes the results: never chosen for the user
+    if (variant_is_mixed(v) || (k.linear && v > 1)) {  // mixed: changes the results; linear: two shapes
       if (variant_ms) variant_ms[v] = -1.0;
       continue;
     }
@@ -551,6 +676,8 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
     nc *= cells[d];
     const bool pl = bc[2 * d] == EXA_BC_PERIODIC, pr = bc[2 * d + 1] == EXA_BC_PERIODIC;
     if (pl != pr) return fail(EXA_ERR_ARG, "exa_mesh_create: periodic must be set on both faces of an axis");
+    if (s->k.linear && !pl)
+      return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create: the linear kernels support periodic meshes only");
     for (int f = 0; f < 2; f++) {
       const int k = bc[2 * d + f];
       if (k != EXA_BC_PERIODIC && k != EXA_BC_OUTFLOW && k != EXA_BC_REFLECTIVE)

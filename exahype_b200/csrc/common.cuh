@@ -13,11 +13,12 @@ constexpr int kMaxOrder = 9;
 constexpr int kMaxB = kMaxOrder + 1;
 
 // One order's 1-D operators, in constant memory. Layouts follow the reference
-// (kernels/DGMatrices.h:47-80): Kxi[k][l], iK1[l][n] row-major. (dudx is only
-// needed by non-conservative products, which no PDE here uses.)
+// (kernels/DGMatrices.h:47-80): Kxi[k][l], iK1[l][n], dudx[l][n] row-major
+// (dudx: derivative of basis function n at node l, used by the linear
+// predictor's spatial gradients).
 struct OrderTables {
   double w[kMaxB], x[kMaxB], FL[kMaxB], FR[kMaxB];
-  double Kxi[kMaxB * kMaxB], iK1[kMaxB * kMaxB];
+  double Kxi[kMaxB * kMaxB], iK1[kMaxB * kMaxB], dudx[kMaxB * kMaxB];
   double lobatto[kMaxB];
   // FP32 copy of Kxi for the mixed-precision Picard sweeps
   float Kxi_f[kMaxB * kMaxB];

@@ -1,0 +1,275 @@
+// Linear ADER-DG kernels for PDEs given by a non-conservative product
+// (PDE::kLinear, e.g. ElasticPDE):
+//   ck_predictor_kernel    spaceTimePredictorLinear (2d/spaceTimePredictorLinear.cpph:35-409,
+//                          3d/spaceTimePredictorLinear.cpph:34-446) + volumeIntegralLinear
+//                          (3d/volumeIntegralLinear.cpph:20-52)
+//   riemann_linear_kernel  riemannSolverLinear (3d/riemannSolverLinear.cpph:20-136)
+//   volume_linear_kernel   volumeIntegralLinear on its own (kernel-level entry point)
+// The surface integral is the corrector's linear form (aderdg.cuh).
+//
+// The predictor is the Cauchy-Kovalevski procedure: time derivative i+1 of
+// the solution is -sum_d B_d(Q_i) grad_d Q_i, evaluated b times; the time
+// averages over [0, dt] weight derivative i by dt^i / (i+1)!. Per derivative
+// level the cell's state sits in shared memory; the gradients are 1-D line
+// contractions with dudx (one thread per (direction, line, variable)), the
+// non-conservative product and both time averages are per node (one thread
+// per node, accumulators in registers). No iteration and no convergence test.
+#pragma once
+#include "aderdg.cuh"
+
+namespace exa {
+
+template <int DIM, int N, class PDE>
+struct CKCfg : Shape<DIM, N, PDE> {
+  using S = Shape<DIM, N, PDE>;
+  static constexpr int CPB = cells_per_block<S::P>();
+  static constexpr int THREADS = CPB * S::P;
+  static constexpr int LINES = S::P / S::b;          // lines per direction
+  static constexpr int QS = S::nD | 1;               // node stride of the state (odd: no bank conflicts)
+  static constexpr int GS = (DIM * S::nV) | 1;       // node stride of the gradients [d][nV]
+  static constexpr int SQ = S::P * QS, SG = S::P * GS;
+  static constexpr size_t SMEM = sizeof(double) * (size_t)CPB * (SQ + SG);
+  static constexpr int GITEMS = CPB * DIM * LINES * S::nV;  // gradient line items per block
+};
+
+// node of line L along direction d at position n; L enumerates the other
+// coordinates in (z, y, x) order (face-node order of the reference)
+template <int DIM, int b>
+__device__ __forceinline__ int line_node(int d, int L, int n) {
+  const int a0 = L / b, a1 = L % b;
+  if (DIM == 2) return d == 0 ? L * b + n : n * b + L;
+  return d == 0 ? (a0 * b + a1) * b + n : d == 1 ? (a0 * b + n) * b + a1 : (n * b + a0) * b + a1;
+}
+
+template <int DIM, int N, class PDE, int MINB = 1>
+__global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS, MINB)
+    ck_predictor_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
+                        double* __restrict__ lduh, const double* __restrict__ dt_ptr, Geometry geo, int ncells,
+                        const int* __restrict__ cell_list, const int* __restrict__ count,
+                        double* __restrict__ lQhi_out, double* __restrict__ lFhi_out) {
+  using C = CKCfg<DIM, N, PDE>;
+  constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, QS = C::QS, GS = C::GS;
+  constexpr int F = C::F;
+  extern __shared__ double smem[];
+  const OrderTables& T = c_tab[N];
+  const int lc = threadIdx.x / P;
+  const int p = threadIdx.x - lc * P;
+  const int slot = blockIdx.x * C::CPB + lc;
+  const int nact = count ? min(*count, ncells) : ncells;
+  const bool active = slot < nact;
+  const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
+  double* sQ = smem + lc * C::SQ;
+  double* sG = smem + C::CPB * C::SQ + lc * C::SG;
+  const int inst = cell_instance(geo, cell);
+  const double dt = dt_ptr[inst];
+  __shared__ double s_idx[C::CPB][3];
+  __shared__ int s_cell[C::CPB];
+  if (p == 0) {
+    s_cell[lc] = active ? cell : -1;
+#pragma unroll
+    for (int d = 0; d < 3; d++) s_idx[lc][d] = d < DIM ? 1.0 / cell_width(geo, inst, d) : 0.0;
+  }
+  // level 0: the solution (parameters included); inactive slots get unit
+  // parameters so that their arithmetic stays finite
+  double qh[nV];
+  {
+#pragma unroll
+    for (int v = 0; v < nD; v++) {
+      const double q = active ? __ldg(luh + ((size_t)cell * P + p) * nD + v) : (v < nV ? 0.0 : 1.0);
+      sQ[p * QS + v] = q;
+      if (v < nV) qh[v] = q;
+    }
+  }
+  double fh[DIM][nV];
+  double fac_i = 0.0, fac_n = 0.5 * dt;  // weights of levels i and i+1 in the time averages
+  for (int i = 0; i < b; i++) {
+    __syncthreads();  // level i complete in sQ; previous per-node phase done with sG
+    // spatial gradients of level i, one line per item, into sG[node][d][v]
+    for (int it = threadIdx.x; it < C::GITEMS; it += C::THREADS) {
+      const int v = it % nV;
+      const int L = (it / nV) % LINES;
+      const int d = (it / (nV * LINES)) % DIM;
+      const int c = it / (nV * LINES * DIM);
+      if (s_cell[c] < 0) continue;
+      const double* q = smem + c * C::SQ;
+      double* g = smem + C::CPB * C::SQ + c * C::SG;
+      const double idx = s_idx[c][d];
+      double f[b];
+#pragma unroll
+      for (int n = 0; n < b; n++) f[n] = idx * q[line_node<DIM, b>(d, L, n) * QS + v];
+#pragma unroll
+      for (int l = 0; l < b; l++) {
+        double s = 0.0;
+#pragma unroll
+        for (int n = 0; n < b; n++) s = fma(f[n], T.dudx[l * b + n], s);
+        g[line_node<DIM, b>(d, L, l) * GS + d * nV + v] = s;
+      }
+    }
+    __syncthreads();
+    // per node: non-conservative product, time averages, next level
+    {
+      double B[DIM][nV];
+      PDE::template ncp<DIM>(sQ + p * QS, reinterpret_cast<const double(*)[nV]>(sG + p * GS), B);
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int v = 0; v < nV; v++) fh[d][v] = i == 0 ? B[d][v] : fma(fac_i, B[d][v], fh[d][v]);
+      if (i + 1 < b) {
+#pragma unroll
+        for (int v = 0; v < nV; v++) {
+          double qn = 0.0;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) qn -= B[d][v];
+          qh[v] = fma(fac_n, qn, qh[v]);
+          sQ[p * QS + v] = qn;  // own node only; parameters stay
+        }
+      }
+      fac_i = fac_n;
+      fac_n = fac_n * (dt / (i + 3));
+    }
+  }
+  __syncthreads();
+  // stage the time averages for the extrapolation: lQhi in sQ, lFhi in sG
+#pragma unroll
+  for (int v = 0; v < nV; v++) sQ[p * QS + v] = qh[v];
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+#pragma unroll
+    for (int v = 0; v < nV; v++) sG[p * GS + d * nV + v] = fh[d][v];
+  if (active) {
+    if (lduh) {  // volumeIntegralLinear
+      const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
+      const double w = (DIM == 3 ? T.w[z] * T.w[y] : T.w[y]) * T.w[x];
+#pragma unroll
+      for (int v = 0; v < nV; v++) {
+        double du = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) du -= w * fh[d][v];
+        lduh[((size_t)cell * P + p) * nV + v] = du;
+      }
+    }
+    if (lQhi_out)
+      for (int v = 0; v < nD; v++) lQhi_out[((size_t)cell * P + p) * nD + v] = sQ[p * QS + v];
+    if (lFhi_out)
+      for (int d = 0; d < DIM; d++)
+        for (int v = 0; v < nV; v++) lFhi_out[(((size_t)cell * DIM + d) * P + p) * nV + v] = fh[d][v];
+  }
+  __syncthreads();
+  // boundary extrapolation: states (parameters included) and normal fluxes
+  constexpr int QITEMS = C::CPB * DIM * LINES * nD;
+  for (int it = threadIdx.x; it < QITEMS; it += C::THREADS) {
+    const int v = it % nD;
+    const int L = (it / nD) % LINES;
+    const int d = (it / (nD * LINES)) % DIM;
+    const int c = it / (nD * LINES * DIM);
+    const int cc = s_cell[c];
+    if (cc < 0) continue;
+    const double* q = smem + c * C::SQ;
+    double sl = 0.0, sr = 0.0;
+#pragma unroll
+    for (int l = 0; l < b; l++) {
+      const double x = q[line_node<DIM, b>(d, L, l) * QS + v];
+      sl += x * T.FL[l];
+      sr += x * T.FR[l];
+    }
+    lQhbnd[(((size_t)cc * 2 * DIM + 2 * d) * F + L) * nD + v] = sl;
+    lQhbnd[(((size_t)cc * 2 * DIM + 2 * d + 1) * F + L) * nD + v] = sr;
+  }
+  constexpr int FITEMS = C::CPB * DIM * LINES * nV;
+  for (int it = threadIdx.x; it < FITEMS; it += C::THREADS) {
+    const int v = it % nV;
+    const int L = (it / nV) % LINES;
+    const int d = (it / (nV * LINES)) % DIM;
+    const int c = it / (nV * LINES * DIM);
+    const int cc = s_cell[c];
+    if (cc < 0) continue;
+    const double* g = smem + C::CPB * C::SQ + c * C::SG;
+    double sl = 0.0, sr = 0.0;
+#pragma unroll
+    for (int l = 0; l < b; l++) {
+      const double x = g[line_node<DIM, b>(d, L, l) * GS + d * nV + v];
+      sl += x * T.FL[l];
+      sr += x * T.FR[l];
+    }
+    lFhbnd[(((size_t)cc * 2 * DIM + 2 * d) * F + L) * nV + v] = sl;
+    lFhbnd[(((size_t)cc * 2 * DIM + 2 * d + 1) * F + L) * nV + v] = sr;
+  }
+}
+
+// riemannSolverLinear, one warp per interior face: face averages of both
+// sides (parameters included), smax from the eigenvalues of both averages,
+// the system matrix Bn once in their mean, then per face node
+// FL = (Bn - smax I)^T dQ and FR = (Bn + smax I)^T dQ with dQ = (QR - QL) / 2.
+// FL goes to the left cell's face 2 dir + 1, FR to the right cell's face
+// 2 dir; the extrapolated fluxes there are not read.
+template <int DIM, int N, class PDE>
+__global__ void __launch_bounds__(128) riemann_linear_kernel(const double* __restrict__ lQhbnd,
+                                                             double* __restrict__ lFhbnd,
+                                                             const int* __restrict__ face_left,
+                                                             const int* __restrict__ face_right,
+                                                             const int* __restrict__ face_dir, int nfaces,
+                                                             const int* __restrict__ gate = nullptr) {
+  using S = Shape<DIM, N, PDE>;
+  constexpr int F = S::F, nV = S::nV, nD = S::nD;
+  __shared__ double sB[4][nV * nV];
+  __shared__ double sDQ[4][F * nV];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int f = blockIdx.x * (blockDim.x >> 5) + w;
+  if (gate && !*gate) return;
+  if (f >= nfaces) return;
+  const int cl = face_left[f], cr = face_right[f], dir = face_dir[f];
+  const double* QL = lQhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nD;
+  const double* QR = lQhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nD;
+  double* FL = lFhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nV;
+  double* FR = lFhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nV;
+  double aL[nD], aR[nD];
+  face_average<DIM, N, PDE>(QL, lane, aL);
+  face_average<DIM, N, PDE>(QR, lane, aR);
+  const double smax = face_smax<DIM, PDE>(aL, aR, dir);
+  if (lane == 0) {
+    double av[nD];
+#pragma unroll
+    for (int k = 0; k < nD; k++) av[k] = 0.5 * (aL[k] + aR[k]);
+    PDE::coefficient_matrix(av, dir, sB[w]);
+  }
+  for (int e = lane; e < F * nV; e += 32) {
+    const int fn = e / nV, k = e - fn * nV;
+    sDQ[w][e] = 0.5 * (QR[fn * nD + k] - QL[fn * nD + k]);
+  }
+  __syncwarp();
+  for (int e = lane; e < F * nV; e += 32) {
+    const int fn = e / nV, j = e - fn * nV;
+    const double* dq = sDQ[w] + fn * nV;
+    double fl = 0.0, fr = 0.0;
+#pragma unroll
+    for (int k = 0; k < nV; k++) {
+      const double bkj = sB[w][k * nV + j];
+      fl = fma(k == j ? bkj - smax : bkj, dq[k], fl);
+      fr = fma(k == j ? bkj + smax : bkj, dq[k], fr);
+    }
+    FL[e] = fl;
+    FR[e] = fr;
+  }
+}
+
+// volumeIntegralLinear alone: lduh = -w_node sum_d lFhi[d], lFhi per cell [d][b^d][nV]
+template <int DIM, int N, class PDE>
+__global__ void volume_linear_kernel(double* __restrict__ lduh, const double* __restrict__ lFhi, int ncells) {
+  using S = Shape<DIM, N, PDE>;
+  constexpr int b = S::b, P = S::P, nV = S::nV;
+  const OrderTables& T = c_tab[N];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)ncells * P) return;
+  const int cell = (int)(i / P), p = (int)(i - (long long)cell * P);
+  const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
+  const double w = (DIM == 3 ? T.w[z] * T.w[y] : T.w[y]) * T.w[x];
+#pragma unroll
+  for (int v = 0; v < nV; v++) {
+    double du = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) du -= w * lFhi[(((size_t)cell * DIM + d) * P + p) * nV + v];
+    lduh[((size_t)cell * P + p) * nV + v] = du;
+  }
+}
+
+}  // namespace exa

@@ -25,6 +25,7 @@ struct EulerPDE {
   static constexpr int nVar = 5;
   static constexpr int nPar = 0;
   static constexpr int nObs = 5;
+  static constexpr bool kLinear = false;  // nonlinear kernels (Picard predictor, Rusanov on fluxes)
 
   __host__ __device__ static double pressure(const double* Q, double irho) {
     const double GAMMA = 1.4;
@@ -118,6 +119,7 @@ struct EulerTestPDE {
   static constexpr int nVar = 5;
   static constexpr int nPar = 1;
   static constexpr int nObs = 5;
+  static constexpr bool kLinear = false;
 
   template <int DIM>
   __host__ __device__ static double pressure(const double* Q, double irho) {
@@ -183,6 +185,100 @@ struct EulerTestPDE {
     if (obsMin[0] <= 0.0) return false;
     if (obsMin[4] <= 0.0) return false;
     return true;
+  }
+};
+
+// Linear elastic waves in velocity-stress form, the PDE of the reference's
+// linear kernel tests (exahype/tests/kernels/c/ElasticityKernelTest2D.cpp:
+// 31-235): variables sxx syy szz sxy syz sxz u v w, material parameters
+// lambda mu rho. A linear PDE supplies what the reference's linear kernels
+// ask of the user solver instead of a flux:
+//   ncp<DIM>(Q, gradQ[DIM][nVar], BgradQ[DIM][nVar]) -- nonConservativeProduct
+//                                                       (BgradQ a DIM x nVar tensor)
+//   coefficient_matrix(Q, d, Bn[nVar][nVar])          -- coefficientMatrix
+//   eigenvalues(Q, d, lambda)                         -- eigenvalues
+// with (BgradQ_d)_k = sum_l Bn_d[l][k] (gradQ_d)_l. The z-direction parts are
+// the ones written out (commented) beside the x and y parts in the test.
+struct ElasticPDE {
+  static constexpr int nVar = 9;
+  static constexpr int nPar = 3;
+  static constexpr int nObs = 9;
+  static constexpr bool kLinear = true;
+
+  template <int DIM>
+  __device__ static void ncp(const double* Q, const double (*G)[nVar], double (*B)[nVar]) {
+    const double lam = Q[9], mu = Q[10], irho = 1.0 / Q[11];
+    const double lm2 = lam + 2 * mu;
+    B[0][0] = -lm2 * G[0][6];
+    B[0][1] = -lam * G[0][6];
+    B[0][2] = -lam * G[0][6];
+    B[0][3] = -mu * G[0][7];
+    B[0][4] = 0.0;
+    B[0][5] = -mu * G[0][8];
+    B[0][6] = -irho * G[0][0];
+    B[0][7] = -irho * G[0][3];
+    B[0][8] = -irho * G[0][5];
+    B[1][0] = -lam * G[1][7];
+    B[1][1] = -lm2 * G[1][7];
+    B[1][2] = -lam * G[1][7];
+    B[1][3] = -mu * G[1][6];
+    B[1][4] = -mu * G[1][8];
+    B[1][5] = 0.0;
+    B[1][6] = -irho * G[1][3];
+    B[1][7] = -irho * G[1][1];
+    B[1][8] = -irho * G[1][4];
+    if (DIM == 3) {
+      B[DIM - 1][0] = -lam * G[DIM - 1][8];
+      B[DIM - 1][1] = -lam * G[DIM - 1][8];
+      B[DIM - 1][2] = -lm2 * G[DIM - 1][8];
+      B[DIM - 1][3] = 0.0;
+      B[DIM - 1][4] = -mu * G[DIM - 1][7];
+      B[DIM - 1][5] = -mu * G[DIM - 1][6];
+      B[DIM - 1][6] = -irho * G[DIM - 1][5];
+      B[DIM - 1][7] = -irho * G[DIM - 1][4];
+      B[DIM - 1][8] = -irho * G[DIM - 1][2];
+    }
+  }
+
+  // Bn row-major [l][k], all other entries zero
+  __device__ static void coefficient_matrix(const double* Q, int d, double* Bn) {
+    for (int i = 0; i < nVar * nVar; i++) Bn[i] = 0.0;
+    const double lam = Q[9], mu = Q[10], irho = 1.0 / Q[11];
+    const double lm2 = lam + 2 * mu;
+    if (d == 0) {
+      Bn[6 * 9 + 0] = -lm2; Bn[6 * 9 + 1] = -lam; Bn[6 * 9 + 2] = -lam; Bn[7 * 9 + 3] = -mu; Bn[8 * 9 + 5] = -mu;
+      Bn[0 * 9 + 6] = -irho; Bn[3 * 9 + 7] = -irho; Bn[5 * 9 + 8] = -irho;
+    } else if (d == 1) {
+      Bn[7 * 9 + 0] = -lam; Bn[7 * 9 + 1] = -lm2; Bn[7 * 9 + 2] = -lam; Bn[6 * 9 + 3] = -mu; Bn[8 * 9 + 4] = -mu;
+      Bn[3 * 9 + 6] = -irho; Bn[1 * 9 + 7] = -irho; Bn[4 * 9 + 8] = -irho;
+    } else {
+      Bn[8 * 9 + 0] = -lam; Bn[8 * 9 + 1] = -lam; Bn[8 * 9 + 2] = -lm2; Bn[7 * 9 + 4] = -mu; Bn[6 * 9 + 5] = -mu;
+      Bn[5 * 9 + 6] = -irho; Bn[4 * 9 + 7] = -irho; Bn[2 * 9 + 8] = -irho;
+    }
+  }
+
+  __device__ static void eigenvalues(const double* Q, int /*d*/, double* lambda) {
+    const double lam = Q[9], mu = Q[10], rho = Q[11];
+    const double cp = sqrt((lam + 2 * mu) / rho);
+    const double cs = sqrt(mu / rho);
+    lambda[0] = -cp;
+    lambda[1] = -cs;
+    lambda[2] = -cs;
+    lambda[3] = 0.0;
+    lambda[4] = 0.0;
+    lambda[5] = 0.0;
+    lambda[6] = cs;
+    lambda[7] = cs;
+    lambda[8] = cp;
+  }
+
+  // max_v |lambda_v| with round-to-nearest operations (max(cp, cs) is exact
+  // in any order), so that the time step matches the reference bit for bit
+  __device__ static double max_abs_eigenvalue_exact(const double* Q, int /*d*/) {
+    const double lam = Q[9], mu = Q[10], rho = Q[11];
+    const double cp = __dsqrt_rn(__ddiv_rn(__dadd_rn(lam, __dmul_rn(2.0, mu)), rho));
+    const double cs = __dsqrt_rn(__ddiv_rn(mu, rho));
+    return (cp < cs) ? cs : cp;
   }
 };
 

@@ -41,6 +41,7 @@ extern "C" {
 /* PDE identifiers. */
 #define EXA_PDE_EULER 0      /* compressible Euler, 5 variables (EulerADERDG demonstrator) */
 #define EXA_PDE_EULER_TEST 1 /* the reference kernel tests' mock Euler with one parameter */
+#define EXA_PDE_ELASTIC 2    /* linear elastic waves, 9 variables + 3 parameters (lambda, mu, rho); linear kernels */
 
 /* Boundary kinds for exa_boundary_conditions / exa_mesh_create. */
 #define EXA_BC_PERIODIC (-1)
@@ -105,6 +106,34 @@ int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* 
  * (ADERDGSolver::solveRiemannProblemAtInterface, ADERDGSolver.cpp:2789-2866). */
 int exa_riemann_solver_nonlinear(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* face_left,
                                  const int* face_right, const int* face_dir, int nfaces, void* stream);
+/* Linear kernels, for solvers of a linear PDE (EXA_PDE_ELASTIC; the reference's
+ * generated glue calls them when the solver is linear,
+ * AbstractGenericADERDGSolverImplementation.template:53-54,85-86,101-149).
+ * The nonlinear entry points above reject a linear solver and vice versa;
+ * exa_corrector applies the linear surface integral for a linear solver.
+ *
+ * spaceTimePredictorLinear (Kernels.h, c/{2d,3d}/spaceTimePredictorLinear.cpph;
+ * Cauchy-Kovalevski with the PDE's non-conservative product) and, when lduh
+ * is not NULL, volumeIntegralLinear; arguments as for the nonlinear
+ * predictor. */
+int exa_space_time_predictor_linear(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
+                                    double* lduh, const double* dt_dev, const double* dx, int ncells,
+                                    const int* cell_list, void* stream);
+/* As above, also writing the time averages per cell (golden-vector replay):
+ * lQhi [b^d][nD] and lFhi [d][b^d][nV] (the reference's tempUnknowns and
+ * tempFluxUnknowns). */
+int exa_space_time_predictor_linear_temps(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
+                                          double* lduh, const double* dt_dev, const double* dx, int ncells,
+                                          double* lQhi, double* lFhi, void* stream);
+/* riemannSolverLinear (c/{2d,3d}/riemannSolverLinear.cpph) for nfaces
+ * interior faces, face arrays as for exa_riemann_solver_nonlinear: the
+ * fluctuations (Bn -/+ smax I)^T (QR - QL)/2 are written to the left / right
+ * cell's lFhbnd slot (the extrapolated fluxes there are not read). */
+int exa_riemann_solver_linear(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* face_left,
+                              const int* face_right, const int* face_dir, int nfaces, void* stream);
+/* volumeIntegralLinear (c/{2d,3d}/volumeIntegralLinear.cpph) on its own:
+ * lduh = -w sum_d lFhi[d], lFhi per cell [d][b^d][nV]. */
+int exa_volume_integral_linear(const exa_solver* s, double* lduh, const double* lFhi, int ncells, void* stream);
 /* boundaryConditions + riemannSolver on boundary faces (ADERDGSolver::
  * applyBoundaryConditions, ADERDGSolver.cpp:2893-2962): face f is face
  * bface[f] of cell bcell[f]; kind is EXA_BC_OUTFLOW or EXA_BC_REFLECTIVE. */

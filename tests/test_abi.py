@@ -21,7 +21,8 @@ def declared_functions():
 def test_header_declares_the_api():
     names = declared_functions()
     for required in ("exa_space_time_predictor_nonlinear", "exa_riemann_solver_nonlinear", "exa_boundary_conditions",
-                     "exa_corrector", "exa_mesh_create", "exa_mesh_step", "exa_solver_create"):
+                     "exa_corrector", "exa_mesh_create", "exa_mesh_step", "exa_solver_create",
+                     "exa_space_time_predictor_linear", "exa_riemann_solver_linear", "exa_volume_integral_linear"):
         assert required in names
 
 
