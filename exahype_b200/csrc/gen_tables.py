@@ -16,6 +16,11 @@ tables:
   (DGMatrices.h:58). The reference prints these three with 13 significant
   digits (DGMatrices.cpp:257-288); the same rounding is applied here so that
   the GPU path multiplies by the same numbers as the reference.
+* ``fineGridProjector1d[j][n][m] = phi_n((j + x_m)/3)`` (AMR prolongation and
+  restriction between a cell and its thirds, DGMatrices.h:109) and
+  ``equidistantGridProjector1d[n][i] = phi_n(i/N)`` (plotting at N+1
+  equidistant points, DGMatrices.h:99), both with 13 significant digits as
+  printed by the reference.
 * ``uh2lim[k][i]`` = mean of phi_k over subcell i of 2N+1,
   ``uh2lob[j][i] = phi_j(lobatto_i)``, and ``lim2uh[i][j]``, the constrained
   least-squares inverse of uh2lim that conserves the cell mean
@@ -167,7 +172,13 @@ def build(N):
         rhs = [2 * uh2lim[j][i] for j in range(b)] + [dxi]
         for j in range(b):
             lim2uh[i][j] = sum(ainv[k][j] * rhs[k] for k in range(b + 1))
+    # AMR: fine[j][n][m] = phi_n((j + x_m) / 3), basis n of the coarse cell at
+    # node m of its j-th third; plotting: equi[n][i] = phi_n(i / N)
+    fine = [[[lagrange(x, n, (j + x[m]) / 3) for m in range(b)] for n in range(b)] for j in range(3)]
+    equi = [[lagrange(x, n, Decimal(i) / N) for i in range(b)] for n in range(b)]
     return dict(
+        fineGridProjector1d=[sig(fine[j][n][m], 13) for j in range(3) for n in range(b) for m in range(b)],
+        equidistantGridProjector1d=[sig(equi[n][i], 13) for n in range(b) for i in range(b)],
         nodes=[float(v) for v in x], weights=[float(v) for v in w],
         lobatto_nodes=[float(v) for v in xl], lobatto_weights=[float(v) for v in wl],
         FLCoeff=[float(v) for v in FL], FRCoeff=[float(v) for v in FR],
@@ -182,7 +193,7 @@ def build(N):
 
 
 NAMES = ["nodes", "weights", "lobatto_nodes", "lobatto_weights", "FLCoeff", "FRCoeff", "FCoeff",
-         "Kxi", "iK1", "dudx", "uh2lim", "lim2uh", "uh2lob"]
+         "Kxi", "iK1", "dudx", "uh2lim", "lim2uh", "uh2lob", "fineGridProjector1d", "equidistantGridProjector1d"]
 
 
 def all_tables():

@@ -24,7 +24,7 @@
 const double* orc_table(const char* name, int N) {
 #define T(nm) if (!strcmp(name, #nm)) return exa_tab_##nm + exa_tab_##nm##_off[N];
   T(nodes) T(weights) T(lobatto_nodes) T(lobatto_weights) T(FLCoeff) T(FRCoeff) T(FCoeff) T(Kxi) T(iK1)
-  T(dudx) T(uh2lim) T(lim2uh) T(uh2lob)
+  T(dudx) T(uh2lim) T(lim2uh) T(uh2lob) T(fineGridProjector1d) T(equidistantGridProjector1d)
 #undef T
   return 0;
 }

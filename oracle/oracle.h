@@ -57,6 +57,22 @@ void orc_lin_volume_integral(const orc_solver* s, double* lduh, const double* lF
 void orc_lin_surface_integral(const orc_solver* s, double* lduh, const double* lFhbnd, const double* dx);
 void orc_lin_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, const double* QR, int dir);
 
+/* AMR transfer operators (amr.c) between a cell / face and its descendant
+ * levelDelta levels finer; subcell / subface indices per axis in
+ * 0 .. 3^levelDelta - 1; nvar values per node (parameters included), nflux
+ * per flux node. Restrictions add to the coarse data. */
+void orc_volume_prolongation(int dim, int N, int nvar, double* luhFine, const double* luhCoarse, int levelDelta,
+                             const int* subcellIndex);
+void orc_volume_restriction(int dim, int N, int nvar, double* luhCoarse, const double* luhFine, int levelDelta,
+                            const int* subcellIndex);
+void orc_face_prolongation(int dim, int N, int nvar, int nflux, double* lQhbndFine, double* lFhbndFine,
+                           const double* lQhbndCoarse, const double* lFhbndCoarse, int levelDelta,
+                           const int* subfaceIndex);
+void orc_face_restriction(int dim, int N, int nvar, int nflux, double* lQhbndCoarse, double* lFhbndCoarse,
+                          const double* lQhbndFine, const double* lFhbndFine, int levelDelta, const int* subfaceIndex);
+/* one cell's values at the (N+1)^d equidistant points (plotters) */
+void orc_equidistant_projection(int dim, int N, int nvar, const double* luh, double* out);
+
 /* table access (generated dg_tables.h) */
 const double* orc_table(const char* name, int order);
 

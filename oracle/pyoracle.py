@@ -384,3 +384,60 @@ class _Prefixed:
 
     def __getattr__(self, name):
         return getattr(self._lib, self._pre + name.replace("orc_lmesh_", ""))
+
+
+# ---- AMR transfer operators and the plotter's vertex projection ---------------
+AMR_OPS = {"volume_prolongation": 0, "volume_restriction": 1, "face_prolongation": 2, "face_restriction": 3}
+
+
+def amr(op, dim, N, nvar, npar, levelDelta, index, coarse=None, fine=None, coarse_flux=None, fine_flux=None,
+        impl="oracle"):
+    """One AMR transfer of the C restatement (impl='oracle') or of the
+    reference's amrRoutines (impl='ref'). Volume data [b^d][nvar+npar], face
+    states [b^(d-1)][nvar+npar] and fluxes [b^(d-1)][nvar]. Prolongations
+    return the fine data (state, flux for faces); restrictions return the
+    coarse data plus the restriction (the inputs `coarse`, `coarse_flux`
+    are what is added to)."""
+    b = N + 1
+    nd = nvar + npar
+    vol, face = b ** dim * nd, b ** (dim - 1) * nd
+    ff = b ** (dim - 1) * nvar
+    idx = (ctypes.c_int * 3)(*(list(index) + [0] * (3 - len(index))))
+    arr = lambda a, n: np.ascontiguousarray(np.zeros(n) if a is None else np.array(a, dtype=np.float64).reshape(-1))
+    k = AMR_OPS[op]
+    if k == 0:
+        out, src, o2, s2 = arr(None, vol), arr(coarse, vol), None, None
+    elif k == 1:
+        out, src, o2, s2 = arr(coarse, vol), arr(fine, vol), None, None
+    elif k == 2:
+        out, src, o2, s2 = arr(None, face), arr(coarse, face), arr(None, ff), arr(coarse_flux, ff)
+    else:
+        out, src, o2, s2 = arr(coarse, face), arr(fine, face), arr(coarse_flux, ff), arr(fine_flux, ff)
+    if impl == "oracle":
+        L = lib()
+        if k == 0:
+            L.orc_volume_prolongation(dim, N, nd, _p(out), _p(src), levelDelta, idx)
+        elif k == 1:
+            L.orc_volume_restriction(dim, N, nd, _p(out), _p(src), levelDelta, idx)
+        elif k == 2:
+            L.orc_face_prolongation(dim, N, nd, nvar, _p(out), _p(o2), _p(src), _p(s2), levelDelta, idx)
+        else:
+            L.orc_face_restriction(dim, N, nd, nvar, _p(out), _p(o2), _p(src), _p(s2), levelDelta, idx)
+    else:
+        f = getattr(reflib(dim), "ref%dd_amr" % dim)
+        rc = f(k, nvar, npar, N, _p(out), _p(o2) if o2 is not None else None, _p(src),
+               _p(s2) if s2 is not None else None, levelDelta, idx)
+        assert rc == 0, "reference AMR routine not built for this shape"
+    return (out, o2) if k >= 2 else out
+
+
+def plot_vertices(dim, N, nvar, luh, impl="oracle"):
+    """one cell's values at the (N+1)^d equidistant plot vertices, x fastest"""
+    b = N + 1
+    u = np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)
+    out = np.zeros(b ** dim * nvar)
+    if impl == "oracle":
+        lib().orc_equidistant_projection(dim, N, nvar, _p(u), _p(out))
+    else:
+        getattr(reflib(dim), "ref%dd_plot_vertices" % dim)(N, nvar, _p(u), _p(out))
+    return out

@@ -410,6 +410,45 @@ void fv_boundary(double* lim, int face) {
   kernels::finitevolumes::commons::c::ghostLayerFillingAtBoundary<S>(s, lim, out, pos);
 }
 
+// ---- AMR transfer operators (amrRoutines.cpph) and the plotter's projection --
+template <int nV, int nP, int b>
+void amr_call(int op, double* a, double* bb, const double* c, const double* d, int levelDelta, const int* index) {
+  tarch::la::Vector<DIMENSIONS, int> cell;
+  tarch::la::Vector<DIMENSIONS - 1, int> face;
+  for (int k = 0; k < DIMENSIONS; k++) cell[k] = index[k];
+  for (int k = 0; k < DIMENSIONS - 1; k++) face[k] = index[k];
+  namespace K = kernels::aderdg::generic::c;
+  switch (op) {
+    case 0: K::volumeUnknownsProlongation<nV, nP, b>(a, c, 0, levelDelta, cell); break;
+    case 1: K::volumeUnknownsRestriction<nV, nP, b>(a, c, 0, levelDelta, cell); break;
+    case 2: K::faceUnknownsProlongation<nV, nP, b>(a, bb, c, d, 0, levelDelta, face); break;
+    default: K::faceUnknownsRestriction<nV, nP, b>(a, bb, c, d, 0, levelDelta, face); break;
+  }
+}
+
+// ADERDG2CartesianVTK::plotVertexData (exahype/plotters/VTK/ADERDG2CartesianVTK.cpp):
+// the solution at the (N+1)^d equidistant vertices of a cell, x fastest
+void plot_vertices(int N, int nvar, const double* u, double* out) {
+  const int b = N + 1, nz = DIMENSIONS == 3 ? b : 1;
+  for (int iz = 0; iz < nz; iz++)
+    for (int iy = 0; iy < b; iy++)
+      for (int ix = 0; ix < b; ix++)
+        for (int v = 0; v < nvar; v++) {
+          double acc = 0.0;
+          for (int gz = 0; gz < nz; gz++)
+            for (int gy = 0; gy < b; gy++)
+              for (int gx = 0; gx < b; gx++) {
+                const int g = (gz * b + gy) * b + gx;
+                acc += kernels::equidistantGridProjector1d[N][gy][iy] * kernels::equidistantGridProjector1d[N][gx][ix] *
+#if DIMENSIONS == 3
+                       kernels::equidistantGridProjector1d[N][gz][iz] *
+#endif
+                       u[g * nvar + v];
+              }
+          out[((iz * b + iy) * b + ix) * nvar + v] = acc;
+        }
+}
+
 }  // namespace
 
 #define DISPATCH_ELASTIC(N, call)                                        \
@@ -499,6 +538,11 @@ int REFNAME(table)(const char* name, int N, double* out) {
   else if (!std::strcmp(name, "uh2lim")) { for (int i = 0; i < b * bl; i++) out[k++] = kernels::uh2lim[N][i]; }
   else if (!std::strcmp(name, "lim2uh")) { for (int i = 0; i < b * bl; i++) out[k++] = kernels::lim2uh[N][i]; }
   else if (!std::strcmp(name, "uh2lob")) { for (int i = 0; i < b * b; i++) out[k++] = kernels::uh2lob[N][i]; }
+  else if (!std::strcmp(name, "fineGridProjector1d")) {
+    for (int j = 0; j < 3; j++) for (int n = 0; n < b; n++) for (int m = 0; m < b; m++) out[k++] = kernels::fineGridProjector1d[N][j][n][m];
+  } else if (!std::strcmp(name, "equidistantGridProjector1d")) {
+    for (int n = 0; n < b; n++) for (int i = 0; i < b; i++) out[k++] = kernels::equidistantGridProjector1d[N][n][i];
+  }
   else return -1;
   return k;
 }
@@ -565,6 +609,35 @@ double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx) {
   if (pde == 2) DISPATCH_ELASTIC(N, r = stable_dt<S>(luh, dx));
   else DISPATCH(pde, N, r = stable_dt<S>(luh, dx));
   return r;
+}
+
+// op: 0 volume prolongation (a = fine, c = coarse), 1 volume restriction
+// (a = coarse += , c = fine), 2 face prolongation (a, bb = fine state, flux;
+// c, d = coarse), 3 face restriction (a, bb = coarse +=; c, d = fine);
+// (nv, np) = variables, parameters
+int REFNAME(amr)(int op, int nv, int np, int N, double* a, double* bb, const double* c, const double* d,
+                 int levelDelta, const int* index) {
+  REFNAME(init)();
+#define AMR_N(NV, NP)                                                                           \
+  if (nv == NV && np == NP) {                                                                   \
+    switch (N) {                                                                                \
+      case 3: amr_call<NV, NP, 4>(op, a, bb, c, d, levelDelta, index); return 0;                \
+      case 4: amr_call<NV, NP, 5>(op, a, bb, c, d, levelDelta, index); return 0;                \
+      case 5: amr_call<NV, NP, 6>(op, a, bb, c, d, levelDelta, index); return 0;                \
+      default: return -1;                                                                       \
+    }                                                                                           \
+  }
+  AMR_N(5, 0)
+  AMR_N(5, 1)
+  AMR_N(9, 3)
+  AMR_N(1, 1)
+#undef AMR_N
+  return -1;
+}
+
+void REFNAME(plot_vertices)(int N, int nvar, const double* u, double* out) {
+  REFNAME(init)();
+  plot_vertices(N, nvar, u, out);
 }
 
 void REFNAME(lin_predictor)(int pde, int N, const double* luh, const double* dx, double dt, double* lQhbnd,

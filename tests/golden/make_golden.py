@@ -79,7 +79,7 @@ def make_ref_tables():
     buf = (ctypes.c_double * 512)()
     out = {}
     for name in ("nodes", "weights", "lobatto_nodes", "lobatto_weights", "FLCoeff", "FRCoeff", "FCoeff", "Kxi",
-                 "iK1", "dudx", "uh2lim", "lim2uh", "uh2lob"):
+                 "iK1", "dudx", "uh2lim", "lim2uh", "uh2lob", "fineGridProjector1d", "equidistantGridProjector1d"):
         for N in range(1, 10):
             n = lib.ref2d_table(name.encode(), N, buf)
             out["%s/%d" % (name, N)] = np.array(buf[:n])

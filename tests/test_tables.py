@@ -17,11 +17,11 @@ REF = np.load(os.path.join(REPO, "tests", "golden", "ref_tables.npz"))
 
 @pytest.mark.parametrize("N", [3, 5])
 def test_13_digit_operators_bit_identical(N):
-    """Kxi, iK1, dudx and FCoeff are stored by the reference with 13
+    """Kxi, iK1, dudx, FCoeff and fineGridProjector1d are stored by the reference with 13
     significant digits; rounding the exact operators the same way reproduces
     them bit for bit for the orders the workloads use."""
     t = gen_tables.build(N)
-    for name in ("Kxi", "iK1", "dudx", "FCoeff"):
+    for name in ("Kxi", "iK1", "dudx", "FCoeff", "fineGridProjector1d"):
         assert np.array_equal(np.array(t[name]), REF["%s/%d" % (name, N)]), name
 
 
@@ -34,7 +34,8 @@ def test_all_tables_close(N):
         assert mine.shape == ref.shape, name
         # the reference's 16-digit quadrature/extrapolation values carry ~1e-15
         # of numerical error; 13-digit tables may differ in the last digit
-        atol = 2e-13 if name in ("Kxi", "iK1", "dudx", "FCoeff") else 1e-14
+        atol = 2e-13 if name in ("Kxi", "iK1", "dudx", "FCoeff", "fineGridProjector1d",
+                                 "equidistantGridProjector1d") else 1e-14
         np.testing.assert_allclose(mine, ref, rtol=3e-12, atol=atol, err_msg=name)
 
 
