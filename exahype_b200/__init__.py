@@ -152,6 +152,39 @@ class Solver:
         _check(load().exa_volume_integral_linear(self._h, _ptr(lduh), _ptr(lFhi), int(ncells), _stream(stream)),
                "exa_volume_integral_linear")
 
+    # -- AMR transfers and the plotter's vertex projection (device arrays) --
+    def volume_unknowns_prolongation(self, luh_fine, luh_coarse, n, fine_cell, coarse_cell, level_delta,
+                                     subcell_index, stream=None):
+        _check(load().exa_volume_unknowns_prolongation(self._h, _ptr(luh_fine), _ptr(luh_coarse), int(n),
+                                                       _ptr(fine_cell), _ptr(coarse_cell), _ptr(level_delta),
+                                                       _ptr(subcell_index), _stream(stream)),
+               "exa_volume_unknowns_prolongation")
+
+    def volume_unknowns_restriction(self, luh_coarse, luh_fine, n, fine_cell, coarse_cell, level_delta,
+                                    subcell_index, stream=None):
+        _check(load().exa_volume_unknowns_restriction(self._h, _ptr(luh_coarse), _ptr(luh_fine), int(n),
+                                                      _ptr(fine_cell), _ptr(coarse_cell), _ptr(level_delta),
+                                                      _ptr(subcell_index), _stream(stream)),
+               "exa_volume_unknowns_restriction")
+
+    def face_unknowns_prolongation(self, q_fine, f_fine, q_coarse, f_coarse, n, fine_slot, coarse_slot, level_delta,
+                                   subface_index, stream=None):
+        _check(load().exa_face_unknowns_prolongation(self._h, _ptr(q_fine), _ptr(f_fine), _ptr(q_coarse),
+                                                     _ptr(f_coarse), int(n), _ptr(fine_slot), _ptr(coarse_slot),
+                                                     _ptr(level_delta), _ptr(subface_index), _stream(stream)),
+               "exa_face_unknowns_prolongation")
+
+    def face_unknowns_restriction(self, q_coarse, f_coarse, q_fine, f_fine, n, fine_slot, coarse_slot, level_delta,
+                                  subface_index, stream=None):
+        _check(load().exa_face_unknowns_restriction(self._h, _ptr(q_coarse), _ptr(f_coarse), _ptr(q_fine),
+                                                    _ptr(f_fine), int(n), _ptr(fine_slot), _ptr(coarse_slot),
+                                                    _ptr(level_delta), _ptr(subface_index), _stream(stream)),
+               "exa_face_unknowns_restriction")
+
+    def plot_vertices(self, luh, vertices, ncells, stream=None):
+        _check(load().exa_plot_vertices(self._h, _ptr(luh), _ptr(vertices), int(ncells), _stream(stream)),
+               "exa_plot_vertices")
+
     def boundary_conditions(self, lQhbnd, lFhbnd, bcell, bface, nb, kind=BC_OUTFLOW, stream=None):
         _check(load().exa_boundary_conditions(self._h, _ptr(lQhbnd), _ptr(lFhbnd), _ptr(bcell), _ptr(bface), int(nb),
                                               int(kind), _stream(stream)), "exa_boundary_conditions")
@@ -276,6 +309,11 @@ class Mesh:
         _check(load().exa_mesh_state(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st), ctypes.byref(sw)),
                "exa_mesh_state")
         return dict(t=t.value, dt=dt.value, steps=st.value, picard_sweeps=sw.value)
+
+    def write_vtk(self, path, binary=False):
+        """legacy VTK unstructured grid of the current solution (the layout of
+        the reference's ADERDG2CartesianVTK vertex plotter)"""
+        _check(load().exa_mesh_write_vtk(self._h, os.fsencode(path), int(bool(binary))), "exa_mesh_write_vtk")
 
     def synchronize(self):
         _check(load().exa_mesh_synchronize(self._h), "exa_mesh_synchronize")

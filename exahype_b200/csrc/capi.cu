@@ -17,6 +17,7 @@
 #include "predictor_lines.cuh"
 #include "limiter.cuh"
 #include "linear.cuh"
+#include "amr.cuh"
 
 namespace exa {
 
@@ -86,8 +87,10 @@ static int upload_tables() {
     if (d == dev) return EXA_OK;
   std::vector<OrderTables> h(kMaxOrder + 1);
   std::vector<LimiterTables> hl(kMaxOrder + 1);
+  std::vector<AmrTables> ha(kMaxOrder + 1);
   std::memset(h.data(), 0, sizeof(OrderTables) * h.size());
   std::memset(hl.data(), 0, sizeof(LimiterTables) * hl.size());
+  std::memset(ha.data(), 0, sizeof(AmrTables) * ha.size());
   for (int N = 1; N <= kMaxOrder; N++) {
     const int b = N + 1, bl = 2 * N + 1;
     OrderTables& t = h[N];
@@ -110,9 +113,13 @@ static int upload_tables() {
       l.uh2lim[i] = exa_tab_uh2lim[exa_tab_uh2lim_off[N] + i];
       l.lim2uh[i] = exa_tab_lim2uh[exa_tab_lim2uh_off[N] + i];
     }
+    for (int i = 0; i < 3 * b * b; i++) ha[N].fine[i] = exa_tab_fineGridProjector1d[exa_tab_fineGridProjector1d_off[N] + i];
+    for (int i = 0; i < b * b; i++)
+      ha[N].equi[i] = exa_tab_equidistantGridProjector1d[exa_tab_equidistantGridProjector1d_off[N] + i];
   }
   EXA_CUDA(cudaMemcpyToSymbol(c_tab, h.data(), sizeof(OrderTables) * h.size()));
   EXA_CUDA(cudaMemcpyToSymbol(g_lim_tab, hl.data(), sizeof(LimiterTables) * hl.size()));
+  EXA_CUDA(cudaMemcpyToSymbol(g_amr_tab, ha.data(), sizeof(AmrTables) * ha.size()));
   done_dev.push_back(dev);
   return EXA_OK;
 }
@@ -132,6 +139,44 @@ struct KernelSet {
                    const int*, cudaStream_t);
   // volumeIntegralLinear on its own (lduh, lFhi, ncells, stream); linear PDEs only
   int (*volume)(double*, const double*, int, cudaStream_t);
+  // AMR transfers (op 0 prolongation, 1 restriction): volume (a, b, n, fine,
+  // coarse, levelDelta, index[3n], op, stream) and face (state a, flux a,
+  // state b, flux b, n, fine slot, coarse slot, levelDelta, index[2n], op,
+  // stream); plot vertices (luh, out, ncells, stream)
+  int (*amr_volume)(double*, const double*, int, const int*, const int*, const int*, const int*, int, cudaStream_t);
+  int (*amr_face)(double*, double*, const double*, const double*, int, const int*, const int*, const int*,
+                  const int*, int, cudaStream_t);
+  int (*plot)(const double*, double*, int, cudaStream_t);
+};
+
+template <int DIM, int N, class PDE>
+struct AmrLaunch {
+  static constexpr int ND = PDE::nVar + PDE::nPar, NV = PDE::nVar;
+  static int volume(double* a, const double* b, int n, const int* fine, const int* coarse, const int* ld,
+                    const int* idx, int op, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    amr_volume_kernel<DIM, N, ND><<<n, 256, 0, st>>>(a, b, n, fine, coarse, ld, idx, op);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int face(double* qa, double* fa, const double* qb, const double* fb, int n, const int* fine,
+                  const int* coarse, const int* ld, const int* idx, int op, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    amr_face_kernel<DIM, N, ND, NV><<<n, 256, 0, st>>>(qa, fa, qb, fb, n, fine, coarse, ld, idx, op);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static int plot(const double* luh, double* out, int n, cudaStream_t st) {
+    if (n <= 0) return EXA_OK;
+    plot_vertex_kernel<DIM, N, ND><<<n, 256, 0, st>>>(luh, out, n);
+    EXA_LAUNCHED();
+    return EXA_OK;
+  }
+  static void fill(KernelSet& k) {
+    k.amr_volume = &volume;
+    k.amr_face = &face;
+    k.plot = &plot;
+  }
 };
 
 template <int DIM, int N, class PDE>
@@ -254,8 +299,9 @@ struct Launch {
   }
   static KernelSet make(int pde) {
     using S = Shape<DIM, N, PDE>;
-    return KernelSet{DIM, N, pde, S::nV, S::nP, S::P, S::F, false, &predictor, &riemann, &boundary, &corrector,
-                     nullptr};
+    KernelSet k{DIM, N, pde, S::nV, S::nP, S::P, S::F, false, &predictor, &riemann, &boundary, &corrector, nullptr};
+    AmrLaunch<DIM, N, PDE>::fill(k);
+    return k;
   }
 };
 
@@ -323,8 +369,9 @@ struct LinearLaunch {
   }
   static KernelSet make(int pde) {
     using S = Shape<DIM, N, PDE>;
-    return KernelSet{DIM, N, pde, S::nV, S::nP, S::P, S::F, true, &predictor, &riemann, &boundary, &corrector,
-                     &volume};
+    KernelSet k{DIM, N, pde, S::nV, S::nP, S::P, S::F, true, &predictor, &riemann, &boundary, &corrector, &volume};
+    AmrLaunch<DIM, N, PDE>::fill(k);
+    return k;
   }
 };
 
@@ -543,6 +590,54 @@ int exa_volume_integral_linear(const exa_solver* s, double* lduh, const double* 
     return fail(EXA_ERR_ARG, "exa_volume_integral_linear: null argument or negative count");
   if (!s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_volume_integral_linear: nonlinear PDE");
   return s->k.volume(lduh, lFhi, ncells, (cudaStream_t)stream);
+}
+
+int exa_volume_unknowns_prolongation(const exa_solver* s, double* luh_fine, const double* luh_coarse, int n,
+                                     const int* fine_cell, const int* coarse_cell, const int* level_delta,
+                                     const int* subcell_index, void* stream) {
+  if (!s || !luh_fine || !luh_coarse || n < 0 ||
+      (n > 0 && (!fine_cell || !coarse_cell || !level_delta || !subcell_index)))
+    return fail(EXA_ERR_ARG, "exa_volume_unknowns_prolongation: null argument or negative count");
+  return s->k.amr_volume(luh_fine, luh_coarse, n, fine_cell, coarse_cell, level_delta, subcell_index, 0,
+                         (cudaStream_t)stream);
+}
+
+int exa_volume_unknowns_restriction(const exa_solver* s, double* luh_coarse, const double* luh_fine, int n,
+                                    const int* fine_cell, const int* coarse_cell, const int* level_delta,
+                                    const int* subcell_index, void* stream) {
+  if (!s || !luh_fine || !luh_coarse || n < 0 ||
+      (n > 0 && (!fine_cell || !coarse_cell || !level_delta || !subcell_index)))
+    return fail(EXA_ERR_ARG, "exa_volume_unknowns_restriction: null argument or negative count");
+  return s->k.amr_volume(luh_coarse, luh_fine, n, fine_cell, coarse_cell, level_delta, subcell_index, 1,
+                         (cudaStream_t)stream);
+}
+
+int exa_face_unknowns_prolongation(const exa_solver* s, double* lQhbnd_fine, double* lFhbnd_fine,
+                                   const double* lQhbnd_coarse, const double* lFhbnd_coarse, int n,
+                                   const int* fine_slot, const int* coarse_slot, const int* level_delta,
+                                   const int* subface_index, void* stream) {
+  if (!s || !lQhbnd_fine || !lFhbnd_fine || !lQhbnd_coarse || !lFhbnd_coarse || n < 0 ||
+      (n > 0 && (!fine_slot || !coarse_slot || !level_delta || !subface_index)))
+    return fail(EXA_ERR_ARG, "exa_face_unknowns_prolongation: null argument or negative count");
+  return s->k.amr_face(lQhbnd_fine, lFhbnd_fine, lQhbnd_coarse, lFhbnd_coarse, n, fine_slot, coarse_slot,
+                       level_delta, subface_index, 0, (cudaStream_t)stream);
+}
+
+int exa_face_unknowns_restriction(const exa_solver* s, double* lQhbnd_coarse, double* lFhbnd_coarse,
+                                  const double* lQhbnd_fine, const double* lFhbnd_fine, int n, const int* fine_slot,
+                                  const int* coarse_slot, const int* level_delta, const int* subface_index,
+                                  void* stream) {
+  if (!s || !lQhbnd_fine || !lFhbnd_fine || !lQhbnd_coarse || !lFhbnd_coarse || n < 0 ||
+      (n > 0 && (!fine_slot || !coarse_slot || !level_delta || !subface_index)))
+    return fail(EXA_ERR_ARG, "exa_face_unknowns_restriction: null argument or negative count");
+  return s->k.amr_face(lQhbnd_coarse, lFhbnd_coarse, lQhbnd_fine, lFhbnd_fine, n, fine_slot, coarse_slot,
+                       level_delta, subface_index, 1, (cudaStream_t)stream);
+}
+
+int exa_plot_vertices(const exa_solver* s, const double* luh, double* vertices, int ncells, void* stream) {
+  if (!s || !luh || !vertices || ncells < 0)
+    return fail(EXA_ERR_ARG, "exa_plot_vertices: null argument or negative count");
+  return s->k.plot(luh, vertices, ncells, (cudaStream_t)stream);
 }
 
 int exa_boundary_conditions(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* bcell,
@@ -985,6 +1080,109 @@ int exa_mesh_set_priority(exa_mesh* m, int level) {
 int exa_mesh_synchronize(exa_mesh* m) {
   if (!m) return fail(EXA_ERR_ARG, "exa_mesh_synchronize: null mesh");
   EXA_CUDA(cudaStreamSynchronize(m->stream));
+  return EXA_OK;
+}
+
+}  // extern "C"
+
+// legacy-VTK writer of exa_mesh_write_vtk: text, or binary with big-endian values
+namespace {
+struct VtkOut {
+  FILE* f;
+  bool bin;
+  template <class T>
+  void put(T v) {
+    if (!bin) return;
+    unsigned char b[sizeof(T)], r[sizeof(T)];
+    std::memcpy(b, &v, sizeof(T));
+    for (size_t i = 0; i < sizeof(T); i++) r[i] = b[sizeof(T) - 1 - i];
+    std::fwrite(r, 1, sizeof(T), f);
+  }
+  void num(double v, const char* sep) {
+    if (bin)
+      put(v);
+    else
+      std::fprintf(f, "%.17g%s", v, sep);
+  }
+  void inum(int v, const char* sep) {
+    if (bin)
+      put((int32_t)v);
+    else
+      std::fprintf(f, "%d%s", v, sep);
+  }
+  void eol() {
+    if (bin) std::fputc('\n', f);
+  }
+};
+}  // namespace
+
+extern "C" {
+
+int exa_mesh_write_vtk(exa_mesh* m, const char* path, int binary) {
+  if (!m || !path) return fail(EXA_ERR_ARG, "exa_mesh_write_vtk: null argument");
+  const KernelSet& k = m->s->k;
+  const int dim = m->dim, N = k.order, b = N + 1, nD = k.nvar + k.npar;
+  const size_t n = m->ncells, P = k.P, sub = dim == 3 ? (size_t)N * N * N : (size_t)N * N;
+  double* dev = nullptr;
+  if (!salloc(&dev, n * P * nD * 8, m->stream)) {
+    cudaGetLastError();
+    return fail(EXA_ERR_NOMEM, "exa_mesh_write_vtk: device allocation failed");
+  }
+  std::vector<double> v(n * P * nD);
+  double t = 0.0;
+  int rc = k.plot(m->luh, dev, (int)n, m->stream);
+  if (!rc && cudaMemcpyAsync(v.data(), dev, v.size() * 8, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess)
+    rc = fail(EXA_ERR_CUDA, "exa_mesh_write_vtk: copy failed");
+  if (!rc && cudaMemcpyAsync(&t, m->scal + 2, 8, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess)
+    rc = fail(EXA_ERR_CUDA, "exa_mesh_write_vtk: copy failed");
+  sfree(dev, m->stream);
+  if (rc) return rc;
+  EXA_CUDA(cudaStreamSynchronize(m->stream));
+  FILE* f = std::fopen(path, binary ? "wb" : "w");
+  if (!f) return fail(EXA_ERR_ARG, std::string("exa_mesh_write_vtk: cannot open ") + path);
+  VtkOut o{f, binary != 0};
+  std::fprintf(f, "# vtk DataFile Version 3.0\nexahype_b200 ADER-DG solution t=%.17g\n%s\nDATASET UNSTRUCTURED_GRID\n",
+               t, binary ? "BINARY" : "ASCII");
+  // every cell is a patch of b^d vertices at offset + (cell + i/N) dx, x fastest
+  std::fprintf(f, "POINTS %zu double\n", n * P);
+  for (size_t c = 0; c < n; c++) {
+    const size_t cx = c % m->cells[0], cy = (c / m->cells[0]) % m->cells[1], cz = c / ((size_t)m->cells[0] * m->cells[1]);
+    for (size_t p = 0; p < P; p++) {
+      const int ix = (int)(p % b), iy = (int)((p / b) % b), iz = dim == 3 ? (int)(p / (b * b)) : 0;
+      o.num(m->offset[0] + (cx + (double)ix / N) * m->geo.dx[0], " ");
+      o.num(m->offset[1] + (cy + (double)iy / N) * m->geo.dx[1], " ");
+      o.num(dim == 3 ? m->offset[2] + (cz + (double)iz / N) * m->geo.dx[2] : 0.0, "\n");
+    }
+  }
+  o.eol();
+  const int nv = dim == 3 ? 8 : 4;
+  std::fprintf(f, "CELLS %zu %zu\n", n * sub, n * sub * (nv + 1));
+  for (size_t c = 0; c < n; c++)
+    for (int kz = 0; kz < (dim == 3 ? N : 1); kz++)
+      for (int ky = 0; ky < N; ky++)
+        for (int kx = 0; kx < N; kx++) {
+          o.inum(nv, " ");
+          // VTK_PIXEL / VTK_VOXEL vertex order: x fastest, then y, then z
+          for (int q = 0; q < nv; q++) {
+            const int dx = q & 1, dy = (q >> 1) & 1, dz = (q >> 2) & 1;
+            const size_t id = c * P + ((size_t)(kz + dz) * b + (ky + dy)) * b + (kx + dx);
+            o.inum((int)id, q + 1 < nv ? " " : "\n");
+          }
+        }
+  o.eol();
+  std::fprintf(f, "CELL_TYPES %zu\n", n * sub);
+  for (size_t i = 0; i < n * sub; i++) o.inum(dim == 3 ? 11 : 8, "\n");
+  o.eol();
+  std::fprintf(f, "POINT_DATA %zu\nSCALARS Q double %d\nLOOKUP_TABLE default\n", n * P, nD);
+  for (size_t i = 0; i < n * P; i++)
+    for (int q = 0; q < nD; q++) o.num(v[i * nD + q], q + 1 < nD ? " " : "\n");
+  o.eol();
+  std::fprintf(f, "SCALARS time double 1\nLOOKUP_TABLE default\n");
+  for (size_t i = 0; i < n * P; i++) o.num(t, "\n");
+  o.eol();
+  const bool ok = std::ferror(f) == 0;
+  std::fclose(f);
+  if (!ok) return fail(EXA_ERR_ARG, std::string("exa_mesh_write_vtk: write error on ") + path);
   return EXA_OK;
 }
 

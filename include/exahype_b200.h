@@ -134,6 +134,35 @@ int exa_riemann_solver_linear(const exa_solver* s, const double* lQhbnd, double*
 /* volumeIntegralLinear (c/{2d,3d}/volumeIntegralLinear.cpph) on its own:
  * lduh = -w sum_d lFhi[d], lFhi per cell [d][b^d][nV]. */
 int exa_volume_integral_linear(const exa_solver* s, double* lduh, const double* lFhi, int ncells, void* stream);
+/* AMR transfer operators (kernels/aderdg/generic/c/{2d,3d}/amrRoutines.cpph,
+ * Kernels.h:159-201), batched: transfer k moves data between fine cell (or
+ * face slot) fine[k] and its ancestor coarse[k], level_delta[k] levels
+ * coarser (1..12); the subcell index holds one base-3 digit per level per axis
+ * (0 .. 3^level_delta - 1), 3 ints per transfer for cells, 2 for faces (2D:
+ * the first is used). Face slots index lQhbnd/lFhbnd as cell * 2d + face.
+ * Prolongations overwrite the fine data; restrictions ADD the restricted
+ * data to the coarse data (atomically, so descendants of one ancestor may
+ * share a call; their sum order is not fixed). Transfers with an invalid
+ * level_delta or index are skipped. All arrays are device arrays. */
+int exa_volume_unknowns_prolongation(const exa_solver* s, double* luh_fine, const double* luh_coarse, int n,
+                                     const int* fine_cell, const int* coarse_cell, const int* level_delta,
+                                     const int* subcell_index, void* stream);
+int exa_volume_unknowns_restriction(const exa_solver* s, double* luh_coarse, const double* luh_fine, int n,
+                                    const int* fine_cell, const int* coarse_cell, const int* level_delta,
+                                    const int* subcell_index, void* stream);
+int exa_face_unknowns_prolongation(const exa_solver* s, double* lQhbnd_fine, double* lFhbnd_fine,
+                                   const double* lQhbnd_coarse, const double* lFhbnd_coarse, int n,
+                                   const int* fine_slot, const int* coarse_slot, const int* level_delta,
+                                   const int* subface_index, void* stream);
+int exa_face_unknowns_restriction(const exa_solver* s, double* lQhbnd_coarse, double* lFhbnd_coarse,
+                                  const double* lQhbnd_fine, const double* lFhbnd_fine, int n, const int* fine_slot,
+                                  const int* coarse_slot, const int* level_delta, const int* subface_index,
+                                  void* stream);
+/* The solution of ncells cells at their (N+1)^d equidistant vertices
+ * (x fastest), vertices [cell][b^d][nD]: what the plotter
+ * ADERDG2CartesianVTK::plotVertexData evaluates with
+ * equidistantGridProjector1d (exahype/plotters/VTK/ADERDG2CartesianVTK.cpp). */
+int exa_plot_vertices(const exa_solver* s, const double* luh, double* vertices, int ncells, void* stream);
 /* boundaryConditions + riemannSolver on boundary faces (ADERDGSolver::
  * applyBoundaryConditions, ADERDGSolver.cpp:2893-2962): face f is face
  * bface[f] of cell bcell[f]; kind is EXA_BC_OUTFLOW or EXA_BC_REFLECTIVE. */
@@ -177,6 +206,12 @@ int exa_mesh_run_until(exa_mesh* m, double t_end, int max_steps, int* steps);
  * number of Picard sweeps executed by the predictor so far */
 int exa_mesh_state(exa_mesh* m, double* t, double* dt, long long* steps, long long* picard_sweeps);
 int exa_mesh_synchronize(exa_mesh* m);
+/* Writes the mesh's current solution as a legacy VTK unstructured grid (text,
+ * or binary when binary != 0): every cell a patch of (N+1)^d vertices with
+ * N^d pixels / voxels, vertex data "Q" (all nD values, from
+ * exa_plot_vertices) and "time" -- the layout of the reference's
+ * ADERDG2CartesianVTK vertex plotter. Synchronises the mesh's stream. */
+int exa_mesh_write_vtk(exa_mesh* m, const char* path, int binary);
 /* Moves the mesh's work to a new stream of stream priority `level` (0: the
  * default, least urgent; each level up is more urgent, capped at the device's
  * range): where several streams' kernels wait for SMs, the higher priority's

@@ -22,7 +22,10 @@ def test_header_declares_the_api():
     names = declared_functions()
     for required in ("exa_space_time_predictor_nonlinear", "exa_riemann_solver_nonlinear", "exa_boundary_conditions",
                      "exa_corrector", "exa_mesh_create", "exa_mesh_step", "exa_solver_create",
-                     "exa_space_time_predictor_linear", "exa_riemann_solver_linear", "exa_volume_integral_linear"):
+                     "exa_space_time_predictor_linear", "exa_riemann_solver_linear", "exa_volume_integral_linear",
+                     "exa_volume_unknowns_prolongation", "exa_volume_unknowns_restriction",
+                     "exa_face_unknowns_prolongation", "exa_face_unknowns_restriction", "exa_plot_vertices",
+                     "exa_mesh_write_vtk"):
         assert required in names
 
 
