@@ -86,14 +86,16 @@ def bytes_per_step(dim, N, ncells, nV=NVAR, nD=NVAR):
 
 def linear_predictor_flops(dim, N, ncells, nV=EL_NVAR, nD=EL_NDATA):
     """Algorithmic FLOPs of the linear predictor (Cauchy-Kovalevski) + volume
-    integral per launch: per derivative level (b of them) 2 d nV b^(d+1)
-    (line gradients) + per node the elastic non-conservative product (3 per
-    direction: 2 products for the moduli, 9 products) and the level update and
-    both time averages (d nV + 2 nV + 2 d nV); per cell once the boundary
-    extrapolation 4 d b^(d-1) b (nD + nV) and the volume integral 2 d nV b^d."""
+    integral per launch: per derivative level (b of them) 2 b^(d+1) per
+    gradient component the elastic product reads (6 of the 9 variables per
+    direction) + per node the product (3 per direction: 2 for the moduli, 9
+    products) and the level update and both time averages
+    (d nV + 2 nV + 2 d nV); per cell once the boundary extrapolation
+    4 d b^(d-1) b (nD + nV) and the volume integral 2 d nV b^d."""
     b = N + 1
     P = b ** dim
-    per_level = 2 * dim * nV * b ** (dim + 1) + P * (dim * (2 + nV) + dim * nV + 2 * nV + 2 * dim * nV)
+    used = 6 * dim  # gradient components the elastic non-conservative product reads
+    per_level = 2 * used * b ** (dim + 1) + P * (dim * (2 + nV) + dim * nV + 2 * nV + 2 * dim * nV)
     per_cell = b * per_level + 4 * dim * b ** (dim - 1) * b * (nD + nV) + 2 * dim * nV * P
     return per_cell * ncells
 
@@ -321,23 +323,38 @@ def run_ours(a):
     e2e = None
     if not a.no_e2e:
         nbytes = int(np.prod(m.solution_shape)) * 8
-        pin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
-        pin.numpy()[:] = m.get_solution().reshape(-1)
+        pin_in = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+        pin_out = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+        pin_in.numpy()[:] = m.get_solution().reshape(-1)
+        ke = max(1, min(a.steps, 10))
+        # streamed: every step uploads its input and downloads its result, the
+        # copies of neighbouring steps overlapping its compute
+        m.step_io(pin_in.data_ptr(), 1, pin_out.data_ptr(), 1, nbytes, 2)  # warm-up (staging buffers)
+        m.synchronize()
         barrier()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ke = max(1, min(a.steps, 10))
         f0.record(stream)
-        for _ in range(ke):
-            m.upload_solution_async(pin.data_ptr(), nbytes)
-            m.step(1)
-            m.download_solution_async(pin.data_ptr(), nbytes)
+        m.step_io(pin_in.data_ptr(), 1, pin_out.data_ptr(), 1, nbytes, ke)
         f1.record(stream)
         f1.synchronize()
-        e2e_ms = f0.elapsed_time(f1)
-        e2e_ms = reduce_max(e2e_ms, world, dev)
+        e2e_ms = reduce_max(f0.elapsed_time(f1), world, dev)
+        # the same one step at a time: upload, step, download, in order
+        barrier()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(ke):
+            m.upload_solution_async(pin_in.data_ptr(), nbytes)
+            m.step(1)
+            m.download_solution_async(pin_out.data_ptr(), nbytes)
+        g1.record(stream)
+        g1.synchronize()
+        ser_ms = reduce_max(g0.elapsed_time(g1), world, dev)
         e2e = {"value": dof_per_step() * ke * world / (e2e_ms / 1e3), "unit": "DoF-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ke,
-               "api": "exa_mesh_copy_solution(H2D) + exa_mesh_step(1) + exa_mesh_copy_solution(D2H)"}
+               "api": "exa_mesh_step_io: per step H2D of the step's input from pinned memory, the step, D2H of its "
+                      "result; the copies of steps k+1 and k-1 overlap step k",
+               "serial": {"value": dof_per_step() * ke * world / (ser_ms / 1e3), "unit": "DoF-updates/s",
+                          "api": "exa_mesh_copy_solution(H2D) + exa_mesh_step(1) + exa_mesh_copy_solution(D2H)"}}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -352,6 +369,7 @@ def run_ours(a):
     lim = None if a.no_limiter else run_limiter_workload(a, world, dev, rank)
     ens = None if a.no_ensemble else run_ensemble_workload(a, world, dev, rank)
     ela = None if a.no_elastic else run_elastic_workload(a, world, dev, rank, fp64_peak)
+    amr = None if a.no_amr else run_amr_workload(a, world, dev, rank)
     srv = None if a.no_serving else run_serving_workload(a, world, dev, rank)
     line = {
         "metric": METRIC, "value": value, "unit": "DoF-updates/s", "n_gpus": world, "steps": a.steps,
@@ -362,7 +380,7 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
-        "mixed": mixed, "limiter": lim, "ensemble": ens, "serving": srv, "elastic": ela,
+        "mixed": mixed, "limiter": lim, "ensemble": ens, "serving": srv, "elastic": ela, "amr": amr,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -436,6 +454,59 @@ def run_elastic_workload(a, world, dev, rank, fp64_peak=None):
                                    "kind": "reference", "sample": "1 full time step of the 27^3 elastic mesh on the "
                                    "reference's linear kernels, %.1f s" % el}
     return out
+
+
+def run_amr_workload(a, world, dev, rank):
+    """AMR transfers and plotting on the 3D N=5 Euler shape: the 27^3 cells
+    of a 9^3 coarse mesh refined once (levelDelta 1): prolongation of every
+    fine cell from its parent, restriction of all of them back into the
+    parents (atomic accumulation), the equidistant vertex projection of the
+    fine mesh; CUDA events, median of 5 launches each after 2 warm-ups.
+    Bytes per launch: the fine data written (read) once, the coarse data
+    read (accumulated) once."""
+    import torch
+    import exahype_b200 as eb
+    N, dim, nd = 5, 3, NVAR
+    P = (N + 1) ** dim
+    s = eb.Solver(dim, N, eb.PDE_EULER)
+    nc, nf = 9 ** 3, 27 ** 3
+    rng = np.random.default_rng(SEED)
+    coarse = torch.as_tensor(rng.normal(size=(nc, P * nd))).to(dev)
+    fine = torch.empty((nf, P * nd), dtype=torch.float64, device=dev)
+    fid = np.arange(nf, dtype=np.int32)
+    fx, fy, fz = fid % 27, (fid // 27) % 27, fid // 729
+    par = ((fz // 3) * 81 + (fy // 3) * 9 + (fx // 3)).astype(np.int32)
+    idx = np.stack([fx % 3, fy % 3, fz % 3], axis=1).astype(np.int32)
+    t = lambda x: torch.as_tensor(np.ascontiguousarray(x)).to(dev)
+    fid_d, par_d, ld_d, idx_d = t(fid), t(par), t(np.ones(nf, dtype=np.int32)), t(idx)
+    verts = torch.empty_like(fine)
+    st = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        ms = []
+        for r in range(7):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            if r >= 2:
+                ms.append(e0.elapsed_time(e1))
+        return reduce_max(float(np.median(ms)), world, dev)
+
+    pro = timed(lambda: s.volume_unknowns_prolongation(fine, coarse, nf, fid_d, par_d, ld_d, idx_d))
+    res = timed(lambda: s.volume_unknowns_restriction(coarse, fine, nf, fid_d, par_d, ld_d, idx_d))
+    plo = timed(lambda: s.plot_vertices(fine, verts, nf))
+    peaks = load_peaks()
+    fb, cb = nf * P * nd * 8, nc * P * nd * 8
+
+    def k(ms, by):
+        gbs = by / (ms / 1e3) / 1e9
+        return dict(ms=ms, bytes=by, achieved=gbs, unit="GB/s", peak=peaks["hbm_gbs"], frac=gbs / peaks["hbm_gbs"])
+
+    return {"workload": "amr_euler3d_N5_9^3_to_27^3", "transfers": nf,
+            "volume_prolongation": k(pro, fb + cb), "volume_restriction": k(res, fb + cb),
+            "plot_vertices": k(plo, 2 * fb), "timing": "median of 5 launches, CUDA events"}
 
 
 def run_limiter_workload(a, world, dev, rank):
@@ -662,13 +733,14 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--serving-full", action="store_true", help="serving: the full-size request mix")
     ap.add_argument("--no-elastic", action="store_true", help="skip the linear-kernel (elastic waves) workload")
+    ap.add_argument("--no-amr", action="store_true", help="skip the AMR transfer / plotting workload")
     ap.add_argument("--workload", default="headline",
-                    choices=["headline", "limiter", "ensemble", "serving", "elastic"],
+                    choices=["headline", "limiter", "ensemble", "serving", "elastic", "amr"],
                     help="limiter / ensemble / serving / elastic: only that workload, as its own JSON line")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
-    if a.workload in ("limiter", "ensemble", "serving", "elastic"):
+    if a.workload in ("limiter", "ensemble", "serving", "elastic", "amr"):
         return run_secondary_only(a)
     return run_ours(a)
 
@@ -681,7 +753,7 @@ def run_secondary_only(a):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     run = {"limiter": run_limiter_workload, "ensemble": run_ensemble_workload,
-           "serving": run_serving_workload, "elastic": run_elastic_workload}[a.workload]
+           "serving": run_serving_workload, "elastic": run_elastic_workload, "amr": run_amr_workload}[a.workload]
     if a.workload == "elastic":
         r = run(a, world, torch.device("cuda", local), rank, None if a.no_fp64_probe else measure_fp64_peak())
     else:

@@ -347,6 +347,13 @@ class Mesh:
         _check(load().exa_mesh_copy_solution(self._h, ctypes.c_void_p(host_ptr), ctypes.c_size_t(nbytes), 1),
                "exa_mesh_copy_solution")
 
+    def step_io(self, host_in_ptr, nin, host_out_ptr, nout, nbytes, nsteps):
+        """nsteps steps, each taking its solution from the host and leaving its
+        result on the host, the copies overlapping the compute of the
+        neighbouring steps (pinned host memory; enqueued, see synchronize())."""
+        _check(load().exa_mesh_step_io(self._h, ctypes.c_void_p(host_in_ptr), int(nin), ctypes.c_void_p(host_out_ptr),
+                                       int(nout), ctypes.c_size_t(nbytes), int(nsteps)), "exa_mesh_step_io")
+
     def download_solution_async(self, host_ptr, nbytes):
         """D2H copy of the solution into a (pinned) host pointer, ordered on the mesh stream."""
         _check(load().exa_mesh_copy_solution(self._h, ctypes.c_void_p(host_ptr), ctypes.c_size_t(nbytes), 0),

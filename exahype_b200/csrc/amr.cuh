@@ -22,22 +22,22 @@
 
 namespace exa {
 
-// per order: fineGridProjector1d [third][n][m] and equidistantGridProjector1d [n][i]
+// per order: fineGridProjector1d [third][n][m], the restriction factors
+// w_n P[third][m][n] / (3 w_m) as [third][m][n], and
+// equidistantGridProjector1d [n][i]
 struct AmrTables {
   double fine[3 * kMaxB * kMaxB];
+  double restr[3 * kMaxB * kMaxB];
   double equi[kMaxB * kMaxB];
 };
 __device__ AmrTables g_amr_tab[kMaxOrder + 1];
 
-// applies a 1-D operator along axis `ax` (0 = fastest) of a tensor with `nax`
-// axes of length b and nv values per node: out[.., m, ..] =
+// applies a 1-D operator along axis AX (0 = fastest) of a tensor with NAX
+// axes of length b and NV values per node: out[.., m, ..] =
 // sum_n op(m, n) in[.., n, ..]; all threads of the block take part
-template <int b, class Op>
-__device__ __forceinline__ void apply_axis(const double* in, double* out, int nax, int ax, int nv, Op op) {
-  int total = nv;
-  for (int k = 0; k < nax; k++) total *= b;
-  int stride = nv;
-  for (int k = 0; k < ax; k++) stride *= b;
+template <int b, int NAX, int AX, int NV, class Op>
+__device__ __forceinline__ void apply_axis(const double* in, double* out, Op op) {
+  constexpr int total = NV * ipow(b, NAX), stride = NV * ipow(b, AX);
   for (int e = threadIdx.x; e < total; e += blockDim.x) {
     const int m = (e / stride) % b;
     const int base = e - m * stride;
@@ -46,6 +46,21 @@ __device__ __forceinline__ void apply_axis(const double* in, double* out, int na
     for (int n = 0; n < b; n++) s = fma(op(m, n), in[base + n * stride], s);
     out[e] = s;
   }
+}
+
+// the operator of each axis in turn (axis k uses ops(k)), ping-ponging
+// between the two buffers; returns the buffer holding the result
+template <int b, int NAX, int NV, class Ops>
+__device__ __forceinline__ double* apply_axes(double* cur, double* nxt, Ops ops) {
+  __syncthreads();
+  apply_axis<b, NAX, 0, NV>(cur, nxt, ops(0));
+  if (NAX == 1) return nxt;
+  __syncthreads();
+  apply_axis<b, NAX, 1, NV>(nxt, cur, ops(1));
+  if (NAX == 2) return cur;
+  __syncthreads();
+  apply_axis<b, NAX, 2, NV>(cur, nxt, ops(2));
+  return nxt;
 }
 
 // levelDelta in 1..kMaxLevelDelta and every index digit-string in
@@ -64,14 +79,12 @@ __device__ __forceinline__ bool valid_index(int ld, const int* index, int nax) {
 // one transfer of `nax`-dimensional nodal data (nv values per node) between
 // levels: restrict == false prolongates src (coarse) into dst (fine),
 // restrict == true restricts src (fine) and adds it to dst (coarse)
-template <int N>
-__device__ void amr_transfer(const double* __restrict__ src, double* __restrict__ dst, int nax, int nv,
-                             int levelDelta, const int* index, bool restrict_, double* bufA, double* bufB) {
+template <int N, int NAX, int NV>
+__device__ void amr_transfer(const double* __restrict__ src, double* __restrict__ dst, int levelDelta,
+                             const int* index, bool restrict_, double* bufA, double* bufB) {
   constexpr int b = N + 1;
+  constexpr int size = NV * ipow(b, NAX);
   const AmrTables& A = g_amr_tab[N];
-  const OrderTables& T = c_tab[N];
-  int size = nv;
-  for (int k = 0; k < nax; k++) size *= b;
   for (int e = threadIdx.x; e < size; e += blockDim.x) bufA[e] = src[e];
   int rest[3] = {index[0], index[1], index[2]};
   int sig = 1;
@@ -79,8 +92,9 @@ __device__ void amr_transfer(const double* __restrict__ src, double* __restrict_
   double* cur = bufA;
   double* nxt = bufB;
   for (int l = 0; l < levelDelta; l++) {
-    int digit[3];
-    for (int k = 0; k < nax; k++) {
+    int digit[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < NAX; k++) {
       if (!restrict_) {  // most significant digit first
         digit[k] = rest[k] / sig;
         rest[k] = rest[k] % sig;
@@ -90,18 +104,14 @@ __device__ void amr_transfer(const double* __restrict__ src, double* __restrict_
       }
     }
     sig = sig > 1 ? sig / 3 : 1;
-    for (int ax = 0; ax < nax; ax++) {
-      __syncthreads();
-      const double* P = A.fine + digit[ax] * b * b;
-      if (!restrict_)
-        apply_axis<b>(cur, nxt, nax, ax, nv, [&](int m, int n) { return P[n * b + m]; });
-      else
-        apply_axis<b>(cur, nxt, nax, ax, nv,
-                      [&](int m, int n) { return T.w[n] * P[m * b + n] / (3.0 * T.w[m]); });
-      double* t = cur;
-      cur = nxt;
-      nxt = t;
-    }
+    const double* tab = restrict_ ? A.restr : A.fine;
+    double* res = apply_axes<b, NAX, NV>(cur, nxt, [&](int ax) {
+      const double* M = tab + digit[ax] * b * b;
+      const bool r = restrict_;
+      return [M, r](int m, int n) { return r ? M[m * b + n] : M[n * b + m]; };
+    });
+    nxt = res == cur ? nxt : cur;
+    cur = res;
   }
   __syncthreads();
   for (int e = threadIdx.x; e < size; e += blockDim.x) {
@@ -110,6 +120,7 @@ __device__ void amr_transfer(const double* __restrict__ src, double* __restrict_
     else
       dst[e] = cur[e];
   }
+  __syncthreads();  // the buffers may be reused by the caller
 }
 
 // op 0: prolongation, 1: restriction. item k: fine cell fine[k], coarse cell
@@ -128,11 +139,11 @@ __global__ void __launch_bounds__(256) amr_volume_kernel(double* __restrict__ lu
   const int index[3] = {idx[3 * k], idx[3 * k + 1], DIM == 3 ? idx[3 * k + 2] : 0};
   if (!valid_index(ld, index, DIM)) return;
   if (op == 0)  // luh_a: fine (written), luh_b: coarse
-    amr_transfer<N>(luh_b + (size_t)coarse[k] * P * ND, luh_a + (size_t)fine[k] * P * ND, DIM, ND, ld, index,
-                    false, bufA, bufB);
+    amr_transfer<N, DIM, ND>(luh_b + (size_t)coarse[k] * P * ND, luh_a + (size_t)fine[k] * P * ND, ld, index, false,
+                             bufA, bufB);
   else  // luh_a: coarse (added to), luh_b: fine
-    amr_transfer<N>(luh_b + (size_t)fine[k] * P * ND, luh_a + (size_t)coarse[k] * P * ND, DIM, ND, ld, index, true,
-                    bufA, bufB);
+    amr_transfer<N, DIM, ND>(luh_b + (size_t)fine[k] * P * ND, luh_a + (size_t)coarse[k] * P * ND, ld, index, true,
+                             bufA, bufB);
 }
 
 // faces: item k moves face slot fine[k] <-> coarse[k] (slot = cell * 2 DIM +
@@ -153,9 +164,8 @@ __global__ void __launch_bounds__(256) amr_face_kernel(double* __restrict__ q_a,
   if (!valid_index(ld, index, DIM - 1)) return;
   const bool r = op != 0;
   const size_t from = r ? fine[k] : coarse[k], to = r ? coarse[k] : fine[k];
-  amr_transfer<N>(q_b + from * F * ND, q_a + to * F * ND, DIM - 1, ND, ld, index, r, bufA, bufB);
-  __syncthreads();
-  amr_transfer<N>(f_b + from * F * NV, f_a + to * F * NV, DIM - 1, NV, ld, index, r, bufA, bufB);
+  amr_transfer<N, DIM - 1, ND>(q_b + from * F * ND, q_a + to * F * ND, ld, index, r, bufA, bufB);
+  amr_transfer<N, DIM - 1, NV>(f_b + from * F * NV, f_a + to * F * NV, ld, index, r, bufA, bufB);
 }
 
 // the solution of every cell at its (N+1)^d equidistant vertices (x fastest),
@@ -169,15 +179,8 @@ __global__ void __launch_bounds__(256) plot_vertex_kernel(const double* __restri
   if (c >= ncells) return;
   const AmrTables& A = g_amr_tab[N];
   for (int e = threadIdx.x; e < P * ND; e += blockDim.x) bufA[e] = luh[(size_t)c * P * ND + e];
-  double* cur = bufA;
-  double* nxt = bufB;
-  for (int ax = 0; ax < DIM; ax++) {
-    __syncthreads();
-    apply_axis<b>(cur, nxt, DIM, ax, ND, [&](int i, int n) { return A.equi[n * b + i]; });
-    double* t = cur;
-    cur = nxt;
-    nxt = t;
-  }
+  const double* E = A.equi;
+  double* cur = apply_axes<b, DIM, ND>(bufA, bufB, [E](int) { return [E](int i, int n) { return E[n * b + i]; }; });
   __syncthreads();
   for (int e = threadIdx.x; e < P * ND; e += blockDim.x) out[(size_t)c * P * ND + e] = cur[e];
 }

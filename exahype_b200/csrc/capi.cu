@@ -114,6 +114,10 @@ static int upload_tables() {
       l.lim2uh[i] = exa_tab_lim2uh[exa_tab_lim2uh_off[N] + i];
     }
     for (int i = 0; i < 3 * b * b; i++) ha[N].fine[i] = exa_tab_fineGridProjector1d[exa_tab_fineGridProjector1d_off[N] + i];
+    for (int j = 0; j < 3; j++)
+      for (int m = 0; m < b; m++)
+        for (int n = 0; n < b; n++)
+          ha[N].restr[(j * b + m) * b + n] = t.w[n] * ha[N].fine[(j * b + m) * b + n] / (3.0 * t.w[m]);
     for (int i = 0; i < b * b; i++)
       ha[N].equi[i] = exa_tab_equidistantGridProjector1d[exa_tab_equidistantGridProjector1d_off[N] + i];
   }
@@ -464,6 +468,11 @@ struct exa_mesh {
   std::vector<int> ev_phase;
   double phase_ms[4] = {0, 0, 0, 0};
   long long phase_launches[4] = {0, 0, 0, 0};
+  // streamed host I/O of exa_mesh_step_io: staging buffers, copy streams and
+  // the events that order them against the mesh stream
+  double *stage_in = nullptr, *stage_out = nullptr;
+  cudaStream_t io_in = nullptr, io_out = nullptr;
+  cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
 };
 
 namespace {
@@ -749,6 +758,14 @@ int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chos
 static void mesh_free(exa_mesh* m) {
   for (cudaEvent_t e : m->ev) cudaEventDestroy(e);
   m->ev.clear();
+  if (m->io_in) cudaStreamSynchronize(m->io_in);
+  if (m->io_out) cudaStreamSynchronize(m->io_out);
+  for (cudaEvent_t e : {m->in_ready, m->in_free, m->out_ready, m->out_free})
+    if (e) cudaEventDestroy(e);
+  sfree(m->stage_in, m->stream);
+  sfree(m->stage_out, m->stream);
+  if (m->io_in) cudaStreamDestroy(m->io_in);
+  if (m->io_out) cudaStreamDestroy(m->io_out);
   for (void* p : {(void*)m->luh, (void*)m->lduh, (void*)m->lQhbnd, (void*)m->lFhbnd, (void*)m->scal, (void*)m->iters,
                   (void*)m->fl, (void*)m->fr, (void*)m->fd, (void*)m->bcell, (void*)m->bface, (void*)m->sweeps})
     sfree(p, m->stream);
@@ -960,6 +977,53 @@ int exa_mesh_step(exa_mesh* m, int nsteps) {
     int rc = mesh_one_step(m);
     if (rc) return rc;
   }
+  return EXA_OK;
+}
+
+int exa_mesh_step_io(exa_mesh* m, const void* host_in, int nin, void* host_out, int nout, size_t nbytes,
+                     int nsteps) {
+  if (!m || !host_in || !host_out || nin < 1 || nout < 1 || nsteps < 0)
+    return fail(EXA_ERR_ARG, "exa_mesh_step_io: bad argument");
+  if (!m->initialised) return fail(EXA_ERR_STATE, "exa_mesh_step_io: call exa_mesh_init first");
+  const size_t bytes = (size_t)m->ncells * m->s->k.P * (m->s->k.nvar + m->s->k.npar) * 8;
+  if (nbytes != bytes) return fail(EXA_ERR_ARG, "exa_mesh_step_io: nbytes does not match the solution size");
+  if (!m->io_in) {
+    EXA_CUDA(cudaStreamCreateWithFlags(&m->io_in, cudaStreamNonBlocking));
+    EXA_CUDA(cudaStreamCreateWithFlags(&m->io_out, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&m->in_ready, &m->in_free, &m->out_ready, &m->out_free})
+      EXA_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    if (!salloc(&m->stage_in, bytes, m->stream) || !salloc(&m->stage_out, bytes, m->stream)) {
+      cudaGetLastError();
+      return fail(EXA_ERR_NOMEM, "exa_mesh_step_io: device allocation failed");
+    }
+    // the staging buffers exist before either copy stream touches them
+    EXA_CUDA(cudaEventRecord(m->in_free, m->stream));
+    EXA_CUDA(cudaEventRecord(m->out_free, m->stream));
+  }
+  const char* in = static_cast<const char*>(host_in);
+  char* out = static_cast<char*>(host_out);
+  for (int k = 0; k < nsteps; k++) {
+    // input k: once the previous input has left the staging buffer
+    EXA_CUDA(cudaStreamWaitEvent(m->io_in, m->in_free, 0));
+    EXA_CUDA(cudaMemcpyAsync(m->stage_in, in + (size_t)(k % nin) * bytes, bytes, cudaMemcpyHostToDevice, m->io_in));
+    EXA_CUDA(cudaEventRecord(m->in_ready, m->io_in));
+    EXA_CUDA(cudaStreamWaitEvent(m->stream, m->in_ready, 0));
+    EXA_CUDA(cudaMemcpyAsync(m->luh, m->stage_in, bytes, cudaMemcpyDeviceToDevice, m->stream));
+    EXA_CUDA(cudaEventRecord(m->in_free, m->stream));
+    int rc = mesh_one_step(m);
+    if (rc) return rc;
+    // result k: once the previous result has left the staging buffer
+    EXA_CUDA(cudaStreamWaitEvent(m->stream, m->out_free, 0));
+    EXA_CUDA(cudaMemcpyAsync(m->stage_out, m->luh, bytes, cudaMemcpyDeviceToDevice, m->stream));
+    EXA_CUDA(cudaEventRecord(m->out_ready, m->stream));
+    EXA_CUDA(cudaStreamWaitEvent(m->io_out, m->out_ready, 0));
+    EXA_CUDA(cudaMemcpyAsync(out + (size_t)(k % nout) * bytes, m->stage_out, bytes, cudaMemcpyDeviceToHost,
+                             m->io_out));
+    EXA_CUDA(cudaEventRecord(m->out_free, m->io_out));
+  }
+  // the mesh stream (what exa_mesh_synchronize and the caller's events see)
+  // completes after the last result is on the host
+  EXA_CUDA(cudaStreamWaitEvent(m->stream, m->out_free, 0));
   return EXA_OK;
 }
 

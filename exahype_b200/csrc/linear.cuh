@@ -19,17 +19,43 @@
 
 namespace exa {
 
+// Order of the gradient items, from a shared-memory bank model (64-bit
+// accesses, 16 bank pairs per half-warp) of the gradient phase's strided line
+// accesses: for 3D with 6 or 5 nodes per axis consecutive threads take
+// consecutive lines of one component, elsewhere consecutive components of
+// one line. Odd node strides keep the per-node phase conflict-free.
+constexpr bool ck_line_major(int dim, int b) { return dim == 3 ? b >= 5 : (b == 6 || b == 4); }
+
+// the (direction, variable) gradient components the PDE's ncp reads
+template <class PDE, int DIM>
+struct GradPairs {
+  int d[DIM * PDE::nVar], v[DIM * PDE::nVar], n;
+  constexpr GradPairs() : d(), v(), n(0) {
+    for (int dd = 0; dd < DIM; dd++)
+      for (int vv = 0; vv < PDE::nVar; vv++)
+        if (PDE::ncp_uses(dd, vv)) {
+          d[n] = dd;
+          v[n] = vv;
+          n++;
+        }
+  }
+};
+
 template <int DIM, int N, class PDE>
 struct CKCfg : Shape<DIM, N, PDE> {
   using S = Shape<DIM, N, PDE>;
   static constexpr int CPB = cells_per_block<S::P>();
   static constexpr int THREADS = CPB * S::P;
   static constexpr int LINES = S::P / S::b;          // lines per direction
-  static constexpr int QS = S::nD | 1;               // node stride of the state (odd: no bank conflicts)
-  static constexpr int GS = (DIM * S::nV) | 1;       // node stride of the gradients [d][nV]
+  static constexpr int QS = S::nD | 1;          // node stride of the state
+  static constexpr int GS = (DIM * S::nV) | 1;  // node stride of the gradients [d][nV]
+  static constexpr bool LMAJ = ck_line_major(DIM, S::b);
   static constexpr int SQ = S::P * QS, SG = S::P * GS;
   static constexpr size_t SMEM = sizeof(double) * (size_t)CPB * (SQ + SG);
-  static constexpr int GITEMS = CPB * DIM * LINES * S::nV;  // gradient line items per block
+  static constexpr int NPAIRS = GradPairs<PDE, DIM>().n;
+  static constexpr int GITEMS = CPB * NPAIRS * LINES;  // gradient line items per block
+  static constexpr int IPT = (GITEMS + THREADS - 1) / THREADS;
+  static_assert(S::P < 1024 && S::nV <= 16 && CPB <= 16, "packed item descriptors");
 };
 
 // node of line L along direction d at position n; L enumerates the other
@@ -82,27 +108,46 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS, MINB)
   }
   double fh[DIM][nV];
   double fac_i = 0.0, fac_n = 0.5 * dt;  // weights of levels i and i+1 in the time averages
+  // the block's gradient items, packed once: first node of the line (10
+  // bits), direction (2), variable (4), cell of the block (4); item k of
+  // thread t is s_desc[k][t], -1: none
+  __shared__ int s_desc[C::IPT][C::THREADS];
+  for (int k = 0; k < C::IPT; k++) {
+    const int it = threadIdx.x + k * C::THREADS;
+    int dsc = -1;
+    if (it < C::GITEMS) {
+      constexpr GradPairs<PDE, DIM> GP;
+      const int L = C::LMAJ ? it % LINES : (it / C::NPAIRS) % LINES;
+      const int pr = C::LMAJ ? (it / LINES) % C::NPAIRS : it % C::NPAIRS;
+      const int c = it / (C::NPAIRS * LINES);
+      const int d = GP.d[pr], v = GP.v[pr];
+      dsc = line_node<DIM, b>(d, L, 0) | d << 10 | v << 12 | c << 16;
+    }
+    s_desc[k][threadIdx.x] = dsc;
+  }
   for (int i = 0; i < b; i++) {
     __syncthreads();  // level i complete in sQ; previous per-node phase done with sG
     // spatial gradients of level i, one line per item, into sG[node][d][v]
-    for (int it = threadIdx.x; it < C::GITEMS; it += C::THREADS) {
-      const int v = it % nV;
-      const int L = (it / nV) % LINES;
-      const int d = (it / (nV * LINES)) % DIM;
-      const int c = it / (nV * LINES * DIM);
+    // (the components ncp reads)
+#pragma unroll 1
+    for (int k = 0; k < C::IPT; k++) {
+      const int dsc = s_desc[k][threadIdx.x];
+      if (dsc < 0) continue;
+      const int node0 = dsc & 1023, d = (dsc >> 10) & 3, v = (dsc >> 12) & 15, c = dsc >> 16;
       if (s_cell[c] < 0) continue;
-      const double* q = smem + c * C::SQ;
-      double* g = smem + C::CPB * C::SQ + c * C::SG;
+      const int step = d == 0 ? 1 : d == 1 ? b : b * b;  // node stride along the line
+      const double* q = smem + c * C::SQ + node0 * QS + v;
+      double* g = smem + C::CPB * C::SQ + c * C::SG + node0 * GS + d * nV + v;
       const double idx = s_idx[c][d];
       double f[b];
 #pragma unroll
-      for (int n = 0; n < b; n++) f[n] = idx * q[line_node<DIM, b>(d, L, n) * QS + v];
+      for (int n = 0; n < b; n++) f[n] = idx * q[n * step * QS];
 #pragma unroll
       for (int l = 0; l < b; l++) {
         double s = 0.0;
 #pragma unroll
         for (int n = 0; n < b; n++) s = fma(f[n], T.dudx[l * b + n], s);
-        g[line_node<DIM, b>(d, L, l) * GS + d * nV + v] = s;
+        g[l * step * GS] = s;
       }
     }
     __syncthreads();

@@ -197,7 +197,9 @@ struct EulerTestPDE {
 //                                                       (BgradQ a DIM x nVar tensor)
 //   coefficient_matrix(Q, d, Bn[nVar][nVar])          -- coefficientMatrix
 //   eigenvalues(Q, d, lambda)                         -- eigenvalues
-// with (BgradQ_d)_k = sum_l Bn_d[l][k] (gradQ_d)_l. The z-direction parts are
+// with (BgradQ_d)_k = sum_l Bn_d[l][k] (gradQ_d)_l, and
+//   ncp_uses(d, v)  which gradient components ncp reads (no counterpart in
+//                   the reference, which computes them all). The z-direction parts are
 // the ones written out (commented) beside the x and y parts in the test.
 struct ElasticPDE {
   static constexpr int nVar = 9;
@@ -238,6 +240,14 @@ struct ElasticPDE {
       B[DIM - 1][7] = -irho * G[DIM - 1][4];
       B[DIM - 1][8] = -irho * G[DIM - 1][2];
     }
+  }
+
+  // which gradient components ncp reads: direction d, variable v (the
+  // predictor computes only these; the others would not change its result)
+  __host__ __device__ static constexpr bool ncp_uses(int d, int v) {
+    return d == 0 ? (v == 0 || v == 3 || v == 5 || v >= 6)
+         : d == 1 ? (v == 1 || v == 3 || v == 4 || v >= 6)
+                  : (v == 2 || v == 4 || v == 5 || v >= 6);
   }
 
   // Bn row-major [l][k], all other entries zero

@@ -196,6 +196,16 @@ int exa_mesh_copy_solution(exa_mesh* m, void* host, size_t nbytes, int to_device
 /* Sets t = t0, computes the first admissible step from the current solution
  * and runs the first predictor (Runner::runAsMaster, Runner.cpp:681-700). */
 int exa_mesh_init(exa_mesh* m, double t0);
+/* nsteps time steps with host input and output streamed around them: step
+ * k first takes its solution from host_in + (k % nin) * nbytes, then steps,
+ * then leaves its result at host_out + (k % nout) * nbytes. The copies run on
+ * two streams of their own through device staging buffers, so the upload of
+ * step k+1 and the download of step k-1 overlap the compute of step k (use
+ * pinned host memory). Returns after enqueuing; the mesh stream completes
+ * after the last download (exa_mesh_synchronize). No counterpart in the
+ * reference: host<->device streaming for servers and end-to-end runs. */
+int exa_mesh_step_io(exa_mesh* m, const void* host_in, int nin, void* host_out, int nout, size_t nbytes,
+                     int nsteps);
 /* nsteps non-fused time steps (Riemann, corrector + dt, predictor) without
  * host synchronisation. */
 int exa_mesh_step(exa_mesh* m, int nsteps);
