@@ -22,44 +22,82 @@
 
 namespace exa {
 
-// per order: fineGridProjector1d [third][n][m], the restriction factors
-// w_n P[third][m][n] / (3 w_m) as [third][m][n], and
-// equidistantGridProjector1d [n][i]
-struct AmrTables {
-  double fine[3 * kMaxB * kMaxB];
-  double restr[3 * kMaxB * kMaxB];
-  double equi[kMaxB * kMaxB];
-};
-__device__ AmrTables g_amr_tab[kMaxOrder + 1];
+// Operator tables in constant memory, packed over the orders 1..9 (offset of
+// order N: sum over lower orders of (N'+1)^2, times 3 for the thirds):
+// fineGridProjector1d [third][n][m], the restriction factors
+// w_n P[third][m][n] / (3 w_m) as [third][m][n], equidistantGridProjector1d
+// [n][i]. A block reads one matrix with block-uniform addresses, so the
+// coefficients come from the constant cache by broadcast.
+constexpr int amr_off(int N) { return N <= 1 ? 0 : amr_off(N - 1) + N * N; }
+constexpr int kAmrSq = amr_off(kMaxOrder + 1);  // sum of (N+1)^2 over N = 1..9
+__constant__ double c_amr_fine[3 * kAmrSq];
+__constant__ double c_amr_restr[3 * kAmrSq];
+__constant__ double c_amr_equi[kAmrSq];
 
 // applies a 1-D operator along axis AX (0 = fastest) of a tensor with NAX
-// axes of length b and NV values per node: out[.., m, ..] =
-// sum_n op(m, n) in[.., n, ..]; all threads of the block take part
-template <int b, int NAX, int AX, int NV, class Op>
-__device__ __forceinline__ void apply_axis(const double* in, double* out, Op op) {
-  constexpr int total = NV * ipow(b, NAX), stride = NV * ipow(b, AX);
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int m = (e / stride) % b;
-    const int base = e - m * stride;
-    double s = 0.0;
+// axes of length b and NV values per node, one thread per line:
+// out[.., m, ..] = sum_n M[m][n] in[.., n, ..], M given as a pointer and
+// row/column strides (compile-time indices: the coefficients are read
+// with uniform addresses); all threads of the block take part
+template <int b, int NAX, int AX, int NV, int RS, int CS>
+__device__ __forceinline__ void apply_axis(const double* in, double* out, const double* M) {
+  constexpr int total = NV * ipow(b, NAX), stride = NV * ipow(b, AX), lines = total / b;
+  for (int it = threadIdx.x; it < lines; it += blockDim.x) {
+    const int lo = it % stride, hi = it / stride;
+    const int base = hi * stride * b + lo;
+    double x[b];
 #pragma unroll
-    for (int n = 0; n < b; n++) s = fma(op(m, n), in[base + n * stride], s);
-    out[e] = s;
+    for (int n = 0; n < b; n++) x[n] = in[base + n * stride];
+#pragma unroll
+    for (int m = 0; m < b; m++) {
+      double s = 0.0;
+#pragma unroll
+      for (int n = 0; n < b; n++) s = fma(M[m * RS + n * CS], x[n], s);
+      out[base + m * stride] = s;
+    }
   }
 }
 
-// the operator of each axis in turn (axis k uses ops(k)), ping-ponging
+// the operator of each axis in turn (axis k uses mats[k]), ping-ponging
 // between the two buffers; returns the buffer holding the result
-template <int b, int NAX, int NV, class Ops>
-__device__ __forceinline__ double* apply_axes(double* cur, double* nxt, Ops ops) {
+template <int b, int NAX, int NV, int RS, int CS>
+__device__ __forceinline__ double* apply_axes(double* cur, double* nxt, const double* const* mats) {
   __syncthreads();
-  apply_axis<b, NAX, 0, NV>(cur, nxt, ops(0));
+  apply_axis<b, NAX, 0, NV, RS, CS>(cur, nxt, mats[0]);
   if (NAX == 1) return nxt;
   __syncthreads();
-  apply_axis<b, NAX, 1, NV>(nxt, cur, ops(1));
+  apply_axis<b, NAX, 1, NV, RS, CS>(nxt, cur, mats[1]);
   if (NAX == 2) return cur;
   __syncthreads();
-  apply_axis<b, NAX, 2, NV>(cur, nxt, ops(2));
+  apply_axis<b, NAX, 2, NV, RS, CS>(cur, nxt, mats[2]);
+  return nxt;
+}
+
+// one axis of a single-level transfer: the digit picks the third; each case
+// has a compile-time table address, so the coefficients are constant-bank
+// operands (prolongation P[n][m], restriction R[m][n])
+template <int N, int NAX, int AX, int NV, bool R>
+__device__ __forceinline__ void transfer_axis(const double* in, double* out, int digit) {
+  constexpr int b = N + 1, base = 3 * amr_off(N), RS = R ? b : 1, CS = R ? 1 : b;
+  const double* tab = R ? c_amr_restr : c_amr_fine;
+  if (digit == 0)
+    apply_axis<b, NAX, AX, NV, RS, CS>(in, out, tab + base);
+  else if (digit == 1)
+    apply_axis<b, NAX, AX, NV, RS, CS>(in, out, tab + base + b * b);
+  else
+    apply_axis<b, NAX, AX, NV, RS, CS>(in, out, tab + base + 2 * b * b);
+}
+
+template <int N, int NAX, int NV, bool R>
+__device__ __forceinline__ double* transfer_level(double* cur, double* nxt, const int* digit) {
+  __syncthreads();
+  transfer_axis<N, NAX, 0, NV, R>(cur, nxt, digit[0]);
+  if (NAX == 1) return nxt;
+  __syncthreads();
+  transfer_axis<N, NAX, 1, NV, R>(nxt, cur, digit[1]);
+  if (NAX == 2) return cur;
+  __syncthreads();
+  transfer_axis<N, NAX, 2, NV, R>(cur, nxt, digit[2]);
   return nxt;
 }
 
@@ -84,7 +122,6 @@ __device__ void amr_transfer(const double* __restrict__ src, double* __restrict_
                              const int* index, bool restrict_, double* bufA, double* bufB) {
   constexpr int b = N + 1;
   constexpr int size = NV * ipow(b, NAX);
-  const AmrTables& A = g_amr_tab[N];
   for (int e = threadIdx.x; e < size; e += blockDim.x) bufA[e] = src[e];
   int rest[3] = {index[0], index[1], index[2]};
   int sig = 1;
@@ -104,12 +141,8 @@ __device__ void amr_transfer(const double* __restrict__ src, double* __restrict_
       }
     }
     sig = sig > 1 ? sig / 3 : 1;
-    const double* tab = restrict_ ? A.restr : A.fine;
-    double* res = apply_axes<b, NAX, NV>(cur, nxt, [&](int ax) {
-      const double* M = tab + digit[ax] * b * b;
-      const bool r = restrict_;
-      return [M, r](int m, int n) { return r ? M[m * b + n] : M[n * b + m]; };
-    });
+    double* res = restrict_ ? transfer_level<N, NAX, NV, true>(cur, nxt, digit)
+                            : transfer_level<N, NAX, NV, false>(cur, nxt, digit);
     nxt = res == cur ? nxt : cur;
     cur = res;
   }
@@ -177,10 +210,10 @@ __global__ void __launch_bounds__(256) plot_vertex_kernel(const double* __restri
   __shared__ double bufA[P * ND], bufB[P * ND];
   const int c = blockIdx.x;
   if (c >= ncells) return;
-  const AmrTables& A = g_amr_tab[N];
   for (int e = threadIdx.x; e < P * ND; e += blockDim.x) bufA[e] = luh[(size_t)c * P * ND + e];
-  const double* E = A.equi;
-  double* cur = apply_axes<b, DIM, ND>(bufA, bufB, [E](int) { return [E](int i, int n) { return E[n * b + i]; }; });
+  const double* E = c_amr_equi + amr_off(N);  // E[n][i]: out[i] = sum_n E[n][i] in[n]
+  const double* mats[3] = {E, E, E};
+  double* cur = apply_axes<b, DIM, ND, 1, b>(bufA, bufB, mats);
   __syncthreads();
   for (int e = threadIdx.x; e < P * ND; e += blockDim.x) out[(size_t)c * P * ND + e] = cur[e];
 }

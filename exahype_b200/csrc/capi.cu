@@ -87,10 +87,10 @@ static int upload_tables() {
     if (d == dev) return EXA_OK;
   std::vector<OrderTables> h(kMaxOrder + 1);
   std::vector<LimiterTables> hl(kMaxOrder + 1);
-  std::vector<AmrTables> ha(kMaxOrder + 1);
+  std::vector<double> afine(3 * kAmrSq, 0.0), arestr(3 * kAmrSq, 0.0), aequi(kAmrSq, 0.0);
   std::memset(h.data(), 0, sizeof(OrderTables) * h.size());
   std::memset(hl.data(), 0, sizeof(LimiterTables) * hl.size());
-  std::memset(ha.data(), 0, sizeof(AmrTables) * ha.size());
+
   for (int N = 1; N <= kMaxOrder; N++) {
     const int b = N + 1, bl = 2 * N + 1;
     OrderTables& t = h[N];
@@ -113,17 +113,20 @@ static int upload_tables() {
       l.uh2lim[i] = exa_tab_uh2lim[exa_tab_uh2lim_off[N] + i];
       l.lim2uh[i] = exa_tab_lim2uh[exa_tab_lim2uh_off[N] + i];
     }
-    for (int i = 0; i < 3 * b * b; i++) ha[N].fine[i] = exa_tab_fineGridProjector1d[exa_tab_fineGridProjector1d_off[N] + i];
+    double* fine = afine.data() + 3 * amr_off(N);
+    for (int i = 0; i < 3 * b * b; i++) fine[i] = exa_tab_fineGridProjector1d[exa_tab_fineGridProjector1d_off[N] + i];
     for (int j = 0; j < 3; j++)
       for (int m = 0; m < b; m++)
         for (int n = 0; n < b; n++)
-          ha[N].restr[(j * b + m) * b + n] = t.w[n] * ha[N].fine[(j * b + m) * b + n] / (3.0 * t.w[m]);
+          arestr[3 * amr_off(N) + (j * b + m) * b + n] = t.w[n] * fine[(j * b + m) * b + n] / (3.0 * t.w[m]);
     for (int i = 0; i < b * b; i++)
-      ha[N].equi[i] = exa_tab_equidistantGridProjector1d[exa_tab_equidistantGridProjector1d_off[N] + i];
+      aequi[amr_off(N) + i] = exa_tab_equidistantGridProjector1d[exa_tab_equidistantGridProjector1d_off[N] + i];
   }
   EXA_CUDA(cudaMemcpyToSymbol(c_tab, h.data(), sizeof(OrderTables) * h.size()));
   EXA_CUDA(cudaMemcpyToSymbol(g_lim_tab, hl.data(), sizeof(LimiterTables) * hl.size()));
-  EXA_CUDA(cudaMemcpyToSymbol(g_amr_tab, ha.data(), sizeof(AmrTables) * ha.size()));
+  EXA_CUDA(cudaMemcpyToSymbol(c_amr_fine, afine.data(), sizeof(double) * afine.size()));
+  EXA_CUDA(cudaMemcpyToSymbol(c_amr_restr, arestr.data(), sizeof(double) * arestr.size()));
+  EXA_CUDA(cudaMemcpyToSymbol(c_amr_equi, aequi.data(), sizeof(double) * aequi.size()));
   done_dev.push_back(dev);
   return EXA_OK;
 }
