@@ -322,31 +322,32 @@ struct LinearLaunch {
   using CC = CorrectorCfg<DIM, N, PDE>;
   using KC = CKCfg<DIM, N, PDE>;
   static_assert(KC::SMEM <= 227 * 1024, "shared memory");
-  template <int MINB>
+  template <int NREG>
   static int launch_ck(const double* luh, double* qb, double* fb, double* du, const double* dt, Geometry g, int n,
                        const int* list, const int* cnt, double* qhi, double* fhi, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
-      EXA_CUDA(cudaFuncSetAttribute(ck_predictor_kernel<DIM, N, PDE, MINB>,
+      EXA_CUDA(cudaFuncSetAttribute(ck_predictor_kernel<DIM, N, PDE, NREG>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KC::SMEM));
       attr = true;
     }
-    ck_predictor_kernel<DIM, N, PDE, MINB><<<(n + KC::CPB - 1) / KC::CPB, KC::THREADS, KC::SMEM, st>>>(
+    ck_predictor_kernel<DIM, N, PDE, NREG><<<(n + KC::CPB - 1) / KC::CPB, KC::THREADS, KC::SMEM, st>>>(
         luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi);
     EXA_LAUNCHED();
     return EXA_OK;
   }
-  // variant 0: register budget of one block per SM; 1: of two blocks per SM
-  // (where their shared memory fits); the autotuner picks between them
+  // variant 0: the register cap of one block per SM; 1: of two blocks per
+  // SM (where their shared memory fits); the autotuner picks
   static constexpr bool kTwo = 2 * KC::SMEM <= 227 * 1024;
+  static constexpr int kReg1 = regs_for_blocks<KC::THREADS, 1>(), kReg2 = regs_for_blocks<KC::THREADS, 2>();
   static int predictor(const double* luh, double* qb, double* fb, double* du, int*, const double* dt, Geometry g,
                        int n, const int* list, const int* cnt, PredictorTemps tmp, bool temps, unsigned long long*,
                        int variant, cudaStream_t st) {
     if (n <= 0) return EXA_OK;
     double* qhi = temps ? tmp.lQhi : nullptr;
     double* fhi = temps ? tmp.lFhi : nullptr;
-    if (variant == 1 && kTwo) return launch_ck<kTwo ? 2 : 1>(luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi, st);
-    return launch_ck<1>(luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi, st);
+    if (variant == 1 && kTwo) return launch_ck<kTwo ? kReg2 : kReg1>(luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi, st);
+    return launch_ck<kReg1>(luh, qb, fb, du, dt, g, n, list, cnt, qhi, fhi, st);
   }
   static int riemann(const double* qb, double* fb, const int* l, const int* r, const int* d, int n, const int* gate,
                      cudaStream_t st) {

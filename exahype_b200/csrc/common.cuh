@@ -40,6 +40,16 @@ __device__ LimiterTables g_lim_tab[kMaxOrder + 1];
 
 constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
 
+// register cap per thread that lets BLOCKS blocks of THREADS threads be
+// resident on one SM: the warps are spread over the 4 sub-partitions, each
+// with 16 K registers, allocated in multiples of 8 per thread
+template <int THREADS, int BLOCKS>
+constexpr int regs_for_blocks() {
+  return (16384 / (((BLOCKS * ((THREADS + 31) / 32)) + 3) / 4 * 32)) / 8 * 8 > 255
+             ? 255
+             : (16384 / (((BLOCKS * ((THREADS + 31) / 32)) + 3) / 4 * 32)) / 8 * 8;
+}
+
 // Minimum-stability constants of stableTimeStepSize (kernels/aderdg/generic/c/3d/stableTimeStepSize.cpph:33-34).
 __host__ __device__ constexpr double pnpm(int N) {
   return N == 0 ? 1.0 : N == 1 ? 0.33 : N == 2 ? 0.17 : N == 3 ? 0.1 : N == 4 ? 0.069 : N == 5 ? 0.045

@@ -67,8 +67,9 @@ __device__ __forceinline__ int line_node(int d, int L, int n) {
   return d == 0 ? (a0 * b + a1) * b + n : d == 1 ? (a0 * b + n) * b + a1 : (n * b + a0) * b + a1;
 }
 
-template <int DIM, int N, class PDE, int MINB = 1>
-__global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS, MINB)
+// NREG: register cap per thread, regs_for_blocks<THREADS, blocks per SM>()
+template <int DIM, int N, class PDE, int NREG>
+__global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
     ck_predictor_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                         double* __restrict__ lduh, const double* __restrict__ dt_ptr, Geometry geo, int ncells,
                         const int* __restrict__ cell_list, const int* __restrict__ count,
@@ -151,22 +152,27 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS, MINB)
       }
     }
     __syncthreads();
-    // per node: non-conservative product, time averages, next level
+    // per node: non-conservative product one direction at a time (few
+    // registers live), time averages, next level
     {
-      double B[DIM][nV];
-      PDE::template ncp<DIM>(sQ + p * QS, reinterpret_cast<const double(*)[nV]>(sG + p * GS), B);
+      double qn[nV];
 #pragma unroll
-      for (int d = 0; d < DIM; d++)
+      for (int v = 0; v < nV; v++) qn[v] = 0.0;
 #pragma unroll
-        for (int v = 0; v < nV; v++) fh[d][v] = i == 0 ? B[d][v] : fma(fac_i, B[d][v], fh[d][v]);
+      for (int d = 0; d < DIM; d++) {
+        double B[nV];
+        PDE::ncp_dir(sQ + p * QS, d, sG + p * GS + d * nV, B);
+#pragma unroll
+        for (int v = 0; v < nV; v++) {
+          fh[d][v] = i == 0 ? B[v] : fma(fac_i, B[v], fh[d][v]);
+          qn[v] -= B[v];
+        }
+      }
       if (i + 1 < b) {
 #pragma unroll
         for (int v = 0; v < nV; v++) {
-          double qn = 0.0;
-#pragma unroll
-          for (int d = 0; d < DIM; d++) qn -= B[d][v];
-          qh[v] = fma(fac_n, qn, qh[v]);
-          sQ[p * QS + v] = qn;  // own node only; parameters stay
+          qh[v] = fma(fac_n, qn[v], qh[v]);
+          sQ[p * QS + v] = qn[v];  // own node only; parameters stay
         }
       }
       fac_i = fac_n;

@@ -195,6 +195,7 @@ struct EulerTestPDE {
 // ask of the user solver instead of a flux:
 //   ncp<DIM>(Q, gradQ[DIM][nVar], BgradQ[DIM][nVar]) -- nonConservativeProduct
 //                                                       (BgradQ a DIM x nVar tensor)
+//   ncp_dir(Q, d, gradQ_d, BgradQ_d)                  -- its direction-d part
 //   coefficient_matrix(Q, d, Bn[nVar][nVar])          -- coefficientMatrix
 //   eigenvalues(Q, d, lambda)                         -- eigenvalues
 // with (BgradQ_d)_k = sum_l Bn_d[l][k] (gradQ_d)_l, and
@@ -207,39 +208,48 @@ struct ElasticPDE {
   static constexpr int nObs = 9;
   static constexpr bool kLinear = true;
 
-  template <int DIM>
-  __device__ static void ncp(const double* Q, const double (*G)[nVar], double (*B)[nVar]) {
+  // the product of one direction: B_d = B_d(Q) gradQ_d (a linear PDE's
+  // product separates by direction)
+  __device__ static void ncp_dir(const double* Q, int d, const double* G, double* B) {
     const double lam = Q[9], mu = Q[10], irho = 1.0 / Q[11];
     const double lm2 = lam + 2 * mu;
-    B[0][0] = -lm2 * G[0][6];
-    B[0][1] = -lam * G[0][6];
-    B[0][2] = -lam * G[0][6];
-    B[0][3] = -mu * G[0][7];
-    B[0][4] = 0.0;
-    B[0][5] = -mu * G[0][8];
-    B[0][6] = -irho * G[0][0];
-    B[0][7] = -irho * G[0][3];
-    B[0][8] = -irho * G[0][5];
-    B[1][0] = -lam * G[1][7];
-    B[1][1] = -lm2 * G[1][7];
-    B[1][2] = -lam * G[1][7];
-    B[1][3] = -mu * G[1][6];
-    B[1][4] = -mu * G[1][8];
-    B[1][5] = 0.0;
-    B[1][6] = -irho * G[1][3];
-    B[1][7] = -irho * G[1][1];
-    B[1][8] = -irho * G[1][4];
-    if (DIM == 3) {
-      B[DIM - 1][0] = -lam * G[DIM - 1][8];
-      B[DIM - 1][1] = -lam * G[DIM - 1][8];
-      B[DIM - 1][2] = -lm2 * G[DIM - 1][8];
-      B[DIM - 1][3] = 0.0;
-      B[DIM - 1][4] = -mu * G[DIM - 1][7];
-      B[DIM - 1][5] = -mu * G[DIM - 1][6];
-      B[DIM - 1][6] = -irho * G[DIM - 1][5];
-      B[DIM - 1][7] = -irho * G[DIM - 1][4];
-      B[DIM - 1][8] = -irho * G[DIM - 1][2];
+    if (d == 0) {
+      B[0] = -lm2 * G[6];
+      B[1] = -lam * G[6];
+      B[2] = -lam * G[6];
+      B[3] = -mu * G[7];
+      B[4] = 0.0;
+      B[5] = -mu * G[8];
+      B[6] = -irho * G[0];
+      B[7] = -irho * G[3];
+      B[8] = -irho * G[5];
+    } else if (d == 1) {
+      B[0] = -lam * G[7];
+      B[1] = -lm2 * G[7];
+      B[2] = -lam * G[7];
+      B[3] = -mu * G[6];
+      B[4] = -mu * G[8];
+      B[5] = 0.0;
+      B[6] = -irho * G[3];
+      B[7] = -irho * G[1];
+      B[8] = -irho * G[4];
+    } else {
+      B[0] = -lam * G[8];
+      B[1] = -lam * G[8];
+      B[2] = -lm2 * G[8];
+      B[3] = 0.0;
+      B[4] = -mu * G[7];
+      B[5] = -mu * G[6];
+      B[6] = -irho * G[5];
+      B[7] = -irho * G[4];
+      B[8] = -irho * G[2];
     }
+  }
+
+  template <int DIM>
+  __device__ static void ncp(const double* Q, const double (*G)[nVar], double (*B)[nVar]) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) ncp_dir(Q, d, G[d], B[d]);
   }
 
   // which gradient components ncp reads: direction d, variable v (the
