@@ -294,6 +294,18 @@ class Mesh:
     def init(self, t0=0.0):
         _check(load().exa_mesh_init(self._h, ctypes.c_double(t0)), "exa_mesh_init")
 
+    def init_fused(self, t0=0.0, weight=0.99):
+        """fused time stepping (predictor right after the update with an
+        estimated step, rerun with weight * stable when the estimate was too
+        large) instead of init()"""
+        _check(load().exa_mesh_init_fused(self._h, ctypes.c_double(t0), ctypes.c_double(weight)),
+               "exa_mesh_init_fused")
+
+    def fused_state(self):
+        p, r = ctypes.c_double(), ctypes.c_longlong()
+        _check(load().exa_mesh_fused_state(self._h, ctypes.byref(p), ctypes.byref(r)), "exa_mesh_fused_state")
+        return dict(predictor_dt=p.value, reruns=r.value)
+
     def step(self, nsteps=1):
         _check(load().exa_mesh_step(self._h, int(nsteps)), "exa_mesh_step")
 

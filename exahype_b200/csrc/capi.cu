@@ -477,6 +477,11 @@ struct exa_mesh {
   double *stage_in = nullptr, *stage_out = nullptr;
   cudaStream_t io_in = nullptr, io_out = nullptr;
   cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
+  // fused time stepping (exa_mesh_init_fused): rerun weight and the device
+  // count of cells whose predictor is rerun (0 or all)
+  bool fused = false;
+  double weight = 0.99;
+  int* rerun = nullptr;
 };
 
 namespace {
@@ -768,6 +773,7 @@ static void mesh_free(exa_mesh* m) {
     if (e) cudaEventDestroy(e);
   sfree(m->stage_in, m->stream);
   sfree(m->stage_out, m->stream);
+  sfree(m->rerun, m->stream);
   if (m->io_in) cudaStreamDestroy(m->io_in);
   if (m->io_out) cudaStreamDestroy(m->io_out);
   for (void* p : {(void*)m->luh, (void*)m->lduh, (void*)m->lQhbnd, (void*)m->lFhbnd, (void*)m->scal, (void*)m->iters,
@@ -917,17 +923,101 @@ int exa_mesh_copy_solution(exa_mesh* m, void* host, size_t nbytes, int to_device
   return EXA_OK;
 }
 
-static int mesh_predict(exa_mesh* m) {
+// The predictor of every cell; fused time stepping runs it with its own step
+// size (scal[5]) and, for the rerun, only when *count (device) is not 0.
+static int mesh_predict(exa_mesh* m, const int* count = nullptr) {
   const KernelSet& k = m->s->k;
   PhaseTimer pt(m, 0);
   m->phase_launches[0] += 2;
-  return k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->scal + 0, m->geo, m->ncells, nullptr,
-                     nullptr, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
+  return k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->scal + (m->fused ? 5 : 0), m->geo,
+                     m->ncells, nullptr, count, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
+}
+
+// Fused time stepping scalars: [0] corrector step, [1] min-reduction target,
+// [2] corrector time stamp, [3] steps, [4] predictor time stamp, [5]
+// predictor step, [6] predictor reruns (ADERDGSolver's _minCorrector*/
+// _minPredictor*). Arithmetic in round-to-nearest operations, as the
+// reference's unfused evaluation.
+__global__ void fused_init_kernel(double* scal) {
+  const double s0 = scal[1];  // min admissible step of the initial data
+  scal[0] = s0;
+  scal[5] = s0;
+  scal[4] = __dadd_rn(scal[2], s0);
+  scal[1] = __longlong_as_double(0x7fefffffffffffffll);
+  scal[6] = 0.0;
+}
+
+// end of a fused step (SolutionUpdate::endIteration,
+// TimeStepSizeComputation::reinitialiseTimeStepDataIfLastPredictorTimeStepSizeWasInstable,
+// ADERDGSolver::startNewTimeStep; TimeStepSizeComputation.cpp:167-204,
+// ADERDGSolver.cpp:559-592): s = min stable step after the update; a
+// predictor step above s is replaced by w s (and the predictor rerun), else
+// the next estimate is the mean of the used step and w s
+__global__ void fused_advance_kernel(double* scal, double w, int* rerun, int ncells) {
+  const double s = scal[1];
+  double next = __longlong_as_double(0x7fefffffffffffffll);
+  next = (s < next) ? s : next;
+  double pdt = scal[5];
+  const double used = (pdt == 0.0) ? s : pdt;
+  const bool unstable = used > s;
+  if (unstable) {
+    const double ws = __dmul_rn(w, s);
+    next = (ws < next) ? ws : next;
+    pdt = ws;
+  } else {
+    const double avg = __dmul_rn(0.5, __dadd_rn(used, __dmul_rn(w, s)));
+    next = (avg < next) ? avg : next;
+  }
+  scal[2] = scal[4];
+  scal[0] = pdt;
+  scal[4] = __dadd_rn(scal[4], pdt);
+  scal[5] = next;
+  scal[1] = __longlong_as_double(0x7fefffffffffffffll);
+  scal[3] += 1.0;
+  if (unstable) scal[6] += 1.0;
+  *rerun = unstable ? ncells : 0;
+}
+
+int exa_mesh_init_fused(exa_mesh* m, double t0, double weight) {
+  if (!m || !(weight > 0.0) || weight > 1.0) return fail(EXA_ERR_ARG, "exa_mesh_init_fused: bad argument");
+  const KernelSet& k = m->s->k;
+  if (!m->rerun && !salloc(&m->rerun, sizeof(int), m->stream)) {
+    cudaGetLastError();
+    m->rerun = nullptr;
+    return fail(EXA_ERR_NOMEM, "exa_mesh_init_fused: device allocation failed");
+  }
+  m->fused = true;
+  m->weight = weight;
+  init_scalars_kernel<<<1, 1, 0, m->stream>>>(m->scal, t0);
+  EXA_LAUNCHED();
+  EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, m->stream));
+  EXA_CUDA(cudaMemsetAsync(m->rerun, 0, sizeof(int), m->stream));
+  int rc = k.corrector(m->luh, nullptr, nullptr, nullptr, m->scal + 1, m->geo, m->ncells, nullptr, 0, nullptr,
+                       m->stream);
+  if (rc) return rc;
+  fused_init_kernel<<<1, 1, 0, m->stream>>>(m->scal);
+  EXA_LAUNCHED();
+  rc = mesh_predict(m);
+  if (rc) return rc;
+  m->initialised = true;
+  return EXA_OK;
+}
+
+int exa_mesh_fused_state(exa_mesh* m, double* predictor_dt, long long* reruns) {
+  if (!m) return fail(EXA_ERR_ARG, "exa_mesh_fused_state: null mesh");
+  if (!m->fused) return fail(EXA_ERR_STATE, "exa_mesh_fused_state: the mesh is not in fused time stepping");
+  double h[7];
+  EXA_CUDA(cudaMemcpyAsync(h, m->scal, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+  EXA_CUDA(cudaStreamSynchronize(m->stream));
+  if (predictor_dt) *predictor_dt = h[5];
+  if (reruns) *reruns = (long long)h[6];
+  return EXA_OK;
 }
 
 int exa_mesh_init(exa_mesh* m, double t0) {
   if (!m) return fail(EXA_ERR_ARG, "exa_mesh_init: null mesh");
   const KernelSet& k = m->s->k;
+  m->fused = false;
   init_scalars_kernel<<<1, 1, 0, m->stream>>>(m->scal, t0);
   EXA_LAUNCHED();
   EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, m->stream));
@@ -967,6 +1057,17 @@ static int mesh_one_step(exa_mesh* m) {
   }
   {
     PhaseTimer pt(m, 3);
+    if (m->fused) {
+      // the predictor of the fused step runs with its own step size right
+      // after the update (no global reduction in between), then the step
+      // bookkeeping, then the rerun, which does nothing unless needed
+      rc = mesh_predict(m);
+      if (rc) return rc;
+      fused_advance_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->weight, m->rerun, m->ncells);
+      EXA_LAUNCHED();
+      m->phase_launches[3] += 1;
+      return mesh_predict(m, m->rerun);
+    }
     advance_kernel<<<1, 1, 0, m->stream>>>(m->scal);
     EXA_LAUNCHED();
     m->phase_launches[3] += 1;

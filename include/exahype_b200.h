@@ -196,6 +196,19 @@ int exa_mesh_copy_solution(exa_mesh* m, void* host, size_t nbytes, int to_device
 /* Sets t = t0, computes the first admissible step from the current solution
  * and runs the first predictor (Runner::runAsMaster, Runner.cpp:681-700). */
 int exa_mesh_init(exa_mesh* m, double t0);
+/* Fused time stepping (the reference's fuse-algorithmic-steps option,
+ * exahype/runners/Runner.cpp:1053-1114, with global time steps): instead of
+ * exa_mesh_init. Every later step runs the predictor right after the update
+ * with an estimated step size, so no global reduction separates the two;
+ * when the stable step of the updated solution turns out smaller than the
+ * estimate, the estimate is replaced by weight * stable and the predictor is
+ * rerun (TimeStepSizeComputation.cpp:167-204, ADERDGSolver.cpp:559-613);
+ * weight in (0, 1] is the reference's fuse-algorithmic-steps-factor.
+ * exa_mesh_state then reports the corrector time stamp and step size. */
+int exa_mesh_init_fused(exa_mesh* m, double t0, double weight);
+/* fused time stepping: the predictor step size estimate and the number of
+ * predictor reruns so far */
+int exa_mesh_fused_state(exa_mesh* m, double* predictor_dt, long long* reruns);
 /* nsteps time steps with host input and output streamed around them: step
  * k first takes its solution from host_in + (k % nin) * nbytes, then steps,
  * then leaves its result at host_out + (k % nout) * nbytes. The copies run on

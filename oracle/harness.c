@@ -11,6 +11,27 @@
  *           4. per cell: predictor + volume integral with the new dt
  *                                                        (mappings/Prediction.cpp)
  *   loop:   while t < t_end && dt > 0 (no clamp of the last step).
+ *
+ * Fused time stepping (the reference's fuse-algorithmic-steps option,
+ * global time stepping, one rank), hrn_init_fused / hrn_step_fused:
+ *   init:   s0 = min stable step of u0; corrector and predictor step s0,
+ *           predictor stamp t0 + s0 (TimeStepSizeComputation::endIteration ->
+ *           ADERDGSolver::updateTimeStepSizesFused, ADERDGSolver.cpp:594-613);
+ *           predictor(u0, s0)
+ *   step:   Riemann / boundary; per cell corrector with the corrector step,
+ *           then at once the predictor with the predictor step (fusedTimeStep,
+ *           ADERDGSolver.cpp:1853-1878); s = min stable step of the updated
+ *           solution; used = predictor step (s if 0); if used > s the
+ *           predictor step becomes w s and the next estimate w s, else the next
+ *           estimate is min(s, (used + w s) / 2)
+ *           (TimeStepSizeComputation.cpp:167-204); startNewTimeStep
+ *           (ADERDGSolver.cpp:559-592): corrector stamp = predictor stamp,
+ *           corrector step = predictor step, predictor stamp += predictor
+ *           step, predictor step = next estimate; if the step was too large
+ *           the predictor is rerun with the new predictor step
+ *           (Runner.cpp:1103-1109, mappings/Prediction.cpp)
+ *   loop:   while corrector stamp < t_end && corrector step > 0
+ *           (Solver::getMinSolverTimeStampOfAllSolvers: the corrector stamp).
  * The per-cell / per-face kernels come from a backend table, so the same
  * sequencing drives both the C restatement and the reference kernels.
  * Cells run in parallel on `nthreads` POSIX threads.
@@ -42,8 +63,13 @@ typedef struct {
   double *luh, *lduh, *lQhbnd, *lFhbnd;
   int *fl, *fr, *fd, nfaces, *bcell, *bface, nb;
   int* iters;
-  double t, dt;
+  double t, dt;     /* corrector time stamp and step size */
+  double pdt;       /* step size of the next predictor call */
   long steps, sweeps;
+  /* fused time stepping */
+  int fused;
+  double w, tp, next;  /* rerun weight, predictor time stamp, next-step estimate */
+  long reruns;
 } hrn_mesh;
 
 static int hrn_cid(const hrn_mesh* m, int i, int j, int k) { return (k * m->cells[1] + j) * m->cells[0] + i; }
@@ -125,7 +151,7 @@ static void hrn_run_range(hrn_job* j) {
   j->dtmin = DBL_MAX;
   for (int i = j->lo; i < j->hi; i++) {
     if (j->phase == 0) { /* predictor + volume integral */
-      m->iters[i] = k->predictor(k->ctx, m->luh + (size_t)i * P * nD, m->dx, m->dt, m->lQhbnd + (size_t)i * D2 * F * nD,
+      m->iters[i] = k->predictor(k->ctx, m->luh + (size_t)i * P * nD, m->dx, m->pdt, m->lQhbnd + (size_t)i * D2 * F * nD,
                                  m->lFhbnd + (size_t)i * D2 * F * nV, m->lduh + (size_t)i * P * nV);
     } else if (j->phase == 1) { /* interior face */
       const int cl = m->fl[i], cr = m->fr[i], d = m->fd[i];
@@ -186,17 +212,68 @@ static void hrn_init(hrn_mesh* m, double t0) {
   m->t = t0;
   m->steps = 0;
   m->sweeps = 0;
+  m->fused = 0;
   m->dt = hrn_parallel(m, 4, m->ncells);
+  m->pdt = m->dt;
   hrn_predict(m);
 }
 
+static void hrn_init_fused(hrn_mesh* m, double t0, double w) {
+  m->t = t0;
+  m->steps = 0;
+  m->sweeps = 0;
+  m->fused = 1;
+  m->w = w;
+  m->reruns = 0;
+  const double s0 = hrn_parallel(m, 4, m->ncells);
+  m->dt = s0;
+  m->pdt = s0;
+  m->tp = t0 + s0;
+  m->next = DBL_MAX;
+  hrn_predict(m);
+}
+
+static void hrn_step_fused(hrn_mesh* m) {
+  hrn_parallel(m, 1, m->nfaces);
+  hrn_parallel(m, 2, m->nb);
+  const double s = hrn_parallel(m, 3, m->ncells); /* corrector with m->dt */
+  hrn_predict(m);                                 /* predictor with m->pdt */
+  double next = DBL_MAX;
+  next = (s < next) ? s : next; /* updateMinNextPredictorTimeStepSize */
+  const double used = (m->pdt == 0.0) ? s : m->pdt;
+  const int unstable = used > s;
+  if (unstable) {
+    const double ws = m->w * s;
+    next = (ws < next) ? ws : next;
+    m->pdt = ws;
+  } else {
+    const double avg = 0.5 * (used + m->w * s);
+    next = (avg < next) ? avg : next;
+  }
+  /* startNewTimeStep */
+  m->t = m->tp;
+  m->dt = m->pdt;
+  m->tp = m->tp + m->pdt;
+  m->pdt = next;
+  m->steps++;
+  if (unstable) {
+    m->reruns++;
+    hrn_predict(m);
+  }
+}
+
 static void hrn_step(hrn_mesh* m, int n) {
+  if (m->fused) {
+    for (int s = 0; s < n; s++) hrn_step_fused(m);
+    return;
+  }
   for (int s = 0; s < n; s++) {
     hrn_parallel(m, 1, m->nfaces);
     hrn_parallel(m, 2, m->nb);
     const double dtn = hrn_parallel(m, 3, m->ncells);
     m->t += m->dt;
     m->dt = dtn;
+    m->pdt = dtn;
     m->steps++;
     hrn_predict(m);
   }

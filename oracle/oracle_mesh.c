@@ -56,6 +56,10 @@ static size_t nsol(hrn_mesh* m) { return (size_t)m->ncells * m->P * m->k.ndata; 
 void orc_mesh_set_solution(void* h, const double* u) { hrn_mesh* m = ((orc_mesh*)h)->m; memcpy(m->luh, u, nsol(m) * 8); }
 void orc_mesh_get_solution(void* h, double* u) { hrn_mesh* m = ((orc_mesh*)h)->m; memcpy(u, m->luh, nsol(m) * 8); }
 void orc_mesh_init(void* h, double t0) { hrn_init(((orc_mesh*)h)->m, t0); }
+/* fused time stepping with rerun weight w (hrn_init_fused in harness.c) */
+void orc_mesh_init_fused(void* h, double t0, double w) { hrn_init_fused(((orc_mesh*)h)->m, t0, w); }
+double orc_mesh_predictor_dt(void* h) { return ((orc_mesh*)h)->m->pdt; }
+long orc_mesh_reruns(void* h) { return ((orc_mesh*)h)->m->reruns; }
 void orc_mesh_step(void* h, int n) { hrn_step(((orc_mesh*)h)->m, n); }
 int orc_mesh_run_until(void* h, double t_end, int max_steps) { return hrn_run_until(((orc_mesh*)h)->m, t_end, max_steps); }
 double orc_mesh_time(void* h) { return ((orc_mesh*)h)->m->t; }

@@ -271,6 +271,11 @@ class Mesh:
     def init(self, t0=0.0):
         self._f("init")(self._h, ctypes.c_double(t0))
 
+    def init_fused(self, t0=0.0, weight=0.99):
+        """fused time stepping (the reference's fuse-algorithmic-steps) with
+        the predictor-rerun weight"""
+        self._f("init_fused")(self._h, ctypes.c_double(t0), ctypes.c_double(weight))
+
     def step(self, n=1):
         self._f("step")(self._h, int(n))
 
@@ -280,6 +285,13 @@ class Mesh:
     def state(self):
         return dict(t=self._f("time")(self._h), dt=self._f("dt")(self._h), steps=self._f("steps")(self._h),
                     picard_sweeps=self._f("sweeps")(self._h))
+
+    def fused_state(self):
+        f = self._f("predictor_dt")
+        f.restype = ctypes.c_double
+        g = self._f("reruns")
+        g.restype = ctypes.c_long
+        return dict(predictor_dt=f(self._h), reruns=g(self._h))
 
 
 class LimitingMesh:

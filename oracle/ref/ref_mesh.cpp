@@ -99,6 +99,9 @@ void REFNAME(mesh_destroy)(void* h) { RefMesh* r = (RefMesh*)h; hrn_destroy(r->m
 void REFNAME(mesh_set_solution)(void* h, const double* u) { hrn_mesh* m = ((RefMesh*)h)->m; memcpy(m->luh, u, nsol(m) * 8); }
 void REFNAME(mesh_get_solution)(void* h, double* u) { hrn_mesh* m = ((RefMesh*)h)->m; memcpy(u, m->luh, nsol(m) * 8); }
 void REFNAME(mesh_init)(void* h, double t0) { hrn_init(((RefMesh*)h)->m, t0); }
+void REFNAME(mesh_init_fused)(void* h, double t0, double w) { hrn_init_fused(((RefMesh*)h)->m, t0, w); }
+double REFNAME(mesh_predictor_dt)(void* h) { return ((RefMesh*)h)->m->pdt; }
+long REFNAME(mesh_reruns)(void* h) { return ((RefMesh*)h)->m->reruns; }
 void REFNAME(mesh_step)(void* h, int n) { hrn_step(((RefMesh*)h)->m, n); }
 int REFNAME(mesh_run_until)(void* h, double t_end, int max_steps) { return hrn_run_until(((RefMesh*)h)->m, t_end, max_steps); }
 double REFNAME(mesh_time)(void* h) { return ((RefMesh*)h)->m->t; }

@@ -75,3 +75,25 @@ def test_limiting_mesh_vs_reference(dim, N, cells, steps):
     assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-13
     assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"] and sa["irregular_steps"] == sb["irregular_steps"]
     assert (ma >= 3).any()  # the limiter was active
+
+
+@pytest.mark.parametrize("dim,N,cells,steps", [(2, 3, (9, 9), 12), (3, 3, (4, 4, 4), 4)])
+def test_fused_mesh_vs_reference(dim, N, cells, steps):
+    """fused time stepping over the C restatement vs over the reference's own
+    kernels (the fused sequencing is the harness's, hrn_step_fused)"""
+    if dim == 2:
+        u, _ = problems.gaussian_pulse_2d(N, cells, seed=3)
+    else:
+        u, _ = problems.gaussian_pulses_3d(N, cells, seed=3)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.Mesh(dim, N, cells, [1.0] * dim, -1, impl=impl, nthreads=4)
+        m.set_solution(u)
+        m.init_fused(0.0, 0.99)
+        m.step(steps)
+        res.append((m.get_solution(), m.state(), m.fused_state()))
+    (a, sa, fa), (b, sb, fb) = res
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-13
+    assert sa["picard_sweeps"] == sb["picard_sweeps"] and sa["steps"] == sb["steps"] == steps
+    assert fa["reruns"] == fb["reruns"] and fa["reruns"] >= 1
+    assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"]
