@@ -89,6 +89,9 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
 
+  // a device-side count that leaves this block without cells: the whole
+  // block returns before its first barrier (a gated launch costs little)
+  if (count && (int)blockIdx.x * C::CPB >= min(*count, ncells)) return;
   const int part_id = threadIdx.x / C::TPC;  // which variable slice
   const int r = threadIdx.x - part_id * C::TPC;
   const int lc = r / P;
@@ -510,6 +513,64 @@ __global__ void __launch_bounds__(128) boundary_kernel(const double* __restrict_
 }
 
 // ---------------------------------------------------------------------------
+// surfaceIntegral + solutionUpdate at node p of one cell (du: the cell's
+// lduh at the node, NULL for no update; Fb: the cell's lFhbnd; q: the node's
+// state, updated in place; invDx: 1/dx per direction, rounded to nearest).
+// Returns the denominator of the node's admissible step 0.9 PNPM / den,
+// den = sum_d maxAbsEigenvalue_d(q) / dx_d.
+template <int DIM, int N, class PDE>
+__device__ __forceinline__ double corrector_node(double* q, const double* __restrict__ du_in,
+                                                 const double* __restrict__ Fb, int p, const Geometry& geo, int inst,
+                                                 const double* __restrict__ dt_ptr, double invDx0, double invDx1,
+                                                 double invDx2) {
+  using S = Shape<DIM, N, PDE>;
+  constexpr int b = S::b, F = S::F, nV = S::nV;
+  const OrderTables& T = c_tab[N];
+  const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
+  const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
+  if (du_in) {
+    double du[nV];
+#pragma unroll
+    for (int v = 0; v < nV; v++) du[v] = du_in[v];
+    // nonlinear: surfaceIntegralNonlinear, flux difference times w / dx;
+    // linear (surfaceIntegralLinear, 3d/surfaceIntegralLinear.cpph:24-91):
+    // the two faces' fluctuations are added, scaled by w divided by dx
+    constexpr bool LIN = PDE::kLinear;
+    {
+      const double us = LIN ? (wz * wy) / cell_width(geo, inst, 0) : (wz * wy) * invDx0;
+      const int fn = DIM == 3 ? z * b + y : y;
+#pragma unroll
+      for (int v = 0; v < nV; v++)
+        du[v] -= (LIN ? Fb[(1 * F + fn) * nV + v] * T.FR[x] + Fb[(0 * F + fn) * nV + v] * T.FL[x]
+                      : Fb[(1 * F + fn) * nV + v] * T.FR[x] - Fb[(0 * F + fn) * nV + v] * T.FL[x]) * us;
+    }
+    {
+      const double us = LIN ? (wz * wx) / cell_width(geo, inst, 1) : (wz * wx) * invDx1;
+      const int fn = DIM == 3 ? z * b + x : x;
+#pragma unroll
+      for (int v = 0; v < nV; v++)
+        du[v] -= (LIN ? Fb[(3 * F + fn) * nV + v] * T.FR[y] + Fb[(2 * F + fn) * nV + v] * T.FL[y]
+                      : Fb[(3 * F + fn) * nV + v] * T.FR[y] - Fb[(2 * F + fn) * nV + v] * T.FL[y]) * us;
+    }
+    if (DIM == 3) {
+      const double us = LIN ? (wy * wx) / cell_width(geo, inst, 2) : (wy * wx) * invDx2;
+      const int fn = y * b + x;
+#pragma unroll
+      for (int v = 0; v < nV; v++)
+        du[v] -= (LIN ? Fb[(5 * F + fn) * nV + v] * T.FR[z] + Fb[(4 * F + fn) * nV + v] * T.FL[z]
+                      : Fb[(5 * F + fn) * nV + v] * T.FR[z] - Fb[(4 * F + fn) * nV + v] * T.FL[z]) * us;
+    }
+    const double us = dt_ptr[inst] / (wz * wy * wx);
+#pragma unroll
+    for (int v = 0; v < nV; v++) q[v] += du[v] * us;
+  }
+  double den = 0.0;
+  den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 0), invDx0));
+  den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 1), invDx1));
+  if (DIM == 3) den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 2), invDx2));
+  return den;
+}
+
 // Corrector: surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90)
 // or, for a linear PDE, surfaceIntegralLinear,
 // solutionUpdate (3d/solutionUpdate.cpph:23-47) and stableTimeStepSize
@@ -530,74 +591,32 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
                      const double* __restrict__ dt_ptr, double* __restrict__ dt_out, Geometry geo, int ncells,
                      const int* __restrict__ cell_list, int do_update, const int* __restrict__ count) {
   using C = CorrectorCfg<DIM, N, PDE>;
-  constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD;
-  const OrderTables& T = c_tab[N];
+  constexpr int P = C::P, F = C::F, nV = C::nV, nD = C::nD;
   __shared__ double red[32];
   const int lc = threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
   const int slot = blockIdx.x * C::CPB + lc;
   // padding threads only join the reduction; count: optional device-side list length
+  if (count && (int)blockIdx.x * C::CPB >= min(*count, ncells)) return;  // whole block
   const bool active = lc < C::CPB && slot < (count ? min(*count, ncells) : ncells);
   double dtmin = __longlong_as_double(0x7fefffffffffffffll);  // DBL_MAX
   int inst = 0;
   if (active) {
     const int cell = cell_list ? cell_list[slot] : slot;
     inst = cell_instance(geo, cell);
-    const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
-    const double wx = T.w[x], wy = T.w[y], wz = DIM == 3 ? T.w[z] : 1.0;
-    const double invDx0 = __ddiv_rn(1.0, cell_width(geo, inst, 0)), invDx1 = __ddiv_rn(1.0, cell_width(geo, inst, 1));
-    const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, cell_width(geo, inst, 2)) : 0.0;
     double* u = luh + ((size_t)cell * P + p) * nD;
     double q[nD];
 #pragma unroll
     for (int v = 0; v < nD; v++) q[v] = u[v];
-    if (do_update) {
-      const double* du_in = lduh + ((size_t)cell * P + p) * nV;
-      const double* Fb = lFhbnd + (size_t)cell * 2 * DIM * F * nV;
-      double du[nV];
+    const double invDx0 = __ddiv_rn(1.0, cell_width(geo, inst, 0)), invDx1 = __ddiv_rn(1.0, cell_width(geo, inst, 1));
+    const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, cell_width(geo, inst, 2)) : 0.0;
+    const double den = corrector_node<DIM, N, PDE>(q, do_update ? lduh + ((size_t)cell * P + p) * nV : nullptr,
+                                                   lFhbnd + (size_t)cell * 2 * DIM * F * nV, p, geo, inst, dt_ptr,
+                                                   invDx0, invDx1, invDx2);
+    dtmin = __ddiv_rn(__dmul_rn(0.9, pnpm(N)), den);
+    if (do_update)
 #pragma unroll
-      for (int v = 0; v < nV; v++) du[v] = du_in[v];
-      // nonlinear: surfaceIntegralNonlinear, flux difference times w / dx;
-      // linear (surfaceIntegralLinear, 3d/surfaceIntegralLinear.cpph:24-91):
-      // the two faces' fluctuations are added, scaled by w divided by dx
-      constexpr bool LIN = PDE::kLinear;
-      {
-        const double us = LIN ? (wz * wy) / cell_width(geo, inst, 0) : (wz * wy) * invDx0;
-        const int fn = DIM == 3 ? z * b + y : y;
-#pragma unroll
-        for (int v = 0; v < nV; v++)
-          du[v] -= (LIN ? Fb[(1 * F + fn) * nV + v] * T.FR[x] + Fb[(0 * F + fn) * nV + v] * T.FL[x]
-                        : Fb[(1 * F + fn) * nV + v] * T.FR[x] - Fb[(0 * F + fn) * nV + v] * T.FL[x]) * us;
-      }
-      {
-        const double us = LIN ? (wz * wx) / cell_width(geo, inst, 1) : (wz * wx) * invDx1;
-        const int fn = DIM == 3 ? z * b + x : x;
-#pragma unroll
-        for (int v = 0; v < nV; v++)
-          du[v] -= (LIN ? Fb[(3 * F + fn) * nV + v] * T.FR[y] + Fb[(2 * F + fn) * nV + v] * T.FL[y]
-                        : Fb[(3 * F + fn) * nV + v] * T.FR[y] - Fb[(2 * F + fn) * nV + v] * T.FL[y]) * us;
-      }
-      if (DIM == 3) {
-        const double us = LIN ? (wy * wx) / cell_width(geo, inst, 2) : (wy * wx) * invDx2;
-        const int fn = y * b + x;
-#pragma unroll
-        for (int v = 0; v < nV; v++)
-          du[v] -= (LIN ? Fb[(5 * F + fn) * nV + v] * T.FR[z] + Fb[(4 * F + fn) * nV + v] * T.FL[z]
-                        : Fb[(5 * F + fn) * nV + v] * T.FR[z] - Fb[(4 * F + fn) * nV + v] * T.FL[z]) * us;
-      }
-      const double us = dt_ptr[inst] / (wz * wy * wx);
-#pragma unroll
-      for (int v = 0; v < nV; v++) {
-        q[v] += du[v] * us;
-        u[v] = q[v];
-      }
-    }
-    double den = 0.0;
-    den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 0), invDx0));
-    den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 1), invDx1));
-    if (DIM == 3) den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 2), invDx2));
-    const double dtp = __ddiv_rn(__dmul_rn(0.9, pnpm(N)), den);
-    dtmin = (dtp < dtmin) ? dtp : dtmin;
+      for (int v = 0; v < nV; v++) u[v] = q[v];
   }
   // A batch block may hold cells of two instances (instances are contiguous
   // cell ranges): then every thread min-combines into its own instance.

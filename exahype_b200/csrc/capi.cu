@@ -240,8 +240,8 @@ struct Launch {
       attr = true;
     }
     const int grid = (n + LC::CPB - 1) / LC::CPB;
-    predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED, TS><<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g,
-                                                                                       n, list, tmp, cnt);
+    predictor_lines_kernel<DIM, N, PDE, TEMPS, MB, MIXED, TS>
+        <<<grid, LC::THREADS, LC::SMEM, st>>>(luh, qb, fb, du, iters, dt, g, n, list, tmp, cnt);
     EXA_LAUNCHED();
     return EXA_OK;
   }
@@ -1055,19 +1055,23 @@ static int mesh_one_step(exa_mesh* m) {
     if (rc) return rc;
     m->phase_launches[2] += 1;
   }
-  {
-    PhaseTimer pt(m, 3);
-    if (m->fused) {
-      // the predictor of the fused step runs with its own step size right
-      // after the update (no global reduction in between), then the step
-      // bookkeeping, then the rerun, which does nothing unless needed
-      rc = mesh_predict(m);
-      if (rc) return rc;
+  if (m->fused) {
+    // fused time stepping: the predictor of the next step runs with its own
+    // step size right after the update (no global reduction in between),
+    // then the step bookkeeping, then the rerun, which does nothing unless
+    // needed (its blocks return at once when the device count is 0)
+    rc = mesh_predict(m);
+    if (rc) return rc;
+    {
+      PhaseTimer pt(m, 3);
       fused_advance_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->weight, m->rerun, m->ncells);
       EXA_LAUNCHED();
       m->phase_launches[3] += 1;
-      return mesh_predict(m, m->rerun);
     }
+    return mesh_predict(m, m->rerun);
+  }
+  {
+    PhaseTimer pt(m, 3);
     advance_kernel<<<1, 1, 0, m->stream>>>(m->scal);
     EXA_LAUNCHED();
     m->phase_launches[3] += 1;

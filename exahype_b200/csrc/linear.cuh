@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
   const int p = threadIdx.x - lc * P;
   const int slot = blockIdx.x * C::CPB + lc;
   const int nact = count ? min(*count, ncells) : ncells;
+  if ((int)blockIdx.x * C::CPB >= nact) return;  // whole block, before its first barrier
   const bool active = slot < nact;
   const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
   double* sQ = smem + lc * C::SQ;

@@ -86,6 +86,9 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
 
+  // a device-side count that leaves this block without cells: the whole
+  // block returns before its first barrier (a gated launch costs little)
+  if (count && (int)blockIdx.x * C::CPB >= min(*count, ncells)) return;
   const int lc = threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
   const int slot = blockIdx.x * C::CPB + lc;

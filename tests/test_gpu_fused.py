@@ -27,11 +27,22 @@ def eb():
 
 
 CASES = [(2, 3, (12, 12), -1, 0, 30, 0.99), (2, 5, (8, 8), 0, 0, 20, 0.9), (3, 3, (5, 5, 5), -1, 0, 10, 0.99),
-         (2, 4, (8, 8), -1, 2, 15, 0.95)]
+         (3, 5, (4, 4, 4), -1, 0, 8, 0.99), (2, 4, (8, 8), -1, 2, 15, 0.95)]
+# predictor variants of the nonlinear cases: 0 (node form), 1, 2, 6, 7 (line
+# forms), 5 (mixed precision); the rerun launch is gated by a device count
+VARIANTS = [0, 1, 2, 5, 6, 7]
 
 
-@pytest.mark.parametrize("dim,N,cells,bc,pde,steps,w", CASES)
-def test_fused_mesh_vs_oracle(eb, dim, N, cells, bc, pde, steps, w):
+def _params():
+    out = []
+    for c in CASES:
+        for v in (VARIANTS if c[4] != 2 else [0]):
+            out.append(c + (v,))
+    return out
+
+
+@pytest.mark.parametrize("dim,N,cells,bc,pde,steps,w,variant", _params())
+def test_fused_mesh_vs_oracle(eb, dim, N, cells, bc, pde, steps, w, variant):
     from exahype_b200 import problems
     if pde == 2:
         u, _ = problems.elastic_pulse(dim, N, cells, seed=2)
@@ -40,6 +51,7 @@ def test_fused_mesh_vs_oracle(eb, dim, N, cells, bc, pde, steps, w):
     else:
         u, _ = problems.gaussian_pulses_3d(N, cells, seed=2)
     s = eb.Solver(dim, N, pde)
+    s.variant = variant
     m = eb.Mesh(s, cells, [0.0] * dim, [1.0] * dim, bc)
     m.set_solution(u)
     m.init_fused(0.0, w)
@@ -49,16 +61,18 @@ def test_fused_mesh_vs_oracle(eb, dim, N, cells, bc, pde, steps, w):
     o.init_fused(0.0, w)
     o.step(steps)
     a, b = m.get_solution(), o.get_solution()
-    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    # mixed variant: FP32 increments in the Picard sweeps (1e-9 bar)
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < (1e-9 if variant == 5 else 1e-12)
     sa, sb = m.state(), o.state()
     assert sa["steps"] == sb["steps"] == steps
     # the stable step of a solution that differs at round-off may differ in
     # its last bit, and the time stamp sums the steps
-    close = lambda x, y: abs(x - y) <= 1e-14 * abs(y)
+    tol = 1e-11 if variant == 5 else 1e-14
+    close = lambda x, y: abs(x - y) <= tol * abs(y)
     assert close(sa["t"], sb["t"]) and close(sa["dt"], sb["dt"])
     fa, fb = m.fused_state(), o.fused_state()
     assert close(fa["predictor_dt"], fb["predictor_dt"]) and fa["reruns"] == fb["reruns"]
-    if pde != 2:
+    if pde != 2 and variant != 5:
         assert sa["picard_sweeps"] == sb["picard_sweeps"]
     # run_until stops on the same step
     t_end = sa["t"] + 4.5 * sa["dt"]
