@@ -578,11 +578,24 @@ __device__ __forceinline__ double corrector_node(double* q, const double* __rest
 // admissible step is min-reduced over the whole launch into *dt_out; the
 // time-step arithmetic uses explicit round-to-nearest operations so that it
 // reproduces the reference's unfused evaluation bit for bit.
+//
+// The block's cells' luh, lduh and lFhbnd are staged in shared memory by
+// coalesced loads (all issued before the first shared store) and luh is
+// written back the same way: per-node accesses of nD consecutive doubles
+// would make every load and store instruction touch 32 sectors.
 template <int DIM, int N, class PDE>
 struct CorrectorCfg : Shape<DIM, N, PDE> {
-  static constexpr int CPB = cells_per_block<Shape<DIM, N, PDE>::P>();
+  using S = Shape<DIM, N, PDE>;
+  static constexpr int CPB = cells_per_block<S::P>();
   // whole warps: the block min-reduction shuffles across full warps
-  static constexpr int THREADS = (CPB * Shape<DIM, N, PDE>::P + 31) / 32 * 32;
+  static constexpr int THREADS = (CPB * S::P + 31) / 32 * 32;
+  // per cell in shared memory: state (node stride QS, odd against bank
+  // conflicts), update (stride nV), face fluxes
+  static constexpr int QS = S::nD | 1;
+  static constexpr int OU = 0, ODU = S::P * QS, OFB = ODU + S::P * S::nV;
+  static constexpr int SC = OFB + 2 * DIM * S::F * S::nV;
+  static constexpr size_t SMEM = sizeof(double) * (size_t)CPB * SC;
+  static_assert(SMEM <= 227 * 1024, "corrector staging exceeds shared memory");
 };
 
 template <int DIM, int N, class PDE>
@@ -591,32 +604,89 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
                      const double* __restrict__ dt_ptr, double* __restrict__ dt_out, Geometry geo, int ncells,
                      const int* __restrict__ cell_list, int do_update, const int* __restrict__ count) {
   using C = CorrectorCfg<DIM, N, PDE>;
-  constexpr int P = C::P, F = C::F, nV = C::nV, nD = C::nD;
+  constexpr int P = C::P, F = C::F, nV = C::nV, nD = C::nD, QS = C::QS, SC = C::SC;
+  constexpr int SU = P * nD, SDU = P * nV, SFB = 2 * DIM * F * nV;  // per-cell global extents
+  extern __shared__ double smem[];
   __shared__ double red[32];
+  __shared__ int s_cell[C::CPB];
   const int lc = threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
   const int slot = blockIdx.x * C::CPB + lc;
-  // padding threads only join the reduction; count: optional device-side list length
-  if (count && (int)blockIdx.x * C::CPB >= min(*count, ncells)) return;  // whole block
-  const bool active = lc < C::CPB && slot < (count ? min(*count, ncells) : ncells);
+  const int nact = count ? min(*count, ncells) : ncells;  // count: optional device-side list length
+  if ((int)blockIdx.x * C::CPB >= nact) return;           // whole block, before its first barrier
+  // padding threads only join the reduction
+  const bool active = lc < C::CPB && slot < nact;
+  if (threadIdx.x < C::CPB) {
+    const int s = blockIdx.x * C::CPB + threadIdx.x;
+    s_cell[threadIdx.x] = s < nact ? (cell_list ? cell_list[s] : s) : -1;
+  }
+  __syncthreads();
+  {
+    // loads of the three arrays into registers, then the shared stores
+    constexpr int KU = (C::CPB * SU + C::THREADS - 1) / C::THREADS;
+    constexpr int KD = (C::CPB * SDU + C::THREADS - 1) / C::THREADS;
+    constexpr int KF = (C::CPB * SFB + C::THREADS - 1) / C::THREADS;
+    double vu[KU], vd[KD], vf[KF];
+#pragma unroll
+    for (int k = 0; k < KU; k++) {
+      const int i = threadIdx.x + k * C::THREADS, c = i / SU, e = i - c * SU;
+      vu[k] = (c < C::CPB && s_cell[c] >= 0) ? luh[(size_t)s_cell[c] * SU + e] : 0.0;
+    }
+    if (do_update) {
+#pragma unroll
+      for (int k = 0; k < KD; k++) {
+        const int i = threadIdx.x + k * C::THREADS, c = i / SDU, e = i - c * SDU;
+        vd[k] = (c < C::CPB && s_cell[c] >= 0) ? lduh[(size_t)s_cell[c] * SDU + e] : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < KF; k++) {
+        const int i = threadIdx.x + k * C::THREADS, c = i / SFB, e = i - c * SFB;
+        vf[k] = (c < C::CPB && s_cell[c] >= 0) ? lFhbnd[(size_t)s_cell[c] * SFB + e] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KU; k++) {
+      const int i = threadIdx.x + k * C::THREADS, c = i / SU, e = i - c * SU;
+      if (c < C::CPB) smem[c * SC + C::OU + (e / nD) * QS + e % nD] = vu[k];
+    }
+    if (do_update) {
+#pragma unroll
+      for (int k = 0; k < KD; k++) {
+        const int i = threadIdx.x + k * C::THREADS, c = i / SDU, e = i - c * SDU;
+        if (c < C::CPB) smem[c * SC + C::ODU + e] = vd[k];
+      }
+#pragma unroll
+      for (int k = 0; k < KF; k++) {
+        const int i = threadIdx.x + k * C::THREADS, c = i / SFB, e = i - c * SFB;
+        if (c < C::CPB) smem[c * SC + C::OFB + e] = vf[k];
+      }
+    }
+  }
+  __syncthreads();
   double dtmin = __longlong_as_double(0x7fefffffffffffffll);  // DBL_MAX
   int inst = 0;
   if (active) {
-    const int cell = cell_list ? cell_list[slot] : slot;
-    inst = cell_instance(geo, cell);
-    double* u = luh + ((size_t)cell * P + p) * nD;
+    inst = cell_instance(geo, s_cell[lc]);
+    double* st = smem + lc * SC;
     double q[nD];
 #pragma unroll
-    for (int v = 0; v < nD; v++) q[v] = u[v];
+    for (int v = 0; v < nD; v++) q[v] = st[C::OU + p * QS + v];
     const double invDx0 = __ddiv_rn(1.0, cell_width(geo, inst, 0)), invDx1 = __ddiv_rn(1.0, cell_width(geo, inst, 1));
     const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, cell_width(geo, inst, 2)) : 0.0;
-    const double den = corrector_node<DIM, N, PDE>(q, do_update ? lduh + ((size_t)cell * P + p) * nV : nullptr,
-                                                   lFhbnd + (size_t)cell * 2 * DIM * F * nV, p, geo, inst, dt_ptr,
-                                                   invDx0, invDx1, invDx2);
+    const double den = corrector_node<DIM, N, PDE>(q, do_update ? st + C::ODU + p * nV : nullptr, st + C::OFB, p,
+                                                   geo, inst, dt_ptr, invDx0, invDx1, invDx2);
     dtmin = __ddiv_rn(__dmul_rn(0.9, pnpm(N)), den);
     if (do_update)
 #pragma unroll
-      for (int v = 0; v < nV; v++) u[v] = q[v];
+      for (int v = 0; v < nV; v++) st[C::OU + p * QS + v] = q[v];
+  }
+  if (do_update) {  // the updated state, written back coalesced
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < (C::CPB * SU + C::THREADS - 1) / C::THREADS; k++) {
+      const int i = threadIdx.x + k * C::THREADS, c = i / SU, e = i - c * SU;
+      if (c < C::CPB && s_cell[c] >= 0) luh[(size_t)s_cell[c] * SU + e] = smem[c * SC + C::OU + (e / nD) * QS + e % nD];
+    }
   }
   // A batch block may hold cells of two instances (instances are contiguous
   // cell ranges): then every thread min-combines into its own instance.

@@ -197,6 +197,23 @@ __global__ void sweep_count_kernel(const int* iters, const int* cell_list, int n
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
 }
 
+template <int DIM, int N, class PDE>
+static int launch_corrector(double* luh, const double* du, const double* fb, const double* dt, double* dtout,
+                            Geometry g, int n, const int* list, int upd, const int* cnt, cudaStream_t st) {
+  using CC = CorrectorCfg<DIM, N, PDE>;
+  if (n <= 0) return EXA_OK;
+  static bool attr = false;
+  if (!attr) {
+    EXA_CUDA(cudaFuncSetAttribute(corrector_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)CC::SMEM));
+    attr = true;
+  }
+  corrector_kernel<DIM, N, PDE><<<(n + CC::CPB - 1) / CC::CPB, CC::THREADS, CC::SMEM, st>>>(luh, du, fb, dt, dtout, g,
+                                                                                           n, list, upd, cnt);
+  EXA_LAUNCHED();
+  return EXA_OK;
+}
+
 // Predictor variants the autotuner chooses from (all FP64):
 //   0 node form, 1 block/SM budget    1 line form, 1 block/SM
 //   2 line form, 2 blocks/SM          3 node form, 2 blocks/SM
@@ -298,11 +315,7 @@ struct Launch {
   }
   static int corrector(double* luh, const double* du, const double* fb, const double* dt, double* dtout, Geometry g,
                        int n, const int* list, int upd, const int* cnt, cudaStream_t st) {
-    if (n <= 0) return EXA_OK;
-    corrector_kernel<DIM, N, PDE><<<(n + CC::CPB - 1) / CC::CPB, CC::THREADS, 0, st>>>(luh, du, fb, dt, dtout, g, n,
-                                                                                      list, upd, cnt);
-    EXA_LAUNCHED();
-    return EXA_OK;
+    return launch_corrector<DIM, N, PDE>(luh, du, fb, dt, dtout, g, n, list, upd, cnt, st);
   }
   static KernelSet make(int pde) {
     using S = Shape<DIM, N, PDE>;
@@ -362,11 +375,7 @@ struct LinearLaunch {
   }
   static int corrector(double* luh, const double* du, const double* fb, const double* dt, double* dtout, Geometry g,
                        int n, const int* list, int upd, const int* cnt, cudaStream_t st) {
-    if (n <= 0) return EXA_OK;
-    corrector_kernel<DIM, N, PDE><<<(n + CC::CPB - 1) / CC::CPB, CC::THREADS, 0, st>>>(luh, du, fb, dt, dtout, g, n,
-                                                                                      list, upd, cnt);
-    EXA_LAUNCHED();
-    return EXA_OK;
+    return launch_corrector<DIM, N, PDE>(luh, du, fb, dt, dtout, g, n, list, upd, cnt, st);
   }
   static int volume(double* du, const double* fhi, int n, cudaStream_t st) {
     if (n <= 0) return EXA_OK;

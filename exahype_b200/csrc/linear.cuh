@@ -189,17 +189,6 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
 #pragma unroll
     for (int v = 0; v < nV; v++) sG[p * GS + d * nV + v] = fh[d][v];
   if (active) {
-    if (lduh) {  // volumeIntegralLinear
-      const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
-      const double w = (DIM == 3 ? T.w[z] * T.w[y] : T.w[y]) * T.w[x];
-#pragma unroll
-      for (int v = 0; v < nV; v++) {
-        double du = 0.0;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) du -= w * fh[d][v];
-        lduh[((size_t)cell * P + p) * nV + v] = du;
-      }
-    }
     if (lQhi_out)
       for (int v = 0; v < nD; v++) lQhi_out[((size_t)cell * P + p) * nD + v] = sQ[p * QS + v];
     if (lFhi_out)
@@ -245,6 +234,29 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
     }
     lFhbnd[(((size_t)cc * 2 * DIM + 2 * d) * F + L) * nV + v] = sl;
     lFhbnd[(((size_t)cc * 2 * DIM + 2 * d + 1) * F + L) * nV + v] = sr;
+  }
+  if (!lduh) return;
+  // volumeIntegralLinear from the staged lFhi, staged in turn in the cell's
+  // state buffer and written by consecutive threads to consecutive addresses
+  // (a thread's own nV values would leave every store instruction a partial
+  // write of 32 sectors)
+  __syncthreads();
+  if (active) {
+    const int x = p % b, y = (p / b) % b, z = DIM == 3 ? p / (b * b) : 0;
+    const double w = (DIM == 3 ? T.w[z] * T.w[y] : T.w[y]) * T.w[x];
+#pragma unroll
+    for (int v = 0; v < nV; v++) {
+      double du = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) du -= w * sG[p * GS + d * nV + v];
+      sQ[p * nV + v] = du;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < C::CPB * P * nV; i += C::THREADS) {
+    const int c = i / (P * nV), e = i - c * (P * nV);
+    const int cc = s_cell[c];
+    if (cc >= 0) lduh[(size_t)cc * P * nV + e] = smem[c * C::SQ + e];
   }
 }
 
