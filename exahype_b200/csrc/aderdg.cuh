@@ -447,15 +447,30 @@ __global__ void __launch_bounds__(128) riemann_kernel(const double* __restrict__
   const double* QR = lQhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nD;
   double* FL = lFhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nV;
   double* FR = lFhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nV;
+  // this lane's flux and state differences are loaded before the face
+  // averages, so that all of the face's loads are in flight together
+  constexpr int E = F * nV, EPL = (E + 31) / 32;
+  double fl[EPL], fr[EPL], dq[EPL];
+#pragma unroll
+  for (int i = 0; i < EPL; i++) {
+    const int e = lane + 32 * i, fn = e / nV, k = e - fn * nV;
+    const bool in = e < E;
+    fl[i] = in ? FL[e] : 0.0;
+    fr[i] = in ? FR[e] : 0.0;
+    dq[i] = in ? QR[fn * nD + k] - QL[fn * nD + k] : 0.0;
+  }
   double aL[nD], aR[nD];
   face_average<DIM, N, PDE>(QL, lane, aL);
   face_average<DIM, N, PDE>(QR, lane, aR);
   const double smax = face_smax<DIM, PDE>(aL, aR, dir);
-  for (int e = lane; e < F * nV; e += 32) {
-    const int fn = e / nV, k = e - fn * nV;
-    const double r = 0.5 * (FR[e] + FL[e]) - 0.5 * smax * (QR[fn * nD + k] - QL[fn * nD + k]);
-    FL[e] = r;
-    FR[e] = r;
+#pragma unroll
+  for (int i = 0; i < EPL; i++) {
+    const int e = lane + 32 * i;
+    if (e < E) {
+      const double r = 0.5 * (fr[i] + fl[i]) - 0.5 * smax * dq[i];
+      FL[e] = r;
+      FR[e] = r;
+    }
   }
 }
 

@@ -286,6 +286,15 @@ __global__ void __launch_bounds__(128) riemann_linear_kernel(const double* __res
   const double* QR = lQhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nD;
   double* FL = lFhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nV;
   double* FR = lFhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nV;
+  // this lane's state differences are loaded before the face averages, so
+  // that all of the face's loads are in flight together
+  constexpr int E = F * nV, EPL = (E + 31) / 32;
+  double dq[EPL];
+#pragma unroll
+  for (int i = 0; i < EPL; i++) {
+    const int e = lane + 32 * i, fn = e / nV, k = e - fn * nV;
+    dq[i] = e < E ? 0.5 * (QR[fn * nD + k] - QL[fn * nD + k]) : 0.0;
+  }
   double aL[nD], aR[nD];
   face_average<DIM, N, PDE>(QL, lane, aL);
   face_average<DIM, N, PDE>(QR, lane, aR);
@@ -296,9 +305,10 @@ __global__ void __launch_bounds__(128) riemann_linear_kernel(const double* __res
     for (int k = 0; k < nD; k++) av[k] = 0.5 * (aL[k] + aR[k]);
     PDE::coefficient_matrix(av, dir, sB[w]);
   }
-  for (int e = lane; e < F * nV; e += 32) {
-    const int fn = e / nV, k = e - fn * nV;
-    sDQ[w][e] = 0.5 * (QR[fn * nD + k] - QL[fn * nD + k]);
+#pragma unroll
+  for (int i = 0; i < EPL; i++) {
+    const int e = lane + 32 * i;
+    if (e < E) sDQ[w][e] = dq[i];
   }
   __syncwarp();
   for (int e = lane; e < F * nV; e += 32) {
