@@ -654,6 +654,15 @@ def run_serving_workload(a, world, dev, rank):
     for dim in (2, 3):
         for o in (3, 5, 7):
             variants[(dim, o)] = eb.Solver(dim, o).autotune(4096)[0]
+    # one untimed pass of the same request stream first: the first use of
+    # each kernel in a process loads its module, and the device memory pool
+    # grows to the mix's peak once; the one-at-a-time arm below runs after it
+    # in the same process and is warm as well
+    warm = serving.request_stream(n, rate, seed=SEED + rank, **kw)
+    for r in warm:
+        r.build_initial()
+    serving.Server(budget, variants).run(warm, keep_results=False)
+    del warm
     reqs = serving.request_stream(n, rate, seed=SEED + rank, **kw)
     for r in reqs:
         r.build_initial()
@@ -680,7 +689,8 @@ def run_serving_workload(a, world, dev, rank):
             "value": res["value"], "unit": "DoF-updates/s", "wall_s": wall,
             "one_at_a_time": {"p50_time_to_solution_s": res_b["p50_s"], "p99_time_to_solution_s": res_b["p99_s"],
                               "value": res_b["value"], "wall_s": wall_b},
-            "timing": "host wall clock from the first arrival to the last result on the host"}
+            "timing": "host wall clock from the first arrival to the last result on the host, after one "
+                      "untimed pass of the same stream (module loading, memory-pool growth)"}
 
 
 def run_mixed_arm(a, u0, fp64_variant, dev):
