@@ -269,6 +269,33 @@ class Mesh:
         self.ncells = n.value
         self.dx = [size[i] / cells[i] for i in range(d)]
 
+    @classmethod
+    def refined(cls, solver, cells, offset, size, box_lo, box_hi):
+        """Periodic mesh of cells[d] coarse cells with the box of coarse cells
+        box_lo[d] <= c[d] < box_hi[d] refined once (3^d fine cells each;
+        exa_mesh_create_refined). Solution order: the unrefined coarse cells
+        (x fastest, refined ones skipped), then the fine cells of the box."""
+        lib = load()
+        d = solver.dim
+        self = cls.__new__(cls)
+        self._h = None
+        c = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
+        o = _dbl3(list(offset) + [0.0] * (3 - len(offset)))
+        s = _dbl3(list(size) + [1.0] * (3 - len(size)))
+        lo = (ctypes.c_int * 3)(*(list(box_lo) + [0] * (3 - len(box_lo))))
+        hi = (ctypes.c_int * 3)(*(list(box_hi) + [1] * (3 - len(box_hi))))
+        h = ctypes.c_void_p()
+        _check(lib.exa_mesh_create_refined(solver._h, c, o, s, lo, hi, ctypes.byref(h)), "exa_mesh_create_refined")
+        self._h = h
+        self.solver = solver
+        self.cells = tuple(cells)
+        self.box = (tuple(box_lo), tuple(box_hi))
+        n = ctypes.c_int()
+        _check(lib.exa_mesh_num_cells(h, ctypes.byref(n)), "exa_mesh_num_cells")
+        self.ncells = n.value
+        self.dx = [size[i] / cells[i] for i in range(d)]
+        return self
+
     def __del__(self):
         try:
             if self._h:

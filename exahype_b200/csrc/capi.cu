@@ -3,6 +3,7 @@
 // kernels like the reference's non-fused time step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cstdio>
@@ -439,6 +440,25 @@ __global__ void take_dt_kernel(double* scal) {
   scal[1] = __longlong_as_double(0x7fefffffffffffffll);
 }
 
+// Refined meshes: lv[0..1] the step size each level's kernels read, lv[2..3]
+// the levels' min-reduction targets. The global step is the min over both
+// levels (global time stepping).
+__global__ void level_reset_kernel(double* lv) {
+  lv[2] = lv[3] = __longlong_as_double(0x7fefffffffffffffll);
+}
+__global__ void level_take_kernel(double* scal, double* lv) {
+  const double s = (lv[3] < lv[2]) ? lv[3] : lv[2];
+  scal[0] = lv[0] = lv[1] = s;
+  lv[2] = lv[3] = __longlong_as_double(0x7fefffffffffffffll);
+}
+__global__ void level_advance_kernel(double* scal, double* lv) {
+  scal[2] += scal[0];
+  const double s = (lv[3] < lv[2]) ? lv[3] : lv[2];
+  scal[0] = lv[0] = lv[1] = s;
+  lv[2] = lv[3] = __longlong_as_double(0x7fefffffffffffffll);
+  scal[3] += 1.0;
+}
+
 // independent FP64 FMA chains: 8 per thread, `iters` rounds
 __global__ void __launch_bounds__(256) fp64_probe_kernel(double* out, int iters, double a, double b) {
   double x[8];
@@ -491,6 +511,21 @@ struct exa_mesh {
   bool fused = false;
   double weight = 0.99;
   int* rerun = nullptr;
+  // statically refined mesh (exa_mesh_create_refined): two levels as two
+  // geometry instances (per-cell level index, per-level widths), per-level
+  // step sizes and min-reduction targets lv[0..1], lv[2..3], the face slots
+  // of the refined cells that face coarse cells (ancestors, zeroed and
+  // restricted into after every predictor) and of the virtual fine cells
+  // across the refined box's faces (descendants, prolongated into)
+  struct {
+    bool on = false;
+    double* lv = nullptr;
+    int* inst = nullptr;
+    double* inst_dx = nullptr;
+    int anc0 = 0, nanc = 0, nres = 0, npro = 0;
+    int *res_f = nullptr, *res_c = nullptr, *res_ld = nullptr, *res_idx = nullptr;
+    int *pro_f = nullptr, *pro_c = nullptr, *pro_ld = nullptr, *pro_idx = nullptr;
+  } ref;
 };
 
 namespace {
@@ -783,6 +818,10 @@ static void mesh_free(exa_mesh* m) {
   sfree(m->stage_in, m->stream);
   sfree(m->stage_out, m->stream);
   sfree(m->rerun, m->stream);
+  for (void* p : {(void*)m->ref.lv, (void*)m->ref.inst, (void*)m->ref.inst_dx, (void*)m->ref.res_f,
+                  (void*)m->ref.res_c, (void*)m->ref.res_ld, (void*)m->ref.res_idx, (void*)m->ref.pro_f,
+                  (void*)m->ref.pro_c, (void*)m->ref.pro_ld, (void*)m->ref.pro_idx})
+    sfree(p, m->stream);
   if (m->io_in) cudaStreamDestroy(m->io_in);
   if (m->io_out) cudaStreamDestroy(m->io_out);
   for (void* p : {(void*)m->luh, (void*)m->lduh, (void*)m->lQhbnd, (void*)m->lFhbnd, (void*)m->scal, (void*)m->iters,
@@ -892,6 +931,192 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
   return EXA_OK;
 }
 
+int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
+                            const int* box_lo, const int* box_hi, exa_mesh** out) {
+  if (!s || !cells || !offset || !size || !box_lo || !box_hi || !out)
+    return fail(EXA_ERR_ARG, "exa_mesh_create_refined: null argument");
+  if (s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create_refined: nonlinear PDEs only");
+  const int dim = s->k.dim, D2 = 2 * dim;
+  std::unique_ptr<exa_mesh> m(new exa_mesh());
+  m->s = s;
+  m->dim = dim;
+  int fe[3] = {1, 1, 1};  // fine cells per axis inside the box
+  long long n_coarse = 1;
+  for (int d = 0; d < dim; d++) {
+    if (cells[d] < 3 || !(size[d] > 0)) return fail(EXA_ERR_ARG, "exa_mesh_create_refined: bad grid");
+    if (box_lo[d] < 1 || box_hi[d] <= box_lo[d] || box_hi[d] > cells[d] - 1)
+      return fail(EXA_ERR_ARG, "exa_mesh_create_refined: the refined box must lie inside the grid with at least "
+                               "one coarse cell around it");
+    m->cells[d] = cells[d];
+    m->offset[d] = offset[d];
+    m->geo.dx[d] = size[d] / cells[d];
+    fe[d] = 3 * (box_hi[d] - box_lo[d]);
+    n_coarse *= cells[d];
+  }
+  for (int d = dim; d < 3; d++) m->geo.dx[d] = 1.0;
+  for (int f = 0; f < 6; f++) m->bc[f] = EXA_BC_PERIODIC;
+  if (n_coarse > (1ll << 26) || (long long)fe[0] * fe[1] * fe[2] > (1ll << 26))
+    return fail(EXA_ERR_ARG, "exa_mesh_create_refined: too many cells");
+  const int cz = dim == 3 ? cells[2] : 1;
+  auto cidx = [&](const int* c) { return (c[2] * cells[1] + c[1]) * cells[0] + c[0]; };
+  auto inbox = [&](const int* c) {
+    for (int d = 0; d < dim; d++)
+      if (c[d] < box_lo[d] || c[d] >= box_hi[d]) return false;
+    return true;
+  };
+  auto on_box_face = [&](const int* c) {
+    for (int d = 0; d < dim; d++)
+      if (c[d] == box_lo[d] || c[d] == box_hi[d] - 1) return true;
+    return false;
+  };
+  // slots: coarse cells, fine cells, ancestors (refined cells on the box's
+  // faces), descendants (one per fine cell and box face it lies on)
+  std::vector<int> cid((size_t)n_coarse, -1), aid((size_t)n_coarse, -1);
+  int n0 = 0;
+  for (int k = 0; k < cz; k++)
+    for (int j = 0; j < cells[1]; j++)
+      for (int i = 0; i < cells[0]; i++) {
+        const int c[3] = {i, j, k};
+        if (!inbox(c)) cid[cidx(c)] = n0++;
+      }
+  const int n1 = fe[0] * fe[1] * fe[2];
+  const int anc0 = n0 + n1;
+  int nanc = 0;
+  for (int k = 0; k < cz; k++)
+    for (int j = 0; j < cells[1]; j++)
+      for (int i = 0; i < cells[0]; i++) {
+        const int c[3] = {i, j, k};
+        if (inbox(c) && on_box_face(c)) aid[cidx(c)] = anc0 + nanc++;
+      }
+  auto fid = [&](const int* f) { return n0 + (f[2] * fe[1] + f[1]) * fe[0] + f[0]; };
+  const int desc0 = anc0 + nanc;
+  int ndesc = 0;
+  std::vector<int> dslot((size_t)n1 * D2, -1);
+  std::vector<int> fl, fr, fd, rf, rc, ridx, pf, pc, pidx;
+  // coarse level: cell-cell and cell-ancestor faces (refined-refined faces
+  // are solved on the fine level)
+  for (int k = 0; k < cz; k++)
+    for (int j = 0; j < cells[1]; j++)
+      for (int i = 0; i < cells[0]; i++) {
+        const int c[3] = {i, j, k};
+        for (int d = 0; d < dim; d++) {
+          int nb[3] = {i, j, k};
+          nb[d] = (c[d] + 1) % cells[d];
+          const bool rc_ = inbox(c), rn = inbox(nb);
+          if (rc_ && rn) continue;
+          fl.push_back(rc_ ? aid[cidx(c)] : cid[cidx(c)]);
+          fr.push_back(rn ? aid[cidx(nb)] : cid[cidx(nb)]);
+          fd.push_back(d);
+        }
+      }
+  // fine level: fine-fine faces, fine-descendant faces, and the face
+  // transfers of the fine cells on the box's faces
+  for (int K = 0; K < fe[2]; K++)
+    for (int J = 0; J < fe[1]; J++)
+      for (int I = 0; I < fe[0]; I++) {
+        const int f[3] = {I, J, K};
+        const int me = fid(f);
+        const int parent[3] = {box_lo[0] + I / 3, box_lo[1] + J / 3, dim == 3 ? box_lo[2] + K / 3 : 0};
+        for (int d = 0; d < dim; d++) {
+          if (f[d] + 1 < fe[d]) {
+            int nb[3] = {I, J, K};
+            nb[d]++;
+            fl.push_back(me);
+            fr.push_back(fid(nb));
+            fd.push_back(d);
+          }
+          // tangential position of this fine face inside the coarse face
+          // (subfaceIndex: the other axes in increasing order)
+          int sub[2] = {0, 0}, ns = 0;
+          for (int e = 0; e < dim; e++)
+            if (e != d) sub[ns++] = f[e] % 3;
+          for (int side = 0; side < 2; side++) {
+            if (side == 0 ? f[d] != 0 : f[d] != fe[d] - 1) continue;
+            const int face = 2 * d + side;
+            const int dsl = desc0 + ndesc++;
+            dslot[(size_t)(me - n0) * D2 + face] = dsl;
+            if (side == 0) {  // descendant below: it is the left cell
+              fl.push_back(dsl);
+              fr.push_back(me);
+            } else {
+              fl.push_back(me);
+              fr.push_back(dsl);
+            }
+            fd.push_back(d);
+            // restriction of this face into the ancestor's same face
+            rf.push_back(me * D2 + face);
+            rc.push_back(aid[cidx(parent)] * D2 + face);
+            ridx.push_back(sub[0]);
+            ridx.push_back(sub[1]);
+            // prolongation of the outside coarse cell's face that the
+            // descendant touches (the descendant sits at that cell's end)
+            int cn[3] = {parent[0], parent[1], parent[2]};
+            cn[d] += side == 0 ? -1 : 1;
+            const int dface = side == 0 ? 2 * d + 1 : 2 * d;
+            pf.push_back(dsl * D2 + dface);
+            pc.push_back(cid[cidx(cn)] * D2 + dface);
+            pidx.push_back(sub[0]);
+            pidx.push_back(sub[1]);
+          }
+        }
+      }
+  const int nslots = desc0 + ndesc;
+  m->ncells = n0 + n1;
+  m->nfaces = (int)fl.size();
+  m->ref.on = true;
+  m->ref.anc0 = anc0;
+  m->ref.nanc = nanc;
+  m->ref.nres = (int)rf.size();
+  m->ref.npro = (int)pf.size();
+  std::vector<int> inst((size_t)m->ncells, 1);
+  std::fill(inst.begin(), inst.begin() + n0, 0);
+  const double idx6[6] = {m->geo.dx[0], m->geo.dx[1], m->geo.dx[2], m->geo.dx[0] / 3.0, m->geo.dx[1] / 3.0,
+                          dim == 3 ? m->geo.dx[2] / 3.0 : 1.0};
+  std::vector<int> ones(std::max<size_t>(1, rf.size() + pf.size()), 1);
+  const size_t P = s->k.P, F = s->k.F, nV = s->k.nvar, nD = s->k.nvar + s->k.npar;
+  const size_t n = m->ncells, ns = nslots;
+  EXA_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  cudaStream_t st = m->stream;
+  auto ia = [&](int** p, size_t cnt) { return salloc(p, std::max<size_t>(1, cnt) * 4, st); };
+  bool ok = salloc(&m->luh, n * P * nD * 8, st) && salloc(&m->lduh, n * P * nV * 8, st) &&
+            salloc(&m->lQhbnd, ns * D2 * F * nD * 8, st) && salloc(&m->lFhbnd, ns * D2 * F * nV * 8, st) &&
+            salloc(&m->scal, 8 * 8, st) && ia(&m->iters, n) && ia(&m->fl, fl.size()) && ia(&m->fr, fl.size()) &&
+            ia(&m->fd, fl.size()) && ia(&m->bcell, 0) && ia(&m->bface, 0) && salloc(&m->sweeps, 8, st) &&
+            salloc(&m->ref.lv, 4 * 8, st) && ia(&m->ref.inst, n) && salloc(&m->ref.inst_dx, 6 * 8, st) &&
+            ia(&m->ref.res_f, rf.size()) && ia(&m->ref.res_c, rf.size()) && ia(&m->ref.res_ld, rf.size()) &&
+            ia(&m->ref.res_idx, 2 * rf.size()) && ia(&m->ref.pro_f, pf.size()) && ia(&m->ref.pro_c, pf.size()) &&
+            ia(&m->ref.pro_ld, pf.size()) && ia(&m->ref.pro_idx, 2 * pf.size());
+  if (!ok) {
+    cudaGetLastError();
+    mesh_free(m.get());
+    return fail(EXA_ERR_NOMEM, "exa_mesh_create_refined: device allocation failed");
+  }
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  };
+  ok = up(m->fl, fl.data(), fl.size() * 4) && up(m->fr, fr.data(), fr.size() * 4) && up(m->fd, fd.data(), fd.size() * 4) &&
+       up(m->ref.inst, inst.data(), n * 4) && up(m->ref.inst_dx, idx6, 6 * 8) &&
+       up(m->ref.res_f, rf.data(), rf.size() * 4) && up(m->ref.res_c, rc.data(), rc.size() * 4) &&
+       up(m->ref.res_ld, ones.data(), rf.size() * 4) && up(m->ref.res_idx, ridx.data(), ridx.size() * 4) &&
+       up(m->ref.pro_f, pf.data(), pf.size() * 4) && up(m->ref.pro_c, pc.data(), pc.size() * 4) &&
+       up(m->ref.pro_ld, ones.data(), pf.size() * 4) && up(m->ref.pro_idx, pidx.data(), pidx.size() * 4);
+  if (!ok) {
+    cudaStreamSynchronize(st);
+    mesh_free(m.get());
+    return fail(EXA_ERR_CUDA, "exa_mesh_create_refined: upload failed");
+  }
+  m->geo.inst = m->ref.inst;
+  m->geo.inst_dx = m->ref.inst_dx;
+  EXA_CUDA(cudaMemsetAsync(m->luh, 0, n * P * nD * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->lduh, 0, n * P * nV * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->lQhbnd, 0, ns * D2 * F * nD * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->lFhbnd, 0, ns * D2 * F * nV * 8, st));
+  EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, st));
+  EXA_CUDA(cudaStreamSynchronize(st));  // the host vectors go out of scope
+  *out = m.release();
+  return EXA_OK;
+}
+
 int exa_mesh_destroy(exa_mesh* m) {
   if (!m) return EXA_OK;
   mesh_free(m);
@@ -934,12 +1159,42 @@ int exa_mesh_copy_solution(exa_mesh* m, void* host, size_t nbytes, int to_device
 
 // The predictor of every cell; fused time stepping runs it with its own step
 // size (scal[5]) and, for the rerun, only when *count (device) is not 0.
+// The step size the kernels read and the new step's min-reduction target
+// (per level on a refined mesh).
+static double* mesh_dt(exa_mesh* m) { return m->ref.on ? m->ref.lv : m->scal + 0; }
+static double* mesh_dt_min(exa_mesh* m) { return m->ref.on ? m->ref.lv + 2 : m->scal + 1; }
+
+// Refined mesh, after every predictor: the ancestors' faces are zeroed and
+// receive the restriction of their fine children's extrapolated states and
+// fluxes (restrictToTopMostParent, ADERDGSolver.cpp:2465-2515, after
+// prepareFaceDataOfAncestor :2300-2331); the descendants' faces receive the
+// prolongation of their coarse parent's (prolongateFaceDataToDescendant
+// :2334-2382). The Riemann solves then pair fine cells with descendants and
+// coarse cells with ancestors (solveRiemannProblemAtInterface :2789, any
+// pair with at least one cell).
+static int mesh_amr_faces(exa_mesh* m) {
+  const KernelSet& k = m->s->k;
+  const size_t D2 = 2 * m->dim, nD = k.nvar + k.npar;
+  EXA_CUDA(cudaMemsetAsync(m->lQhbnd + (size_t)m->ref.anc0 * D2 * k.F * nD, 0, (size_t)m->ref.nanc * D2 * k.F * nD * 8,
+                           m->stream));
+  EXA_CUDA(cudaMemsetAsync(m->lFhbnd + (size_t)m->ref.anc0 * D2 * k.F * k.nvar, 0,
+                           (size_t)m->ref.nanc * D2 * k.F * k.nvar * 8, m->stream));
+  int rc = k.amr_face(m->lQhbnd, m->lFhbnd, m->lQhbnd, m->lFhbnd, m->ref.nres, m->ref.res_f, m->ref.res_c,
+                      m->ref.res_ld, m->ref.res_idx, 1, m->stream);
+  if (rc) return rc;
+  return k.amr_face(m->lQhbnd, m->lFhbnd, m->lQhbnd, m->lFhbnd, m->ref.npro, m->ref.pro_f, m->ref.pro_c,
+                    m->ref.pro_ld, m->ref.pro_idx, 0, m->stream);
+}
+
 static int mesh_predict(exa_mesh* m, const int* count = nullptr) {
   const KernelSet& k = m->s->k;
   PhaseTimer pt(m, 0);
   m->phase_launches[0] += 2;
-  return k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->scal + (m->fused ? 5 : 0), m->geo,
-                     m->ncells, nullptr, count, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
+  int rc = k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->fused ? m->scal + 5 : mesh_dt(m), m->geo,
+                       m->ncells, nullptr, count, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
+  if (rc || !m->ref.on) return rc;
+  m->phase_launches[0] += 3;
+  return mesh_amr_faces(m);
 }
 
 // Fused time stepping scalars: [0] corrector step, [1] min-reduction target,
@@ -989,6 +1244,7 @@ __global__ void fused_advance_kernel(double* scal, double w, int* rerun, int nce
 
 int exa_mesh_init_fused(exa_mesh* m, double t0, double weight) {
   if (!m || !(weight > 0.0) || weight > 1.0) return fail(EXA_ERR_ARG, "exa_mesh_init_fused: bad argument");
+  if (m->ref.on) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_init_fused: refined meshes step non-fused");
   const KernelSet& k = m->s->k;
   if (!m->rerun && !salloc(&m->rerun, sizeof(int), m->stream)) {
     cudaGetLastError();
@@ -1029,12 +1285,19 @@ int exa_mesh_init(exa_mesh* m, double t0) {
   m->fused = false;
   init_scalars_kernel<<<1, 1, 0, m->stream>>>(m->scal, t0);
   EXA_LAUNCHED();
+  if (m->ref.on) {
+    level_reset_kernel<<<1, 1, 0, m->stream>>>(m->ref.lv);
+    EXA_LAUNCHED();
+  }
   EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, m->stream));
   // first admissible step from the initial data, then the first predictor
-  int rc = k.corrector(m->luh, nullptr, nullptr, nullptr, m->scal + 1, m->geo, m->ncells, nullptr, 0, nullptr,
+  int rc = k.corrector(m->luh, nullptr, nullptr, nullptr, mesh_dt_min(m), m->geo, m->ncells, nullptr, 0, nullptr,
                        m->stream);
   if (rc) return rc;
-  take_dt_kernel<<<1, 1, 0, m->stream>>>(m->scal);
+  if (m->ref.on)
+    level_take_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->ref.lv);
+  else
+    take_dt_kernel<<<1, 1, 0, m->stream>>>(m->scal);
   EXA_LAUNCHED();
   rc = mesh_predict(m);
   if (rc) return rc;
@@ -1059,7 +1322,7 @@ static int mesh_one_step(exa_mesh* m) {
   }
   {
     PhaseTimer pt(m, 2);
-    rc = k.corrector(m->luh, m->lduh, m->lFhbnd, m->scal + 0, m->scal + 1, m->geo, m->ncells, nullptr, 1, nullptr,
+    rc = k.corrector(m->luh, m->lduh, m->lFhbnd, mesh_dt(m), mesh_dt_min(m), m->geo, m->ncells, nullptr, 1, nullptr,
                      m->stream);
     if (rc) return rc;
     m->phase_launches[2] += 1;
@@ -1081,7 +1344,10 @@ static int mesh_one_step(exa_mesh* m) {
   }
   {
     PhaseTimer pt(m, 3);
-    advance_kernel<<<1, 1, 0, m->stream>>>(m->scal);
+    if (m->ref.on)
+      level_advance_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->ref.lv);
+    else
+      advance_kernel<<<1, 1, 0, m->stream>>>(m->scal);
     EXA_LAUNCHED();
     m->phase_launches[3] += 1;
   }
@@ -1302,6 +1568,7 @@ extern "C" {
 
 int exa_mesh_write_vtk(exa_mesh* m, const char* path, int binary) {
   if (!m || !path) return fail(EXA_ERR_ARG, "exa_mesh_write_vtk: null argument");
+  if (m->ref.on) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_write_vtk: uniform meshes only");
   const KernelSet& k = m->s->k;
   const int dim = m->dim, N = k.order, b = N + 1, nD = k.nvar + k.npar;
   const size_t n = m->ncells, P = k.P, sub = dim == 3 ? (size_t)N * N * N : (size_t)N * N;

@@ -185,3 +185,35 @@ def elastic_pulse(dim, order, cells, seed=0):
     Q[..., 10] = 1.0 + 0.2 * s
     Q[..., 11] = 1.0 + 0.3 * s
     return Q, dict(centre=c.tolist(), direction=direction.tolist(), phase=phase.tolist())
+
+
+def refined_node_coordinates(dim, order, cells, box_lo, box_hi, offset=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0)):
+    """(ncells, b^dim, dim) node coordinates of a mesh made by
+    exa_mesh_create_refined: the unrefined coarse cells (x fastest), then the
+    fine cells of the refined box (x fastest)."""
+    Xc = node_coordinates(dim, order, cells, offset, size)
+    idx = np.indices(tuple(reversed(cells[:dim]))).reshape(dim, -1)[::-1]  # (dim, ncoarse), x first
+    inbox = np.ones(idx.shape[1], dtype=bool)
+    for d in range(dim):
+        inbox &= (idx[d] >= box_lo[d]) & (idx[d] < box_hi[d])
+    dx = [size[d] / cells[d] for d in range(dim)]
+    fe = [3 * (box_hi[d] - box_lo[d]) for d in range(dim)]
+    boff = [offset[d] + box_lo[d] * dx[d] for d in range(dim)] + [0.0] * (3 - dim)
+    bsize = [(box_hi[d] - box_lo[d]) * dx[d] for d in range(dim)] + [1.0] * (3 - dim)
+    Xf = node_coordinates(dim, order, fe, boff, bsize)
+    return np.concatenate([Xc[~inbox], Xf], axis=0)
+
+
+def pulse_refined(dim, order, cells, box_lo, box_hi, seed=0):
+    """Gaussian density pulse (amplitude 0.3, width 0.1) centred in the
+    refined box plus a seeded offset U[-0.05, 0.05]^dim, carried by the
+    velocity (1, 0.5, 0.25) through the box's faces; p = 1; periodic unit
+    domain. Returns luh in the refined mesh's cell order."""
+    rng = np.random.default_rng(seed)
+    c = np.array([(box_lo[d] + box_hi[d]) / (2.0 * cells[d]) for d in range(dim)])
+    c = c + rng.uniform(-0.05, 0.05, size=dim)
+    X = refined_node_coordinates(dim, order, cells, box_lo, box_hi)
+    rho = 1.0 + 0.3 * np.exp(-_periodic_d2(X, c) / 0.01)
+    vel = np.zeros(rho.shape + (3,))
+    vel[..., :dim] = np.array([1.0, 0.5, 0.25][:dim])
+    return conserved(rho, vel, np.ones_like(rho))

@@ -184,6 +184,23 @@ int exa_reset_min(double* dev, void* stream);
  * on both faces of an axis). Allocates all device state. */
 int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset, const double* size, const int* bc,
                     exa_mesh** out);
+/* A statically refined periodic mesh: the coarse grid of exa_mesh_create with
+ * the box of coarse cells box_lo[d] <= c[d] < box_hi[d] refined once (3^d
+ * fine cells each; at least one coarse cell must surround the box). Global
+ * time stepping; the same exa_mesh_* calls step it (not exa_mesh_init_fused,
+ * not exa_mesh_write_vtk). Solution order: the unrefined coarse cells
+ * (x fastest over the coarse grid, refined ones skipped), then the fine cells
+ * (x fastest over the box's fine grid). Replaces the spacetree's hanging-face
+ * handling for this layout: after every predictor the refined cells that
+ * face coarse cells (ancestors) receive the restriction of their fine
+ * children's face data (ADERDGSolver::restrictToTopMostParent,
+ * exahype/solvers/ADERDGSolver.cpp:2465-2515) and the virtual fine cells
+ * across the box's faces (descendants) the prolongation of their coarse
+ * parent's (prolongateFaceDataToDescendant, :2334-2382); Riemann problems
+ * pair coarse cells with ancestors and fine cells with descendants
+ * (solveRiemannProblemAtInterface, :2789). Nonlinear PDEs only. */
+int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
+                            const int* box_lo, const int* box_hi, exa_mesh** out);
 int exa_mesh_destroy(exa_mesh* m);
 int exa_mesh_num_cells(const exa_mesh* m, int* ncells);
 /* host <-> device solution, luh layout above, cells in x-fastest order */

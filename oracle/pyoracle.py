@@ -294,6 +294,152 @@ class Mesh:
         return dict(predictor_dt=f(self._h), reruns=g(self._h))
 
 
+class RefinedMesh:
+    """A periodic coarse grid with one box of coarse cells refined once (3^d
+    fine cells each), stepped with global time steps by per-cell calls of the
+    C restatement (impl='oracle') or of the compiled reference kernels
+    (impl='ref'); small meshes only (a Python loop over cells and faces).
+
+    Sequencing restated from the reference's traversals for such a mesh
+    (exahype/solvers/ADERDGSolver.cpp): after the predictor of every cell,
+    the refined coarse cells that face unrefined ones (ancestors) get their
+    faces zeroed (prepareFaceDataOfAncestor :2300-2331) and the fine children's
+    extrapolated states and fluxes restricted into them
+    (restrictToTopMostParent :2465-2515, faceUnknownsRestriction); the
+    virtual fine cells across the box's faces (descendants) get their coarse
+    parent's face prolongated (prolongateFaceDataToDescendant :2334-2382,
+    faceUnknownsProlongation). Riemann problems are solved for every pair of
+    same-level neighbours of which one is a cell (solveRiemannProblemAtInterface
+    :2789): coarse-coarse, coarse-ancestor, fine-fine and fine-descendant.
+    Then surface integral, update and stable step of every cell with its own
+    width; the step is the minimum over all cells.
+
+    Cell order: the unrefined coarse cells (x fastest), then the box's fine
+    cells (x fastest)."""
+
+    def __init__(self, dim, order, cells, size, box_lo, box_hi, impl="oracle"):
+        self.dim, self.order = dim, order
+        self.K = Kernels(dim, order, 0, impl)
+        self.impl = impl
+        d = dim
+        cells = list(cells)[:d]
+        lo, hi = list(box_lo)[:d], list(box_hi)[:d]
+        self.dx0 = [size[i] / cells[i] for i in range(d)]
+        self.dx1 = [x / 3.0 for x in self.dx0]
+        fe = [3 * (hi[i] - lo[i]) for i in range(d)]
+        inbox = lambda c: all(lo[i] <= c[i] < hi[i] for i in range(d))  # noqa: E731
+        onface = lambda c: any(c[i] == lo[i] or c[i] == hi[i] - 1 for i in range(d))  # noqa: E731
+        rng = lambda ext: [tuple(reversed(t)) for t in np.ndindex(*reversed(ext))]  # noqa: E731  x fastest
+        coarse = rng(cells)
+        self.cid = {}
+        for c in coarse:
+            if not inbox(c):
+                self.cid[c] = len(self.cid)
+        n0 = len(self.cid)
+        fine = rng(fe)
+        self.fid = {f: n0 + i for i, f in enumerate(fine)}
+        self.ncells = n0 + len(fine)
+        self.level = [0] * n0 + [1] * len(fine)
+        self.aid = {}
+        for c in coarse:
+            if inbox(c) and onface(c):
+                self.aid[c] = self.ncells + len(self.aid)
+        nslot = self.ncells + len(self.aid)
+        self.pairs, self.restr, self.prol = [], [], []
+        for c in coarse:
+            for i in range(d):
+                nb = list(c)
+                nb[i] = (c[i] + 1) % cells[i]
+                nb = tuple(nb)
+                a, b = inbox(c), inbox(nb)
+                if a and b:
+                    continue
+                self.pairs.append((self.aid[c] if a else self.cid[c], self.aid[nb] if b else self.cid[nb], i))
+        for f in fine:
+            me = self.fid[f]
+            parent = tuple(lo[i] + f[i] // 3 for i in range(d))
+            for i in range(d):
+                if f[i] + 1 < fe[i]:
+                    nb = list(f)
+                    nb[i] += 1
+                    self.pairs.append((me, self.fid[tuple(nb)], i))
+                sub = [f[e] % 3 for e in range(d) if e != i]
+                for side in (0, 1):
+                    if f[i] != (0 if side == 0 else fe[i] - 1):
+                        continue
+                    face = 2 * i + side
+                    desc = nslot
+                    nslot += 1
+                    self.pairs.append((desc, me, i) if side == 0 else (me, desc, i))
+                    self.restr.append((me, face, self.aid[parent], face, sub))
+                    cn = list(parent)
+                    cn[i] += -1 if side == 0 else 1
+                    dface = 2 * i + 1 if side == 0 else 2 * i
+                    self.prol.append((self.cid[tuple(cn)], dface, desc, dface, sub))
+        K = self.K
+        self.nslot = nslot
+        self.Q = np.zeros((nslot, 2 * d, K.F * K.ndata))
+        self.Fb = np.zeros((nslot, 2 * d, K.F * K.nvar))
+        self.u = np.zeros((self.ncells, K.P, K.ndata))
+        self.du = np.zeros((self.ncells, K.P * K.nvar))
+        self.t, self.dt, self.steps, self.sweeps = 0.0, 0.0, 0, 0
+
+    def _dx(self, c):
+        return self.dx1 if self.level[c] else self.dx0
+
+    def set_solution(self, u):
+        self.u = np.array(u, dtype=np.float64).reshape(self.u.shape)
+
+    def get_solution(self):
+        return self.u.copy()
+
+    def _stable(self):
+        return min(self.K.stable_dt(self.u[c], self._dx(c)) for c in range(self.ncells))
+
+    def _predict(self):
+        K, d = self.K, self.dim
+        for c in range(self.ncells):
+            o = K.predictor(self.u[c], self._dx(c), self.dt)
+            self.Q[c] = o["lQhbnd"].reshape(2 * d, -1)
+            self.Fb[c] = o["lFhbnd"].reshape(2 * d, -1)
+            self.du[c] = o["lduh"]
+            self.sweeps += int(o["iterations"])
+        for a in set(x[2] for x in self.restr):
+            self.Q[a] = 0.0
+            self.Fb[a] = 0.0
+        for f, face, a, aface, sub in self.restr:
+            q, fl = amr("face_restriction", d, self.order, K.nvar, K.ndata - K.nvar, 1, sub, coarse=self.Q[a, aface],
+                        fine=self.Q[f, face], coarse_flux=self.Fb[a, aface], fine_flux=self.Fb[f, face],
+                        impl=self.impl)
+            self.Q[a, aface], self.Fb[a, aface] = q, fl
+        for c, face, dsl, dface, sub in self.prol:
+            q, fl = amr("face_prolongation", d, self.order, K.nvar, K.ndata - K.nvar, 1, sub,
+                        coarse=self.Q[c, face], coarse_flux=self.Fb[c, face], impl=self.impl)
+            self.Q[dsl, dface], self.Fb[dsl, dface] = q, fl
+
+    def init(self, t0=0.0):
+        self.t, self.steps, self.sweeps = t0, 0, 0
+        self.dt = self._stable()
+        self._predict()
+
+    def step(self, n=1):
+        K = self.K
+        for _ in range(n):
+            for l, r, i in self.pairs:
+                fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1], self.Q[r, 2 * i], i)
+                self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i] = fl, fr
+            for c in range(self.ncells):
+                du = K.surface_integral(self.du[c], self.Fb[c].reshape(-1), self._dx(c))
+                self.u[c] = K.solution_update(self.u[c], du, self.dt).reshape(self.u[c].shape)
+            self.t += self.dt
+            self.steps += 1
+            self.dt = self._stable()
+            self._predict()
+
+    def state(self):
+        return dict(t=self.t, dt=self.dt, steps=self.steps, picard_sweeps=self.sweeps)
+
+
 class LimitingMesh:
     """Uniform mesh with the a-posteriori subcell limiter, run by the oracle's
     limiting harness (oracle/limiting_harness.c) over the C restatement."""

@@ -1,0 +1,81 @@
+"""Statically refined meshes (exa_mesh_create_refined) on the GPU against the
+oracle's restatement of the reference's hanging-face sequencing
+(pyoracle.RefinedMesh over the C kernels): ancestors receive the restriction
+of their fine children's face data, descendants the prolongation of their
+coarse parent's, Riemann problems pair cells with both.
+
+Bar: solution 1e-12 relative L2 (the restriction's additions run in any
+order on the GPU), equal step and Picard sweep counts, time and step size to
+1e-13 relative; a constant state stays constant to 1e-10 (the 13-digit
+operator tables leave round-off of that order)."""
+import numpy as np
+import pytest
+
+import pyoracle
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eb():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    import exahype_b200
+    exahype_b200.load()
+    return exahype_b200
+
+
+CASES = [(2, 3, (9, 9), (3, 3), (6, 6), 10, 0), (2, 5, (7, 8), (2, 3), (4, 5), 6, 3),
+         (3, 3, (4, 4, 4), (1, 1, 1), (2, 2, 2), 4, 0), (3, 5, (5, 5, 5), (2, 2, 2), (3, 3, 3), 3, 2),
+         (3, 5, (5, 5, 5), (2, 2, 2), (3, 3, 3), 3, 0)]
+
+
+@pytest.mark.parametrize("dim,N,cells,lo,hi,steps,variant", CASES)
+def test_refined_mesh_vs_oracle(eb, dim, N, cells, lo, hi, steps, variant):
+    from exahype_b200 import problems
+    u = problems.pulse_refined(dim, N, cells, lo, hi, seed=4)
+    s = eb.Solver(dim, N)
+    s.variant = variant
+    m = eb.Mesh.refined(s, cells, [0.0] * dim, [1.0] * dim, lo, hi)
+    o = pyoracle.RefinedMesh(dim, N, cells, [1.0] * dim, lo, hi)
+    assert m.ncells == o.ncells == u.shape[0]
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init(0.0)
+    o.init(0.0)
+    assert m.state()["dt"] == o.state()["dt"]  # from identical data: bit-identical
+    m.step(steps)
+    o.step(steps)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    sa, sb = m.state(), o.state()
+    assert sa["steps"] == sb["steps"] == steps
+    assert sa["picard_sweeps"] == sb["picard_sweeps"]
+    close = lambda x, y: abs(x - y) <= 1e-13 * abs(y)  # noqa: E731
+    assert close(sa["t"], sb["t"]) and close(sa["dt"], sb["dt"])
+    # the pulse crossed into and through the refined box
+    assert np.linalg.norm(a - u) / np.linalg.norm(u) > 1e-6
+
+
+def test_refined_mesh_free_stream(eb):
+    s = eb.Solver(2, 5)
+    m = eb.Mesh.refined(s, (9, 9), [0.0, 0.0], [1.0, 1.0], (3, 3), (6, 6))
+    u = np.zeros(m.solution_shape)
+    u[..., 0], u[..., 1], u[..., 2], u[..., 4] = 1.0, 0.4, -0.2, 2.5
+    m.set_solution(u)
+    m.init(0.0)
+    m.step(20)
+    assert np.abs(m.get_solution() - u).max() < 1e-10
+
+
+def test_refined_mesh_arguments(eb):
+    s = eb.Solver(2, 3)
+    for lo, hi in (((0, 3), (6, 6)), ((3, 3), (9, 6)), ((4, 3), (4, 6))):
+        with pytest.raises(eb.ExaError):
+            eb.Mesh.refined(s, (9, 9), [0.0, 0.0], [1.0, 1.0], lo, hi)
+    m = eb.Mesh.refined(s, (9, 9), [0.0, 0.0], [1.0, 1.0], (3, 3), (6, 6))
+    with pytest.raises(eb.ExaError):
+        m.init_fused(0.0, 0.99)
+    with pytest.raises(eb.ExaError):
+        eb.Mesh.refined(eb.Solver(2, 3, eb.PDE_ELASTIC), (9, 9), [0.0, 0.0], [1.0, 1.0], (3, 3), (6, 6))
