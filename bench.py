@@ -383,6 +383,7 @@ def run_ours(a):
     ens = None if a.no_ensemble else run_ensemble_workload(a, world, dev, rank)
     ela = None if a.no_elastic else run_elastic_workload(a, world, dev, rank, fp64_peak)
     amr = None if a.no_amr else run_amr_workload(a, world, dev, rank)
+    refined = None if a.no_refined else run_refined_workload(a, world, dev, rank)
     srv = None if a.no_serving else run_serving_workload(a, world, dev, rank)
     line = {
         "metric": METRIC, "value": value, "unit": "DoF-updates/s", "n_gpus": world, "steps": a.steps,
@@ -393,7 +394,7 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (solution 170 MB, face data 142 MB)"},
         "roofline": roof, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
-        "mixed": mixed, "fused": fused, "limiter": lim, "ensemble": ens, "serving": srv, "elastic": ela, "amr": amr,
+        "mixed": mixed, "fused": fused, "limiter": lim, "ensemble": ens, "serving": srv, "elastic": ela, "amr": amr, "refined": refined,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -466,6 +467,65 @@ def run_elastic_workload(a, world, dev, rank, fp64_peak=None):
             out["cpu_baseline"] = {"value": dof_step / el, "unit": "DoF-updates/s", "cores": nthreads,
                                    "kind": "reference", "sample": "1 full time step of the 27^3 elastic mesh on the "
                                    "reference's linear kernels, %.1f s" % el}
+    return out
+
+
+def run_refined_workload(a, world, dev, rank):
+    """A statically refined mesh (exa_mesh_create_refined): 3D Euler N=5, the
+    27^3 periodic pulse mesh with its central 9^3 coarse cells refined once
+    (18,954 coarse + 19,683 fine cells), global time steps; warm-up steps,
+    then min(steps, 20) timed steps with CUDA events on the mesh stream and
+    the per-phase split (the predictor phase includes the ancestors' face
+    restriction and the descendants' face prolongation); max over ranks. CPU
+    baseline: one step of a 9^3 mesh with its central 3^3 cells refined
+    (1,431 cells) through the reference's kernels compiled from its sources,
+    driven per cell by the oracle's refined-mesh sequencing on one thread."""
+    import torch
+    import exahype_b200 as eb
+    from exahype_b200 import problems
+    cells, lo, hi = (27, 27, 27), (9, 9, 9), (18, 18, 18)
+    u0 = problems.pulse_refined(3, 5, cells, lo, hi, seed=SEED + rank)
+    s = eb.Solver(3, 5, eb.PDE_EULER)
+    s.variant = a.variant if a.variant is not None else 2
+    m = eb.Mesh.refined(s, cells, [0.0] * 3, [1.0] * 3, lo, hi)
+    m.set_solution(u0)
+    m.init(0.0)
+    stream = torch.cuda.ExternalStream(m.stream_handle, device=dev)
+    m.step(max(3, a.warmup))
+    m.synchronize()
+    st0 = m.state()
+    k = max(1, min(a.steps, 20))
+    m.phase_times(reset=True)
+    m.set_profiling(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(k)
+    e1.record(stream)
+    e1.synchronize()
+    m.set_profiling(False)
+    ph = m.phase_times(reset=True)
+    ms = reduce_max(e0.elapsed_time(e1), world, dev)
+    dof_step = m.ncells * 6 ** 3 * 5
+    out = {"workload": "euler3d_N5_27^3_periodic_central_9^3_refined_once", "cells": m.ncells,
+           "value": dof_step * k * world / (ms / 1e3), "unit": "DoF-updates/s", "steps": k, "ms_per_step": ms / k,
+           "dof_per_step": dof_step, "predictor_variant": s.variant,
+           "phase_ms_per_step": {n: v[0] / k for n, v in ph.items()},
+           "picard_sweeps_per_step": (m.state()["picard_sweeps"] - st0["picard_sweeps"]) / k,
+           "timing": "exa_mesh_step(k) on the refined mesh, CUDA events on the mesh stream"}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import pyoracle
+        if pyoracle.ref_available(3):
+            sc, sl, sh = (9, 9, 9), (3, 3, 3), (6, 6, 6)
+            r = pyoracle.RefinedMesh(3, 5, sc, [1.0] * 3, sl, sh, impl="ref")
+            r.set_solution(problems.pulse_refined(3, 5, sc, sl, sh, seed=SEED))
+            r.init(0.0)
+            t0 = time.perf_counter()
+            r.step(1)
+            el = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": r.ncells * 6 ** 3 * 5 / el, "unit": "DoF-updates/s", "cores": 1,
+                                   "kind": "reference", "sample": "1 step of a 9^3 mesh with its central 3^3 cells "
+                                   "refined (%d cells), the reference's kernels per cell, %.1f s" % (r.ncells, el)}
     return out
 
 
@@ -795,13 +855,14 @@ def main():
     ap.add_argument("--serving-full", action="store_true", help="serving: the full-size request mix")
     ap.add_argument("--no-elastic", action="store_true", help="skip the linear-kernel (elastic waves) workload")
     ap.add_argument("--no-amr", action="store_true", help="skip the AMR transfer / plotting workload")
+    ap.add_argument("--no-refined", action="store_true", help="skip the statically refined mesh workload")
     ap.add_argument("--workload", default="headline",
-                    choices=["headline", "limiter", "ensemble", "serving", "elastic", "amr"],
-                    help="limiter / ensemble / serving / elastic: only that workload, as its own JSON line")
+                    choices=["headline", "limiter", "ensemble", "serving", "elastic", "amr", "refined"],
+                    help="limiter / ensemble / serving / elastic / amr / refined: only that workload, as its own JSON line")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
-    if a.workload in ("limiter", "ensemble", "serving", "elastic", "amr"):
+    if a.workload in ("limiter", "ensemble", "serving", "elastic", "amr", "refined"):
         return run_secondary_only(a)
     return run_ours(a)
 
@@ -814,7 +875,8 @@ def run_secondary_only(a):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     run = {"limiter": run_limiter_workload, "ensemble": run_ensemble_workload,
-           "serving": run_serving_workload, "elastic": run_elastic_workload, "amr": run_amr_workload}[a.workload]
+           "serving": run_serving_workload, "elastic": run_elastic_workload, "amr": run_amr_workload,
+           "refined": run_refined_workload}[a.workload]
     if a.workload == "elastic":
         r = run(a, world, torch.device("cuda", local), rank, None if a.no_fp64_probe else measure_fp64_peak())
     else:
