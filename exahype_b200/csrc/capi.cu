@@ -935,7 +935,6 @@ int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double*
                             const int* box_lo, const int* box_hi, exa_mesh** out) {
   if (!s || !cells || !offset || !size || !box_lo || !box_hi || !out)
     return fail(EXA_ERR_ARG, "exa_mesh_create_refined: null argument");
-  if (s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create_refined: nonlinear PDEs only");
   const int dim = s->k.dim, D2 = 2 * dim;
   std::unique_ptr<exa_mesh> m(new exa_mesh());
   m->s = s;

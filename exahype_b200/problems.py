@@ -172,11 +172,14 @@ def elastic_pulse(dim, order, cells, seed=0):
     rho = 1 + 0.3 s, lambda = 2 + 0.5 s, mu = 1 + 0.2 s with
     s = sin(2 pi (x + phase_x)) sin(2 pi (y + phase_y)), phases ~ U[0, 1].
     Returns luh (ncells, b^d, 12): sxx syy szz sxy syz sxz u v w lambda mu rho."""
+    return _elastic_at(node_coordinates(dim, order, cells), dim, seed)
+
+
+def _elastic_at(X, dim, seed):
     rng = np.random.default_rng(seed)
     c = rng.uniform(0.3, 0.7, size=dim)
     direction = rng.uniform(-1.0, 1.0, size=3)
     phase = rng.uniform(0.0, 1.0, size=2)
-    X = node_coordinates(dim, order, cells)
     g = np.exp(-_periodic_d2(X, c) / 0.01)
     s = np.sin(2 * np.pi * (X[..., 0] + phase[0])) * np.sin(2 * np.pi * (X[..., 1] + phase[1]))
     Q = np.zeros(X.shape[:-1] + (12,))
@@ -217,3 +220,9 @@ def pulse_refined(dim, order, cells, box_lo, box_hi, seed=0):
     vel = np.zeros(rho.shape + (3,))
     vel[..., :dim] = np.array([1.0, 0.5, 0.25][:dim])
     return conserved(rho, vel, np.ones_like(rho))
+
+
+def elastic_pulse_refined(dim, order, cells, box_lo, box_hi, seed=0):
+    """elastic_pulse's fields at the nodes of a refined mesh (cell order of
+    refined_node_coordinates). Returns luh (ncells, b^d, 12)."""
+    return _elastic_at(refined_node_coordinates(dim, order, cells, box_lo, box_hi), dim, seed)[0]

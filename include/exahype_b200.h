@@ -198,7 +198,7 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
  * across the box's faces (descendants) the prolongation of their coarse
  * parent's (prolongateFaceDataToDescendant, :2334-2382); Riemann problems
  * pair coarse cells with ancestors and fine cells with descendants
- * (solveRiemannProblemAtInterface, :2789). Nonlinear PDEs only. */
+ * (solveRiemannProblemAtInterface, :2789). */
 int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
                             const int* box_lo, const int* box_hi, exa_mesh** out);
 int exa_mesh_destroy(exa_mesh* m);

@@ -317,9 +317,10 @@ class RefinedMesh:
     Cell order: the unrefined coarse cells (x fastest), then the box's fine
     cells (x fastest)."""
 
-    def __init__(self, dim, order, cells, size, box_lo, box_hi, impl="oracle"):
-        self.dim, self.order = dim, order
-        self.K = Kernels(dim, order, 0, impl)
+    def __init__(self, dim, order, cells, size, box_lo, box_hi, pde=0, impl="oracle"):
+        self.dim, self.order, self.pde = dim, order, pde
+        self.linear = pde == 2
+        self.K = Kernels(dim, order, pde, impl)
         self.impl = impl
         d = dim
         cells = list(cells)[:d]
@@ -399,11 +400,14 @@ class RefinedMesh:
     def _predict(self):
         K, d = self.K, self.dim
         for c in range(self.ncells):
-            o = K.predictor(self.u[c], self._dx(c), self.dt)
+            if self.linear:
+                o = K.lin_predictor(self.u[c], self._dx(c), self.dt)
+            else:
+                o = K.predictor(self.u[c], self._dx(c), self.dt)
+                self.sweeps += int(o["iterations"])
             self.Q[c] = o["lQhbnd"].reshape(2 * d, -1)
             self.Fb[c] = o["lFhbnd"].reshape(2 * d, -1)
             self.du[c] = o["lduh"]
-            self.sweeps += int(o["iterations"])
         for a in set(x[2] for x in self.restr):
             self.Q[a] = 0.0
             self.Fb[a] = 0.0
@@ -426,10 +430,15 @@ class RefinedMesh:
         K = self.K
         for _ in range(n):
             for l, r, i in self.pairs:
-                fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1], self.Q[r, 2 * i], i)
+                if self.linear:
+                    fl, fr = K.lin_riemann(self.Q[l, 2 * i + 1], self.Q[r, 2 * i], i)
+                else:
+                    fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1],
+                                       self.Q[r, 2 * i], i)
                 self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i] = fl, fr
             for c in range(self.ncells):
-                du = K.surface_integral(self.du[c], self.Fb[c].reshape(-1), self._dx(c))
+                si = K.lin_surface_integral if self.linear else K.surface_integral
+                du = si(self.du[c], self.Fb[c].reshape(-1), self._dx(c))
                 self.u[c] = K.solution_update(self.u[c], du, self.dt).reshape(self.u[c].shape)
             self.t += self.dt
             self.steps += 1

@@ -28,6 +28,22 @@ def test_refined_oracle_vs_reference_kernels(dim, N, cells, lo, hi, steps):
     assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"]
 
 
+def test_refined_oracle_elastic_vs_reference_kernels():
+    if not pyoracle.ref_available(2):
+        pytest.skip("compiled reference kernels not built")
+    from exahype_b200 import problems
+    cells, lo, hi = (7, 7), (2, 2), (5, 5)
+    u = problems.elastic_pulse_refined(2, 4, cells, lo, hi, seed=4)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.RefinedMesh(2, 4, cells, [1.0, 1.0], lo, hi, pde=2, impl=impl)
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(3)
+        res.append(m.get_solution())
+    assert np.linalg.norm(res[0] - res[1]) / np.linalg.norm(res[1]) < 1e-12
+
+
 def test_refined_oracle_free_stream():
     m = pyoracle.RefinedMesh(2, 3, (9, 9), [1.0, 1.0], (3, 3), (6, 6))
     u = np.zeros((m.ncells, 16, 5))
