@@ -275,6 +275,15 @@ class Mesh:
         box_lo[d] <= c[d] < box_hi[d] refined once (3^d fine cells each;
         exa_mesh_create_refined). Solution order: the unrefined coarse cells
         (x fastest, refined ones skipped), then the fine cells of the box."""
+        return cls.nested(solver, cells, offset, size, [(box_lo, box_hi)])
+
+    @classmethod
+    def nested(cls, solver, cells, offset, size, boxes):
+        """Periodic mesh with nested refined boxes (exa_mesh_create_nested):
+        boxes[k] = (lo, hi) in the cell coordinates of level k (level 0 the
+        coarse grid; level k+1 box k refined once, coordinates over the whole
+        domain at that level). Solution order: the unrefined cells of each
+        level in turn, x fastest."""
         lib = load()
         d = solver.dim
         self = cls.__new__(cls)
@@ -282,14 +291,15 @@ class Mesh:
         c = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
         o = _dbl3(list(offset) + [0.0] * (3 - len(offset)))
         s = _dbl3(list(size) + [1.0] * (3 - len(size)))
-        lo = (ctypes.c_int * 3)(*(list(box_lo) + [0] * (3 - len(box_lo))))
-        hi = (ctypes.c_int * 3)(*(list(box_hi) + [1] * (3 - len(box_hi))))
+        nb = len(boxes)
+        lo = (ctypes.c_int * (3 * nb))(*sum((list(b[0]) + [0] * (3 - len(b[0])) for b in boxes), []))
+        hi = (ctypes.c_int * (3 * nb))(*sum((list(b[1]) + [1] * (3 - len(b[1])) for b in boxes), []))
         h = ctypes.c_void_p()
-        _check(lib.exa_mesh_create_refined(solver._h, c, o, s, lo, hi, ctypes.byref(h)), "exa_mesh_create_refined")
+        _check(lib.exa_mesh_create_nested(solver._h, c, o, s, nb, lo, hi, ctypes.byref(h)), "exa_mesh_create_nested")
         self._h = h
         self.solver = solver
         self.cells = tuple(cells)
-        self.box = (tuple(box_lo), tuple(box_hi))
+        self.boxes = [(tuple(b[0]), tuple(b[1])) for b in boxes]
         n = ctypes.c_int()
         _check(lib.exa_mesh_num_cells(h, ctypes.byref(n)), "exa_mesh_num_cells")
         self.ncells = n.value

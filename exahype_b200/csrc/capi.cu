@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <climits>
 #include <cstdio>
@@ -440,22 +441,25 @@ __global__ void take_dt_kernel(double* scal) {
   scal[1] = __longlong_as_double(0x7fefffffffffffffll);
 }
 
-// Refined meshes: lv[0..1] the step size each level's kernels read, lv[2..3]
-// the levels' min-reduction targets. The global step is the min over both
-// levels (global time stepping).
-__global__ void level_reset_kernel(double* lv) {
-  lv[2] = lv[3] = __longlong_as_double(0x7fefffffffffffffll);
+// Refined meshes with L levels: lv[0..L-1] the step size each level's
+// kernels read, lv[L..2L-1] the levels' min-reduction targets. The global
+// step is the min over all levels (global time stepping).
+__global__ void level_reset_kernel(double* lv, int L) {
+  for (int l = 0; l < L; l++) lv[L + l] = __longlong_as_double(0x7fefffffffffffffll);
 }
-__global__ void level_take_kernel(double* scal, double* lv) {
-  const double s = (lv[3] < lv[2]) ? lv[3] : lv[2];
-  scal[0] = lv[0] = lv[1] = s;
-  lv[2] = lv[3] = __longlong_as_double(0x7fefffffffffffffll);
+__device__ void level_take(double* scal, double* lv, int L) {
+  double s = __longlong_as_double(0x7fefffffffffffffll);
+  for (int l = 0; l < L; l++) {
+    s = (lv[L + l] < s) ? lv[L + l] : s;
+    lv[L + l] = __longlong_as_double(0x7fefffffffffffffll);
+  }
+  scal[0] = s;
+  for (int l = 0; l < L; l++) lv[l] = s;
 }
-__global__ void level_advance_kernel(double* scal, double* lv) {
+__global__ void level_take_kernel(double* scal, double* lv, int L) { level_take(scal, lv, L); }
+__global__ void level_advance_kernel(double* scal, double* lv, int L) {
   scal[2] += scal[0];
-  const double s = (lv[3] < lv[2]) ? lv[3] : lv[2];
-  scal[0] = lv[0] = lv[1] = s;
-  lv[2] = lv[3] = __longlong_as_double(0x7fefffffffffffffll);
+  level_take(scal, lv, L);
   scal[3] += 1.0;
 }
 
@@ -511,14 +515,16 @@ struct exa_mesh {
   bool fused = false;
   double weight = 0.99;
   int* rerun = nullptr;
-  // statically refined mesh (exa_mesh_create_refined): two levels as two
-  // geometry instances (per-cell level index, per-level widths), per-level
-  // step sizes and min-reduction targets lv[0..1], lv[2..3], the face slots
-  // of the refined cells that face coarse cells (ancestors, zeroed and
-  // restricted into after every predictor) and of the virtual fine cells
-  // across the refined box's faces (descendants, prolongated into)
+  // statically refined mesh (exa_mesh_create_nested / _refined): nlev
+  // levels as geometry instances (per-cell level index, per-level widths),
+  // per-level step sizes and min-reduction targets lv[0..nlev-1],
+  // lv[nlev..2 nlev-1], the face slots of the refined cells that face
+  // coarser cells (ancestors, zeroed and restricted into after every
+  // predictor) and of the virtual finer cells across each refined box's
+  // faces (descendants, prolongated into)
   struct {
     bool on = false;
+    int nlev = 1;
     double* lv = nullptr;
     int* inst = nullptr;
     double* inst_dx = nullptr;
@@ -931,178 +937,204 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
   return EXA_OK;
 }
 
-int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
-                            const int* box_lo, const int* box_hi, exa_mesh** out) {
+// Topology of a nested refined mesh: level 0 is the periodic grid, level l
+// >= 1 the box box[l-1] of level l-1 (in level-(l-1) cell coordinates)
+// refined once. Slots: the cells of every level (level by level, x fastest,
+// refined positions skipped), then the ancestors (refined positions on their
+// box's faces), then the descendants (one per cell on a refined box's face
+// and face it lies on).
+namespace {
+struct NestedTopo {
+  int dim = 0, L = 1, ncells = 0, anc0 = 0, nanc = 0, nslots = 0;
+  std::vector<int> level;                              // per cell
+  std::vector<int> fl, fr, fd;                          // Riemann pairs
+  std::vector<int> rf, rc, ridx, pf, pc, pidx;          // restriction / prolongation items
+};
+
+// returns an error message, or nullptr
+static const char* nested_topology(int dim, const int* cells, int nb, const int* lo, const int* hi, NestedTopo& t) {
+  const int L = nb + 1, D2 = 2 * dim;
+  t.dim = dim;
+  t.L = L;
+  // region of level l in level-l coordinates: [r0, r1)
+  std::vector<std::array<int, 3>> r0(L), r1(L);
+  for (int d = 0; d < 3; d++) {
+    r0[0][d] = 0;
+    r1[0][d] = d < dim ? cells[d] : 1;
+  }
+  for (int l = 1; l < L; l++)
+    for (int d = 0; d < 3; d++) {
+      const int bl = lo[3 * (l - 1) + d], bh = hi[3 * (l - 1) + d];
+      if (d < dim) {
+        if (bl < r0[l - 1][d] + 1 || bh <= bl || bh > r1[l - 1][d] - 1)
+          return "each refined box must lie inside its level's region with at least one cell around it";
+        r0[l][d] = 3 * bl;
+        r1[l][d] = 3 * bh;
+      } else {
+        r0[l][d] = 0;
+        r1[l][d] = 1;
+      }
+    }
+  long long total = 0;
+  for (int l = 0; l < L; l++) total += (long long)(r1[l][0] - r0[l][0]) * (r1[l][1] - r0[l][1]) * (r1[l][2] - r0[l][2]);
+  if (total > (1ll << 27)) return "too many cells";
+  // per level: position -> cell slot (or ancestor slot, or -1)
+  std::vector<std::vector<int>> cid(L), aid(L);
+  auto ext = [&](int l, int d) { return r1[l][d] - r0[l][d]; };
+  auto pidx_ = [&](int l, const int* p) {
+    return ((size_t)(p[2] - r0[l][2]) * ext(l, 1) + (p[1] - r0[l][1])) * ext(l, 0) + (p[0] - r0[l][0]);
+  };
+  auto refined = [&](int l, const int* p) {  // inside box l+1
+    if (l + 1 >= L) return false;
+    for (int d = 0; d < dim; d++)
+      if (p[d] < lo[3 * l + d] || p[d] >= hi[3 * l + d]) return false;
+    return true;
+  };
+  auto on_box_face = [&](int l, const int* p) {  // refined and on box l+1's faces
+    for (int d = 0; d < dim; d++)
+      if (p[d] == lo[3 * l + d] || p[d] == hi[3 * l + d] - 1) return true;
+    return false;
+  };
+  auto for_region = [&](int l, auto&& fn) {
+    int p[3];
+    for (p[2] = r0[l][2]; p[2] < r1[l][2]; p[2]++)
+      for (p[1] = r0[l][1]; p[1] < r1[l][1]; p[1]++)
+        for (p[0] = r0[l][0]; p[0] < r1[l][0]; p[0]++) fn(p);
+  };
+  int n = 0;
+  for (int l = 0; l < L; l++) {
+    cid[l].assign((size_t)ext(l, 0) * ext(l, 1) * ext(l, 2), -1);
+    aid[l].assign(cid[l].size(), -1);
+    for_region(l, [&](const int* p) {
+      if (!refined(l, p)) {
+        cid[l][pidx_(l, p)] = n++;
+        t.level.push_back(l);
+      }
+    });
+  }
+  t.ncells = n;
+  t.anc0 = n;
+  for (int l = 0; l + 1 < L; l++)
+    for_region(l, [&](const int* p) {
+      if (refined(l, p) && on_box_face(l, p)) aid[l][pidx_(l, p)] = n++, t.nanc++;
+    });
+  for (int l = 0; l < L; l++)
+    for_region(l, [&](const int* p) {
+      const bool rp = refined(l, p);
+      const int me = rp ? aid[l][pidx_(l, p)] : cid[l][pidx_(l, p)];
+      for (int d = 0; d < dim; d++) {
+        int q[3] = {p[0], p[1], p[2]};
+        q[d] = p[d] + 1;
+        if (l == 0) q[d] %= cells[d];  // periodic coarse grid
+        if (q[d] < r1[l][d]) {         // same-level neighbour: skip refined pairs
+          const bool rq = refined(l, q);
+          if (!(rp && rq)) {
+            t.fl.push_back(me);
+            t.fr.push_back(rq ? aid[l][pidx_(l, q)] : cid[l][pidx_(l, q)]);
+            t.fd.push_back(d);
+          }
+        }
+        if (l == 0 || rp) continue;
+        // a cell on its region's face: a descendant across it (the coarse
+        // neighbour's virtual child), with the face transfers
+        int sub[2] = {0, 0}, ns = 0;
+        for (int e = 0; e < dim; e++)
+          if (e != d) sub[ns++] = p[e] % 3;
+        const int parent[3] = {p[0] / 3, p[1] / 3, dim == 3 ? p[2] / 3 : 0};
+        for (int side = 0; side < 2; side++) {
+          if (p[d] != (side == 0 ? r0[l][d] : r1[l][d] - 1)) continue;
+          const int face = 2 * d + side, desc = n++;
+          t.fl.push_back(side == 0 ? desc : me);
+          t.fr.push_back(side == 0 ? me : desc);
+          t.fd.push_back(d);
+          t.rf.push_back(me * D2 + face);
+          t.rc.push_back(aid[l - 1][pidx_(l - 1, parent)] * D2 + face);
+          t.ridx.push_back(sub[0]);
+          t.ridx.push_back(sub[1]);
+          int cn[3] = {parent[0], parent[1], parent[2]};
+          cn[d] += side == 0 ? -1 : 1;
+          const int dface = side == 0 ? 2 * d + 1 : 2 * d;
+          t.pf.push_back(desc * D2 + dface);
+          t.pc.push_back(cid[l - 1][pidx_(l - 1, cn)] * D2 + dface);
+          t.pidx.push_back(sub[0]);
+          t.pidx.push_back(sub[1]);
+        }
+      }
+    });
+  t.nslots = n;
+  return nullptr;
+}
+}  // namespace
+
+int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* offset, const double* size,
+                           int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out) {
   if (!s || !cells || !offset || !size || !box_lo || !box_hi || !out)
-    return fail(EXA_ERR_ARG, "exa_mesh_create_refined: null argument");
+    return fail(EXA_ERR_ARG, "exa_mesh_create_nested: null argument");
+  if (nboxes < 1 || nboxes > 8) return fail(EXA_ERR_ARG, "exa_mesh_create_nested: 1 to 8 refined boxes");
   const int dim = s->k.dim, D2 = 2 * dim;
   std::unique_ptr<exa_mesh> m(new exa_mesh());
   m->s = s;
   m->dim = dim;
-  int fe[3] = {1, 1, 1};  // fine cells per axis inside the box
-  long long n_coarse = 1;
   for (int d = 0; d < dim; d++) {
-    if (cells[d] < 3 || !(size[d] > 0)) return fail(EXA_ERR_ARG, "exa_mesh_create_refined: bad grid");
-    if (box_lo[d] < 1 || box_hi[d] <= box_lo[d] || box_hi[d] > cells[d] - 1)
-      return fail(EXA_ERR_ARG, "exa_mesh_create_refined: the refined box must lie inside the grid with at least "
-                               "one coarse cell around it");
+    if (cells[d] < 3 || !(size[d] > 0)) return fail(EXA_ERR_ARG, "exa_mesh_create_nested: bad grid");
     m->cells[d] = cells[d];
     m->offset[d] = offset[d];
     m->geo.dx[d] = size[d] / cells[d];
-    fe[d] = 3 * (box_hi[d] - box_lo[d]);
-    n_coarse *= cells[d];
   }
   for (int d = dim; d < 3; d++) m->geo.dx[d] = 1.0;
   for (int f = 0; f < 6; f++) m->bc[f] = EXA_BC_PERIODIC;
-  if (n_coarse > (1ll << 26) || (long long)fe[0] * fe[1] * fe[2] > (1ll << 26))
-    return fail(EXA_ERR_ARG, "exa_mesh_create_refined: too many cells");
-  const int cz = dim == 3 ? cells[2] : 1;
-  auto cidx = [&](const int* c) { return (c[2] * cells[1] + c[1]) * cells[0] + c[0]; };
-  auto inbox = [&](const int* c) {
-    for (int d = 0; d < dim; d++)
-      if (c[d] < box_lo[d] || c[d] >= box_hi[d]) return false;
-    return true;
-  };
-  auto on_box_face = [&](const int* c) {
-    for (int d = 0; d < dim; d++)
-      if (c[d] == box_lo[d] || c[d] == box_hi[d] - 1) return true;
-    return false;
-  };
-  // slots: coarse cells, fine cells, ancestors (refined cells on the box's
-  // faces), descendants (one per fine cell and box face it lies on)
-  std::vector<int> cid((size_t)n_coarse, -1), aid((size_t)n_coarse, -1);
-  int n0 = 0;
-  for (int k = 0; k < cz; k++)
-    for (int j = 0; j < cells[1]; j++)
-      for (int i = 0; i < cells[0]; i++) {
-        const int c[3] = {i, j, k};
-        if (!inbox(c)) cid[cidx(c)] = n0++;
-      }
-  const int n1 = fe[0] * fe[1] * fe[2];
-  const int anc0 = n0 + n1;
-  int nanc = 0;
-  for (int k = 0; k < cz; k++)
-    for (int j = 0; j < cells[1]; j++)
-      for (int i = 0; i < cells[0]; i++) {
-        const int c[3] = {i, j, k};
-        if (inbox(c) && on_box_face(c)) aid[cidx(c)] = anc0 + nanc++;
-      }
-  auto fid = [&](const int* f) { return n0 + (f[2] * fe[1] + f[1]) * fe[0] + f[0]; };
-  const int desc0 = anc0 + nanc;
-  int ndesc = 0;
-  std::vector<int> dslot((size_t)n1 * D2, -1);
-  std::vector<int> fl, fr, fd, rf, rc, ridx, pf, pc, pidx;
-  // coarse level: cell-cell and cell-ancestor faces (refined-refined faces
-  // are solved on the fine level)
-  for (int k = 0; k < cz; k++)
-    for (int j = 0; j < cells[1]; j++)
-      for (int i = 0; i < cells[0]; i++) {
-        const int c[3] = {i, j, k};
-        for (int d = 0; d < dim; d++) {
-          int nb[3] = {i, j, k};
-          nb[d] = (c[d] + 1) % cells[d];
-          const bool rc_ = inbox(c), rn = inbox(nb);
-          if (rc_ && rn) continue;
-          fl.push_back(rc_ ? aid[cidx(c)] : cid[cidx(c)]);
-          fr.push_back(rn ? aid[cidx(nb)] : cid[cidx(nb)]);
-          fd.push_back(d);
-        }
-      }
-  // fine level: fine-fine faces, fine-descendant faces, and the face
-  // transfers of the fine cells on the box's faces
-  for (int K = 0; K < fe[2]; K++)
-    for (int J = 0; J < fe[1]; J++)
-      for (int I = 0; I < fe[0]; I++) {
-        const int f[3] = {I, J, K};
-        const int me = fid(f);
-        const int parent[3] = {box_lo[0] + I / 3, box_lo[1] + J / 3, dim == 3 ? box_lo[2] + K / 3 : 0};
-        for (int d = 0; d < dim; d++) {
-          if (f[d] + 1 < fe[d]) {
-            int nb[3] = {I, J, K};
-            nb[d]++;
-            fl.push_back(me);
-            fr.push_back(fid(nb));
-            fd.push_back(d);
-          }
-          // tangential position of this fine face inside the coarse face
-          // (subfaceIndex: the other axes in increasing order)
-          int sub[2] = {0, 0}, ns = 0;
-          for (int e = 0; e < dim; e++)
-            if (e != d) sub[ns++] = f[e] % 3;
-          for (int side = 0; side < 2; side++) {
-            if (side == 0 ? f[d] != 0 : f[d] != fe[d] - 1) continue;
-            const int face = 2 * d + side;
-            const int dsl = desc0 + ndesc++;
-            dslot[(size_t)(me - n0) * D2 + face] = dsl;
-            if (side == 0) {  // descendant below: it is the left cell
-              fl.push_back(dsl);
-              fr.push_back(me);
-            } else {
-              fl.push_back(me);
-              fr.push_back(dsl);
-            }
-            fd.push_back(d);
-            // restriction of this face into the ancestor's same face
-            rf.push_back(me * D2 + face);
-            rc.push_back(aid[cidx(parent)] * D2 + face);
-            ridx.push_back(sub[0]);
-            ridx.push_back(sub[1]);
-            // prolongation of the outside coarse cell's face that the
-            // descendant touches (the descendant sits at that cell's end)
-            int cn[3] = {parent[0], parent[1], parent[2]};
-            cn[d] += side == 0 ? -1 : 1;
-            const int dface = side == 0 ? 2 * d + 1 : 2 * d;
-            pf.push_back(dsl * D2 + dface);
-            pc.push_back(cid[cidx(cn)] * D2 + dface);
-            pidx.push_back(sub[0]);
-            pidx.push_back(sub[1]);
-          }
-        }
-      }
-  const int nslots = desc0 + ndesc;
-  m->ncells = n0 + n1;
-  m->nfaces = (int)fl.size();
+  NestedTopo t;
+  if (const char* err = nested_topology(dim, cells, nboxes, box_lo, box_hi, t))
+    return fail(EXA_ERR_ARG, std::string("exa_mesh_create_nested: ") + err);
+  const int L = t.L;
+  m->ncells = t.ncells;
+  m->nfaces = (int)t.fl.size();
   m->ref.on = true;
-  m->ref.anc0 = anc0;
-  m->ref.nanc = nanc;
-  m->ref.nres = (int)rf.size();
-  m->ref.npro = (int)pf.size();
-  std::vector<int> inst((size_t)m->ncells, 1);
-  std::fill(inst.begin(), inst.begin() + n0, 0);
-  const double idx6[6] = {m->geo.dx[0], m->geo.dx[1], m->geo.dx[2], m->geo.dx[0] / 3.0, m->geo.dx[1] / 3.0,
-                          dim == 3 ? m->geo.dx[2] / 3.0 : 1.0};
-  std::vector<int> ones(std::max<size_t>(1, rf.size() + pf.size()), 1);
+  m->ref.nlev = L;
+  m->ref.anc0 = t.anc0;
+  m->ref.nanc = t.nanc;
+  m->ref.nres = (int)t.rf.size();
+  m->ref.npro = (int)t.pf.size();
+  // each level's width is its parent level's divided by 3 (as a spacetree
+  // computes the width of a child cell)
+  std::vector<double> ldx(3 * (size_t)L);
+  for (int d = 0; d < 3; d++) ldx[d] = m->geo.dx[d];
+  for (int l = 1; l < L; l++)
+    for (int d = 0; d < 3; d++) ldx[3 * l + d] = d < dim ? ldx[3 * (l - 1) + d] / 3.0 : 1.0;
+  std::vector<int> ones(std::max<size_t>(1, t.rf.size() + t.pf.size()), 1);
   const size_t P = s->k.P, F = s->k.F, nV = s->k.nvar, nD = s->k.nvar + s->k.npar;
-  const size_t n = m->ncells, ns = nslots;
+  const size_t n = m->ncells, ns = t.nslots;
   EXA_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
   cudaStream_t st = m->stream;
   auto ia = [&](int** p, size_t cnt) { return salloc(p, std::max<size_t>(1, cnt) * 4, st); };
   bool ok = salloc(&m->luh, n * P * nD * 8, st) && salloc(&m->lduh, n * P * nV * 8, st) &&
             salloc(&m->lQhbnd, ns * D2 * F * nD * 8, st) && salloc(&m->lFhbnd, ns * D2 * F * nV * 8, st) &&
-            salloc(&m->scal, 8 * 8, st) && ia(&m->iters, n) && ia(&m->fl, fl.size()) && ia(&m->fr, fl.size()) &&
-            ia(&m->fd, fl.size()) && ia(&m->bcell, 0) && ia(&m->bface, 0) && salloc(&m->sweeps, 8, st) &&
-            salloc(&m->ref.lv, 4 * 8, st) && ia(&m->ref.inst, n) && salloc(&m->ref.inst_dx, 6 * 8, st) &&
-            ia(&m->ref.res_f, rf.size()) && ia(&m->ref.res_c, rf.size()) && ia(&m->ref.res_ld, rf.size()) &&
-            ia(&m->ref.res_idx, 2 * rf.size()) && ia(&m->ref.pro_f, pf.size()) && ia(&m->ref.pro_c, pf.size()) &&
-            ia(&m->ref.pro_ld, pf.size()) && ia(&m->ref.pro_idx, 2 * pf.size());
+            salloc(&m->scal, 8 * 8, st) && ia(&m->iters, n) && ia(&m->fl, t.fl.size()) && ia(&m->fr, t.fl.size()) &&
+            ia(&m->fd, t.fl.size()) && ia(&m->bcell, 0) && ia(&m->bface, 0) && salloc(&m->sweeps, 8, st) &&
+            salloc(&m->ref.lv, 2 * (size_t)L * 8, st) && ia(&m->ref.inst, n) &&
+            salloc(&m->ref.inst_dx, ldx.size() * 8, st) && ia(&m->ref.res_f, t.rf.size()) &&
+            ia(&m->ref.res_c, t.rf.size()) && ia(&m->ref.res_ld, t.rf.size()) && ia(&m->ref.res_idx, t.ridx.size()) &&
+            ia(&m->ref.pro_f, t.pf.size()) && ia(&m->ref.pro_c, t.pf.size()) && ia(&m->ref.pro_ld, t.pf.size()) &&
+            ia(&m->ref.pro_idx, t.pidx.size());
   if (!ok) {
     cudaGetLastError();
     mesh_free(m.get());
-    return fail(EXA_ERR_NOMEM, "exa_mesh_create_refined: device allocation failed");
+    return fail(EXA_ERR_NOMEM, "exa_mesh_create_nested: device allocation failed");
   }
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
   };
-  ok = up(m->fl, fl.data(), fl.size() * 4) && up(m->fr, fr.data(), fr.size() * 4) && up(m->fd, fd.data(), fd.size() * 4) &&
-       up(m->ref.inst, inst.data(), n * 4) && up(m->ref.inst_dx, idx6, 6 * 8) &&
-       up(m->ref.res_f, rf.data(), rf.size() * 4) && up(m->ref.res_c, rc.data(), rc.size() * 4) &&
-       up(m->ref.res_ld, ones.data(), rf.size() * 4) && up(m->ref.res_idx, ridx.data(), ridx.size() * 4) &&
-       up(m->ref.pro_f, pf.data(), pf.size() * 4) && up(m->ref.pro_c, pc.data(), pc.size() * 4) &&
-       up(m->ref.pro_ld, ones.data(), pf.size() * 4) && up(m->ref.pro_idx, pidx.data(), pidx.size() * 4);
+  ok = up(m->fl, t.fl.data(), t.fl.size() * 4) && up(m->fr, t.fr.data(), t.fr.size() * 4) &&
+       up(m->fd, t.fd.data(), t.fd.size() * 4) && up(m->ref.inst, t.level.data(), n * 4) &&
+       up(m->ref.inst_dx, ldx.data(), ldx.size() * 8) && up(m->ref.res_f, t.rf.data(), t.rf.size() * 4) &&
+       up(m->ref.res_c, t.rc.data(), t.rc.size() * 4) && up(m->ref.res_ld, ones.data(), t.rf.size() * 4) &&
+       up(m->ref.res_idx, t.ridx.data(), t.ridx.size() * 4) && up(m->ref.pro_f, t.pf.data(), t.pf.size() * 4) &&
+       up(m->ref.pro_c, t.pc.data(), t.pc.size() * 4) && up(m->ref.pro_ld, ones.data(), t.pf.size() * 4) &&
+       up(m->ref.pro_idx, t.pidx.data(), t.pidx.size() * 4);
   if (!ok) {
     cudaStreamSynchronize(st);
     mesh_free(m.get());
-    return fail(EXA_ERR_CUDA, "exa_mesh_create_refined: upload failed");
+    return fail(EXA_ERR_CUDA, "exa_mesh_create_nested: upload failed");
   }
   m->geo.inst = m->ref.inst;
   m->geo.inst_dx = m->ref.inst_dx;
@@ -1114,6 +1146,11 @@ int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double*
   EXA_CUDA(cudaStreamSynchronize(st));  // the host vectors go out of scope
   *out = m.release();
   return EXA_OK;
+}
+
+int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
+                            const int* box_lo, const int* box_hi, exa_mesh** out) {
+  return exa_mesh_create_nested(s, cells, offset, size, 1, box_lo, box_hi, out);
 }
 
 int exa_mesh_destroy(exa_mesh* m) {
@@ -1161,7 +1198,7 @@ int exa_mesh_copy_solution(exa_mesh* m, void* host, size_t nbytes, int to_device
 // The step size the kernels read and the new step's min-reduction target
 // (per level on a refined mesh).
 static double* mesh_dt(exa_mesh* m) { return m->ref.on ? m->ref.lv : m->scal + 0; }
-static double* mesh_dt_min(exa_mesh* m) { return m->ref.on ? m->ref.lv + 2 : m->scal + 1; }
+static double* mesh_dt_min(exa_mesh* m) { return m->ref.on ? m->ref.lv + m->ref.nlev : m->scal + 1; }
 
 // Refined mesh, after every predictor: the ancestors' faces are zeroed and
 // receive the restriction of their fine children's extrapolated states and
@@ -1285,7 +1322,7 @@ int exa_mesh_init(exa_mesh* m, double t0) {
   init_scalars_kernel<<<1, 1, 0, m->stream>>>(m->scal, t0);
   EXA_LAUNCHED();
   if (m->ref.on) {
-    level_reset_kernel<<<1, 1, 0, m->stream>>>(m->ref.lv);
+    level_reset_kernel<<<1, 1, 0, m->stream>>>(m->ref.lv, m->ref.nlev);
     EXA_LAUNCHED();
   }
   EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, m->stream));
@@ -1294,7 +1331,7 @@ int exa_mesh_init(exa_mesh* m, double t0) {
                        m->stream);
   if (rc) return rc;
   if (m->ref.on)
-    level_take_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->ref.lv);
+    level_take_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->ref.lv, m->ref.nlev);
   else
     take_dt_kernel<<<1, 1, 0, m->stream>>>(m->scal);
   EXA_LAUNCHED();
@@ -1344,7 +1381,7 @@ static int mesh_one_step(exa_mesh* m) {
   {
     PhaseTimer pt(m, 3);
     if (m->ref.on)
-      level_advance_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->ref.lv);
+      level_advance_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->ref.lv, m->ref.nlev);
     else
       advance_kernel<<<1, 1, 0, m->stream>>>(m->scal);
     EXA_LAUNCHED();

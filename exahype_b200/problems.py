@@ -194,17 +194,33 @@ def refined_node_coordinates(dim, order, cells, box_lo, box_hi, offset=(0.0, 0.0
     """(ncells, b^dim, dim) node coordinates of a mesh made by
     exa_mesh_create_refined: the unrefined coarse cells (x fastest), then the
     fine cells of the refined box (x fastest)."""
-    Xc = node_coordinates(dim, order, cells, offset, size)
-    idx = np.indices(tuple(reversed(cells[:dim]))).reshape(dim, -1)[::-1]  # (dim, ncoarse), x first
-    inbox = np.ones(idx.shape[1], dtype=bool)
-    for d in range(dim):
-        inbox &= (idx[d] >= box_lo[d]) & (idx[d] < box_hi[d])
-    dx = [size[d] / cells[d] for d in range(dim)]
-    fe = [3 * (box_hi[d] - box_lo[d]) for d in range(dim)]
-    boff = [offset[d] + box_lo[d] * dx[d] for d in range(dim)] + [0.0] * (3 - dim)
-    bsize = [(box_hi[d] - box_lo[d]) * dx[d] for d in range(dim)] + [1.0] * (3 - dim)
-    Xf = node_coordinates(dim, order, fe, boff, bsize)
-    return np.concatenate([Xc[~inbox], Xf], axis=0)
+    return nested_node_coordinates(dim, order, cells, [(box_lo, box_hi)], offset, size)
+
+
+def nested_node_coordinates(dim, order, cells, boxes, offset=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0)):
+    """(ncells, b^dim, dim) node coordinates of a mesh made by
+    exa_mesh_create_nested: level by level, the unrefined cells of the
+    level's region (x fastest). boxes[k] = (lo, hi) in level-k cell
+    coordinates."""
+    out = []
+    r0, r1 = [0] * dim, list(cells[:dim])
+    for lev in range(len(boxes) + 1):
+        f = 3 ** lev
+        dx = [size[d] / (cells[d] * f) for d in range(dim)]
+        ext = [r1[d] - r0[d] for d in range(dim)]
+        off = [offset[d] + r0[d] * dx[d] for d in range(dim)] + [0.0] * (3 - dim)
+        sz = [ext[d] * dx[d] for d in range(dim)] + [1.0] * (3 - dim)
+        X = node_coordinates(dim, order, ext, off, sz)
+        if lev < len(boxes):
+            lo, hi = boxes[lev]
+            idx = np.indices(tuple(reversed(ext))).reshape(dim, -1)[::-1]  # (dim, ncells), x first
+            inbox = np.ones(idx.shape[1], dtype=bool)
+            for d in range(dim):
+                inbox &= (idx[d] + r0[d] >= lo[d]) & (idx[d] + r0[d] < hi[d])
+            X = X[~inbox]
+            r0, r1 = [3 * lo[d] for d in range(dim)], [3 * hi[d] for d in range(dim)]
+        out.append(X)
+    return np.concatenate(out, axis=0)
 
 
 def pulse_refined(dim, order, cells, box_lo, box_hi, seed=0):
@@ -212,10 +228,17 @@ def pulse_refined(dim, order, cells, box_lo, box_hi, seed=0):
     refined box plus a seeded offset U[-0.05, 0.05]^dim, carried by the
     velocity (1, 0.5, 0.25) through the box's faces; p = 1; periodic unit
     domain. Returns luh in the refined mesh's cell order."""
+    return pulse_nested(dim, order, cells, [(box_lo, box_hi)], seed)
+
+
+def pulse_nested(dim, order, cells, boxes, seed=0):
+    """pulse_refined on a nested mesh (centre: the first box's centre plus a
+    seeded offset U[-0.05, 0.05]^dim)."""
     rng = np.random.default_rng(seed)
+    box_lo, box_hi = boxes[0]
     c = np.array([(box_lo[d] + box_hi[d]) / (2.0 * cells[d]) for d in range(dim)])
     c = c + rng.uniform(-0.05, 0.05, size=dim)
-    X = refined_node_coordinates(dim, order, cells, box_lo, box_hi)
+    X = nested_node_coordinates(dim, order, cells, boxes)
     rho = 1.0 + 0.3 * np.exp(-_periodic_d2(X, c) / 0.01)
     vel = np.zeros(rho.shape + (3,))
     vel[..., :dim] = np.array([1.0, 0.5, 0.25][:dim])

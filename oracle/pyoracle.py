@@ -317,66 +317,77 @@ class RefinedMesh:
     Cell order: the unrefined coarse cells (x fastest), then the box's fine
     cells (x fastest)."""
 
-    def __init__(self, dim, order, cells, size, box_lo, box_hi, pde=0, impl="oracle"):
+    def __init__(self, dim, order, cells, size, box_lo=None, box_hi=None, pde=0, impl="oracle", boxes=None):
+        """boxes: nested refined boxes, boxes[k] = (lo, hi) in level-k cell
+        coordinates (level k+1 is box k refined once); box_lo/box_hi: one box."""
         self.dim, self.order, self.pde = dim, order, pde
         self.linear = pde == 2
         self.K = Kernels(dim, order, pde, impl)
         self.impl = impl
         d = dim
         cells = list(cells)[:d]
-        lo, hi = list(box_lo)[:d], list(box_hi)[:d]
-        self.dx0 = [size[i] / cells[i] for i in range(d)]
-        self.dx1 = [x / 3.0 for x in self.dx0]
-        fe = [3 * (hi[i] - lo[i]) for i in range(d)]
-        inbox = lambda c: all(lo[i] <= c[i] < hi[i] for i in range(d))  # noqa: E731
-        onface = lambda c: any(c[i] == lo[i] or c[i] == hi[i] - 1 for i in range(d))  # noqa: E731
-        rng = lambda ext: [tuple(reversed(t)) for t in np.ndindex(*reversed(ext))]  # noqa: E731  x fastest
-        coarse = rng(cells)
-        self.cid = {}
-        for c in coarse:
-            if not inbox(c):
-                self.cid[c] = len(self.cid)
-        n0 = len(self.cid)
-        fine = rng(fe)
-        self.fid = {f: n0 + i for i, f in enumerate(fine)}
-        self.ncells = n0 + len(fine)
-        self.level = [0] * n0 + [1] * len(fine)
-        self.aid = {}
-        for c in coarse:
-            if inbox(c) and onface(c):
-                self.aid[c] = self.ncells + len(self.aid)
-        nslot = self.ncells + len(self.aid)
+        boxes = [(list(lo)[:d], list(hi)[:d]) for lo, hi in (boxes if boxes is not None else [(box_lo, box_hi)])]
+        L = len(boxes) + 1
+        self.dxl = [[size[i] / cells[i] for i in range(d)]]  # a child's width: its parent's / 3
+        for lev in range(1, L):
+            self.dxl.append([x / 3.0 for x in self.dxl[-1]])
+        r0, r1 = [[0] * d], [list(cells)]
+        for lo, hi in boxes:
+            r0.append([3 * x for x in lo])
+            r1.append([3 * x for x in hi])
+        refined = lambda lev, c: lev + 1 < L and all(boxes[lev][0][i] <= c[i] < boxes[lev][1][i] for i in range(d))  # noqa: E731
+        onface = lambda lev, c: any(c[i] == boxes[lev][0][i] or c[i] == boxes[lev][1][i] - 1 for i in range(d))  # noqa: E731
+        # positions of a level's region, x fastest
+        region = lambda lev: [tuple(r0[lev][i] + t[d - 1 - i] for i in range(d))  # noqa: E731
+                              for t in np.ndindex(*[r1[lev][i] - r0[lev][i] for i in reversed(range(d))])]
+        self.cid = [dict() for _ in range(L)]
+        self.level = []
+        n = 0
+        for lev in range(L):
+            for c in region(lev):
+                if not refined(lev, c):
+                    self.cid[lev][c] = n
+                    self.level.append(lev)
+                    n += 1
+        self.ncells = n
+        self.aid = [dict() for _ in range(L)]
+        for lev in range(L - 1):
+            for c in region(lev):
+                if refined(lev, c) and onface(lev, c):
+                    self.aid[lev][c] = n
+                    n += 1
         self.pairs, self.restr, self.prol = [], [], []
-        for c in coarse:
-            for i in range(d):
-                nb = list(c)
-                nb[i] = (c[i] + 1) % cells[i]
-                nb = tuple(nb)
-                a, b = inbox(c), inbox(nb)
-                if a and b:
-                    continue
-                self.pairs.append((self.aid[c] if a else self.cid[c], self.aid[nb] if b else self.cid[nb], i))
-        for f in fine:
-            me = self.fid[f]
-            parent = tuple(lo[i] + f[i] // 3 for i in range(d))
-            for i in range(d):
-                if f[i] + 1 < fe[i]:
-                    nb = list(f)
-                    nb[i] += 1
-                    self.pairs.append((me, self.fid[tuple(nb)], i))
-                sub = [f[e] % 3 for e in range(d) if e != i]
-                for side in (0, 1):
-                    if f[i] != (0 if side == 0 else fe[i] - 1):
+        for lev in range(L):
+            for c in region(lev):
+                rc = refined(lev, c)
+                me = self.aid[lev].get(c, -1) if rc else self.cid[lev][c]  # -1: refined, inside its box
+                for i in range(d):
+                    q = list(c)
+                    q[i] += 1
+                    if lev == 0:
+                        q[i] %= cells[i]
+                    q = tuple(q)
+                    if q[i] < r1[lev][i]:
+                        rq = refined(lev, q)
+                        if not (rc and rq):
+                            self.pairs.append((me, self.aid[lev][q] if rq else self.cid[lev][q], i))
+                    if lev == 0 or rc:
                         continue
-                    face = 2 * i + side
-                    desc = nslot
-                    nslot += 1
-                    self.pairs.append((desc, me, i) if side == 0 else (me, desc, i))
-                    self.restr.append((me, face, self.aid[parent], face, sub))
-                    cn = list(parent)
-                    cn[i] += -1 if side == 0 else 1
-                    dface = 2 * i + 1 if side == 0 else 2 * i
-                    self.prol.append((self.cid[tuple(cn)], dface, desc, dface, sub))
+                    sub = [c[e] % 3 for e in range(d) if e != i]
+                    parent = tuple(x // 3 for x in c)
+                    for side in (0, 1):
+                        if c[i] != (r0[lev][i] if side == 0 else r1[lev][i] - 1):
+                            continue
+                        face = 2 * i + side
+                        desc = n
+                        n += 1
+                        self.pairs.append((desc, me, i) if side == 0 else (me, desc, i))
+                        self.restr.append((me, face, self.aid[lev - 1][parent], face, sub))
+                        cn = list(parent)
+                        cn[i] += -1 if side == 0 else 1
+                        dface = 2 * i + 1 if side == 0 else 2 * i
+                        self.prol.append((self.cid[lev - 1][tuple(cn)], dface, desc, dface, sub))
+        nslot = n
         K = self.K
         self.nslot = nslot
         self.Q = np.zeros((nslot, 2 * d, K.F * K.ndata))
@@ -386,7 +397,7 @@ class RefinedMesh:
         self.t, self.dt, self.steps, self.sweeps = 0.0, 0.0, 0, 0
 
     def _dx(self, c):
-        return self.dx1 if self.level[c] else self.dx0
+        return self.dxl[self.level[c]]
 
     def set_solution(self, u):
         self.u = np.array(u, dtype=np.float64).reshape(self.u.shape)

@@ -81,6 +81,52 @@ def test_refined_elastic_mesh_vs_oracle(eb, dim, N, cells, lo, hi, steps):
     assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"]
 
 
+NESTED = [(2, 3, (9, 9), [((3, 3), (6, 6)), ((10, 10), (17, 17))], 8, 0),
+          (2, 5, (9, 9), [((3, 3), (6, 6)), ((10, 11), (15, 17)), ((31, 34), (44, 50))], 4, 3),
+          (3, 3, (4, 4, 4), [((1, 1, 1), (3, 3, 3)), ((4, 4, 4), (5, 5, 5))], 3, 2)]
+
+
+@pytest.mark.parametrize("dim,N,cells,boxes,steps,variant", NESTED)
+def test_nested_mesh_vs_oracle(eb, dim, N, cells, boxes, steps, variant):
+    """nested refined boxes (three and four levels): every level's hanging
+    faces through its own ancestors and descendants"""
+    from exahype_b200 import problems
+    u = problems.pulse_nested(dim, N, cells, boxes, seed=6)
+    s = eb.Solver(dim, N)
+    s.variant = variant
+    m = eb.Mesh.nested(s, cells, [0.0] * dim, [1.0] * dim, boxes)
+    o = pyoracle.RefinedMesh(dim, N, cells, [1.0] * dim, boxes=boxes)
+    assert m.ncells == o.ncells == u.shape[0]
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init(0.0)
+    o.init(0.0)
+    assert m.state()["dt"] == o.state()["dt"]
+    m.step(steps)
+    o.step(steps)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    sa, sb = m.state(), o.state()
+    assert sa["steps"] == sb["steps"] == steps
+    assert sa["picard_sweeps"] == sb["picard_sweeps"]
+    assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"]
+
+
+def test_nested_mesh_free_stream_and_arguments(eb):
+    s = eb.Solver(2, 3)
+    boxes = [((3, 3), (6, 6)), ((10, 10), (17, 17))]
+    m = eb.Mesh.nested(s, (9, 9), [0.0, 0.0], [1.0, 1.0], boxes)
+    u = np.zeros(m.solution_shape)
+    u[..., 0], u[..., 1], u[..., 2], u[..., 4] = 1.0, 0.4, -0.2, 2.5
+    m.set_solution(u)
+    m.init(0.0)
+    m.step(10)
+    assert np.abs(m.get_solution() - u).max() < 1e-10
+    for bad in ([((3, 3), (6, 6)), ((9, 10), (17, 17))], [((3, 3), (6, 6)), ((10, 10), (18, 17))]):
+        with pytest.raises(eb.ExaError):  # the inner box touches its level's region
+            eb.Mesh.nested(s, (9, 9), [0.0, 0.0], [1.0, 1.0], bad)
+
+
 def test_refined_mesh_free_stream(eb):
     s = eb.Solver(2, 5)
     m = eb.Mesh.refined(s, (9, 9), [0.0, 0.0], [1.0, 1.0], (3, 3), (6, 6))

@@ -44,6 +44,24 @@ def test_refined_oracle_elastic_vs_reference_kernels():
     assert np.linalg.norm(res[0] - res[1]) / np.linalg.norm(res[1]) < 1e-12
 
 
+def test_nested_oracle_vs_reference_kernels():
+    if not pyoracle.ref_available(2):
+        pytest.skip("compiled reference kernels not built")
+    from exahype_b200 import problems
+    cells, boxes = (9, 9), [((3, 3), (6, 6)), ((10, 10), (17, 17))]
+    u = problems.pulse_nested(2, 3, cells, boxes, seed=6)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.RefinedMesh(2, 3, cells, [1.0, 1.0], boxes=boxes, impl=impl)
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(3)
+        res.append((m.get_solution(), m.state()))
+    (a, sa), (b, sb) = res
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    assert sa["picard_sweeps"] == sb["picard_sweeps"]
+
+
 def test_refined_oracle_free_stream():
     m = pyoracle.RefinedMesh(2, 3, (9, 9), [1.0, 1.0], (3, 3), (6, 6))
     u = np.zeros((m.ncells, 16, 5))
