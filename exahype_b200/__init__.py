@@ -278,12 +278,13 @@ class Mesh:
         return cls.nested(solver, cells, offset, size, [(box_lo, box_hi)])
 
     @classmethod
-    def nested(cls, solver, cells, offset, size, boxes):
+    def nested(cls, solver, cells, offset, size, boxes, bc=BC_PERIODIC):
         """Periodic mesh with nested refined boxes (exa_mesh_create_nested):
         boxes[k] = (lo, hi) in the cell coordinates of level k (level 0 the
         coarse grid; level k+1 box k refined once, coordinates over the whole
-        domain at that level). Solution order: the unrefined cells of each
-        level in turn, x fastest."""
+        domain at that level). bc: periodic or outflow, per domain face or
+        one for all. Solution order: the unrefined cells of each level in
+        turn, x fastest."""
         lib = load()
         d = solver.dim
         self = cls.__new__(cls)
@@ -295,7 +296,11 @@ class Mesh:
         lo = (ctypes.c_int * (3 * nb))(*sum((list(b[0]) + [0] * (3 - len(b[0])) for b in boxes), []))
         hi = (ctypes.c_int * (3 * nb))(*sum((list(b[1]) + [1] * (3 - len(b[1])) for b in boxes), []))
         h = ctypes.c_void_p()
-        _check(lib.exa_mesh_create_nested(solver._h, c, o, s, nb, lo, hi, ctypes.byref(h)), "exa_mesh_create_nested")
+        if isinstance(bc, int):
+            bc = [bc] * (2 * d)
+        bcs = (ctypes.c_int * 6)(*(list(bc) + [BC_PERIODIC] * (6 - len(bc))))
+        _check(lib.exa_mesh_create_nested(solver._h, c, o, s, bcs, nb, lo, hi, ctypes.byref(h)),
+               "exa_mesh_create_nested")
         self._h = h
         self.solver = solver
         self.cells = tuple(cells)

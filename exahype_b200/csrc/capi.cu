@@ -948,11 +948,13 @@ struct NestedTopo {
   int dim = 0, L = 1, ncells = 0, anc0 = 0, nanc = 0, nslots = 0;
   std::vector<int> level;                              // per cell
   std::vector<int> fl, fr, fd;                          // Riemann pairs
+  std::vector<int> bcell, bface;                        // outflow faces of level-0 cells
   std::vector<int> rf, rc, ridx, pf, pc, pidx;          // restriction / prolongation items
 };
 
 // returns an error message, or nullptr
-static const char* nested_topology(int dim, const int* cells, int nb, const int* lo, const int* hi, NestedTopo& t) {
+static const char* nested_topology(int dim, const int* cells, int nb, const int* lo, const int* hi, const int* bc,
+                                   NestedTopo& t) {
   const int L = nb + 1, D2 = 2 * dim;
   t.dim = dim;
   t.L = L;
@@ -1025,8 +1027,13 @@ static const char* nested_topology(int dim, const int* cells, int nb, const int*
       for (int d = 0; d < dim; d++) {
         int q[3] = {p[0], p[1], p[2]};
         q[d] = p[d] + 1;
-        if (l == 0) q[d] %= cells[d];  // periodic coarse grid
-        if (q[d] < r1[l][d]) {         // same-level neighbour: skip refined pairs
+        if (l == 0 && bc[2 * d] != EXA_BC_PERIODIC) {  // outflow domain faces (never refined: margin)
+          if (p[d] == 0) t.bcell.push_back(me), t.bface.push_back(2 * d);
+          if (q[d] == cells[d]) t.bcell.push_back(me), t.bface.push_back(2 * d + 1);
+        } else if (l == 0) {
+          q[d] %= cells[d];  // periodic coarse grid
+        }
+        if (q[d] < r1[l][d]) {  // same-level neighbour: skip refined pairs
           const bool rq = refined(l, q);
           if (!(rp && rq)) {
             t.fl.push_back(me);
@@ -1067,7 +1074,7 @@ static const char* nested_topology(int dim, const int* cells, int nb, const int*
 }  // namespace
 
 int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* offset, const double* size,
-                           int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out) {
+                           const int* bc, int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out) {
   if (!s || !cells || !offset || !size || !box_lo || !box_hi || !out)
     return fail(EXA_ERR_ARG, "exa_mesh_create_nested: null argument");
   if (nboxes < 1 || nboxes > 8) return fail(EXA_ERR_ARG, "exa_mesh_create_nested: 1 to 8 refined boxes");
@@ -1082,9 +1089,18 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
     m->geo.dx[d] = size[d] / cells[d];
   }
   for (int d = dim; d < 3; d++) m->geo.dx[d] = 1.0;
-  for (int f = 0; f < 6; f++) m->bc[f] = EXA_BC_PERIODIC;
+  for (int f = 0; f < 6; f++) {
+    const int k = bc && f < 2 * dim ? bc[f] : EXA_BC_PERIODIC;
+    if (k != EXA_BC_PERIODIC && k != EXA_BC_OUTFLOW)
+      return fail(EXA_ERR_ARG, "exa_mesh_create_nested: boundaries must be periodic or outflow");
+    if (f % 2 == 1 && (k == EXA_BC_PERIODIC) != (m->bc[f - 1] == EXA_BC_PERIODIC))
+      return fail(EXA_ERR_ARG, "exa_mesh_create_nested: periodic must be set on both faces of an axis");
+    if (k != EXA_BC_PERIODIC && s->k.linear)
+      return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create_nested: the linear kernels support periodic meshes only");
+    m->bc[f] = k;
+  }
   NestedTopo t;
-  if (const char* err = nested_topology(dim, cells, nboxes, box_lo, box_hi, t))
+  if (const char* err = nested_topology(dim, cells, nboxes, box_lo, box_hi, m->bc, t))
     return fail(EXA_ERR_ARG, std::string("exa_mesh_create_nested: ") + err);
   const int L = t.L;
   m->ncells = t.ncells;
@@ -1110,8 +1126,8 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
   bool ok = salloc(&m->luh, n * P * nD * 8, st) && salloc(&m->lduh, n * P * nV * 8, st) &&
             salloc(&m->lQhbnd, ns * D2 * F * nD * 8, st) && salloc(&m->lFhbnd, ns * D2 * F * nV * 8, st) &&
             salloc(&m->scal, 8 * 8, st) && ia(&m->iters, n) && ia(&m->fl, t.fl.size()) && ia(&m->fr, t.fl.size()) &&
-            ia(&m->fd, t.fl.size()) && ia(&m->bcell, 0) && ia(&m->bface, 0) && salloc(&m->sweeps, 8, st) &&
-            salloc(&m->ref.lv, 2 * (size_t)L * 8, st) && ia(&m->ref.inst, n) &&
+            ia(&m->fd, t.fl.size()) && ia(&m->bcell, t.bcell.size()) && ia(&m->bface, t.bcell.size()) &&
+            salloc(&m->sweeps, 8, st) && salloc(&m->ref.lv, 2 * (size_t)L * 8, st) && ia(&m->ref.inst, n) &&
             salloc(&m->ref.inst_dx, ldx.size() * 8, st) && ia(&m->ref.res_f, t.rf.size()) &&
             ia(&m->ref.res_c, t.rf.size()) && ia(&m->ref.res_ld, t.rf.size()) && ia(&m->ref.res_idx, t.ridx.size()) &&
             ia(&m->ref.pro_f, t.pf.size()) && ia(&m->ref.pro_c, t.pf.size()) && ia(&m->ref.pro_ld, t.pf.size()) &&
@@ -1130,12 +1146,15 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
        up(m->ref.res_c, t.rc.data(), t.rc.size() * 4) && up(m->ref.res_ld, ones.data(), t.rf.size() * 4) &&
        up(m->ref.res_idx, t.ridx.data(), t.ridx.size() * 4) && up(m->ref.pro_f, t.pf.data(), t.pf.size() * 4) &&
        up(m->ref.pro_c, t.pc.data(), t.pc.size() * 4) && up(m->ref.pro_ld, ones.data(), t.pf.size() * 4) &&
-       up(m->ref.pro_idx, t.pidx.data(), t.pidx.size() * 4);
+       up(m->ref.pro_idx, t.pidx.data(), t.pidx.size() * 4) && up(m->bcell, t.bcell.data(), t.bcell.size() * 4) &&
+       up(m->bface, t.bface.data(), t.bface.size() * 4);
   if (!ok) {
     cudaStreamSynchronize(st);
     mesh_free(m.get());
     return fail(EXA_ERR_CUDA, "exa_mesh_create_nested: upload failed");
   }
+  m->boff[EXA_BC_OUTFLOW] = 0;
+  m->nbfaces[EXA_BC_OUTFLOW] = (int)t.bcell.size();
   m->geo.inst = m->ref.inst;
   m->geo.inst_dx = m->ref.inst_dx;
   EXA_CUDA(cudaMemsetAsync(m->luh, 0, n * P * nD * 8, st));
@@ -1150,7 +1169,7 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
 
 int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
                             const int* box_lo, const int* box_hi, exa_mesh** out) {
-  return exa_mesh_create_nested(s, cells, offset, size, 1, box_lo, box_hi, out);
+  return exa_mesh_create_nested(s, cells, offset, size, nullptr, 1, box_lo, box_hi, out);
 }
 
 int exa_mesh_destroy(exa_mesh* m) {

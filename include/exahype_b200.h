@@ -201,7 +201,9 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
  * (solveRiemannProblemAtInterface, :2789). */
 int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
                             const int* box_lo, const int* box_hi, exa_mesh** out);
-/* The same with nboxes nested refined boxes (1..8): box k (box_lo/box_hi
+/* The same with nboxes nested refined boxes (1..8) and optional domain
+ * boundaries bc[2d] (NULL: periodic; EXA_BC_PERIODIC or EXA_BC_OUTFLOW per
+ * axis, outflow for nonlinear PDEs only): box k (box_lo/box_hi
  * [3k .. 3k+2]) is given in the cell coordinates of level k (level 0 the
  * coarse grid, level k+1 the box k refined once, whose coordinates run over
  * the whole domain at that level: 3^(k+1) cells[d]) and must lie inside
@@ -209,7 +211,7 @@ int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double*
  * the unrefined cells of level 0, then of level 1, ..., each x fastest over
  * its region. exa_mesh_create_refined is the case nboxes = 1. */
 int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* offset, const double* size,
-                           int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out);
+                           const int* bc, int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out);
 int exa_mesh_destroy(exa_mesh* m);
 int exa_mesh_num_cells(const exa_mesh* m, int* ncells);
 /* host <-> device solution, luh layout above, cells in x-fastest order */

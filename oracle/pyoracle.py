@@ -317,9 +317,12 @@ class RefinedMesh:
     Cell order: the unrefined coarse cells (x fastest), then the box's fine
     cells (x fastest)."""
 
-    def __init__(self, dim, order, cells, size, box_lo=None, box_hi=None, pde=0, impl="oracle", boxes=None):
+    def __init__(self, dim, order, cells, size, box_lo=None, box_hi=None, pde=0, impl="oracle", boxes=None, bc=-1):
         """boxes: nested refined boxes, boxes[k] = (lo, hi) in level-k cell
-        coordinates (level k+1 is box k refined once); box_lo/box_hi: one box."""
+        coordinates (level k+1 is box k refined once); box_lo/box_hi: one box.
+        bc: -1 periodic or 0 outflow, one for all or per domain face
+        (boundaryConditions with outflow values on the level-0 cells'
+        domain faces, ADERDGSolver.cpp:2893-2976)."""
         self.dim, self.order, self.pde = dim, order, pde
         self.linear = pde == 2
         self.K = Kernels(dim, order, pde, impl)
@@ -356,7 +359,8 @@ class RefinedMesh:
                 if refined(lev, c) and onface(lev, c):
                     self.aid[lev][c] = n
                     n += 1
-        self.pairs, self.restr, self.prol = [], [], []
+        bcs = [bc] * (2 * d) if isinstance(bc, int) else list(bc)
+        self.pairs, self.restr, self.prol, self.bnd = [], [], [], []
         for lev in range(L):
             for c in region(lev):
                 rc = refined(lev, c)
@@ -364,7 +368,12 @@ class RefinedMesh:
                 for i in range(d):
                     q = list(c)
                     q[i] += 1
-                    if lev == 0:
+                    if lev == 0 and bcs[2 * i] != -1:
+                        if c[i] == 0:
+                            self.bnd.append((me, 2 * i))
+                        if q[i] == cells[i]:
+                            self.bnd.append((me, 2 * i + 1))
+                    elif lev == 0:
                         q[i] %= cells[i]
                     q = tuple(q)
                     if q[i] < r1[lev][i]:
@@ -447,6 +456,8 @@ class RefinedMesh:
                     fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1],
                                        self.Q[r, 2 * i], i)
                 self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i] = fl, fr
+            for c, face in self.bnd:
+                self.Fb[c, face] = K.boundary_face(self.Fb[c, face], self.Q[c, face], face)
             for c in range(self.ncells):
                 si = K.lin_surface_integral if self.linear else K.surface_integral
                 du = si(self.du[c], self.Fb[c].reshape(-1), self._dx(c))

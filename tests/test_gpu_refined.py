@@ -112,6 +112,29 @@ def test_nested_mesh_vs_oracle(eb, dim, N, cells, boxes, steps, variant):
     assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"]
 
 
+def test_nested_mesh_outflow_vs_oracle(eb):
+    """outflow domain faces on the coarse level (their boundary Riemann
+    problems with the outflow state run every step)"""
+    from exahype_b200 import problems
+    cells, boxes = (9, 9), [((3, 3), (6, 6)), ((10, 10), (17, 17))]
+    u = problems.pulse_nested(2, 3, cells, boxes, seed=6)
+    s = eb.Solver(2, 3)
+    m = eb.Mesh.nested(s, cells, [0.0, 0.0], [1.0, 1.0], boxes, bc=eb.BC_OUTFLOW)
+    o = pyoracle.RefinedMesh(2, 3, cells, [1.0, 1.0], boxes=boxes, bc=0)
+    assert len(o.bnd) == 4 * 9
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init(0.0)
+    o.init(0.0)
+    m.step(10)
+    o.step(10)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    assert m.state()["picard_sweeps"] == o.state()["picard_sweeps"]
+    with pytest.raises(eb.ExaError):  # periodic on one face of an axis only
+        eb.Mesh.nested(s, cells, [0.0, 0.0], [1.0, 1.0], boxes, bc=[-1, 0, 0, 0])
+
+
 def test_nested_mesh_free_stream_and_arguments(eb):
     s = eb.Solver(2, 3)
     boxes = [((3, 3), (6, 6)), ((10, 10), (17, 17))]
