@@ -369,6 +369,12 @@ class Mesh:
         the reference's ADERDG2CartesianVTK vertex plotter)"""
         _check(load().exa_mesh_write_vtk(self._h, os.fsencode(path), int(bool(binary))), "exa_mesh_write_vtk")
 
+    def write_vtk_legendre(self, path, binary=False):
+        """legacy VTK unstructured grid of the nodal values at the
+        Gauss-Legendre nodes (the reference's ADERDG2LegendreVTK vertex plotter)"""
+        _check(load().exa_mesh_write_vtk_legendre(self._h, os.fsencode(path), int(bool(binary))),
+               "exa_mesh_write_vtk_legendre")
+
     def synchronize(self):
         _check(load().exa_mesh_synchronize(self._h), "exa_mesh_synchronize")
 

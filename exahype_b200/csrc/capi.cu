@@ -1621,41 +1621,50 @@ struct VtkOut {
 
 extern "C" {
 
-int exa_mesh_write_vtk(exa_mesh* m, const char* path, int binary) {
-  if (!m || !path) return fail(EXA_ERR_ARG, "exa_mesh_write_vtk: null argument");
-  if (m->ref.on) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_write_vtk: uniform meshes only");
+// legendre == 0: ADERDG2CartesianVTK (the solution projected to the (N+1)^d
+// equidistant vertices of every cell); legendre != 0: ADERDG2LegendreVTK
+// (exahype/plotters/VTK/ADERDG2LegendreVTK.cpp:280-380: the nodal values at
+// the Gauss-Legendre nodes, offset + (cell + x_i) dx, no projection). Both
+// connect the (N+1)^d points of a cell by N^d pixels / voxels.
+static int mesh_write_vtk(exa_mesh* m, const char* path, int binary, int legendre, const char* fn) {
+  if (!m || !path) return fail(EXA_ERR_ARG, std::string(fn) + ": null argument");
+  if (m->ref.on) return fail(EXA_ERR_UNSUPPORTED, std::string(fn) + ": uniform meshes only");
   const KernelSet& k = m->s->k;
   const int dim = m->dim, N = k.order, b = N + 1, nD = k.nvar + k.npar;
   const size_t n = m->ncells, P = k.P, sub = dim == 3 ? (size_t)N * N * N : (size_t)N * N;
   double* dev = nullptr;
-  if (!salloc(&dev, n * P * nD * 8, m->stream)) {
+  if (!legendre && !salloc(&dev, n * P * nD * 8, m->stream)) {
     cudaGetLastError();
-    return fail(EXA_ERR_NOMEM, "exa_mesh_write_vtk: device allocation failed");
+    return fail(EXA_ERR_NOMEM, std::string(fn) + ": device allocation failed");
   }
   std::vector<double> v(n * P * nD);
   double t = 0.0;
-  int rc = k.plot(m->luh, dev, (int)n, m->stream);
-  if (!rc && cudaMemcpyAsync(v.data(), dev, v.size() * 8, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess)
-    rc = fail(EXA_ERR_CUDA, "exa_mesh_write_vtk: copy failed");
+  int rc = legendre ? EXA_OK : k.plot(m->luh, dev, (int)n, m->stream);
+  if (!rc && cudaMemcpyAsync(v.data(), legendre ? m->luh : dev, v.size() * 8, cudaMemcpyDeviceToHost, m->stream) !=
+                 cudaSuccess)
+    rc = fail(EXA_ERR_CUDA, std::string(fn) + ": copy failed");
   if (!rc && cudaMemcpyAsync(&t, m->scal + 2, 8, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess)
-    rc = fail(EXA_ERR_CUDA, "exa_mesh_write_vtk: copy failed");
-  sfree(dev, m->stream);
+    rc = fail(EXA_ERR_CUDA, std::string(fn) + ": copy failed");
+  if (dev) sfree(dev, m->stream);
   if (rc) return rc;
   EXA_CUDA(cudaStreamSynchronize(m->stream));
   FILE* f = std::fopen(path, binary ? "wb" : "w");
-  if (!f) return fail(EXA_ERR_ARG, std::string("exa_mesh_write_vtk: cannot open ") + path);
+  if (!f) return fail(EXA_ERR_ARG, std::string(fn) + ": cannot open " + path);
   VtkOut o{f, binary != 0};
   std::fprintf(f, "# vtk DataFile Version 3.0\nexahype_b200 ADER-DG solution t=%.17g\n%s\nDATASET UNSTRUCTURED_GRID\n",
                t, binary ? "BINARY" : "ASCII");
-  // every cell is a patch of b^d vertices at offset + (cell + i/N) dx, x fastest
+  // every cell is a patch of b^d vertices at offset + (cell + xi) dx, x
+  // fastest, xi = i/N (equidistant) or the i-th Gauss-Legendre node
+  double xi[16];
+  for (int i = 0; i < b; i++) xi[i] = legendre ? exa_tab_nodes[exa_tab_nodes_off[N] + i] : (double)i / N;
   std::fprintf(f, "POINTS %zu double\n", n * P);
   for (size_t c = 0; c < n; c++) {
     const size_t cx = c % m->cells[0], cy = (c / m->cells[0]) % m->cells[1], cz = c / ((size_t)m->cells[0] * m->cells[1]);
     for (size_t p = 0; p < P; p++) {
       const int ix = (int)(p % b), iy = (int)((p / b) % b), iz = dim == 3 ? (int)(p / (b * b)) : 0;
-      o.num(m->offset[0] + (cx + (double)ix / N) * m->geo.dx[0], " ");
-      o.num(m->offset[1] + (cy + (double)iy / N) * m->geo.dx[1], " ");
-      o.num(dim == 3 ? m->offset[2] + (cz + (double)iz / N) * m->geo.dx[2] : 0.0, "\n");
+      o.num(m->offset[0] + (cx + xi[ix]) * m->geo.dx[0], " ");
+      o.num(m->offset[1] + (cy + xi[iy]) * m->geo.dx[1], " ");
+      o.num(dim == 3 ? m->offset[2] + (cz + xi[iz]) * m->geo.dx[2] : 0.0, "\n");
     }
   }
   o.eol();
@@ -1686,8 +1695,16 @@ int exa_mesh_write_vtk(exa_mesh* m, const char* path, int binary) {
   o.eol();
   const bool ok = std::ferror(f) == 0;
   std::fclose(f);
-  if (!ok) return fail(EXA_ERR_ARG, std::string("exa_mesh_write_vtk: write error on ") + path);
+  if (!ok) return fail(EXA_ERR_ARG, std::string(fn) + ": write error on " + path);
   return EXA_OK;
+}
+
+int exa_mesh_write_vtk(exa_mesh* m, const char* path, int binary) {
+  return mesh_write_vtk(m, path, binary, 0, "exa_mesh_write_vtk");
+}
+
+int exa_mesh_write_vtk_legendre(exa_mesh* m, const char* path, int binary) {
+  return mesh_write_vtk(m, path, binary, 1, "exa_mesh_write_vtk_legendre");
 }
 
 }  // extern "C"

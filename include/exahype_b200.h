@@ -263,6 +263,11 @@ int exa_mesh_synchronize(exa_mesh* m);
  * exa_plot_vertices) and "time" -- the layout of the reference's
  * ADERDG2CartesianVTK vertex plotter. Synchronises the mesh's stream. */
 int exa_mesh_write_vtk(exa_mesh* m, const char* path, int binary);
+/* The same layout with the points at every cell's Gauss-Legendre nodes and
+ * the nodal values as they are (no projection) -- the reference's
+ * ADERDG2LegendreVTK vertex plotter
+ * (exahype/plotters/VTK/ADERDG2LegendreVTK.cpp:280-380). */
+int exa_mesh_write_vtk_legendre(exa_mesh* m, const char* path, int binary);
 /* Moves the mesh's work to a new stream of stream priority `level` (0: the
  * default, least urgent; each level up is more urgent, capped at the device's
  * range): where several streams' kernels wait for SMs, the higher priority's

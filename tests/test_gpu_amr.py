@@ -220,3 +220,28 @@ def test_write_vtk(eb, tmp_path, dim, N, cells):
     assert np.array_equal(res[0]["cells"], res[1]["cells"])
     assert np.array_equal(res[0]["points"], res[1]["points"])  # text uses 17 digits: round-trips exactly
     assert np.array_equal(res[0]["Q"], res[1]["Q"])
+
+
+@pytest.mark.parametrize("dim,N,cells", [(2, 3, (4, 5)), (3, 5, (2, 3, 2))])
+def test_write_vtk_legendre(eb, tmp_path, dim, N, cells):
+    """ADERDG2LegendreVTK layout: the points are every cell's Gauss-Legendre
+    nodes and the values the nodal solution itself, text and binary alike"""
+    from exahype_b200 import problems
+    s = eb.Solver(dim, N, eb.PDE_EULER)
+    m = eb.Mesh(s, cells, [0.5] * dim, [1.5] * dim, eb.BC_PERIODIC)
+    u = problems.gaussian_pulse_2d(N, cells, seed=1)[0] if dim == 2 else problems.gaussian_pulses_3d(N, cells, seed=1)[0]
+    m.set_solution(u)
+    m.init(0.0)
+    m.step(2)
+    sol = m.get_solution()
+    X = problems.node_coordinates(dim, N, cells, offset=(0.5, 0.5, 0.5), size=(1.5, 1.5, 1.5)).reshape(-1, dim)
+    res = []
+    for binary in (False, True):
+        path = str(tmp_path / ("l%d.vtk" % binary))
+        m.write_vtk_legendre(path, binary=binary)
+        v = read_vtk(path)
+        assert np.array_equal(v["Q"], sol.reshape(-1, 5))
+        assert np.allclose(v["points"][:, :dim], X, rtol=0, atol=1e-14)
+        assert len(v["types"]) == int(np.prod(cells)) * N ** dim
+        res.append(v)
+    assert np.array_equal(res[0]["points"], res[1]["points"])
