@@ -498,6 +498,11 @@ class LimitingMesh:
                                       ctypes.byref(irr)), "exa_lmesh_state")
         return dict(t=t.value, dt=dt.value, steps=st.value, picard_sweeps=sw.value, irregular_steps=irr.value)
 
+    def write_vtk(self, path, binary=False):
+        """legacy VTK of the DG solution with the limiter status as vertex
+        data (the reference's LimitingADERDG2CartesianVTK vertex plotter)"""
+        _check(load().exa_lmesh_write_vtk(self._h, os.fsencode(path), int(bool(binary))), "exa_lmesh_write_vtk")
+
     def status(self):
         s = np.empty(self.ncells, dtype=np.int32)
         _check(load().exa_lmesh_get_status(self._h, s.ctypes.data_as(ctypes.c_void_p)), "exa_lmesh_get_status")

@@ -1626,7 +1626,8 @@ extern "C" {
 // (exahype/plotters/VTK/ADERDG2LegendreVTK.cpp:280-380: the nodal values at
 // the Gauss-Legendre nodes, offset + (cell + x_i) dx, no projection). Both
 // connect the (N+1)^d points of a cell by N^d pixels / voxels.
-static int mesh_write_vtk(exa_mesh* m, const char* path, int binary, int legendre, const char* fn) {
+static int mesh_write_vtk(exa_mesh* m, const char* path, int binary, int legendre, const char* fn,
+                          const int* status_dev = nullptr) {
   if (!m || !path) return fail(EXA_ERR_ARG, std::string(fn) + ": null argument");
   if (m->ref.on) return fail(EXA_ERR_UNSUPPORTED, std::string(fn) + ": uniform meshes only");
   const KernelSet& k = m->s->k;
@@ -1644,6 +1645,10 @@ static int mesh_write_vtk(exa_mesh* m, const char* path, int binary, int legendr
                  cudaSuccess)
     rc = fail(EXA_ERR_CUDA, std::string(fn) + ": copy failed");
   if (!rc && cudaMemcpyAsync(&t, m->scal + 2, 8, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess)
+    rc = fail(EXA_ERR_CUDA, std::string(fn) + ": copy failed");
+  std::vector<int> status(status_dev ? n : 0);
+  if (!rc && status_dev &&
+      cudaMemcpyAsync(status.data(), status_dev, n * 4, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess)
     rc = fail(EXA_ERR_CUDA, std::string(fn) + ": copy failed");
   if (dev) sfree(dev, m->stream);
   if (rc) return rc;
@@ -1693,6 +1698,11 @@ static int mesh_write_vtk(exa_mesh* m, const char* path, int binary, int legendr
   std::fprintf(f, "SCALARS time double 1\nLOOKUP_TABLE default\n");
   for (size_t i = 0; i < n * P; i++) o.num(t, "\n");
   o.eol();
+  if (status_dev) {  // LimitingADERDG2CartesianVTK's vertex "Limiter-Status" (the cell's status)
+    std::fprintf(f, "SCALARS Limiter-Status double 1\nLOOKUP_TABLE default\n");
+    for (size_t i = 0; i < n * P; i++) o.num((double)status[i / P], "\n");
+    o.eol();
+  }
   const bool ok = std::ferror(f) == 0;
   std::fclose(f);
   if (!ok) return fail(EXA_ERR_ARG, std::string(fn) + ": write error on " + path);
@@ -2229,6 +2239,11 @@ int exa_lmesh_set_solution(exa_lmesh* lm, const double* h) {
 int exa_lmesh_get_solution(exa_lmesh* lm, double* h) {
   if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_get_solution: null mesh");
   return exa_mesh_get_solution(lm->m, h);
+}
+
+int exa_lmesh_write_vtk(exa_lmesh* lm, const char* path, int binary) {
+  if (!lm) return fail(EXA_ERR_ARG, "exa_lmesh_write_vtk: null mesh");
+  return mesh_write_vtk(lm->m, path, binary, 0, "exa_lmesh_write_vtk", lm->s);
 }
 
 int exa_lmesh_set_fv_initial(exa_lmesh* lm, const double* h) {

@@ -350,6 +350,12 @@ int exa_lmesh_destroy(exa_lmesh* m);
 /* host <-> device DG solution (layout and cell order of exa_mesh) */
 int exa_lmesh_set_solution(exa_lmesh* m, const double* luh_host);
 int exa_lmesh_get_solution(exa_lmesh* m, double* luh_host);
+/* exa_mesh_write_vtk's layout for a limiting mesh (the DG solution, which
+ * the limiter keeps current in limited cells too) plus the vertex data
+ * "Limiter-Status" (each vertex its cell's status) -- the reference's
+ * LimitingADERDG2CartesianVTK vertex plotter
+ * (exahype/plotters/VTK/LimitingADERDG2CartesianVTK.cpp:251-300). */
+int exa_lmesh_write_vtk(exa_lmesh* lm, const char* path, int binary);
 /* Optional FV initial condition at the subcell centres, [cell][(2N+1)^d][5]
  * (the FV solver's adjustSolution at t = 0); limiter patches allocated at
  * initialisation start from it instead of from the DG projection. */

@@ -184,6 +184,10 @@ def read_vtk(path):
     header()
     header()
     out["time"] = values(npts, "d")
+    if pos < len(data):  # further vertex scalars (one value each)
+        name = header()[1]
+        header()
+        out[name] = values(npts, "d")
     return out
 
 
@@ -245,3 +249,27 @@ def test_write_vtk_legendre(eb, tmp_path, dim, N, cells):
         assert len(v["types"]) == int(np.prod(cells)) * N ** dim
         res.append(v)
     assert np.array_equal(res[0]["points"], res[1]["points"])
+
+
+def test_lmesh_write_vtk(eb, tmp_path):
+    """LimitingADERDG2CartesianVTK layout: the projected DG solution of a
+    limiting mesh and every vertex's cell limiter status"""
+    from exahype_b200 import problems
+    N, cells = 3, (10, 10)
+    s = eb.Solver(2, N, eb.PDE_EULER)
+    lu, fv, _ = problems.explosion(2, N, cells, seed=0)
+    g = eb.LimitingMesh(s, cells, [0.0, 0.0], [1.0, 1.0], eb.BC_OUTFLOW)
+    g.set_solution(lu)
+    g.set_fv_initial(fv)
+    g.init(0.0)
+    g.step(3)
+    sol, st = g.get_solution(), g.status()
+    assert (st > 0).any()
+    b, n = N + 1, cells[0] * cells[1]
+    ref_q = np.concatenate([pyoracle.plot_vertices(2, N, 5, sol[c]).reshape(-1, 5) for c in range(n)])
+    for binary in (False, True):
+        path = str(tmp_path / ("lm%d.vtk" % binary))
+        g.write_vtk(path, binary=binary)
+        v = read_vtk(path)
+        assert rel(v["Q"], ref_q) < RTOL
+        assert np.array_equal(v["Limiter-Status"], np.repeat(st, b * b).astype(np.float64))
