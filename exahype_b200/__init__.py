@@ -369,6 +369,13 @@ class Mesh:
         the reference's ADERDG2CartesianVTK vertex plotter)"""
         _check(load().exa_mesh_write_vtk(self._h, os.fsencode(path), int(bool(binary))), "exa_mesh_write_vtk")
 
+    def validate(self):
+        """number of cells with a non-finite value in their solution, update
+        or face data (exa_mesh_validate)"""
+        n = ctypes.c_longlong()
+        _check(load().exa_mesh_validate(self._h, ctypes.byref(n)), "exa_mesh_validate")
+        return n.value
+
     def write_vtk_legendre(self, path, binary=False):
         """legacy VTK unstructured grid of the nodal values at the
         Gauss-Legendre nodes (the reference's ADERDG2LegendreVTK vertex plotter)"""

@@ -463,6 +463,22 @@ __global__ void level_advance_kernel(double* scal, double* lv, int L) {
   scal[3] += 1.0;
 }
 
+// validateNoNansInADERDGSolver (exahype/solvers/ADERDGSolver.cpp:1778-1829)
+// as a scan: flag[cell] = 1 where any of the cell's `per_cell` values is not
+// finite; then the flags are counted
+__global__ void __launch_bounds__(256) nonfinite_flag_kernel(const double* __restrict__ a, size_t per_cell,
+                                                             size_t total, int* __restrict__ flag) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite(a[i])) flag[i / per_cell] = 1;
+}
+__global__ void __launch_bounds__(256) count_flags_kernel(const int* __restrict__ flag, int n,
+                                                          unsigned long long* __restrict__ count) {
+  unsigned long long c = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c += flag[i] != 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
 // independent FP64 FMA chains: 8 per thread, `iters` rounds
 __global__ void __launch_bounds__(256) fp64_probe_kernel(double* out, int iters, double a, double b) {
   double x[8];
@@ -1477,6 +1493,40 @@ int exa_mesh_state(exa_mesh* m, double* t, double* dt, long long* steps, long lo
   if (dt) *dt = h[0];
   if (steps) *steps = (long long)h[3];
   if (sweeps) *sweeps = (long long)sw;
+  return EXA_OK;
+}
+
+int exa_mesh_validate(exa_mesh* m, long long* nonfinite_cells) {
+  if (!m || !nonfinite_cells) return fail(EXA_ERR_ARG, "exa_mesh_validate: null argument");
+  const KernelSet& k = m->s->k;
+  const size_t n = m->ncells, P = k.P, F = k.F, nV = k.nvar, nD = k.nvar + k.npar, D2 = 2 * m->dim;
+  int* flag = nullptr;
+  unsigned long long* cnt = nullptr;
+  if (!salloc(&flag, n * 4, m->stream) || !salloc(&cnt, 8, m->stream)) {
+    cudaGetLastError();
+    if (flag) sfree(flag, m->stream);
+    return fail(EXA_ERR_NOMEM, "exa_mesh_validate: device allocation failed");
+  }
+  EXA_CUDA(cudaMemsetAsync(flag, 0, n * 4, m->stream));
+  EXA_CUDA(cudaMemsetAsync(cnt, 0, 8, m->stream));
+  const struct {
+    const double* a;
+    size_t per;
+  } arrays[4] = {{m->luh, P * nD}, {m->lduh, P * nV}, {m->lQhbnd, D2 * F * nD}, {m->lFhbnd, D2 * F * nV}};
+  for (const auto& x : arrays) {
+    const size_t total = n * x.per;
+    const int grid = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    if (total) nonfinite_flag_kernel<<<grid, 256, 0, m->stream>>>(x.a, x.per, total, flag);
+    EXA_LAUNCHED();
+  }
+  count_flags_kernel<<<std::max(1, std::min((int)((n + 255) / 256), 148 * 4)), 256, 0, m->stream>>>(flag, (int)n, cnt);
+  EXA_LAUNCHED();
+  unsigned long long h = 0;
+  EXA_CUDA(cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, m->stream));
+  sfree(flag, m->stream);
+  sfree(cnt, m->stream);
+  EXA_CUDA(cudaStreamSynchronize(m->stream));
+  *nonfinite_cells = (long long)h;
   return EXA_OK;
 }
 

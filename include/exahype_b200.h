@@ -257,6 +257,11 @@ int exa_mesh_run_until(exa_mesh* m, double t_end, int max_steps, int* steps);
  * number of Picard sweeps executed by the predictor so far */
 int exa_mesh_state(exa_mesh* m, double* t, double* dt, long long* steps, long long* picard_sweeps);
 int exa_mesh_synchronize(exa_mesh* m);
+/* validateNoNansInADERDGSolver (exahype/solvers/ADERDGSolver.cpp:1778-1829)
+ * as a status instead of assertions: *nonfinite_cells = the number of cells
+ * with a non-finite value in their solution, update, or extrapolated state
+ * or flux face data. Synchronises the mesh's stream. */
+int exa_mesh_validate(exa_mesh* m, long long* nonfinite_cells);
 /* Writes the mesh's current solution as a legacy VTK unstructured grid (text,
  * or binary when binary != 0): every cell a patch of (N+1)^d vertices with
  * N^d pixels / voxels, vertex data "Q" (all nD values, from

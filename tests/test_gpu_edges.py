@@ -120,3 +120,27 @@ def test_corrector_min_over_a_list(eb):
         else:
             assert np.array_equal(got[c], u[c])
     assert dmin.item() == min(dts)
+
+
+def test_nan_in_the_input_is_a_status(eb):
+    """a non-finite value planted in the host-prepared input is reported by
+    exa_mesh_validate, stepping goes on without a trap (the step-size
+    minimum skips NaN, as std::min in the reference does) and the NaN
+    spreads to the neighbours; a clean mesh reports 0"""
+    from exahype_b200 import problems
+    u, _ = problems.gaussian_pulse_2d(3, (8, 8), seed=0)
+    s = eb.Solver(2, 3)
+    m = eb.Mesh(s, (8, 8), [0.0, 0.0], [1.0, 1.0], eb.BC_PERIODIC)
+    m.set_solution(u)
+    m.init(0.0)
+    m.step(2)
+    assert m.validate() == 0
+    bad = u.copy()
+    bad[13, 5, 4] = np.nan
+    m.set_solution(bad)
+    m.init(0.0)
+    n0 = m.validate()
+    assert n0 >= 1
+    assert np.isfinite(m.state()["dt"]) and m.state()["dt"] > 0
+    assert m.run_until(1.0, max_steps=3) == 3
+    assert m.validate() > n0
