@@ -547,6 +547,10 @@ struct exa_mesh {
     int anc0 = 0, nanc = 0, nres = 0, npro = 0;
     int *res_f = nullptr, *res_c = nullptr, *res_ld = nullptr, *res_idx = nullptr;
     int *pro_f = nullptr, *pro_c = nullptr, *pro_ld = nullptr, *pro_idx = nullptr;
+    // host copies for the VTK writers: each cell's level and grid position,
+    // each level's widths
+    std::vector<int> level, pos;
+    std::vector<double> ldx;
   } ref;
 };
 
@@ -963,6 +967,7 @@ namespace {
 struct NestedTopo {
   int dim = 0, L = 1, ncells = 0, anc0 = 0, nanc = 0, nslots = 0;
   std::vector<int> level;                              // per cell
+  std::vector<int> pos;                                // per cell: position in its level's grid (3 ints)
   std::vector<int> fl, fr, fd;                          // Riemann pairs
   std::vector<int> bcell, bface;                        // outflow faces of level-0 cells
   std::vector<int> rf, rc, ridx, pf, pc, pidx;          // restriction / prolongation items
@@ -1027,6 +1032,7 @@ static const char* nested_topology(int dim, const int* cells, int nb, const int*
       if (!refined(l, p)) {
         cid[l][pidx_(l, p)] = n++;
         t.level.push_back(l);
+        t.pos.insert(t.pos.end(), {p[0], p[1], p[2]});
       }
     });
   }
@@ -1173,6 +1179,9 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
   m->nbfaces[EXA_BC_OUTFLOW] = (int)t.bcell.size();
   m->geo.inst = m->ref.inst;
   m->geo.inst_dx = m->ref.inst_dx;
+  m->ref.level = t.level;
+  m->ref.pos = t.pos;
+  m->ref.ldx = ldx;
   EXA_CUDA(cudaMemsetAsync(m->luh, 0, n * P * nD * 8, st));
   EXA_CUDA(cudaMemsetAsync(m->lduh, 0, n * P * nV * 8, st));
   EXA_CUDA(cudaMemsetAsync(m->lQhbnd, 0, ns * D2 * F * nD * 8, st));
@@ -1679,7 +1688,6 @@ extern "C" {
 static int mesh_write_vtk(exa_mesh* m, const char* path, int binary, int legendre, const char* fn,
                           const int* status_dev = nullptr) {
   if (!m || !path) return fail(EXA_ERR_ARG, std::string(fn) + ": null argument");
-  if (m->ref.on) return fail(EXA_ERR_UNSUPPORTED, std::string(fn) + ": uniform meshes only");
   const KernelSet& k = m->s->k;
   const int dim = m->dim, N = k.order, b = N + 1, nD = k.nvar + k.npar;
   const size_t n = m->ncells, P = k.P, sub = dim == 3 ? (size_t)N * N * N : (size_t)N * N;
@@ -1714,12 +1722,18 @@ static int mesh_write_vtk(exa_mesh* m, const char* path, int binary, int legendr
   for (int i = 0; i < b; i++) xi[i] = legendre ? exa_tab_nodes[exa_tab_nodes_off[N] + i] : (double)i / N;
   std::fprintf(f, "POINTS %zu double\n", n * P);
   for (size_t c = 0; c < n; c++) {
-    const size_t cx = c % m->cells[0], cy = (c / m->cells[0]) % m->cells[1], cz = c / ((size_t)m->cells[0] * m->cells[1]);
+    // the cell's grid position and widths (its level's on a refined mesh)
+    size_t cp[3] = {c % m->cells[0], (c / m->cells[0]) % m->cells[1], c / ((size_t)m->cells[0] * m->cells[1])};
+    const double* w = m->geo.dx;
+    if (m->ref.on) {
+      for (int d = 0; d < 3; d++) cp[d] = (size_t)m->ref.pos[3 * c + d];
+      w = &m->ref.ldx[3 * (size_t)m->ref.level[c]];
+    }
     for (size_t p = 0; p < P; p++) {
       const int ix = (int)(p % b), iy = (int)((p / b) % b), iz = dim == 3 ? (int)(p / (b * b)) : 0;
-      o.num(m->offset[0] + (cx + xi[ix]) * m->geo.dx[0], " ");
-      o.num(m->offset[1] + (cy + xi[iy]) * m->geo.dx[1], " ");
-      o.num(dim == 3 ? m->offset[2] + (cz + xi[iz]) * m->geo.dx[2] : 0.0, "\n");
+      o.num(m->offset[0] + (cp[0] + xi[ix]) * w[0], " ");
+      o.num(m->offset[1] + (cp[1] + xi[iy]) * w[1], " ");
+      o.num(dim == 3 ? m->offset[2] + (cp[2] + xi[iz]) * w[2] : 0.0, "\n");
     }
   }
   o.eol();

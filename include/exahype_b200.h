@@ -187,8 +187,8 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
 /* A statically refined periodic mesh: the coarse grid of exa_mesh_create with
  * the box of coarse cells box_lo[d] <= c[d] < box_hi[d] refined once (3^d
  * fine cells each; at least one coarse cell must surround the box). Global
- * time stepping; the same exa_mesh_* calls step it (not exa_mesh_init_fused,
- * not exa_mesh_write_vtk). Solution order: the unrefined coarse cells
+ * time stepping; the same exa_mesh_* calls step and write it (not
+ * exa_mesh_init_fused). Solution order: the unrefined coarse cells
  * (x fastest over the coarse grid, refined ones skipped), then the fine cells
  * (x fastest over the box's fine grid). Replaces the spacetree's hanging-face
  * handling for this layout: after every predictor the refined cells that

@@ -169,5 +169,35 @@ def test_refined_mesh_arguments(eb):
     m = eb.Mesh.refined(s, (9, 9), [0.0, 0.0], [1.0, 1.0], (3, 3), (6, 6))
     with pytest.raises(eb.ExaError):
         m.init_fused(0.0, 0.99)
-    with pytest.raises(eb.ExaError):
-        m.write_vtk("/dev/null")
+
+
+
+def test_nested_mesh_write_vtk(eb, tmp_path):
+    """both VTK layouts on a nested mesh: every cell's points at its own
+    level's position and width"""
+    import importlib.util
+    import os
+    from exahype_b200 import problems
+    spec = importlib.util.spec_from_file_location("amr_t", os.path.join(os.path.dirname(__file__), "test_gpu_amr.py"))
+    amr_t = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(amr_t)
+    cells, boxes = (9, 9), [((3, 3), (6, 6)), ((10, 10), (17, 17))]
+    s = eb.Solver(2, 3)
+    m = eb.Mesh.nested(s, cells, [0.0, 0.0], [1.0, 1.0], boxes)
+    u = problems.pulse_nested(2, 3, cells, boxes, seed=6)
+    m.set_solution(u)
+    m.init(0.0)
+    m.step(2)
+    sol = m.get_solution()
+    path = str(tmp_path / "nested_l.vtk")
+    m.write_vtk_legendre(path, binary=True)
+    v = amr_t.read_vtk(path)
+    X = problems.nested_node_coordinates(2, 3, cells, boxes).reshape(-1, 2)
+    assert np.allclose(v["points"][:, :2], X, rtol=0, atol=1e-14)
+    assert np.array_equal(v["Q"], sol.reshape(-1, 5))
+    path = str(tmp_path / "nested_c.vtk")
+    m.write_vtk(path)
+    v = amr_t.read_vtk(path)
+    ref_q = np.concatenate([pyoracle.plot_vertices(2, 3, 5, sol[c]).reshape(-1, 5) for c in range(m.ncells)])
+    assert np.max(np.abs(v["Q"] - ref_q)) <= 1e-12 * np.max(np.abs(ref_q))
+    assert np.allclose(v["points"].min(axis=0)[:2], 0.0) and np.allclose(v["points"].max(axis=0)[:2], 1.0)
