@@ -1149,7 +1149,7 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
             salloc(&m->lQhbnd, ns * D2 * F * nD * 8, st) && salloc(&m->lFhbnd, ns * D2 * F * nV * 8, st) &&
             salloc(&m->scal, 8 * 8, st) && ia(&m->iters, n) && ia(&m->fl, t.fl.size()) && ia(&m->fr, t.fl.size()) &&
             ia(&m->fd, t.fl.size()) && ia(&m->bcell, t.bcell.size()) && ia(&m->bface, t.bcell.size()) &&
-            salloc(&m->sweeps, 8, st) && salloc(&m->ref.lv, 2 * (size_t)L * 8, st) && ia(&m->ref.inst, n) &&
+            salloc(&m->sweeps, 8, st) && salloc(&m->ref.lv, 3 * (size_t)L * 8, st) && ia(&m->ref.inst, n) &&
             salloc(&m->ref.inst_dx, ldx.size() * 8, st) && ia(&m->ref.res_f, t.rf.size()) &&
             ia(&m->ref.res_c, t.rf.size()) && ia(&m->ref.res_ld, t.rf.size()) && ia(&m->ref.res_idx, t.ridx.size()) &&
             ia(&m->ref.pro_f, t.pf.size()) && ia(&m->ref.pro_c, t.pf.size()) && ia(&m->ref.pro_ld, t.pf.size()) &&
@@ -1270,7 +1270,8 @@ static int mesh_predict(exa_mesh* m, const int* count = nullptr) {
   const KernelSet& k = m->s->k;
   PhaseTimer pt(m, 0);
   m->phase_launches[0] += 2;
-  int rc = k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, m->fused ? m->scal + 5 : mesh_dt(m), m->geo,
+  double* dt = m->fused ? (m->ref.on ? m->ref.lv + 2 * m->ref.nlev : m->scal + 5) : mesh_dt(m);
+  int rc = k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, dt, m->geo,
                        m->ncells, nullptr, count, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
   if (rc || !m->ref.on) return rc;
   m->phase_launches[0] += 3;
@@ -1282,13 +1283,38 @@ static int mesh_predict(exa_mesh* m, const int* count = nullptr) {
 // predictor step, [6] predictor reruns (ADERDGSolver's _minCorrector*/
 // _minPredictor*). Arithmetic in round-to-nearest operations, as the
 // reference's unfused evaluation.
-__global__ void fused_init_kernel(double* scal) {
-  const double s0 = scal[1];  // min admissible step of the initial data
+// Refined meshes (lv != NULL, L levels): the min-reduction targets are
+// lv[L..2L-1], and the levels' corrector and predictor steps lv[0..L-1] and
+// lv[2L..3L-1] are copies of scal[0] and scal[5].
+__device__ double fused_take_min(double* scal, double* lv, int L) {
+  const double big = __longlong_as_double(0x7fefffffffffffffll);
+  if (!lv) {
+    const double s = scal[1];
+    scal[1] = big;
+    return s;
+  }
+  double s = big;
+  for (int l = 0; l < L; l++) {
+    s = (lv[L + l] < s) ? lv[L + l] : s;
+    lv[L + l] = big;
+  }
+  return s;
+}
+__device__ void fused_copy_levels(const double* scal, double* lv, int L) {
+  if (!lv) return;
+  for (int l = 0; l < L; l++) {
+    lv[l] = scal[0];
+    lv[2 * L + l] = scal[5];
+  }
+}
+
+__global__ void fused_init_kernel(double* scal, double* lv, int L) {
+  const double s0 = fused_take_min(scal, lv, L);  // min admissible step of the initial data
   scal[0] = s0;
   scal[5] = s0;
   scal[4] = __dadd_rn(scal[2], s0);
-  scal[1] = __longlong_as_double(0x7fefffffffffffffll);
   scal[6] = 0.0;
+  fused_copy_levels(scal, lv, L);
 }
 
 // end of a fused step (SolutionUpdate::endIteration,
@@ -1297,8 +1323,8 @@ __global__ void fused_init_kernel(double* scal) {
 // ADERDGSolver.cpp:559-592): s = min stable step after the update; a
 // predictor step above s is replaced by w s (and the predictor rerun), else
 // the next estimate is the mean of the used step and w s
-__global__ void fused_advance_kernel(double* scal, double w, int* rerun, int ncells) {
-  const double s = scal[1];
+__global__ void fused_advance_kernel(double* scal, double w, int* rerun, int ncells, double* lv, int L) {
+  const double s = fused_take_min(scal, lv, L);
   double next = __longlong_as_double(0x7fefffffffffffffll);
   next = (s < next) ? s : next;
   double pdt = scal[5];
@@ -1316,15 +1342,14 @@ __global__ void fused_advance_kernel(double* scal, double w, int* rerun, int nce
   scal[0] = pdt;
   scal[4] = __dadd_rn(scal[4], pdt);
   scal[5] = next;
-  scal[1] = __longlong_as_double(0x7fefffffffffffffll);
   scal[3] += 1.0;
   if (unstable) scal[6] += 1.0;
   *rerun = unstable ? ncells : 0;
+  fused_copy_levels(scal, lv, L);
 }
 
 int exa_mesh_init_fused(exa_mesh* m, double t0, double weight) {
   if (!m || !(weight > 0.0) || weight > 1.0) return fail(EXA_ERR_ARG, "exa_mesh_init_fused: bad argument");
-  if (m->ref.on) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_init_fused: refined meshes step non-fused");
   const KernelSet& k = m->s->k;
   if (!m->rerun && !salloc(&m->rerun, sizeof(int), m->stream)) {
     cudaGetLastError();
@@ -1335,12 +1360,16 @@ int exa_mesh_init_fused(exa_mesh* m, double t0, double weight) {
   m->weight = weight;
   init_scalars_kernel<<<1, 1, 0, m->stream>>>(m->scal, t0);
   EXA_LAUNCHED();
+  if (m->ref.on) {
+    level_reset_kernel<<<1, 1, 0, m->stream>>>(m->ref.lv, m->ref.nlev);
+    EXA_LAUNCHED();
+  }
   EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, m->stream));
   EXA_CUDA(cudaMemsetAsync(m->rerun, 0, sizeof(int), m->stream));
-  int rc = k.corrector(m->luh, nullptr, nullptr, nullptr, m->scal + 1, m->geo, m->ncells, nullptr, 0, nullptr,
+  int rc = k.corrector(m->luh, nullptr, nullptr, nullptr, mesh_dt_min(m), m->geo, m->ncells, nullptr, 0, nullptr,
                        m->stream);
   if (rc) return rc;
-  fused_init_kernel<<<1, 1, 0, m->stream>>>(m->scal);
+  fused_init_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->ref.on ? m->ref.lv : nullptr, m->ref.nlev);
   EXA_LAUNCHED();
   rc = mesh_predict(m);
   if (rc) return rc;
@@ -1416,7 +1445,8 @@ static int mesh_one_step(exa_mesh* m) {
     if (rc) return rc;
     {
       PhaseTimer pt(m, 3);
-      fused_advance_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->weight, m->rerun, m->ncells);
+      fused_advance_kernel<<<1, 1, 0, m->stream>>>(m->scal, m->weight, m->rerun, m->ncells,
+                                                   m->ref.on ? m->ref.lv : nullptr, m->ref.nlev);
       EXA_LAUNCHED();
       m->phase_launches[3] += 1;
     }

@@ -417,13 +417,14 @@ class RefinedMesh:
     def _stable(self):
         return min(self.K.stable_dt(self.u[c], self._dx(c)) for c in range(self.ncells))
 
-    def _predict(self):
+    def _predict(self, dt=None):
         K, d = self.K, self.dim
+        dt = self.dt if dt is None else dt
         for c in range(self.ncells):
             if self.linear:
-                o = K.lin_predictor(self.u[c], self._dx(c), self.dt)
+                o = K.lin_predictor(self.u[c], self._dx(c), dt)
             else:
-                o = K.predictor(self.u[c], self._dx(c), self.dt)
+                o = K.predictor(self.u[c], self._dx(c), dt)
                 self.sweeps += int(o["iterations"])
             self.Q[c] = o["lQhbnd"].reshape(2 * d, -1)
             self.Fb[c] = o["lFhbnd"].reshape(2 * d, -1)
@@ -443,25 +444,68 @@ class RefinedMesh:
 
     def init(self, t0=0.0):
         self.t, self.steps, self.sweeps = t0, 0, 0
+        self.fused = False
         self.dt = self._stable()
         self._predict()
 
-    def step(self, n=1):
+    def init_fused(self, t0=0.0, weight=0.99):
+        """fused time stepping, restating oracle/harness.c hrn_init_fused /
+        hrn_step_fused (the reference's fuse-algorithmic-steps): the
+        predictor runs right after the update with its own step estimate"""
+        self.t, self.steps, self.sweeps, self.reruns = t0, 0, 0, 0
+        self.fused, self.w = True, weight
+        s0 = self._stable()
+        self.dt = self.pdt = s0
+        self.tp = t0 + s0
+        self._predict(self.pdt)
+
+    def fused_state(self):
+        return dict(predictor_dt=self.pdt, reruns=self.reruns)
+
+    def _update(self):
         K = self.K
+        for l, r, i in self.pairs:
+            if self.linear:
+                fl, fr = K.lin_riemann(self.Q[l, 2 * i + 1], self.Q[r, 2 * i], i)
+            else:
+                fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1],
+                                   self.Q[r, 2 * i], i)
+            self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i] = fl, fr
+        for c, face in self.bnd:
+            self.Fb[c, face] = K.boundary_face(self.Fb[c, face], self.Q[c, face], face)
+        for c in range(self.ncells):
+            si = K.lin_surface_integral if self.linear else K.surface_integral
+            du = si(self.du[c], self.Fb[c].reshape(-1), self._dx(c))
+            self.u[c] = K.solution_update(self.u[c], du, self.dt).reshape(self.u[c].shape)
+
+    def _step_fused(self):
+        self._update()
+        s = self._stable()
+        self._predict(self.pdt)
+        nxt = s
+        used = s if self.pdt == 0.0 else self.pdt
+        unstable = used > s
+        if unstable:
+            ws = self.w * s
+            nxt = min(nxt, ws)
+            self.pdt = ws
+        else:
+            nxt = min(nxt, 0.5 * (used + self.w * s))
+        self.t = self.tp
+        self.dt = self.pdt
+        self.tp = self.tp + self.pdt
+        self.pdt = nxt
+        self.steps += 1
+        if unstable:
+            self.reruns += 1
+            self._predict(self.pdt)
+
+    def step(self, n=1):
         for _ in range(n):
-            for l, r, i in self.pairs:
-                if self.linear:
-                    fl, fr = K.lin_riemann(self.Q[l, 2 * i + 1], self.Q[r, 2 * i], i)
-                else:
-                    fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1],
-                                       self.Q[r, 2 * i], i)
-                self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i] = fl, fr
-            for c, face in self.bnd:
-                self.Fb[c, face] = K.boundary_face(self.Fb[c, face], self.Q[c, face], face)
-            for c in range(self.ncells):
-                si = K.lin_surface_integral if self.linear else K.surface_integral
-                du = si(self.du[c], self.Fb[c].reshape(-1), self._dx(c))
-                self.u[c] = K.solution_update(self.u[c], du, self.dt).reshape(self.u[c].shape)
+            if getattr(self, "fused", False):
+                self._step_fused()
+                continue
+            self._update()
             self.t += self.dt
             self.steps += 1
             self.dt = self._stable()

@@ -166,10 +166,6 @@ def test_refined_mesh_arguments(eb):
     for lo, hi in (((0, 3), (6, 6)), ((3, 3), (9, 6)), ((4, 3), (4, 6))):
         with pytest.raises(eb.ExaError):
             eb.Mesh.refined(s, (9, 9), [0.0, 0.0], [1.0, 1.0], lo, hi)
-    m = eb.Mesh.refined(s, (9, 9), [0.0, 0.0], [1.0, 1.0], (3, 3), (6, 6))
-    with pytest.raises(eb.ExaError):
-        m.init_fused(0.0, 0.99)
-
 
 
 def test_nested_mesh_write_vtk(eb, tmp_path):
@@ -201,3 +197,30 @@ def test_nested_mesh_write_vtk(eb, tmp_path):
     ref_q = np.concatenate([pyoracle.plot_vertices(2, 3, 5, sol[c]).reshape(-1, 5) for c in range(m.ncells)])
     assert np.max(np.abs(v["Q"] - ref_q)) <= 1e-12 * np.max(np.abs(ref_q))
     assert np.allclose(v["points"].min(axis=0)[:2], 0.0) and np.allclose(v["points"].max(axis=0)[:2], 1.0)
+
+
+@pytest.mark.parametrize("boxes,w", [([((3, 3), (6, 6))], 0.99), ([((3, 3), (6, 6)), ((10, 10), (17, 17))], 0.9)])
+def test_nested_mesh_fused_vs_oracle(eb, boxes, w):
+    """fused time stepping on refined meshes: the predictor of every level
+    runs right after the update with the estimated step, rerun with
+    weight * stable when the estimate was too large"""
+    from exahype_b200 import problems
+    cells = (9, 9)
+    u = problems.pulse_nested(2, 3, cells, boxes, seed=8)
+    s = eb.Solver(2, 3)
+    m = eb.Mesh.nested(s, cells, [0.0, 0.0], [1.0, 1.0], boxes)
+    o = pyoracle.RefinedMesh(2, 3, cells, [1.0, 1.0], boxes=boxes)
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init_fused(0.0, w)
+    o.init_fused(0.0, w)
+    m.step(12)
+    o.step(12)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    sa, sb = m.state(), o.state()
+    assert sa["steps"] == sb["steps"] == 12 and sa["picard_sweeps"] == sb["picard_sweeps"]
+    close = lambda x, y: abs(x - y) <= 1e-13 * abs(y)  # noqa: E731
+    assert close(sa["t"], sb["t"]) and close(sa["dt"], sb["dt"])
+    fa, fb = m.fused_state(), o.fused_state()
+    assert close(fa["predictor_dt"], fb["predictor_dt"]) and fa["reruns"] == fb["reruns"]
