@@ -285,6 +285,13 @@ class Mesh:
         domain at that level). bc: periodic or outflow, per domain face or
         one for all. Solution order: the unrefined cells of each level in
         turn, x fastest."""
+        return cls.boxes(solver, cells, offset, size, [(k, lo, hi) for k, (lo, hi) in enumerate(boxes)], bc)
+
+    @classmethod
+    def boxes(cls, solver, cells, offset, size, boxes, bc=BC_PERIODIC):
+        """Mesh refined by boxes (exa_mesh_create_boxes): boxes[k] = (level,
+        lo, hi), the positions lo <= p < hi of that level refined once
+        (several boxes per level refine their union)."""
         lib = load()
         d = solver.dim
         self = cls.__new__(cls)
@@ -293,18 +300,19 @@ class Mesh:
         o = _dbl3(list(offset) + [0.0] * (3 - len(offset)))
         s = _dbl3(list(size) + [1.0] * (3 - len(size)))
         nb = len(boxes)
-        lo = (ctypes.c_int * (3 * nb))(*sum((list(b[0]) + [0] * (3 - len(b[0])) for b in boxes), []))
-        hi = (ctypes.c_int * (3 * nb))(*sum((list(b[1]) + [1] * (3 - len(b[1])) for b in boxes), []))
-        h = ctypes.c_void_p()
+        lev = (ctypes.c_int * nb)(*[int(b[0]) for b in boxes])
+        lo = (ctypes.c_int * (3 * nb))(*sum((list(b[1]) + [0] * (3 - len(b[1])) for b in boxes), []))
+        hi = (ctypes.c_int * (3 * nb))(*sum((list(b[2]) + [1] * (3 - len(b[2])) for b in boxes), []))
         if isinstance(bc, int):
             bc = [bc] * (2 * d)
         bcs = (ctypes.c_int * 6)(*(list(bc) + [BC_PERIODIC] * (6 - len(bc))))
-        _check(lib.exa_mesh_create_nested(solver._h, c, o, s, bcs, nb, lo, hi, ctypes.byref(h)),
-               "exa_mesh_create_nested")
+        h = ctypes.c_void_p()
+        _check(lib.exa_mesh_create_boxes(solver._h, c, o, s, bcs, nb, lev, lo, hi, ctypes.byref(h)),
+               "exa_mesh_create_boxes")
         self._h = h
         self.solver = solver
         self.cells = tuple(cells)
-        self.boxes = [(tuple(b[0]), tuple(b[1])) for b in boxes]
+        self.boxes = [(int(b[0]), tuple(b[1]), tuple(b[2])) for b in boxes]
         n = ctypes.c_int()
         _check(lib.exa_mesh_num_cells(h, ctypes.byref(n)), "exa_mesh_num_cells")
         self.ncells = n.value

@@ -973,64 +973,91 @@ struct NestedTopo {
   std::vector<int> rf, rc, ridx, pf, pc, pidx;          // restriction / prolongation items
 };
 
-// returns an error message, or nullptr
-static const char* nested_topology(int dim, const int* cells, int nb, const int* lo, const int* hi, const int* bc,
-                                   NestedTopo& t) {
-  const int L = nb + 1, D2 = 2 * dim;
+// A refined mesh from boxes: box k refines the positions lo_k <= p < hi_k
+// of level box_level[k] (in that level's cell coordinates over the whole
+// domain: 3^l cells[d] per axis at level l). The region of level l >= 1 is
+// the union of the level-(l-1) boxes, refined once; every box must lie
+// inside its level's region with one cell of margin, so that hanging faces
+// join neighbouring levels only. Returns an error message, or nullptr.
+static const char* boxes_topology(int dim, const int* cells, const int* bc, int nb, const int* box_level,
+                                  const int* lo, const int* hi, NestedTopo& t) {
+  int L = 1;
+  for (int k = 0; k < nb; k++) {
+    if (box_level[k] < 0 || box_level[k] > 7) return "box levels must be 0..7";
+    L = std::max(L, box_level[k] + 2);
+  }
+  const int D2 = 2 * dim;
   t.dim = dim;
   t.L = L;
-  // region of level l in level-l coordinates: [r0, r1)
+  // bounding rectangle [r0, r1) of every level's region
   std::vector<std::array<int, 3>> r0(L), r1(L);
-  for (int d = 0; d < 3; d++) {
-    r0[0][d] = 0;
-    r1[0][d] = d < dim ? cells[d] : 1;
-  }
-  for (int l = 1; l < L; l++)
-    for (int d = 0; d < 3; d++) {
-      const int bl = lo[3 * (l - 1) + d], bh = hi[3 * (l - 1) + d];
-      if (d < dim) {
-        if (bl < r0[l - 1][d] + 1 || bh <= bl || bh > r1[l - 1][d] - 1)
-          return "each refined box must lie inside its level's region with at least one cell around it";
-        r0[l][d] = 3 * bl;
-        r1[l][d] = 3 * bh;
-      } else {
-        r0[l][d] = 0;
-        r1[l][d] = 1;
+  for (int d = 0; d < 3; d++) r0[0][d] = 0, r1[0][d] = d < dim ? cells[d] : 1;
+  for (int l = 1; l < L; l++) {
+    bool any = false;
+    for (int d = 0; d < 3; d++) r0[l][d] = INT_MAX, r1[l][d] = INT_MIN;
+    for (int k = 0; k < nb; k++) {
+      if (box_level[k] != l - 1) continue;
+      any = true;
+      for (int d = 0; d < 3; d++) {
+        const int a = d < dim ? 3 * lo[3 * k + d] : 0, b = d < dim ? 3 * hi[3 * k + d] : 1;
+        r0[l][d] = std::min(r0[l][d], a);
+        r1[l][d] = std::max(r1[l][d], b);
       }
     }
-  long long total = 0;
-  for (int l = 0; l < L; l++) total += (long long)(r1[l][0] - r0[l][0]) * (r1[l][1] - r0[l][1]) * (r1[l][2] - r0[l][2]);
-  if (total > (1ll << 27)) return "too many cells";
-  // per level: position -> cell slot (or ancestor slot, or -1)
-  std::vector<std::vector<int>> cid(L), aid(L);
+    if (!any) return "every level below the finest needs at least one box";
+  }
   auto ext = [&](int l, int d) { return r1[l][d] - r0[l][d]; };
-  auto pidx_ = [&](int l, const int* p) {
-    return ((size_t)(p[2] - r0[l][2]) * ext(l, 1) + (p[1] - r0[l][1])) * ext(l, 0) + (p[0] - r0[l][0]);
-  };
-  auto refined = [&](int l, const int* p) {  // inside box l+1
-    if (l + 1 >= L) return false;
-    for (int d = 0; d < dim; d++)
-      if (p[d] < lo[3 * l + d] || p[d] >= hi[3 * l + d]) return false;
+  for (int l = 0; l < L; l++)
+    if ((double)ext(l, 0) * ext(l, 1) * ext(l, 2) > (double)(1ll << 27)) return "too many cells";
+  auto inrect = [&](int l, const int* p) {
+    for (int d = 0; d < 3; d++)
+      if (p[d] < r0[l][d] || p[d] >= r1[l][d]) return false;
     return true;
   };
-  auto on_box_face = [&](int l, const int* p) {  // refined and on box l+1's faces
-    for (int d = 0; d < dim; d++)
-      if (p[d] == lo[3 * l + d] || p[d] == hi[3 * l + d] - 1) return true;
-    return false;
+  auto idx = [&](int l, const int* p) {
+    return ((size_t)(p[2] - r0[l][2]) * ext(l, 1) + (p[1] - r0[l][1])) * ext(l, 0) + (p[0] - r0[l][0]);
   };
-  auto for_region = [&](int l, auto&& fn) {
+  // state per level and position: 0 outside the region, 1 cell, 2 refined
+  std::vector<std::vector<unsigned char>> st(L);
+  for (int l = 0; l < L; l++) st[l].assign((size_t)ext(l, 0) * ext(l, 1) * ext(l, 2), l == 0 ? 1 : 0);
+  auto for_rect = [&](const int* a, const int* b, auto&& fn) {
     int p[3];
-    for (p[2] = r0[l][2]; p[2] < r1[l][2]; p[2]++)
-      for (p[1] = r0[l][1]; p[1] < r1[l][1]; p[1]++)
-        for (p[0] = r0[l][0]; p[0] < r1[l][0]; p[0]++) fn(p);
+    for (p[2] = a[2]; p[2] < b[2]; p[2]++)
+      for (p[1] = a[1]; p[1] < b[1]; p[1]++)
+        for (p[0] = a[0]; p[0] < b[0]; p[0]++) fn(p);
   };
+  for (int k = 0; k < nb; k++) {  // the region of the next level
+    const int l = box_level[k];
+    int a[3] = {0, 0, 0}, b[3] = {1, 1, 1};
+    for (int d = 0; d < dim; d++) a[d] = 3 * lo[3 * k + d], b[d] = 3 * hi[3 * k + d];
+    if (a[0] >= b[0] || a[1] >= b[1] || a[2] >= b[2]) return "empty box";
+    for_rect(a, b, [&](const int* p) { st[l + 1][idx(l + 1, p)] = 1; });
+  }
+  const char* err = nullptr;
+  for (int k = 0; k < nb && !err; k++) {  // margins, then mark refined
+    const int l = box_level[k];
+    int a[3] = {0, 0, 0}, b[3] = {1, 1, 1};
+    for (int d = 0; d < dim; d++) a[d] = lo[3 * k + d] - 1, b[d] = hi[3 * k + d] + 1;
+    for_rect(a, b, [&](const int* p) {
+      if (!inrect(l, p) || st[l][idx(l, p)] == 0) err = "each box must lie inside its level's region with one cell around it";
+    });
+  }
+  if (err) return err;
+  for (int k = 0; k < nb; k++) {
+    const int l = box_level[k];
+    int a[3] = {0, 0, 0}, b[3] = {1, 1, 1};
+    for (int d = 0; d < dim; d++) a[d] = lo[3 * k + d], b[d] = hi[3 * k + d];
+    for_rect(a, b, [&](const int* p) { st[l][idx(l, p)] = 2; });
+  }
+  auto state = [&](int l, const int* p) { return inrect(l, p) ? st[l][idx(l, p)] : (unsigned char)0; };
+  // slots: cells level by level (x fastest), then ancestors, then descendants
+  std::vector<std::vector<int>> slot(L);
   int n = 0;
   for (int l = 0; l < L; l++) {
-    cid[l].assign((size_t)ext(l, 0) * ext(l, 1) * ext(l, 2), -1);
-    aid[l].assign(cid[l].size(), -1);
-    for_region(l, [&](const int* p) {
-      if (!refined(l, p)) {
-        cid[l][pidx_(l, p)] = n++;
+    slot[l].assign(st[l].size(), -1);
+    for_rect(r0[l].data(), r1[l].data(), [&](const int* p) {
+      if (st[l][idx(l, p)] == 1) {
+        slot[l][idx(l, p)] = n++;
         t.level.push_back(l);
         t.pos.insert(t.pos.end(), {p[0], p[1], p[2]});
       }
@@ -1038,53 +1065,64 @@ static const char* nested_topology(int dim, const int* cells, int nb, const int*
   }
   t.ncells = n;
   t.anc0 = n;
-  for (int l = 0; l + 1 < L; l++)
-    for_region(l, [&](const int* p) {
-      if (refined(l, p) && on_box_face(l, p)) aid[l][pidx_(l, p)] = n++, t.nanc++;
+  auto nb_pos = [&](int l, const int* p, int d, int s, int* q) {  // the neighbour across face 2d+s
+    q[0] = p[0], q[1] = p[1], q[2] = p[2];
+    q[d] += s ? 1 : -1;
+    if (l == 0 && bc[2 * d] == EXA_BC_PERIODIC) q[d] = (q[d] + cells[d]) % cells[d];
+  };
+  for (int l = 0; l + 1 < L; l++)  // ancestors: refined positions facing a cell
+    for_rect(r0[l].data(), r1[l].data(), [&](const int* p) {
+      if (st[l][idx(l, p)] != 2) return;
+      bool faces_cell = false;
+      for (int d = 0; d < dim; d++)
+        for (int s = 0; s < 2; s++) {
+          int q[3];
+          nb_pos(l, p, d, s, q);
+          faces_cell |= state(l, q) == 1;
+        }
+      if (faces_cell) slot[l][idx(l, p)] = n++, t.nanc++;
     });
   for (int l = 0; l < L; l++)
-    for_region(l, [&](const int* p) {
-      const bool rp = refined(l, p);
-      const int me = rp ? aid[l][pidx_(l, p)] : cid[l][pidx_(l, p)];
+    for_rect(r0[l].data(), r1[l].data(), [&](const int* p) {
+      const unsigned char sp = st[l][idx(l, p)];
+      if (sp == 0) return;
+      const int me = slot[l][idx(l, p)];  // -1: refined and facing no cell
       for (int d = 0; d < dim; d++) {
-        int q[3] = {p[0], p[1], p[2]};
-        q[d] = p[d] + 1;
-        if (l == 0 && bc[2 * d] != EXA_BC_PERIODIC) {  // outflow domain faces (never refined: margin)
-          if (p[d] == 0) t.bcell.push_back(me), t.bface.push_back(2 * d);
-          if (q[d] == cells[d]) t.bcell.push_back(me), t.bface.push_back(2 * d + 1);
-        } else if (l == 0) {
-          q[d] %= cells[d];  // periodic coarse grid
+        int q[3];
+        nb_pos(l, p, d, 1, q);
+        const unsigned char sq = state(l, q);
+        if (sq != 0 && !(sp == 2 && sq == 2)) {  // same-level pair with at least one cell
+          t.fl.push_back(me);
+          t.fr.push_back(slot[l][idx(l, q)]);
+          t.fd.push_back(d);
         }
-        if (q[d] < r1[l][d]) {  // same-level neighbour: skip refined pairs
-          const bool rq = refined(l, q);
-          if (!(rp && rq)) {
-            t.fl.push_back(me);
-            t.fr.push_back(rq ? aid[l][pidx_(l, q)] : cid[l][pidx_(l, q)]);
-            t.fd.push_back(d);
+        if (sp != 1) continue;
+        for (int s = 0; s < 2; s++) {
+          int r[3];
+          nb_pos(l, p, d, s, r);
+          if (state(l, r) != 0) continue;
+          if (l == 0) {  // a domain face (outflow)
+            t.bcell.push_back(me);
+            t.bface.push_back(2 * d + s);
+            continue;
           }
-        }
-        if (l == 0 || rp) continue;
-        // a cell on its region's face: a descendant across it (the coarse
-        // neighbour's virtual child), with the face transfers
-        int sub[2] = {0, 0}, ns = 0;
-        for (int e = 0; e < dim; e++)
-          if (e != d) sub[ns++] = p[e] % 3;
-        const int parent[3] = {p[0] / 3, p[1] / 3, dim == 3 ? p[2] / 3 : 0};
-        for (int side = 0; side < 2; side++) {
-          if (p[d] != (side == 0 ? r0[l][d] : r1[l][d] - 1)) continue;
-          const int face = 2 * d + side, desc = n++;
-          t.fl.push_back(side == 0 ? desc : me);
-          t.fr.push_back(side == 0 ? me : desc);
+          // a cell on its region's face: a descendant across it (the coarse
+          // neighbour's virtual child), with the face transfers
+          int sub[2] = {0, 0}, ns = 0;
+          for (int e = 0; e < dim; e++)
+            if (e != d) sub[ns++] = p[e] % 3;
+          const int parent[3] = {p[0] / 3, p[1] / 3, dim == 3 ? p[2] / 3 : 0};
+          const int rparent[3] = {r[0] / 3, r[1] / 3, dim == 3 ? r[2] / 3 : 0};
+          const int face = 2 * d + s, dface = 2 * d + (1 - s), desc = n++;
+          t.fl.push_back(s == 0 ? desc : me);
+          t.fr.push_back(s == 0 ? me : desc);
           t.fd.push_back(d);
           t.rf.push_back(me * D2 + face);
-          t.rc.push_back(aid[l - 1][pidx_(l - 1, parent)] * D2 + face);
+          t.rc.push_back(slot[l - 1][idx(l - 1, parent)] * D2 + face);
           t.ridx.push_back(sub[0]);
           t.ridx.push_back(sub[1]);
-          int cn[3] = {parent[0], parent[1], parent[2]};
-          cn[d] += side == 0 ? -1 : 1;
-          const int dface = side == 0 ? 2 * d + 1 : 2 * d;
           t.pf.push_back(desc * D2 + dface);
-          t.pc.push_back(cid[l - 1][pidx_(l - 1, cn)] * D2 + dface);
+          t.pc.push_back(slot[l - 1][idx(l - 1, rparent)] * D2 + dface);
           t.pidx.push_back(sub[0]);
           t.pidx.push_back(sub[1]);
         }
@@ -1095,17 +1133,18 @@ static const char* nested_topology(int dim, const int* cells, int nb, const int*
 }
 }  // namespace
 
-int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* offset, const double* size,
-                           const int* bc, int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out) {
-  if (!s || !cells || !offset || !size || !box_lo || !box_hi || !out)
-    return fail(EXA_ERR_ARG, "exa_mesh_create_nested: null argument");
-  if (nboxes < 1 || nboxes > 8) return fail(EXA_ERR_ARG, "exa_mesh_create_nested: 1 to 8 refined boxes");
+int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* offset, const double* size,
+                          const int* bc, int nboxes, const int* box_level, const int* box_lo, const int* box_hi,
+                          exa_mesh** out) {
+  if (!s || !cells || !offset || !size || !box_level || !box_lo || !box_hi || !out)
+    return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: null argument");
+  if (nboxes < 1 || nboxes > 4096) return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: 1 to 4096 refined boxes");
   const int dim = s->k.dim, D2 = 2 * dim;
   std::unique_ptr<exa_mesh> m(new exa_mesh());
   m->s = s;
   m->dim = dim;
   for (int d = 0; d < dim; d++) {
-    if (cells[d] < 3 || !(size[d] > 0)) return fail(EXA_ERR_ARG, "exa_mesh_create_nested: bad grid");
+    if (cells[d] < 3 || !(size[d] > 0)) return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: bad grid");
     m->cells[d] = cells[d];
     m->offset[d] = offset[d];
     m->geo.dx[d] = size[d] / cells[d];
@@ -1114,16 +1153,16 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
   for (int f = 0; f < 6; f++) {
     const int k = bc && f < 2 * dim ? bc[f] : EXA_BC_PERIODIC;
     if (k != EXA_BC_PERIODIC && k != EXA_BC_OUTFLOW)
-      return fail(EXA_ERR_ARG, "exa_mesh_create_nested: boundaries must be periodic or outflow");
+      return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: boundaries must be periodic or outflow");
     if (f % 2 == 1 && (k == EXA_BC_PERIODIC) != (m->bc[f - 1] == EXA_BC_PERIODIC))
-      return fail(EXA_ERR_ARG, "exa_mesh_create_nested: periodic must be set on both faces of an axis");
+      return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: periodic must be set on both faces of an axis");
     if (k != EXA_BC_PERIODIC && s->k.linear)
-      return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create_nested: the linear kernels support periodic meshes only");
+      return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create_boxes: the linear kernels support periodic meshes only");
     m->bc[f] = k;
   }
   NestedTopo t;
-  if (const char* err = nested_topology(dim, cells, nboxes, box_lo, box_hi, m->bc, t))
-    return fail(EXA_ERR_ARG, std::string("exa_mesh_create_nested: ") + err);
+  if (const char* err = boxes_topology(dim, cells, m->bc, nboxes, box_level, box_lo, box_hi, t))
+    return fail(EXA_ERR_ARG, std::string("exa_mesh_create_boxes: ") + err);
   const int L = t.L;
   m->ncells = t.ncells;
   m->nfaces = (int)t.fl.size();
@@ -1157,7 +1196,7 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
   if (!ok) {
     cudaGetLastError();
     mesh_free(m.get());
-    return fail(EXA_ERR_NOMEM, "exa_mesh_create_nested: device allocation failed");
+    return fail(EXA_ERR_NOMEM, "exa_mesh_create_boxes: device allocation failed");
   }
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
@@ -1173,7 +1212,7 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
   if (!ok) {
     cudaStreamSynchronize(st);
     mesh_free(m.get());
-    return fail(EXA_ERR_CUDA, "exa_mesh_create_nested: upload failed");
+    return fail(EXA_ERR_CUDA, "exa_mesh_create_boxes: upload failed");
   }
   m->boff[EXA_BC_OUTFLOW] = 0;
   m->nbfaces[EXA_BC_OUTFLOW] = (int)t.bcell.size();
@@ -1190,6 +1229,13 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
   EXA_CUDA(cudaStreamSynchronize(st));  // the host vectors go out of scope
   *out = m.release();
   return EXA_OK;
+}
+
+int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* offset, const double* size,
+                           const int* bc, int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out) {
+  if (nboxes < 1 || nboxes > 8) return fail(EXA_ERR_ARG, "exa_mesh_create_nested: 1 to 8 refined boxes");
+  const int level[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+  return exa_mesh_create_boxes(s, cells, offset, size, bc, nboxes, level, box_lo, box_hi, out);
 }
 
 int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,

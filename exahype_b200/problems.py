@@ -199,27 +199,50 @@ def refined_node_coordinates(dim, order, cells, box_lo, box_hi, offset=(0.0, 0.0
 
 def nested_node_coordinates(dim, order, cells, boxes, offset=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0)):
     """(ncells, b^dim, dim) node coordinates of a mesh made by
-    exa_mesh_create_nested: level by level, the unrefined cells of the
-    level's region (x fastest). boxes[k] = (lo, hi) in level-k cell
-    coordinates."""
+    exa_mesh_create_nested: boxes[k] = (lo, hi) in level-k cell coordinates."""
+    return boxes_node_coordinates(dim, order, cells, [(k, lo, hi) for k, (lo, hi) in enumerate(boxes)], offset, size)
+
+
+def box_levels(dim, cells, boxes):
+    """Per level: (r0, state) with r0 the bounding rectangle's lower corner
+    and state an array over it (z, y, x order) holding 0 outside the level's
+    region, 1 for a cell, 2 for a refined position; boxes = [(level, lo, hi)]."""
+    L = max(b[0] for b in boxes) + 2
     out = []
-    r0, r1 = [0] * dim, list(cells[:dim])
-    for lev in range(len(boxes) + 1):
-        f = 3 ** lev
-        dx = [size[d] / (cells[d] * f) for d in range(dim)]
-        ext = [r1[d] - r0[d] for d in range(dim)]
+    for lev in range(L):
+        if lev == 0:
+            r0, r1 = [0] * dim, list(cells[:dim])
+        else:
+            sub = [b for b in boxes if b[0] == lev - 1]
+            r0 = [min(3 * b[1][d] for b in sub) for d in range(dim)]
+            r1 = [max(3 * b[2][d] for b in sub) for d in range(dim)]
+        shape = tuple(r1[d] - r0[d] for d in reversed(range(dim)))
+        st = np.ones(shape, dtype=np.int8) if lev == 0 else np.zeros(shape, dtype=np.int8)
+        if lev > 0:
+            for b in boxes:
+                if b[0] == lev - 1:
+                    sl = tuple(slice(3 * b[1][d] - r0[d], 3 * b[2][d] - r0[d]) for d in reversed(range(dim)))
+                    st[sl] = 1
+        out.append([r0, st])
+    for b in boxes:
+        r0, st = out[b[0]]
+        sl = tuple(slice(b[1][d] - r0[d], b[2][d] - r0[d]) for d in reversed(range(dim)))
+        st[sl] = 2
+    return out
+
+
+def boxes_node_coordinates(dim, order, cells, boxes, offset=(0.0, 0.0, 0.0), size=(1.0, 1.0, 1.0)):
+    """(ncells, b^dim, dim) node coordinates of a mesh made by
+    exa_mesh_create_boxes: level by level, the cells x fastest over the
+    level's bounding rectangle. boxes = [(level, lo, hi)]."""
+    out = []
+    for lev, (r0, st) in enumerate(box_levels(dim, cells, boxes)):
+        ext = list(reversed(st.shape))
+        dx = [size[d] / (cells[d] * 3 ** lev) for d in range(dim)]
         off = [offset[d] + r0[d] * dx[d] for d in range(dim)] + [0.0] * (3 - dim)
         sz = [ext[d] * dx[d] for d in range(dim)] + [1.0] * (3 - dim)
         X = node_coordinates(dim, order, ext, off, sz)
-        if lev < len(boxes):
-            lo, hi = boxes[lev]
-            idx = np.indices(tuple(reversed(ext))).reshape(dim, -1)[::-1]  # (dim, ncells), x first
-            inbox = np.ones(idx.shape[1], dtype=bool)
-            for d in range(dim):
-                inbox &= (idx[d] + r0[d] >= lo[d]) & (idx[d] + r0[d] < hi[d])
-            X = X[~inbox]
-            r0, r1 = [3 * lo[d] for d in range(dim)], [3 * hi[d] for d in range(dim)]
-        out.append(X)
+        out.append(X[st.reshape(-1) == 1])
     return np.concatenate(out, axis=0)
 
 
@@ -234,11 +257,17 @@ def pulse_refined(dim, order, cells, box_lo, box_hi, seed=0):
 def pulse_nested(dim, order, cells, boxes, seed=0):
     """pulse_refined on a nested mesh (centre: the first box's centre plus a
     seeded offset U[-0.05, 0.05]^dim)."""
+    return pulse_boxes(dim, order, cells, [(k, lo, hi) for k, (lo, hi) in enumerate(boxes)], seed)
+
+
+def pulse_boxes(dim, order, cells, boxes, seed=0):
+    """pulse_refined on a mesh refined by boxes = [(level, lo, hi)] (centre:
+    the first box's centre plus a seeded offset U[-0.05, 0.05]^dim)."""
     rng = np.random.default_rng(seed)
-    box_lo, box_hi = boxes[0]
-    c = np.array([(box_lo[d] + box_hi[d]) / (2.0 * cells[d]) for d in range(dim)])
+    lev, box_lo, box_hi = boxes[0]
+    c = np.array([(box_lo[d] + box_hi[d]) / (2.0 * cells[d] * 3 ** lev) for d in range(dim)])
     c = c + rng.uniform(-0.05, 0.05, size=dim)
-    X = nested_node_coordinates(dim, order, cells, boxes)
+    X = boxes_node_coordinates(dim, order, cells, boxes)
     rho = 1.0 + 0.3 * np.exp(-_periodic_d2(X, c) / 0.01)
     vel = np.zeros(rho.shape + (3,))
     vel[..., :dim] = np.array([1.0, 0.5, 0.25][:dim])

@@ -212,6 +212,18 @@ int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double*
  * its region. exa_mesh_create_refined is the case nboxes = 1. */
 int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* offset, const double* size,
                            const int* bc, int nboxes, const int* box_lo, const int* box_hi, exa_mesh** out);
+/* The general form: box k refines the positions box_lo <= p < box_hi
+ * ([3k .. 3k+2]) of level box_level[k] (0..7; level-l coordinates span the
+ * whole domain, 3^l cells[d] per axis). Several boxes may refine one level
+ * (overlapping or touching boxes refine their union); the region of level
+ * l >= 1 is the union of the level-(l-1) boxes refined once, and every box
+ * must lie inside its level's region with one cell of margin. Solution
+ * order: level by level, the cells of each level x fastest over the
+ * level's bounding rectangle. exa_mesh_create_nested is the case
+ * box_level[k] = k. */
+int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* offset, const double* size,
+                          const int* bc, int nboxes, const int* box_level, const int* box_lo, const int* box_hi,
+                          exa_mesh** out);
 int exa_mesh_destroy(exa_mesh* m);
 int exa_mesh_num_cells(const exa_mesh* m, int* ncells);
 /* host <-> device solution, luh layout above, cells in x-fastest order */

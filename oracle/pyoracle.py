@@ -317,11 +317,13 @@ class RefinedMesh:
     Cell order: the unrefined coarse cells (x fastest), then the box's fine
     cells (x fastest)."""
 
-    def __init__(self, dim, order, cells, size, box_lo=None, box_hi=None, pde=0, impl="oracle", boxes=None, bc=-1):
-        """boxes: nested refined boxes, boxes[k] = (lo, hi) in level-k cell
-        coordinates (level k+1 is box k refined once); box_lo/box_hi: one box.
-        bc: -1 periodic or 0 outflow, one for all or per domain face
-        (boundaryConditions with outflow values on the level-0 cells'
+    def __init__(self, dim, order, cells, size, box_lo=None, box_hi=None, pde=0, impl="oracle", boxes=None, bc=-1,
+                 level_boxes=None):
+        """level_boxes: [(level, lo, hi)], the positions lo <= p < hi of that
+        level refined once (several boxes per level refine their union);
+        boxes: nested boxes, boxes[k] = (lo, hi) at level k; box_lo/box_hi:
+        one box. bc: -1 periodic or 0 outflow, one for all or per domain
+        face (boundaryConditions with outflow values on the level-0 cells'
         domain faces, ADERDGSolver.cpp:2893-2976)."""
         self.dim, self.order, self.pde = dim, order, pde
         self.linear = pde == 2
@@ -329,73 +331,80 @@ class RefinedMesh:
         self.impl = impl
         d = dim
         cells = list(cells)[:d]
-        boxes = [(list(lo)[:d], list(hi)[:d]) for lo, hi in (boxes if boxes is not None else [(box_lo, box_hi)])]
-        L = len(boxes) + 1
+        if level_boxes is None:
+            nest = boxes if boxes is not None else [(box_lo, box_hi)]
+            level_boxes = [(k, lo, hi) for k, (lo, hi) in enumerate(nest)]
+        level_boxes = [(int(l), list(lo)[:d], list(hi)[:d]) for l, lo, hi in level_boxes]
+        L = max(b[0] for b in level_boxes) + 2
         self.dxl = [[size[i] / cells[i] for i in range(d)]]  # a child's width: its parent's / 3
         for lev in range(1, L):
             self.dxl.append([x / 3.0 for x in self.dxl[-1]])
-        r0, r1 = [[0] * d], [list(cells)]
-        for lo, hi in boxes:
-            r0.append([3 * x for x in lo])
-            r1.append([3 * x for x in hi])
-        refined = lambda lev, c: lev + 1 < L and all(boxes[lev][0][i] <= c[i] < boxes[lev][1][i] for i in range(d))  # noqa: E731
-        onface = lambda lev, c: any(c[i] == boxes[lev][0][i] or c[i] == boxes[lev][1][i] - 1 for i in range(d))  # noqa: E731
-        # positions of a level's region, x fastest
-        region = lambda lev: [tuple(r0[lev][i] + t[d - 1 - i] for i in range(d))  # noqa: E731
-                              for t in np.ndindex(*[r1[lev][i] - r0[lev][i] for i in reversed(range(d))])]
+        bcs = [bc] * (2 * d) if isinstance(bc, int) else list(bc)
+        box_pos = lambda lo, hi, s=1: [tuple(s * lo[i] + t[d - 1 - i] for i in range(d))  # noqa: E731
+                                       for t in np.ndindex(*[s * (hi[i] - lo[i]) for i in reversed(range(d))])]
+        # state per level: position -> 1 (cell) or 2 (refined)
+        state = [dict() for _ in range(L)]
+        for c in box_pos([0] * d, cells):
+            state[0][c] = 1
+        for lev, lo, hi in level_boxes:
+            for c in box_pos(lo, hi, 3):
+                state[lev + 1][c] = 1
+        for lev, lo, hi in level_boxes:
+            for c in box_pos(lo, hi):
+                state[lev][c] = 2
+
+        def nbr(lev, c, i, s):
+            q = list(c)
+            q[i] += 1 if s else -1
+            if lev == 0 and bcs[2 * i] == -1:
+                q[i] %= cells[i]
+            return tuple(q)
+
+        order_key = lambda c: tuple(reversed(c))  # noqa: E731  x fastest
         self.cid = [dict() for _ in range(L)]
         self.level = []
         n = 0
         for lev in range(L):
-            for c in region(lev):
-                if not refined(lev, c):
+            for c in sorted(state[lev], key=order_key):
+                if state[lev][c] == 1:
                     self.cid[lev][c] = n
                     self.level.append(lev)
                     n += 1
         self.ncells = n
         self.aid = [dict() for _ in range(L)]
         for lev in range(L - 1):
-            for c in region(lev):
-                if refined(lev, c) and onface(lev, c):
+            for c in sorted(state[lev], key=order_key):
+                if state[lev][c] == 2 and any(state[lev].get(nbr(lev, c, i, s)) == 1 for i in range(d) for s in (0, 1)):
                     self.aid[lev][c] = n
                     n += 1
-        bcs = [bc] * (2 * d) if isinstance(bc, int) else list(bc)
+        slot = lambda lev, c: self.cid[lev].get(c, self.aid[lev].get(c, -1))  # noqa: E731
         self.pairs, self.restr, self.prol, self.bnd = [], [], [], []
         for lev in range(L):
-            for c in region(lev):
-                rc = refined(lev, c)
-                me = self.aid[lev].get(c, -1) if rc else self.cid[lev][c]  # -1: refined, inside its box
+            for c in sorted(state[lev], key=order_key):
+                sc = state[lev][c]
+                me = slot(lev, c)
                 for i in range(d):
-                    q = list(c)
-                    q[i] += 1
-                    if lev == 0 and bcs[2 * i] != -1:
-                        if c[i] == 0:
-                            self.bnd.append((me, 2 * i))
-                        if q[i] == cells[i]:
-                            self.bnd.append((me, 2 * i + 1))
-                    elif lev == 0:
-                        q[i] %= cells[i]
-                    q = tuple(q)
-                    if q[i] < r1[lev][i]:
-                        rq = refined(lev, q)
-                        if not (rc and rq):
-                            self.pairs.append((me, self.aid[lev][q] if rq else self.cid[lev][q], i))
-                    if lev == 0 or rc:
+                    q = nbr(lev, c, i, 1)
+                    sq = state[lev].get(q, 0)
+                    if sq and not (sc == 2 and sq == 2):
+                        self.pairs.append((me, slot(lev, q), i))
+                    if sc != 1:
                         continue
-                    sub = [c[e] % 3 for e in range(d) if e != i]
-                    parent = tuple(x // 3 for x in c)
                     for side in (0, 1):
-                        if c[i] != (r0[lev][i] if side == 0 else r1[lev][i] - 1):
+                        r = nbr(lev, c, i, side)
+                        if state[lev].get(r, 0):
                             continue
                         face = 2 * i + side
+                        if lev == 0:
+                            self.bnd.append((me, face))
+                            continue
+                        sub = [c[e] % 3 for e in range(d) if e != i]
                         desc = n
                         n += 1
                         self.pairs.append((desc, me, i) if side == 0 else (me, desc, i))
-                        self.restr.append((me, face, self.aid[lev - 1][parent], face, sub))
-                        cn = list(parent)
-                        cn[i] += -1 if side == 0 else 1
-                        dface = 2 * i + 1 if side == 0 else 2 * i
-                        self.prol.append((self.cid[lev - 1][tuple(cn)], dface, desc, dface, sub))
+                        self.restr.append((me, face, self.aid[lev - 1][tuple(x // 3 for x in c)], face, sub))
+                        dface = 2 * i + 1 - side
+                        self.prol.append((self.cid[lev - 1][tuple(x // 3 for x in r)], dface, desc, dface, sub))
         nslot = n
         K = self.K
         self.nslot = nslot

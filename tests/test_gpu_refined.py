@@ -224,3 +224,43 @@ def test_nested_mesh_fused_vs_oracle(eb, boxes, w):
     assert close(sa["t"], sb["t"]) and close(sa["dt"], sb["dt"])
     fa, fb = m.fused_state(), o.fused_state()
     assert close(fa["predictor_dt"], fb["predictor_dt"]) and fa["reruns"] == fb["reruns"]
+
+
+BOXES = [(2, 3, (12, 12), [(0, (2, 2), (5, 5)), (0, (7, 6), (10, 10)), (1, (8, 8), (12, 12))], 6, 0, -1),
+         (2, 5, (12, 9), [(0, (2, 2), (5, 4)), (0, (5, 2), (7, 7)), (0, (8, 3), (10, 6))], 4, 2, 0),
+         (3, 3, (6, 5, 5), [(0, (1, 1, 1), (3, 3, 3)), (0, (3, 2, 2), (5, 4, 4))], 3, 6, -1)]
+
+
+@pytest.mark.parametrize("dim,N,cells,boxes,steps,variant,bc", BOXES)
+def test_boxes_mesh_vs_oracle(eb, dim, N, cells, boxes, steps, variant, bc):
+    """several refined boxes per level (disjoint, touching and overlapping:
+    their union is refined), one level refined again, outflow or periodic"""
+    from exahype_b200 import problems
+    u = problems.pulse_boxes(dim, N, cells, boxes, seed=9)
+    s = eb.Solver(dim, N)
+    s.variant = variant
+    m = eb.Mesh.boxes(s, cells, [0.0] * dim, [1.0] * dim, boxes, bc=bc)
+    o = pyoracle.RefinedMesh(dim, N, cells, [1.0] * dim, level_boxes=boxes, bc=bc)
+    assert m.ncells == o.ncells == u.shape[0]
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init(0.0)
+    o.init(0.0)
+    assert m.state()["dt"] == o.state()["dt"]
+    m.step(steps)
+    o.step(steps)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    sa, sb = m.state(), o.state()
+    assert sa["steps"] == sb["steps"] == steps and sa["picard_sweeps"] == sb["picard_sweeps"]
+    assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"]
+
+
+def test_boxes_mesh_arguments(eb):
+    s = eb.Solver(2, 3)
+    for boxes in ([(0, (0, 2), (5, 5))],                       # no margin to the domain
+                  [(0, (2, 2), (5, 5)), (1, (6, 6), (9, 9))],  # no margin inside level 1
+                  [(1, (8, 8), (12, 12))],                     # level 1 has no region
+                  [(0, (3, 3), (3, 5))]):                      # empty
+        with pytest.raises(eb.ExaError):
+            eb.Mesh.boxes(s, (12, 12), [0.0, 0.0], [1.0, 1.0], boxes)

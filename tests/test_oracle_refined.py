@@ -62,6 +62,22 @@ def test_nested_oracle_vs_reference_kernels():
     assert sa["picard_sweeps"] == sb["picard_sweeps"]
 
 
+def test_boxes_oracle_vs_reference_kernels():
+    if not pyoracle.ref_available(2):
+        pytest.skip("compiled reference kernels not built")
+    from exahype_b200 import problems
+    cells, boxes = (12, 12), [(0, (2, 2), (5, 5)), (0, (7, 6), (10, 10)), (1, (8, 8), (12, 12))]
+    u = problems.pulse_boxes(2, 3, cells, boxes, seed=9)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.RefinedMesh(2, 3, cells, [1.0, 1.0], level_boxes=boxes, impl=impl)
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(2)
+        res.append(m.get_solution())
+    assert np.linalg.norm(res[0] - res[1]) / np.linalg.norm(res[1]) < 1e-12
+
+
 def test_refined_oracle_free_stream():
     m = pyoracle.RefinedMesh(2, 3, (9, 9), [1.0, 1.0], (3, 3), (6, 6))
     u = np.zeros((m.ncells, 16, 5))
