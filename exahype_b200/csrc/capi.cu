@@ -969,7 +969,7 @@ struct NestedTopo {
   std::vector<int> level;                              // per cell
   std::vector<int> pos;                                // per cell: position in its level's grid (3 ints)
   std::vector<int> fl, fr, fd;                          // Riemann pairs
-  std::vector<int> bcell, bface;                        // outflow faces of level-0 cells
+  std::vector<int> bcell, bface, bkind;                 // domain faces of level-0 cells and their kinds
   std::vector<int> rf, rc, ridx, pf, pc, pidx;          // restriction / prolongation items
 };
 
@@ -1101,9 +1101,10 @@ static const char* boxes_topology(int dim, const int* cells, const int* bc, int 
           int r[3];
           nb_pos(l, p, d, s, r);
           if (state(l, r) != 0) continue;
-          if (l == 0) {  // a domain face (outflow)
+          if (l == 0) {  // a domain face
             t.bcell.push_back(me);
             t.bface.push_back(2 * d + s);
+            t.bkind.push_back(bc[2 * d + s]);
             continue;
           }
           // a cell on its region's face: a descendant across it (the coarse
@@ -1152,8 +1153,8 @@ int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* o
   for (int d = dim; d < 3; d++) m->geo.dx[d] = 1.0;
   for (int f = 0; f < 6; f++) {
     const int k = bc && f < 2 * dim ? bc[f] : EXA_BC_PERIODIC;
-    if (k != EXA_BC_PERIODIC && k != EXA_BC_OUTFLOW)
-      return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: boundaries must be periodic or outflow");
+    if (k != EXA_BC_PERIODIC && k != EXA_BC_OUTFLOW && k != EXA_BC_REFLECTIVE)
+      return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: unknown boundary kind");
     if (f % 2 == 1 && (k == EXA_BC_PERIODIC) != (m->bc[f - 1] == EXA_BC_PERIODIC))
       return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: periodic must be set on both faces of an axis");
     if (k != EXA_BC_PERIODIC && s->k.linear)
@@ -1163,6 +1164,17 @@ int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* o
   NestedTopo t;
   if (const char* err = boxes_topology(dim, cells, m->bc, nboxes, box_level, box_lo, box_hi, t))
     return fail(EXA_ERR_ARG, std::string("exa_mesh_create_boxes: ") + err);
+  {  // domain faces grouped by kind: outflow, then reflective
+    std::vector<int> bc2, bf2;
+    for (int kd = 0; kd < 2; kd++) {
+      m->boff[kd] = (int)bc2.size();
+      for (size_t i = 0; i < t.bcell.size(); i++)
+        if (t.bkind[i] == kd) bc2.push_back(t.bcell[i]), bf2.push_back(t.bface[i]);
+      m->nbfaces[kd] = (int)bc2.size() - m->boff[kd];
+    }
+    t.bcell.swap(bc2);
+    t.bface.swap(bf2);
+  }
   const int L = t.L;
   m->ncells = t.ncells;
   m->nfaces = (int)t.fl.size();
@@ -1214,8 +1226,7 @@ int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* o
     mesh_free(m.get());
     return fail(EXA_ERR_CUDA, "exa_mesh_create_boxes: upload failed");
   }
-  m->boff[EXA_BC_OUTFLOW] = 0;
-  m->nbfaces[EXA_BC_OUTFLOW] = (int)t.bcell.size();
+
   m->geo.inst = m->ref.inst;
   m->geo.inst_dx = m->ref.inst_dx;
   m->ref.level = t.level;

@@ -202,8 +202,9 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
 int exa_mesh_create_refined(const exa_solver* s, const int* cells, const double* offset, const double* size,
                             const int* box_lo, const int* box_hi, exa_mesh** out);
 /* The same with nboxes nested refined boxes (1..8) and optional domain
- * boundaries bc[2d] (NULL: periodic; EXA_BC_PERIODIC or EXA_BC_OUTFLOW per
- * axis, outflow for nonlinear PDEs only): box k (box_lo/box_hi
+ * boundaries bc[2d] (NULL: periodic; EXA_BC_PERIODIC on both faces of an
+ * axis, or EXA_BC_OUTFLOW / EXA_BC_REFLECTIVE per face, those for nonlinear
+ * PDEs only): box k (box_lo/box_hi
  * [3k .. 3k+2]) is given in the cell coordinates of level k (level 0 the
  * coarse grid, level k+1 the box k refined once, whose coordinates run over
  * the whole domain at that level: 3^(k+1) cells[d]) and must lie inside

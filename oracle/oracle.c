@@ -368,6 +368,26 @@ void orc_boundary_face(const orc_solver* s, double* FIn, const double* QIn, cons
     orc_riemann(s, FIn, FOut, QIn, QOut, dir);
 }
 
+/* Reflective walls: the boundaryValues of the reference's Euler demonstrator
+ * (Demonstrators/EulerADERDG/MyEulerSolver_ADERDG.cpp:82-87) -- the inside
+ * state with its normal momentum negated and that state's normal flux --
+ * then the Rusanov flux as in orc_boundary_face. Euler only. */
+void orc_boundary_face_reflective(const orc_solver* s, double* FIn, const double* QIn, int faceIndex) {
+  geo g = mkgeo(s);
+  const int dir = (faceIndex - faceIndex % 2) / 2;
+  double QOut[100 * 6], FOut[100 * 5], F[3 * 5];
+  for (int fn = 0; fn < g.F; fn++) {
+    for (int v = 0; v < g.nD; v++) QOut[fn * g.nD + v] = QIn[fn * g.nD + v];
+    QOut[fn * g.nD + 1 + dir] = -QOut[fn * g.nD + 1 + dir];
+    orc_flux(s, QOut + fn * g.nD, F);
+    for (int v = 0; v < g.nV; v++) FOut[fn * g.nV + v] = F[5 * dir + v];
+  }
+  if (faceIndex % 2 == 0)
+    orc_riemann(s, FOut, FIn, QOut, QIn, dir);
+  else
+    orc_riemann(s, FIn, FOut, QIn, QOut, dir);
+}
+
 /* surfaceIntegralNonlinear: 3d/surfaceIntegralNonlinear.cpph:21-90, 2d:26-67 */
 void orc_surface_integral(const orc_solver* s, double* lduh, const double* lFhbnd, const double* dx) {
   geo g = mkgeo(s);

@@ -38,6 +38,7 @@ void orc_volume_integral(const orc_solver* s, double* lduh, const double* lFhi, 
 void orc_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, const double* QR, int dir);
 void orc_boundary_face(const orc_solver* s, double* FIn, const double* QIn, const double* centre,
                        const double* size, double t, double dt, int faceIndex);
+void orc_boundary_face_reflective(const orc_solver* s, double* FIn, const double* QIn, int faceIndex);
 void orc_surface_integral(const orc_solver* s, double* lduh, const double* lFhbnd, const double* dx);
 void orc_solution_update(const orc_solver* s, double* luh, const double* lduh, double dt);
 double orc_stable_dt(const orc_solver* s, const double* luh, const double* dx);

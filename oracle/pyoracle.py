@@ -203,8 +203,15 @@ class Kernels:
         self._l.orc_musclhancock(ctypes.byref(self._s), _p(new), _p(old), _p(dx), ctypes.c_double(dt))
         return new
 
-    def boundary_face(self, FIn, QIn, face_index, centre=(0.5, 0.5, 0.5), size=(0.1, 0.1, 0.1), t=0.0, dt=0.0):
+    def boundary_face(self, FIn, QIn, face_index, centre=(0.5, 0.5, 0.5), size=(0.1, 0.1, 0.1), t=0.0, dt=0.0,
+                      kind=0):
+        """kind 0: outflow values; 1: reflective walls (C restatement only)"""
         FIn = np.array(FIn, dtype=np.float64).reshape(-1)
+        if kind == 1:
+            self._l.orc_boundary_face_reflective(ctypes.byref(self._s), _p(FIn),
+                                                 _p(np.ascontiguousarray(QIn, dtype=np.float64).reshape(-1)),
+                                                 ctypes.c_int(face_index))
+            return FIn
         c = np.ascontiguousarray(np.resize(np.asarray(centre, dtype=np.float64), 3))
         s = np.ascontiguousarray(np.resize(np.asarray(size, dtype=np.float64), 3))
         self._call("boundary_face", _p(FIn), _p(np.ascontiguousarray(QIn, dtype=np.float64).reshape(-1)), _p(c),
@@ -322,9 +329,9 @@ class RefinedMesh:
         """level_boxes: [(level, lo, hi)], the positions lo <= p < hi of that
         level refined once (several boxes per level refine their union);
         boxes: nested boxes, boxes[k] = (lo, hi) at level k; box_lo/box_hi:
-        one box. bc: -1 periodic or 0 outflow, one for all or per domain
-        face (boundaryConditions with outflow values on the level-0 cells'
-        domain faces, ADERDGSolver.cpp:2893-2976)."""
+        one box. bc: -1 periodic, 0 outflow or 1 reflective, one for all or
+        per domain face (boundaryConditions on the level-0 cells' domain
+        faces, ADERDGSolver.cpp:2893-2976)."""
         self.dim, self.order, self.pde = dim, order, pde
         self.linear = pde == 2
         self.K = Kernels(dim, order, pde, impl)
@@ -335,7 +342,7 @@ class RefinedMesh:
             nest = boxes if boxes is not None else [(box_lo, box_hi)]
             level_boxes = [(k, lo, hi) for k, (lo, hi) in enumerate(nest)]
         level_boxes = [(int(l), list(lo)[:d], list(hi)[:d]) for l, lo, hi in level_boxes]
-        L = max(b[0] for b in level_boxes) + 2
+        L = max([b[0] + 2 for b in level_boxes] + [1])
         self.dxl = [[size[i] / cells[i] for i in range(d)]]  # a child's width: its parent's / 3
         for lev in range(1, L):
             self.dxl.append([x / 3.0 for x in self.dxl[-1]])
@@ -396,7 +403,7 @@ class RefinedMesh:
                             continue
                         face = 2 * i + side
                         if lev == 0:
-                            self.bnd.append((me, face))
+                            self.bnd.append((me, face, bcs[face]))
                             continue
                         sub = [c[e] % 3 for e in range(d) if e != i]
                         desc = n
@@ -480,8 +487,8 @@ class RefinedMesh:
                 fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1],
                                    self.Q[r, 2 * i], i)
             self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i] = fl, fr
-        for c, face in self.bnd:
-            self.Fb[c, face] = K.boundary_face(self.Fb[c, face], self.Q[c, face], face)
+        for c, face, kind in self.bnd:
+            self.Fb[c, face] = K.boundary_face(self.Fb[c, face], self.Q[c, face], face, kind=kind)
         for c in range(self.ncells):
             si = K.lin_surface_integral if self.linear else K.surface_integral
             du = si(self.du[c], self.Fb[c].reshape(-1), self._dx(c))
