@@ -319,6 +319,21 @@ class Mesh:
         self.dx = [size[i] / cells[i] for i in range(d)]
         return self
 
+    def regrid(self, boxes):
+        """replace the refinement (exa_mesh_regrid): boxes = [(level, lo,
+        hi)], may be empty; the data moves by copy, prolongation or
+        restriction, t and the step count are kept"""
+        lib = load()
+        nb = len(boxes)
+        lev = (ctypes.c_int * max(1, nb))(*[int(b[0]) for b in boxes])
+        lo = (ctypes.c_int * max(3, 3 * nb))(*sum((list(b[1]) + [0] * (3 - len(b[1])) for b in boxes), []))
+        hi = (ctypes.c_int * max(3, 3 * nb))(*sum((list(b[2]) + [1] * (3 - len(b[2])) for b in boxes), []))
+        _check(lib.exa_mesh_regrid(self._h, nb, lev, lo, hi), "exa_mesh_regrid")
+        self.boxes = [(int(b[0]), tuple(b[1]), tuple(b[2])) for b in boxes]
+        n = ctypes.c_int()
+        _check(lib.exa_mesh_num_cells(self._h, ctypes.byref(n)), "exa_mesh_num_cells")
+        self.ncells = n.value
+
     def __del__(self):
         try:
             if self._h:

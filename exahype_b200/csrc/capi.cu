@@ -479,6 +479,17 @@ __global__ void __launch_bounds__(256) count_flags_kernel(const int* __restrict_
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
 
+// dst cell to[k] = src cell from[k], per_cell doubles each
+__global__ void __launch_bounds__(256) copy_cells_kernel(double* __restrict__ dst, const double* __restrict__ src,
+                                                         size_t per_cell, int n, const int* __restrict__ to,
+                                                         const int* __restrict__ from) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)n * per_cell;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t k = i / per_cell, e = i - k * per_cell;
+    dst[(size_t)to[k] * per_cell + e] = src[(size_t)from[k] * per_cell + e];
+  }
+}
+
 // independent FP64 FMA chains: 8 per thread, `iters` rounds
 __global__ void __launch_bounds__(256) fp64_probe_kernel(double* out, int iters, double a, double b) {
   double x[8];
@@ -503,11 +514,28 @@ struct exa_solver {
   int variant = 0;  // predictor variant (set by exa_solver_autotune / exa_solver_set_variant)
 };
 
+// one level of a refined mesh on the host: the bounding rectangle [r0, r1)
+// of its region, per position 0 outside / 1 cell / 2 refined, and the cell
+// index (or -1)
+struct LevelMap {
+  std::array<int, 3> r0{}, r1{};
+  std::vector<unsigned char> st;
+  std::vector<int> cell;
+  bool inside(const int* p) const {
+    for (int d = 0; d < 3; d++)
+      if (p[d] < r0[d] || p[d] >= r1[d]) return false;
+    return true;
+  }
+  size_t at(const int* p) const {
+    return ((size_t)(p[2] - r0[2]) * (r1[1] - r0[1]) + (p[1] - r0[1])) * (r1[0] - r0[0]) + (p[0] - r0[0]);
+  }
+};
+
 struct exa_mesh {
   const exa_solver* s = nullptr;
   int dim = 0, cells[3] = {1, 1, 1}, ncells = 0, bc[6] = {0, 0, 0, 0, 0, 0};
   Geometry geo{};
-  double offset[3] = {0, 0, 0};
+  double offset[3] = {0, 0, 0}, size[3] = {1, 1, 1};
   double *luh = nullptr, *lduh = nullptr, *lQhbnd = nullptr, *lFhbnd = nullptr, *scal = nullptr;
   int *iters = nullptr, *fl = nullptr, *fr = nullptr, *fd = nullptr, *bcell = nullptr, *bface = nullptr;
   int nfaces = 0, nbfaces[3] = {0, 0, 0};  // boundary faces grouped by kind: outflow, reflective
@@ -551,6 +579,7 @@ struct exa_mesh {
     // each level's widths
     std::vector<int> level, pos;
     std::vector<double> ldx;
+    std::vector<LevelMap> maps;  // per level (for exa_mesh_regrid)
   } ref;
 };
 
@@ -971,6 +1000,7 @@ struct NestedTopo {
   std::vector<int> fl, fr, fd;                          // Riemann pairs
   std::vector<int> bcell, bface, bkind;                 // domain faces of level-0 cells and their kinds
   std::vector<int> rf, rc, ridx, pf, pc, pidx;          // restriction / prolongation items
+  std::vector<LevelMap> maps;                           // per level
 };
 
 // A refined mesh from boxes: box k refines the positions lo_k <= p < hi_k
@@ -1130,6 +1160,16 @@ static const char* boxes_topology(int dim, const int* cells, const int* bc, int 
       }
     });
   t.nslots = n;
+  t.maps.resize(L);
+  for (int l = 0; l < L; l++) {
+    LevelMap& mp = t.maps[l];
+    mp.r0 = r0[l];
+    mp.r1 = r1[l];
+    mp.st = st[l];
+    mp.cell.assign(st[l].size(), -1);
+    for (size_t i = 0; i < st[l].size(); i++)
+      if (st[l][i] == 1) mp.cell[i] = slot[l][i];
+  }
   return nullptr;
 }
 }  // namespace
@@ -1137,9 +1177,9 @@ static const char* boxes_topology(int dim, const int* cells, const int* bc, int 
 int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* offset, const double* size,
                           const int* bc, int nboxes, const int* box_level, const int* box_lo, const int* box_hi,
                           exa_mesh** out) {
-  if (!s || !cells || !offset || !size || !box_level || !box_lo || !box_hi || !out)
+  if (!s || !cells || !offset || !size || !out || (nboxes > 0 && (!box_level || !box_lo || !box_hi)))
     return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: null argument");
-  if (nboxes < 1 || nboxes > 4096) return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: 1 to 4096 refined boxes");
+  if (nboxes < 0 || nboxes > 4096) return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: 0 to 4096 refined boxes");
   const int dim = s->k.dim, D2 = 2 * dim;
   std::unique_ptr<exa_mesh> m(new exa_mesh());
   m->s = s;
@@ -1148,6 +1188,7 @@ int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* o
     if (cells[d] < 3 || !(size[d] > 0)) return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: bad grid");
     m->cells[d] = cells[d];
     m->offset[d] = offset[d];
+    m->size[d] = size[d];
     m->geo.dx[d] = size[d] / cells[d];
   }
   for (int d = dim; d < 3; d++) m->geo.dx[d] = 1.0;
@@ -1232,6 +1273,7 @@ int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* o
   m->ref.level = t.level;
   m->ref.pos = t.pos;
   m->ref.ldx = ldx;
+  m->ref.maps = std::move(t.maps);
   EXA_CUDA(cudaMemsetAsync(m->luh, 0, n * P * nD * 8, st));
   EXA_CUDA(cudaMemsetAsync(m->lduh, 0, n * P * nV * 8, st));
   EXA_CUDA(cudaMemsetAsync(m->lQhbnd, 0, ns * D2 * F * nD * 8, st));
@@ -1623,6 +1665,121 @@ int exa_mesh_validate(exa_mesh* m, long long* nonfinite_cells) {
   sfree(cnt, m->stream);
   EXA_CUDA(cudaStreamSynchronize(m->stream));
   *nonfinite_cells = (long long)h;
+  return EXA_OK;
+}
+
+// Data of a regridded mesh (ADERDGSolver::prolongateVolumeData /
+// restrictVolumeData, exahype/solvers/ADERDGSolver.cpp:1437-1470,1694-1735,
+// volumeUnknownsProlongation / volumeUnknownsRestriction): a new cell that
+// was a cell keeps its data; one inside a coarser old cell gets that cell's
+// prolongation (levelDelta = the level difference); one covering finer old
+// cells gets the sum of their restrictions. Then the time stamp and step
+// count are kept, the admissible step is recomputed from the new solution
+// and the predictor runs on every cell.
+int exa_mesh_regrid(exa_mesh* m, int nboxes, const int* box_level, const int* box_lo, const int* box_hi) {
+  if (!m) return fail(EXA_ERR_ARG, "exa_mesh_regrid: null mesh");
+  if (!m->ref.on) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_regrid: create the mesh with exa_mesh_create_boxes");
+  if (!m->initialised) return fail(EXA_ERR_STATE, "exa_mesh_regrid: call exa_mesh_init first");
+  if (m->fused) return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_regrid: meshes in fused time stepping are not regridded");
+  exa_mesh* nm = nullptr;
+  int rc = exa_mesh_create_boxes(m->s, m->cells, m->offset, m->size, m->bc, nboxes, box_level, box_lo, box_hi, &nm);
+  if (rc) return rc;
+  std::unique_ptr<exa_mesh, int (*)(exa_mesh*)> guard(nm, exa_mesh_destroy);
+  const KernelSet& k = m->s->k;
+  const int dim = m->dim, oldL = (int)m->ref.maps.size();
+  std::vector<int> cto, cfrom, pf, pc, pld, pidx, rfine, rcoarse, rld, ridx;
+  for (int c = 0; c < nm->ncells; c++) {
+    const int l = nm->ref.level[c];
+    const int* p = &nm->ref.pos[3 * (size_t)c];
+    int lv = std::min(l, oldL - 1), a[3] = {p[0], p[1], p[2]};
+    for (int i = lv; i < l; i++)
+      for (int d = 0; d < dim; d++) a[d] /= 3;
+    // the finest old level whose region holds this position's ancestor
+    while (lv > 0 && !(m->ref.maps[lv].inside(a) && m->ref.maps[lv].st[m->ref.maps[lv].at(a)] != 0)) {
+      lv--;
+      for (int d = 0; d < dim; d++) a[d] /= 3;
+    }
+    const LevelMap& om = m->ref.maps[lv];
+    const unsigned char sa = om.st[om.at(a)];
+    if (sa == 1 && lv == l) {  // the same cell
+      cto.push_back(c);
+      cfrom.push_back(om.cell[om.at(a)]);
+    } else if (sa == 1) {  // inside a coarser old cell
+      const int ld = l - lv;
+      int f = 1;
+      for (int i = 0; i < ld; i++) f *= 3;
+      pf.push_back(c);
+      pc.push_back(om.cell[om.at(a)]);
+      pld.push_back(ld);
+      for (int d = 0; d < 3; d++) pidx.push_back(d < dim ? p[d] - a[d] * f : 0);
+    } else {  // refined in the old mesh: the finer old cells inside it
+      for (int l2 = l + 1; l2 < oldL; l2++) {
+        const LevelMap& fm = m->ref.maps[l2];
+        int f = 1;
+        for (int i = l; i < l2; i++) f *= 3;
+        int q0[3] = {0, 0, 0}, q1[3] = {1, 1, 1};
+        for (int d = 0; d < dim; d++) q0[d] = std::max(p[d] * f, fm.r0[d]), q1[d] = std::min((p[d] + 1) * f, fm.r1[d]);
+        int q[3];
+        for (q[2] = q0[2]; q[2] < q1[2]; q[2]++)
+          for (q[1] = q0[1]; q[1] < q1[1]; q[1]++)
+            for (q[0] = q0[0]; q[0] < q1[0]; q[0]++) {
+              if (fm.st[fm.at(q)] != 1) continue;
+              rfine.push_back(fm.cell[fm.at(q)]);
+              rcoarse.push_back(c);
+              rld.push_back(l2 - l);
+              for (int d = 0; d < 3; d++) ridx.push_back(d < dim ? q[d] - p[d] * f : 0);
+            }
+      }
+    }
+  }
+  // device lists (one allocation), then the transfers on the new stream
+  // once the old stream is idle
+  std::vector<int> all;
+  auto put = [&](const std::vector<int>& v) {
+    const size_t off = all.size();
+    all.insert(all.end(), v.begin(), v.end());
+    return off;
+  };
+  const size_t o_cto = put(cto), o_cfrom = put(cfrom), o_pf = put(pf), o_pc = put(pc), o_pld = put(pld),
+               o_pidx = put(pidx), o_rf = put(rfine), o_rc = put(rcoarse), o_rld = put(rld), o_ridx = put(ridx);
+  int* dl = nullptr;
+  if (!salloc(&dl, std::max<size_t>(1, all.size()) * 4, nm->stream)) {
+    cudaGetLastError();
+    return fail(EXA_ERR_NOMEM, "exa_mesh_regrid: device allocation failed");
+  }
+  EXA_CUDA(cudaStreamSynchronize(m->stream));
+  if (!all.empty()) EXA_CUDA(cudaMemcpyAsync(dl, all.data(), all.size() * 4, cudaMemcpyHostToDevice, nm->stream));
+  const size_t per = (size_t)k.P * (k.nvar + k.npar);
+  if (!cto.empty()) {
+    copy_cells_kernel<<<std::min<size_t>((cto.size() * per + 255) / 256, 148 * 16), 256, 0, nm->stream>>>(
+        nm->luh, m->luh, per, (int)cto.size(), dl + o_cto, dl + o_cfrom);
+    EXA_LAUNCHED();
+  }
+  rc = k.amr_volume(nm->luh, m->luh, (int)pf.size(), dl + o_pf, dl + o_pc, dl + o_pld, dl + o_pidx, 0, nm->stream);
+  if (!rc)
+    rc = k.amr_volume(nm->luh, m->luh, (int)rfine.size(), dl + o_rf, dl + o_rc, dl + o_rld, dl + o_ridx, 1,
+                      nm->stream);
+  if (!rc && cudaMemcpyAsync(nm->scal, m->scal, 8 * 8, cudaMemcpyDeviceToDevice, nm->stream) != cudaSuccess)
+    rc = fail(EXA_ERR_CUDA, "exa_mesh_regrid: copy failed");
+  if (!rc && cudaMemcpyAsync(nm->sweeps, m->sweeps, 8, cudaMemcpyDeviceToDevice, nm->stream) != cudaSuccess)
+    rc = fail(EXA_ERR_CUDA, "exa_mesh_regrid: copy failed");
+  if (!rc) {  // the new admissible step from the transferred solution, then the predictor
+    level_reset_kernel<<<1, 1, 0, nm->stream>>>(nm->ref.lv, nm->ref.nlev);
+    EXA_LAUNCHED();
+    rc = k.corrector(nm->luh, nullptr, nullptr, nullptr, mesh_dt_min(nm), nm->geo, nm->ncells, nullptr, 0, nullptr,
+                     nm->stream);
+  }
+  if (!rc) {
+    level_take_kernel<<<1, 1, 0, nm->stream>>>(nm->scal, nm->ref.lv, nm->ref.nlev);
+    EXA_LAUNCHED();
+    rc = mesh_predict(nm);
+  }
+  cudaStreamSynchronize(nm->stream);  // the old arrays are read until here
+  sfree(dl, nm->stream);
+  if (rc) return rc;
+  nm->initialised = true;
+  nm->profiling = m->profiling;
+  std::swap(*m, *nm);  // the caller's handle now holds the new mesh; the guard frees the old one
   return EXA_OK;
 }
 

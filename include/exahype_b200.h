@@ -225,6 +225,17 @@ int exa_mesh_create_nested(const exa_solver* s, const int* cells, const double* 
 int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* offset, const double* size,
                           const int* bc, int nboxes, const int* box_level, const int* box_lo, const int* box_hi,
                           exa_mesh** out);
+/* Static AMR between steps: replaces the refinement of a mesh made by
+ * exa_mesh_create_boxes (nboxes may be 0: the coarse grid alone) by the
+ * given boxes. A cell of the new mesh that was a cell keeps its data, one
+ * inside a coarser old cell gets that cell's prolongation, one covering
+ * finer old cells the sum of their restrictions (prolongateVolumeData /
+ * restrictVolumeData, exahype/solvers/ADERDGSolver.cpp:1437-1470,1694-1735).
+ * The time stamp and step count are kept; the admissible step is recomputed
+ * from the new solution and the predictor runs on every cell. The handle
+ * stays valid; the mesh's stream (exa_mesh_stream) and cell count change.
+ * Not for meshes in fused time stepping. Synchronises the old stream. */
+int exa_mesh_regrid(exa_mesh* m, int nboxes, const int* box_level, const int* box_lo, const int* box_hi);
 int exa_mesh_destroy(exa_mesh* m);
 int exa_mesh_num_cells(const exa_mesh* m, int* ncells);
 /* host <-> device solution, luh layout above, cells in x-fastest order */

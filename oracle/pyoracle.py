@@ -336,6 +336,7 @@ class RefinedMesh:
         self.linear = pde == 2
         self.K = Kernels(dim, order, pde, impl)
         self.impl = impl
+        self._args = (dim, order, cells, size, pde, impl, bc)
         d = dim
         cells = list(cells)[:d]
         if level_boxes is None:
@@ -367,6 +368,7 @@ class RefinedMesh:
                 q[i] %= cells[i]
             return tuple(q)
 
+        self.lstate = state
         order_key = lambda c: tuple(reversed(c))  # noqa: E731  x fastest
         self.cid = [dict() for _ in range(L)]
         self.level = []
@@ -423,6 +425,52 @@ class RefinedMesh:
 
     def _dx(self, c):
         return self.dxl[self.level[c]]
+
+    def regrid(self, level_boxes):
+        """static AMR between steps, restating exa_mesh_regrid's data
+        transfer with the reference's AMR operators: a cell that stays keeps
+        its data, a new cell inside a coarser old cell gets that cell's
+        volume prolongation, one covering finer old cells the sum of their
+        volume restrictions (ADERDGSolver.cpp:1437-1470,1694-1735); t and the
+        step count are kept, the step size recomputed, the predictor rerun"""
+        dim, order, cells, size, pde, impl, bc = self._args
+        new = RefinedMesh(dim, order, cells, size, pde=pde, impl=impl, bc=bc, level_boxes=level_boxes)
+        K, d = self.K, self.dim
+        npar = K.ndata - K.nvar
+        old_pos = [None] * self.ncells
+        for lev, ids in enumerate(self.cid):
+            for c, i in ids.items():
+                old_pos[i] = (lev, c)
+        oldL = len(self.lstate)
+        for lev, ids in enumerate(new.cid):
+            for p, i in ids.items():
+                lv = min(lev, oldL - 1)
+                a = tuple(x // 3 ** (lev - lv) for x in p)
+                while lv > 0 and self.lstate[lv].get(a, 0) == 0:
+                    lv -= 1
+                    a = tuple(x // 3 for x in a)
+                sa = self.lstate[lv][a]
+                if sa == 1 and lv == lev:
+                    new.u[i] = self.u[self.cid[lv][a]]
+                elif sa == 1:
+                    ld = lev - lv
+                    sub = [p[e] - a[e] * 3 ** ld for e in range(d)]
+                    new.u[i] = amr("volume_prolongation", d, order, K.nvar, npar, ld, sub,
+                                   coarse=self.u[self.cid[lv][a]], impl=impl).reshape(new.u[i].shape)
+                else:
+                    acc = np.zeros(new.u[i].size)
+                    for j, (l2, q) in enumerate(old_pos):
+                        if l2 <= lev or any(q[e] // 3 ** (l2 - lev) != p[e] for e in range(d)):
+                            continue
+                        sub = [q[e] - p[e] * 3 ** (l2 - lev) for e in range(d)]
+                        acc = amr("volume_restriction", d, order, K.nvar, npar, l2 - lev, sub, coarse=acc,
+                                  fine=self.u[j], impl=impl)
+                    new.u[i] = acc.reshape(new.u[i].shape)
+        new.t, new.steps, new.sweeps = self.t, self.steps, self.sweeps
+        new.fused = False
+        new.dt = new._stable()
+        new._predict()
+        self.__dict__.update(new.__dict__)
 
     def set_solution(self, u):
         self.u = np.array(u, dtype=np.float64).reshape(self.u.shape)

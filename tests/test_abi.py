@@ -26,7 +26,7 @@ def test_header_declares_the_api():
                      "exa_volume_unknowns_prolongation", "exa_volume_unknowns_restriction",
                      "exa_face_unknowns_prolongation", "exa_face_unknowns_restriction", "exa_plot_vertices",
                      "exa_mesh_write_vtk", "exa_mesh_step_io", "exa_mesh_init_fused", "exa_mesh_fused_state",
-                     "exa_mesh_create_refined", "exa_mesh_create_nested", "exa_mesh_write_vtk_legendre", "exa_lmesh_write_vtk", "exa_mesh_validate", "exa_mesh_create_boxes"):
+                     "exa_mesh_create_refined", "exa_mesh_create_nested", "exa_mesh_write_vtk_legendre", "exa_lmesh_write_vtk", "exa_mesh_validate", "exa_mesh_create_boxes", "exa_mesh_regrid"):
         assert required in names
 
 

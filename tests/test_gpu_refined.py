@@ -296,3 +296,52 @@ def test_reflective_walls_vs_oracle(eb, boxes, bc):
     assert np.isfinite(b).all()
     assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
     assert m.state()["picard_sweeps"] == o.state()["picard_sweeps"]
+
+
+@pytest.mark.parametrize("dim,N,cells,seq", [
+    (2, 3, (9, 9), [[(0, (3, 3), (6, 6))], [(0, (4, 3), (7, 7)), (1, (13, 11), (18, 17))], [],
+                    [(0, (2, 2), (8, 5))]]),
+    (3, 3, (5, 5, 5), [[], [(0, (1, 1, 1), (3, 3, 3))], [(0, (2, 2, 2), (4, 4, 4)), (1, (7, 7, 7), (11, 10, 10))]])])
+def test_regrid_vs_oracle(eb, dim, N, cells, seq):
+    """static AMR between steps: refine, move, coarsen and refine twice;
+    every transfer (copy, prolongation over one or two levels, restriction
+    of one or two finer levels) against the oracle's restatement"""
+    from exahype_b200 import problems
+    s = eb.Solver(dim, N)
+    u = problems.pulse_boxes(dim, N, cells, seq[0], seed=12) if seq[0] else \
+        (problems.gaussian_pulse_2d(N, cells, seed=12)[0] if dim == 2 else problems.gaussian_pulses_3d(N, cells, seed=12)[0])
+    m = eb.Mesh.boxes(s, cells, [0.0] * dim, [1.0] * dim, seq[0])
+    o = pyoracle.RefinedMesh(dim, N, cells, [1.0] * dim, level_boxes=seq[0])
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init(0.0)
+    o.init(0.0)
+    close = lambda x, y: abs(x - y) <= 1e-13 * abs(y)  # noqa: E731
+    for boxes in seq[1:] + [seq[0]]:
+        m.step(2)
+        o.step(2)
+        m.regrid(boxes)
+        o.regrid(boxes)
+        assert m.ncells == o.ncells
+        a, b = m.get_solution(), o.get_solution()
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+        sa, sb = m.state(), o.state()
+        assert sa["steps"] == sb["steps"] and sa["picard_sweeps"] == sb["picard_sweeps"]
+        assert close(sa["t"], sb["t"]) and close(sa["dt"], sb["dt"])
+
+
+def test_regrid_keeps_a_constant_state(eb):
+    s = eb.Solver(2, 5)
+    m = eb.Mesh.boxes(s, (9, 9), [0.0, 0.0], [1.0, 1.0], [])
+    u = np.zeros(m.solution_shape)
+    u[..., 0], u[..., 1], u[..., 4] = 1.0, 0.3, 2.5
+    m.set_solution(u)
+    m.init(0.0)
+    for boxes in ([(0, (3, 3), (6, 6)), (1, (10, 10), (17, 17))], [(0, (2, 4), (5, 7))], []):
+        m.regrid(boxes)
+        m.step(1)
+        v = m.get_solution()
+        assert np.abs(v[..., 0] - 1.0).max() < 1e-10 and np.abs(v[..., 1] - 0.3).max() < 1e-10
+    with pytest.raises(eb.ExaError):
+        m.regrid([(0, (0, 0), (3, 3))])  # no margin
+    assert m.validate() == 0

@@ -78,6 +78,27 @@ def test_boxes_oracle_vs_reference_kernels():
     assert np.linalg.norm(res[0] - res[1]) / np.linalg.norm(res[1]) < 1e-12
 
 
+def test_regrid_oracle_vs_reference_kernels():
+    """the regrid transfers through the C restatement's and the reference's
+    compiled amrRoutines agree"""
+    if not pyoracle.ref_available(2):
+        pytest.skip("compiled reference kernels not built")
+    from exahype_b200 import problems
+    b1, b2 = [(0, (3, 3), (6, 6))], [(0, (4, 3), (7, 7)), (1, (13, 11), (18, 17))]
+    u = problems.pulse_boxes(2, 3, (9, 9), b1, seed=12)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.RefinedMesh(2, 3, (9, 9), [1.0, 1.0], level_boxes=b1, impl=impl)
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(1)
+        m.regrid(b2)
+        m.step(1)
+        m.regrid([])
+        res.append(m.get_solution())
+    assert np.linalg.norm(res[0] - res[1]) / np.linalg.norm(res[1]) < 1e-12
+
+
 def test_refined_oracle_free_stream():
     m = pyoracle.RefinedMesh(2, 3, (9, 9), [1.0, 1.0], (3, 3), (6, 6))
     u = np.zeros((m.ncells, 16, 5))
