@@ -512,6 +512,16 @@ def run_refined_workload(a, world, dev, rank):
            "phase_ms_per_step": {n: v[0] / k for n, v in ph.items()},
            "picard_sweeps_per_step": (m.state()["picard_sweeps"] - st0["picard_sweeps"]) / k,
            "timing": "exa_mesh_step(k) on the refined mesh, CUDA events on the mesh stream"}
+    # one regrid (exa_mesh_regrid): the refined box moved by 3 coarse cells
+    # along x -- host topology, copies, prolongations, restrictions, the new
+    # step size and the predictor of every cell; host wall clock
+    m.synchronize()
+    t0 = time.perf_counter()
+    m.regrid([(0, (12, 9, 9), (21, 18, 18))])
+    m.synchronize()
+    out["regrid"] = {"ms": (time.perf_counter() - t0) * 1e3, "cells_after": m.ncells,
+                     "what": "the central 9^3 refined box moved by 3 coarse cells along x (host wall clock, "
+                             "topology build, data transfer, new step size and predictor included)"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         sys.path.insert(0, os.path.join(REPO, "oracle"))
         import pyoracle
