@@ -651,3 +651,62 @@ class Batch:
         h = ctypes.c_void_p()
         _check(load().exa_batch_stream(self._h, ctypes.byref(h)), "exa_batch_stream")
         return h.value or 0
+
+
+def cell_positions(mesh):
+    """(level, position) of every cell of a mesh made by Mesh.boxes / nested /
+    refined, in the solution's cell order (the same rule as
+    exa_mesh_create_boxes: level by level, x fastest over each level's
+    bounding rectangle)."""
+    from . import problems
+    d = mesh.solver.dim
+    out = []
+    boxes = getattr(mesh, "boxes", None)
+    for lev, (r0, st) in enumerate(problems.box_levels(d, mesh.cells, boxes) if boxes else
+                                   [[[0] * d, np.ones(tuple(reversed(mesh.cells[:d])), dtype=np.int8)]]):
+        idx = np.argwhere(st == 1)  # (z, y, x) order, x fastest
+        for t in idx:
+            out.append((lev, tuple(int(r0[i] + t[d - 1 - i]) for i in range(d))))
+    return out
+
+
+def adapt_boxes(mesh, flags, max_level):
+    """The refinement of a mesh after a refinement criterion, as boxes for
+    Mesh.regrid: the cells with flags[c] set (refinementCriterion ->
+    Refine, evaluated by the caller per cell) below max_level are refined,
+    refined positions that still hold a flagged finer cell stay refined, and
+    coarser levels are refined around every refined position so that each
+    keeps one cell of margin inside its level's region (the reference's
+    spacetree keeps the same 2:1-like balance with its helper cells);
+    positions within one cell of the domain boundary are never refined.
+    Returns [(level, lo, hi)] with one box per run of refined positions
+    along x."""
+    d = mesh.solver.dim
+    cells = list(mesh.cells[:d])
+    pos = cell_positions(mesh)
+    F = [set() for _ in range(max_level)]
+    for (lev, p), f in zip(pos, flags):
+        if f and lev < max_level:
+            F[lev].add(p)
+        for up in range(1, lev + 1):  # flagged or not: a finer cell's ancestors stay refined if it is flagged
+            if f and lev - up < max_level:
+                F[lev - up].add(tuple(x // 3 ** up for x in p))
+    # margins: every refined position at level l needs its neighbourhood
+    # inside level l's region, i.e. the parents of that neighbourhood refined
+    nbh = [tuple(o) for o in np.ndindex(*([3] * d))]
+    for lev in range(max_level - 1, 0, -1):
+        for p in list(F[lev]):
+            for o in nbh:
+                F[lev - 1].add(tuple((p[i] + o[i] - 1) // 3 for i in range(d)))
+    F[0] = {p for p in F[0] if all(1 <= p[i] <= cells[i] - 2 for i in range(d))}
+    for lev in range(1, max_level):  # drop what lost its region
+        region = F[lev - 1]
+        F[lev] = {p for p in F[lev] if all(tuple((p[i] + o[i] - 1) // 3 for i in range(d)) in region for o in nbh)}
+    boxes = []
+    for lev in range(max_level):
+        for p in sorted(F[lev], key=lambda c: tuple(reversed(c))):
+            if boxes and boxes[-1][0] == lev and boxes[-1][2][0] == p[0] and list(boxes[-1][1][1:]) == list(p[1:]):
+                boxes[-1][2][0] = p[0] + 1
+            else:
+                boxes.append((lev, list(p), [p[i] + 1 for i in range(d)]))
+    return [(lev, tuple(lo), tuple(hi)) for lev, lo, hi in boxes]

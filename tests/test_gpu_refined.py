@@ -345,3 +345,32 @@ def test_regrid_keeps_a_constant_state(eb):
     with pytest.raises(eb.ExaError):
         m.regrid([(0, (0, 0), (3, 3))])  # no margin
     assert m.validate() == 0
+
+
+def test_adaptive_refinement_loop_vs_oracle(eb):
+    """a refinement criterion (density variation within a cell) drives
+    adapt_boxes and regrid between steps; the oracle follows the same boxes"""
+    from exahype_b200 import problems
+    cells = (9, 9)
+    u, _ = problems.gaussian_pulse_2d(3, cells, seed=13)
+    s = eb.Solver(2, 3)
+    m = eb.Mesh.boxes(s, cells, [0.0, 0.0], [1.0, 1.0], [])
+    o = pyoracle.RefinedMesh(2, 3, cells, [1.0, 1.0], level_boxes=[])
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init(0.0)
+    o.init(0.0)
+    refined_once = False
+    for _ in range(3):
+        v = m.get_solution()[..., 0]
+        flags = (v.max(axis=1) - v.min(axis=1)) / v.mean(axis=1) > 0.02
+        boxes = eb.adapt_boxes(m, flags, 2)
+        refined_once |= bool(boxes)
+        m.regrid(boxes)
+        o.regrid(boxes)
+        m.step(2)
+        o.step(2)
+        a, b = m.get_solution(), o.get_solution()
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+        assert m.validate() == 0
+    assert refined_once and m.ncells > 81
