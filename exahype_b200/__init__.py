@@ -670,30 +670,57 @@ def cell_positions(mesh):
     return out
 
 
-def adapt_boxes(mesh, flags, max_level):
+# refinement controls a criterion returns per cell, with the reference's
+# values (exahype::solvers::Solver::RefinementControl, Solver.h:446)
+KEEP, REFINE, ERASE = 0, 1, 2
+
+
+def adapt_boxes(mesh, controls, max_level):
     """The refinement of a mesh after a refinement criterion, as boxes for
-    Mesh.regrid: the cells with flags[c] set (refinementCriterion ->
-    Refine, evaluated by the caller per cell) below max_level are refined,
-    refined positions that still hold a flagged finer cell stay refined, and
-    coarser levels are refined around every refined position so that each
-    keeps one cell of margin inside its level's region (the reference's
-    spacetree keeps the same 2:1-like balance with its helper cells);
-    positions within one cell of the domain boundary are never refined.
-    Returns [(level, lo, hi)] with one box per run of refined positions
-    along x."""
+    Mesh.regrid. controls[c] is the criterion's answer for cell c (in the
+    solution's cell order): KEEP (0), REFINE (1) or ERASE (2); booleans read
+    as REFINE / KEEP.
+
+    Follows the reference's rules (ADERDGSolver::markForRefinement,
+    ADERDGSolver.cpp:1078-1150): a cell below max_level that answers REFINE is
+    refined; a refined position is erased only when every one of its 3^d
+    children is an unrefined cell that answers ERASE (any child that answers
+    KEEP or REFINE, or is refined itself, vetoes it), so KEEP leaves the
+    refinement as it is. Coarser levels are then refined around every
+    refined position so that each keeps one cell of margin inside its
+    level's region (the reference's spacetree keeps the same 2:1-like
+    balance with its helper cells); positions within one cell of the domain
+    boundary are never refined. Returns [(level, lo, hi)] with one box per
+    run of refined positions along x."""
+    from . import problems
     d = mesh.solver.dim
     cells = list(mesh.cells[:d])
     pos = cell_positions(mesh)
+    ctrl = {}
+    for (lev, p), c in zip(pos, controls):
+        ctrl[(lev, p)] = int(c)
     F = [set() for _ in range(max_level)]
-    for (lev, p), f in zip(pos, flags):
-        if f and lev < max_level:
+    # the current refinement, minus the positions all of whose children erase
+    boxes_now = getattr(mesh, "boxes", None) or []
+    kids = [tuple(o) for o in np.ndindex(*([3] * d))]
+    if boxes_now:
+        for lev, (r0, st) in enumerate(problems.box_levels(d, mesh.cells, boxes_now)):
+            if lev >= max_level:
+                continue
+            for t in np.argwhere(st == 2):
+                p = tuple(int(r0[i] + t[d - 1 - i]) for i in range(d))
+                erase = all(ctrl.get((lev + 1, tuple(3 * p[i] + k[i] for i in range(d)))) == ERASE for k in kids)
+                if not erase:
+                    F[lev].add(p)
+    for (lev, p), c in ctrl.items():
+        if c == REFINE and lev < max_level:
             F[lev].add(p)
-        for up in range(1, lev + 1):  # flagged or not: a finer cell's ancestors stay refined if it is flagged
-            if f and lev - up < max_level:
-                F[lev - up].add(tuple(x // 3 ** up for x in p))
+    for lev in range(max_level - 1, 0, -1):  # ancestors of refined positions stay refined
+        for p in list(F[lev]):
+            F[lev - 1].add(tuple(x // 3 for x in p))
     # margins: every refined position at level l needs its neighbourhood
     # inside level l's region, i.e. the parents of that neighbourhood refined
-    nbh = [tuple(o) for o in np.ndindex(*([3] * d))]
+    nbh = kids
     for lev in range(max_level - 1, 0, -1):
         for p in list(F[lev]):
             for o in nbh:

@@ -348,8 +348,9 @@ def test_regrid_keeps_a_constant_state(eb):
 
 
 def test_adaptive_refinement_loop_vs_oracle(eb):
-    """a refinement criterion (density variation within a cell) drives
-    adapt_boxes and regrid between steps; the oracle follows the same boxes"""
+    """a refinement criterion (density variation within a cell: REFINE above
+    2 %, ERASE below 0.5 %, KEEP between) drives adapt_boxes and regrid
+    between steps; the oracle follows the same boxes"""
     from exahype_b200 import problems
     cells = (9, 9)
     u, _ = problems.gaussian_pulse_2d(3, cells, seed=13)
@@ -363,8 +364,9 @@ def test_adaptive_refinement_loop_vs_oracle(eb):
     refined_once = False
     for _ in range(3):
         v = m.get_solution()[..., 0]
-        flags = (v.max(axis=1) - v.min(axis=1)) / v.mean(axis=1) > 0.02
-        boxes = eb.adapt_boxes(m, flags, 2)
+        var = (v.max(axis=1) - v.min(axis=1)) / v.mean(axis=1)
+        controls = np.where(var > 0.02, eb.REFINE, np.where(var < 0.005, eb.ERASE, eb.KEEP))
+        boxes = eb.adapt_boxes(m, controls, 2)
         refined_once |= bool(boxes)
         m.regrid(boxes)
         o.regrid(boxes)
