@@ -1747,6 +1747,18 @@ int exa_mesh_regrid(exa_mesh* m, int nboxes, const int* box_level, const int* bo
     cudaGetLastError();
     return fail(EXA_ERR_NOMEM, "exa_mesh_regrid: device allocation failed");
   }
+  // frees the device lists on every return, once the new mesh's stream (which
+  // reads them) is idle; declared after `guard`, so it runs before the new
+  // mesh is destroyed on an error path (after the swap below the stream
+  // belongs to the caller's handle and stays alive)
+  struct ListGuard {
+    int* p;
+    cudaStream_t s;
+    ~ListGuard() {
+      cudaStreamSynchronize(s);
+      sfree(p, s);
+    }
+  } dl_guard{dl, nm->stream};
   EXA_CUDA(cudaStreamSynchronize(m->stream));
   if (!all.empty()) EXA_CUDA(cudaMemcpyAsync(dl, all.data(), all.size() * 4, cudaMemcpyHostToDevice, nm->stream));
   const size_t per = (size_t)k.P * (k.nvar + k.npar);
@@ -1775,10 +1787,16 @@ int exa_mesh_regrid(exa_mesh* m, int nboxes, const int* box_level, const int* bo
     rc = mesh_predict(nm);
   }
   cudaStreamSynchronize(nm->stream);  // the old arrays are read until here
-  sfree(dl, nm->stream);
   if (rc) return rc;
   nm->initialised = true;
+  // the per-phase times: the old mesh's pending events folded into its
+  // totals, which carry over to the new mesh (regridding does not reset them)
+  if ((rc = exa_mesh_phase_times(m, nullptr, nullptr, 0))) return rc;
   nm->profiling = m->profiling;
+  for (int i = 0; i < 4; i++) {
+    nm->phase_ms[i] = m->phase_ms[i];
+    nm->phase_launches[i] = m->phase_launches[i];
+  }
   std::swap(*m, *nm);  // the caller's handle now holds the new mesh; the guard frees the old one
   return EXA_OK;
 }
@@ -2419,15 +2437,44 @@ int exa_fv_musclhancock_update(const exa_solver* s, double* lim, double* lim_old
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
 
+// The current context of the calling thread (the device's primary context
+// once the runtime has touched it), through the driver entry point the
+// runtime exposes, so that the library needs no link against the driver.
+static void* current_context() {
+  typedef int (*CtxGetCurrent)(void**);
+  static CtxGetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(f);
+  }();
+  void* ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
+// The device address of g_noalloc_scratch for the current device, looked up
+// with cudaGetSymbolAddress on the first call per device and context (the
+// host-side name of the array is no device address) and cached under the
+// context it was found in: after a reset of the device the module is loaded
+// into a new primary context and the address is looked up again.
 static int noalloc_scratch(double** out) {
   static std::mutex mu;
-  static std::vector<std::pair<int, double*>> per_device;
+  struct Entry {
+    int dev;
+    void* ctx;
+    double* p;
+  };
+  static std::vector<Entry> per_device;
   int dev = 0;
   EXA_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
+  void* ctx = current_context();
   for (const auto& e : per_device)
-    if (e.first == dev) {
-      *out = e.second;
+    if (e.dev == dev && e.ctx == ctx && ctx) {
+      *out = e.p;
       return EXA_OK;
     }
   void* p = nullptr;
@@ -2435,7 +2482,15 @@ static int noalloc_scratch(double** out) {
   if (e != cudaSuccess || !p)
     return fail(EXA_ERR_CUDA, std::string("exa_fv_musclhancock_update_noalloc: cudaGetSymbolAddress: ") +
                                   cudaGetErrorString(e));
-  per_device.emplace_back(dev, static_cast<double*>(p));
+  ctx = current_context();  // the lookup makes the runtime's context current if it was not yet
+  for (auto& en : per_device)
+    if (en.dev == dev) {
+      en.ctx = ctx;
+      en.p = static_cast<double*>(p);
+      *out = en.p;
+      return EXA_OK;
+    }
+  per_device.push_back(Entry{dev, ctx, static_cast<double*>(p)});
   *out = static_cast<double*>(p);
   return EXA_OK;
 }

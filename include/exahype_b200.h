@@ -347,8 +347,9 @@ int exa_fv_musclhancock_update(const exa_solver* s, double* lim, double* lim_old
  * exceeds it is rejected with EXA_ERR_UNSUPPORTED. Nothing in it has to start
  * at zero. All calls share the array: calls that overlap in time (on
  * different streams or threads) race on it and must be serialised. The first
- * call on a device looks the array up and sets kernel attributes; make it
- * before any stream capture begins. */
+ * call on a device (and the first after a reset of that device) looks the
+ * array up and sets kernel attributes; make it before any stream capture
+ * begins. */
 int exa_fv_musclhancock_update_noalloc(const exa_solver* s, double* lim, double* lim_old, double* luh,
                                        const double* dt_dev, const double* dx, int ncells, const int* cell_list,
                                        void* stream);

@@ -1,7 +1,11 @@
 """exa_fv_musclhancock_update_noalloc (library-owned static scratch, no device
 allocation) against exa_fv_musclhancock_update (caller scratch): two calls in a
 row, each fed the previous call's output, must agree bit for bit -- both run
-the same per-cell computation, only the scratch and the grid size differ."""
+the same per-cell computation, only the scratch and the grid size differ.
+
+The 32 MiB static array holds the scratch of 151 blocks for 3D N=3 and of 47
+for 3D N=5; the larger cases list more cells than that, so the static path's
+blocks loop over several cells each and reuse their slice of the array."""
 import numpy as np
 import pytest
 
@@ -26,8 +30,12 @@ def states(rng, shape):
     return q
 
 
-@pytest.mark.parametrize("dim,order,n", [(3, 3, 200), (3, 5, 60), (2, 5, 150)])
-def test_noalloc_matches_caller_scratch_two_calls(eb, dim, order, n):
+STATIC_BYTES = 32 << 20
+
+
+@pytest.mark.parametrize("dim,order,n,beyond_cap", [(3, 3, 200, False), (3, 5, 60, False), (2, 5, 150, False),
+                                                    (3, 5, 200, True), (3, 3, 800, True)])
+def test_noalloc_matches_caller_scratch_two_calls(eb, dim, order, n, beyond_cap):
     rng = np.random.default_rng(7 * dim + order)
     E = 2 * order + 5
     lim0 = torch.as_tensor(states(rng, (n, E ** dim))).cuda()
@@ -37,6 +45,9 @@ def test_noalloc_matches_caller_scratch_two_calls(eb, dim, order, n):
     m = int(cells.numel())
     s = eb.Solver(dim, order)
     nb = s.fv_musclhancock_scratch_bytes(m)
+    if beyond_cap:
+        per_block = s.fv_musclhancock_scratch_bytes(1)
+        assert m > STATIC_BYTES // per_block, "this case must list more cells than the static array's blocks"
     scratch = torch.empty(max(nb, 8) // 8, dtype=torch.float64, device="cuda")
 
     a_lim, a_old = lim0.clone(), torch.zeros_like(lim0)
