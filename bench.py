@@ -192,25 +192,56 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def cpu_reference_run(steps, warmup, nthreads, cells=CELLS):
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_build(fast=True):
+    """('ref_fast', description) for the timed -O3 build of the reference
+    kernels when this CPU can run one, else ('ref', description of the
+    parity build)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle
+    if fast:
+        path, name = pyoracle.fast_build(DIM)
+        if path:
+            return "ref_fast", "reference kernels built -O3 -march=%s (FMA contraction on)" % name
+    return "ref", "reference kernels, parity build (-O2 -ffp-contract=off)"
+
+
+def cpu_reference_run(steps, warmup, nthreads, cells=CELLS, runs=1, fast=True):
     """The reference's own generic kernels (compiled from its sources into
-    oracle/_ref) driven by the oracle harness on the host cores."""
+    oracle/_ref) driven by the oracle harness on the host cores: `warmup`
+    steps, then `runs` timed runs of `steps` steps each (continuing the same
+    run); the value is from the median run."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import pyoracle
     from exahype_b200 import problems
     if not pyoracle.ref_available(DIM):
         return None
+    impl, build = ref_build(fast)
     u, _ = problems.gaussian_pulses_3d(ORDER, cells, seed=SEED)
-    m = pyoracle.Mesh(DIM, ORDER, cells, [1.0] * DIM, -1, impl="ref", nthreads=nthreads)
+    m = pyoracle.Mesh(DIM, ORDER, cells, [1.0] * DIM, -1, impl=impl, nthreads=nthreads)
     m.set_solution(u)
     m.init(0.0)
     if warmup:
         m.step(warmup)
-    t0 = time.perf_counter()
-    m.step(steps)
-    el = time.perf_counter() - t0
+    times = []
+    for _ in range(max(1, runs)):
+        t0 = time.perf_counter()
+        m.step(steps)
+        times.append(time.perf_counter() - t0)
+    el = float(np.median(times))
     dof = int(np.prod(cells)) * (ORDER + 1) ** DIM * NVAR * steps
-    return dict(value=dof / el, seconds=el, steps=steps, cells=list(cells))
+    return dict(value=dof / el, seconds=el, run_seconds=times, steps=steps, cells=list(cells), build=build,
+                cpu=cpu_model())
 
 
 def run_reference_arm(a):
@@ -218,11 +249,14 @@ def run_reference_arm(a):
     if rank != 0:
         return 0
     nthreads = os.cpu_count() or 1
-    r = cpu_reference_run(a.steps, a.warmup, nthreads)
+    runs = 5
+    r = cpu_reference_run(a.steps, a.warmup, nthreads, runs=runs)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference kernels built from the "
                           "reference sources) is not present in this tree"}))
         return 0
+    # the parity build (what the tests compare against), one run, for comparison
+    rp = cpu_reference_run(a.steps, 0, nthreads, runs=1, fast=False) if r["build"].find("-O3") >= 0 else None
     ms = 1000.0 * r["seconds"] / a.steps
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "DoF-updates/s", "n_gpus": a.gpus,
@@ -231,10 +265,15 @@ def run_reference_arm(a):
         "config": {"workload": WORKLOAD, "dim": DIM, "order": ORDER, "cells": list(CELLS),
                    "dof_per_step": dof_per_step(), "l2": "inputs larger than L2 (170 MB solution)"},
         "cpu_baseline": {"value": r["value"], "unit": "DoF-updates/s", "cores": nthreads, "kind": "reference",
-                         "sample": "%d full time steps of the 27^3 mesh after %d warm-up steps" % (a.steps,
-                                                                                                  a.warmup)},
+                         "cpu": r["cpu"], "build": r["build"],
+                         "sample": "median of %d runs of %d full time steps of the 27^3 mesh after %d warm-up steps"
+                                   " (run times %s s)" % (runs, a.steps, a.warmup,
+                                                          ", ".join("%.2f" % x for x in r["run_seconds"]))},
         "e2e": {"value": r["value"], "unit": "DoF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if rp is not None:
+        line["parity_build"] = {"value": rp["value"], "unit": "DoF-updates/s", "build": rp["build"],
+                                "sample": "1 run of %d steps" % a.steps}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -371,11 +410,12 @@ def run_ours(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         nthreads = os.cpu_count() or 1
-        r = cpu_reference_run(1, 0, nthreads)
+        r = cpu_reference_run(3, 1, nthreads, runs=5)
         if r is not None:
             cpu = {"value": r["value"], "unit": "DoF-updates/s", "cores": nthreads, "kind": "reference",
-                   "sample": "1 full time step of the 27^3 mesh (after the initial predictor) on the "
-                             "reference's generic kernels, %.1f s" % r["seconds"]}
+                   "cpu": r["cpu"], "build": r["build"],
+                   "sample": "median of 5 runs of 3 full time steps of the 27^3 mesh (after 1 warm-up step) on the "
+                             "reference's generic kernels, %.1f s per run" % r["seconds"]}
     launches = sum(v[1] for v in ph.values())
     mixed = None if a.no_mixed else run_mixed_arm(a, u0, s.variant, dev)
     fused = None if a.no_fused else run_fused_arm(a, u0, s.variant, dev)
@@ -458,14 +498,16 @@ def run_elastic_workload(a, world, dev, rank, fp64_peak=None):
         import pyoracle
         if pyoracle.ref_available(EL_DIM):
             nthreads = os.cpu_count() or 1
-            r = pyoracle.Mesh(EL_DIM, EL_ORDER, EL_CELLS, [1.0] * EL_DIM, -1, pde=2, impl="ref", nthreads=nthreads)
+            r = pyoracle.Mesh(EL_DIM, EL_ORDER, EL_CELLS, [1.0] * EL_DIM, -1, pde=2, impl=ref_build()[0],
+                             nthreads=nthreads)
             r.set_solution(u0)
             r.init(0.0)
             t0 = time.perf_counter()
             r.step(1)
             el = time.perf_counter() - t0
             out["cpu_baseline"] = {"value": dof_step / el, "unit": "DoF-updates/s", "cores": nthreads,
-                                   "kind": "reference", "sample": "1 full time step of the 27^3 elastic mesh on the "
+                                   "kind": "reference", "build": ref_build()[1],
+                                   "sample": "1 full time step of the 27^3 elastic mesh on the "
                                    "reference's linear kernels, %.1f s" % el}
     return out
 
@@ -527,14 +569,15 @@ def run_refined_workload(a, world, dev, rank):
         import pyoracle
         if pyoracle.ref_available(3):
             sc, sl, sh = (9, 9, 9), (3, 3, 3), (6, 6, 6)
-            r = pyoracle.RefinedMesh(3, 5, sc, [1.0] * 3, sl, sh, impl="ref")
+            r = pyoracle.RefinedMesh(3, 5, sc, [1.0] * 3, sl, sh, impl=ref_build()[0])
             r.set_solution(problems.pulse_refined(3, 5, sc, sl, sh, seed=SEED))
             r.init(0.0)
             t0 = time.perf_counter()
             r.step(1)
             el = time.perf_counter() - t0
             out["cpu_baseline"] = {"value": r.ncells * 6 ** 3 * 5 / el, "unit": "DoF-updates/s", "cores": 1,
-                                   "kind": "reference", "sample": "1 step of a 9^3 mesh with its central 3^3 cells "
+                                   "kind": "reference", "build": ref_build()[1],
+                                   "sample": "1 step of a 9^3 mesh with its central 3^3 cells "
                                    "refined (%d cells), the reference's kernels per cell, %.1f s" % (r.ncells, el)}
     return out
 
@@ -632,7 +675,8 @@ def run_limiter_workload(a, world, dev, rank):
         import pyoracle
         if pyoracle.ref_available(LIM_DIM):
             nthreads = os.cpu_count() or 1
-            r = pyoracle.RefLimitingMesh(LIM_DIM, LIM_ORDER, LIM_CELLS, [1.0] * LIM_DIM, 0, nthreads=nthreads)
+            r = pyoracle.RefLimitingMesh(LIM_DIM, LIM_ORDER, LIM_CELLS, [1.0] * LIM_DIM, 0, nthreads=nthreads,
+                                         fast=ref_build()[0] == "ref_fast")
             r.set_solution(luh)
             r.set_fv_initial(fv)
             r.init(0.0)
@@ -641,7 +685,7 @@ def run_limiter_workload(a, world, dev, rank):
             r.step(k)
             el = time.perf_counter() - t0
             out["cpu_baseline"] = {"value": dof_step * k / el, "unit": "DoF-updates/s", "cores": nthreads,
-                                   "kind": "reference",
+                                   "kind": "reference", "build": ref_build()[1],
                                    "sample": "the first %d steps of the same workload on the reference's "
                                              "limiter/MUSCL-Hancock/ADER-DG kernels, %.1f s" % (k, el)}
     return out

@@ -35,11 +35,21 @@ class _Solver(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("order", ctypes.c_int), ("pde", ctypes.c_int)]
 
 
+def reference_root():
+    """The reference checkout: $EXAHYPE_REFERENCE, else a directory named
+    'reference' beside this repository; None when neither holds the
+    reference's kernels."""
+    for ref in (os.environ.get("EXAHYPE_REFERENCE"), os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")):
+        if ref and os.path.isdir(os.path.join(ref, "ExaHyPE", "kernels")):
+            return os.path.abspath(ref)
+    return None
+
+
 def build():
     """Builds liboracle.so (and oracle/_ref when the reference checkout exists)."""
     subprocess.check_call(["make", "-s", "-C", HERE])
-    ref = os.environ.get("EXAHYPE_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "ExaHyPE", "kernels")):
+    ref = reference_root()
+    if ref:
         subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref])
 
 
@@ -64,17 +74,49 @@ def lib():
 
 _ref = {}
 
+# the timed builds of the reference kernels (oracle/ref/Makefile, target
+# 'fast'): -O3 for the build host's CPU, for x86-64-v4 and for x86-64-v3, with
+# the instruction-set flags each one needs from the CPU that runs it
+_V3 = {"avx", "avx2", "fma", "bmi1", "bmi2", "movbe", "f16c", "abm", "xsave"}
+_V4 = _V3 | {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}
+
 
 def ref_available(dim=2):
     return os.path.exists(os.path.join(HERE, "_ref", "libexaref%dd.so" % dim))
 
 
-def reflib(dim):
-    if dim not in _ref:
-        l = ctypes.CDLL(os.path.join(HERE, "_ref", "libexaref%dd.so" % dim))
+def _cpu_flags(path="/proc/cpuinfo"):
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def fast_build(dim):
+    """(path, name) of the fastest timed build of the reference kernels that
+    this CPU can run, or (None, reason)."""
+    d = os.path.join(HERE, "_ref", "fast")
+    host = _cpu_flags()
+    built_on = _cpu_flags(os.path.join(d, "build_host_cpuinfo.txt"))
+    for name, need in (("native", built_on), ("x86-64-v4", _V4), ("x86-64-v3", _V3)):
+        p = os.path.join(d, "libexaref%dd.%s.so" % (dim, name))
+        if os.path.exists(p) and need and need <= host:
+            return p, name
+    return None, "no timed build of the reference kernels runs on this CPU (or none was built)"
+
+
+def reflib(dim, fast=False):
+    key = (dim, fast)
+    if key not in _ref:
+        path = fast_build(dim)[0] if fast else os.path.join(HERE, "_ref", "libexaref%dd.so" % dim)
+        l = ctypes.CDLL(path)
         getattr(l, "ref%dd_stable_dt" % dim).restype = ctypes.c_double
-        _ref[dim] = l
-    return _ref[dim]
+        _ref[key] = l
+    return _ref[key]
 
 
 class Kernels:
@@ -89,7 +131,7 @@ class Kernels:
         self.P = self.b ** dim
         self.F = self.b ** (dim - 1)
         self._s = _Solver(dim, order, pde)
-        self._l = lib() if impl == "oracle" else reflib(dim)
+        self._l = lib() if impl == "oracle" else reflib(dim, fast=impl == "ref_fast")
         self._pre = "orc_" if impl == "oracle" else "ref%dd_" % dim
 
     def _call(self, name, *args):
@@ -229,7 +271,8 @@ def table(name, order):
 
 class Mesh:
     """Uniform mesh run by the oracle harness (oracle/harness.c) over the C
-    restatement (impl='oracle') or the compiled reference kernels (impl='ref')."""
+    restatement (impl='oracle'), the compiled reference kernels (impl='ref',
+    the parity build) or their timed -O3 build (impl='ref_fast')."""
 
     def __init__(self, dim, order, cells, size, bc, pde=0, impl="oracle", nthreads=1):
         self.dim, self.order, self.pde, self.impl = dim, order, pde, impl
@@ -245,7 +288,7 @@ class Mesh:
             create.restype = ctypes.c_void_p
             self._h = ctypes.c_void_p(create(dim, order, pde, ci, sz, b, nthreads))
         else:
-            self._l = reflib(dim)
+            self._l = reflib(dim, fast=impl == "ref_fast")
             self._pre = "ref%dd_mesh_" % dim
             create = getattr(self._l, self._pre + "create")
             create.restype = ctypes.c_void_p
@@ -650,12 +693,13 @@ class LimitingMesh:
 
 
 class RefLimitingMesh(LimitingMesh):
-    """The limiting harness over the reference's own kernels (oracle/_ref)."""
+    """The limiting harness over the reference's own kernels (oracle/_ref; the
+    timed -O3 build with fast=True)."""
 
     def __init__(self, dim, order, cells, size, bc, helper_layers=1, cure_steps=0, relax=1e-4, scale=1e-3,
-                 nthreads=1):
+                 nthreads=1, fast=False):
         self.dim, self.order = dim, order
-        l = reflib(dim)
+        l = reflib(dim, fast=fast)
         pre = "ref%dd_lmesh_" % dim
         ci = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
         sz = (ctypes.c_double * 3)(*(list(size) + [1.0] * (3 - len(size))))

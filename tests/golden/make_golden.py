@@ -89,8 +89,14 @@ def make_ref_tables():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (default: $EXAHYPE_REFERENCE, else a "
+                    "directory named 'reference' beside this repository)")
     a = ap.parse_args()
+    if a.ref is None:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import pyoracle
+        a.ref = pyoracle.reference_root()
+        assert a.ref, "no reference checkout found"
     kv = make_kernel_vectors(a.ref)
     print("kernel_vectors: %d arrays" % len(kv))
     if os.path.exists(os.path.join(REPO, "oracle", "_ref", "libexaref2d.so")):
