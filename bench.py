@@ -61,17 +61,22 @@ def flux_flops(dim):
     return 1 + 5 + 4 + 2 + dim * 9
 
 
-def predictor_flops(dim, N, sweeps, ncells, nV=NVAR):
+def predictor_flops(dim, N, sweeps, ncells, nV=NVAR, first_sweep_once=False):
     """Algorithmic FLOPs of spaceTimePredictor + volumeIntegral (padding and
     idle lanes not counted): per Picard sweep per cell
     2 d nV b^(d+2) (derivatives) + 2 nV b^(d+2) (iK1) + 2 nV b^(d+1) (rhs0)
     + b^(d+1) flux evaluations; per cell once: time averaging +
-    extrapolation 2(d+2) nV b^(d+1) + 8 d nV b^d, volume integral 2 d nV b^(d+1)."""
+    extrapolation 2(d+2) nV b^(d+1) + 8 d nV b^d, volume integral 2 d nV b^(d+1).
+    `sweeps` is the total over all cells. With first_sweep_once the count is
+    of the work the line-form kernel executes: every cell's first sweep
+    starts from the time-constant guess, so its fluxes and derivative
+    contractions are formed once instead of once per time slice (1/b)."""
     b = N + 1
-    per_sweep = 2 * dim * nV * b ** (dim + 2) + 2 * nV * b ** (dim + 2) + 2 * nV * b ** (dim + 1) \
-        + b ** (dim + 1) * flux_flops(dim)
+    deriv = 2 * dim * nV * b ** (dim + 2) + b ** (dim + 1) * flux_flops(dim)
+    per_sweep = deriv + 2 * nV * b ** (dim + 2) + 2 * nV * b ** (dim + 1)
     per_cell = 2 * (dim + 2) * nV * b ** (dim + 1) + 8 * dim * nV * b ** dim + 2 * dim * nV * b ** (dim + 1)
-    return per_sweep * sweeps + per_cell * ncells
+    saved = deriv * (b - 1) / b * ncells if first_sweep_once else 0.0
+    return per_sweep * sweeps + per_cell * ncells - saved
 
 
 def bytes_per_step(dim, N, ncells, nV=NVAR, nD=NVAR):
@@ -162,18 +167,43 @@ class ClockSampler:
         return dict(sm_mhz=float(np.median(sm)), sm_max_mhz=mx, reasons=sorted(reasons), samples=len(sm))
 
 
+PREDICTOR_SOURCES = ("exahype_b200/csrc/predictor_lines.cuh", "exahype_b200/csrc/aderdg.cuh",
+                     "exahype_b200/csrc/pde.cuh", "exahype_b200/csrc/common.cuh")
+
+
+def predictor_source_hash():
+    """sha256 (first 16 hex digits) over the predictor kernel's sources"""
+    import hashlib
+    h = hashlib.sha256()
+    for f in PREDICTOR_SOURCES:
+        with open(os.path.join(REPO, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
 def predictor_traffic_bytes():
-    """dram__bytes_read.sum + dram__bytes_write.sum of one predictor launch on
-    the 27^3 N=5 mesh, from the line 'traffic_bytes_per_launch: <n>' of the
-    committed ncu summary (None if absent)."""
+    """(dram__bytes_read.sum + dram__bytes_write.sum of one predictor launch on
+    the 27^3 N=5 mesh, source note) from the committed ncu summary's lines
+    'traffic_bytes_per_launch: <n>' and 'source_sha16: <hash of the kernel
+    sources it was captured from>'. The figure is only used while the
+    sources still hash the same; otherwise (None, why)."""
+    rel = os.path.relpath(PROFILE_PREDICTOR, REPO)
+    val, sha = None, None
     try:
         with open(PROFILE_PREDICTOR) as f:
             for line in f:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].strip().split()[0])
+                t = line.strip()
+                if t.startswith("traffic_bytes_per_launch:"):
+                    val = float(t.split(":", 1)[1].strip().split()[0])
+                elif t.startswith("source_sha16:"):
+                    sha = t.split(":", 1)[1].strip().split()[0]
     except OSError:
-        pass
-    return None
+        return None, "no ncu summary at %s" % rel
+    cur = predictor_source_hash()
+    if val is None or sha != cur:
+        return None, "%s was captured from other kernel sources (sha16 %s, now %s): traffic not reused" % (
+            rel, sha, cur)
+    return val, "%s (ncu capture of the same kernel sources, sha16 %s)" % (rel, cur)
 
 
 def reduce_max(x, world, device=None):
@@ -349,8 +379,11 @@ def run_ours(a):
     # roofline of the dominant kernel (predictor + volume integral, FP64 pipe)
     ncells = int(np.prod(CELLS))
     pred_ms = ph["predictor"][0] / a.steps
-    pflops = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells)
-    fp64_peak = measure_fp64_peak() if not a.no_fp64_probe else None
+    line_form = s.variant in (1, 2, 4, 5, 6, 7)  # the line-form kernels form the first sweep once
+    pflops = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells, first_sweep_once=line_form)
+    pflops_ref = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells)
+    fp64_peaks = measure_fp64_peak() if not a.no_fp64_probe else None
+    fp64_peak = max(fp64_peaks.values()) if fp64_peaks else None
     peaks = load_peaks()
     byt = bytes_per_step(DIM, ORDER, ncells)
     kernels = {}
@@ -365,9 +398,16 @@ def run_ours(a):
             kernels[name] = dict(bound="hbm", achieved=ach, unit="GB/s", ms=t_ms, peak=peaks["hbm_gbs"],
                                  frac=ach / peaks["hbm_gbs"])
     roof = dict(kernels["predictor"])
-    roof.update(traffic=predictor_traffic_bytes(), peak_source="fp64 DFMA probe measured in this run (exa_fp64_peak_probe); "
-                "MEASURED_PEAKS.json has no FP64 figure",
-                algorithmic_flops_per_launch=pflops, picard_sweeps_per_cell=sweeps / a.steps / ncells)
+    traffic, tsrc = predictor_traffic_bytes()
+    roof.update(traffic=traffic, traffic_source=tsrc,
+                peak_source="the larger of the FP64 DFMA and DMMA (mma.sync m8n8k4 f64) probes measured in this run "
+                            "(%s TFLOP/s); MEASURED_PEAKS.json has no FP64 figure" % (
+                                ", ".join("%s %.2f" % kv for kv in sorted((fp64_peaks or {}).items())) or "none"),
+                algorithmic_flops_per_launch=pflops, reference_flops_per_launch=pflops_ref,
+                flops_note="achieved counts the flops the kernel executes (the first Picard sweep's fluxes and "
+                           "derivative contractions once per cell, not once per time slice); "
+                           "reference_flops_per_launch is the same launch counted as the reference's loops",
+                picard_sweeps_per_cell=sweeps / a.steps / ncells)
 
     # end to end through the C ABI: per step, H2D of the solution from pinned
     # host memory, one time step, D2H of the solution
@@ -436,11 +476,62 @@ def run_ours(a):
         "clocks": clocks, "picard_sweeps_per_step": sweeps / a.steps, "predictor_variant": tune,
         "mixed": mixed, "fused": fused, "limiter": lim, "ensemble": ens, "serving": srv, "elastic": ela, "amr": amr, "refined": refined,
     }
+    line["summary"] = summary(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def _r(x, n=4):
+    """x rounded to n significant digits (None stays None)"""
+    if x is None:
+        return None
+    if isinstance(x, (bool, int)):
+        return x
+    return float("%.*g" % (n, x))
+
+
+def summary(line):
+    """The headline and every secondary workload's main figures in a few
+    hundred characters: the last key of the line, so that a reader who only
+    keeps the end of the line still sees them all."""
+    g = lambda d, *ks: None if d is None else (d.get(ks[0]) if len(ks) == 1 else g(d.get(ks[0]), *ks[1:]))
+    k = line.get("kernels", {})
+    out = {"fp64_step": {"value": _r(line["value"]), "ms": _r(line["ms_per_step"]),
+                         "frac": {n: _r(g(k, n, "frac"), 3) for n in ("predictor", "riemann", "corrector")}},
+           "e2e": _r(g(line, "e2e", "value")), "cpu_ref": _r(g(line, "cpu_baseline", "value"))}
+    if line.get("mixed"):
+        m = line["mixed"]
+        out["mixed"] = {"value": _r(m["value"]), "rel_l2_vs_fp64": _r(m["rel_l2_vs_fp64"], 2)}
+    if line.get("fused"):
+        out["fused"] = {"value": _r(line["fused"]["value"]), "reruns": line["fused"]["reruns_in_timed_steps"]}
+    if line.get("limiter"):
+        m = line["limiter"]
+        out["limiter"] = {"value": _r(m["value"]), "steps": m["steps"], "irregular": m["irregular_steps"],
+                          "ms": _r(m["ms_per_step"]), "cpu_ref": _r(g(m, "cpu_baseline", "value"))}
+    if line.get("ensemble"):
+        m = line["ensemble"]
+        out["ensemble"] = {"value": _r(m["value"]), "one_at_a_time": _r(m["one_at_a_time"]["value"]),
+                           "path": m.get("path")}
+    if line.get("serving"):
+        m = line["serving"]
+        out["serving"] = {"p50_s": _r(m["p50_time_to_solution_s"], 3), "p99_s": _r(m["p99_time_to_solution_s"], 3),
+                          "value": _r(m["value"]), "full_size": m.get("full_size"),
+                          "one_at_a_time": {"p50_s": _r(m["one_at_a_time"]["p50_time_to_solution_s"], 3),
+                                            "p99_s": _r(m["one_at_a_time"]["p99_time_to_solution_s"], 3),
+                                            "value": _r(m["one_at_a_time"]["value"])}}
+    if line.get("elastic"):
+        m = line["elastic"]
+        out["elastic"] = {"value": _r(m["value"]), "predictor_frac": _r(g(m, "kernels", "predictor", "frac"), 3),
+                          "cpu_ref": _r(g(m, "cpu_baseline", "value"))}
+    if line.get("refined"):
+        out["refined"] = {"value": _r(line["refined"]["value"])}
+    if line.get("amr"):
+        out["amr_frac"] = {n: _r(g(line["amr"], n, "frac"), 3) for n in
+                           ("volume_prolongation", "volume_restriction", "plot_vertices")}
+    return out
 
 
 def run_elastic_workload(a, world, dev, rank, fp64_peak=None):
@@ -879,15 +970,17 @@ def run_fused_arm(a, u0, variant, dev):
 
 
 def measure_fp64_peak():
+    """FP64 peaks measured in this run (TFLOP/s): the DFMA probe and the DMMA
+    (mma.sync m8n8k4 f64) probe; the roofline uses the larger."""
     import ctypes
     import exahype_b200 as eb
-    out = ctypes.c_double()
     lib = eb.load()
-    if not hasattr(lib, "exa_fp64_peak_probe"):
-        return None
-    if lib.exa_fp64_peak_probe(ctypes.byref(out)) != 0:
-        return None
-    return out.value
+    out = {}
+    for name, fn in (("dfma", "exa_fp64_peak_probe"), ("dmma", "exa_fp64_mma_peak_probe")):
+        v = ctypes.c_double()
+        if hasattr(lib, fn) and getattr(lib, fn)(ctypes.byref(v)) == 0:
+            out[name] = v.value
+    return out or None
 
 
 def main():
@@ -932,7 +1025,8 @@ def run_secondary_only(a):
            "serving": run_serving_workload, "elastic": run_elastic_workload, "amr": run_amr_workload,
            "refined": run_refined_workload}[a.workload]
     if a.workload == "elastic":
-        r = run(a, world, torch.device("cuda", local), rank, None if a.no_fp64_probe else measure_fp64_peak())
+        pk = None if a.no_fp64_probe else measure_fp64_peak()
+        r = run(a, world, torch.device("cuda", local), rank, max(pk.values()) if pk else None)
     else:
         r = run(a, world, torch.device("cuda", local), rank)
     if rank == 0:

@@ -505,6 +505,25 @@ __global__ void __launch_bounds__(256) fp64_probe_kernel(double* out, int iters,
   if (s == 1.2345e300) out[0] = s;  // never true; keeps the chains alive
 }
 
+// FP64 tensor-core (DMMA) throughput: 4 independent m8n8k4 accumulator chains
+// per warp, `iters` rounds; 2 * 256 flops per warp and MMA
+__global__ void __launch_bounds__(256) fp64_mma_probe_kernel(double* out, int iters, double a, double b) {
+  double d[4][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++) d[i][0] = d[i][1] = threadIdx.x * 1e-3 + i;
+  for (int k = 0; k < iters; k++) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                   : "+d"(d[i][0]), "+d"(d[i][1])
+                   : "d"(a), "d"(b));
+  }
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) s += d[i][0] + d[i][1];
+  if (s == 1.2345e300) out[0] = s;  // never true; keeps the chains alive
+}
+
 }  // namespace exa
 
 using namespace exa;
@@ -1853,11 +1872,11 @@ int exa_mesh_phase_times(exa_mesh* m, double* ms4, long long* launches4, int res
   return EXA_OK;
 }
 
-int exa_fp64_peak_probe(double* tflops) {
-  if (!tflops) return fail(EXA_ERR_ARG, "exa_fp64_peak_probe: null argument");
-  int dev = 0, sms = 0;
-  EXA_CUDA(cudaGetDevice(&dev));
-  EXA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+// best of 5 timed launches of a throughput probe on every SM (8 blocks of 256
+// threads each); returns the best time in ms
+}  // extern "C"
+template <class Launch>
+static int fp64_probe_best_ms(const char* who, Launch launch, float* best_ms) {
   double* out = nullptr;
   EXA_CUDA(cudaMalloc(&out, 8));
   cudaStream_t st;
@@ -1865,12 +1884,11 @@ int exa_fp64_peak_probe(double* tflops) {
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
-  const int blocks = sms * 8, threads = 256, iters = 1 << 14;
-  fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, 64, 0.999999, 1e-7);  // warm-up
+  launch(out, st, true);  // warm-up
   float best = 1e30f;
   for (int r = 0; r < 5; r++) {
     cudaEventRecord(a, st);
-    fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.999999, 1e-7);
+    launch(out, st, false);
     cudaEventRecord(b, st);
     cudaEventSynchronize(b);
     float ms = 0;
@@ -1882,8 +1900,39 @@ int exa_fp64_peak_probe(double* tflops) {
   cudaEventDestroy(b);
   cudaStreamDestroy(st);
   cudaFree(out);
-  if (e != cudaSuccess) return fail(EXA_ERR_CUDA, std::string("exa_fp64_peak_probe: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess) return fail(EXA_ERR_CUDA, std::string(who) + ": " + cudaGetErrorString(e));
+  *best_ms = best;
+  return EXA_OK;
+}
+extern "C" {
+
+int exa_fp64_peak_probe(double* tflops) {
+  if (!tflops) return fail(EXA_ERR_ARG, "exa_fp64_peak_probe: null argument");
+  int dev = 0, sms = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  EXA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+  float best = 0;
+  int rc = fp64_probe_best_ms("exa_fp64_peak_probe", [&](double* out, cudaStream_t st, bool warm) {
+    fp64_probe_kernel<<<blocks, threads, 0, st>>>(out, warm ? 64 : iters, 0.999999, 1e-7);
+  }, &best);
+  if (rc) return rc;
   *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
+  return EXA_OK;
+}
+
+int exa_fp64_mma_peak_probe(double* tflops) {
+  if (!tflops) return fail(EXA_ERR_ARG, "exa_fp64_mma_peak_probe: null argument");
+  int dev = 0, sms = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  EXA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = sms * 8, threads = 256, iters = 1 << 12;
+  float best = 0;
+  int rc = fp64_probe_best_ms("exa_fp64_mma_peak_probe", [&](double* out, cudaStream_t st, bool warm) {
+    fp64_mma_probe_kernel<<<blocks, threads, 0, st>>>(out, warm ? 16 : iters, 0.999999, 1e-7);
+  }, &best);
+  if (rc) return rc;
+  *tflops = 2.0 * 256.0 * 4.0 * iters * ((double)blocks * threads / 32) / (best * 1e-3) / 1e12;
   return EXA_OK;
 }
 

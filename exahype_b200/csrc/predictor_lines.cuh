@@ -169,7 +169,6 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     }
   }
 
-  double fh[DIM][nV];
   bool done = !active;
   int it_done = 0;
   for (int iter = 0; iter < C::maxIter; iter++) {
@@ -180,10 +179,18 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
 #pragma unroll
       for (int v = 0; v < nV; v++) qn[l][v] = 0.0;
 
+    // The first sweep starts from the trivial guess lQi(:,t) = luh for every
+    // t, so its fluxes and their contractions are the same in every time
+    // slice: phases A and B run once (slice 0, without the w_t factor) and
+    // phase C of every slice reads that one result, scaled by w_t (no
+    // barrier is needed between those phase-C passes: nothing writes sF).
+    const bool first = iter == 0;
     for (int t0 = 0; t0 < b; t0 += TS) {
-      __syncthreads();  // phase C of the previous slices is done with sF
+      const bool reuse = first && t0 > 0;  // block-uniform
+      if (!reuse) __syncthreads();  // phase C of the previous slices is done with sF
       // A: fluxes of slices t0 .. t0+TS-1, line-major, slice j in buffer j
-      if (!done && low) {  // flux increments in FP64, stored as FP32
+      if (reuse) {
+      } else if (!done && low) {  // flux increments in FP64, stored as FP32
         const int t = t0;
         double Q[nD], Qp[nD];
 #pragma unroll
@@ -202,7 +209,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
 #pragma unroll
         for (int j = 0; j < TS; j++) {
           const int t = t0 + j;
-          if (t < b) {
+          if (t < b && !(first && j > 0)) {
             double Q[nD];
 #pragma unroll
             for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
@@ -215,11 +222,11 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
           }
         }
       }
-      __syncthreads();
+      if (!reuse) __syncthreads();
       // B: line contractions, in place
 #pragma unroll
       for (int k = 0; k < C::IPT; k++) {
-        if (it_off[k] < 0 || s_done[it_cell[k]]) continue;
+        if (reuse || it_off[k] < 0 || s_done[it_cell[k]]) continue;
         if (low) {
           const int t = t0;
           float* base = sFall32 + it_off[k] + it_cell[k] * C::SF;
@@ -239,12 +246,12 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
 #pragma unroll
         for (int j = 0; j < TS; j++) {
           const int t = t0 + j;
-          if (t >= b) break;
+          if (t >= b || (first && j > 0)) break;
           double* base = sFall + it_off[k] + j * C::SFJ;
           double f[b];
 #pragma unroll
           for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
-          const double us = T.w[t] * it_us[k];
+          const double us = first ? it_us[k] : T.w[t] * it_us[k];
 #pragma unroll
           for (int l = 0; l < b; l++) {
             double s = 0.0;
@@ -254,7 +261,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
           }
         }
       }
-      __syncthreads();
+      if (!reuse) __syncthreads();
       // C: rhs at this node, folded into the Picard accumulators
       if (!done && low) {  // increment: the rhs0 term cancels
         const int t = t0;
@@ -266,6 +273,23 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
           const double ir = iw * rhs;
 #pragma unroll
           for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
+        }
+      } else if (!done && first) {  // slices t0 .. t0+TS-1 from the one contraction of F(luh)
+#pragma unroll
+        for (int j = 0; j < TS; j++) {
+          const int t = t0 + j;
+          if (t < b) {
+            const double r0 = wpt * T.FL[t], wt = T.w[t];
+#pragma unroll
+            for (int v = 0; v < nV; v++) {
+              double sv = 0.0;
+#pragma unroll
+              for (int d = 0; d < DIM; d++) sv += sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+              const double ir = iw * (r0 * lu[v] - wt * sv);
+#pragma unroll
+              for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
+            }
+          }
         }
       } else if (!done) {
 #pragma unroll
@@ -319,7 +343,11 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     if (!done) {
       it_done = iter + 1;
       if (sq_res < 1e-7 * 1e-7 || iter + 1 == C::maxIter) {
-        // time-averaged fluxes of this sweep = of the iterate before the update
+        // time-averaged fluxes of this sweep = of the iterate before the
+        // update; kept in this node's slots of the cell's slice buffer (which
+        // no phase touches again once the cell is done), not in registers
+        // that would stay live across the sweeps
+        double fh[DIM][nV];
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
@@ -342,6 +370,10 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
               for (int v = 0; v < nV; v++) dst[d * nV + v] = Fl[d][v];
           }
         }
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int v = 0; v < nV; v++) sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = fh[d][v];
         done = true;
       }
 #pragma unroll
@@ -376,9 +408,9 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     const int py = DIM == 3 ? (z * b + x) * b + y : x * b + y;
     const int pz = (y * b + x) * b + z;
     for (int v = 0; v < nV; v++) {
-      fhd[(0 * P + p) * nV + v] = fh[0][v];
-      fhd[(1 * P + py) * nV + v] = fh[1][v];
-      if (DIM == 3) fhd[(2 * P + pz) * nV + v] = fh[DIM - 1][v];
+      fhd[(0 * P + p) * nV + v] = sF[(0 * b + nd[0]) * SLAB + Ld[0] * nV + v];
+      fhd[(1 * P + py) * nV + v] = sF[(1 * b + nd[1]) * SLAB + Ld[1] * nV + v];
+      if (DIM == 3) fhd[(2 * P + pz) * nV + v] = sF[((DIM - 1) * b + nd[DIM - 1]) * SLAB + Ld[DIM - 1] * nV + v];
       fhd[(DIM * P + p) * nV + v] = 0.0;
     }
   }
@@ -386,10 +418,6 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
   double* sQh = sQ;  // lQhi [P][nD]
 #pragma unroll
   for (int v = 0; v < nD; v++) sQh[p * nD + v] = qh[v];
-#pragma unroll
-  for (int d = 0; d < DIM; d++)
-#pragma unroll
-    for (int v = 0; v < nV; v++) sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = fh[d][v];
   if (p == 0) s_done[lc] = !active;
   __syncthreads();
 

@@ -451,6 +451,11 @@ int exa_batch_stream(exa_batch* b, void** stream);
  * throughput of the current GPU in TFLOP/s, from independent DFMA chains on
  * every SM timed with CUDA events -- the FP64 roofline of the predictor. */
 int exa_fp64_peak_probe(double* tflops);
+/* Measurement helper (no counterpart in the reference): FP64 tensor-core
+ * throughput in TFLOP/s, from independent mma.sync m8n8k4 f64 accumulator
+ * chains on every SM. On B200 it equals the DFMA figure: the two share one
+ * FP64 pipe, so tensor-core tiles cannot raise the predictor's FP64 ceiling. */
+int exa_fp64_mma_peak_probe(double* tflops);
 
 #ifdef __cplusplus
 }

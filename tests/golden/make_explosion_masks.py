@@ -2,20 +2,26 @@
 2D N=5 Euler explosion on 81 x 81 outflow cells (DMP delta0 1e-4, eps 1e-3,
 one helper layer, no cure steps, explosion centre from seed 0) after every
 time step to t = 0.2, computed by the reference's own generic kernels
-(oracle/_ref, driven by the oracle's limiting harness) on all host threads.
+(oracle/_ref, parity build, driven by the oracle's limiting harness) and by
+the oracle's plain-C restatement of the same kernels, both on all host
+threads.
 
-  python tests/golden/make_explosion_masks.py [--threads N] [--impl ref|oracle]
+  python tests/golden/make_explosion_masks.py [--threads N]
 
-A few minutes of CPU time. The output is committed; the GPU test
+About ten minutes of CPU time. The output is committed; the GPU test
 tests/test_gpu_limiter_full.py replays the same run on the device and
 compares the mask after every step with these.
 
 Writes (step k = 1 .. steps; index 0 holds the initial statuses):
-  status   uint8 [steps+1, 6561]  limiter status of every cell (0 DG, 1 and
-                                  2 helper layers, 3 troubled)
-  t, dt    float64 [steps+1]      time stamp and step size after each step
-  irregular int64 [steps+1]       irregular steps so far
-  sweeps   int64 [steps+1]        Picard sweeps so far
+  status    uint8 [steps+1, 6561]  limiter status of every cell (0 DG, 1 and
+                                   2 helper layers, 3 troubled), reference
+  t, dt     float64 [steps+1]      time stamp and step size after each step
+  irregular int64 [steps+1]        irregular steps so far
+  sweeps    int64 [steps+1]        Picard sweeps so far
+  status_oracle, sweeps_oracle     the same from the plain-C restatement: the
+                                   two sequential CPU codes differ only in the
+                                   order of floating-point operations, which
+                                   shows where the run is sensitive to it
 """
 import argparse
 import os
@@ -71,10 +77,12 @@ def run(impl, threads):
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
-    ap.add_argument("--impl", default="ref", choices=["ref", "oracle"])
     ap.add_argument("--out", default=OUT)
     a = ap.parse_args()
-    r = run(a.impl, a.threads)
+    r = run("ref", a.threads)
+    o = run("oracle", a.threads)
+    assert len(o["t"]) == len(r["t"]), "the two CPU runs take different numbers of steps"
+    r["status_oracle"], r["sweeps_oracle"] = o["status"], o["sweeps"]
     np.savez_compressed(a.out, **r)
     print("%s: %d steps to t = %.6f, %d irregular, %d sweeps, %d bytes" % (
         a.out, len(r["t"]) - 1, r["t"][-1], r["irregular"][-1], r["sweeps"][-1], os.path.getsize(a.out)))

@@ -10,12 +10,29 @@ reference's loop, no clamp of the last step).
 Expected values: tests/golden/explosion_masks_81sq_N5.npz, the limiter
 status of every cell after every step of the same run by the reference's
 generic kernels compiled from its sources (oracle/_ref, parity build, driven
-by the oracle's limiting harness), made by tests/golden/make_explosion_masks.py.
+by the oracle's limiting harness), and by the oracle's plain-C restatement
+of those kernels; made by tests/golden/make_explosion_masks.py.
 
-Bar: the status of every cell (troubled cells and both helper layers) equal
-after every step; the same number of steps, irregular steps (steps with a
-local recomputation) and Picard sweeps at every step; time and step size to
-1e-12 relative (the two sum the same values in different orders).
+What the two CPU runs show: they are sequential codes that differ only in
+the order of floating-point operations, and their masks are identical for
+the first 551 of 755 steps; from step 552, when the blast reaches the domain
+corners, they disagree on 1,370 (step, cell) pairs, all in 38 cells within
+four cells of a corner. One cell's Picard stop test (squared update summed
+over the cell < 1e-14) already falls on different sides of the threshold at
+step 344, so the sweep counts part there. The troubled-cell decisions at the
+corners are thus decided by round-off in any implementation that does not
+repeat the reference's operation order exactly.
+
+Bar for the GPU against the reference:
+* the mask of every cell identical at every step before the first step at
+  which the two CPU runs disagree (steps 0..551), and the same number of
+  steps to t >= 0.2 (755);
+* the number of irregular steps (local recomputations) identical at every
+  step, time and step size to 1e-12 relative at every step;
+* after that, every differing (step, cell) lies within four cells of a domain
+  corner, and there are at most twice as many as between the two CPU runs;
+* Picard sweep counts may differ (borderline stop tests; the CPU runs differ
+  by 2,813 sweeps of 8.95 M by the end), by at most 0.1 % of the total.
 """
 import os
 
@@ -37,13 +54,21 @@ def eb():
     return exahype_b200
 
 
+def near_corner(cells, n=81, r=4):
+    x, y = cells % n, cells // n
+    return (np.minimum(x, n - 1 - x) < r) & (np.minimum(y, n - 1 - y) < r)
+
+
 def test_explosion_81x81_mask_every_step_to_t02(eb):
     from exahype_b200 import problems
     ref = np.load(GOLDEN)
     status, t_ref, dt_ref = ref["status"], ref["t"], ref["dt"]
-    irr_ref, sw_ref = ref["irregular"], ref["sweeps"]
+    irr_ref, sw_ref, status_o = ref["irregular"], ref["sweeps"], ref["status_oracle"]
     nsteps = len(t_ref) - 1
     assert t_ref[-1] >= 0.2 > t_ref[-2] and nsteps > 700
+    cpu_diff = status != status_o
+    first_cpu = int(np.nonzero(cpu_diff.any(axis=1))[0][0])
+    assert first_cpu > 500 and near_corner(np.nonzero(cpu_diff.any(axis=0))[0]).all()
 
     luh, fv, _ = problems.explosion(2, 5, (81, 81), seed=0)
     s = eb.Solver(2, 5)
@@ -52,23 +77,40 @@ def test_explosion_81x81_mask_every_step_to_t02(eb):
     g.set_fv_initial(fv)
     g.init(0.0)
 
-    def check(k):
-        sg = g.status()
-        diff = np.nonzero(sg != status[k])[0]
-        assert diff.size == 0, "step %d: status differs in %d cells, first %s: gpu %s reference %s" % (
-            k, diff.size, diff[:8].tolist(), sg[diff[:8]].tolist(), status[k][diff[:8]].tolist())
+    gpu_status = np.empty_like(status)
+    irr_diff = []
+    t_rel = dt_rel = 0.0
+    st = None
+    for k in range(nsteps + 1):
+        if k:
+            g.step(1)
+        gpu_status[k] = g.status()
         st = g.state()
         assert st["steps"] == k
-        assert st["irregular_steps"] == irr_ref[k], (k, st, irr_ref[k])
-        assert st["picard_sweeps"] == sw_ref[k], (k, st, sw_ref[k])
-        assert abs(st["t"] - t_ref[k]) <= 1e-12 * max(t_ref[k], 1e-300), (k, st["t"], t_ref[k])
-        assert abs(st["dt"] - dt_ref[k]) <= 1e-12 * dt_ref[k], (k, st["dt"], dt_ref[k])
-        return st
-
-    check(0)
-    for k in range(1, nsteps + 1):
-        g.step(1)
-        st = check(k)
-    # the reference's loop ends here too: t >= 0.2 after exactly nsteps steps
-    assert st["t"] >= 0.2
+        if st["irregular_steps"] != irr_ref[k]:
+            irr_diff.append((k, st["irregular_steps"], int(irr_ref[k])))
+        t_rel = max(t_rel, abs(st["t"] - t_ref[k]) / max(t_ref[k], 1e-300))
+        dt_rel = max(dt_rel, abs(st["dt"] - dt_ref[k]) / dt_ref[k])
+    d = gpu_status != status
+    steps_d = np.nonzero(d.any(axis=1))[0]
+    first_gpu = int(steps_d[0]) if steps_d.size else None
+    dcells = np.nonzero(d.any(axis=0))[0]
+    vs_oracle = int((gpu_status != status_o).sum())
+    sweep_gap = st["picard_sweeps"] - int(sw_ref[-1])
+    print("explosion 81x81 to t=0.2, GPU vs reference: %d steps; masks identical through step %s, then %d "
+          "differing (step, cell) pairs in %d steps and %d cells (CPU restatement vs reference: from step %d, "
+          "%d pairs; GPU vs CPU restatement: %d pairs); irregular-count differences %d; sweeps %+d of %d; "
+          "max relative t %.2e dt %.2e" % (
+              nsteps, (first_gpu - 1) if first_gpu is not None else nsteps, int(d.sum()), steps_d.size,
+              dcells.size, first_cpu, int(cpu_diff.sum()), vs_oracle, len(irr_diff), sweep_gap, int(sw_ref[-1]),
+              t_rel, dt_rel))
+    assert first_gpu is None or first_gpu >= first_cpu, (
+        "mask differs at step %d, before the CPU runs part (%d): cells %s" % (
+            first_gpu, first_cpu, np.nonzero(d[first_gpu])[0][:8].tolist()))
+    assert st["t"] >= 0.2 and st["steps"] == nsteps
+    assert not irr_diff, "irregular-step count differs at %d steps, first %s" % (len(irr_diff), irr_diff[:3])
+    assert t_rel <= 1e-12 and dt_rel <= 1e-12, (t_rel, dt_rel)
+    assert near_corner(dcells).all(), "mask differences away from the corners: %s" % dcells[~near_corner(dcells)][:8]
+    assert d.sum() <= 2 * cpu_diff.sum(), (int(d.sum()), int(cpu_diff.sum()))
+    assert abs(sweep_gap) <= 1e-3 * sw_ref[-1]
     assert (status[-1] == 3).any() and irr_ref[-1] > 0.9 * nsteps
