@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libexahype_b200.so")
 PDE_EULER = 0
 PDE_EULER_TEST = 1
 PDE_ELASTIC = 2  # linear elastic waves: 9 variables + lambda, mu, rho; linear kernels
+PDE_EULER_SOURCE_NCP = 3  # the kernel-test mock with an algebraic source and a non-conservative product
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE = -1, 0, 1
 # predictor variants beyond the autotuned 0..3: the mixed-precision predictor
 PREDICTOR_MIXED, PREDICTOR_MIXED_2 = 4, 5

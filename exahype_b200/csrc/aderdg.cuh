@@ -78,6 +78,50 @@ struct PredictorTemps {  // optional reference-layout temporaries (golden replay
   double *lQi, *lFi, *lQhi, *lFhi;
 };
 
+// The source term of a PDE with an algebraic source and/or a
+// non-conservative product at space-time node (x, y, z; t) of a cell whose
+// iterate lQi sits in shared memory (node stride QS): S = algebraicSource(Q)
+// - B(Q) gradQ, the gradients contracted from the iterate's lines with dudx
+// and 1/dx (3d/spaceTimePredictorNonlinear.cpph:171-174, 199-202, 228-231,
+// 238-276; 2d :145-148, 169-172, 180-211).
+template <int DIM, int N, class PDE>
+__device__ __forceinline__ void node_source(const double* sQ, int QS, int t, int x, int y, int z, double invDx0,
+                                            double invDx1, double invDx2, double* S) {
+  using Sh = Shape<DIM, N, PDE>;
+  constexpr int b = Sh::b, nV = Sh::nV, nD = Sh::nD;
+  const OrderTables& T = c_tab[N];
+  const int p = (z * b + y) * b + x;
+  double Q[nD];
+#pragma unroll
+  for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
+  if constexpr (PDE::kSource) {
+    PDE::algebraicSource(Q, S);
+  } else {
+#pragma unroll
+    for (int v = 0; v < nV; v++) S[v] = 0.0;
+  }
+  if constexpr (PDE::kNCP) {
+    double G[DIM][nV];
+#pragma unroll
+    for (int v = 0; v < nV; v++) {
+      double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+      for (int n = 0; n < b; n++) {
+        gx += invDx0 * sQ[((z * b + y) * b + n) * QS + t * nD + v] * T.dudx[x * b + n];
+        gy += invDx1 * sQ[((z * b + n) * b + x) * QS + t * nD + v] * T.dudx[y * b + n];
+        if (DIM == 3) gz += invDx2 * sQ[((n * b + y) * b + x) * QS + t * nD + v] * T.dudx[z * b + n];
+      }
+      G[0][v] = gx;
+      G[1][v] = gy;
+      if (DIM == 3) G[DIM - 1][v] = gz;
+    }
+    double B[nV];
+    PDE::template ncp<DIM>(Q, G, B);
+#pragma unroll
+    for (int v = 0; v < nV; v++) S[v] -= B[v];
+  }
+}
+
 template <int DIM, int N, class PDE, bool TEMPS, int VSPLIT, int MINB>
 __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREADS, MINB)
     predictor_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
@@ -86,6 +130,8 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
                      const int* __restrict__ count) {
   using C = PredictorCfg<DIM, N, PDE, VSPLIT, MINB>;
   constexpr int b = C::b, P = C::P, F = C::F, nV = C::nV, nD = C::nD, NVT = C::NVT, QS = C::QS;
+  constexpr bool SRC = PDE::kSource || PDE::kNCP;  // useSource || useNCP
+  static_assert(!SRC || VSPLIT == 1, "the source term is formed per node by one thread");
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
 
@@ -136,6 +182,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
   }
 
   double fh[DIM][nV];  // lead threads: time-averaged fluxes of the last sweep
+  double sh[SRC ? nV : 1];  // and the time-averaged source (lShi)
   bool done = !active;
   int it_done = 0;
   for (int iter = 0; iter < C::maxIter; iter++) {
@@ -199,11 +246,20 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
         const double usy = (T.w[t] * wz) * wx * dt * invDx1;
         const double usz = DIM == 3 ? (T.w[t] * wy) * wx * dt * invDx2 : 0.0;
         const double r0 = wpt * T.FL[t];
+        // source and non-conservative product, weighted w_t w_xyz dt (:238-276)
+        double src[SRC ? nV : 1];
+        if constexpr (SRC) {
+          node_source<DIM, N, PDE>(sQ, QS, t, x, y, z, invDx0, invDx1, invDx2, src);
+          const double uss = (DIM == 3 ? ((T.w[t] * wz) * wy) * wx : (T.w[t] * wy) * wx) * dt;
+#pragma unroll
+          for (int v = 0; v < nV; v++) src[v] *= uss;
+        }
         // discrete time integral (:280-311): lQi_new[l] += iw rhs[t] iK1[l][t]
 #pragma unroll
         for (int j = 0; j < NVT; j++) {
           double rhs = r0 * lu[j] - usx * ax[j] - usy * ay[j];
           if (DIM == 3) rhs -= usz * az[j];
+          if constexpr (SRC) rhs += src[j];
           const double ir = iw * rhs;
 #pragma unroll
           for (int l = 0; l < b; l++) qn[l][j] = fma(ir, T.iK1[l * b + t], qn[l][j]);
@@ -252,6 +308,10 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
           for (int d = 0; d < DIM; d++)
 #pragma unroll
             for (int v = 0; v < nV; v++) fh[d][v] = 0.0;
+          if constexpr (SRC) {
+#pragma unroll
+            for (int v = 0; v < nV; v++) sh[v] = 0.0;
+          }
           for (int t = 0; t < b; t++) {
             double Q[nD];
 #pragma unroll
@@ -262,12 +322,22 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
             for (int d = 0; d < DIM; d++)
 #pragma unroll
               for (int v = 0; v < nV; v++) fh[d][v] += Fl[d][v] * T.w[t];
+            double St[SRC ? nV : 1];
+            if constexpr (SRC) {  // lShi (:391-396), from the same iterate
+              node_source<DIM, N, PDE>(sQ, QS, t, x, y, z, invDx0, invDx1, invDx2, St);
+#pragma unroll
+              for (int v = 0; v < nV; v++) sh[v] += St[v] * T.w[t];
+            }
             if (TEMPS) {
               double* dst = tmp.lFi + (((size_t)cell * b + t) * P + p) * (DIM + 1) * nV;
 #pragma unroll
               for (int d = 0; d < DIM; d++)
 #pragma unroll
                 for (int v = 0; v < nV; v++) dst[d * nV + v] = Fl[d][v];
+              if constexpr (SRC) {
+#pragma unroll
+                for (int v = 0; v < nV; v++) dst[DIM * nV + v] = St[v];
+              }
             }
           }
         }
@@ -311,7 +381,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
       fhd[(0 * P + p) * nV + v] = fh[0][v];
       fhd[(1 * P + py) * nV + v] = fh[1][v];
       if (DIM == 3) fhd[(2 * P + pz) * nV + v] = fh[DIM - 1][v];
-      fhd[(DIM * P + p) * nV + v] = 0.0;
+      fhd[(DIM * P + p) * nV + v] = SRC ? sh[SRC ? v : 0] : 0.0;
     }
   }
   __syncthreads();  // everyone has read its lQi row
@@ -350,6 +420,7 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
         for (int m = 0; m < b; m++) sz = fma(sK[z * b + m], Fz[m * b * b * nV], sz);
         du += sz * usz;
       }
+      if constexpr (SRC) du += wpt * sh[v];  // useSourceOrNCP: + w_xyz lShi (3d :206-224, 2d :158-172)
       dst[v] = du;
     }
   }
@@ -393,11 +464,11 @@ __global__ void __launch_bounds__(PredictorCfg<DIM, N, PDE, VSPLIT, MINB>::THREA
 }
 
 // ---------------------------------------------------------------------------
-// Rusanov flux on interior faces: riemannSolverNonlinear<useNCP=false>
+// Rusanov flux on interior faces: riemannSolverNonlinear<useNCP>
 // (3d/riemannSolverNonlinear.cpph:37-117). One warp per face: weighted face
 // averages of both states by warp-shuffle reduction, one smax per face from
 // the averaged states, then F = (FL+FR)/2 - smax (QR-QL)/2 written to both
-// sides. The face joins cell `left` (its face 2*dir+1) and cell `right` (its
+// sides (with a non-conservative product, plus / minus half its value). The face joins cell `left` (its face 2*dir+1) and cell `right` (its
 // face 2*dir).
 template <int DIM, int N, class PDE>
 __device__ __forceinline__ void face_average(const double* Q, int lane, double* avg) {
@@ -428,6 +499,24 @@ __device__ __forceinline__ double face_smax(const double* aL, const double* aR, 
     if (sR < fabs(LR[k])) sR = fabs(LR[k]);
   }
   return (sL < sR) ? sR : sL;
+}
+
+// Component k of the non-conservative product at one face node of a PDE
+// with kNCP: B(Qavg) gradQ with Qavg = (QL + QR) / 2 and gradQ zero but for
+// the normal direction's row QR - QL (riemannSolverNonlinear.cpph 3d :92-100,
+// 2d :86-93).
+template <int DIM, class PDE>
+__device__ __forceinline__ double face_ncp(const double* QL, const double* QR, int dir, int k) {
+  constexpr int nV = PDE::nVar, nD = PDE::nVar + PDE::nPar;
+  double Qavg[nD], G[DIM][nV], B[nV];
+#pragma unroll
+  for (int l = 0; l < nD; l++) Qavg[l] = l < nV ? 0.5 * (QR[l] + QL[l]) : 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+#pragma unroll
+    for (int l = 0; l < nV; l++) G[d][l] = d == dir ? QR[l] - QL[l] : 0.0;
+  PDE::template ncp<DIM>(Qavg, G, B);
+  return B[k];
 }
 
 template <int DIM, int N, class PDE>
@@ -468,8 +557,17 @@ __global__ void __launch_bounds__(128) riemann_kernel(const double* __restrict__
     const int e = lane + 32 * i;
     if (e < E) {
       const double r = 0.5 * (fr[i] + fl[i]) - 0.5 * smax * dq[i];
-      FL[e] = r;
-      FR[e] = r;
+      if constexpr (PDE::kNCP) {
+        // useNCP (:92-110): the product of the node's mean state and its jump
+        // along the normal splits into fluctuations, + on the left, - on the right
+        const int fn = e / nV, k = e - fn * nV;
+        const double half = 0.5 * face_ncp<DIM, PDE>(QL + fn * nD, QR + fn * nD, dir, k);
+        FL[e] = r + half;
+        FR[e] = r - half;
+      } else {
+        FL[e] = r;
+        FR[e] = r;
+      }
     }
   }
 }
@@ -521,8 +619,15 @@ __global__ void __launch_bounds__(128) boundary_kernel(const double* __restrict_
 #pragma unroll
     for (int k = 0; k < nV; k++) {
       const double fi = FIn[fn * nV + k], qi = QIn[fn * nD + k];
-      FIn[fn * nV + k] = even ? 0.5 * (fi + fo[k]) - 0.5 * smax * (qi - qo[k])
-                              : 0.5 * (fo[k] + fi) - 0.5 * smax * (qo[k] - qi);
+      double r = even ? 0.5 * (fi + fo[k]) - 0.5 * smax * (qi - qo[k])
+                      : 0.5 * (fo[k] + fi) - 0.5 * smax * (qo[k] - qi);
+      if constexpr (PDE::kNCP) {  // the cell is the right side of an even face, the left of an odd one
+        if (even)
+          r -= 0.5 * face_ncp<DIM, PDE>(qo, QIn + fn * nD, dir, k);
+        else
+          r += 0.5 * face_ncp<DIM, PDE>(QIn + fn * nD, qo, dir, k);
+      }
+      FIn[fn * nV + k] = r;
     }
   }
 }
@@ -690,7 +795,11 @@ __global__ void __launch_bounds__(CorrectorCfg<DIM, N, PDE>::THREADS)
     const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, cell_width(geo, inst, 2)) : 0.0;
     const double den = corrector_node<DIM, N, PDE>(q, do_update ? st + C::ODU + p * nV : nullptr, st + C::OFB, p,
                                                    geo, inst, dt_ptr, invDx0, invDx1, invDx2);
-    dtmin = __ddiv_rn(__dmul_rn(0.9, pnpm(N)), den);
+    // dt = std::min(dt, candidate) from DBL_MAX, as the reference: a NaN or
+    // infinite candidate (a node with negative pressure, a zero denominator)
+    // never replaces the running minimum, here nor in the reductions below
+    const double cand = __ddiv_rn(__dmul_rn(0.9, pnpm(N)), den);
+    dtmin = (cand < dtmin) ? cand : dtmin;
     if (do_update)
 #pragma unroll
       for (int v = 0; v < nV; v++) st[C::OU + p * QS + v] = q[v];

@@ -275,7 +275,11 @@ struct Launch {
                        unsigned long long* acc, int variant, cudaStream_t st) {
     if (n <= 0) return EXA_OK;
     int rc;
-    if (temps)
+    if constexpr (PDE::kSource || PDE::kNCP)  // source terms: the node form (1 or 2 blocks per SM)
+      rc = temps ? launch_pred<true, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st)
+           : variant == 3 ? launch_pred<false, 1, 2>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st)
+                          : launch_pred<false, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
+    else if (temps)
       rc = variant == 1 || variant == 2 ? launch_lines<true, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st)
                                         : launch_pred<true, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else if (variant == 1 || (variant == 2 && !kLines2))
@@ -396,6 +400,7 @@ struct LinearLaunch {
 
 #define EXA_ORDERS_EULER(X, D) X(D, 3, EulerPDE, 0) X(D, 4, EulerPDE, 0) X(D, 5, EulerPDE, 0) X(D, 7, EulerPDE, 0)
 #define EXA_ORDERS_TEST(X, D) X(D, 3, EulerTestPDE, 1) X(D, 5, EulerTestPDE, 1)
+#define EXA_ORDERS_SOURCE_NCP(X, D) X(D, 3, EulerSourceNCPPDE, 3) X(D, 5, EulerSourceNCPPDE, 3)
 #define EXA_ORDERS_ELASTIC(X, D) X(D, 3, ElasticPDE, 2) X(D, 4, ElasticPDE, 2) X(D, 5, ElasticPDE, 2)
 
 static bool find_kernels(int dim, int order, int pde, KernelSet* out) {
@@ -408,6 +413,8 @@ static bool find_kernels(int dim, int order, int pde, KernelSet* out) {
   EXA_ORDERS_EULER(X, 3)
   EXA_ORDERS_TEST(X, 2)
   EXA_ORDERS_TEST(X, 3)
+  EXA_ORDERS_SOURCE_NCP(X, 2)
+  EXA_ORDERS_SOURCE_NCP(X, 3)
 #undef X
 #define X(D, NN, PDE_, ID)                                     \
   if (dim == D && order == NN && pde == ID) {                 \

@@ -8,6 +8,10 @@
 //   fvBoundaryValues(...)           -- the FV solver's boundaryValues(x,t,dt,faceIndex,normal,QIn,QOut)
 //   isPhysicallyAdmissible(min,max) -- isPhysicallyAdmissible(...)
 //   observables(Q, obs)             -- mapDiscreteMaximumPrincipleObservables(...)
+//   kSource, kNCP                   -- the generated glue's useSource / useNCP
+// and, where kSource / kNCP are set,
+//   algebraicSource(Q, S[nVar])                     -- algebraicSource(Q, S)
+//   ncp<DIM>(Q, gradQ[DIM][nVar], BgradQ[nVar])     -- nonConservativeProduct(Q, gradQ, BgradQ)
 // New PDEs are added by writing such a struct and instantiating the kernel
 // templates for it (see capi.cu).
 #pragma once
@@ -26,6 +30,7 @@ struct EulerPDE {
   static constexpr int nPar = 0;
   static constexpr int nObs = 5;
   static constexpr bool kLinear = false;  // nonlinear kernels (Picard predictor, Rusanov on fluxes)
+  static constexpr bool kSource = false, kNCP = false;
 
   __host__ __device__ static double pressure(const double* Q, double irho) {
     const double GAMMA = 1.4;
@@ -120,6 +125,7 @@ struct EulerTestPDE {
   static constexpr int nPar = 1;
   static constexpr int nObs = 5;
   static constexpr bool kLinear = false;
+  static constexpr bool kSource = false, kNCP = false;
 
   template <int DIM>
   __host__ __device__ static double pressure(const double* Q, double irho) {
@@ -188,6 +194,34 @@ struct EulerTestPDE {
   }
 };
 
+// The kernel-test mock with an algebraic source and a non-conservative
+// product switched on (useSource = useNCP = true): the source is this
+// library's choice (momentum damping, an energy source proportional to the
+// density), the product is the tests' non-zero mock
+// (exahype/tests/kernels/c/GenericEulerKernelTest3D.cpp:84-110, 2D :80-103,
+// with _setNcpAndMatrixBToZero false). It exercises the predictor's source
+// branch (3d/spaceTimePredictorNonlinear.cpph:238-276), the time-averaged
+// source of the volume integral and the Riemann solver's fluctuations
+// (3d/riemannSolverNonlinear.cpph:92-110).
+struct EulerSourceNCPPDE : EulerTestPDE {
+  static constexpr bool kSource = true, kNCP = true;
+  __device__ static void algebraicSource(const double* Q, double* S) {
+    S[0] = 0.0;
+    S[1] = -0.5 * Q[1];
+    S[2] = -0.5 * Q[2];
+    S[3] = -0.5 * Q[3];
+    S[4] = 0.1 * Q[0];
+  }
+  template <int DIM>
+  __device__ static void ncp(const double* Q, const double (*G)[nVar], double* B) {
+    B[0] = Q[0];
+    B[1] = Q[3];
+    B[2] = 3.0;
+    B[3] = G[0][0];
+    B[4] = 0.7;
+  }
+};
+
 // Linear elastic waves in velocity-stress form, the PDE of the reference's
 // linear kernel tests (exahype/tests/kernels/c/ElasticityKernelTest2D.cpp:
 // 31-235): variables sxx syy szz sxy syz sxz u v w, material parameters
@@ -207,6 +241,7 @@ struct ElasticPDE {
   static constexpr int nPar = 3;
   static constexpr int nObs = 9;
   static constexpr bool kLinear = true;
+  static constexpr bool kSource = false, kNCP = false;  // (its product enters the linear kernels directly)
 
   // the product of one direction: B_d = B_d(Q) gradQ_d (a linear PDE's
   // product separates by direction)
@@ -316,5 +351,7 @@ struct Hooks<EulerTestPDE, DIM> {
     return EulerTestPDE::max_abs_eigenvalue_exact<DIM>(Q, d);
   }
 };
+template <int DIM>
+struct Hooks<EulerSourceNCPPDE, DIM> : Hooks<EulerTestPDE, DIM> {};
 
 }  // namespace exa

@@ -42,6 +42,14 @@ extern "C" {
 #define EXA_PDE_EULER 0      /* compressible Euler, 5 variables (EulerADERDG demonstrator) */
 #define EXA_PDE_EULER_TEST 1 /* the reference kernel tests' mock Euler with one parameter */
 #define EXA_PDE_ELASTIC 2    /* linear elastic waves, 9 variables + 3 parameters (lambda, mu, rho); linear kernels */
+/* EXA_PDE_EULER_TEST with useSource = useNCP = true: an algebraic source
+ * (momentum damping, an energy source proportional to the density) and the
+ * kernel tests' non-zero non-conservative product mock
+ * (exahype/tests/kernels/c/GenericEulerKernelTest3D.cpp:84-110); orders 3
+ * and 5. The predictor's source branch runs in the node-form kernel (the
+ * line form has none), the Riemann and boundary kernels add the product's
+ * fluctuations, the volume integral the time-averaged source. */
+#define EXA_PDE_EULER_SOURCE_NCP 3
 
 /* Boundary kinds for exa_boundary_conditions / exa_mesh_create. */
 #define EXA_BC_PERIODIC (-1)

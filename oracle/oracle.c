@@ -30,7 +30,37 @@ const double* orc_table(const char* name, int N) {
 }
 
 int orc_nvar(const orc_solver* s) { return s->pde == 2 ? 9 : 5; }
-int orc_npar(const orc_solver* s) { return s->pde == 1 ? 1 : s->pde == 2 ? 3 : 0; }
+int orc_npar(const orc_solver* s) { return (s->pde == 1 || s->pde == 3) ? 1 : s->pde == 2 ? 3 : 0; }
+
+/* pde 3: the kernel-test mock with an algebraic source and its
+ * non-conservative product switched on (useSource = useNCP = true) */
+static int use_source(const orc_solver* s) { return s->pde == 3; }
+static int use_ncp(const orc_solver* s) { return s->pde == 3; }
+
+/* algebraicSource (UserSolverInterface.h:92) of pde 3: momentum damping and
+ * an energy source proportional to the density; zero for the other PDEs */
+void orc_source(const orc_solver* s, const double* Q, double* S) {
+  for (int v = 0; v < 5; v++) S[v] = 0.0;
+  if (s->pde != 3) return;
+  S[1] = -0.5 * Q[1];
+  S[2] = -0.5 * Q[2];
+  S[3] = -0.5 * Q[3];
+  S[4] = 0.1 * Q[0];
+}
+
+/* nonConservativeProduct (UserSolverInterface.h:116) of the nonlinear
+ * kernels: BgradQ[nV] from Q and gradQ[dim][nV]. pde 3: the non-zero mock of
+ * exahype/tests/kernels/c/GenericEulerKernelTest2D.cpp:80-103 and
+ * GenericEulerKernelTest3D.cpp:84-110 (_setNcpAndMatrixBToZero false). */
+void orc_ncp_nonlinear(const orc_solver* s, const double* Q, const double* gradQ, double* BgradQ) {
+  for (int v = 0; v < 5; v++) BgradQ[v] = 0.0;
+  if (s->pde != 3) return;
+  BgradQ[0] = Q[0];
+  BgradQ[1] = Q[3];
+  BgradQ[2] = 3.0;
+  BgradQ[3] = gradQ[0];
+  BgradQ[4] = 0.7;
+}
 
 /* ---- PDE hooks ----------------------------------------------------------
  * pde 0: Demonstrators/EulerADERDG/MyEulerSolver_ADERDG.cpp:102-135
@@ -100,7 +130,7 @@ static double dmin(double a, double b) { return (b < a) ? b : a; } /* std::min *
 /* ---- geometry helpers --------------------------------------------------- */
 typedef struct {
   int d, N, b, nz, nV, nD, P, F;
-  const double *w, *FL, *FR, *Kxi, *iK1;
+  const double *w, *FL, *FR, *Kxi, *iK1, *dudx;
   double wz[MAXB]; /* z-weights: w in 3D, {1.0} in 2D */
 } geo;
 
@@ -119,6 +149,7 @@ static geo mkgeo(const orc_solver* s) {
   g.FR = orc_table("FRCoeff", g.N);
   g.Kxi = orc_table("Kxi", g.N);
   g.iK1 = orc_table("iK1", g.N);
+  g.dudx = orc_table("dudx", g.N);
   for (int i = 0; i < MAXB; i++) g.wz[i] = (s->dim == 3 && i < g.b) ? g.w[i] : 1.0;
   return g;
 }
@@ -191,6 +222,37 @@ static int picard(const orc_solver* s, const geo* g, const double* luh, const do
               for (int v = 0; v < nV; v++)
                 for (int n = 0; n < b; n++) RHS(t, l, y, x, v) -= us * LFI(t, n, y, x, 2, v) * g->Kxi[n * b + l];
           }
+      /* gradients of lQi for the non-conservative product (:171-174,
+       * :199-202, :228-231; 2d :145-148, :169-172), then the algebraic
+       * source minus the product, stored in the source block of lFi and
+       * added to rhs with w_t w_xyz dt (:238-276; 2d :180-211) */
+      if (use_source(s) || use_ncp(s))
+        for (int z = 0; z < nz; z++)
+          for (int y = 0; y < b; y++)
+            for (int x = 0; x < b; x++) {
+              double gq[3 * 5];
+              for (int i = 0; i < 3 * 5; i++) gq[i] = 0.0;
+              if (use_ncp(s))
+                for (int v = 0; v < nV; v++)
+                  for (int n = 0; n < b; n++) {
+                    gq[0 * 5 + v] += 1.0 * invDx[0] * LQI(z, y, n, t, v) * g->dudx[x * b + n];
+                    gq[1 * 5 + v] += 1.0 * invDx[1] * LQI(z, n, x, t, v) * g->dudx[y * b + n];
+                    if (d == 3) gq[2 * 5 + v] += 1.0 * invDx[2] * LQI(n, y, x, t, v) * g->dudx[z * b + n];
+                  }
+              const double weight =
+                  d == 3 ? g->w[t] * g->w[z] * g->w[y] * g->w[x] : g->w[t] * g->w[y] * g->w[x];
+              const double us = weight * dt;
+              double S[5], ncp[5];
+              orc_source(s, &LQI(z, y, x, t, 0), S);
+              if (use_ncp(s)) {
+                orc_ncp_nonlinear(s, &LQI(z, y, x, t, 0), gq, ncp);
+                for (int v = 0; v < nV; v++) S[v] -= ncp[v];
+              }
+              for (int v = 0; v < nV; v++) {
+                LFI(t, z, y, x, d, v) = S[v];
+                RHS(t, z, y, x, v) += us * S[v];
+              }
+            }
     }
     /* discrete time integral and residual :280-311 */
     double sq_res = 0.0;
@@ -222,7 +284,7 @@ static int picard(const orc_solver* s, const geo* g, const double* luh, const do
  * the variable: x:(z,y,x) y:(z,x,y) z:(y,x,z); face nodes for direction d run
  * over the other coordinates in (z,y,x) order. */
 static void time_average_extrapolate(const geo* g, const double* lQi, const double* lFi, double* lQhi, double* lFhi,
-                                     double* lQhbnd, double* lFhbnd) {
+                                     double* lQhbnd, double* lFhbnd, int source_block) {
   const int b = g->b, nV = g->nV, nD = g->nD, d = g->d, nz = g->nz, dd1 = d + 1;
   const int P = g->P, F = g->F;
   memset(lQhi, 0, sizeof(double) * P * nD);
@@ -237,6 +299,9 @@ static void time_average_extrapolate(const geo* g, const double* lQi, const doub
             lFhi[1 * P * nV + fy * nV + v] += lFi[((m * P + PT(*g, z, y, x)) * dd1 + 1) * nV + v] * g->w[m];
             if (d == 3)
               lFhi[2 * P * nV + fz * nV + v] += lFi[((m * P + PT(*g, z, y, x)) * dd1 + 2) * nV + v] * g->w[m];
+            /* lShi, the time-averaged source (3d :391-396, 2d :328-332) */
+            if (source_block)
+              lFhi[d * P * nV + PT(*g, z, y, x) * nV + v] += lFi[((m * P + PT(*g, z, y, x)) * dd1 + d) * nV + v] * g->w[m];
           }
         for (int v = 0; v < nD; v++)
           for (int m = 0; m < b; m++)
@@ -293,6 +358,14 @@ void orc_volume_integral(const orc_solver* s, double* lduh, const double* lFhi, 
       }
     }
   }
+  /* useSourceOrNCP: lduh += w_xyz lShi (3d :206-224, 2d :158-172) */
+  if (use_source(s) || use_ncp(s))
+    for (int z = 0; z < g.nz; z++)
+      for (int y = 0; y < b; y++)
+        for (int x = 0; x < b; x++) {
+          const double weight = g.d == 3 ? g.w[z] * g.w[y] * g.w[x] : g.w[y] * g.w[x];
+          for (int v = 0; v < nV; v++) lduh[PT(g, z, y, x) * nV + v] += weight * lFhi[(g.d * P + PT(g, z, y, x)) * nV + v];
+        }
 }
 
 int orc_predictor(const orc_solver* s, const double* luh, const double* dx, double dt, double* lQhbnd,
@@ -306,7 +379,7 @@ int orc_predictor(const orc_solver* s, const double* luh, const double* dx, doub
   double* lQhi = (double*)malloc(sizeof(double) * g.P * g.nD);
   double* lFhi = (double*)malloc(sizeof(double) * g.P * g.nV * (g.d + 1));
   const int it = picard(s, &g, luh, dx, dt, lQi, lFi, rhs);
-  time_average_extrapolate(&g, lQi, lFi, lQhi, lFhi, lQhbnd, lFhbnd);
+  time_average_extrapolate(&g, lQi, lFi, lQhi, lFhi, lQhbnd, lFhbnd, use_source(s) || use_ncp(s));
   if (lduh) orc_volume_integral(s, lduh, lFhi, dx);
   if (lQi_out) memcpy(lQi_out, lQi, sizeof(double) * st * g.nD);
   if (lFi_out) memcpy(lFi_out, lFi, sizeof(double) * st * (g.d + 1) * g.nV);
@@ -320,7 +393,7 @@ int orc_predictor(const orc_solver* s, const double* luh, const double* dx, doub
   return it;
 }
 
-/* riemannSolverNonlinear<useNCP=false>: 3d/riemannSolverNonlinear.cpph:37-117,
+/* riemannSolverNonlinear<useNCP>: 3d/riemannSolverNonlinear.cpph:37-117,
  * 2d/riemannSolverNonlinear.cpph:37-111 */
 void orc_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, const double* QR, int dir) {
   geo g = mkgeo(s);
@@ -344,11 +417,25 @@ void orc_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, 
     if (smR < fabs(LR[k])) smR = fabs(LR[k]);
   }
   const double smax = dmax(smL, smR);
-  for (int fn = 0; fn < g.F; fn++)
+  double gradQ[3 * 5] = {0}, Qavg[8] = {0}, ncp[5] = {0};
+  for (int fn = 0; fn < g.F; fn++) {
+    if (use_ncp(s)) { /* useNCP (3d :92-100, 2d :86-93): one-sided jump along the normal */
+      for (int l = 0; l < nV; l++) {
+        gradQ[dir * 5 + l] = QR[fn * nD + l] - QL[fn * nD + l];
+        Qavg[l] = 0.5 * (QR[fn * nD + l] + QL[fn * nD + l]);
+      }
+      orc_ncp_nonlinear(s, Qavg, gradQ, ncp);
+    }
     for (int k = 0; k < nV; k++) {
       FL[fn * nV + k] = 0.5 * (FR[fn * nV + k] + FL[fn * nV + k]) - 0.5 * smax * (QR[fn * nD + k] - QL[fn * nD + k]);
-      FR[fn * nV + k] = FL[fn * nV + k];
+      if (use_ncp(s)) {
+        FR[fn * nV + k] = FL[fn * nV + k] - 0.5 * ncp[k];
+        FL[fn * nV + k] = FL[fn * nV + k] + 0.5 * ncp[k];
+      } else {
+        FR[fn * nV + k] = FL[fn * nV + k];
+      }
     }
+  }
 }
 
 /* ADERDGSolver::applyBoundaryConditions (exahype/solvers/ADERDGSolver.cpp:2893-2962)

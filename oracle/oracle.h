@@ -17,7 +17,9 @@ extern "C" {
 /* PDE ids: 0 = Euler as in the EulerADERDG demonstrator (outflow boundary),
  *          1 = the "2.5D" Euler mock of the reference kernel tests (nPar = 1),
  *          2 = linear elastic waves of the reference kernel tests (nVar = 9,
- *              nPar = 3: lambda, mu, rho; linear kernels only). */
+ *              nPar = 3: lambda, mu, rho; linear kernels only),
+ *          3 = pde 1 with an algebraic source and the kernel tests' non-zero
+ *              non-conservative product (useSource = useNCP = true). */
 typedef struct {
   int dim;   /* 2 or 3 */
   int order; /* N, basis size N+1 */
@@ -47,6 +49,9 @@ double orc_stable_dt(const orc_solver* s, const double* luh, const double* dx);
 void orc_flux(const orc_solver* s, const double* Q, double* F /* [dim][nV] */);
 void orc_eigenvalues(const orc_solver* s, const double* Q, int d, double* lambda);
 void orc_ncp(const orc_solver* s, const double* Q, const double* gradQ /* [dim][nV] */, double* BgradQ);
+void orc_source(const orc_solver* s, const double* Q, double* S /* [nV] */);
+void orc_ncp_nonlinear(const orc_solver* s, const double* Q, const double* gradQ /* [dim][nV] */,
+                       double* BgradQ /* [nV] */);
 void orc_coefficient_matrix(const orc_solver* s, const double* Q, int d, double* Bn /* [nV][nV] */);
 
 /* Linear kernels (linear.c): spaceTimePredictorLinear (Cauchy-Kovalevski,

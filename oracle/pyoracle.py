@@ -127,7 +127,7 @@ class Kernels:
         self.dim, self.order, self.pde, self.impl = dim, order, pde, impl
         self.b = order + 1
         self.nvar = 9 if pde == 2 else 5
-        self.ndata = self.nvar + {1: 1, 2: 3}.get(pde, 0)
+        self.ndata = self.nvar + {1: 1, 2: 3, 3: 1}.get(pde, 0)
         self.P = self.b ** dim
         self.F = self.b ** (dim - 1)
         self._s = _Solver(dim, order, pde)
@@ -297,7 +297,7 @@ class Mesh:
                        ("sweeps", ctypes.c_long), ("run_until", ctypes.c_int)):
             getattr(self._l, self._pre + nm).restype = rt
         self.ncells = int(np.prod(cells))
-        self.shape = (self.ncells, (order + 1) ** dim, {1: 6, 2: 12}.get(pde, 5))
+        self.shape = (self.ncells, (order + 1) ** dim, {1: 6, 2: 12, 3: 6}.get(pde, 5))
 
     def _f(self, nm):
         return getattr(self._l, self._pre + nm)

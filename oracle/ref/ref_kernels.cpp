@@ -4,12 +4,16 @@
 // compiled once per dimension (-DDIMENSIONS=2/3) against the unmodified
 // reference sources by oracle/ref/Makefile and never ships with the product.
 //
-// The PDE classes below restate the two PDEs the reference uses for this
-// path:
+// The PDE classes below restate the PDEs the reference uses for this path:
 //   * EulerDemo  -- Demonstrators/EulerADERDG/MyEulerSolver_ADERDG.cpp:102-160
 //                   (5 variables, gamma 1.4, 3 momentum components in 2D too)
 //   * EulerTest  -- exahype/tests/kernels/c/GenericEulerKernelTest{2D,3D}.cpp:28-77
 //                   ("2.5D" Euler in 2D, one material parameter)
+//   * EulerSourceNCP -- EulerTest with useSource = useNCP = true: an algebraic
+//                   source of this repository's choosing and the kernel tests'
+//                   non-zero non-conservative product mock
+//                   (GenericEulerKernelTest3D.cpp:84-110 with
+//                   _setNcpAndMatrixBToZero false)
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -52,6 +56,7 @@ struct PDEBase : public exahype::solvers::ADERDGSolver {
   static constexpr double CFL = 0.9;
   static constexpr int PatchSize = 2 * N_ + 1;
   static constexpr int GhostLayerWidth = 2;
+  static constexpr bool kSourceNCP = false;  // instantiate the kernels with useSource = useNCP = true
   long fluxCalls = 0;
   int getDMPObservables() const override { return NumberOfVariables; }
   int getNodesPerCoordinateAxis() const override { return N_ + 1; }
@@ -157,6 +162,25 @@ struct EulerTest : public PDEBase<N_, 1> {
   }
   // GenericEulerKernelTest{2D,3D}.cpp: the zero system matrix of the mock
   void coefficientMatrix(const double* const, const int, double* Bn) { std::fill_n(Bn, 25, 0.0); }
+};
+
+template <int N_>
+struct EulerSourceNCP : public EulerTest<N_> {
+  static constexpr bool kSourceNCP = true;
+  void algebraicSource(const double* const Q, double* S) {
+    S[0] = 0.0;
+    S[1] = -0.5 * Q[1];
+    S[2] = -0.5 * Q[2];
+    S[3] = -0.5 * Q[3];
+    S[4] = 0.1 * Q[0];
+  }
+  void nonConservativeProduct(const double* const Q, const double* const gradQ, double* BgradQ) {
+    BgradQ[0] = Q[0];
+    BgradQ[1] = Q[3];
+    BgradQ[2] = 3.0;
+    BgradQ[3] = gradQ[0];
+    BgradQ[4] = 0.7;
+  }
 };
 
 // The kernel tests' linear elastic-wave PDE (exahype/tests/kernels/c/
@@ -273,9 +297,10 @@ int predictor(const double* luh, const double* dxa, double dt, double* lQhbnd, d
   double* stf[2] = {lFi, gradQ};
   std::fill_n(lFi, st * (DIMENSIONS + 1) * nV, 0.0);
   S s;
-  kernels::aderdg::generic::c::spaceTimePredictorNonlinear<false, true, false, false, S>(
+  constexpr bool SN = S::kSourceNCP;
+  kernels::aderdg::generic::c::spaceTimePredictorNonlinear<SN, true, SN, false, S>(
       s, lQhbnd, lFhbnd, stu, stf, lQhi, lFhi, luh, vec(dxa), dt);
-  if (lduh) kernels::aderdg::generic::c::volumeIntegralNonlinear<false, true, false, nV, b>(lduh, lFi, lFhi, vec(dxa));
+  if (lduh) kernels::aderdg::generic::c::volumeIntegralNonlinear<SN, true, false, nV, b>(lduh, lFi, lFhi, vec(dxa));
   if (lQi_out) std::copy_n(lQi, st * nD, lQi_out);
   if (lFi_out) std::copy_n(lFi, st * (DIMENSIONS + 1) * nV, lFi_out);
   if (lQhi_out) std::copy_n(lQhi, sp * nD, lQhi_out);
@@ -286,7 +311,7 @@ int predictor(const double* luh, const double* dxa, double dt, double* lQhbnd, d
 template <class S>
 void riemann(double* FL, double* FR, const double* QL, const double* QR, double dt, int dir) {
   S s;
-  kernels::aderdg::generic::c::riemannSolverNonlinear<false, S>(s, FL, FR, QL, QR, dt, dir);
+  kernels::aderdg::generic::c::riemannSolverNonlinear<S::kSourceNCP, S>(s, FL, FR, QL, QR, dt, dir);
 }
 
 // ADERDGSolver::applyBoundaryConditions (exahype/solvers/ADERDGSolver.cpp:2893-2962)
@@ -302,9 +327,9 @@ void boundary_face(double* FIn, const double* QIn, const double* centre, const d
   kernels::aderdg::generic::c::boundaryConditions<S>(s, FOut, QOut, FIn, QIn, vec(centre), vec(size), t, dt,
                                                       faceIndex, dir);
   if (faceIndex % 2 == 0)
-    kernels::aderdg::generic::c::riemannSolverNonlinear<false, S>(s, FOut, FIn, QOut, QIn, dt, dir);
+    kernels::aderdg::generic::c::riemannSolverNonlinear<S::kSourceNCP, S>(s, FOut, FIn, QOut, QIn, dt, dir);
   else
-    kernels::aderdg::generic::c::riemannSolverNonlinear<false, S>(s, FIn, FOut, QIn, QOut, dt, dir);
+    kernels::aderdg::generic::c::riemannSolverNonlinear<S::kSourceNCP, S>(s, FIn, FOut, QIn, QOut, dt, dir);
 }
 
 template <class S>
@@ -483,6 +508,12 @@ void plot_vertices(int N, int nvar, const double* u, double* out) {
         case 4: { typedef EulerDemo<4> S; call; } break;                    \
         case 5: { typedef EulerDemo<5> S; call; } break;                    \
         case 7: { typedef EulerDemo<7> S; call; } break;                    \
+        default: std::fprintf(stderr, "ref: order %d not built\n", N);     \
+      }                                                                     \
+    } else if (pde == 3) {                                                  \
+      switch (N) {                                                          \
+        case 3: { typedef EulerSourceNCP<3> S; call; } break;               \
+        case 5: { typedef EulerSourceNCP<5> S; call; } break;               \
         default: std::fprintf(stderr, "ref: order %d not built\n", N);     \
       }                                                                     \
     } else {                                                                \

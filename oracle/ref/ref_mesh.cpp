@@ -84,7 +84,7 @@ void* REFNAME(mesh_create)(int order, int pde, const int* cells, const double* s
   RefMesh* r = new RefMesh();
   r->c.pde = pde;
   r->c.N = order;
-  hrn_backend k = {&r->c, DIMENSIONS, order, 5, 5 + (pde == 1 ? 1 : 0), be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  hrn_backend k = {&r->c, DIMENSIONS, order, 5, 5 + (pde == 1 || pde == 3 ? 1 : 0), be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
   if (pde == 2) {
     k.nvar = 9;
     k.ndata = 12;

@@ -144,3 +144,23 @@ def test_nan_in_the_input_is_a_status(eb):
     assert np.isfinite(m.state()["dt"]) and m.state()["dt"] > 0
     assert m.run_until(1.0, max_steps=3) == 3
     assert m.validate() > n0
+
+
+def test_step_size_skips_non_finite_nodes_in_every_block(eb):
+    """stableTimeStepSize keeps dt = std::min(dt, CFL PNPM / den) from
+    DBL_MAX: a node whose denominator is NaN (negative pressure, a NaN
+    value) never replaces the minimum. With such a node in every block of
+    the launch, the mesh step size is still the minimum over all finite
+    nodes, equal to the oracle's"""
+    from exahype_b200 import problems
+    u, _ = problems.gaussian_pulse_2d(3, (8, 8), seed=1)
+    bad = u.copy()
+    for c in range(0, 64, 5):  # every 16-cell block gets several
+        bad[c, (3 * c) % 16, 4] = -1.0  # negative energy: negative pressure, NaN sound speed
+    s = eb.Solver(2, 3)
+    m = eb.Mesh(s, (8, 8), [0.0, 0.0], [1.0, 1.0], eb.BC_PERIODIC)
+    m.set_solution(bad)
+    m.init(0.0)
+    k = pyoracle.Kernels(2, 3, pde=0)
+    exp = min(k.stable_dt(bad[c], [0.125, 0.125]) for c in range(64))
+    assert np.isfinite(exp) and m.state()["dt"] == exp
