@@ -114,15 +114,24 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
   // bits), direction (2), variable (4), cell of the block (4); item k of
   // thread t is s_desc[k][t], -1: none
   __shared__ int s_desc[C::IPT][C::THREADS];
+  // the (direction, variable) pairs, copied with compile-time indices (a
+  // runtime index into the constexpr table would build a copy of it in every
+  // thread's local memory)
+  __shared__ int s_pair[C::NPAIRS];
+  if (threadIdx.x == 0) {
+    constexpr GradPairs<PDE, DIM> GP;
+#pragma unroll
+    for (int i = 0; i < C::NPAIRS; i++) s_pair[i] = GP.d[i] | GP.v[i] << 4;
+  }
+  __syncthreads();
   for (int k = 0; k < C::IPT; k++) {
     const int it = threadIdx.x + k * C::THREADS;
     int dsc = -1;
     if (it < C::GITEMS) {
-      constexpr GradPairs<PDE, DIM> GP;
       const int L = C::LMAJ ? it % LINES : (it / C::NPAIRS) % LINES;
       const int pr = C::LMAJ ? (it / LINES) % C::NPAIRS : it % C::NPAIRS;
       const int c = it / (C::NPAIRS * LINES);
-      const int d = GP.d[pr], v = GP.v[pr];
+      const int d = s_pair[pr] & 15, v = s_pair[pr] >> 4;
       dsc = line_node<DIM, b>(d, L, 0) | d << 10 | v << 12 | c << 16;
     }
     s_desc[k][threadIdx.x] = dsc;
@@ -191,9 +200,9 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
   if (active) {
     if (lQhi_out)
       for (int v = 0; v < nD; v++) lQhi_out[((size_t)cell * P + p) * nD + v] = sQ[p * QS + v];
-    if (lFhi_out)
+    if (lFhi_out)  // from the staged copy: indexing fh here would put it in local memory
       for (int d = 0; d < DIM; d++)
-        for (int v = 0; v < nV; v++) lFhi_out[(((size_t)cell * DIM + d) * P + p) * nV + v] = fh[d][v];
+        for (int v = 0; v < nV; v++) lFhi_out[(((size_t)cell * DIM + d) * P + p) * nV + v] = sG[p * GS + d * nV + v];
   }
   __syncthreads();
   // boundary extrapolation: states (parameters included) and normal fluxes
