@@ -845,41 +845,45 @@ def run_ensemble_workload(a, world, dev, rank, steps=50):
 def run_serving_workload(a, world, dev, rank):
     """Continuous-batching serving of a seeded Poisson stream of independent
     Euler solves (exahype_b200.serving) against the same requests served one
-    at a time on the plain FP64 path. Default mix (scaled so both arms take
-    seconds): 48 requests at 40/s, 70 % 2D with 27..243 cells per side, 30 %
-    3D with 9..27, N in {3,5,7}, 20 % limiter explosions, 10..100 steps,
-    64 GB device budget; --serving-full uses 3D sides 9..81, 10..200 steps and
-    a 120 GB budget."""
+    at a time on the plain FP64 path. Default mix (the full ranges): 32
+    requests at 10/s, 70 % 2D with 27..243 cells per side, 30 % 3D with
+    9..81, N in {3,5,7}, 20 % limiter explosions, 10..200 steps, 120 GB
+    device budget; --serving-small uses 3D sides 9..27, 10..100 steps, 48
+    requests at 40/s and a 64 GB budget. Initial data are built once, before
+    any timing; a warm-up pass serves the same stream with one step per
+    request (module loading, memory-pool growth to the mix's peak)."""
     from exahype_b200 import serving
     import exahype_b200 as eb
-    full = a.serving_full
-    kw = dict(sides_2d=(27, 243), sides_3d=(9, 81) if full else (9, 27), steps=(10, 200) if full else (10, 100))
-    n, rate, budget = (96, 10.0, 120e9) if full else (48, 40.0, 64e9)
+    small = a.serving_small
+    kw = dict(sides_2d=(27, 243), sides_3d=(9, 27) if small else (9, 81), steps=(10, 100) if small else (10, 200))
+    n, rate, budget = (48, 40.0, 64e9) if small else (32, 10.0, 120e9)
     variants = {}
     for dim in (2, 3):
         for o in (3, 5, 7):
             variants[(dim, o)] = eb.Solver(dim, o).autotune(4096)[0]
-    # one untimed pass of the same request stream first: the first use of
-    # each kernel in a process loads its module, and the device memory pool
-    # grows to the mix's peak once; the one-at-a-time arm below runs after it
-    # in the same process and is warm as well
-    warm = serving.request_stream(n, rate, seed=SEED + rank, **kw)
-    for r in warm:
-        r.build_initial()
-    serving.Server(budget, variants).run(warm, keep_results=False)
-    del warm
-    reqs = serving.request_stream(n, rate, seed=SEED + rank, **kw)
-    for r in reqs:
-        r.build_initial()
+    reqs0 = serving.request_stream(n, rate, seed=SEED + rank, **kw)
+    sizer = serving.Server(budget, variants)
+    for r in reqs0:
+        if sizer.bytes_for(r) <= budget:  # a request over the budget is rejected unbuilt
+            r.build_initial()
+
+    def clone(rs, steps=None):
+        out = []
+        for r in rs:
+            c = serving.Request(r.rid, r.arrival, r.dim, r.order, r.cells, r.kind, steps or r.steps, r.seed)
+            c.luh, c.fv = r.luh, r.fv
+            out.append(c)
+        return out
+
+    serving.Server(budget, variants).run(clone(reqs0, steps=1), keep_results=False)
+    reqs = clone(reqs0)
     srv = serving.Server(budget, variants)
     t0 = time.perf_counter()
     done, rejected = srv.run(reqs, keep_results=False)
     wall = time.perf_counter() - t0
     res = serving.summarise(done, wall)
     rej = {r.rid for r in rejected}
-    base = [r for r in serving.request_stream(n, rate, seed=SEED + rank, **kw) if r.rid not in rej]
-    for r in base:
-        r.build_initial()
+    base = clone([r for r in reqs0 if r.rid not in rej])
     t0 = time.perf_counter()
     serving.run_one_at_a_time(base, variants, keep_results=False)
     wall_b = time.perf_counter() - t0
@@ -888,14 +892,15 @@ def run_serving_workload(a, world, dev, rank):
     for r in reqs:
         k = "%dD_%s" % (r.dim, r.kind)
         kinds[k] = kinds.get(k, 0) + 1
-    return {"workload": "serving_poisson_%d_requests" % n, "full_size": bool(full), "rate_per_s": rate,
+    return {"workload": "serving_poisson_%d_requests" % n, "full_size": not small, "rate_per_s": rate,
             "budget_bytes": budget, "rejected_over_budget": len(rejected), "mix": kinds,
+            "sides_3d": list(kw["sides_3d"]), "steps_range": list(kw["steps"]),
             "p50_time_to_solution_s": res["p50_s"], "p99_time_to_solution_s": res["p99_s"],
             "value": res["value"], "unit": "DoF-updates/s", "wall_s": wall,
             "one_at_a_time": {"p50_time_to_solution_s": res_b["p50_s"], "p99_time_to_solution_s": res_b["p99_s"],
                               "value": res_b["value"], "wall_s": wall_b},
-            "timing": "host wall clock from the first arrival to the last result on the host, after one "
-                      "untimed pass of the same stream (module loading, memory-pool growth)"}
+            "timing": "host wall clock from the first arrival to the last result on the host, after a warm-up "
+                      "pass of the same stream with one step per request (module loading, memory-pool growth)"}
 
 
 def run_mixed_arm(a, u0, fp64_variant, dev):
@@ -969,6 +974,100 @@ def run_fused_arm(a, u0, variant, dev):
                       "estimate was too large)"}
 
 
+def run_mixed_table(a, world, dev, rank):
+    """The mixed-precision predictor (FP64 first sweep, FP32 increment sweeps;
+    variants 4 and 5) against the FP64 path on each workload the mixed form
+    is named for: per workload the FP64 (autotuned shape) and both mixed
+    register budgets, CUDA events on the mesh stream, Picard sweeps per cell
+    and step, and the mixed solution's relative L2 distance from the FP64
+    one at the end. Workloads: the 27^3 N=5 3D pulses (20 steps), a 2D N=7
+    81^2 pulse mesh (20 steps), the 81^2 N=5 explosion with the limiter
+    (100 steps), and the 256-instance ragged 2D ensemble (20 steps). (3D N=7
+    has no mixed form: its line-form working set does not fit in shared
+    memory; the library rejects the variant there.)"""
+    import torch
+    import exahype_b200 as eb
+    from exahype_b200 import problems
+
+    def timed(m, k, stream_handle):
+        st = torch.cuda.ExternalStream(stream_handle, device=dev)
+        m.step(2)
+        m.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        m.step(k)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    rows = []
+    for name, dim, order, cells, steps, limiter in (
+            ("euler3d_N5_27^3_pulses", 3, 5, (27, 27, 27), 20, False),
+            ("euler2d_N7_81^2_pulse", 2, 7, (81, 81), 20, False),
+            ("euler2d_N5_81^2_explosion_limiter", 2, 5, (81, 81), 100, True)):
+        if limiter:
+            u0, fv, _ = problems.explosion(dim, order, cells, seed=SEED)
+        elif dim == 3:
+            u0, _ = problems.gaussian_pulses_3d(order, cells, seed=SEED)
+        else:
+            u0, _ = problems.gaussian_pulse_2d(order, cells, seed=SEED)
+        ncells = int(np.prod(cells))
+        res, sols = {}, {}
+        fp64_variant = eb.Solver(dim, order).autotune(min(4096, ncells))[0]
+        for label, variant in (("fp64", fp64_variant), ("mixed", eb.PREDICTOR_MIXED),
+                               ("mixed_2", eb.PREDICTOR_MIXED_2)):
+            s = eb.Solver(dim, order)
+            s.variant = variant
+            if limiter:
+                m = eb.LimitingMesh(s, cells, [0.0] * dim, [1.0] * dim, eb.BC_OUTFLOW, helper_layers=1, cure_steps=0)
+                m.set_solution(u0)
+                m.set_fv_initial(fv)
+            else:
+                m = eb.Mesh(s, cells, [0.0] * dim, [1.0] * dim, eb.BC_PERIODIC)
+                m.set_solution(u0)
+            m.init(0.0)
+            sw0 = m.state()["picard_sweeps"]
+            ms = timed(m, steps, m.stream_handle)
+            st = m.state()
+            sols[label] = m.get_solution()
+            res[label] = {"variant": variant, "ms_per_step": ms,
+                          "sweeps_per_cell_step": (st["picard_sweeps"] - sw0) / ((steps + 2) * ncells)}
+            del m
+        for label in ("mixed", "mixed_2"):
+            res[label]["rel_l2_vs_fp64"] = float(np.linalg.norm(sols[label] - sols["fp64"]) /
+                                                 np.linalg.norm(sols["fp64"]))
+            res[label]["speed_vs_fp64"] = res["fp64"]["ms_per_step"] / res[label]["ms_per_step"]
+        rows.append(dict(workload=name, steps=steps, **res))
+    # the ragged ensemble: every (dim, order) group with the mixed variant
+    ens = problems.pulse_ensemble(256, seed=SEED + rank)
+    out_e, sols = {}, {}
+    for label in ("fp64", "mixed"):
+        bt = eb.Batch()
+        for p in ens:
+            bt.add(2, p["order"], p["cells"], [1.0, 1.0], eb.BC_PERIODIC, p["luh"])
+        bt.commit()
+        if label == "mixed":
+            for o in (3, 5, 7):
+                bt.set_variant(2, o, eb.PREDICTOR_MIXED)
+        bt.step(2)
+        bt.synchronize()
+        st = torch.cuda.ExternalStream(bt.stream_handle, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        bt.step(20)
+        e1.record(st)
+        e1.synchronize()
+        out_e[label] = {"ms_per_step": e0.elapsed_time(e1) / 20, "sweeps": bt.sweeps()}
+        sols[label] = [bt.get_solution(i) for i in range(len(ens))]
+        del bt
+    err = max(float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_)) for a_, b_ in zip(sols["mixed"], sols["fp64"]))
+    out_e["mixed"]["max_instance_rel_l2_vs_fp64"] = err
+    out_e["mixed"]["speed_vs_fp64"] = out_e["fp64"]["ms_per_step"] / out_e["mixed"]["ms_per_step"]
+    rows.append(dict(workload="euler2d_pulse_ensemble_256", steps=20, **out_e))
+    return {"workload": "mixed_vs_fp64_table", "rows": rows,
+            "timing": "CUDA events on the mesh / batch stream after 2 untimed steps"}
+
+
 def measure_fp64_peak():
     """FP64 peaks measured in this run (TFLOP/s): the DFMA probe and the DMMA
     (mma.sync m8n8k4 f64) probe; the roofline uses the larger."""
@@ -999,17 +1098,18 @@ def main():
     ap.add_argument("--limiter-steps", type=int, default=0, help="limiter workload: K steps instead of t = 0.2")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
-    ap.add_argument("--serving-full", action="store_true", help="serving: the full-size request mix")
+    ap.add_argument("--serving-small", action="store_true",
+                    help="serving: the reduced request mix (3D sides 9..27, 10..100 steps)")
     ap.add_argument("--no-elastic", action="store_true", help="skip the linear-kernel (elastic waves) workload")
     ap.add_argument("--no-amr", action="store_true", help="skip the AMR transfer / plotting workload")
     ap.add_argument("--no-refined", action="store_true", help="skip the statically refined mesh workload")
     ap.add_argument("--workload", default="headline",
-                    choices=["headline", "limiter", "ensemble", "serving", "elastic", "amr", "refined"],
+                    choices=["headline", "limiter", "ensemble", "serving", "elastic", "amr", "refined", "mixed-table"],
                     help="limiter / ensemble / serving / elastic / amr / refined: only that workload, as its own JSON line")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
-    if a.workload in ("limiter", "ensemble", "serving", "elastic", "amr", "refined"):
+    if a.workload in ("limiter", "ensemble", "serving", "elastic", "amr", "refined", "mixed-table"):
         return run_secondary_only(a)
     return run_ours(a)
 
@@ -1023,7 +1123,7 @@ def run_secondary_only(a):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     run = {"limiter": run_limiter_workload, "ensemble": run_ensemble_workload,
            "serving": run_serving_workload, "elastic": run_elastic_workload, "amr": run_amr_workload,
-           "refined": run_refined_workload}[a.workload]
+           "refined": run_refined_workload, "mixed-table": run_mixed_table}[a.workload]
     if a.workload == "elastic":
         pk = None if a.no_fp64_probe else measure_fp64_peak()
         r = run(a, world, torch.device("cuda", local), rank, max(pk.values()) if pk else None)

@@ -105,10 +105,22 @@ def gaussian_pulses_3d(order, cells=(27, 27, 27), seed=0, npulses=4):
     widths = rng.uniform(0.05, 0.15, size=npulses)
     centres = rng.uniform(0.0, 1.0, size=(npulses, 3))
     vel0 = rng.uniform(-0.5, 0.5, size=3)
-    X = node_coordinates(3, order, cells)
-    rho = np.ones(X.shape[:-1])
+    # the Gaussian of the minimum-image distance factors by axis: per pulse
+    # three 1-D factors over (cell, node) of each axis, one outer product
+    x = gl_nodes(order)
+    nx, ny, nz = cells
+    rho = np.ones((nz, ny, nx) + (order + 1,) * 3)
     for a, w, c in zip(amps, widths, centres):
-        rho += a * np.exp(-_periodic_d2(X, c) / (w * w))
+        f = []
+        for d, n in enumerate((nx, ny, nz)):
+            X = (np.arange(n)[:, None] + x[None, :]) * (1.0 / n)
+            dd = X - c[d]
+            dd -= np.round(dd)
+            f.append(np.exp(-dd * dd / (w * w)))
+        fx, fy, fz = f
+        rho += a * (fz[:, None, None, :, None, None] * fy[None, :, None, None, :, None]) * \
+            fx[None, None, :, None, None, :]
+    rho = rho.reshape(nx * ny * nz, -1)
     vel = np.broadcast_to(vel0, rho.shape + (3,))
     return conserved(rho, vel, np.ones_like(rho)), dict(amps=amps.tolist(), widths=widths.tolist(),
                                                         centres=centres.tolist(), velocity=vel0.tolist())
@@ -155,14 +167,23 @@ def explosion(dim, order, cells, seed=0, radius=0.2):
     rng = np.random.default_rng(seed)
     c = rng.uniform(0.4, 0.6, size=dim)
 
-    def state(X):
-        inside = np.sum((X - c) ** 2, axis=-1) < radius * radius
-        rho = np.where(inside, 1.0, 0.125)
-        p = np.where(inside, 1.0, 0.1)
-        return conserved(rho, np.zeros(rho.shape + (3,)), p)
+    def state(pts):
+        # |x - c|^2 summed over the axes in order, from per-axis squares over
+        # (cell, point) of each axis (the coordinates are (cell + point) dx)
+        sq = [((np.arange(cells[d])[:, None] + pts[None, :]) * (1.0 / cells[d]) - c[d]) ** 2 for d in range(dim)]
+        if dim == 2:
+            r2 = sq[0][None, :, None, :] + sq[1][:, None, :, None]  # (cy, cx, py, px)
+        else:
+            r2 = (sq[0][None, None, :, None, None, :] + sq[1][None, :, None, None, :, None]) + \
+                sq[2][:, None, None, :, None, None]  # (cz, cy, cx, pz, py, px)
+        inside = (r2 < radius * radius).reshape(int(np.prod(cells[:dim])), -1)
+        Q = np.zeros(inside.shape + (5,))
+        Q[..., 0] = np.where(inside, 1.0, 0.125)
+        Q[..., 4] = np.where(inside, 1.0, 0.1) / (GAMMA - 1)
+        return Q
 
-    return (state(node_coordinates(dim, order, cells)), state(subcell_coordinates(dim, order, cells)),
-            dict(centre=c.tolist()))
+    B = 2 * order + 1
+    return state(gl_nodes(order)), state((np.arange(B) + 0.5) / B), dict(centre=c.tolist())
 
 
 def elastic_pulse(dim, order, cells, seed=0):
