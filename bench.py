@@ -321,6 +321,8 @@ def run_ours(a):
 
     u0, _ = problems.gaussian_pulses_3d(ORDER, CELLS, seed=SEED + rank)
     s = eb.Solver(DIM, ORDER, eb.PDE_EULER)
+    if a.variant is not None:
+        s.variant = a.variant  # also for the initial predictor
     m = eb.Mesh(s, CELLS, [0.0] * DIM, [1.0] * DIM, eb.BC_PERIODIC)
     m.set_solution(u0)
     m.init(0.0)

@@ -479,14 +479,27 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     lQhbnd[(((size_t)cell_c * 2 * DIM + 2 * d + 1) * LINES + L) * nD + v] = sr;
   }
   __syncthreads();
-  if (!active || !lduh) return;
-  double* dst = lduh + ((size_t)cell * P + p) * nV;
+  if (!lduh) return;
+  // the volume integral at this node, staged in the cell's lQi buffer (free
+  // now) and written by consecutive threads to consecutive addresses: a
+  // node's own nV doubles per thread would make every store instruction a
+  // partial write of 32 sectors
+  if (active) {
 #pragma unroll
-  for (int v = 0; v < nV; v++) {
-    double du = 0.0;
+    for (int v = 0; v < nV; v++) {
+      double du = 0.0;
 #pragma unroll
-    for (int d = 0; d < DIM; d++) du += sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
-    dst[v] = du;
+      for (int d = 0; d < DIM; d++) du += sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+      sQ[p * nV + v] = du;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < C::CPB * P * nV; i += C::THREADS) {
+    const int c = i / (P * nV), e = i - c * (P * nV);
+    if (s_done[c]) continue;
+    const int slot_c = blockIdx.x * C::CPB + c;
+    const int cell_c = cell_list ? cell_list[slot_c] : slot_c;
+    lduh[(size_t)cell_c * P * nV + e] = smem[c * C::SQ + e];
   }
 }
 
