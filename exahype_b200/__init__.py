@@ -283,7 +283,7 @@ class Mesh:
         """Periodic mesh with nested refined boxes (exa_mesh_create_nested):
         boxes[k] = (lo, hi) in the cell coordinates of level k (level 0 the
         coarse grid; level k+1 box k refined once, coordinates over the whole
-        domain at that level). bc: periodic or outflow, per domain face or
+        domain at that level). bc: periodic, outflow or reflective, per domain face or
         one for all. Solution order: the unrefined cells of each level in
         turn, x fastest."""
         return cls.boxes(solver, cells, offset, size, [(k, lo, hi) for k, (lo, hi) in enumerate(boxes)], bc)

@@ -335,7 +335,7 @@ struct Launch {
 // with the linear volume integral, the linear Riemann solver, and the
 // corrector with the linear surface integral. The predictor has one shape, so
 // the variant is ignored; there are no Picard sweeps to count. Boundary
-// conditions are not provided for linear PDEs (periodic meshes only).
+// faces: the PDE's boundaryValues and the linear Riemann solve against them.
 template <int DIM, int N, class PDE>
 struct LinearLaunch {
   using CC = CorrectorCfg<DIM, N, PDE>;
@@ -375,9 +375,12 @@ struct LinearLaunch {
     EXA_LAUNCHED();
     return EXA_OK;
   }
-  static int boundary(const double*, double*, const int*, const int*, int n, int, const int*, cudaStream_t) {
+  static int boundary(const double* qb, double* fb, const int* c, const int* f, int n, int kind, const int* gate,
+                      cudaStream_t st) {
     if (n <= 0) return EXA_OK;
-    return fail(EXA_ERR_UNSUPPORTED, "boundary conditions: the linear kernels support periodic meshes only");
+    boundary_linear_kernel<DIM, N, PDE><<<(n + 3) / 4, 128, 0, st>>>(qb, fb, c, f, n, kind, gate);
+    EXA_LAUNCHED();
+    return EXA_OK;
   }
   static int corrector(double* luh, const double* du, const double* fb, const double* dt, double* dtout, Geometry g,
                        int n, const int* list, int upd, const int* cnt, cudaStream_t st) {
@@ -927,8 +930,6 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
     nc *= cells[d];
     const bool pl = bc[2 * d] == EXA_BC_PERIODIC, pr = bc[2 * d + 1] == EXA_BC_PERIODIC;
     if (pl != pr) return fail(EXA_ERR_ARG, "exa_mesh_create: periodic must be set on both faces of an axis");
-    if (s->k.linear && !pl)
-      return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create: the linear kernels support periodic meshes only");
     for (int f = 0; f < 2; f++) {
       const int k = bc[2 * d + f];
       if (k != EXA_BC_PERIODIC && k != EXA_BC_OUTFLOW && k != EXA_BC_REFLECTIVE)
@@ -1224,8 +1225,6 @@ int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* o
       return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: unknown boundary kind");
     if (f % 2 == 1 && (k == EXA_BC_PERIODIC) != (m->bc[f - 1] == EXA_BC_PERIODIC))
       return fail(EXA_ERR_ARG, "exa_mesh_create_boxes: periodic must be set on both faces of an axis");
-    if (k != EXA_BC_PERIODIC && s->k.linear)
-      return fail(EXA_ERR_UNSUPPORTED, "exa_mesh_create_boxes: the linear kernels support periodic meshes only");
     m->bc[f] = k;
   }
   NestedTopo t;

@@ -269,12 +269,59 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
   }
 }
 
-// riemannSolverLinear, one warp per interior face: face averages of both
-// sides (parameters included), smax from the eigenvalues of both averages,
-// the system matrix Bn once in their mean, then per face node
-// FL = (Bn - smax I)^T dQ and FR = (Bn + smax I)^T dQ with dQ = (QR - QL) / 2.
-// FL goes to the left cell's face 2 dir + 1, FR to the right cell's face
-// 2 dir; the extrapolated fluxes there are not read.
+// The linear Riemann solve of one face by one warp: face averages of both
+// sides (parameters included), smax from both averages' eigenvalues, Bn from
+// the PDE's coefficient_matrix in their mean (shared memory, sBw), then per
+// face node FL = (Bn - smax I)^T dQ and FR = (Bn + smax I)^T dQ with
+// dQ = (QR - QL) / 2 (staged in sDQw). FL or FR may be NULL (not written).
+template <int DIM, int N, class PDE>
+__device__ __forceinline__ void linear_face_flux(const double* QL, const double* QR, double* FL, double* FR, int dir,
+                                                 int lane, double* sBw, double* sDQw) {
+  using S = Shape<DIM, N, PDE>;
+  constexpr int F = S::F, nV = S::nV, nD = S::nD;
+  // this lane's state differences are loaded before the face averages, so
+  // that all of the face's loads are in flight together
+  constexpr int E = F * nV, EPL = (E + 31) / 32;
+  double dq[EPL];
+#pragma unroll
+  for (int i = 0; i < EPL; i++) {
+    const int e = lane + 32 * i, fn = e / nV, k = e - fn * nV;
+    dq[i] = e < E ? 0.5 * (QR[fn * nD + k] - QL[fn * nD + k]) : 0.0;
+  }
+  double aL[nD], aR[nD];
+  face_average<DIM, N, PDE>(QL, lane, aL);
+  face_average<DIM, N, PDE>(QR, lane, aR);
+  const double smax = face_smax<DIM, PDE>(aL, aR, dir);
+  if (lane == 0) {
+    double av[nD];
+#pragma unroll
+    for (int k = 0; k < nD; k++) av[k] = 0.5 * (aL[k] + aR[k]);
+    PDE::coefficient_matrix(av, dir, sBw);
+  }
+#pragma unroll
+  for (int i = 0; i < EPL; i++) {
+    const int e = lane + 32 * i;
+    if (e < E) sDQw[e] = dq[i];
+  }
+  __syncwarp();
+  for (int e = lane; e < F * nV; e += 32) {
+    const int fn = e / nV, j = e - fn * nV;
+    const double* d = sDQw + fn * nV;
+    double fl = 0.0, fr = 0.0;
+#pragma unroll
+    for (int k = 0; k < nV; k++) {
+      const double bkj = sBw[k * nV + j];
+      fl = fma(k == j ? bkj - smax : bkj, d[k], fl);
+      fr = fma(k == j ? bkj + smax : bkj, d[k], fr);
+    }
+    if (FL) FL[e] = fl;
+    if (FR) FR[e] = fr;
+  }
+}
+
+// riemannSolverLinear on interior faces, one warp per face. FL goes to the
+// left cell's face 2 dir + 1, FR to the right cell's face 2 dir; the
+// extrapolated fluxes there are not read.
 template <int DIM, int N, class PDE>
 __global__ void __launch_bounds__(128) riemann_linear_kernel(const double* __restrict__ lQhbnd,
                                                              double* __restrict__ lFhbnd,
@@ -295,44 +342,41 @@ __global__ void __launch_bounds__(128) riemann_linear_kernel(const double* __res
   const double* QR = lQhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nD;
   double* FL = lFhbnd + ((size_t)cl * 2 * DIM + 2 * dir + 1) * F * nV;
   double* FR = lFhbnd + ((size_t)cr * 2 * DIM + 2 * dir) * F * nV;
-  // this lane's state differences are loaded before the face averages, so
-  // that all of the face's loads are in flight together
-  constexpr int E = F * nV, EPL = (E + 31) / 32;
-  double dq[EPL];
-#pragma unroll
-  for (int i = 0; i < EPL; i++) {
-    const int e = lane + 32 * i, fn = e / nV, k = e - fn * nV;
-    dq[i] = e < E ? 0.5 * (QR[fn * nD + k] - QL[fn * nD + k]) : 0.0;
-  }
-  double aL[nD], aR[nD];
-  face_average<DIM, N, PDE>(QL, lane, aL);
-  face_average<DIM, N, PDE>(QR, lane, aR);
-  const double smax = face_smax<DIM, PDE>(aL, aR, dir);
-  if (lane == 0) {
-    double av[nD];
-#pragma unroll
-    for (int k = 0; k < nD; k++) av[k] = 0.5 * (aL[k] + aR[k]);
-    PDE::coefficient_matrix(av, dir, sB[w]);
-  }
-#pragma unroll
-  for (int i = 0; i < EPL; i++) {
-    const int e = lane + 32 * i;
-    if (e < E) sDQ[w][e] = dq[i];
+  linear_face_flux<DIM, N, PDE>(QL, QR, FL, FR, dir, lane, sB[w], sDQ[w]);
+}
+
+// Boundary faces of a linear solver: ADERDGSolver::applyBoundaryConditions
+// (exahype/solvers/ADERDGSolver.cpp:2893-2962) -- the PDE's boundaryValues
+// at every face node (boundaryConditions, 3d/boundaryConditions.cpph:24-85),
+// staged in shared memory, then riemannSolverLinear with the outside state on
+// the outer side (QOut, QIn for an even face, QIn, QOut for an odd one); only
+// the cell's own fluctuation is written. One warp per boundary face.
+template <int DIM, int N, class PDE>
+__global__ void __launch_bounds__(128) boundary_linear_kernel(const double* __restrict__ lQhbnd,
+                                                              double* __restrict__ lFhbnd,
+                                                              const int* __restrict__ bcell,
+                                                              const int* __restrict__ bface, int nb, int kind,
+                                                              const int* __restrict__ gate = nullptr) {
+  using S = Shape<DIM, N, PDE>;
+  constexpr int F = S::F, nV = S::nV, nD = S::nD;
+  __shared__ double sB[4][nV * nV];
+  __shared__ double sDQ[4][F * nV];
+  __shared__ double sQO[4][F * nD];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int f = blockIdx.x * (blockDim.x >> 5) + w;
+  if (f >= nb || (gate && !*gate)) return;
+  const int c = bcell[f], face = bface[f], dir = face >> 1;
+  const double* QIn = lQhbnd + ((size_t)c * 2 * DIM + face) * F * nD;
+  double* FIn = lFhbnd + ((size_t)c * 2 * DIM + face) * F * nV;
+  for (int fn = lane; fn < F; fn += 32) {
+    double fo[nV];
+    PDE::template boundaryValues<DIM>(kind, dir, FIn + fn * nV, QIn + fn * nD, fo, sQO[w] + fn * nD);
   }
   __syncwarp();
-  for (int e = lane; e < F * nV; e += 32) {
-    const int fn = e / nV, j = e - fn * nV;
-    const double* dq = sDQ[w] + fn * nV;
-    double fl = 0.0, fr = 0.0;
-#pragma unroll
-    for (int k = 0; k < nV; k++) {
-      const double bkj = sB[w][k * nV + j];
-      fl = fma(k == j ? bkj - smax : bkj, dq[k], fl);
-      fr = fma(k == j ? bkj + smax : bkj, dq[k], fr);
-    }
-    FL[e] = fl;
-    FR[e] = fr;
-  }
+  if ((face & 1) == 0)
+    linear_face_flux<DIM, N, PDE>(sQO[w], QIn, nullptr, FIn, dir, lane, sB[w], sDQ[w]);
+  else
+    linear_face_flux<DIM, N, PDE>(QIn, sQO[w], FIn, nullptr, dir, lane, sB[w], sDQ[w]);
 }
 
 // volumeIntegralLinear alone: lduh = -w_node sum_d lFhi[d], lFhi per cell [d][b^d][nV]

@@ -243,6 +243,19 @@ struct ElasticPDE {
   static constexpr bool kLinear = true;
   static constexpr bool kSource = false, kNCP = false;  // (its product enters the linear kernels directly)
 
+  // boundaryValues (this library's; the reference's kernel tests define
+  // none for this PDE): kOutflow copies the inside state, kReflective is a
+  // rigid wall, the inside state with the three velocities negated; the
+  // material parameters are copied
+  template <int DIM>
+  __device__ static void boundaryValues(int kind, int /*normal*/, const double* FIn, const double* QIn, double* FOut,
+                                        double* QOut) {
+    for (int v = 0; v < nVar + nPar; v++) QOut[v] = QIn[v];
+    if (kind == kReflective)
+      for (int v = 6; v < 9; v++) QOut[v] = -QOut[v];
+    for (int v = 0; v < nVar; v++) FOut[v] = FIn[v];
+  }
+
   // the product of one direction: B_d = B_d(Q) gradQ_d (a linear PDE's
   // product separates by direction)
   __device__ static void ncp_dir(const double* Q, int d, const double* G, double* B) {

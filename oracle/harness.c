@@ -53,6 +53,9 @@ typedef struct {
   void (*surface_integral)(void* ctx, double* lduh, const double* lFhbnd, const double* dx);
   void (*solution_update)(void* ctx, double* luh, const double* lduh, double dt);
   double (*stable_dt)(void* ctx, const double* luh, const double* dx);
+  /* optional: a boundary face that needs the boundary kind of its domain
+   * face (0 outflow, 1 reflective); used instead of boundary_face when set */
+  void (*boundary_face_kind)(void* ctx, double* FIn, const double* QIn, int faceIndex, int kind);
 } hrn_backend;
 
 typedef struct {
@@ -159,7 +162,11 @@ static void hrn_run_range(hrn_job* j) {
                  m->lQhbnd + ((size_t)cl * D2 + 2 * d + 1) * F * nD, m->lQhbnd + ((size_t)cr * D2 + 2 * d) * F * nD, d);
     } else if (j->phase == 2) { /* boundary face */
       const int c = m->bcell[i], f = m->bface[i];
-      k->boundary_face(k->ctx, m->lFhbnd + ((size_t)c * D2 + f) * F * nV, m->lQhbnd + ((size_t)c * D2 + f) * F * nD, f);
+      if (k->boundary_face_kind)
+        k->boundary_face_kind(k->ctx, m->lFhbnd + ((size_t)c * D2 + f) * F * nV,
+                              m->lQhbnd + ((size_t)c * D2 + f) * F * nD, f, m->bc[f]);
+      else
+        k->boundary_face(k->ctx, m->lFhbnd + ((size_t)c * D2 + f) * F * nV, m->lQhbnd + ((size_t)c * D2 + f) * F * nD, f);
     } else if (j->phase == 3) { /* corrector + admissible step */
       double* u = m->luh + (size_t)i * P * nD;
       double* du = m->lduh + (size_t)i * P * nV;

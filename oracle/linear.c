@@ -16,6 +16,9 @@
  *                             3d/surfaceIntegralLinear.cpph:24-91
  *   riemannSolverLinear       2d/riemannSolverLinear.cpph:23-126,
  *                             3d/riemannSolverLinear.cpph:20-136
+ *   boundaryConditions        2d/boundaryConditions.cpph:24-72,
+ *                             3d/boundaryConditions.cpph:24-85, then
+ *                             riemannSolverLinear (boundary faces)
  *
  * Dimension-generic form as in oracle.c: a 2D cell is a 3D cell with one
  * z-layer of unit weight. Every 2D product of the reference either has no
@@ -344,4 +347,29 @@ void orc_lin_riemann(const orc_solver* s, double* FL, double* FR, const double* 
       FR[fn * nV + j] = fr;
     }
   }
+}
+
+/* Boundary faces of a linear solver: ADERDGSolver::applyBoundaryConditions
+ * (exahype/solvers/ADERDGSolver.cpp:2893-2962) with the generic
+ * boundaryConditions kernel (3d/boundaryConditions.cpph:24-85) -- the user's
+ * boundaryValues at every face node -- followed by riemannSolverLinear with
+ * the outside state on the outer side (FOut, FIn, QOut, QIn for an even
+ * face, FIn, FOut, QIn, QOut for an odd one); only the cell's own
+ * fluctuation is kept. boundaryValues of the elastic-wave PDE (this
+ * repository's, the reference's kernel tests define none): kind 0 copies
+ * the inside state (outflow), kind 1 a rigid wall, the inside state with
+ * the three velocities negated; parameters are copied. */
+void orc_lin_boundary_face(const orc_solver* s, double* FIn, const double* QIn, int faceIndex, int kind) {
+  const lgeo g = lmk(s);
+  const int dir = (faceIndex - faceIndex % 2) / 2;
+  double QOut[100 * 12], FOut[100 * 9];
+  memcpy(QOut, QIn, sizeof(double) * g.F * g.nD);
+  memcpy(FOut, FIn, sizeof(double) * g.F * g.nV);
+  if (kind == 1 && s->pde == 2)
+    for (int fn = 0; fn < g.F; fn++)
+      for (int v = 6; v < 9; v++) QOut[fn * g.nD + v] = -QOut[fn * g.nD + v];
+  if (faceIndex % 2 == 0)
+    orc_lin_riemann(s, FOut, FIn, QOut, QIn, dir);
+  else
+    orc_lin_riemann(s, FIn, FOut, QIn, QOut, dir);
 }

@@ -62,6 +62,9 @@ void orc_lin_predictor(const orc_solver* s, const double* luh, const double* dx,
 void orc_lin_volume_integral(const orc_solver* s, double* lduh, const double* lFhi, const double* dx);
 void orc_lin_surface_integral(const orc_solver* s, double* lduh, const double* lFhbnd, const double* dx);
 void orc_lin_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, const double* QR, int dir);
+/* boundary face of a linear solver: boundaryValues (kind 0 outflow, 1 rigid
+ * wall) + riemannSolverLinear, the cell's own fluctuation into FIn */
+void orc_lin_boundary_face(const orc_solver* s, double* FIn, const double* QIn, int faceIndex, int kind);
 
 /* AMR transfer operators (amr.c) between a cell / face and its descendant
  * levelDelta levels finer; subcell / subface indices per axis in

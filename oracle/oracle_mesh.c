@@ -18,8 +18,8 @@ static void be_surf(void* c, double* du, const double* fb, const double* dx) { o
 static void be_upd(void* c, double* u, const double* du, double dt) { orc_solution_update((const orc_solver*)c, u, du, dt); }
 static double be_dt(void* c, const double* u, const double* dx) { return orc_stable_dt((const orc_solver*)c, u, dx); }
 
-/* linear PDEs (pde 2): Cauchy-Kovalevski predictor, linear Riemann solver and
- * surface integral; periodic meshes only (no boundary kernels) */
+/* linear PDEs (pde 2): Cauchy-Kovalevski predictor, linear Riemann solver,
+ * surface integral and boundary faces (outflow, rigid wall) */
 static int be_lpred(void* c, const double* luh, const double* dx, double dt, double* qb, double* fb, double* du) {
   orc_lin_predictor((const orc_solver*)c, luh, dx, dt, qb, fb, du, 0, 0);
   return 0;
@@ -29,6 +29,9 @@ static void be_lriem(void* c, double* FL, double* FR, const double* QL, const do
 }
 static void be_lsurf(void* c, double* du, const double* fb, const double* dx) {
   orc_lin_surface_integral((const orc_solver*)c, du, fb, dx);
+}
+static void be_lbnd(void* c, double* FIn, const double* QIn, int f, int kind) {
+  orc_lin_boundary_face((const orc_solver*)c, FIn, QIn, f, kind);
 }
 
 typedef struct {
@@ -47,6 +50,7 @@ void* orc_mesh_create(int dim, int order, int pde, const int* cells, const doubl
     k.predictor = be_lpred;
     k.riemann = be_lriem;
     k.surface_integral = be_lsurf;
+    k.boundary_face_kind = be_lbnd;
   }
   om->m = hrn_create(&k, cells, size, bc, nthreads);
   return om;

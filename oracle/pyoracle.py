@@ -205,6 +205,14 @@ class Kernels:
             self._call("lin_riemann", _p(FL), _p(FR), _p(QL), _p(QR), ctypes.c_double(0.0), ctypes.c_int(direction))
         return FL, FR
 
+    def lin_boundary_face(self, FIn, QIn, face_index, kind=0):
+        """boundary face of a linear solver (kind 0 outflow, 1 rigid wall):
+        the cell's own fluctuation, returned as a new array"""
+        FIn = np.array(FIn, dtype=np.float64).reshape(-1)
+        QIn = np.ascontiguousarray(QIn, dtype=np.float64).reshape(-1)
+        self._call("lin_boundary_face", _p(FIn), _p(QIn), ctypes.c_int(face_index), ctypes.c_int(kind))
+        return FIn
+
     def lin_surface_integral(self, lduh, lFhbnd, dx):
         lduh = np.array(lduh, dtype=np.float64).reshape(-1)
         dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
@@ -578,8 +586,9 @@ class RefinedMesh:
                 fl, fr = K.riemann(self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i], self.Q[l, 2 * i + 1],
                                    self.Q[r, 2 * i], i)
             self.Fb[l, 2 * i + 1], self.Fb[r, 2 * i] = fl, fr
+        bf = K.lin_boundary_face if self.linear else K.boundary_face
         for c, face, kind in self.bnd:
-            self.Fb[c, face] = K.boundary_face(self.Fb[c, face], self.Q[c, face], face, kind=kind)
+            self.Fb[c, face] = bf(self.Fb[c, face], self.Q[c, face], face, kind=kind)
         for c in range(self.ncells):
             si = K.lin_surface_integral if self.linear else K.surface_integral
             du = si(self.du[c], self.Fb[c].reshape(-1), self._dx(c))

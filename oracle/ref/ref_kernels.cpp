@@ -197,6 +197,17 @@ struct Elastic {
     for (int d = 0; d < DIMENSIONS; d++) std::fill_n(F[d], 9, 0.0);
   }
   void algebraicSource(const double* const, double* S) { std::fill_n(S, 9, 0.0); }
+  // boundaryValues (this repository's; the kernel tests define none): kind 0
+  // copies the inside state (outflow), kind 1 a rigid wall (the three
+  // velocities negated); set per call through boundary_kind
+  static thread_local int boundary_kind;
+  void boundaryValues(const double* const, const double, const double, const int, const int,
+                      const double* const fluxIn, const double* const stateIn, double* fluxOut, double* stateOut) {
+    std::copy_n(stateIn, 12, stateOut);
+    std::copy_n(fluxIn, 9, fluxOut);
+    if (boundary_kind == 1)
+      for (int v = 6; v < 9; v++) stateOut[v] = -stateOut[v];
+  }
   void eigenvalues(const double* const Q, const int, double* lambda) {
     std::fill_n(lambda, 9, 0.0);
     const double lam = Q[9], mu = Q[10], rho0 = Q[11];
@@ -272,6 +283,9 @@ struct Elastic {
 #undef B
   }
 };
+
+template <int N_>
+thread_local int Elastic<N_>::boundary_kind = 0;
 
 template <int D> using Vec = tarch::la::Vector<D, double>;
 
@@ -375,6 +389,24 @@ template <class S>
 void lin_riemann(double* FL, double* FR, const double* QL, const double* QR, double dt, int dir) {
   S s;
   kernels::aderdg::generic::c::riemannSolverLinear<true, S>(s, FL, FR, QL, QR, dt, dir);
+}
+// ADERDGSolver::applyBoundaryConditions (exahype/solvers/ADERDGSolver.cpp:2893-2962)
+// for a linear solver: boundaryConditions, then riemannSolverLinear
+template <class S>
+void lin_boundary_face(double* FIn, const double* QIn, int faceIndex, int kind) {
+  constexpr int b = S::Order + 1;
+  constexpr int nV = S::NumberOfVariables, nD = nV + S::NumberOfParameters;
+  constexpr int nf = ipow(b, DIMENSIONS - 1);
+  double QOut[nf * nD], FOut[nf * nV];
+  S s;
+  S::boundary_kind = kind;
+  const int dir = (faceIndex - faceIndex % 2) / 2;
+  Vec<DIMENSIONS> c(0.5), h(0.1);
+  kernels::aderdg::generic::c::boundaryConditions<S>(s, FOut, QOut, FIn, QIn, c, h, 0.0, 0.0, faceIndex, dir);
+  if (faceIndex % 2 == 0)
+    kernels::aderdg::generic::c::riemannSolverLinear<true, S>(s, FOut, FIn, QOut, QIn, 0.0, dir);
+  else
+    kernels::aderdg::generic::c::riemannSolverLinear<true, S>(s, FIn, FOut, QIn, QOut, 0.0, dir);
 }
 template <class S>
 void lin_surface(double* lduh, const double* lFhbnd, const double* dxa) {
@@ -681,6 +713,11 @@ void REFNAME(lin_riemann)(int pde, int N, double* FL, double* FR, const double* 
                           int dir) {
   REFNAME(init)();
   DISPATCH_LIN(pde, N, lin_riemann<S>(FL, FR, QL, QR, dt, dir));
+}
+void REFNAME(lin_boundary_face)(int pde, int N, double* FIn, const double* QIn, int faceIndex, int kind) {
+  REFNAME(init)();
+  if (pde != 2) return;
+  DISPATCH_ELASTIC(N, lin_boundary_face<S>(FIn, QIn, faceIndex, kind));
 }
 void REFNAME(lin_surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx) {
   REFNAME(init)();

@@ -30,6 +30,7 @@ void REFNAME(lin_predictor)(int pde, int N, const double* luh, const double* dx,
 void REFNAME(lin_riemann)(int pde, int N, double* FL, double* FR, const double* QL, const double* QR, double dt,
                           int dir);
 void REFNAME(lin_surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx);
+void REFNAME(lin_boundary_face)(int pde, int N, double* FIn, const double* QIn, int faceIndex, int kind);
 void REFNAME(init)();
 void REFNAME(project_fv)(int N, const double* luh, double* lim);
 void REFNAME(project_dg)(int N, const double* lim, double* luh);
@@ -74,6 +75,10 @@ void be_lsurf(void* c, double* du, const double* fb, const double* dx) {
   Ctx* x = (Ctx*)c;
   REFNAME(lin_surface_integral)(x->pde, x->N, du, fb, dx);
 }
+void be_lbnd(void* c, double* FIn, const double* QIn, int f, int kind) {
+  Ctx* x = (Ctx*)c;
+  REFNAME(lin_boundary_face)(x->pde, x->N, FIn, QIn, f, kind);
+}
 struct RefMesh { Ctx c; hrn_mesh* m; };
 size_t nsol(hrn_mesh* m) { return (size_t)m->ncells * m->P * m->k.ndata; }
 }
@@ -91,6 +96,7 @@ void* REFNAME(mesh_create)(int order, int pde, const int* cells, const double* s
     k.predictor = be_lpred;
     k.riemann = be_lriem;
     k.surface_integral = be_lsurf;
+    k.boundary_face_kind = be_lbnd;
   }
   r->m = hrn_create(&k, cells, size, bc, nthreads);
   return r;

@@ -180,9 +180,101 @@ def test_linear_solver_api_errors(eb):
     with pytest.raises(eb.ExaError):
         s.space_time_predictor(x, x, x, x, x, [1, 1], 1)  # the nonlinear predictor rejects a linear solver
     with pytest.raises(eb.ExaError):
-        eb.Mesh(s, (4, 4), [0, 0], [1, 1], eb.BC_OUTFLOW)  # periodic meshes only
+        eb.Mesh(s, (4, 4), [0, 0], [1, 1], [eb.BC_OUTFLOW, eb.BC_PERIODIC, 0, 0])  # periodic on one face only
     e = eb.Solver(2, 3, eb.PDE_EULER)
     with pytest.raises(eb.ExaError):
         e.riemann_solver_linear(x, x, None, None, None, 0)  # and the linear kernels reject a nonlinear one
     chosen, ms = s.autotune(64)
     assert chosen in (0, 1) and ms[0] > 0 and ms[1] > 0 and all(v == -1.0 for v in ms[2:])
+
+
+@pytest.mark.parametrize("dim,N", [(2, 3), (2, 5), (3, 3), (3, 5)])
+def test_linear_boundary_faces_vs_oracle_and_reference(eb, dim, N):
+    """boundaryConditions + riemannSolverLinear on boundary faces
+    (ADERDGSolver.cpp:2893-2962): outflow and rigid wall, every face index,
+    against the oracle and the reference's kernels compiled from source"""
+    rng = np.random.default_rng(31 * dim + N)
+    s = eb.Solver(dim, N, eb.PDE_ELASTIC)
+    b = N + 1
+    F, D2, n = b ** (dim - 1), 2 * dim, 9
+    qb = np.stack([random_elastic(rng, 1, D2 * F).reshape(D2, F, 12) for _ in range(n)])
+    fb = rng.normal(size=(n, D2, F, 9))
+    bc = np.arange(n, dtype=np.int32) % n
+    bf = (np.arange(n) % D2).astype(np.int32)
+    impls = ["oracle"] + (["ref"] if pyoracle.ref_available(dim) else [])
+    for kind in (eb.BC_OUTFLOW, eb.BC_REFLECTIVE):
+        fbd = dev(fb)
+        s.boundary_conditions(dev(qb), fbd, dev(bc, torch.int32), dev(bf, torch.int32), n, kind)
+        got = host(fbd)
+        for impl in impls:
+            k = pyoracle.Kernels(dim, N, pde=2, impl=impl)
+            exp = fb.copy()
+            for c, f in zip(bc, bf):
+                exp[c, f] = k.lin_boundary_face(fb[c, f], qb[c, f], int(f), 1 if kind == eb.BC_REFLECTIVE else 0).reshape(F, 9)
+            assert rel(got, exp) < RTOL, (impl, kind)
+        touched = np.zeros((n, D2), bool)
+        touched[bc, bf] = True
+        assert np.array_equal(got[~touched], fb[~touched])  # other faces untouched
+        if kind == eb.BC_OUTFLOW:
+            assert np.abs(got[touched]).max() == 0.0  # no jump, no fluctuation
+        else:
+            assert np.abs(got[touched]).max() > 0.1
+
+
+BCS = [(2, 4, (12, 12), "outflow", 12), (2, 3, (10, 8), "mixed", 12), (3, 3, (5, 5, 5), "wall", 5),
+       (3, 5, (4, 4, 4), "mixed", 3)]
+
+
+def bc_list(name, dim):
+    if name == "outflow":
+        return [0] * (2 * dim)
+    if name == "wall":
+        return [1] * (2 * dim)
+    return ([1, 1, 0, 1, -1, -1])[:2 * dim]  # x walls, y outflow / wall, z periodic
+
+
+@pytest.mark.parametrize("dim,N,cells,bcname,steps", BCS)
+def test_elastic_mesh_boundaries_vs_oracle(eb, dim, N, cells, bcname, steps):
+    """elastic waves on uniform meshes with outflow and rigid-wall faces,
+    against the oracle and the reference's kernels"""
+    from exahype_b200 import problems
+    bc = bc_list(bcname, dim)
+    code = {-1: eb.BC_PERIODIC, 0: eb.BC_OUTFLOW, 1: eb.BC_REFLECTIVE}
+    u, _ = problems.elastic_pulse(dim, N, cells, seed=13)
+    s = eb.Solver(dim, N, eb.PDE_ELASTIC)
+    m = eb.Mesh(s, cells, [0.0] * dim, [1.0] * dim, [code[k] for k in bc])
+    m.set_solution(u)
+    m.init(0.0)
+    m.step(steps)
+    a, sa = m.get_solution(), m.state()
+    impls = ["oracle"] + (["ref"] if pyoracle.ref_available(dim) else [])
+    for impl in impls:
+        o = pyoracle.Mesh(dim, N, cells, [1.0] * dim, bc, pde=2, impl=impl, nthreads=8)
+        o.set_solution(u)
+        o.init(0.0)
+        o.step(steps)
+        b_, sb = o.get_solution(), o.state()
+        assert np.linalg.norm(a - b_) / np.linalg.norm(b_) < RTOL, impl
+        assert sa["steps"] == sb["steps"] == steps and sa["dt"] == sb["dt"], impl
+    assert np.array_equal(a[..., 9:], u[..., 9:])
+
+
+def test_refined_elastic_mesh_with_walls_vs_oracle(eb):
+    """a refined elastic mesh whose domain faces are rigid walls (x) and
+    outflow (y): the boundary faces of the coarse cells"""
+    from exahype_b200 import problems
+    dim, N, cells, lo, hi, steps = 2, 3, (7, 7), (2, 2), (5, 5), 6
+    u = problems.elastic_pulse_refined(dim, N, cells, lo, hi, seed=4)
+    s = eb.Solver(dim, N, eb.PDE_ELASTIC)
+    m = eb.Mesh.nested(s, cells, [0.0] * dim, [1.0] * dim, [(lo, hi)],
+                       bc=[eb.BC_REFLECTIVE, eb.BC_REFLECTIVE, eb.BC_OUTFLOW, eb.BC_OUTFLOW])
+    o = pyoracle.RefinedMesh(dim, N, cells, [1.0] * dim, lo, hi, pde=2, bc=[1, 1, 0, 0])
+    m.set_solution(u)
+    o.set_solution(u)
+    m.init(0.0)
+    o.init(0.0)
+    m.step(steps)
+    o.step(steps)
+    a, b = m.get_solution(), o.get_solution()
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    assert m.state()["steps"] == o.state()["steps"] == steps

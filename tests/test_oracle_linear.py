@@ -169,3 +169,55 @@ def test_elastic_mesh_vs_reference(dim, N, cells, steps):
     assert sa["dt"] == sb["dt"] and sa["steps"] == sb["steps"] == steps
     # parameters are carried unchanged
     assert np.array_equal(a[..., 9:], u[..., 9:])
+
+
+@needs_ref
+@pytest.mark.parametrize("dim,N", [(2, 3), (2, 5), (3, 3), (3, 5)])
+def test_elastic_boundary_faces_vs_reference(dim, N):
+    """boundaryConditions + riemannSolverLinear on every face of a cell, for
+    outflow (the inside state copied: no jump, no fluctuation) and a rigid
+    wall (velocities negated)"""
+    rng = np.random.default_rng(7 * dim + N)
+    o, r = pyoracle.Kernels(dim, N, 2), pyoracle.Kernels(dim, N, 2, impl="ref")
+    F = (N + 1) ** (dim - 1)
+    QIn = random_elastic(rng, F)
+    FIn = rng.normal(size=F * 9)
+    for face in range(2 * dim):
+        for kind in (0, 1):
+            a = o.lin_boundary_face(FIn, QIn, face, kind)
+            b = r.lin_boundary_face(FIn, QIn, face, kind)
+            assert np.max(np.abs(a - b)) <= 1e-14 * max(np.max(np.abs(b)), 1.0), (face, kind)
+            if kind == 0:
+                assert np.max(np.abs(a)) == 0.0
+            else:
+                assert np.max(np.abs(a)) > 0.1
+    # a wall against a state at rest leaves stresses only: the fluctuation is
+    # that of the velocity jump alone, so a zero-velocity state gives zero
+    Q0 = QIn.copy()
+    Q0[:, 6:9] = 0.0
+    assert np.max(np.abs(o.lin_boundary_face(FIn, Q0, 0, 1))) == 0.0
+
+
+@needs_ref
+@pytest.mark.parametrize("dim,N,cells,bc,steps", [(2, 4, (8, 8), 0, 8), (2, 3, (8, 6), [1, 1, 0, 1], 8),
+                                                  (3, 3, (4, 4, 4), 1, 3)])
+def test_elastic_mesh_boundaries_vs_reference(dim, N, cells, bc, steps):
+    """uniform elastic meshes with outflow and rigid-wall domain faces: the
+    oracle harness over the C restatement vs over the reference's kernels"""
+    u, _ = problems.elastic_pulse(dim, N, cells, seed=9)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.Mesh(dim, N, cells, [1.0] * dim, bc, pde=2, impl=impl, nthreads=4)
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(steps)
+        res.append((m.get_solution(), m.state()))
+    (a, sa), (b, sb) = res
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-13
+    assert sa["dt"] == sb["dt"] and sa["steps"] == sb["steps"] == steps
+    # the boundaries change the solution against the periodic mesh
+    m = pyoracle.Mesh(dim, N, cells, [1.0] * dim, -1, pde=2, nthreads=4)
+    m.set_solution(u)
+    m.init(0.0)
+    m.step(steps)
+    assert np.linalg.norm(m.get_solution() - a) / np.linalg.norm(a) > 1e-8

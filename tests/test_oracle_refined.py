@@ -107,3 +107,21 @@ def test_refined_oracle_free_stream():
     m.init(0.0)
     m.step(3)
     assert np.abs(m.get_solution() - u).max() < 1e-10
+
+
+def test_refined_oracle_elastic_walls_vs_reference_kernels():
+    """the linear kernels' boundary faces on a refined mesh: rigid walls in x,
+    outflow in y"""
+    if not pyoracle.ref_available(2):
+        pytest.skip("compiled reference kernels not built")
+    from exahype_b200 import problems
+    cells, lo, hi = (7, 7), (2, 2), (5, 5)
+    u = problems.elastic_pulse_refined(2, 3, cells, lo, hi, seed=4)
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.RefinedMesh(2, 3, cells, [1.0, 1.0], lo, hi, pde=2, impl=impl, bc=[1, 1, 0, 0])
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(4)
+        res.append(m.get_solution())
+    assert np.linalg.norm(res[0] - res[1]) / np.linalg.norm(res[1]) < 1e-12
