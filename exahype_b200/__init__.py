@@ -26,6 +26,7 @@ PDE_EULER = 0
 PDE_EULER_TEST = 1
 PDE_ELASTIC = 2  # linear elastic waves: 9 variables + lambda, mu, rho; linear kernels
 PDE_EULER_SOURCE_NCP = 3  # the kernel-test mock with an algebraic source and a non-conservative product
+PDE_ELASTIC_POINT_SOURCE = 4  # PDE_ELASTIC with a Ricker-wavelet point source (Solver.set_point_source)
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE = -1, 0, 1
 # predictor variants beyond the autotuned 0..3: the mixed-precision predictor
 PREDICTOR_MIXED, PREDICTOR_MIXED_2 = 4, 5
@@ -103,7 +104,7 @@ class Solver:
         self.unknowns_per_cell, self.data_per_cell, self.data_per_face, self.fluxes_per_face = list(z)
         self.nvar = self.unknowns_per_cell // (order + 1) ** dim
         self.ndata = self.data_per_cell // (order + 1) ** dim
-        self.linear = pde == PDE_ELASTIC
+        self.linear = pde in (PDE_ELASTIC, PDE_ELASTIC_POINT_SOURCE)
 
     def __del__(self):
         try:
@@ -143,6 +144,22 @@ class Solver:
         _check(load().exa_space_time_predictor_linear_temps(
             self._h, _ptr(luh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(lduh), _ptr(dt_dev), _dbl3(dx), int(ncells),
             _ptr(lQhi), _ptr(lFhi), _stream(stream)), "exa_space_time_predictor_linear_temps")
+
+    def set_point_source(self, x0, t0=0.1, f0=8.0, amplitude=1.0):
+        """the point source of PDE_ELASTIC_POINT_SOURCE: a Ricker wavelet of
+        peak frequency f0 and delay t0 on the normal stresses at x0"""
+        x = (ctypes.c_double * 3)(*(list(x0) + [0.0] * (3 - len(x0))))
+        _check(load().exa_solver_set_point_source(self._h, x, ctypes.c_double(t0), ctypes.c_double(f0),
+                                                  ctypes.c_double(amplitude)), "exa_solver_set_point_source")
+
+    def space_time_predictor_linear_point_source(self, luh, lQhbnd, lFhbnd, lduh, t_dev, dt_dev, dx, centres, ncells,
+                                                 cell_list=None, lQhi=None, lFhi=None, stream=None):
+        """the linear predictor with the point source evaluated per cell
+        (centres: device [ncells][3]; t_dev: the solution's time stamp)"""
+        _check(load().exa_space_time_predictor_linear_point_source(
+            self._h, _ptr(luh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(lduh), _ptr(t_dev), _ptr(dt_dev), _dbl3(dx),
+            _ptr(centres), int(ncells), _ptr(cell_list), _ptr(lQhi), _ptr(lFhi), _stream(stream)),
+            "exa_space_time_predictor_linear_point_source")
 
     def riemann_solver_linear(self, lQhbnd, lFhbnd, face_left, face_right, face_dir, nfaces, stream=None):
         _check(load().exa_riemann_solver_linear(self._h, _ptr(lQhbnd), _ptr(lFhbnd), _ptr(face_left),

@@ -36,6 +36,12 @@ struct Geometry {
   double dx[3];
   const int* inst;
   const double* inst_dx;
+  // point sources (PDE::kPointSource): cell centres [cell][3], the time
+  // stamp of the solution the predictor starts from (one for all cells), the
+  // source's parameters; no centres: no source
+  const double* centre;
+  const double* time;
+  double ps[6];
 };
 __device__ __forceinline__ int cell_instance(const Geometry& g, int cell) { return g.inst ? g.inst[cell] : 0; }
 __device__ __forceinline__ double cell_width(const Geometry& g, int inst, int d) {

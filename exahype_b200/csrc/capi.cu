@@ -156,6 +156,7 @@ struct KernelSet {
   int (*amr_face)(double*, double*, const double*, const double*, int, const int*, const int*, const int*,
                   const int*, int, cudaStream_t);
   int (*plot)(const double*, double*, int, cudaStream_t);
+  bool point_source;  // the PDE has a point source (usePointSource)
 };
 
 template <int DIM, int N, class PDE>
@@ -397,6 +398,7 @@ struct LinearLaunch {
     using S = Shape<DIM, N, PDE>;
     KernelSet k{DIM, N, pde, S::nV, S::nP, S::P, S::F, true, &predictor, &riemann, &boundary, &corrector, &volume};
     AmrLaunch<DIM, N, PDE>::fill(k);
+    k.point_source = PDE::kPointSource;
     return k;
   }
 };
@@ -405,6 +407,7 @@ struct LinearLaunch {
 #define EXA_ORDERS_TEST(X, D) X(D, 3, EulerTestPDE, 1) X(D, 5, EulerTestPDE, 1)
 #define EXA_ORDERS_SOURCE_NCP(X, D) X(D, 3, EulerSourceNCPPDE, 3) X(D, 5, EulerSourceNCPPDE, 3)
 #define EXA_ORDERS_ELASTIC(X, D) X(D, 3, ElasticPDE, 2) X(D, 4, ElasticPDE, 2) X(D, 5, ElasticPDE, 2)
+#define EXA_ORDERS_ELASTIC_PS(X, D) X(D, 3, ElasticPointSourcePDE, 4) X(D, 5, ElasticPointSourcePDE, 4)
 
 static bool find_kernels(int dim, int order, int pde, KernelSet* out) {
 #define X(D, NN, PDE_, ID)                                     \
@@ -426,6 +429,8 @@ static bool find_kernels(int dim, int order, int pde, KernelSet* out) {
   }
   EXA_ORDERS_ELASTIC(X, 2)
   EXA_ORDERS_ELASTIC(X, 3)
+  EXA_ORDERS_ELASTIC_PS(X, 2)
+  EXA_ORDERS_ELASTIC_PS(X, 3)
 #undef X
   return false;
 }
@@ -541,6 +546,9 @@ using namespace exa;
 struct exa_solver {
   KernelSet k;
   int variant = 0;  // predictor variant (set by exa_solver_autotune / exa_solver_set_variant)
+  // point source of a PDE with one (exa_solver_set_point_source): position
+  // x0[3], delay t0, peak frequency f0, amplitude
+  double ps[6] = {0.5, 0.5, 0.5, 0.1, 8.0, 1.0};
 };
 
 // one level of a refined mesh on the host: the bounding rectangle [r0, r1)
@@ -570,6 +578,7 @@ struct exa_mesh {
   int nfaces = 0, nbfaces[3] = {0, 0, 0};  // boundary faces grouped by kind: outflow, reflective
   int boff[3] = {0, 0, 0};
   unsigned long long* sweeps = nullptr;
+  double* centre = nullptr;  // cell centres [cell][3] (point-source PDEs only)
   cudaStream_t stream = nullptr;
   bool initialised = false;
   // optional per-phase event timing
@@ -669,7 +678,20 @@ int exa_solver_sizes(const exa_solver* s, int* z) {
 static Geometry geom(const exa_solver* s, const double* dx) {
   Geometry g{};
   for (int d = 0; d < 3; d++) g.dx[d] = d < s->k.dim ? dx[d] : 1.0;
+  for (int i = 0; i < 6; i++) g.ps[i] = s->ps[i];
   return g;
+}
+
+int exa_solver_set_point_source(exa_solver* s, const double* x0, double t0, double f0, double amplitude) {
+  if (!s || !x0) return fail(EXA_ERR_ARG, "exa_solver_set_point_source: null argument");
+  if (!s->k.point_source) return fail(EXA_ERR_UNSUPPORTED, "exa_solver_set_point_source: the PDE has no point source");
+  if (!std::isfinite(t0) || !std::isfinite(f0) || !std::isfinite(amplitude))
+    return fail(EXA_ERR_ARG, "exa_solver_set_point_source: non-finite parameter");
+  for (int d = 0; d < 3; d++) s->ps[d] = d < s->k.dim ? x0[d] : 0.0;
+  s->ps[3] = t0;
+  s->ps[4] = f0;
+  s->ps[5] = amplitude;
+  return EXA_OK;
 }
 
 int exa_space_time_predictor_nonlinear(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
@@ -708,8 +730,28 @@ int exa_space_time_predictor_linear(const exa_solver* s, const double* luh, doub
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_linear: null argument or negative count");
   if (!s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_linear: nonlinear PDE");
+  if (s->k.point_source)
+    return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_linear: point-source PDE, use _linear_point_source");
   return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, nullptr, dt_dev, geom(s, dx), ncells, cell_list, nullptr,
                         PredictorTemps{}, false, nullptr, s->variant, (cudaStream_t)stream);
+}
+
+int exa_space_time_predictor_linear_point_source(const exa_solver* s, const double* luh, double* lQhbnd,
+                                                 double* lFhbnd, double* lduh, const double* t_dev,
+                                                 const double* dt_dev, const double* dx, const double* centres,
+                                                 int ncells, const int* cell_list, double* lQhi, double* lFhi,
+                                                 void* stream) {
+  if (!s || !luh || !lQhbnd || !lFhbnd || !t_dev || !dt_dev || !dx || !centres || ncells < 0 || (!lQhi != !lFhi))
+    return fail(EXA_ERR_ARG, "exa_space_time_predictor_linear_point_source: null argument or negative count");
+  if (!s->k.linear || !s->k.point_source)
+    return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_linear_point_source: the PDE has no point source");
+  Geometry g = geom(s, dx);
+  g.centre = centres;
+  g.time = t_dev;
+  const bool temps = lQhi != nullptr;
+  return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, nullptr, dt_dev, g, ncells, cell_list, nullptr,
+                        PredictorTemps{nullptr, nullptr, lQhi, lFhi}, temps, nullptr, s->variant,
+                        (cudaStream_t)stream);
 }
 
 int exa_space_time_predictor_linear_temps(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
@@ -718,6 +760,8 @@ int exa_space_time_predictor_linear_temps(const exa_solver* s, const double* luh
   if (!s || !luh || !lQhbnd || !lFhbnd || !dt_dev || !dx || ncells < 0 || !lQhi || !lFhi)
     return fail(EXA_ERR_ARG, "exa_space_time_predictor_linear_temps: null argument or negative count");
   if (!s->k.linear) return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_linear_temps: nonlinear PDE");
+  if (s->k.point_source)
+    return fail(EXA_ERR_UNSUPPORTED, "exa_space_time_predictor_linear_temps: point-source PDE, use _linear_point_source");
   return s->k.predictor(luh, lQhbnd, lFhbnd, lduh, nullptr, dt_dev, geom(s, dx), ncells, nullptr, nullptr,
                         PredictorTemps{nullptr, nullptr, lQhi, lFhi}, true, nullptr, s->variant,
                         (cudaStream_t)stream);
@@ -909,9 +953,34 @@ static void mesh_free(exa_mesh* m) {
   if (m->io_in) cudaStreamDestroy(m->io_in);
   if (m->io_out) cudaStreamDestroy(m->io_out);
   for (void* p : {(void*)m->luh, (void*)m->lduh, (void*)m->lQhbnd, (void*)m->lFhbnd, (void*)m->scal, (void*)m->iters,
-                  (void*)m->fl, (void*)m->fr, (void*)m->fd, (void*)m->bcell, (void*)m->bface, (void*)m->sweeps})
+                  (void*)m->fl, (void*)m->fr, (void*)m->fd, (void*)m->bcell, (void*)m->bface, (void*)m->sweeps,
+                  (void*)m->centre})
     sfree(p, m->stream);
   if (m->stream) cudaStreamDestroy(m->stream);
+}
+
+// Cell centres of a point-source PDE's mesh: cell c at grid position p of a
+// level of widths h spans [offset + p h, offset + (p + 1) h]; its centre is
+// offset + p h + h / 2 (the cell offset plus half its size, as the reference
+// passes it to pointSource, ADERDGSolver.cpp:1929). pos: 3 ints per cell;
+// widths: 3 doubles per level (level per cell, or all 0).
+static int mesh_centres(exa_mesh* m, const std::vector<int>& pos, const std::vector<int>* level,
+                        const std::vector<double>& widths) {
+  if (!m->s->k.point_source) return EXA_OK;
+  std::vector<double> c(3 * (size_t)m->ncells, 0.0);
+  for (size_t i = 0; i < (size_t)m->ncells; i++) {
+    const double* h = &widths[3 * (size_t)(level ? (*level)[i] : 0)];
+    for (int d = 0; d < m->dim; d++) c[3 * i + d] = (m->offset[d] + pos[3 * i + d] * h[d]) + 0.5 * h[d];
+  }
+  if (!salloc(&m->centre, c.size() * 8, m->stream)) {
+    cudaGetLastError();
+    m->centre = nullptr;
+    return fail(EXA_ERR_NOMEM, "mesh: device allocation of the cell centres failed");
+  }
+  EXA_CUDA(cudaMemcpyAsync(m->centre, c.data(), c.size() * 8, cudaMemcpyHostToDevice, m->stream));
+  EXA_CUDA(cudaStreamSynchronize(m->stream));  // c goes out of scope
+  m->geo.centre = m->centre;
+  return EXA_OK;
 }
 
 int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset, const double* size, const int* bc,
@@ -1009,6 +1078,19 @@ int exa_mesh_create(const exa_solver* s, const int* cells, const double* offset,
   EXA_CUDA(cudaMemsetAsync(m->lFhbnd, 0, n * D2 * F * nV * 8, st));
   EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, st));
   EXA_CUDA(cudaStreamSynchronize(st));
+  if (s->k.point_source) {
+    std::vector<int> pos(3 * n, 0);
+    for (size_t c = 0; c < n; c++) {
+      pos[3 * c] = (int)(c % m->cells[0]);
+      pos[3 * c + 1] = (int)((c / m->cells[0]) % m->cells[1]);
+      pos[3 * c + 2] = (int)(c / ((size_t)m->cells[0] * m->cells[1]));
+    }
+    const std::vector<double> w(m->geo.dx, m->geo.dx + 3);
+    if (int rc = mesh_centres(m.get(), pos, nullptr, w)) {
+      mesh_free(m.get());
+      return rc;
+    }
+  }
   *out = m.release();
   return EXA_OK;
 }
@@ -1305,6 +1387,10 @@ int exa_mesh_create_boxes(const exa_solver* s, const int* cells, const double* o
   EXA_CUDA(cudaMemsetAsync(m->lFhbnd, 0, ns * D2 * F * nV * 8, st));
   EXA_CUDA(cudaMemsetAsync(m->sweeps, 0, 8, st));
   EXA_CUDA(cudaStreamSynchronize(st));  // the host vectors go out of scope
+  if (int rc = mesh_centres(m.get(), m->ref.pos, &m->ref.level, m->ref.ldx)) {
+    mesh_free(m.get());
+    return rc;
+  }
   *out = m.release();
   return EXA_OK;
 }
@@ -1390,12 +1476,20 @@ static int mesh_amr_faces(exa_mesh* m) {
                     m->ref.pro_ld, m->ref.pro_idx, 0, m->stream);
 }
 
-static int mesh_predict(exa_mesh* m, const int* count = nullptr) {
+// after_update: the fused scheme's predictor right after the update, whose
+// solution carries the predictor time stamp scal[4]; every other predictor
+// call starts from the corrector time stamp scal[2] (point sources)
+static int mesh_predict(exa_mesh* m, const int* count = nullptr, bool after_update = false) {
   const KernelSet& k = m->s->k;
   PhaseTimer pt(m, 0);
   m->phase_launches[0] += 2;
   double* dt = m->fused ? (m->ref.on ? m->ref.lv + 2 * m->ref.nlev : m->scal + 5) : mesh_dt(m);
-  int rc = k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, dt, m->geo,
+  Geometry g = m->geo;
+  if (k.point_source) {
+    g.time = m->scal + (after_update ? 4 : 2);
+    for (int i = 0; i < 6; i++) g.ps[i] = m->s->ps[i];
+  }
+  int rc = k.predictor(m->luh, m->lQhbnd, m->lFhbnd, m->lduh, m->iters, dt, g,
                        m->ncells, nullptr, count, PredictorTemps{}, false, m->sweeps, m->s->variant, m->stream);
   if (rc || !m->ref.on) return rc;
   m->phase_launches[0] += 3;
@@ -1565,7 +1659,7 @@ static int mesh_one_step(exa_mesh* m) {
     // step size right after the update (no global reduction in between),
     // then the step bookkeeping, then the rerun, which does nothing unless
     // needed (its blocks return at once when the device count is 0)
-    rc = mesh_predict(m);
+    rc = mesh_predict(m, nullptr, true);
     if (rc) return rc;
     {
       PhaseTimer pt(m, 3);

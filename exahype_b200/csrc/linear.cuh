@@ -2,8 +2,10 @@
 // (PDE::kLinear, e.g. ElasticPDE):
 //   ck_predictor_kernel    spaceTimePredictorLinear (2d/spaceTimePredictorLinear.cpph:35-409,
 //                          3d/spaceTimePredictorLinear.cpph:34-446) + volumeIntegralLinear
-//                          (3d/volumeIntegralLinear.cpph:20-52)
+//                          (3d/volumeIntegralLinear.cpph:20-52); for a PDE with a point
+//                          source also pointSource (3d/pointSource.cpph:28-143)
 //   riemann_linear_kernel  riemannSolverLinear (3d/riemannSolverLinear.cpph:20-136)
+//   boundary_linear_kernel boundaryConditions + riemannSolverLinear on boundary faces
 //   volume_linear_kernel   volumeIntegralLinear on its own (kernel-level entry point)
 // The surface integral is the corrector's linear form (aderdg.cuh).
 //
@@ -67,6 +69,90 @@ __device__ __forceinline__ int line_node(int d, int L, int n) {
   return d == 0 ? (a0 * b + a1) * b + n : d == 1 ? (a0 * b + n) * b + a1 : (n * b + a0) * b + a1;
 }
 
+// Lagrange basis polynomial i of the Gauss-Legendre nodes of order N at xi
+// (the reference's basisFunctions[N][i], kernels/DGBasisFunctions.h:53), as
+// the product over the other nodes
+template <int N>
+__device__ double lagrange_at(int i, double xi) {
+  const OrderTables& T = c_tab[N];
+  double r = 1.0;
+#pragma unroll
+  for (int m = 0; m < N + 1; m++)
+    if (m != i) r = __dmul_rn(r, __ddiv_rn(__dsub_rn(xi, T.x[m]), __dsub_rn(T.x[i], T.x[m])));
+  return r;
+}
+
+// Whether the point source of PDE::sourcePosition lies in the closed cell of
+// centre c and widths h, tested on the reference coordinates as pointSource
+// tests them
+template <int DIM, class PDE>
+__device__ bool point_source_in_cell(const Geometry& geo, const double* c, const double* h) {
+  double x0[3];
+  PDE::sourcePosition(geo.ps, x0);
+  bool in = true;
+#pragma unroll
+  for (int e = 0; e < DIM; e++) {
+    const double xr = __ddiv_rn(__dsub_rn(x0[e], __dsub_rn(c[e], __ddiv_rn(h[e], 2.0))), h[e]);
+    in = in && xr >= 0.0 && xr <= 1.0;
+  }
+  return in;
+}
+
+// pointSource (2d/pointSource.cpph:30-127, 3d/pointSource.cpph:28-143) at
+// node p of the cell of centre c and widths h, time slot n (0: t; n >= 1:
+// Gauss-Legendre time node n - 1 of [t, t + dt]): the PDE's source at the
+// node's position, projected onto the node's basis function at the source's
+// reference coordinates and divided by the node's quadrature weight and the
+// cell's widths; zero where the source lies outside the closed cell. The
+// reference's operations in its order, rounded one by one.
+template <int DIM, int N, class PDE>
+__device__ void node_point_source(const Geometry& geo, const double* c, const double* h, int p, double t, double dt,
+                                  int n, double* out) {
+  constexpr int b = N + 1;
+  const OrderTables& T = c_tab[N];
+  const int ix = p % b, iy = (p / b) % b, iz = DIM == 3 ? p / (b * b) : 0;
+  const double tn = n == 0 ? t : __dadd_rn(__dmul_rn(dt, T.x[n - 1]), t);
+  double x[3] = {0.0, 0.0, 0.0}, x0[3];
+  x[0] = __dadd_rn(c[0], __dmul_rn(h[0], __dsub_rn(T.x[ix], 0.5)));
+  x[1] = __dadd_rn(c[1], __dmul_rn(h[1], __dsub_rn(T.x[iy], 0.5)));
+  if (DIM == 3) x[2] = __dadd_rn(c[2], __dmul_rn(h[2], __dsub_rn(T.x[iz], 0.5)));
+  PDE::pointSource(x, tn, dt, out, x0, geo.ps);
+  double xr[3] = {0.0, 0.0, 0.0};
+  bool in = true;
+#pragma unroll
+  for (int e = 0; e < DIM; e++) {
+    xr[e] = __ddiv_rn(__dsub_rn(x0[e], __dsub_rn(c[e], __ddiv_rn(h[e], 2.0))), h[e]);
+    in = in && xr[e] >= 0.0 && xr[e] <= 1.0;
+  }
+  double phi, den;
+  if (DIM == 3) {
+    phi = __dmul_rn(__dmul_rn(lagrange_at<N>(iz, xr[2]), lagrange_at<N>(iy, xr[1])), lagrange_at<N>(ix, xr[0]));
+    den = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(T.w[iz], h[2]), T.w[iy]), h[1]), T.w[ix]), h[0]);
+  } else {
+    phi = __dmul_rn(lagrange_at<N>(iy, xr[1]), lagrange_at<N>(ix, xr[0]));
+    den = __dmul_rn(__dmul_rn(__dmul_rn(T.w[iy], h[1]), T.w[ix]), h[0]);
+  }
+#pragma unroll
+  for (int v = 0; v < PDE::nVar; v++) out[v] = in ? __ddiv_rn(__dmul_rn(phi, out[v]), den) : 0.0;
+}
+
+// sum over the time slots n = 1..b of w[n-1] * pointSource (the time
+// integral the predictor adds, 3d/spaceTimePredictorLinear.cpph:77-90 and
+// :294-308)
+template <int DIM, int N, class PDE>
+__device__ void node_point_source_sum(const Geometry& geo, const double* c, const double* h, int p, double t,
+                                      double dt, double* sum) {
+  const OrderTables& T = c_tab[N];
+#pragma unroll
+  for (int v = 0; v < PDE::nVar; v++) sum[v] = 0.0;
+  for (int n = 1; n < N + 2; n++) {
+    double val[PDE::nVar];
+    node_point_source<DIM, N, PDE>(geo, c, h, p, t, dt, n, val);
+#pragma unroll
+    for (int v = 0; v < PDE::nVar; v++) sum[v] = __dadd_rn(sum[v], __dmul_rn(T.w[n - 1], val[v]));
+  }
+}
+
 // NREG: register cap per thread, regs_for_blocks<THREADS, blocks per SM>()
 template <int DIM, int N, class PDE, int NREG>
 __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
@@ -97,13 +183,36 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
 #pragma unroll
     for (int d = 0; d < 3; d++) s_idx[lc][d] = d < DIM ? 1.0 / cell_width(geo, inst, d) : 0.0;
   }
+  // point sources: this cell's centre, widths and time stamp, and whether
+  // the source lies in it (the same for all threads of the cell)
+  constexpr bool PS = PDE::kPointSource;
+  double pc[3] = {0.0, 0.0, 0.0}, ph[3] = {1.0, 1.0, 1.0}, pt = 0.0;
+  bool src = false;
+  if constexpr (PS) {
+    if (active && geo.centre) {
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        pc[d] = geo.centre[3 * (size_t)cell + d];
+        ph[d] = cell_width(geo, inst, d);
+      }
+      pt = *geo.time;
+      src = point_source_in_cell<DIM, PDE>(geo, pc, ph);
+    }
+  }
   // level 0: the solution (parameters included); inactive slots get unit
-  // parameters so that their arithmetic stays finite
+  // parameters so that their arithmetic stays finite. A point source adds dt
+  // times its time integral (3d/spaceTimePredictorLinear.cpph:77-90).
   double qh[nV];
   {
+    double psw[nV];
+#pragma unroll
+    for (int v = 0; v < nV; v++) psw[v] = 0.0;
+    if constexpr (PS)
+      if (src) node_point_source_sum<DIM, N, PDE>(geo, pc, ph, p, pt, dt, psw);
 #pragma unroll
     for (int v = 0; v < nD; v++) {
-      const double q = active ? __ldg(luh + ((size_t)cell * P + p) * nD + v) : (v < nV ? 0.0 : 1.0);
+      double q = active ? __ldg(luh + ((size_t)cell * P + p) * nD + v) : (v < nV ? 0.0 : 1.0);
+      if (v < nV && PS && src) q = __dadd_rn(q, __dmul_rn(dt, psw[v]));
       sQ[p * QS + v] = q;
       if (v < nV) qh[v] = q;
     }
@@ -165,9 +274,12 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
     // per node: non-conservative product one direction at a time (few
     // registers live), time averages, next level
     {
+      // level 1 starts from the point source's value at t (:93-101)
       double qn[nV];
 #pragma unroll
       for (int v = 0; v < nV; v++) qn[v] = 0.0;
+      if constexpr (PS)
+        if (src && i == 0) node_point_source<DIM, N, PDE>(geo, pc, ph, p, pt, dt, 0, qn);
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
         double B[nV];
@@ -187,6 +299,16 @@ __global__ void __launch_bounds__(CKCfg<DIM, N, PDE>::THREADS) __maxnreg__(NREG)
       }
       fac_i = fac_n;
       fac_n = fac_n * (dt / (i + 3));
+    }
+  }
+  if constexpr (PS) {
+    if (src) {  // the time integral of the source, split over the directions (:294-308)
+      double psw[nV];
+      node_point_source_sum<DIM, N, PDE>(geo, pc, ph, p, pt, dt, psw);
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int v = 0; v < nV; v++) fh[d][v] = __dadd_rn(fh[d][v], __ddiv_rn(psw[v], (double)DIM));
     }
   }
   __syncthreads();

@@ -242,6 +242,7 @@ struct ElasticPDE {
   static constexpr int nObs = 9;
   static constexpr bool kLinear = true;
   static constexpr bool kSource = false, kNCP = false;  // (its product enters the linear kernels directly)
+  static constexpr bool kPointSource = false;           // the generated glue's usePointSource
 
   // boundaryValues (this library's; the reference's kernel tests define
   // none for this PDE): kOutflow copies the inside state, kReflective is a
@@ -347,6 +348,30 @@ struct ElasticPDE {
     const double cp = __dsqrt_rn(__ddiv_rn(__dadd_rn(lam, __dmul_rn(2.0, mu)), rho));
     const double cs = __dsqrt_rn(__ddiv_rn(mu, rho));
     return (cp < cs) ? cs : cp;
+  }
+};
+
+// ElasticPDE with a point source (usePointSource = true): the source of this
+// library's point-source mock (the reference's kernel tests define none), a
+// Ricker wavelet of peak frequency f0 and delay t0, amplitude amp, on the
+// three normal stresses, located at x0 whatever the node position x
+// (UserSolverInterface::pointSource(x, t, dt, forceVector, x0),
+// exahype/solvers/UserSolverInterface.h:75). ps = {x0[3], t0, f0, amp} comes
+// from the solver. sourcePosition gives x0 without a node: the kernels skip
+// the cells whose closed box does not hold it.
+struct ElasticPointSourcePDE : ElasticPDE {
+  static constexpr bool kPointSource = true;
+  __device__ static void pointSource(const double* /*x*/, double t, double /*dt*/, double* force, double* x0,
+                                     const double* ps) {
+    const double r = (3.14159265358979323846 * ps[4]) * (t - ps[3]);
+    const double a = r * r;
+    const double w = ps[5] * ((1.0 - 2.0 * a) * exp(-a));
+#pragma unroll
+    for (int v = 0; v < nVar; v++) force[v] = v < 3 ? w : 0.0;
+    sourcePosition(ps, x0);
+  }
+  __device__ static void sourcePosition(const double* ps, double* x0) {
+    for (int d = 0; d < 3; d++) x0[d] = ps[d];
   }
 };
 

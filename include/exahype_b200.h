@@ -50,6 +50,12 @@ extern "C" {
  * line form has none), the Riemann and boundary kernels add the product's
  * fluctuations, the volume integral the time-averaged source. */
 #define EXA_PDE_EULER_SOURCE_NCP 3
+/* EXA_PDE_ELASTIC with a point source (usePointSource = true): a Ricker
+ * wavelet on the three normal stresses at a fixed position, parameters set
+ * by exa_solver_set_point_source; orders 3 and 5. Its predictor is
+ * exa_space_time_predictor_linear_point_source; meshes evaluate the source
+ * themselves. */
+#define EXA_PDE_ELASTIC_POINT_SOURCE 4
 
 /* Boundary kinds for exa_boundary_conditions / exa_mesh_create. */
 #define EXA_BC_PERIODIC (-1)
@@ -90,6 +96,12 @@ int exa_solver_sizes(const exa_solver* s, int* sizes4);
 #define EXA_PREDICTOR_MIXED_2 5  /* mixed line form, 2 blocks per SM where they fit */
 int exa_solver_autotune(exa_solver* s, int ncells, double* variant_ms, int* chosen);
 int exa_solver_set_variant(exa_solver* s, int variant);
+/* The point source of EXA_PDE_ELASTIC_POINT_SOURCE (the user's pointSource,
+ * exahype/solvers/UserSolverInterface.h:75, of this library's point-source
+ * PDE): force amplitude * (1 - 2 a) exp(-a), a = (pi f0 (t - t0))^2, on the
+ * normal stresses, located at x0[dim]. Defaults: x0 = (0.5, 0.5, 0.5),
+ * t0 = 0.1, f0 = 8, amplitude 1. EXA_ERR_UNSUPPORTED for other PDEs. */
+int exa_solver_set_point_source(exa_solver* s, const double* x0, double t0, double f0, double amplitude);
 int exa_solver_get_variant(const exa_solver* s, int* variant);
 
 /* spaceTimePredictor (Kernels.h:85-95) + volumeIntegral (Kernels.h:104-106)
@@ -114,7 +126,7 @@ int exa_space_time_predictor_nonlinear_temps(const exa_solver* s, const double* 
  * (ADERDGSolver::solveRiemannProblemAtInterface, ADERDGSolver.cpp:2789-2866). */
 int exa_riemann_solver_nonlinear(const exa_solver* s, const double* lQhbnd, double* lFhbnd, const int* face_left,
                                  const int* face_right, const int* face_dir, int nfaces, void* stream);
-/* Linear kernels, for solvers of a linear PDE (EXA_PDE_ELASTIC; the reference's
+/* Linear kernels, for solvers of a linear PDE (EXA_PDE_ELASTIC[_POINT_SOURCE]; the reference's
  * generated glue calls them when the solver is linear,
  * AbstractGenericADERDGSolverImplementation.template:53-54,85-86,101-149).
  * The nonlinear entry points above reject a linear solver and vice versa;
@@ -133,6 +145,19 @@ int exa_space_time_predictor_linear(const exa_solver* s, const double* luh, doub
 int exa_space_time_predictor_linear_temps(const exa_solver* s, const double* luh, double* lQhbnd, double* lFhbnd,
                                           double* lduh, const double* dt_dev, const double* dx, int ncells,
                                           double* lQhi, double* lFhi, void* stream);
+/* The linear predictor of a point-source PDE (spaceTimePredictorLinear
+ * <usePointSource = true>, after the glue's pointSource(t, dt, centre, dx,
+ * forces) of each cell, ADERDGSolver.cpp:1929-1960 and
+ * c/{2d,3d}/pointSource.cpph): *t_dev is the time stamp of the solution the
+ * predictor starts from, centres[3 * cell + d] (device) the cells' centres;
+ * a cell whose closed box does not hold the source is predicted without it.
+ * lQhi / lFhi: optional time averages as for _temps (both or neither). The
+ * two entry points above reject a point-source PDE. */
+int exa_space_time_predictor_linear_point_source(const exa_solver* s, const double* luh, double* lQhbnd,
+                                                 double* lFhbnd, double* lduh, const double* t_dev,
+                                                 const double* dt_dev, const double* dx, const double* centres,
+                                                 int ncells, const int* cell_list, double* lQhi, double* lFhi,
+                                                 void* stream);
 /* riemannSolverLinear (c/{2d,3d}/riemannSolverLinear.cpph) for nfaces
  * interior faces, face arrays as for exa_riemann_solver_nonlinear: the
  * fluctuations (Bn -/+ smax I)^T (QR - QL)/2 are written to the left / right

@@ -56,6 +56,11 @@ typedef struct {
   /* optional: a boundary face that needs the boundary kind of its domain
    * face (0 outflow, 1 reflective); used instead of boundary_face when set */
   void (*boundary_face_kind)(void* ctx, double* FIn, const double* QIn, int faceIndex, int kind);
+  /* optional: a predictor that needs the cell's centre and the time stamp of
+   * the solution it starts from (point sources); used instead of predictor
+   * when set */
+  int (*predictor_at)(void* ctx, const double* luh, const double* dx, const double* centre, double t, double dt,
+                      double* lQhbnd, double* lFhbnd, double* lduh);
 } hrn_backend;
 
 typedef struct {
@@ -68,6 +73,7 @@ typedef struct {
   int* iters;
   double t, dt;     /* corrector time stamp and step size */
   double pdt;       /* step size of the next predictor call */
+  double pt;        /* time stamp of the solution the next predictor call starts from */
   long steps, sweeps;
   /* fused time stepping */
   int fused;
@@ -153,7 +159,14 @@ static void hrn_run_range(hrn_job* j) {
   const int P = m->P, F = m->F, nV = k->nvar, nD = k->ndata, D2 = 2 * m->dim;
   j->dtmin = DBL_MAX;
   for (int i = j->lo; i < j->hi; i++) {
-    if (j->phase == 0) { /* predictor + volume integral */
+    if (j->phase == 0 && k->predictor_at) { /* predictor + volume integral at the cell's centre */
+      const int ijk[3] = {i % m->cells[0], (i / m->cells[0]) % m->cells[1], i / (m->cells[0] * m->cells[1])};
+      double centre[3];
+      for (int d = 0; d < 3; d++) centre[d] = ijk[d] * m->dx[d] + 0.5 * m->dx[d];
+      m->iters[i] = k->predictor_at(k->ctx, m->luh + (size_t)i * P * nD, m->dx, centre, m->pt, m->pdt,
+                                    m->lQhbnd + (size_t)i * D2 * F * nD, m->lFhbnd + (size_t)i * D2 * F * nV,
+                                    m->lduh + (size_t)i * P * nV);
+    } else if (j->phase == 0) { /* predictor + volume integral */
       m->iters[i] = k->predictor(k->ctx, m->luh + (size_t)i * P * nD, m->dx, m->pdt, m->lQhbnd + (size_t)i * D2 * F * nD,
                                  m->lFhbnd + (size_t)i * D2 * F * nV, m->lduh + (size_t)i * P * nV);
     } else if (j->phase == 1) { /* interior face */
@@ -222,6 +235,7 @@ static void hrn_init(hrn_mesh* m, double t0) {
   m->fused = 0;
   m->dt = hrn_parallel(m, 4, m->ncells);
   m->pdt = m->dt;
+  m->pt = t0;
   hrn_predict(m);
 }
 
@@ -237,6 +251,7 @@ static void hrn_init_fused(hrn_mesh* m, double t0, double w) {
   m->pdt = s0;
   m->tp = t0 + s0;
   m->next = DBL_MAX;
+  m->pt = t0;
   hrn_predict(m);
 }
 
@@ -244,6 +259,7 @@ static void hrn_step_fused(hrn_mesh* m) {
   hrn_parallel(m, 1, m->nfaces);
   hrn_parallel(m, 2, m->nb);
   const double s = hrn_parallel(m, 3, m->ncells); /* corrector with m->dt */
+  m->pt = m->tp;                                  /* the updated solution's stamp */
   hrn_predict(m);                                 /* predictor with m->pdt */
   double next = DBL_MAX;
   next = (s < next) ? s : next; /* updateMinNextPredictorTimeStepSize */
@@ -265,6 +281,7 @@ static void hrn_step_fused(hrn_mesh* m) {
   m->steps++;
   if (unstable) {
     m->reruns++;
+    m->pt = m->t;
     hrn_predict(m);
   }
 }
@@ -281,6 +298,7 @@ static void hrn_step(hrn_mesh* m, int n) {
     m->t += m->dt;
     m->dt = dtn;
     m->pdt = dtn;
+    m->pt = m->t;
     m->steps++;
     hrn_predict(m);
   }

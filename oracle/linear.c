@@ -7,9 +7,11 @@
  *
  *   spaceTimePredictorLinear  2d/spaceTimePredictorLinear.cpph:35-409,
  *                             3d/spaceTimePredictorLinear.cpph:34-446
- *                             (Cauchy-Kovalevski procedure; usePointSource,
- *                             useSource and the 2D flux branch off, the
- *                             non-conservative product on)
+ *                             (Cauchy-Kovalevski procedure; useSource and
+ *                             the 2D flux branch off, the non-conservative
+ *                             product on, usePointSource for pde 4)
+ *   pointSource               2d/pointSource.cpph:30-127,
+ *                             3d/pointSource.cpph:28-143
  *   volumeIntegralLinear      2d/volumeIntegralLinear.cpph:26-50,
  *                             3d/volumeIntegralLinear.cpph:20-52
  *   surfaceIntegralLinear     2d/surfaceIntegralLinear.cpph:24-66,
@@ -72,7 +74,7 @@ static lgeo lmk(const orc_solver* s) {
 void orc_ncp(const orc_solver* s, const double* Q, const double* gradQ, double* BgradQ) {
   const int nV = orc_nvar(s);
   for (int i = 0; i < nV * s->dim; i++) BgradQ[i] = 0.0;
-  if (s->pde != 2) return;
+  if (!ORC_ELASTIC(s)) return;
   const double lam = Q[9], mu = Q[10], irho = 1.0 / Q[11];
   const double* gx = gradQ;
   const double* gy = gradQ + nV;
@@ -116,7 +118,7 @@ void orc_ncp(const orc_solver* s, const double* Q, const double* gradQ, double* 
 void orc_coefficient_matrix(const orc_solver* s, const double* Q, int d, double* Bn) {
   const int nV = orc_nvar(s);
   for (int i = 0; i < nV * nV; i++) Bn[i] = 0.0;
-  if (s->pde != 2) return;
+  if (!ORC_ELASTIC(s)) return;
   const double lam = Q[9], mu = Q[10], irho = 1.0 / Q[11];
 #define B(r, c) Bn[(r - 1) * nV + (c - 1)]
   if (d == 0) {
@@ -155,6 +157,11 @@ void orc_coefficient_matrix(const orc_solver* s, const double* Q, int d, double*
  * tempFluxUnknowns) are optional outputs. */
 void orc_lin_predictor(const orc_solver* s, const double* luh, const double* dx, double dt, double* lQhbnd,
                        double* lFhbnd, double* lduh, double* lQhi_out, double* lFhi_out) {
+  orc_lin_predictor_ps(s, luh, dx, dt, 0, lQhbnd, lFhbnd, lduh, lQhi_out, lFhi_out);
+}
+
+void orc_lin_predictor_ps(const orc_solver* s, const double* luh, const double* dx, double dt, const double* PSi,
+                          double* lQhbnd, double* lFhbnd, double* lduh, double* lQhi_out, double* lFhi_out) {
   const lgeo g = lmk(s);
   const int b = g.b, nV = g.nV, nD = g.nD, d = g.d, P = g.P, F = g.F, nz = g.nz;
   double* lQi = (double*)calloc((size_t)(b + 1) * P * nD, sizeof(double)); /* [i][p][nD] */
@@ -168,6 +175,19 @@ void orc_lin_predictor(const orc_solver* s, const double* luh, const double* dx,
   /* zeroth time derivative = initial condition (2d:60-68, 3d:58-67) */
   for (int p = 0; p < P; p++)
     for (int v = 0; v < nD; v++) QI(0, p, v) = luh[p * nD + v];
+#define PS(n, p, v) PSi[((size_t)(n) * P + (p)) * nV + (v)]
+  if (PSi) {
+    /* the time integral of the source into derivative 0 (2d:73-84, 3d:77-90),
+     * its value at t into derivative 1 (2d:88-94, 3d:93-101) */
+    for (int p = 0; p < P; p++)
+      for (int v = 0; v < nV; v++) {
+        double sum = 0.0;
+        for (int n = 1; n < b + 1; n++) sum = sum + g.w[n - 1] * PS(n, p, v);
+        QI(0, p, v) += dt * sum;
+      }
+    for (int p = 0; p < P; p++)
+      for (int v = 0; v < nV; v++) QI(1, p, v) += PS(0, p, v);
+  }
   /* Cauchy-Kovalevski (2d:126-232, 3d:123-227) */
   for (int i = 0; i < b; i++) {
     memset(gradQ, 0, sizeof(double) * P * d * nV);
@@ -216,6 +236,15 @@ void orc_lin_predictor(const orc_solver* s, const double* luh, const double* dx,
         for (int v = 0; v < nV; v++) lFh[((size_t)m * P + p) * nV + v] += dtavFac * FI(i, p, m, v);
     dtavFac *= dt / (i + 2);
   }
+  if (PSi) /* the time integral of the source, split over the directions (2d:310-324, 3d:294-308) */
+    for (int m = 0; m < d; m++)
+      for (int p = 0; p < P; p++)
+        for (int v = 0; v < nV; v++) {
+          double sum = 0.0;
+          for (int n = 1; n < b + 1; n++) sum = sum + g.w[n - 1] * PS(n, p, v);
+          lFh[((size_t)m * P + p) * nV + v] += sum / d;
+        }
+#undef PS
   /* boundary extrapolation (2d:318-405, 3d:308-440) */
   memset(lQhbnd, 0, sizeof(double) * 2 * d * F * nD);
   memset(lFhbnd, 0, sizeof(double) * 2 * d * F * nV);
@@ -365,11 +394,79 @@ void orc_lin_boundary_face(const orc_solver* s, double* FIn, const double* QIn, 
   double QOut[100 * 12], FOut[100 * 9];
   memcpy(QOut, QIn, sizeof(double) * g.F * g.nD);
   memcpy(FOut, FIn, sizeof(double) * g.F * g.nV);
-  if (kind == 1 && s->pde == 2)
+  if (kind == 1 && ORC_ELASTIC(s))
     for (int fn = 0; fn < g.F; fn++)
       for (int v = 6; v < 9; v++) QOut[fn * g.nD + v] = -QOut[fn * g.nD + v];
   if (faceIndex % 2 == 0)
     orc_lin_riemann(s, FOut, FIn, QOut, QIn, dir);
   else
     orc_lin_riemann(s, FIn, FOut, QIn, QOut, dir);
+}
+
+/* ---- point sources -------------------------------------------------------
+ * The point-source mock of pde 4 (this repository's; the reference's kernel
+ * tests define none): a Ricker wavelet of peak frequency f0 and delay t0,
+ * amplitude amp, on the three normal stresses, located at x0 whatever the
+ * node position x (UserSolverInterface::pointSource(x, t, dt, forceVector,
+ * x0), exahype/solvers/UserSolverInterface.h:75). */
+static void elastic_point_source(const orc_solver* s, const double* x, double t, double dt, double* force,
+                                 double* x0) {
+  (void)x;
+  (void)dt;
+  const double r = 3.14159265358979323846 * s->ps[4] * (t - s->ps[3]);
+  const double a = r * r;
+  const double w = s->ps[5] * ((1.0 - 2.0 * a) * exp(-a));
+  for (int v = 0; v < 9; v++) force[v] = v < 3 ? w : 0.0;
+  for (int d = 0; d < 3; d++) x0[d] = s->ps[d];
+}
+
+/* Lagrange basis polynomial i of the Gauss-Legendre nodes of order N at xi
+ * (the reference's basisFunctions[N][i], DGBasisFunctions.h:53, as the
+ * product over the other nodes) */
+static double lagrange(const double* nodes, int b, int i, double xi) {
+  double r = 1.0;
+  for (int m = 0; m < b; m++)
+    if (m != i) r *= (xi - nodes[m]) / (nodes[i] - nodes[m]);
+  return r;
+}
+
+void orc_point_source(const orc_solver* s, double t, double dt, const double* centre, const double* dx, double* PSi) {
+  const lgeo g = lmk(s);
+  const int b = g.b, nV = g.nV, P = g.P, d = g.d;
+  const double* nodes = orc_table("nodes", g.N);
+  for (int n = 0; n < b + 1; n++) {
+    const double tn = n == 0 ? t : dt * nodes[n - 1] + t;
+    for (int p = 0; p < P; p++) {
+      /* node (z, y, x) of the cell; 2D: (y, x) */
+      const int ix = p % b, iy = (p / b) % b, iz = d == 3 ? p / (b * b) : 0;
+      double x[3] = {0, 0, 0}, x0[3] = {0, 0, 0}, xr[3] = {0, 0, 0};
+      if (d == 3) x[2] = centre[2] + dx[2] * (nodes[iz] - 0.5);
+      x[1] = centre[1] + dx[1] * (nodes[iy] - 0.5);
+      x[0] = centre[0] + dx[0] * (nodes[ix] - 0.5);
+      double* out = PSi + ((size_t)n * P + p) * nV;
+      elastic_point_source(s, x, tn, dt, out, x0);
+      int inside = 1;
+      for (int e = 0; e < d; e++) {
+        const double off = centre[e] - dx[e] / 2.;
+        xr[e] = x0[e] - off;
+        xr[e] /= dx[e];
+        inside = inside && xr[e] >= 0. && xr[e] <= 1.0;
+      }
+      for (int v = 0; v < nV; v++) {
+        if (!inside) {
+          out[v] = 0.0;
+          continue;
+        }
+        double value;
+        if (d == 3) {
+          value = lagrange(nodes, b, iz, xr[2]) * lagrange(nodes, b, iy, xr[1]) * lagrange(nodes, b, ix, xr[0]) * out[v];
+          value /= ((g.w[iz]) * dx[2] * (g.w[iy]) * dx[1] * (g.w[ix]) * dx[0]);
+        } else {
+          value = lagrange(nodes, b, iy, xr[1]) * lagrange(nodes, b, ix, xr[0]) * out[v];
+          value /= ((g.w[iy]) * dx[1] * (g.w[ix]) * dx[0]);
+        }
+        out[v] = value;
+      }
+    }
+  }
 }

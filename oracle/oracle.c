@@ -29,8 +29,8 @@ const double* orc_table(const char* name, int N) {
   return 0;
 }
 
-int orc_nvar(const orc_solver* s) { return s->pde == 2 ? 9 : 5; }
-int orc_npar(const orc_solver* s) { return (s->pde == 1 || s->pde == 3) ? 1 : s->pde == 2 ? 3 : 0; }
+int orc_nvar(const orc_solver* s) { return ORC_ELASTIC(s) ? 9 : 5; }
+int orc_npar(const orc_solver* s) { return (s->pde == 1 || s->pde == 3) ? 1 : ORC_ELASTIC(s) ? 3 : 0; }
 
 /* pde 3: the kernel-test mock with an algebraic source and its
  * non-conservative product switched on (useSource = useNCP = true) */
@@ -97,7 +97,7 @@ void orc_flux(const orc_solver* s, const double* Q, double* F) {
 }
 
 void orc_eigenvalues(const orc_solver* s, const double* Q, int d, double* lambda) {
-  if (s->pde == 2) { /* elastic waves: ElasticityKernelTest2D.cpp:99-125 */
+  if (ORC_ELASTIC(s)) { /* elastic waves: ElasticityKernelTest2D.cpp:99-125 */
     const double lam = Q[9], mu = Q[10], rho0 = Q[11];
     const double cp = sqrt((lam + 2 * mu) / rho0);
     const double cs = sqrt(mu / rho0);

@@ -19,12 +19,18 @@ extern "C" {
  *          2 = linear elastic waves of the reference kernel tests (nVar = 9,
  *              nPar = 3: lambda, mu, rho; linear kernels only),
  *          3 = pde 1 with an algebraic source and the kernel tests' non-zero
- *              non-conservative product (useSource = useNCP = true). */
+ *              non-conservative product (useSource = useNCP = true),
+ *          4 = pde 2 with a point source (usePointSource = true): ps holds
+ *              its position x0[3], delay t0, peak frequency f0, amplitude. */
 typedef struct {
   int dim;   /* 2 or 3 */
   int order; /* N, basis size N+1 */
   int pde;
+  double ps[6];
 } orc_solver;
+
+/* the elastic-wave PDEs (2, 4) */
+#define ORC_ELASTIC(s) ((s)->pde == 2 || (s)->pde == 4)
 
 int orc_nvar(const orc_solver* s);
 int orc_npar(const orc_solver* s);
@@ -59,6 +65,14 @@ void orc_coefficient_matrix(const orc_solver* s, const double* Q, int d, double*
  * [b^d][nD] and lFhi [d][b^d][nV] optional. */
 void orc_lin_predictor(const orc_solver* s, const double* luh, const double* dx, double dt, double* lQhbnd,
                        double* lFhbnd, double* lduh, double* lQhi, double* lFhi);
+/* the same with point sources (usePointSource = true): PSi [b+1][b^d][nV]
+ * from orc_point_source (NULL: none) */
+void orc_lin_predictor_ps(const orc_solver* s, const double* luh, const double* dx, double dt, const double* PSi,
+                          double* lQhbnd, double* lFhbnd, double* lduh, double* lQhi, double* lFhi);
+/* pointSource (2d/pointSource.cpph:30-127, 3d/pointSource.cpph:28-143): the
+ * PDE's point source at every (time slot, node) of the cell with the given
+ * centre and widths, projected onto the cell's basis; PSi [b+1][b^d][nV] */
+void orc_point_source(const orc_solver* s, double t, double dt, const double* centre, const double* dx, double* PSi);
 void orc_lin_volume_integral(const orc_solver* s, double* lduh, const double* lFhi, const double* dx);
 void orc_lin_surface_integral(const orc_solver* s, double* lduh, const double* lFhbnd, const double* dx);
 void orc_lin_riemann(const orc_solver* s, double* FL, double* FR, const double* QL, const double* QR, int dir);

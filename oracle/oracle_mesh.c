@@ -18,7 +18,7 @@ static void be_surf(void* c, double* du, const double* fb, const double* dx) { o
 static void be_upd(void* c, double* u, const double* du, double dt) { orc_solution_update((const orc_solver*)c, u, du, dt); }
 static double be_dt(void* c, const double* u, const double* dx) { return orc_stable_dt((const orc_solver*)c, u, dx); }
 
-/* linear PDEs (pde 2): Cauchy-Kovalevski predictor, linear Riemann solver,
+/* linear PDEs (pde 2, 4): Cauchy-Kovalevski predictor, linear Riemann solver,
  * surface integral and boundary faces (outflow, rigid wall) */
 static int be_lpred(void* c, const double* luh, const double* dx, double dt, double* qb, double* fb, double* du) {
   orc_lin_predictor((const orc_solver*)c, luh, dx, dt, qb, fb, du, 0, 0);
@@ -33,6 +33,18 @@ static void be_lsurf(void* c, double* du, const double* fb, const double* dx) {
 static void be_lbnd(void* c, double* FIn, const double* QIn, int f, int kind) {
   orc_lin_boundary_face((const orc_solver*)c, FIn, QIn, f, kind);
 }
+/* point sources (pde 4): pointSource at the cell's centre, then the linear
+ * predictor with usePointSource */
+static int be_lpred_ps(void* c, const double* luh, const double* dx, const double* centre, double t, double dt,
+                       double* qb, double* fb, double* du) {
+  const orc_solver* s = (const orc_solver*)c;
+  const int b = s->order + 1, P = s->dim == 3 ? b * b * b : b * b;
+  double* PSi = (double*)malloc(sizeof(double) * (b + 1) * P * orc_nvar(s));
+  orc_point_source(s, t, dt, centre, dx, PSi);
+  orc_lin_predictor_ps(s, luh, dx, dt, PSi, qb, fb, du, 0, 0);
+  free(PSi);
+  return 0;
+}
 
 typedef struct {
   orc_solver s;
@@ -46,14 +58,19 @@ void* orc_mesh_create(int dim, int order, int pde, const int* cells, const doubl
   om->s.pde = pde;
   hrn_backend k = {&om->s, dim, order, orc_nvar(&om->s), orc_nvar(&om->s) + orc_npar(&om->s),
                    be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
-  if (pde == 2) {
+  if (ORC_ELASTIC(&om->s)) {
     k.predictor = be_lpred;
     k.riemann = be_lriem;
     k.surface_integral = be_lsurf;
     k.boundary_face_kind = be_lbnd;
+    if (pde == 4) k.predictor_at = be_lpred_ps;
   }
   om->m = hrn_create(&k, cells, size, bc, nthreads);
   return om;
+}
+/* the point source of pde 4: x0[3], t0, f0, amplitude */
+void orc_mesh_set_point_source(void* h, const double* ps) {
+  for (int i = 0; i < 6; i++) ((orc_mesh*)h)->s.ps[i] = ps[i];
 }
 void orc_mesh_destroy(void* h) { orc_mesh* om = (orc_mesh*)h; hrn_destroy(om->m); free(om); }
 static size_t nsol(hrn_mesh* m) { return (size_t)m->ncells * m->P * m->k.ndata; }

@@ -32,7 +32,18 @@ def _pi(a):
 
 
 class _Solver(ctypes.Structure):
-    _fields_ = [("dim", ctypes.c_int), ("order", ctypes.c_int), ("pde", ctypes.c_int)]
+    _fields_ = [("dim", ctypes.c_int), ("order", ctypes.c_int), ("pde", ctypes.c_int), ("ps", ctypes.c_double * 6)]
+
+
+# the point source of pde 4 (elastic waves with a Ricker-wavelet source on the
+# normal stresses): position x0[3], delay t0, peak frequency f0, amplitude
+DEFAULT_POINT_SOURCE = (0.5, 0.5, 0.5, 0.1, 8.0, 1.0)
+
+
+def _ps6(point_source):
+    ps = list(DEFAULT_POINT_SOURCE if point_source is None else point_source)
+    assert len(ps) == 6
+    return (ctypes.c_double * 6)(*[float(x) for x in ps])
 
 
 def reference_root():
@@ -123,14 +134,16 @@ class Kernels:
     """Per-cell / per-face kernels of one (dim, order, pde), either the C
     restatement (impl='oracle') or the compiled reference (impl='ref')."""
 
-    def __init__(self, dim, order, pde=0, impl="oracle"):
+    def __init__(self, dim, order, pde=0, impl="oracle", point_source=None):
+        """point_source (pde 4): x0[3], t0, f0, amplitude"""
         self.dim, self.order, self.pde, self.impl = dim, order, pde, impl
         self.b = order + 1
-        self.nvar = 9 if pde == 2 else 5
-        self.ndata = self.nvar + {1: 1, 2: 3, 3: 1}.get(pde, 0)
+        self.nvar = 9 if pde in (2, 4) else 5
+        self.ndata = self.nvar + {1: 1, 2: 3, 3: 1, 4: 3}.get(pde, 0)
         self.P = self.b ** dim
         self.F = self.b ** (dim - 1)
-        self._s = _Solver(dim, order, pde)
+        self.ps = _ps6(point_source)
+        self._s = _Solver(dim, order, pde, self.ps)
         self._l = lib() if impl == "oracle" else reflib(dim, fast=impl == "ref_fast")
         self._pre = "orc_" if impl == "oracle" else "ref%dd_" % dim
 
@@ -192,6 +205,40 @@ class Kernels:
         qb, fb = np.zeros(2 * d * F * nD), np.zeros(2 * d * F * nV)
         du, qh, fh = np.zeros(P * nV), np.zeros(P * nD), np.zeros(d * P * nV)
         self._call("lin_predictor", _p(luh), _p(dx), ctypes.c_double(dt), _p(qb), _p(fb), _p(du), _p(qh), _p(fh))
+        return dict(lQhbnd=qb, lFhbnd=fb, lduh=du, lQhi=qh, lFhi=fh)
+
+    def point_source(self, t, dt, centre, dx):
+        """pointSource of the cell with the given centre and widths:
+        PSi [b+1][b^d][nV]"""
+        c = np.ascontiguousarray(np.resize(np.asarray(centre, dtype=np.float64), 3))
+        dx = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        psi = np.zeros((self.b + 1) * self.P * self.nvar)
+        if self.impl == "oracle":
+            self._l.orc_point_source(ctypes.byref(self._s), ctypes.c_double(t), ctypes.c_double(dt), _p(c), _p(dx),
+                                     _p(psi))
+        else:
+            getattr(self._l, self._pre + "point_source")(self.order, self.ps, ctypes.c_double(t), ctypes.c_double(dt),
+                                                        _p(c), _p(dx), _p(psi))
+        return psi.reshape(self.b + 1, self.P, self.nvar)
+
+    def lin_predictor_at(self, luh, dx, dt, centre, t):
+        """the linear predictor with point sources (usePointSource): the
+        cell's pointSource at centre from t over [t, t + dt], then
+        spaceTimePredictorLinear and volumeIntegralLinear"""
+        P, F, d, nV, nD = self.P, self.F, self.dim, self.nvar, self.ndata
+        luh = np.ascontiguousarray(luh, dtype=np.float64).reshape(-1)
+        dx3 = np.ascontiguousarray(np.resize(np.asarray(dx, dtype=np.float64), 3))
+        c = np.ascontiguousarray(np.resize(np.asarray(centre, dtype=np.float64), 3))
+        qb, fb = np.zeros(2 * d * F * nD), np.zeros(2 * d * F * nV)
+        du, qh, fh = np.zeros(P * nV), np.zeros(P * nD), np.zeros(d * P * nV)
+        if self.impl == "oracle":
+            psi = np.ascontiguousarray(self.point_source(t, dt, centre, dx).reshape(-1))
+            self._l.orc_lin_predictor_ps(ctypes.byref(self._s), _p(luh), _p(dx3), ctypes.c_double(dt), _p(psi),
+                                         _p(qb), _p(fb), _p(du), _p(qh), _p(fh))
+        else:
+            getattr(self._l, self._pre + "lin_predictor_ps")(self.order, self.ps, _p(c), ctypes.c_double(t), _p(luh),
+                                                            _p(dx3), ctypes.c_double(dt), _p(qb), _p(fb), _p(du),
+                                                            _p(qh), _p(fh))
         return dict(lQhbnd=qb, lFhbnd=fb, lduh=du, lQhi=qh, lFhi=fh)
 
     def lin_riemann(self, QL, QR, direction):
@@ -282,7 +329,8 @@ class Mesh:
     restatement (impl='oracle'), the compiled reference kernels (impl='ref',
     the parity build) or their timed -O3 build (impl='ref_fast')."""
 
-    def __init__(self, dim, order, cells, size, bc, pde=0, impl="oracle", nthreads=1):
+    def __init__(self, dim, order, cells, size, bc, pde=0, impl="oracle", nthreads=1, point_source=None):
+        """point_source (pde 4): x0[3], t0, f0, amplitude"""
         self.dim, self.order, self.pde, self.impl = dim, order, pde, impl
         ci = (ctypes.c_int * 3)(*(list(cells) + [1] * (3 - len(cells))))
         sz = (ctypes.c_double * 3)(*(list(size) + [1.0] * (3 - len(size))))
@@ -305,7 +353,9 @@ class Mesh:
                        ("sweeps", ctypes.c_long), ("run_until", ctypes.c_int)):
             getattr(self._l, self._pre + nm).restype = rt
         self.ncells = int(np.prod(cells))
-        self.shape = (self.ncells, (order + 1) ** dim, {1: 6, 2: 12, 3: 6}.get(pde, 5))
+        self.shape = (self.ncells, (order + 1) ** dim, {1: 6, 2: 12, 3: 6, 4: 12}.get(pde, 5))
+        if pde == 4:
+            self._f("set_point_source")(self._h, _ps6(point_source))
 
     def _f(self, nm):
         return getattr(self._l, self._pre + nm)
@@ -376,7 +426,7 @@ class RefinedMesh:
     cells (x fastest)."""
 
     def __init__(self, dim, order, cells, size, box_lo=None, box_hi=None, pde=0, impl="oracle", boxes=None, bc=-1,
-                 level_boxes=None):
+                 level_boxes=None, point_source=None):
         """level_boxes: [(level, lo, hi)], the positions lo <= p < hi of that
         level refined once (several boxes per level refine their union);
         boxes: nested boxes, boxes[k] = (lo, hi) at level k; box_lo/box_hi:
@@ -384,10 +434,11 @@ class RefinedMesh:
         per domain face (boundaryConditions on the level-0 cells' domain
         faces, ADERDGSolver.cpp:2893-2976)."""
         self.dim, self.order, self.pde = dim, order, pde
-        self.linear = pde == 2
-        self.K = Kernels(dim, order, pde, impl)
+        self.linear = pde in (2, 4)
+        self.K = Kernels(dim, order, pde, impl, point_source=point_source)
         self.impl = impl
         self._args = (dim, order, cells, size, pde, impl, bc)
+        self._point_source = point_source
         d = dim
         cells = list(cells)[:d]
         if level_boxes is None:
@@ -431,6 +482,13 @@ class RefinedMesh:
                     self.level.append(lev)
                     n += 1
         self.ncells = n
+        # cell centres (point sources): position p at level l spans
+        # [p dx_l, (p + 1) dx_l]
+        self.centre = np.zeros((n, 3))
+        for lev in range(L):
+            for c, i in self.cid[lev].items():
+                for e in range(d):
+                    self.centre[i, e] = c[e] * self.dxl[lev][e] + 0.5 * self.dxl[lev][e]
         self.aid = [dict() for _ in range(L)]
         for lev in range(L - 1):
             for c in sorted(state[lev], key=order_key):
@@ -485,7 +543,8 @@ class RefinedMesh:
         volume restrictions (ADERDGSolver.cpp:1437-1470,1694-1735); t and the
         step count are kept, the step size recomputed, the predictor rerun"""
         dim, order, cells, size, pde, impl, bc = self._args
-        new = RefinedMesh(dim, order, cells, size, pde=pde, impl=impl, bc=bc, level_boxes=level_boxes)
+        new = RefinedMesh(dim, order, cells, size, pde=pde, impl=impl, bc=bc, level_boxes=level_boxes,
+                          point_source=self._point_source)
         K, d = self.K, self.dim
         npar = K.ndata - K.nvar
         old_pos = [None] * self.ncells
@@ -532,11 +591,16 @@ class RefinedMesh:
     def _stable(self):
         return min(self.K.stable_dt(self.u[c], self._dx(c)) for c in range(self.ncells))
 
-    def _predict(self, dt=None):
+    def _predict(self, dt=None, t=None):
+        """t: time stamp of the solution the predictor starts from (point
+        sources)"""
         K, d = self.K, self.dim
         dt = self.dt if dt is None else dt
+        t = self.t if t is None else t
         for c in range(self.ncells):
-            if self.linear:
+            if self.pde == 4:
+                o = K.lin_predictor_at(self.u[c], self._dx(c), dt, self.centre[c], t)
+            elif self.linear:
                 o = K.lin_predictor(self.u[c], self._dx(c), dt)
             else:
                 o = K.predictor(self.u[c], self._dx(c), dt)
@@ -597,7 +661,7 @@ class RefinedMesh:
     def _step_fused(self):
         self._update()
         s = self._stable()
-        self._predict(self.pdt)
+        self._predict(self.pdt, t=self.tp)
         nxt = s
         used = s if self.pdt == 0.0 else self.pdt
         unstable = used > s

@@ -31,6 +31,7 @@ template <typename T> inline T abs(T x) { return x < 0 ? -x : x; }
 #include "kernels/GaussLegendreQuadrature.h"
 #include "kernels/GaussLobattoQuadrature.h"
 #include "kernels/DGMatrices.h"
+#include "kernels/DGBasisFunctions.h"
 #include "kernels/LimiterProjectionMatrices.h"
 #include "kernels/limiter/generic/Limiter.h"
 #include "kernels/finitevolumes/riemannsolvers/c/riemannsolvers.h"
@@ -201,6 +202,18 @@ struct Elastic {
   // copies the inside state (outflow), kind 1 a rigid wall (the three
   // velocities negated); set per call through boundary_kind
   static thread_local int boundary_kind;
+  // pointSource (UserSolverInterface.h:75; this repository's mock, the
+  // kernel tests define none): a Ricker wavelet of peak frequency f0 and delay
+  // t0, amplitude amp, on the three normal stresses, at x0 whatever x; the
+  // parameters x0[3], t0, f0, amp are set per call through point_source
+  static thread_local double point_source[6];
+  void pointSource(const double* const, const double t, const double, double* forceVector, double* x0) {
+    const double r = 3.14159265358979323846 * point_source[4] * (t - point_source[3]);
+    const double a = r * r;
+    const double w = point_source[5] * ((1.0 - 2.0 * a) * std::exp(-a));
+    for (int v = 0; v < 9; v++) forceVector[v] = v < 3 ? w : 0.0;
+    for (int d = 0; d < DIMENSIONS; d++) x0[d] = point_source[d];
+  }
   void boundaryValues(const double* const, const double, const double, const int, const int,
                       const double* const fluxIn, const double* const stateIn, double* fluxOut, double* stateOut) {
     std::copy_n(stateIn, 12, stateOut);
@@ -286,6 +299,8 @@ struct Elastic {
 
 template <int N_>
 thread_local int Elastic<N_>::boundary_kind = 0;
+template <int N_>
+thread_local double Elastic<N_>::point_source[6] = {0, 0, 0, 0, 0, 0};
 
 template <int D> using Vec = tarch::la::Vector<D, double>;
 
@@ -381,6 +396,37 @@ void lin_predictor(const double* luh, const double* dxa, double dt, double* lQhb
   S s;
   kernels::aderdg::generic::c::spaceTimePredictorLinear<false, false, false, true, S>(
       s, lQhbnd, lFhbnd, stu, stf, lQh, lFh, luh, vec(dxa), dt, nullptr);
+  if (lduh) kernels::aderdg::generic::c::volumeIntegralLinear<false, false, nV, b>(lduh, lFh, vec(dxa));
+  if (lQhi_out) std::copy_n(lQh, sp * nD, lQhi_out);
+  if (lFhi_out) std::copy_n(lFh, sp * DIMENSIONS * nV, lFhi_out);
+}
+// pointSource (kernels/aderdg/generic/c/{2d,3d}/pointSource.cpph) for the
+// cell with the given centre and widths, into PSi [b+1][b^d][nV]
+template <class S>
+void point_source(const double* ps, double t, double dt, const double* centre, const double* dxa, double* PSi) {
+  S s;
+  std::copy_n(ps, 6, S::point_source);
+  kernels::aderdg::generic::c::pointSource<S>(s, t, dt, vec(centre), vec(dxa), S::NumberOfVariables,
+                                              S::NumberOfParameters, S::Order + 1, PSi);
+}
+// the same predictor with usePointSource = true, the source of the cell at
+// centre evaluated from t over [t, t + dt] (ADERDGSolver.cpp:1929-1960: the
+// glue's pointSource, then spaceTimePredictor with its forces)
+template <class S>
+void lin_predictor_ps(const double* ps, const double* centre, double t, const double* luh, const double* dxa,
+                      double dt, double* lQhbnd, double* lFhbnd, double* lduh, double* lQhi_out, double* lFhi_out) {
+  constexpr int b = S::Order + 1;
+  constexpr int nV = S::NumberOfVariables, nD = nV + S::NumberOfParameters;
+  constexpr int sp = ipow(b, DIMENSIONS);
+  constexpr int st = sp * b;
+  static thread_local double lQi[(st + sp) * nD], lFi[st * (2 * DIMENSIONS + 1) * nV], gradQ[st * DIMENSIONS * nV];
+  static thread_local double lQh[sp * nD], lFh[sp * (DIMENSIONS + 1) * nV], PSi[(b + 1) * sp * nV];
+  double* stu[2] = {lQi, nullptr};
+  double* stf[2] = {lFi, gradQ};
+  point_source<S>(ps, t, dt, centre, dxa, PSi);
+  S s;
+  kernels::aderdg::generic::c::spaceTimePredictorLinear<true, false, false, true, S>(
+      s, lQhbnd, lFhbnd, stu, stf, lQh, lFh, luh, vec(dxa), dt, PSi);
   if (lduh) kernels::aderdg::generic::c::volumeIntegralLinear<false, false, nV, b>(lduh, lFh, vec(dxa));
   if (lQhi_out) std::copy_n(lQh, sp * nD, lQhi_out);
   if (lFhi_out) std::copy_n(lFh, sp * DIMENSIONS * nV, lFhi_out);
@@ -521,7 +567,7 @@ void plot_vertices(int N, int nvar, const double* u, double* out) {
 // linear kernels: the elastic-wave PDE, or (pde 1) the Euler mock
 #define DISPATCH_LIN(pde, N, call)                                       \
   do {                                                                  \
-    if (pde == 2) {                                                     \
+    if (pde == 2 || pde == 4) {                                         \
       DISPATCH_ELASTIC(N, call);                                        \
     } else {                                                            \
       switch (N) {                                                      \
@@ -579,6 +625,7 @@ void REFNAME(init)() {
   kernels::initGaussLobattoNodesAndWeights(orders);
   kernels::initDGMatrices(orders);
   kernels::initLimiterProjectionMatrices(orders);
+  kernels::initBasisFunctions(orders);
   done = true;
 }
 
@@ -637,7 +684,7 @@ void REFNAME(surface_integral)(int pde, int N, double* lduh, const double* lFhbn
 
 void REFNAME(solution_update)(int pde, int N, double* luh, const double* lduh, double dt) {
   REFNAME(init)();
-  if (pde == 2) DISPATCH_ELASTIC(N, update<S>(luh, lduh, dt));
+  if (pde == 2 || pde == 4) DISPATCH_ELASTIC(N, update<S>(luh, lduh, dt));
   else DISPATCH(pde, N, update<S>(luh, lduh, dt));
 }
 
@@ -669,7 +716,7 @@ void REFNAME(fv_boundary)(int N, double* lim, int face) { DISPATCH_EULER(N, fv_b
 double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx) {
   REFNAME(init)();
   double r = -1;
-  if (pde == 2) DISPATCH_ELASTIC(N, r = stable_dt<S>(luh, dx));
+  if (pde == 2 || pde == 4) DISPATCH_ELASTIC(N, r = stable_dt<S>(luh, dx));
   else DISPATCH(pde, N, r = stable_dt<S>(luh, dx));
   return r;
 }
@@ -716,8 +763,19 @@ void REFNAME(lin_riemann)(int pde, int N, double* FL, double* FR, const double* 
 }
 void REFNAME(lin_boundary_face)(int pde, int N, double* FIn, const double* QIn, int faceIndex, int kind) {
   REFNAME(init)();
-  if (pde != 2) return;
+  if (pde != 2 && pde != 4) return;
   DISPATCH_ELASTIC(N, lin_boundary_face<S>(FIn, QIn, faceIndex, kind));
+}
+void REFNAME(point_source)(int N, const double* ps, double t, double dt, const double* centre, const double* dx,
+                           double* PSi) {
+  REFNAME(init)();
+  DISPATCH_ELASTIC(N, point_source<S>(ps, t, dt, centre, dx, PSi));
+}
+void REFNAME(lin_predictor_ps)(int N, const double* ps, const double* centre, double t, const double* luh,
+                               const double* dx, double dt, double* lQhbnd, double* lFhbnd, double* lduh,
+                               double* lQhi, double* lFhi) {
+  REFNAME(init)();
+  DISPATCH_ELASTIC(N, lin_predictor_ps<S>(ps, centre, t, luh, dx, dt, lQhbnd, lFhbnd, lduh, lQhi, lFhi));
 }
 void REFNAME(lin_surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx) {
   REFNAME(init)();

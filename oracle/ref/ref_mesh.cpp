@@ -1,6 +1,7 @@
 // Oracle-only: the uniform-mesh harness (oracle/harness.c) driving the
 // reference's own kernels (ref_kernels.cpp). This is the CPU baseline path:
 // the reference's generic kernels, parallel across cells on POSIX threads.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -31,6 +32,9 @@ void REFNAME(lin_riemann)(int pde, int N, double* FL, double* FR, const double* 
                           int dir);
 void REFNAME(lin_surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx);
 void REFNAME(lin_boundary_face)(int pde, int N, double* FIn, const double* QIn, int faceIndex, int kind);
+void REFNAME(lin_predictor_ps)(int N, const double* ps, const double* centre, double t, const double* luh,
+                               const double* dx, double dt, double* lQhbnd, double* lFhbnd, double* lduh,
+                               double* lQhi, double* lFhi);
 void REFNAME(init)();
 void REFNAME(project_fv)(int N, const double* luh, double* lim);
 void REFNAME(project_dg)(int N, const double* lim, double* luh);
@@ -43,7 +47,7 @@ void REFNAME(fv_boundary)(int N, double* lim, int face);
 }
 
 namespace {
-struct Ctx { int pde, N; };
+struct Ctx { int pde, N; double ps[6]; };
 int be_pred(void* c, const double* luh, const double* dx, double dt, double* qb, double* fb, double* du) {
   Ctx* x = (Ctx*)c;
   return REFNAME(predictor)(x->pde, x->N, luh, dx, dt, qb, fb, du, nullptr, nullptr, nullptr, nullptr);
@@ -61,7 +65,8 @@ void be_surf(void* c, double* du, const double* fb, const double* dx) { Ctx* x =
 void be_upd(void* c, double* u, const double* du, double dt) { Ctx* x = (Ctx*)c; REFNAME(solution_update)(x->pde, x->N, u, du, dt); }
 double be_dt(void* c, const double* u, const double* dx) { Ctx* x = (Ctx*)c; return REFNAME(stable_dt)(x->pde, x->N, u, dx); }
 // linear PDE (elastic waves): Cauchy-Kovalevski predictor, linear Riemann
-// solver and surface integral; periodic meshes only
+// solver, surface integral and boundary faces; with point sources (pde 4)
+// the predictor of each cell runs after its pointSource
 int be_lpred(void* c, const double* luh, const double* dx, double dt, double* qb, double* fb, double* du) {
   Ctx* x = (Ctx*)c;
   REFNAME(lin_predictor)(x->pde, x->N, luh, dx, dt, qb, fb, du, nullptr, nullptr);
@@ -79,6 +84,12 @@ void be_lbnd(void* c, double* FIn, const double* QIn, int f, int kind) {
   Ctx* x = (Ctx*)c;
   REFNAME(lin_boundary_face)(x->pde, x->N, FIn, QIn, f, kind);
 }
+int be_lpred_ps(void* c, const double* luh, const double* dx, const double* centre, double t, double dt, double* qb,
+                double* fb, double* du) {
+  Ctx* x = (Ctx*)c;
+  REFNAME(lin_predictor_ps)(x->N, x->ps, centre, t, luh, dx, dt, qb, fb, du, nullptr, nullptr);
+  return 0;
+}
 struct RefMesh { Ctx c; hrn_mesh* m; };
 size_t nsol(hrn_mesh* m) { return (size_t)m->ncells * m->P * m->k.ndata; }
 }
@@ -90,17 +101,19 @@ void* REFNAME(mesh_create)(int order, int pde, const int* cells, const double* s
   r->c.pde = pde;
   r->c.N = order;
   hrn_backend k = {&r->c, DIMENSIONS, order, 5, 5 + (pde == 1 || pde == 3 ? 1 : 0), be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
-  if (pde == 2) {
+  if (pde == 2 || pde == 4) {
     k.nvar = 9;
     k.ndata = 12;
     k.predictor = be_lpred;
     k.riemann = be_lriem;
     k.surface_integral = be_lsurf;
     k.boundary_face_kind = be_lbnd;
+    if (pde == 4) k.predictor_at = be_lpred_ps;
   }
   r->m = hrn_create(&k, cells, size, bc, nthreads);
   return r;
 }
+void REFNAME(mesh_set_point_source)(void* h, const double* ps) { std::copy_n(ps, 6, ((RefMesh*)h)->c.ps); }
 void REFNAME(mesh_destroy)(void* h) { RefMesh* r = (RefMesh*)h; hrn_destroy(r->m); delete r; }
 void REFNAME(mesh_set_solution)(void* h, const double* u) { hrn_mesh* m = ((RefMesh*)h)->m; memcpy(m->luh, u, nsol(m) * 8); }
 void REFNAME(mesh_get_solution)(void* h, double* u) { hrn_mesh* m = ((RefMesh*)h)->m; memcpy(u, m->luh, nsol(m) * 8); }
