@@ -737,7 +737,10 @@ def run_limiter_workload(a, world, dev, rank):
     from exahype_b200 import problems
     luh, fv, _ = problems.explosion(LIM_DIM, LIM_ORDER, LIM_CELLS, seed=SEED + rank)
     s = eb.Solver(LIM_DIM, LIM_ORDER, eb.PDE_EULER)
-    s.autotune(int(np.prod(LIM_CELLS)))
+    if a.variant is not None:
+        s.variant = a.variant
+    else:
+        s.autotune(int(np.prod(LIM_CELLS)))
     m = eb.LimitingMesh(s, LIM_CELLS, [0.0] * LIM_DIM, [1.0] * LIM_DIM, eb.BC_OUTFLOW, helper_layers=1, cure_steps=0)
     m.set_solution(luh)
     m.set_fv_initial(fv)
@@ -761,6 +764,7 @@ def run_limiter_workload(a, world, dev, rank):
     out = {"workload": LIM_WORKLOAD, "value": dof_step * n * world / (ms / 1e3), "unit": "DoF-updates/s",
            "steps": n, "ms_per_step": ms / max(n, 1), "t_end": st["t"], "irregular_steps": st["irregular_steps"],
            "picard_sweeps": st["picard_sweeps"], "final_status_counts": np.bincount(status, minlength=4).tolist(),
+           "predictor_variant": s.variant,
            "timing": "exa_lmesh_run_until(0.2): the step captured once as a CUDA graph (capture inside the "
                      "timed region), replayed 16 steps per host check of t, CUDA events"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -2272,10 +2272,10 @@ struct LimLaunch {
                                   (int)PC::SMEM));
     EXA_CUDA(cudaFuncSetAttribute(lim_seed_kernel<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)PROJ_SMEM));
-    EXA_CUDA(cudaFuncSetAttribute(lim_reinit_kernel<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)PROJ_SMEM));
-    EXA_CUDA(cudaFuncSetAttribute(lim_recompute_kernel<DIM, N, PDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)PROJ_SMEM));
+    EXA_CUDA(cudaFuncSetAttribute(lim_reinit_kernel<DIM, N, typename PC::Group>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(PROJ_SMEM * PC::CELLS)));
+    EXA_CUDA(cudaFuncSetAttribute(lim_recompute_kernel<DIM, N, PDE, typename PC::Group>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(PROJ_SMEM * PC::CELLS)));
     EXA_CUDA(cudaFuncSetAttribute(lim_project_kernel<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)PROJ_SMEM));
     done = true;
@@ -2358,7 +2358,7 @@ struct LimLaunch {
     for (int it = 0; it < lm->T; it++) {
       int rc = merge(lm, 0, gate);
       if (rc) return rc;
-      lim_spread_cells_kernel<DIM, N><<<(m->ncells + 127) / 128, 128, 0, m->stream>>>(
+      lim_spread_cells_kernel<DIM, N><<<(m->ncells + 3) / 4, 128, 0, m->stream>>>(
           m->ncells, lm->s, lm->cure, lm->fs, lm->has_lim, lm->lim, lm->lim_prev, params(lm), gate);
       EXA_LAUNCHED();
     }
@@ -2435,11 +2435,15 @@ struct LimLaunch {
     // MUSCL-Hancock (lists come out empty when run holds 0)
     EXA_CUDA(cudaMemcpyAsync(lm->luh_prev, m->luh, (size_t)n * L::P * L::nV * sizeof(double),
                              cudaMemcpyDeviceToDevice, st));
-    if ((rc = select(lm, INT_MIN, lm->A, lm->listA, lm->flags + 1, run))) return rc;
+    // both lists from the statuses before the update (the corrector does not
+    // change them); counters flags[1], flags[2]
+    EXA_CUDA(cudaMemsetAsync(lm->flags + 1, 0, 2 * sizeof(int), st));
+    lim_select2_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, lm->s, INT_MIN, lm->A, lm->listA, lm->flags + 1, lm->A,
+                                                        INT_MAX, lm->listF, lm->flags + 2, run);
+    EXA_LAUNCHED();
     if ((rc = k.corrector(m->luh, m->lduh, m->lFhbnd, m->scal + 0, nullptr, m->geo, n, lm->listA, 1, lm->flags + 1,
                           st)))
       return rc;
-    if ((rc = select(lm, lm->A, INT_MAX, lm->listF, lm->flags + 2, run))) return rc;
     if ((rc = muscl(lm, run))) return rc;
     lim_post_update_kernel<DIM, N, PDE, typename PC::Group>
         <<<(n + PC::CELLS - 1) / PC::CELLS, PC::THREADS, PC::POST_SMEM, st>>>(
@@ -2451,13 +2455,15 @@ struct LimLaunch {
     // that run skips)
     const int* g = lm->flags;
     if ((rc = spread(lm, g))) return rc;
-    lim_reinit_kernel<DIM, N><<<n, 128, PROJ_SMEM, st>>>(n, m->luh, lm->luh_prev, lm->s, lm->s_prev, lm->cure,
+    lim_reinit_kernel<DIM, N, typename PC::Group><<<(n + PC::CELLS - 1) / PC::CELLS, 128, PROJ_SMEM * PC::CELLS, st>>>(
+        n, m->luh, lm->luh_prev, lm->s, lm->s_prev, lm->cure,
                                                           lm->has_lim, lm->lim, lm->lim_prev, prm, g);
     EXA_LAUNCHED();
     if ((rc = halo(lm, g))) return rc;
     if ((rc = select(lm, lm->A, INT_MAX, lm->listF, lm->flags + 2, g))) return rc;
     if ((rc = muscl(lm, g))) return rc;
-    lim_recompute_kernel<DIM, N, PDE><<<n, 128, PROJ_SMEM, st>>>(n, m->luh, lm->luh_prev, lm->s, lm->s_prev,
+    lim_recompute_kernel<DIM, N, PDE, typename PC::Group>
+        <<<(n + PC::CELLS - 1) / PC::CELLS, 128, PROJ_SMEM * PC::CELLS, st>>>(n, m->luh, lm->luh_prev, lm->s, lm->s_prev,
                                                                   lm->lim, lm->lim_prev, m->geo, prm, m->scal + 4, g);
     EXA_LAUNCHED();
     lim_advance_kernel<<<1, 1, 0, st>>>(m->scal, lm->flags, run);

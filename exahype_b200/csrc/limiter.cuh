@@ -68,7 +68,41 @@ struct WarpGroup {
 template <int DIM, int IN, int OUT, class G = BlockGroup, class Src, class Dst>
 __device__ void tensor_map(Src src, Dst dst, const double* M, double* tmp) {
   constexpr int nV = 5;
-  if (DIM == 2) {
+  if constexpr (DIM == 2 && std::is_same<G, WarpGroup>::value) {
+    // one warp: a lane per (row, column) pair with the 5 variables unrolled,
+    // so that the index arithmetic is paid once per pair and dst sees a
+    // compile-time variable; every output is the same fma chain, in the same
+    // order, as in the generic form below
+    for (int i = G::tid(); i < IN * OUT; i += 32) {
+      const int xo = i % OUT, y = i / OUT;
+      double s[nV];
+#pragma unroll
+      for (int v = 0; v < nV; v++) s[v] = 0.0;
+#pragma unroll
+      for (int x = 0; x < IN; x++) {
+        const double m = M[x * OUT + xo];
+#pragma unroll
+        for (int v = 0; v < nV; v++) s[v] += src(0, y, x, v) * m;
+      }
+#pragma unroll
+      for (int v = 0; v < nV; v++) tmp[i * nV + v] = s[v];
+    }
+    G::sync();
+    for (int i = G::tid(); i < OUT * OUT; i += 32) {
+      const int xo = i % OUT, yo = i / OUT;
+      double s[nV];
+#pragma unroll
+      for (int v = 0; v < nV; v++) s[v] = 0.0;
+#pragma unroll
+      for (int y = 0; y < IN; y++) {
+        const double m = M[y * OUT + yo];
+#pragma unroll
+        for (int v = 0; v < nV; v++) s[v] += tmp[(y * OUT + xo) * nV + v] * m;
+      }
+#pragma unroll
+      for (int v = 0; v < nV; v++) dst(0, yo, xo, v, s[v]);
+    }
+  } else if (DIM == 2) {
     // t[y][xo][v] = sum_x src(y,x,v) M[x][xo]
     for (int i = G::tid(); i < IN * OUT * nV; i += G::size()) {
       const int v = i % nV, xo = (i / nV) % OUT, y = i / (nV * OUT);
@@ -647,6 +681,21 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
     s_prev[cell] = st;
     s_flags[0] = has_lim[cell];
   }
+  // one warp per cell: the cell's face min/max blocks, facewise statuses and
+  // cure counter are loaded now, one value per lane, so that the status
+  // machine at the end waits on no global load
+  constexpr bool kWarp = std::is_same<G, WarpGroup>::value;
+  double pmn = 0.0, pmx = 0.0;
+  int pfs = 0, pcure = 0;
+  if constexpr (kWarp) {
+    const int j = G::tid();
+    if (j < D2 * 5) {
+      pmn = minB[(size_t)cell * D2 * 5 + j];
+      pmx = maxB[(size_t)cell * D2 * 5 + j];
+    }
+    if (j < D2) pfs = fs[cell * D2 + j];
+    if (j == 0) pcure = cure[cell];
+  }
   G::sync();
   if (st > 0 && st < prm.A) {
     if (!s_flags[0])
@@ -710,7 +759,80 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
     }
     GroupReduce<G>::minmax5(fmn, fmx, red);
   }
-  if (G::tid() == 0) {
+  if constexpr (kWarp) {
+    // the same as the block form below, lane v < 5 taking variable v
+    const int lane = G::tid(), v = lane % 5;
+    double mnv = mn[0], mxv = mx[0], fmnv = 0.0, fmxv = 0.0;
+#pragma unroll
+    for (int w = 1; w < 5; w++)
+      if (w == v) {
+        mnv = mn[w];
+        mxv = mx[w];
+      }
+    if (st >= prm.A) {
+      fmnv = fmn[0];
+      fmxv = fmx[0];
+#pragma unroll
+      for (int w = 1; w < 5; w++)
+        if (w == v) {
+          fmnv = fmn[w];
+          fmxv = fmx[w];
+        }
+    }
+    // discreteMaximumPrincipleAndMinAndMaxSearch (Limiter.cpp:114-165)
+    double bmin = __shfl_sync(0xffffffffu, pmn, v), bmax = __shfl_sync(0xffffffffu, pmx, v);
+#pragma unroll
+    for (int i = 1; i < D2; i++) {
+      const double a = __shfl_sync(0xffffffffu, pmn, i * 5 + v), c = __shfl_sync(0xffffffffu, pmx, i * 5 + v);
+      bmin = (a < bmin) ? a : bmin;
+      bmax = (bmax < c) ? c : bmax;
+    }
+    double sd = (bmax - bmin) * prm.scale;
+    sd = (sd < prm.relax) ? prm.relax : sd;
+    const bool okv = !((mnv < (bmin - sd)) || (mxv > (bmax + sd)));
+    bool ok = __all_sync(0xffffffffu, lane >= 5 || okv);
+    if (ok) ok = PDE::isPhysicallyAdmissible(mn, mx);  // on the new local min/max
+    double* mnB = minB + (size_t)cell * D2 * 5;
+    double* mxB = maxB + (size_t)cell * D2 * 5;
+    if (st >= prm.A) {
+      if (lane < D2 * 5) {
+        mnB[lane] = fmnv;
+        mxB[lane] = fmxv;
+      }
+    } else if (lane < 5) {
+      mnB[v] = mnv;
+      mxB[v] = mxv;
+      mnB[v + 5] = bmin;
+      mxB[v + 5] = bmax;
+    }
+    int fm = 0;
+#pragma unroll
+    for (int i = 0; i < D2; i++) fm = max(fm, __shfl_sync(0xffffffffu, pfs, i));
+    if (lane < D2) fs[cell * D2 + lane] = 0;
+    if (lane == 0) {
+      int ns;
+      if (!ok) {
+        cure[cell] = prm.cure_steps + 1;
+        if (!(st > prm.A)) atomicOr(irregular, 1);
+        ns = prm.T;
+      } else if (st >= prm.T) {
+        ns = prm.T;
+        int c = pcure - 1;
+        if (c == 0) {
+          ns = prm.T - 1;
+          c = prm.cure_steps + 1;
+        }
+        cure[cell] = c;
+      } else {
+        ns = fm;
+      }
+      s[cell] = ns;
+      const int had = (st == 0) ? 0 : (st < prm.A ? 1 : s_flags[0]);
+      s_flags[1] = ns;
+      s_flags[2] = (ns > 0 && !had);
+      if (s_flags[2]) has_lim[cell] = 1;
+    }
+  } else if (G::tid() == 0) {
     double* mnB = minB + (size_t)cell * D2 * 5;
     double* mxB = maxB + (size_t)cell * D2 * 5;
     // discreteMaximumPrincipleAndMinAndMaxSearch (Limiter.cpp:114-165)
@@ -766,35 +888,49 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
 }
 
 // One limiter status spreading sweep, cell part (updateLimiterStatusDuringLimiterStatusSpreading,
-// :392-405); one thread per cell. The face part is lim_merge_faces_kernel(minmax = 0).
+// :392-405); one warp per cell (the status by lane 0, a newly required patch
+// zeroed by the whole warp). The face part is lim_merge_faces_kernel(minmax = 0).
 template <int DIM, int N>
 __global__ void lim_spread_cells_kernel(int ncells, int* __restrict__ s, int* __restrict__ cure,
                                         int* __restrict__ fs, int* __restrict__ has_lim, double* __restrict__ lim,
                                         double* __restrict__ lim_prev, LimParams prm, const int* __restrict__ gate) {
   using L = LimShape<DIM, N>;
   constexpr int D2 = 2 * DIM;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (c >= ncells || (gate && !*gate)) return;
-  int ns;
-  if (s[c] < prm.T) {
-    ns = 0;
-    for (int i = 0; i < D2; i++) ns = max(ns, fs[c * D2 + i]);
-  } else {
-    ns = prm.T;
-    cure[c] = prm.cure_steps + 1;
+  int alloc = 0;
+  if (lane == 0) {
+    int ns;
+    if (s[c] < prm.T) {
+      ns = 0;
+      for (int i = 0; i < D2; i++) ns = max(ns, fs[c * D2 + i]);
+    } else {
+      ns = prm.T;
+      cure[c] = prm.cure_steps + 1;
+    }
+    s[c] = ns;
+    for (int i = 0; i < D2; i++) fs[c * D2 + i] = 0;
+    alloc = ns > 0 && !has_lim[c];
+    if (alloc) has_lim[c] = 1;
   }
-  s[c] = ns;
-  for (int i = 0; i < D2; i++) fs[c * D2 + i] = 0;
-  if (ns > 0 && !has_lim[c]) {
+  if (__shfl_sync(0xffffffffu, alloc, 0)) {
     double* l = lim + (size_t)c * L::LS;
     double* lp = lim_prev + (size_t)c * L::LS;
-    for (int i = 0; i < L::LS; i++) l[i] = lp[i] = 0.0;
-    has_lim[c] = 1;
+    for (int i = lane; i < L::LS; i += 32) l[i] = lp[i] = 0.0;
   }
 }
 
-// reinitialiseSolversLocally (:1329-1360), one block per cell.
+// scratch of one cell's projections (either direction)
 template <int DIM, int N>
+constexpr int proj_tmp() {
+  using L = LimShape<DIM, N>;
+  return tensor_tmp<DIM, L::b, L::B>() > tensor_tmp<DIM, L::B, L::b>() ? tensor_tmp<DIM, L::b, L::B>()
+                                                                         : tensor_tmp<DIM, L::B, L::b>();
+}
+
+// reinitialiseSolversLocally (:1329-1360). G: one block per cell, or one
+// warp per cell with blockDim.x / 32 cells per block (2D).
+template <int DIM, int N, class G = BlockGroup>
 __global__ void __launch_bounds__(128) lim_reinit_kernel(int ncells, double* __restrict__ luh,
                                                          double* __restrict__ luh_prev, const int* __restrict__ s,
                                                          const int* __restrict__ s_prev, int* __restrict__ cure,
@@ -802,12 +938,13 @@ __global__ void __launch_bounds__(128) lim_reinit_kernel(int ncells, double* __r
                                                          double* __restrict__ lim_prev, LimParams prm,
                                                          const int* __restrict__ gate) {
   using L = LimShape<DIM, N>;
-  extern __shared__ double tmp[];
-  const int c = blockIdx.x;
+  extern __shared__ double smem[];
+  double* tmp = smem + G::index() * proj_tmp<DIM, N>();
+  const int c = blockIdx.x * (blockDim.x / G::size()) + G::index();
   if (c >= ncells || !*gate) return;
   const int st = s[c];
   if (st <= 0) {
-    if (threadIdx.x == 0) has_lim[c] = 0;
+    if (G::tid() == 0) has_lim[c] = 0;
     return;
   }
   double* u = luh + (size_t)c * L::P * L::nV;
@@ -815,37 +952,38 @@ __global__ void __launch_bounds__(128) lim_reinit_kernel(int ncells, double* __r
   double* l = lim + (size_t)c * L::LS;
   double* lp = lim_prev + (size_t)c * L::LS;
   if (s_prev[c] >= prm.A) {
-    for (int i = threadIdx.x; i < L::LS; i += blockDim.x) {
+    for (int i = G::tid(); i < L::LS; i += G::size()) {
       const double a = l[i];
       l[i] = lp[i];
       lp[i] = a;
     }
-    __syncthreads();
-    project_dg_block<DIM, N>(l, u, tmp);
+    G::sync();
+    project_dg_block<DIM, N, G>(l, u, tmp);
   } else {
-    for (int i = threadIdx.x; i < L::P * L::nV; i += blockDim.x) {
+    for (int i = G::tid(); i < L::P * L::nV; i += G::size()) {
       const double a = u[i];
       u[i] = up[i];
       up[i] = a;
     }
-    __syncthreads();
-    project_fv_block<DIM, N>(u, l, tmp);
+    G::sync();
+    project_fv_block<DIM, N, G>(u, l, tmp);
   }
-  if (threadIdx.x == 0 && st >= prm.T) cure[c] = prm.cure_steps + 1;
+  if (G::tid() == 0 && st >= prm.T) cure[c] = prm.cure_steps + 1;
 }
 
 // recomputeSolutionLocally (:1396-1436) for cells with 0 < s < A, then the
 // admissible step of every cell (the FV-active cells were re-updated by
-// lim_muscl_kernel just before). One block per cell.
-template <int DIM, int N, class PDE>
+// lim_muscl_kernel just before). G as for lim_reinit_kernel.
+template <int DIM, int N, class PDE, class G = BlockGroup>
 __global__ void __launch_bounds__(128) lim_recompute_kernel(int ncells, double* __restrict__ luh,
                                                             double* __restrict__ luh_prev, const int* __restrict__ s,
                                                             const int* __restrict__ s_prev, double* __restrict__ lim,
                                                             double* __restrict__ lim_prev, Geometry geo, LimParams prm,
                                                             double* __restrict__ dt_min, const int* __restrict__ gate) {
   using L = LimShape<DIM, N>;
-  extern __shared__ double tmp[];
-  const int c = blockIdx.x;
+  extern __shared__ double smem[];
+  double* tmp = smem + G::index() * proj_tmp<DIM, N>();
+  const int c = blockIdx.x * (blockDim.x / G::size()) + G::index();
   if (c >= ncells || !*gate) return;
   const int st = s[c];
   double* u = luh + (size_t)c * L::P * L::nV;
@@ -853,29 +991,29 @@ __global__ void __launch_bounds__(128) lim_recompute_kernel(int ncells, double* 
     double* l = lim + (size_t)c * L::LS;
     if (s_prev[c] < prm.A) {
       double* up = luh_prev + (size_t)c * L::P * L::nV;
-      for (int i = threadIdx.x; i < L::P * L::nV; i += blockDim.x) {
+      for (int i = G::tid(); i < L::P * L::nV; i += G::size()) {
         const double a = u[i];
         u[i] = up[i];
         up[i] = a;
       }
-      __syncthreads();
-      project_fv_block<DIM, N>(u, l, tmp);
+      G::sync();
+      project_fv_block<DIM, N, G>(u, l, tmp);
     } else {
       double* lp = lim_prev + (size_t)c * L::LS;
-      for (int i = threadIdx.x; i < L::LS; i += blockDim.x) {
+      for (int i = G::tid(); i < L::LS; i += G::size()) {
         const double a = l[i];
         l[i] = lp[i];
         lp[i] = a;
       }
-      __syncthreads();
-      project_dg_block<DIM, N>(l, u, tmp);
+      G::sync();
+      project_dg_block<DIM, N, G>(l, u, tmp);
     }
   }
-  __syncthreads();
+  G::sync();
   const double invDx0 = __ddiv_rn(1.0, geo.dx[0]), invDx1 = __ddiv_rn(1.0, geo.dx[1]);
   const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, geo.dx[2]) : 0.0;
   double dtm = __longlong_as_double(0x7fefffffffffffffll);
-  for (int p = threadIdx.x; p < L::P; p += blockDim.x) {
+  for (int p = G::tid(); p < L::P; p += G::size()) {
     const double* q = u + p * L::nV;
     double den = 0.0;
     den = __dadd_rn(den, __dmul_rn(Hooks<PDE, DIM>::max_abs_eig_exact(q, 0), invDx0));
@@ -889,7 +1027,8 @@ __global__ void __launch_bounds__(128) lim_recompute_kernel(int ncells, double* 
     const double x = __shfl_xor_sync(0xffffffffu, dtm, o);
     dtm = (x < dtm) ? x : dtm;
   }
-  if ((threadIdx.x & 31) == 0) atomic_min_pos_double(dt_min, dtm);
+  // warps without a node hold DBL_MAX: no atomic
+  if ((threadIdx.x & 31) == 0 && (threadIdx.x & ~31) % G::size() < L::P) atomic_min_pos_double(dt_min, dtm);
 }
 
 // Batched projections for the kernel-level entry points: one block per listed
@@ -918,6 +1057,17 @@ __global__ void lim_select_kernel(int ncells, const int* __restrict__ s, int lo,
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (gate && !*gate) return;
   if (c < ncells && s[c] >= lo && s[c] < hi) list[atomicAdd(count, 1)] = c;
+}
+// Two such lists from one pass: lo1 <= s < hi1 and lo2 <= s < hi2.
+__global__ void lim_select2_kernel(int ncells, const int* __restrict__ s, int lo1, int hi1, int* __restrict__ list1,
+                                   int* __restrict__ count1, int lo2, int hi2, int* __restrict__ list2,
+                                   int* __restrict__ count2, const int* __restrict__ gate) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gate && !*gate) return;
+  if (c >= ncells) return;
+  const int sc = s[c];
+  if (sc >= lo1 && sc < hi1) list1[atomicAdd(count1, 1)] = c;
+  if (sc >= lo2 && sc < hi2) list2[atomicAdd(count2, 1)] = c;
 }
 
 }  // namespace exa
