@@ -472,7 +472,7 @@ class LimitingMesh:
     """Uniform Cartesian mesh with the a-posteriori subcell limiter
     (LimitingADERDGSolver): DG cells, FV-limited cells with MUSCL-Hancock
     patches of (2N+1)^d subcells, limiter status spreading and local
-    recomputation, all device-resident. Euler PDE; periodic or outflow faces.
+    recomputation, all device-resident. Euler PDE; periodic, outflow or reflective faces.
 
     helper_layers, cure_steps, relax and scale are the reference's
     helper-layers, steps-till-cured, DMP relaxation parameter (delta0) and

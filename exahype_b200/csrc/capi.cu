@@ -2364,13 +2364,12 @@ struct LimLaunch {
     }
     return EXA_OK;
   }
-  static int halo(exa_lmesh* lm, const int* gate) {
+  static int halo(exa_lmesh* lm, const int* gate) {  // boundary faces: outflow, then reflective (grouped)
     exa_mesh* m = lm->m;
-    const int nb = m->nbfaces[EXA_BC_OUTFLOW], total = m->nfaces + nb;
+    const int nb0 = m->nbfaces[EXA_BC_OUTFLOW], nb = nb0 + m->nbfaces[EXA_BC_REFLECTIVE], total = m->nfaces + nb;
     if (total <= 0) return EXA_OK;
     lim_fv_halo_kernel<DIM, N><<<(total + 3) / 4, 128, 0, m->stream>>>(
-        m->fl, m->fr, m->fd, m->nfaces, m->bcell + m->boff[EXA_BC_OUTFLOW], m->bface + m->boff[EXA_BC_OUTFLOW], nb,
-        lm->s, lm->has_lim, lm->lim, lm->A, gate);
+        m->fl, m->fr, m->fd, m->nfaces, m->bcell, m->bface, nb, nb0, lm->s, lm->has_lim, lm->lim, lm->A, gate);
     EXA_LAUNCHED();
     return EXA_OK;
   }
@@ -2427,9 +2426,10 @@ struct LimLaunch {
     // read); FV halo exchange and FV boundary on FV-active faces
     if ((rc = merge(lm, 1, run))) return rc;
     if ((rc = k.riemann(m->lQhbnd, m->lFhbnd, m->fl, m->fr, m->fd, m->nfaces, run, st))) return rc;
-    if ((rc = k.boundary(m->lQhbnd, m->lFhbnd, m->bcell + m->boff[EXA_BC_OUTFLOW], m->bface + m->boff[EXA_BC_OUTFLOW],
-                         m->nbfaces[EXA_BC_OUTFLOW], EXA_BC_OUTFLOW, run, st)))
-      return rc;
+    for (int kd : {EXA_BC_OUTFLOW, EXA_BC_REFLECTIVE})
+      if ((rc = k.boundary(m->lQhbnd, m->lFhbnd, m->bcell + m->boff[kd], m->bface + m->boff[kd], m->nbfaces[kd], kd,
+                           run, st)))
+        return rc;
     if ((rc = halo(lm, run))) return rc;
     // update: DG cells (s < A) by the corrector, FV-active cells by
     // MUSCL-Hancock (lists come out empty when run holds 0)
@@ -2688,9 +2688,6 @@ int exa_lmesh_create(const exa_solver* s, const int* cells, const double* offset
   if (s->k.pde != EXA_PDE_EULER) return fail(EXA_ERR_UNSUPPORTED, "exa_lmesh_create: the limiter supports EXA_PDE_EULER");
   if (helper_layers < 1 || helper_layers > 8 || cure_steps < 0 || !(relax >= 0) || !(scale >= 0))
     return fail(EXA_ERR_ARG, "exa_lmesh_create: helper_layers 1..8, cure_steps >= 0, relax/scale >= 0");
-  for (int f = 0; f < 2 * s->k.dim; f++)
-    if (bc[f] != EXA_BC_PERIODIC && bc[f] != EXA_BC_OUTFLOW)
-      return fail(EXA_ERR_UNSUPPORTED, "exa_lmesh_create: boundary faces must be periodic or outflow");
   LimOps ops{};
   if (!find_lim_ops(s->k.dim, s->k.order, &ops))
     return fail(EXA_ERR_UNSUPPORTED, "exa_lmesh_create: no limiter kernels for this order");

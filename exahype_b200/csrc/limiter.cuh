@@ -281,7 +281,7 @@ template <int DIM, int N>
 __global__ void __launch_bounds__(128) lim_fv_halo_kernel(const int* __restrict__ fl, const int* __restrict__ fr,
                                                           const int* __restrict__ fd, int nfaces,
                                                           const int* __restrict__ bcell, const int* __restrict__ bface,
-                                                          int nb, const int* __restrict__ s,
+                                                          int nb, int nb_out, const int* __restrict__ s,
                                                           const int* __restrict__ has_lim, double* __restrict__ lim,
                                                           int A, const int* __restrict__ gate) {
   using L = LimShape<DIM, N>;
@@ -313,16 +313,23 @@ __global__ void __launch_bounds__(128) lim_fv_halo_kernel(const int* __restrict_
       l2[cell_at(d, aa, c, k) * nV + v] = l1[cell_at(d, aa, c, B + k) * nV + v];
     }
   } else {
+    // boundary faces: the first nb_out outflow, the others rigid walls
     const int bf = f - nfaces, c = bcell[bf], face = bface[bf], d = face >> 1, side = face & 1;
+    const bool wall = bf >= nb_out;
     if (!(s[c] >= A) || !has_lim[c]) return;
     double* l = lim + (size_t)c * L::LS;
     for (int i = lane; i < WORK; i += 32) {
       const int v = i % nV, k = (i / nV) % kGW, t = i / (nV * kGW);
       const int a = DIM == 3 ? t / B + kGW : 0, cc = (DIM == 3 ? t % B : t) + kGW;
-      const int K = kGW - k - 1;  // mirrored layer, outflow: stateOut = stateIn
+      // the mirrored layer is the inside state; at 3D y- and z-left faces the
+      // reference's boundaryLayerExtraction (commons.cpph:551-562, :581-592)
+      // takes the first interior layer for both ghost layers
+      const int K = kGW - k - 1;
       const int gi = side ? B + kGW + k : k;
-      const int si = side ? B + K : kGW + K;
-      l[cell_at(d, a, cc, gi) * nV + v] = l[cell_at(d, a, cc, si) * nV + v];
+      const int si = side ? B + K : kGW + ((DIM == 3 && d >= 1) ? 0 : K);
+      // PDE::fvBoundaryValues: outflow copies it, the wall negates the normal momentum
+      const double q = l[cell_at(d, a, cc, si) * nV + v];
+      l[cell_at(d, a, cc, gi) * nV + v] = (wall && v == 1 + d) ? -q : q;
     }
   }
 }

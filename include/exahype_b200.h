@@ -393,7 +393,9 @@ int exa_fv_musclhancock_update_noalloc(const exa_solver* s, double* lim, double*
  * blocks per face and, while its status is > 0, an FV patch of (2N+1)^d
  * subcells with 2 ghost layers (MUSCL-Hancock, minmod, Rusanov;
  * GenericFiniteVolumesMUSCLHancockInC). Euler PDE only (EXA_PDE_EULER);
- * boundary faces must be periodic or outflow.
+ * boundary faces periodic, outflow or reflective (the EulerADERDG
+ * demonstrator's walls: normal momentum negated in the DG boundaryValues,
+ * MyEulerSolver_ADERDG.cpp:63-87, and in the FV solver's, MyEulerSolver_FV.cpp:47-62).
  *   helper_layers h: activeFV status A = h+1, troubled status T = 2h+1
  *     (LimitingADERDGSolver.h:452-458 and the generated solver's constructor);
  *   cure_steps: iterationsToCureTroubledCell (:452-458), the specification

@@ -16,6 +16,7 @@
 #include <string.h>
 
 #include "oracle.h"
+void orc_fv_boundary_fill_kind(const orc_solver* s, double* lim, int face, int kind);
 
 #define GW 2 /* ghost layer width (GenericFiniteVolumesMUSCLHancockInC.java:12) */
 
@@ -338,10 +339,15 @@ void orc_fv_ghost_fill(const orc_solver* s, double* lim, const double* nb, int f
       }
 }
 
-/* FV boundary face, outflow: boundaryLayerExtraction + boundaryConditions
- * (stateOut = stateIn, mirrored layer order) + ghostLayerFillingAtBoundary
- * (commons.cpph:98-334, FiniteVolumesSolver.cpp:805-842). */
-void orc_fv_boundary_fill(const orc_solver* s, double* lim, int face) {
+/* FV boundary face: boundaryLayerExtraction + boundaryConditions (the inside
+ * state of the mirrored layer through the FV solver's boundaryValues) +
+ * ghostLayerFillingAtBoundary (commons.cpph:98-334, FiniteVolumesSolver.cpp:
+ * 805-842). kind 0 outflow: stateOut = stateIn; kind 1 reflective, the
+ * EulerADERDG demonstrator's MyEulerSolver_FV.cpp:47-62: the normal momentum
+ * negated. */
+void orc_fv_boundary_fill(const orc_solver* s, double* lim, int face) { orc_fv_boundary_fill_kind(s, lim, face, 0); }
+
+void orc_fv_boundary_fill_kind(const orc_solver* s, double* lim, int face, int kind) {
   const int B = 2 * s->order + 1, E = E_of(s), nV = orc_nvar(s), pB = GW, pE = GW + B;
   const int d = face / 2, side = face % 2;
   const int d3 = s->dim == 3;
@@ -350,13 +356,18 @@ void orc_fv_boundary_fill(const orc_solver* s, double* lim, int face) {
     for (int c = pB; c < pE; c++)
       for (int k = 0; k < GW; k++) {
         const int K = GW - k - 1;
-        /* left face: ghost k <- interior layer pB+K; right face: ghost pE+k <- interior pE-GW+K */
+        /* left face: ghost k <- interior layer pB+K; right face: ghost pE+k <- interior pE-GW+K.
+         * 3D y- and z-left faces: the reference's boundaryLayerExtraction
+         * (commons.cpph:551-562, :581-592) copies the first interior layer
+         * pB into both boundary layers, so both ghosts come from pB. */
         const int gi = side ? pE + k : k;
-        const int si = side ? pE - GW + K : pB + K;
+        const int si = side ? pE - GW + K : (d3 && d >= 1 ? pB : pB + K);
         int dz, dy, dx, sz, sy, sx;
         if (d == 0) { dz = a; dy = c; dx = gi; sz = a; sy = c; sx = si; }
         else if (d == 1) { dz = a; dy = gi; dx = c; sz = a; sy = si; sx = c; }
         else { dz = gi; dy = a; dx = c; sz = si; sy = a; sx = c; }
-        memcpy(lim + ((dz * E + dy) * E + dx) * nV, lim + ((sz * E + sy) * E + sx) * nV, sizeof(double) * nV);
+        double* out = lim + ((dz * E + dy) * E + dx) * nV;
+        memcpy(out, lim + ((sz * E + sy) * E + sx) * nV, sizeof(double) * nV);
+        if (kind == 1) out[1 + d] = -out[1 + d];
       }
 }

@@ -10,7 +10,8 @@
  *   (mergeNeighboursBasedOnLimiterStatus, :1560-1628); DMP min/max of the two
  *   face blocks (mergeSolutionMinMaxOnFace, :1654-1690); facewise statuses
  *   max(0, max(min(s1,T),min(s2,T)) - 1) (ADERDGSolver.cpp:2544-2560).
- *   Boundary faces: DG boundary if s < A, FV boundary otherwise.
+ *   Boundary faces: DG boundary if s < A, FV boundary otherwise (outflow or
+ *   reflective, per domain face).
  * update (per cell, LimitingADERDGSolver::updateSolution :843-908):
  *   s == 0: DG corrector; 0 < s < A: DG corrector, FV copy = projection;
  *   s >= A: MUSCL-Hancock on the FV patch, DG solution = its projection.
@@ -45,6 +46,9 @@ typedef struct {
   void (*fv_ghost)(void* ctx, double* lim, const double* nb, int face);
   void (*fv_boundary)(void* ctx, double* lim, int face);
   int fv_size; /* doubles per FV patch incl. ghosts */
+  /* optional: an FV boundary face that needs the boundary kind of its domain
+   * face (0 outflow, 1 reflective); used instead of fv_boundary when set */
+  void (*fv_boundary_kind)(void* ctx, double* lim, int face, int kind);
 } lhrn_backend;
 
 typedef struct {
@@ -279,11 +283,19 @@ static void lh_merge(lhrn* r, int recompute) {
   for (int f = 0; f < m->nb; f++) {
     const int c = m->bcell[f], face = m->bface[f];
     if (r->s[c] < r->A) {
-      if (!recompute)
-        k->boundary_face(k->ctx, m->lFhbnd + ((size_t)c * D2 + face) * F * nV,
-                         m->lQhbnd + ((size_t)c * D2 + face) * F * nD, face);
+      if (!recompute) {
+        double* FIn = m->lFhbnd + ((size_t)c * D2 + face) * F * nV;
+        const double* QIn = m->lQhbnd + ((size_t)c * D2 + face) * F * nD;
+        if (k->boundary_face_kind)
+          k->boundary_face_kind(k->ctx, FIn, QIn, face, m->bc[face]);
+        else
+          k->boundary_face(k->ctx, FIn, QIn, face);
+      }
     } else if (r->has_lim[c]) {
-      r->L.fv_boundary(k->ctx, LH_LIM(r, c), face);
+      if (r->L.fv_boundary_kind)
+        r->L.fv_boundary_kind(k->ctx, LH_LIM(r, c), face, m->bc[face]);
+      else
+        r->L.fv_boundary(k->ctx, LH_LIM(r, c), face);
     }
   }
 }

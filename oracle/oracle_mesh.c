@@ -14,6 +14,13 @@ static void be_bnd(void* c, double* FIn, const double* QIn, int f) {
   const double z[3] = {0, 0, 0};
   orc_boundary_face((const orc_solver*)c, FIn, QIn, z, z, 0.0, 0.0, f);
 }
+/* Euler (pde 0): outflow, or the demonstrator's reflective walls */
+static void be_bnd_kind(void* c, double* FIn, const double* QIn, int f, int kind) {
+  if (kind == 1)
+    orc_boundary_face_reflective((const orc_solver*)c, FIn, QIn, f);
+  else
+    be_bnd(c, FIn, QIn, f);
+}
 static void be_surf(void* c, double* du, const double* fb, const double* dx) { orc_surface_integral((const orc_solver*)c, du, fb, dx); }
 static void be_upd(void* c, double* u, const double* du, double dt) { orc_solution_update((const orc_solver*)c, u, du, dt); }
 static double be_dt(void* c, const double* u, const double* dx) { return orc_stable_dt((const orc_solver*)c, u, dx); }
@@ -58,6 +65,7 @@ void* orc_mesh_create(int dim, int order, int pde, const int* cells, const doubl
   om->s.pde = pde;
   hrn_backend k = {&om->s, dim, order, orc_nvar(&om->s), orc_nvar(&om->s) + orc_npar(&om->s),
                    be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  if (pde == 0) k.boundary_face_kind = be_bnd_kind;
   if (ORC_ELASTIC(&om->s)) {
     k.predictor = be_lpred;
     k.riemann = be_lriem;
@@ -109,6 +117,8 @@ static int lb_adm(void* c, const double* m) { return orc_admissible((const orc_s
 static void lb_fvu(void* c, double* ln, const double* lo, const double* dx, double dt) { orc_musclhancock((const orc_solver*)c, ln, lo, dx, dt); }
 static void lb_fvg(void* c, double* l, const double* nb, int f) { orc_fv_ghost_fill((const orc_solver*)c, l, nb, f); }
 static void lb_fvb(void* c, double* l, int f) { orc_fv_boundary_fill((const orc_solver*)c, l, f); }
+void orc_fv_boundary_fill_kind(const orc_solver* s, double* lim, int face, int kind);
+static void lb_fvb_kind(void* c, double* l, int f, int kind) { orc_fv_boundary_fill_kind((const orc_solver*)c, l, f, kind); }
 
 typedef struct {
   orc_solver s;
@@ -122,7 +132,9 @@ void* orc_lmesh_create(int dim, int order, const int* cells, const double* size,
   om->s.order = order;
   om->s.pde = 0;
   hrn_backend k = {&om->s, dim, order, 5, 5, be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  k.boundary_face_kind = be_bnd_kind;
   lhrn_backend L = {lb_pfv, lb_pdg, lb_lmm, lb_smm, lb_dmp, lb_adm, lb_fvu, lb_fvg, lb_fvb, orc_fv_patch_size(&om->s)};
+  L.fv_boundary_kind = lb_fvb_kind;
   om->r = lhrn_create(&k, &L, cells, size, bc, nthreads, helper_layers, cure_steps, relax, scale);
   return om;
 }

@@ -275,6 +275,18 @@ class Kernels:
         return lduh
 
     # limiter kernels of the C restatement (oracle/limiter.c); Euler only
+    def fv_boundary(self, lim, face, kind=0):
+        """FV ghost layers of a boundary face (boundaryLayerExtraction +
+        boundaryConditions + ghostLayerFillingAtBoundary; kind 0 outflow, 1
+        reflective); Euler, pde 0; returns the filled patch"""
+        lim = np.array(lim, dtype=np.float64).reshape(-1)
+        if self.impl == "oracle":
+            self._l.orc_fv_boundary_fill_kind(ctypes.byref(self._s), _p(lim), ctypes.c_int(face), ctypes.c_int(kind))
+        else:
+            getattr(self._l, self._pre + "fv_boundary_kind")(self.order, _p(lim), ctypes.c_int(face),
+                                                            ctypes.c_int(kind))
+        return lim
+
     def fv_patch_size(self):
         E = 2 * self.order + 5
         return E ** self.dim * 5
@@ -302,12 +314,19 @@ class Kernels:
 
     def boundary_face(self, FIn, QIn, face_index, centre=(0.5, 0.5, 0.5), size=(0.1, 0.1, 0.1), t=0.0, dt=0.0,
                       kind=0):
-        """kind 0: outflow values; 1: reflective walls (C restatement only)"""
+        """kind 0: outflow values; 1: reflective walls (the demonstrator's
+        boundaryValues; Euler, pde 0, for the reference's kernels)"""
         FIn = np.array(FIn, dtype=np.float64).reshape(-1)
-        if kind == 1:
+        if kind == 1 and self.impl == "oracle":
             self._l.orc_boundary_face_reflective(ctypes.byref(self._s), _p(FIn),
                                                  _p(np.ascontiguousarray(QIn, dtype=np.float64).reshape(-1)),
                                                  ctypes.c_int(face_index))
+            return FIn
+        if kind == 1:
+            assert self.pde == 0
+            getattr(self._l, self._pre + "boundary_face_kind")(
+                self.order, _p(FIn), _p(np.ascontiguousarray(QIn, dtype=np.float64).reshape(-1)),
+                ctypes.c_int(face_index), ctypes.c_int(1))
             return FIn
         c = np.ascontiguousarray(np.resize(np.asarray(centre, dtype=np.float64), 3))
         s = np.ascontiguousarray(np.resize(np.asarray(size, dtype=np.float64), 3))

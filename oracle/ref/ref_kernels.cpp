@@ -105,21 +105,37 @@ struct EulerDemo : public PDEBase<N_, 0> {
     lambda[3] = u_n;
     lambda[4] = u_n + c;
   }
-  // outflow: copy the inside state and flux (ADER-DG hook)
-  void boundaryValues(const double* const, const double, const double, const int, const int,
+  // boundaryValues of the ADER-DG and the FV solver, the kind set per call
+  // through boundary_kind: 0 outflow (the inside state and flux copied), 1
+  // the demonstrator's reflective walls (MyEulerSolver_ADERDG.cpp:63-87: the
+  // normal momentum negated and that state's normal flux; the FV solver's
+  // MyEulerSolver_FV.cpp:47-62: the normal momentum negated), restated
+  static thread_local int boundary_kind;
+  void boundaryValues(const double* const, const double, const double, const int, const int normalNonZero,
                       const double* const fluxIn, const double* const stateIn, double* fluxOut, double* stateOut) {
     std::copy_n(stateIn, 5, stateOut);
-    std::copy_n(fluxIn, 5, fluxOut);
+    if (boundary_kind == 1) {
+      stateOut[1 + normalNonZero] = -stateOut[1 + normalNonZero];
+      double F0[3][5] = {};
+      double* F[3] = {F0[0], F0[1], F0[2]};
+      flux(stateOut, F);
+      std::copy_n(F[normalNonZero], 5, fluxOut);
+    } else {
+      std::copy_n(fluxIn, 5, fluxOut);
+    }
   }
-  // outflow (FV hook)
-  void boundaryValues(const double* const, const double, const double, const int, const int,
+  void boundaryValues(const double* const, const double, const double, const int, const int normalNonZero,
                       const double* const stateIn, double* stateOut) {
     std::copy_n(stateIn, 5, stateOut);
+    if (boundary_kind == 1) stateOut[1 + normalNonZero] = -stateOut[1 + normalNonZero];
   }
   double riemannSolver(double* fL, double* fR, const double* qL, const double* qR, int normalNonZero) {
     return kernels::finitevolumes::riemannsolvers::c::rusanov<false, true, EulerDemo<N_>>(*this, fL, fR, qL, qR, normalNonZero);
   }
 };
+
+template <int N_>
+thread_local int EulerDemo<N_>::boundary_kind = 0;
 
 // The kernel-test mock PDE (2.5D in 2D; one material parameter).
 template <int N_>
@@ -712,6 +728,16 @@ double REFNAME(musclhancock)(int N, double* lnew, const double* lold, const doub
 }
 void REFNAME(fv_ghost)(int N, double* lim, const double* nb, int face) { DISPATCH_EULER(N, fv_ghost<S>(lim, nb, face)); }
 void REFNAME(fv_boundary)(int N, double* lim, int face) { DISPATCH_EULER(N, fv_boundary<S>(lim, face)); }
+// the demonstrator's Euler PDE with the boundary kind of the domain face
+// (0 outflow, 1 reflective): FV ghost layers, DG boundary face
+void REFNAME(fv_boundary_kind)(int N, double* lim, int face, int kind) {
+  DISPATCH_EULER(N, { S::boundary_kind = kind; fv_boundary<S>(lim, face); S::boundary_kind = 0; });
+}
+void REFNAME(boundary_face_kind)(int N, double* FIn, const double* QIn, int faceIndex, int kind) {
+  REFNAME(init)();
+  const double c[3] = {0.5, 0.5, 0.5}, h[3] = {0.1, 0.1, 0.1};
+  DISPATCH_EULER(N, { S::boundary_kind = kind; boundary_face<S>(FIn, QIn, c, h, 0.0, 0.0, faceIndex); S::boundary_kind = 0; });
+}
 
 double REFNAME(stable_dt)(int pde, int N, const double* luh, const double* dx) {
   REFNAME(init)();

@@ -32,6 +32,8 @@ void REFNAME(lin_riemann)(int pde, int N, double* FL, double* FR, const double* 
                           int dir);
 void REFNAME(lin_surface_integral)(int pde, int N, double* lduh, const double* lFhbnd, const double* dx);
 void REFNAME(lin_boundary_face)(int pde, int N, double* FIn, const double* QIn, int faceIndex, int kind);
+void REFNAME(boundary_face_kind)(int N, double* FIn, const double* QIn, int faceIndex, int kind);
+void REFNAME(fv_boundary_kind)(int N, double* lim, int face, int kind);
 void REFNAME(lin_predictor_ps)(int N, const double* ps, const double* centre, double t, const double* luh,
                                const double* dx, double dt, double* lQhbnd, double* lFhbnd, double* lduh,
                                double* lQhi, double* lFhi);
@@ -60,6 +62,10 @@ void be_bnd(void* c, double* FIn, const double* QIn, int f) {
   Ctx* x = (Ctx*)c;
   const double z[3] = {0, 0, 0};
   REFNAME(boundary_face)(x->pde, x->N, FIn, QIn, z, z, 0.0, 0.0, f);
+}
+// the demonstrator's Euler PDE (pde 0): outflow or reflective walls
+void be_bnd_kind(void* c, double* FIn, const double* QIn, int f, int kind) {
+  REFNAME(boundary_face_kind)(((Ctx*)c)->N, FIn, QIn, f, kind);
 }
 void be_surf(void* c, double* du, const double* fb, const double* dx) { Ctx* x = (Ctx*)c; REFNAME(surface_integral)(x->pde, x->N, du, fb, dx); }
 void be_upd(void* c, double* u, const double* du, double dt) { Ctx* x = (Ctx*)c; REFNAME(solution_update)(x->pde, x->N, u, du, dt); }
@@ -101,6 +107,7 @@ void* REFNAME(mesh_create)(int order, int pde, const int* cells, const double* s
   r->c.pde = pde;
   r->c.N = order;
   hrn_backend k = {&r->c, DIMENSIONS, order, 5, 5 + (pde == 1 || pde == 3 ? 1 : 0), be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  if (pde == 0) k.boundary_face_kind = be_bnd_kind;
   if (pde == 2 || pde == 4) {
     k.nvar = 9;
     k.ndata = 12;
@@ -139,6 +146,7 @@ int lb_adm(void* c, const double* m) { return !(m[0] <= 0.0) && !(m[4] <= 0.0); 
 void lb_fvu(void* c, double* ln, const double* lo, const double* dx, double dt) { REFNAME(musclhancock)(((Ctx*)c)->N, ln, lo, dx, dt); }
 void lb_fvg(void* c, double* l, const double* nb, int f) { REFNAME(fv_ghost)(((Ctx*)c)->N, l, nb, f); }
 void lb_fvb(void* c, double* l, int f) { REFNAME(fv_boundary)(((Ctx*)c)->N, l, f); }
+void lb_fvb_kind(void* c, double* l, int f, int kind) { REFNAME(fv_boundary_kind)(((Ctx*)c)->N, l, f, kind); }
 struct RefLMesh { Ctx c; lhrn* r; };
 }
 
@@ -152,7 +160,9 @@ void* REFNAME(lmesh_create)(int order, const int* cells, const double* size, con
   const int B = 2 * order + 1, E = B + 4;
   const int fv = (DIMENSIONS == 3 ? E * E * E : E * E) * 5;
   hrn_backend k = {&r->c, DIMENSIONS, order, 5, 5, be_pred, be_riem, be_bnd, be_surf, be_upd, be_dt};
+  k.boundary_face_kind = be_bnd_kind;
   lhrn_backend L = {lb_pfv, lb_pdg, lb_lmm, lb_smm, lb_dmp, lb_adm, lb_fvu, lb_fvg, lb_fvb, fv};
+  L.fv_boundary_kind = lb_fvb_kind;
   r->r = lhrn_create(&k, &L, cells, size, bc, nthreads, helper_layers, cure_steps, relax, scale);
   return r;
 }

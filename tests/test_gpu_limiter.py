@@ -44,10 +44,10 @@ def interior(lim, dim, order):
     return lim.reshape(n, E, E, E, 5)[:, 2:2 + B, 2:2 + B, 2:2 + B].reshape(n, -1, 5)
 
 
-def make_pair(eb, dim, order, cells, bc, helper, cure, seed, fv_ic=True, problem="explosion"):
+def make_pair(eb, dim, order, cells, bc, helper, cure, seed, fv_ic=True, problem="explosion", radius=0.2):
     from exahype_b200 import problems
     if problem == "explosion":
-        luh, fv, _ = problems.explosion(dim, order, cells, seed=seed)
+        luh, fv, _ = problems.explosion(dim, order, cells, seed=seed, radius=radius)
     else:
         luh, _ = problems.gaussian_pulse_2d(order, cells, seed=seed)
         fv = None
@@ -117,6 +117,33 @@ def test_limiting_mesh_3d_outflow(eb, order, cells, steps):
         g.step(1)
         o.step(1)
         compare(g, o, 3, order, "step %d" % (k + 1), check_lim=(k % 3 == 2))
+
+
+@pytest.mark.parametrize("dim,order,cells,bc,steps,helper,cure", [
+    (2, 5, (16, 16), 1, 40, 2, 10),  # the demonstrator's walls, helper layers and cure steps
+    (2, 3, (14, 10), [1, 1, 0, 0], 30, 1, 0),
+    (3, 3, (5, 5, 5), 1, 8, 1, 0),
+    (3, 3, (5, 5, 5), 0, 8, 1, 0),  # outflow: the 3D y-/z-left ghost layers of the reference
+])
+def test_limiting_mesh_walls_and_boundary_patches(eb, dim, order, cells, bc, steps, helper, cure):
+    """a wide explosion whose front reaches every domain face: FV patches on
+    boundary cells with reflective walls (the demonstrator's DG and FV
+    boundaryValues: normal momentum negated) or outflow"""
+    _, g, o = make_pair(eb, dim, order, cells, bc, helper, cure, seed=2, radius=0.45)
+    compare(g, o, dim, order, "init")
+    fv_on_edge = False
+    A = helper + 1
+    for k in range(steps):
+        g.step(1)
+        o.step(1)
+        st = compare(g, o, dim, order, "step %d" % (k + 1), check_lim=(k % 3 == 2))
+        grid = st.reshape(tuple(reversed(cells)))
+        for ax in range(dim):
+            for end in (0, -1):
+                idx = [slice(None)] * dim
+                idx[ax] = end
+                fv_on_edge |= bool((grid[tuple(idx)] >= A).any())
+    assert fv_on_edge
 
 
 def test_limiting_mesh_periodic_and_projection_seed(eb):

@@ -97,3 +97,82 @@ def test_fused_mesh_vs_reference(dim, N, cells, steps):
     assert sa["picard_sweeps"] == sb["picard_sweeps"] and sa["steps"] == sb["steps"] == steps
     assert fa["reruns"] == fb["reruns"] and fa["reruns"] >= 1
     assert abs(sa["t"] - sb["t"]) <= 1e-13 * sb["t"]
+
+
+@pytest.mark.parametrize("dim,N", [(2, 3), (2, 5), (3, 3), (3, 5)])
+def test_boundary_kinds_vs_reference(dim, N):
+    """boundary faces of the demonstrator's Euler PDE against the reference's
+    kernels: the FV ghost layers of every boundary face for outflow and
+    reflective walls (boundaryLayerExtraction + boundaryConditions +
+    ghostLayerFillingAtBoundary, bit for bit, the 3D y- and z-left faces
+    included, where the reference's extraction repeats the first interior
+    layer), and the DG boundary face with reflective walls (boundaryConditions
+    + riemannSolverNonlinear)"""
+    rng = np.random.default_rng(dim * 11 + N)
+    o, r = pyoracle.Kernels(dim, N, 0), pyoracle.Kernels(dim, N, 0, impl="ref")
+    E = 2 * N + 1 + 4
+    lim = rng.normal(size=E ** dim * 5)
+    for face in range(2 * dim):
+        for kind in (0, 1):
+            assert np.array_equal(o.fv_boundary(lim, face, kind), r.fv_boundary(lim, face, kind)), (face, kind)
+    F = (N + 1) ** (dim - 1)
+    Q = np.zeros((F, 5))
+    Q[:, 0] = 1 + 0.2 * rng.random(F)
+    Q[:, 1:4] = 0.3 * (rng.random((F, 3)) - 0.5)
+    Q[:, 4] = 2.5 + rng.random(F)
+    FIn = rng.normal(size=F * 5)
+    for face in range(2 * dim):
+        a, b = o.boundary_face(FIn, Q, face, kind=1), r.boundary_face(FIn, Q, face, kind=1)
+        assert np.max(np.abs(a - b)) <= 1e-14 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("dim,N,cells,bc,steps", [(2, 5, (12, 12), 1, 30), (2, 3, (14, 10), [1, 1, 0, 0], 30),
+                                                  (3, 3, (4, 4, 4), 1, 6), (3, 3, (4, 4, 4), 0, 6)])
+def test_limiting_mesh_boundaries_vs_reference(dim, N, cells, bc, steps):
+    """a wide explosion whose front reaches every domain face, with reflective
+    walls (the demonstrator's DG and FV boundaryValues) or outflow: identical
+    troubled-cell masks at every step, fields to 1e-13"""
+    u, fv, _ = problems.explosion(dim, N, cells, seed=2, radius=0.45)
+    res = []
+    for cls in (pyoracle.LimitingMesh, pyoracle.RefLimitingMesh):
+        m = cls(dim, N, cells, (1.0,) * dim, bc)
+        m.set_solution(u)
+        m.set_fv_initial(fv)
+        m.init(0.0)
+        masks = []
+        for _ in range(steps):
+            m.step(1)
+            masks.append(m.status().copy())
+        res.append((m.get_solution(), np.array(masks), m.state()))
+    (a, ma, sa), (b, mb, sb) = res
+    assert np.array_equal(ma, mb)
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-13
+    assert sa["irregular_steps"] == sb["irregular_steps"]
+    # FV-active cells on the domain boundary
+    st = ma.reshape(steps, *reversed(cells))
+    edge = np.zeros(st.shape[1:], bool)
+    for ax in range(dim):
+        idx = [slice(None)] * dim
+        idx[ax] = 0
+        edge[tuple(idx)] = True
+        idx[ax] = -1
+        edge[tuple(idx)] = True
+    assert (st[:, edge] >= 2).any()
+
+
+def test_reflective_dg_mesh_vs_reference():
+    """a pressure pulse at rest between reflective walls (DG only)"""
+    cells = (9, 9)
+    u, _ = problems.gaussian_pulse_2d(3, cells, seed=10)
+    u[..., 1:4] = 0.0
+    u[..., 4] = u[..., 0] / 0.4
+    res = []
+    for impl in ("oracle", "ref"):
+        m = pyoracle.Mesh(2, 3, cells, [1.0, 1.0], 1, impl=impl, nthreads=4)
+        m.set_solution(u)
+        m.init(0.0)
+        m.step(15)
+        res.append((m.get_solution(), m.state()))
+    (a, sa), (b, sb) = res
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-13
+    assert sa["picard_sweeps"] == sb["picard_sweeps"]
