@@ -10,7 +10,8 @@
 // flux value from shared memory). Per time slice:
 //   A  one thread per node evaluates the flux and stores it line-major,
 //      sF[d][n][L][v]: d direction, n position along d, L the line (the other
-//      coordinates in (z,y,x) order), v the variable;
+//      two coordinates, in (z,y,x) order or swapped, per direction), v the
+//      variable;
 //   B  one thread per (d, L, v) loads its line once, forms all b outputs
 //      sum_n F[n] Kxi[n][l] with the stiffness entries as compile-time-indexed
 //      constant-bank operands, scales by the line's quadrature factor and
@@ -30,6 +31,17 @@ constexpr int line_slab(int b, int dim, int lines5) {
   return dim == 3 ? (b == 6 ? 190 : b == 4 ? 84 : b == 8 ? 322 : b == 5 ? 137 : lines5 + 1)
                   : (b == 6 ? 30 : b == 4 ? 20 : b == 8 ? 42 : b == 5 ? 25 : lines5 + 1);
 }
+// 3D, b = 6, five variables: a stride and line order per direction. Phases A
+// and C access the slab node by node (the thread's node fixes n and the line
+// in every direction); with one common stride the x direction's 16-lane
+// groups hit the same bank pair up to three times (63 wavefronts per
+// direction triple and 216 nodes against 42 conflict-free). Strides 181 / 190
+// / 180 with the x direction's line index in (y, z) order give 50, phase B
+// staying conflict-free (its items are consecutive along the lines).
+constexpr int line_slab_dir(int b, int dim, int nv, int d, int fallback) {
+  return (dim == 3 && b == 6 && nv == 5) ? (d == 0 ? 181 : d == 1 ? 190 : 180) : fallback;
+}
+constexpr bool line_swap_dir(int b, int dim, int nv, int d) { return dim == 3 && b == 6 && nv == 5 && d == 0; }
 
 // MIXED: the mixed-precision form (see predictor_lines_kernel) keeps each
 // node's last FP32 update in shared memory, SD doubles per cell.
@@ -44,26 +56,43 @@ struct LinesCfg : Shape<DIM, N, PDE> {
   static constexpr int SR = S::P + 1;
   static constexpr int SD = MIXED ? (S::P * S::b * S::nV + 1) / 2 : 0;
   static constexpr int SLAB0 = S::nV == 5 ? line_slab(S::b, DIM, LINES * 5) : LINES * S::nV + 1;
+  static constexpr int SS0 = line_slab_dir(S::b, DIM, S::nV, 0, SLAB0);
+  static constexpr int SS1 = line_slab_dir(S::b, DIM, S::nV, 1, SLAB0);
+  static constexpr int SS2 = line_slab_dir(S::b, DIM, S::nV, 2, SLAB0);
+  static constexpr int SFJ0 = S::b * (SS0 + SS1 + (DIM == 3 ? SS2 : 0));
   // padded strides (bank-conflict-free) where they fit in 227 KB, packed otherwise
   static constexpr bool kPad =
-      sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + TS * DIM * S::b * SLAB0 + SR + SD)) <= 227 * 1024;
-  static constexpr int SLAB = kPad ? SLAB0 : LINES * S::nV;
+      sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + TS * SFJ0 + SR + SD)) <= 227 * 1024;
   static constexpr int QS = kPad ? S::b * S::nD + 1 : S::b * S::nD;  // lQi node stride
   static constexpr int SQ = S::P * QS;
-  static constexpr int SFJ = DIM * S::b * SLAB;  // one slice
+  // per direction d: stride along the line, first element, line order
+  static constexpr __host__ __device__ int sstride(int d) {
+    return kPad ? (d == 0 ? SS0 : d == 1 ? SS1 : SS2) : LINES * S::nV;
+  }
+  static constexpr __host__ __device__ int sbase(int d) {
+    return S::b * (d > 0 ? sstride(0) : 0) + S::b * (d > 1 ? sstride(1) : 0);
+  }
+  static constexpr __host__ __device__ bool sswap(int d) { return kPad && line_swap_dir(S::b, DIM, S::nV, d); }
+  static constexpr int SFJ = sbase(DIM - 1) + S::b * sstride(DIM - 1);  // one slice
   static constexpr int SF = TS * SFJ;
   static constexpr size_t SMEM = sizeof(double) * (size_t)(CPB * (SQ + SF + SR + SD));
   static constexpr int ITEMS = CPB * DIM * LINES * S::nV;  // phase-B work items per block
   static constexpr int IPT = (ITEMS + THREADS - 1) / THREADS;  // items per thread
 };
 
-// node p = (z, y, x) -> position n along direction d and line index L
+// node p = (z, y, x) -> position n along direction d and line index L (the
+// face-node order of the direction's faces: the other two coordinates, the
+// slower one first)
 template <int DIM, int b>
 __device__ __forceinline__ void node_line(int d, int z, int y, int x, int& n, int& L) {
   if (d == 0) { n = x; L = z * b + y; }
   else if (d == 1) { n = y; L = z * b + x; }
   else { n = z; L = y * b + x; }
 }
+// a line's face-node index <-> its index in the slab (the same, or its two
+// coordinates swapped; the map is its own inverse)
+template <int b>
+__device__ __forceinline__ int line_swapped(bool swap, int L) { return swap ? (L % b) * b + L / b : L; }
 
 // MIXED: the first sweep is the FP64 sweep above; every later sweep k works
 // on increments. Its flux increment dF = F(q^k) - F(q^k - d^k) (d^k the
@@ -82,7 +111,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
                            const int* __restrict__ count) {
   using C = LinesCfg<DIM, N, PDE, MINB, MIXED, TS>;
   static_assert(!MIXED || TS == 1, "the mixed form works one slice at a time");
-  constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, SLAB = C::SLAB, QS = C::QS;
+  constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, QS = C::QS;
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
 
@@ -125,9 +154,14 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     s_idx[lc][1] = invDx1;
     s_idx[lc][2] = invDx2;
   }
-  int nd[DIM], Ld[DIM];
+  // this node's slot in each direction's part of a slice (+ v)
+  int sa[DIM];
 #pragma unroll
-  for (int d = 0; d < DIM; d++) node_line<DIM, b>(d, z, y, x, nd[d], Ld[d]);
+  for (int d = 0; d < DIM; d++) {
+    int n, L;
+    node_line<DIM, b>(d, z, y, x, n, L);
+    sa[d] = C::sbase(d) + n * C::sstride(d) + line_swapped<b>(C::sswap(d), L) * nV;
+  }
 
   double lu[nV];
   {
@@ -149,21 +183,17 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
   __syncthreads();  // s_w
   // this thread's phase-B items (direction, line, variable): slice offset,
   // cell, and the line's quadrature factor w_a w_c dt / dx_d (times w_t later)
-  int it_off[C::IPT], it_cell[C::IPT];
+  // (their slab offsets are recomputed where used: kept in registers next to
+  // these factors they spill)
   double it_us[C::IPT];
 #pragma unroll
   for (int k = 0; k < C::IPT; k++) {
     const int it = threadIdx.x + k * C::THREADS;
-    it_off[k] = -1;
-    it_cell[k] = 0;
     it_us[k] = 0.0;
     if (it < C::ITEMS) {
-      const int v = it % nV;
-      const int L = (it / nV) % LINES;
+      const int L = (it / nV) % LINES;  // slab order; the factor is symmetric in the two coordinates
       const int d = (it / (nV * LINES)) % DIM;
       const int c = it / (nV * LINES * DIM);
-      it_off[k] = c * C::SF + d * b * SLAB + L * nV + v;
-      it_cell[k] = c;
       const int a0 = L / b, a1 = L % b;
       it_us[k] = (DIM == 3 ? s_w[a0] : 1.0) * s_w[a1] * s_dt[c] * s_idx[c][d];
     }
@@ -187,7 +217,9 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     const bool first = iter == 0;
     for (int t0 = 0; t0 < b; t0 += TS) {
       const bool reuse = first && t0 > 0;  // block-uniform
-      if (!reuse) __syncthreads();  // phase C of the previous slices is done with sF
+      // phase C of the previous slices is done with sF (at t0 = 0 the
+      // prologue's or the residual's barriers already ordered that)
+      if (!reuse && t0 > 0) __syncthreads();
       // A: fluxes of slices t0 .. t0+TS-1, line-major, slice j in buffer j
       if (reuse) {
       } else if (!done && low) {  // flux increments in FP64, stored as FP32
@@ -204,7 +236,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
         for (int d = 0; d < DIM; d++)
 #pragma unroll
           for (int v = 0; v < nV; v++)
-            sF32[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = (float)(Fl[d][v] - Fp[d][v]);
+            sF32[sa[d] + v] = (float)(Fl[d][v] - Fp[d][v]);
       } else if (!done) {
 #pragma unroll
         for (int j = 0; j < TS; j++) {
@@ -218,7 +250,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
 #pragma unroll
             for (int d = 0; d < DIM; d++)
 #pragma unroll
-              for (int v = 0; v < nV; v++) sF[j * C::SFJ + (d * b + nd[d]) * SLAB + Ld[d] * nV + v] = Fl[d][v];
+              for (int v = 0; v < nV; v++) sF[j * C::SFJ + sa[d] + v] = Fl[d][v];
           }
         }
       }
@@ -226,20 +258,26 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
       // B: line contractions, in place
 #pragma unroll
       for (int k = 0; k < C::IPT; k++) {
-        if (reuse || it_off[k] < 0 || s_done[it_cell[k]]) continue;
+        const int it = threadIdx.x + k * C::THREADS;
+        if (reuse || it >= C::ITEMS) continue;
+        const int ic = it / (nV * LINES * DIM);
+        if (s_done[ic]) continue;
+        const int id = (it / (nV * LINES)) % DIM;
+        const int is = C::sstride(id);
+        const int io = ic * C::SF + C::sbase(id) + it % (nV * LINES);
         if (low) {
           const int t = t0;
-          float* base = sFall32 + it_off[k] + it_cell[k] * C::SF;
+          float* base = sFall32 + io + ic * C::SF;
           float f[b];
 #pragma unroll
-          for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
+          for (int n = 0; n < b; n++) f[n] = base[n * is];
           const float us = (float)(T.w[t] * it_us[k]);
 #pragma unroll
           for (int l = 0; l < b; l++) {
             float s = 0.0f;
 #pragma unroll
             for (int n = 0; n < b; n++) s = fmaf(f[n], T.Kxi_f[n * b + l], s);
-            base[l * SLAB] = us * s;
+            base[l * is] = us * s;
           }
           continue;
         }
@@ -247,17 +285,17 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
         for (int j = 0; j < TS; j++) {
           const int t = t0 + j;
           if (t >= b || (first && j > 0)) break;
-          double* base = sFall + it_off[k] + j * C::SFJ;
+          double* base = sFall + io + j * C::SFJ;
           double f[b];
 #pragma unroll
-          for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
+          for (int n = 0; n < b; n++) f[n] = base[n * is];
           const double us = first ? it_us[k] : T.w[t] * it_us[k];
 #pragma unroll
           for (int l = 0; l < b; l++) {
             double s = 0.0;
 #pragma unroll
             for (int n = 0; n < b; n++) s = fma(f[n], T.Kxi[n * b + l], s);
-            base[l * SLAB] = us * s;
+            base[l * is] = us * s;
           }
         }
       }
@@ -269,7 +307,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
         for (int v = 0; v < nV; v++) {
           double rhs = 0.0;
 #pragma unroll
-          for (int d = 0; d < DIM; d++) rhs -= (double)sF32[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+          for (int d = 0; d < DIM; d++) rhs -= (double)sF32[sa[d] + v];
           const double ir = iw * rhs;
 #pragma unroll
           for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
@@ -284,7 +322,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
             for (int v = 0; v < nV; v++) {
               double sv = 0.0;
 #pragma unroll
-              for (int d = 0; d < DIM; d++) sv += sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+              for (int d = 0; d < DIM; d++) sv += sF[sa[d] + v];
               const double ir = iw * (r0 * lu[v] - wt * sv);
 #pragma unroll
               for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
@@ -301,7 +339,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
             for (int v = 0; v < nV; v++) {
               double rhs = r0 * lu[v];
 #pragma unroll
-              for (int d = 0; d < DIM; d++) rhs -= sF[j * C::SFJ + (d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+              for (int d = 0; d < DIM; d++) rhs -= sF[j * C::SFJ + sa[d] + v];
               const double ir = iw * rhs;
 #pragma unroll
               for (int l = 0; l < b; l++) qn[l][v] = fma(ir, T.iK1[l * b + t], qn[l][v]);
@@ -346,16 +384,27 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
         // time-averaged fluxes of this sweep = of the iterate before the
         // update; kept in this node's slots of the cell's slice buffer (which
         // no phase touches again once the cell is done), not in registers
-        // that would stay live across the sweeps
+        // that would stay live across the sweeps. Each slice of the new
+        // iterate replaces the old one as soon as its flux is taken, so the
+        // accumulators, the fluxes and the whole new iterate are never live
+        // together (they would spill).
         double fh[DIM][nV];
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
           for (int v = 0; v < nV; v++) fh[d][v] = 0.0;
+#pragma unroll
         for (int t = 0; t < b; t++) {
           double Q[nD];
 #pragma unroll
           for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
+#pragma unroll
+          for (int v = 0; v < nV; v++) {
+            if (low)
+              sQ[p * QS + t * nD + v] += qn[t][v];
+            else
+              sQ[p * QS + t * nD + v] = qn[t][v];
+          }
           double Fl[DIM][nV];
           PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -373,21 +422,26 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int v = 0; v < nV; v++) sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v] = fh[d][v];
+          for (int v = 0; v < nV; v++) sF[sa[d] + v] = fh[d][v];
         done = true;
+      } else {
+#pragma unroll
+        for (int l = 0; l < b; l++)
+#pragma unroll
+          for (int v = 0; v < nV; v++) {
+            if (low)
+              sQ[p * QS + l * nD + v] += qn[l][v];
+            else
+              sQ[p * QS + l * nD + v] = qn[l][v];
+          }
       }
-#pragma unroll
-      for (int l = 0; l < b; l++)
-#pragma unroll
-        for (int v = 0; v < nV; v++) {
-          if (low)
-            sQ[p * QS + l * nD + v] += qn[l][v];
-          else
-            sQ[p * QS + l * nD + v] = qn[l][v];
-        }
     }
     if (p == 0) s_done[lc] = done;
-    if (!__syncthreads_or(!done)) break;
+    if constexpr (C::CPB == 1) {  // one cell: every thread read the same sum
+      if (done) break;
+    } else if (!__syncthreads_or(!done)) {
+      break;
+    }
   }
   if (iters && active && p == 0) iters[cell] = it_done;
 
@@ -408,9 +462,9 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     const int py = DIM == 3 ? (z * b + x) * b + y : x * b + y;
     const int pz = (y * b + x) * b + z;
     for (int v = 0; v < nV; v++) {
-      fhd[(0 * P + p) * nV + v] = sF[(0 * b + nd[0]) * SLAB + Ld[0] * nV + v];
-      fhd[(1 * P + py) * nV + v] = sF[(1 * b + nd[1]) * SLAB + Ld[1] * nV + v];
-      if (DIM == 3) fhd[(2 * P + pz) * nV + v] = sF[((DIM - 1) * b + nd[DIM - 1]) * SLAB + Ld[DIM - 1] * nV + v];
+      fhd[(0 * P + p) * nV + v] = sF[sa[0] + v];
+      fhd[(1 * P + py) * nV + v] = sF[sa[1] + v];
+      if (DIM == 3) fhd[(2 * P + pz) * nV + v] = sF[sa[DIM - 1] + v];
       fhd[(DIM * P + p) * nV + v] = 0.0;
     }
   }
@@ -425,16 +479,18 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
   // (transposed stiffness, quadrature factor w_a w_c / dx), in place
   for (int it = threadIdx.x; it < C::ITEMS; it += C::THREADS) {
     const int v = it % nV;
-    const int L = (it / nV) % LINES;
+    const int Ls = (it / nV) % LINES;  // slab order
     const int d = (it / (nV * LINES)) % DIM;
     const int c = it / (nV * LINES * DIM);
     if (s_done[c]) continue;
     const int slot_c = blockIdx.x * C::CPB + c;
     const int cell_c = cell_list ? cell_list[slot_c] : slot_c;
-    double* base = sFall + c * C::SF + d * b * SLAB + L * nV + v;
+    const int is = C::sstride(d);
+    const int L = line_swapped<b>(C::sswap(d), Ls);  // face-node order
+    double* base = sFall + c * C::SF + C::sbase(d) + Ls * nV + v;
     double f[b];
 #pragma unroll
-    for (int n = 0; n < b; n++) f[n] = base[n * SLAB];
+    for (int n = 0; n < b; n++) f[n] = base[n * is];
     double sl = 0.0, sr = 0.0;
 #pragma unroll
     for (int l = 0; l < b; l++) {
@@ -450,7 +506,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
       double s = 0.0;
 #pragma unroll
       for (int m = 0; m < b; m++) s = fma(T.Kxi[k * b + m], f[m], s);
-      base[k * SLAB] = s * us;
+      base[k * is] = s * us;
     }
   }
   // extrapolated states from lQhi lines
@@ -489,7 +545,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     for (int v = 0; v < nV; v++) {
       double du = 0.0;
 #pragma unroll
-      for (int d = 0; d < DIM; d++) du += sF[(d * b + nd[d]) * SLAB + Ld[d] * nV + v];
+      for (int d = 0; d < DIM; d++) du += sF[sa[d] + v];
       sQ[p * nV + v] = du;
     }
   }
