@@ -331,7 +331,7 @@ def run_ours(a):
         # predictor shape chosen on the workload itself: one timed mesh step
         # per FP64 variant (after one untimed), before the warm-up steps
         vms = {}
-        for v in (0, 1, 2, 3, 6, 7):
+        for v in (0, 1, 2, 3, 6, 7, 8, 9):
             s.variant = v
             m.step(1)
             t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -381,7 +381,7 @@ def run_ours(a):
     # roofline of the dominant kernel (predictor + volume integral, FP64 pipe)
     ncells = int(np.prod(CELLS))
     pred_ms = ph["predictor"][0] / a.steps
-    line_form = s.variant in (1, 2, 4, 5, 6, 7)  # the line-form kernels form the first sweep once
+    line_form = s.variant in (1, 2, 4, 5, 6, 7, 8, 9)  # the line-form kernels form the first sweep once
     pflops = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells, first_sweep_once=line_form)
     pflops_ref = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells)
     fp64_peaks = measure_fp64_peak() if not a.no_fp64_probe else None
@@ -621,7 +621,10 @@ def run_refined_workload(a, world, dev, rank):
     cells, lo, hi = (27, 27, 27), (9, 9, 9), (18, 18, 18)
     u0 = problems.pulse_refined(3, 5, cells, lo, hi, seed=SEED + rank)
     s = eb.Solver(3, 5, eb.PDE_EULER)
-    s.variant = a.variant if a.variant is not None else 2
+    if a.variant is not None:
+        s.variant = a.variant
+    else:
+        s.autotune(4096)
     m = eb.Mesh.refined(s, cells, [0.0] * 3, [1.0] * 3, lo, hi)
     m.set_solution(u0)
     m.init(0.0)

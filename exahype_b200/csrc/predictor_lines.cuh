@@ -19,8 +19,18 @@
 //   C  one thread per node adds its three directional contributions to the
 //      rhs and folds the rhs into its Picard accumulators through iK1.
 // Shared memory per cell: lQi [P][b][nD], one line-major slice, residuals.
+//
+// TM (3D, one cell per block, five state variables): the Picard iterate lQi
+// lives in tensor memory instead (tmem.cuh: each thread owns one TMEM lane,
+// 60 columns of it), so that its reads and writes (phase A, the residual, the
+// update, the time average) leave the shared-memory pipe, which bounds this
+// kernel. The tensor-memory instructions are warp-collective, so the block
+// is rounded up to whole warps (216 nodes: 224 threads); the 8 threads
+// without a node take part in those instructions and in the phase-B items
+// only.
 #pragma once
 #include "aderdg.cuh"
+#include "tmem.cuh"
 
 namespace exa {
 
@@ -47,11 +57,11 @@ constexpr bool line_swap_dir(int b, int dim, int nv, int d) { return dim == 3 &&
 // node's last FP32 update in shared memory, SD doubles per cell.
 // TS: time slices per phase (each phase of a Picard sweep handles TS slices
 // between two barriers; TS slice buffers per cell).
-template <int DIM, int N, class PDE, int MINB, bool MIXED = false, int TS = 1>
+template <int DIM, int N, class PDE, int MINB, bool MIXED = false, int TS = 1, bool TM = false>
 struct LinesCfg : Shape<DIM, N, PDE> {
   using S = Shape<DIM, N, PDE>;
   static constexpr int CPB = cells_per_block<S::P>();
-  static constexpr int THREADS = CPB * S::P;
+  static constexpr int THREADS = TM ? (CPB * S::P + 31) / 32 * 32 : CPB * S::P;
   static constexpr int LINES = S::P / S::b;  // lines per direction = face nodes
   static constexpr int SR = S::P + 1;
   static constexpr int SD = MIXED ? (S::P * S::b * S::nV + 1) / 2 : 0;
@@ -64,7 +74,15 @@ struct LinesCfg : Shape<DIM, N, PDE> {
   static constexpr bool kPad =
       sizeof(double) * (size_t)(CPB * (S::P * (S::b * S::nD + 1) + TS * SFJ0 + SR + SD)) <= 227 * 1024;
   static constexpr int QS = kPad ? S::b * S::nD + 1 : S::b * S::nD;  // lQi node stride
-  static constexpr int SQ = S::P * QS;
+  // TM: 32-bit columns per thread and per CTA (the warps of a lane quadrant
+  // take consecutive column ranges)
+  static constexpr int TCOL = 64;
+  static constexpr int TCOLS = TCOL * ((THREADS / 32 + 3) / 4);
+  static_assert(!TM || (CPB == 1 && !MIXED && S::nD == 5 && 2 * S::b * S::nD <= TCOL && THREADS <= 256),
+                "tensor-memory iterate: one cell per block, five doubles per node and slice");
+  // lQi region (TM: none; the region later holds the time-averaged state and
+  // the staged volume integral of every node)
+  static constexpr int SQ = TM ? S::P * (S::nD > S::nV ? S::nD : S::nV) : S::P * QS;
   // per direction d: stride along the line, first element, line order
   static constexpr __host__ __device__ int sstride(int d) {
     return kPad ? (d == 0 ? SS0 : d == 1 ? SS1 : SS2) : LINES * S::nV;
@@ -103,14 +121,15 @@ __device__ __forceinline__ int line_swapped(bool swap, int L) { return swap ? (L
 // cancels in the difference, so FP32 only ever carries the increments, whose
 // rounding (relative 6e-8 of the update) is far below the stop test's scale.
 // The stop test and the outputs are as in the FP64 form.
-template <int DIM, int N, class PDE, bool TEMPS, int MINB, bool MIXED = false, int TS = 1>
-__global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREADS, MINB)
+template <int DIM, int N, class PDE, bool TEMPS, int MINB, bool MIXED = false, int TS = 1, bool TM = false>
+__global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::THREADS, MINB)
     predictor_lines_kernel(const double* __restrict__ luh, double* __restrict__ lQhbnd, double* __restrict__ lFhbnd,
                            double* __restrict__ lduh, int* __restrict__ iters, const double* __restrict__ dt_ptr,
                            Geometry geo, int ncells, const int* __restrict__ cell_list, PredictorTemps tmp,
                            const int* __restrict__ count) {
-  using C = LinesCfg<DIM, N, PDE, MINB, MIXED, TS>;
+  using C = LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>;
   static_assert(!MIXED || TS == 1, "the mixed form works one slice at a time");
+  static_assert(!TM || !TEMPS, "the tensor-memory form writes no temporaries");
   constexpr int b = C::b, P = C::P, nV = C::nV, nD = C::nD, LINES = C::LINES, QS = C::QS;
   extern __shared__ double smem[];
   const OrderTables& T = c_tab[N];
@@ -118,12 +137,27 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
   // a device-side count that leaves this block without cells: the whole
   // block returns before its first barrier (a gated launch costs little)
   if (count && (int)blockIdx.x * C::CPB >= min(*count, ncells)) return;
-  const int lc = threadIdx.x / P;
+  const int lc = TM ? 0 : threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
+  const bool nd_ok = !TM || p < P;  // TM: the threads past the last node hold none
+  // TM: the CTA's tensor memory (warp 0 allocates it here and frees it after
+  // the last read of the iterate)
+  const int warp = threadIdx.x >> 5;
+  constexpr bool tm = TM;
+  __shared__ uint32_t s_tbase;
+  uint32_t taddr = 0;
+  if constexpr (TM) {
+    if (warp == 0) tmem::alloc(&s_tbase, C::TCOLS);
+    tmem::fence_before_sync();
+    __syncthreads();
+    tmem::fence_after_sync();
+    taddr = s_tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(C::TCOL * (warp >> 2));
+  }
   const int slot = blockIdx.x * C::CPB + lc;
   const bool active = slot < (count ? min(*count, ncells) : ncells);  // count: optional device-side list length
   const int cell = active ? (cell_list ? cell_list[slot] : slot) : 0;
   double* sQ = smem + lc * C::SQ;
+  double* sQn = sQ + p * QS;  // this node's iterate (not TM)
   double* sF = smem + C::CPB * C::SQ + lc * C::SF;
   double* sR = smem + C::CPB * (C::SQ + C::SF) + lc * C::SR;
   double* sFall = smem + C::CPB * C::SQ;
@@ -163,18 +197,48 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     sa[d] = C::sbase(d) + n * C::sstride(d) + line_swapped<b>(C::sswap(d), L) * nV;
   }
 
+  // slice t of this node's iterate: load (nD values), store (the nV variables
+  // the iteration updates; the parameters keep their initial values)
+  auto q_ld = [&](int t, double* Q) {
+    if (tm) {
+      uint32_t r[10];
+      tmem::ld10(taddr + 10u * t, r);
+      tmem::wait_ld(r);
+      tmem::unpack5(r, Q);
+    } else {
+#pragma unroll
+      for (int v = 0; v < nD; v++) Q[v] = sQn[t * nD + v];
+    }
+  };
+  auto q_st = [&](int t, const double* Q) {
+    if (tm) {
+      uint32_t r[10];
+      tmem::pack5(Q, r);
+      tmem::st10(taddr + 10u * t, r);
+    } else {
+#pragma unroll
+      for (int v = 0; v < nV; v++) sQn[t * nD + v] = Q[v];
+    }
+  };
+
   double lu[nV];
   {
     const double* src = luh + ((size_t)cell * P + p) * nD;
     double q[nD];
 #pragma unroll
-    for (int v = 0; v < nD; v++) q[v] = active ? __ldg(src + v) : 0.0;
+    for (int v = 0; v < nD; v++) q[v] = active && nd_ok ? __ldg(src + v) : 0.0;
 #pragma unroll
     for (int v = 0; v < nV; v++) lu[v] = q[v];
 #pragma unroll
-    for (int t = 0; t < b; t++)
+    for (int t = 0; t < b; t++) {
+      if (tm) {
+        q_st(t, q);  // nD == nV
+      } else {
 #pragma unroll
-      for (int v = 0; v < nD; v++) sQ[p * QS + t * nD + v] = q[v];
+        for (int v = 0; v < nD; v++) sQn[t * nD + v] = q[v];
+      }
+    }
+    if (tm) tmem::wait_st();
   }
 
   // Which cells of the block still iterate; phase B skips converged cells.
@@ -226,7 +290,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
         const int t = t0;
         double Q[nD], Qp[nD];
 #pragma unroll
-        for (int v = 0; v < nD; v++) Q[v] = Qp[v] = sQ[p * QS + t * nD + v];
+        for (int v = 0; v < nD; v++) Q[v] = Qp[v] = sQn[t * nD + v];
 #pragma unroll
         for (int v = 0; v < nV; v++) Qp[v] -= (double)sD[(p * b + t) * nV + v];
         double Fl[DIM][nV], Fp[DIM][nV];
@@ -243,8 +307,8 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
           const int t = t0 + j;
           if (t < b && !(first && j > 0)) {
             double Q[nD];
-#pragma unroll
-            for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
+            q_ld(t, Q);
+            if (!nd_ok) continue;
             double Fl[DIM][nV];
             PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -301,7 +365,8 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
       }
       if (!reuse) __syncthreads();
       // C: rhs at this node, folded into the Picard accumulators
-      if (!done && low) {  // increment: the rhs0 term cancels
+      if (!nd_ok) {
+      } else if (!done && low) {  // increment: the rhs0 term cancels
         const int t = t0;
 #pragma unroll
         for (int v = 0; v < nV; v++) {
@@ -352,15 +417,18 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
     double part = 0.0;
     if (!done) {
 #pragma unroll
-      for (int l = 0; l < b; l++)
+      for (int l = 0; l < b; l++) {
+        double qo[nD];
+        if (!low) q_ld(l, qo);
 #pragma unroll
         for (int v = 0; v < nV; v++) {
-          const double dq = low ? qn[l][v] : qn[l][v] - sQ[p * QS + l * nD + v];
+          const double dq = low ? qn[l][v] : qn[l][v] - qo[v];
           part = fma(dq, dq, part);
           if (MIXED) sD[(p * b + l) * nV + v] = (float)dq;  // own node only: no barrier needed
         }
+      }
     }
-    sR[p] = part;
+    if (nd_ok) sR[p] = part;
     __syncthreads();
     {
       constexpr int kFullWarps = C::THREADS / 32;
@@ -396,15 +464,14 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
 #pragma unroll
         for (int t = 0; t < b; t++) {
           double Q[nD];
+          q_ld(t, Q);
+          if (low) {
 #pragma unroll
-          for (int v = 0; v < nD; v++) Q[v] = sQ[p * QS + t * nD + v];
-#pragma unroll
-          for (int v = 0; v < nV; v++) {
-            if (low)
-              sQ[p * QS + t * nD + v] += qn[t][v];
-            else
-              sQ[p * QS + t * nD + v] = qn[t][v];
+            for (int v = 0; v < nV; v++) sQn[t * nD + v] += qn[t][v];
+          } else {
+            q_st(t, qn[t]);
           }
+          if (!nd_ok) continue;
           double Fl[DIM][nV];
           PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -419,22 +486,24 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
               for (int v = 0; v < nV; v++) dst[d * nV + v] = Fl[d][v];
           }
         }
+        if (nd_ok)
 #pragma unroll
-        for (int d = 0; d < DIM; d++)
+          for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int v = 0; v < nV; v++) sF[sa[d] + v] = fh[d][v];
+            for (int v = 0; v < nV; v++) sF[sa[d] + v] = fh[d][v];
         done = true;
       } else {
 #pragma unroll
-        for (int l = 0; l < b; l++)
+        for (int l = 0; l < b; l++) {
+          if (low) {
 #pragma unroll
-          for (int v = 0; v < nV; v++) {
-            if (low)
-              sQ[p * QS + l * nD + v] += qn[l][v];
-            else
-              sQ[p * QS + l * nD + v] = qn[l][v];
+            for (int v = 0; v < nV; v++) sQn[l * nD + v] += qn[l][v];
+          } else {
+            q_st(l, qn[l]);
           }
+        }
       }
+      if (tm) tmem::wait_st();  // the next sweep (or the time average) reads them
     }
     if (p == 0) s_done[lc] = done;
     if constexpr (C::CPB == 1) {  // one cell: every thread read the same sum
@@ -448,15 +517,17 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
   // time average of lQi (lQhi)
   double qh[nD];
 #pragma unroll
-  for (int v = 0; v < nD; v++) {
-    double s = 0.0;
+  for (int v = 0; v < nD; v++) qh[v] = 0.0;
 #pragma unroll
-    for (int m = 0; m < b; m++) s += sQ[p * QS + m * nD + v] * T.w[m];
-    qh[v] = s;
+  for (int m = 0; m < b; m++) {
+    double Q[nD];
+    q_ld(m, Q);
+#pragma unroll
+    for (int v = 0; v < nD; v++) qh[v] += Q[v] * T.w[m];
   }
   if (TEMPS && active) {
     double* dq = tmp.lQi + ((size_t)cell * P + p) * b * nD;
-    for (int i = 0; i < b * nD; i++) dq[i] = sQ[p * QS + i];
+    for (int i = 0; i < b * nD; i++) dq[i] = sQn[i];
     for (int v = 0; v < nD; v++) tmp.lQhi[((size_t)cell * P + p) * nD + v] = qh[v];
     double* fhd = tmp.lFhi + (size_t)cell * (DIM + 1) * P * nV;
     const int py = DIM == 3 ? (z * b + x) * b + y : x * b + y;
@@ -468,10 +539,16 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
       fhd[(DIM * P + p) * nV + v] = 0.0;
     }
   }
+  if constexpr (TM) tmem::fence_before_sync();
   __syncthreads();
+  if constexpr (TM) {  // every warp has read its iterate (each load waited)
+    tmem::fence_after_sync();
+    if (warp == 0) tmem::dealloc(s_tbase, C::TCOLS);
+  }
   double* sQh = sQ;  // lQhi [P][nD]
 #pragma unroll
-  for (int v = 0; v < nD; v++) sQh[p * nD + v] = qh[v];
+  for (int v = 0; v < nD; v++)
+    if (nd_ok) sQh[p * nD + v] = qh[v];
   if (p == 0) s_done[lc] = !active;
   __syncthreads();
 
@@ -540,7 +617,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS>::THREAD
   // now) and written by consecutive threads to consecutive addresses: a
   // node's own nV doubles per thread would make every store instruction a
   // partial write of 32 sectors
-  if (active) {
+  if (active && nd_ok) {
 #pragma unroll
     for (int v = 0; v < nV; v++) {
       double du = 0.0;

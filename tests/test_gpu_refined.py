@@ -28,7 +28,7 @@ def eb():
 
 CASES = [(2, 3, (9, 9), (3, 3), (6, 6), 10, 0), (2, 5, (7, 8), (2, 3), (4, 5), 6, 3),
          (3, 3, (4, 4, 4), (1, 1, 1), (2, 2, 2), 4, 0), (3, 5, (5, 5, 5), (2, 2, 2), (3, 3, 3), 3, 2),
-         (3, 5, (5, 5, 5), (2, 2, 2), (3, 3, 3), 3, 0)]
+         (3, 5, (5, 5, 5), (2, 2, 2), (3, 3, 3), 3, 0), (3, 5, (5, 5, 5), (2, 2, 2), (3, 3, 3), 3, 8)]
 
 
 @pytest.mark.parametrize("dim,N,cells,lo,hi,steps,variant", CASES)
