@@ -168,7 +168,7 @@ class ClockSampler:
 
 
 PREDICTOR_SOURCES = ("exahype_b200/csrc/predictor_lines.cuh", "exahype_b200/csrc/aderdg.cuh",
-                     "exahype_b200/csrc/pde.cuh", "exahype_b200/csrc/common.cuh")
+                     "exahype_b200/csrc/pde.cuh", "exahype_b200/csrc/common.cuh", "exahype_b200/csrc/tmem.cuh")
 
 
 def predictor_source_hash():
@@ -181,14 +181,15 @@ def predictor_source_hash():
     return h.hexdigest()[:16]
 
 
-def predictor_traffic_bytes():
+def predictor_traffic_bytes(variant):
     """(dram__bytes_read.sum + dram__bytes_write.sum of one predictor launch on
     the 27^3 N=5 mesh, source note) from the committed ncu summary's lines
-    'traffic_bytes_per_launch: <n>' and 'source_sha16: <hash of the kernel
-    sources it was captured from>'. The figure is only used while the
-    sources still hash the same; otherwise (None, why)."""
+    'traffic_bytes_per_launch: <n>', 'captured_variant: <v>' and
+    'source_sha16: <hash of the kernel sources it was captured from>'. The
+    figure is only used while the sources still hash the same and the run
+    uses the captured variant; otherwise (None, why)."""
     rel = os.path.relpath(PROFILE_PREDICTOR, REPO)
-    val, sha = None, None
+    val, sha, var = None, None, None
     try:
         with open(PROFILE_PREDICTOR) as f:
             for line in f:
@@ -197,13 +198,18 @@ def predictor_traffic_bytes():
                     val = float(t.split(":", 1)[1].strip().split()[0])
                 elif t.startswith("source_sha16:"):
                     sha = t.split(":", 1)[1].strip().split()[0]
+                elif t.startswith("captured_variant:"):
+                    var = int(t.split(":", 1)[1].strip().split()[0])
     except OSError:
         return None, "no ncu summary at %s" % rel
     cur = predictor_source_hash()
     if val is None or sha != cur:
         return None, "%s was captured from other kernel sources (sha16 %s, now %s): traffic not reused" % (
             rel, sha, cur)
-    return val, "%s (ncu capture of the same kernel sources, sha16 %s)" % (rel, cur)
+    if var != variant:
+        return None, "%s was captured for predictor variant %s, this run uses %d: traffic not reused" % (
+            rel, var, variant)
+    return val, "%s (ncu capture of the same kernel sources and variant, sha16 %s)" % (rel, cur)
 
 
 def reduce_max(x, world, device=None):
@@ -331,7 +337,7 @@ def run_ours(a):
         # predictor shape chosen on the workload itself: one timed mesh step
         # per FP64 variant (after one untimed), before the warm-up steps
         vms = {}
-        for v in (0, 1, 2, 3, 6, 7, 8, 9):
+        for v in (0, 1, 2, 3, 6, 7, 8):
             s.variant = v
             m.step(1)
             t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -381,7 +387,7 @@ def run_ours(a):
     # roofline of the dominant kernel (predictor + volume integral, FP64 pipe)
     ncells = int(np.prod(CELLS))
     pred_ms = ph["predictor"][0] / a.steps
-    line_form = s.variant in (1, 2, 4, 5, 6, 7, 8, 9)  # the line-form kernels form the first sweep once
+    line_form = s.variant in (1, 2, 4, 5, 6, 7, 8)  # the line-form kernels form the first sweep once
     pflops = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells, first_sweep_once=line_form)
     pflops_ref = predictor_flops(DIM, ORDER, sweeps / a.steps, ncells)
     fp64_peaks = measure_fp64_peak() if not a.no_fp64_probe else None
@@ -400,7 +406,7 @@ def run_ours(a):
             kernels[name] = dict(bound="hbm", achieved=ach, unit="GB/s", ms=t_ms, peak=peaks["hbm_gbs"],
                                  frac=ach / peaks["hbm_gbs"])
     roof = dict(kernels["predictor"])
-    traffic, tsrc = predictor_traffic_bytes()
+    traffic, tsrc = predictor_traffic_bytes(s.variant)
     roof.update(traffic=traffic, traffic_source=tsrc,
                 peak_source="the larger of the FP64 DFMA and DMMA (mma.sync m8n8k4 f64) probes measured in this run "
                             "(%s TFLOP/s); MEASURED_PEAKS.json has no FP64 figure" % (

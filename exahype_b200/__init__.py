@@ -254,7 +254,7 @@ class Solver:
     def autotune(self, ncells=4096):
         """Times every predictor variant on `ncells` synthetic cells, keeps the
         fastest; returns (chosen, [ms per variant])."""
-        n = 10  # EXA_PREDICTOR_VARIANTS; the mixed variants 4 and 5 report -1 (not timed)
+        n = 9  # EXA_PREDICTOR_VARIANTS; the mixed variants 4 and 5 report -1 (not timed)
         ms = (ctypes.c_double * n)()
         ch = ctypes.c_int()
         _check(load().exa_solver_autotune(self._h, int(ncells), ms, ctypes.byref(ch)), "exa_solver_autotune")

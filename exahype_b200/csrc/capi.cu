@@ -225,11 +225,10 @@ static int launch_corrector(double* luh, const double* du, const double* fb, con
 //   8 line form, Picard iterate in tensor memory, two slices per phase,
 //     2 blocks/SM (3D shapes with one cell per block and five state
 //     variables; elsewhere as variant 6)
-//   9 as 8 with three time slices per phase
 // and the mixed-precision line form (FP32 increment sweeps after the first
 // FP64 sweep), selected explicitly, never by the autotuner:
 //   4 mixed line form, 1 block/SM     5 mixed line form, 2 blocks/SM
-constexpr int kAllVariants = 10;
+constexpr int kAllVariants = 9;
 constexpr bool variant_is_mixed(int v) { return v == 4 || v == 5; }
 
 template <int DIM, int N, class PDE>
@@ -274,7 +273,7 @@ struct Launch {
   static constexpr bool kMixed2 = 2 * LinesCfg<DIM, N, PDE, 2, true>::SMEM <= 227 * 1024;
   static constexpr bool kSlices2 = 2 * LinesCfg<DIM, N, PDE, 2, false, 2>::SMEM <= 227 * 1024;
   static constexpr bool kSlices1 = LinesCfg<DIM, N, PDE, 1, false, 2>::SMEM <= 227 * 1024;
-  // the tensor-memory iterate (variants 8 and 9): 3D, one cell per block,
+  // the tensor-memory iterate (variant 8): 3D, one cell per block,
   // five doubles per node and slice, whole warps of at most 256 threads
   using Sh = Shape<DIM, N, PDE>;
   static constexpr bool kTmemShape = DIM == 3 && Sh::nD == 5 && cells_per_block<Sh::P>() == 1 &&
@@ -284,7 +283,7 @@ struct Launch {
     if constexpr (kTmemShape) return 2 * LinesCfg<DIM, N, PDE, 2, false, TS, true>::SMEM <= 227 * 1024;
     else return false;
   }
-  static constexpr bool kTmem2 = tmem_fits<2>(), kTmem3 = tmem_fits<3>();
+  static constexpr bool kTmem2 = tmem_fits<2>();
 
   static int predictor(const double* luh, double* qb, double* fb, double* du, int* iters, const double* dt,
                        Geometry g, int n, const int* list, const int* cnt, PredictorTemps tmp, bool temps,
@@ -310,11 +309,9 @@ struct Launch {
       rc = launch_lines<false, kMixed2 ? 2 : 1, true>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else if (variant == 8 && kTmem2)
       rc = launch_lines<false, 2, false, 2, kTmem2>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
-    else if (variant == 9 && kTmem3)
-      rc = launch_lines<false, 2, false, 3, kTmem3>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
-    else if ((variant == 6 || variant == 8 || variant == 9) && kSlices2)
+    else if ((variant == 6 || variant == 8) && kSlices2)
       rc = launch_lines<false, 2, false, kSlices2 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
-    else if (variant == 6 || variant == 7 || variant == 8 || variant == 9)
+    else if (variant == 6 || variant == 7 || variant == 8)
       rc = launch_lines<false, 1, false, kSlices1 ? 2 : 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);
     else
       rc = launch_pred<false, 1, 1>(luh, qb, fb, du, iters, dt, g, n, list, cnt, tmp, st);

@@ -60,6 +60,6 @@ def test_mixed_vs_fp64_oracle(eb, dim, order, cells, steps, variant):
 def test_mixed_variants_are_selectable_not_autotuned(eb):
     s = eb.Solver(3, 5)
     chosen, ms = s.autotune(256)
-    assert chosen in (0, 1, 2, 3, 6, 7, 8, 9) and len(ms) == 10 and ms[4] == ms[5] == -1.0
+    assert chosen in (0, 1, 2, 3, 6, 7, 8) and len(ms) == 9 and ms[4] == ms[5] == -1.0
     s.variant = eb.PREDICTOR_MIXED_2
     assert s.variant == 5
