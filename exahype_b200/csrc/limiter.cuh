@@ -61,6 +61,35 @@ struct WarpGroup {
   __device__ static void sync() { __syncwarp(); }
 };
 
+// Exchanges the contents of a[0..n) and b[0..n) (the reference swaps a
+// patch's solution and previous-solution pointers; here both live in dense
+// per-cell arrays). Each thread issues the loads of eight elements of both
+// arrays before any store, so that a group of one warp waits on a few
+// memory round trips, not one per 32 elements.
+template <class G>
+__device__ __forceinline__ void swap_group(double* __restrict__ a, double* __restrict__ b, int n) {
+  constexpr int K = 8;
+  for (int i0 = G::tid(); i0 < n; i0 += K * G::size()) {
+    double x[K], y[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int i = i0 + k * G::size();
+      if (i < n) {
+        x[k] = a[i];
+        y[k] = b[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int i = i0 + k * G::size();
+      if (i < n) {
+        a[i] = y[k];
+        b[i] = x[k];
+      }
+    }
+  }
+}
+
 // Separable tensor-product maps for one cell, executed by one thread group.
 // out[o1..][v] = sum_in src[in..][v] prod_d M[in_d][o_d], M row-major [IN][OUT].
 // Summation is per axis (x, then y, then z) rather than the reference's single
@@ -708,11 +737,7 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
     if (!s_flags[0])
       for (int i = G::tid(); i < L::LS; i += G::size()) l[i] = lp[i] = 0.0;
     G::sync();
-    for (int i = G::tid(); i < L::LS; i += G::size()) {
-      const double a = l[i];
-      l[i] = lp[i];
-      lp[i] = a;
-    }
+    swap_group<G>(l, lp, L::LS);
     G::sync();
     project_fv_block<DIM, N, G>(u, l, tmp, g_lim_tab[N].uh2lim);
     if (G::tid() == 0) has_lim[cell] = 1;
@@ -959,19 +984,11 @@ __global__ void __launch_bounds__(128) lim_reinit_kernel(int ncells, double* __r
   double* l = lim + (size_t)c * L::LS;
   double* lp = lim_prev + (size_t)c * L::LS;
   if (s_prev[c] >= prm.A) {
-    for (int i = G::tid(); i < L::LS; i += G::size()) {
-      const double a = l[i];
-      l[i] = lp[i];
-      lp[i] = a;
-    }
+    swap_group<G>(l, lp, L::LS);
     G::sync();
     project_dg_block<DIM, N, G>(l, u, tmp);
   } else {
-    for (int i = G::tid(); i < L::P * L::nV; i += G::size()) {
-      const double a = u[i];
-      u[i] = up[i];
-      up[i] = a;
-    }
+    swap_group<G>(u, up, L::P * L::nV);
     G::sync();
     project_fv_block<DIM, N, G>(u, l, tmp);
   }
@@ -998,20 +1015,12 @@ __global__ void __launch_bounds__(128) lim_recompute_kernel(int ncells, double* 
     double* l = lim + (size_t)c * L::LS;
     if (s_prev[c] < prm.A) {
       double* up = luh_prev + (size_t)c * L::P * L::nV;
-      for (int i = G::tid(); i < L::P * L::nV; i += G::size()) {
-        const double a = u[i];
-        u[i] = up[i];
-        up[i] = a;
-      }
+      swap_group<G>(u, up, L::P * L::nV);
       G::sync();
       project_fv_block<DIM, N, G>(u, l, tmp);
     } else {
       double* lp = lim_prev + (size_t)c * L::LS;
-      for (int i = G::tid(); i < L::LS; i += G::size()) {
-        const double a = l[i];
-        l[i] = lp[i];
-        lp[i] = a;
-      }
+      swap_group<G>(l, lp, L::LS);
       G::sync();
       project_dg_block<DIM, N, G>(l, u, tmp);
     }
