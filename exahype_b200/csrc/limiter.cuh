@@ -61,6 +61,26 @@ struct WarpGroup {
   __device__ static void sync() { __syncwarp(); }
 };
 
+// Copies src[0..n) to dst[0..n), eight loads per thread in flight before the
+// stores (dst may be shared memory).
+template <class G>
+__device__ __forceinline__ void copy_group(double* __restrict__ dst, const double* __restrict__ src, int n) {
+  constexpr int K = 8;
+  for (int i0 = G::tid(); i0 < n; i0 += K * G::size()) {
+    double x[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int i = i0 + k * G::size();
+      if (i < n) x[k] = src[i];
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int i = i0 + k * G::size();
+      if (i < n) dst[i] = x[k];
+    }
+  }
+}
+
 // Exchanges the contents of a[0..n) and b[0..n) (the reference swaps a
 // patch's solution and previous-solution pointers; here both live in dense
 // per-cell arrays). Each thread issues the loads of eight elements of both
@@ -747,9 +767,9 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
   const double invDx0 = __ddiv_rn(1.0, geo.dx[0]), invDx1 = __ddiv_rn(1.0, geo.dx[1]);
   const double invDx2 = DIM == 3 ? __ddiv_rn(1.0, geo.dx[2]) : 0.0;
   // stage the (final) DG solution and the projection tables of this order
-  for (int i = G::tid(); i < L::P * nV; i += G::size()) su[i] = u[i];
-  for (int i = G::tid(); i < L::b * L::b; i += G::size()) slob[i] = g_lim_tab[N].uh2lob[i];
-  for (int i = G::tid(); i < L::b * L::B; i += G::size()) slim[i] = g_lim_tab[N].uh2lim[i];
+  copy_group<G>(su, u, L::P * nV);
+  copy_group<G>(slob, g_lim_tab[N].uh2lob, L::b * L::b);
+  copy_group<G>(slim, g_lim_tab[N].uh2lim, L::b * L::B);
   G::sync();
   double dtm = __longlong_as_double(0x7fefffffffffffffll);
   for (int p = G::tid(); p < L::P; p += G::size()) {
@@ -780,6 +800,7 @@ __global__ void __launch_bounds__(128) lim_post_update_kernel(
       fmn[v] = __longlong_as_double(0x7fefffffffffffffll);
       fmx[v] = -fmn[v];
     }
+#pragma unroll 4
     for (int i = G::tid(); i < L::PB; i += G::size()) {
       const int x = i % L::B, y = (i / L::B) % L::B, z = DIM == 3 ? i / (L::B * L::B) : 0;
       const double* q = l + lim_index<DIM, N>(z, y, x) * nV;
