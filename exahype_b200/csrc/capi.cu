@@ -111,6 +111,14 @@ static int upload_tables() {
       t.Kxi_f[i] = (float)t.Kxi[i];
       l.uh2lob[i] = exa_tab_uh2lob[exa_tab_uh2lob_off[N] + i];
     }
+    if (b % 2 == 0) {
+      const int hh = b / 2;
+      for (int n = 0; n < hh; n++)
+        for (int m = 0; m < hh; m++) {
+          t.KxiP[n * hh + m] = 0.5 * (t.Kxi[n * b + m] + t.Kxi[(b - 1 - n) * b + m]);
+          t.KxiQ[n * hh + m] = 0.5 * (t.Kxi[n * b + m] - t.Kxi[(b - 1 - n) * b + m]);
+        }
+    }
     for (int i = 0; i < b * bl; i++) {
       l.uh2lim[i] = exa_tab_uh2lim[exa_tab_uh2lim_off[N] + i];
       l.lim2uh[i] = exa_tab_lim2uh[exa_tab_lim2uh_off[N] + i];

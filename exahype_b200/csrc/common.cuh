@@ -22,6 +22,14 @@ struct OrderTables {
   double lobatto[kMaxB];
   // FP32 copy of Kxi for the mixed-precision Picard sweeps
   float Kxi_f[kMaxB * kMaxB];
+  // even b: Kxi is centro-antisymmetric (Kxi[b-1-n][b-1-l] = -Kxi[n][l], the
+  // Gauss-Legendre nodes being symmetric), so a line contraction
+  // out_l = sum_n f_n Kxi[n][l] splits into the even and odd parts of f:
+  // with h = b/2, fp_n = f_n + f_(b-1-n), fm_n = f_n - f_(b-1-n) (n < h),
+  // A_l = sum_n fp_n KxiP[n][l], B_l = sum_n fm_n KxiQ[n][l] (l < h):
+  // out_l = B_l + A_l, out_(b-1-l) = B_l - A_l, where
+  // KxiP[n][l] = (Kxi[n][l] + Kxi[b-1-n][l]) / 2, KxiQ the difference / 2
+  double KxiP[(kMaxB / 2) * (kMaxB / 2)], KxiQ[(kMaxB / 2) * (kMaxB / 2)];
 };
 
 // Limiter projections of one order, in global memory (they are read by

@@ -354,12 +354,33 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::TH
 #pragma unroll
           for (int n = 0; n < b; n++) f[n] = base[n * is];
           const double us = first ? it_us[k] : T.w[t] * it_us[k];
+          if constexpr (b % 2 == 0) {  // even and odd parts (OrderTables::KxiP/KxiQ)
+            constexpr int h = b / 2;
+            double fp[h], fm[h];
 #pragma unroll
-          for (int l = 0; l < b; l++) {
-            double s = 0.0;
+            for (int n = 0; n < h; n++) {
+              fp[n] = f[n] + f[b - 1 - n];
+              fm[n] = f[n] - f[b - 1 - n];
+            }
 #pragma unroll
-            for (int n = 0; n < b; n++) s = fma(f[n], T.Kxi[n * b + l], s);
-            base[l * is] = us * s;
+            for (int l = 0; l < h; l++) {
+              double A = 0.0, Bq = 0.0;
+#pragma unroll
+              for (int n = 0; n < h; n++) {
+                A = fma(fp[n], T.KxiP[n * h + l], A);
+                Bq = fma(fm[n], T.KxiQ[n * h + l], Bq);
+              }
+              base[l * is] = us * (Bq + A);
+              base[(b - 1 - l) * is] = us * (Bq - A);
+            }
+          } else {
+#pragma unroll
+            for (int l = 0; l < b; l++) {
+              double s = 0.0;
+#pragma unroll
+              for (int n = 0; n < b; n++) s = fma(f[n], T.Kxi[n * b + l], s);
+              base[l * is] = us * s;
+            }
           }
         }
       }
