@@ -173,7 +173,7 @@ struct AmrLaunch {
   static int volume(double* a, const double* b, int n, const int* fine, const int* coarse, const int* ld,
                     const int* idx, int op, cudaStream_t st) {
     if (n <= 0) return EXA_OK;
-    amr_volume_kernel<DIM, N, ND><<<n, 256, 0, st>>>(a, b, n, fine, coarse, ld, idx, op);
+    amr_volume_kernel<DIM, N, ND><<<n, 128, 0, st>>>(a, b, n, fine, coarse, ld, idx, op);
     EXA_LAUNCHED();
     return EXA_OK;
   }
