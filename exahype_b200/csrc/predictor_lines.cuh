@@ -449,24 +449,40 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::TH
         }
       }
     }
-    if (nd_ok) sR[p] = part;
-    __syncthreads();
-    {
-      constexpr int kFullWarps = C::THREADS / 32;
-      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      if (warp < kFullWarps) {
-        for (int c = warp; c < C::CPB; c += kFullWarps) {
-          double* rr = smem + C::CPB * (C::SQ + C::SF) + c * C::SR;
-          double acc = 0.0;
-          for (int i = lane; i < P; i += 32) acc += rr[i];
+    double sq_res;
+    if constexpr (TM) {
+      // whole warps, one cell: each warp sums its lanes (the threads without
+      // a node add zero), one barrier, every thread adds the warp sums in
+      // the same order
+      constexpr int NW = C::THREADS / 32;
+      double acc = nd_ok ? part : 0.0;
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-          if (lane == 0) rr[P] = acc;
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if ((threadIdx.x & 31) == 0) sR[warp] = acc;
+      __syncthreads();
+      sq_res = 0.0;
+#pragma unroll
+      for (int w = 0; w < NW; w++) sq_res += sR[w];
+    } else {
+      if (nd_ok) sR[p] = part;
+      __syncthreads();
+      {
+        constexpr int kFullWarps = C::THREADS / 32;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (warp < kFullWarps) {
+          for (int c = warp; c < C::CPB; c += kFullWarps) {
+            double* rr = smem + C::CPB * (C::SQ + C::SF) + c * C::SR;
+            double acc = 0.0;
+            for (int i = lane; i < P; i += 32) acc += rr[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) rr[P] = acc;
+          }
         }
       }
+      __syncthreads();
+      sq_res = sR[P];
     }
-    __syncthreads();
-    const double sq_res = sR[P];
     if (!done) {
       it_done = iter + 1;
       if (sq_res < 1e-7 * 1e-7 || iter + 1 == C::maxIter) {
