@@ -231,8 +231,8 @@ static int launch_corrector(double* luh, const double* du, const double* fb, con
 //   6 line form, two time slices per phase, 2 blocks/SM
 //   7 line form, two time slices per phase, 1 block/SM
 //   8 line form, Picard iterate in tensor memory, two slices per phase,
-//     2 blocks/SM (3D shapes with one cell per block and five state
-//     variables; elsewhere as variant 6)
+//     2 blocks/SM (orders up to 5 with five state variables; elsewhere as
+//     variant 6)
 // and the mixed-precision line form (FP32 increment sweeps after the first
 // FP64 sweep), selected explicitly, never by the autotuner:
 //   4 mixed line form, 1 block/SM     5 mixed line form, 2 blocks/SM
@@ -281,11 +281,12 @@ struct Launch {
   static constexpr bool kMixed2 = 2 * LinesCfg<DIM, N, PDE, 2, true>::SMEM <= 227 * 1024;
   static constexpr bool kSlices2 = 2 * LinesCfg<DIM, N, PDE, 2, false, 2>::SMEM <= 227 * 1024;
   static constexpr bool kSlices1 = LinesCfg<DIM, N, PDE, 1, false, 2>::SMEM <= 227 * 1024;
-  // the tensor-memory iterate (variant 8): 3D, one cell per block,
-  // five doubles per node and slice, whole warps of at most 256 threads
+  // the tensor-memory iterate (variant 8): five doubles per node and slice
+  // (at most 60 columns: N <= 5), a block of whole warps of at most 256 threads
   using Sh = Shape<DIM, N, PDE>;
-  static constexpr bool kTmemShape = DIM == 3 && Sh::nD == 5 && cells_per_block<Sh::P>() == 1 &&
-                                     (Sh::P + 31) / 32 * 32 <= 256 && 2 * Sh::b * Sh::nD <= 64;
+  static constexpr bool kTmemShape = Sh::nD == 5 && Sh::nV == 5 &&
+                                     (cells_per_block<Sh::P>() * Sh::P + 31) / 32 * 32 <= 256 &&
+                                     2 * Sh::b * Sh::nD <= 64;
   template <int TS>
   static constexpr bool tmem_fits() {
     if constexpr (kTmemShape) return 2 * LinesCfg<DIM, N, PDE, 2, false, TS, true>::SMEM <= 227 * 1024;

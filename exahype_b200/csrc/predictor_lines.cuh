@@ -20,14 +20,18 @@
 //      rhs and folds the rhs into its Picard accumulators through iK1.
 // Shared memory per cell: lQi [P][b][nD], one line-major slice, residuals.
 //
-// TM (3D, one cell per block, five state variables): the Picard iterate lQi
-// lives in tensor memory instead (tmem.cuh: each thread owns one TMEM lane,
-// 60 columns of it), so that its reads and writes (phase A, the residual, the
-// update, the time average) leave the shared-memory pipe, which bounds this
-// kernel. The tensor-memory instructions are warp-collective, so the block
-// is rounded up to whole warps (216 nodes: 224 threads); the 8 threads
-// without a node take part in those instructions and in the phase-B items
-// only.
+// TM (five state variables, at most 60 columns per thread): the Picard
+// iterate lQi lives in tensor memory instead (tmem.cuh: each thread owns one
+// TMEM lane, 60 columns of it), so that its reads and writes (phase A, the
+// residual, the update, the time average) leave the shared-memory pipe,
+// which bounds this kernel. The tensor-memory instructions are
+// warp-collective, so the block is rounded up to whole warps (3D N=5, 216
+// nodes: 224 threads; 2D N=5, seven cells of 36: 256); the threads without
+// a node take part in those instructions and in the phase-B items only.
+// With several cells per block a warp can hold nodes of cells in different
+// states (iterating, converged), so there every tensor-memory instruction is
+// issued under block-uniform control only, and per-cell work is selected by
+// the data (a converged cell stores its unchanged iterate back).
 #pragma once
 #include "aderdg.cuh"
 #include "tmem.cuh"
@@ -78,8 +82,8 @@ struct LinesCfg : Shape<DIM, N, PDE> {
   // take consecutive column ranges)
   static constexpr int TCOL = 64;
   static constexpr int TCOLS = TCOL * ((THREADS / 32 + 3) / 4);
-  static_assert(!TM || (CPB == 1 && !MIXED && S::nD == 5 && 2 * S::b * S::nD <= TCOL && THREADS <= 256),
-                "tensor-memory iterate: one cell per block, five doubles per node and slice");
+  static_assert(!TM || (!MIXED && S::nD == 5 && S::nV == 5 && 2 * S::b * S::nD <= TCOL && THREADS <= 256),
+                "tensor-memory iterate: five doubles per node and slice, at most 256 threads");
   // lQi region (TM: none; the region later holds the time-averaged state and
   // the staged volume integral of every node)
   static constexpr int SQ = TM ? S::P * (S::nD > S::nV ? S::nD : S::nV) : S::P * QS;
@@ -137,9 +141,10 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::TH
   // a device-side count that leaves this block without cells: the whole
   // block returns before its first barrier (a gated launch costs little)
   if (count && (int)blockIdx.x * C::CPB >= min(*count, ncells)) return;
-  const int lc = TM ? 0 : threadIdx.x / P;
+  const int lc = TM ? min((int)threadIdx.x / P, C::CPB - 1) : threadIdx.x / P;
   const int p = threadIdx.x - lc * P;
   const bool nd_ok = !TM || p < P;  // TM: the threads past the last node hold none
+  constexpr bool kTMany = TM && C::CPB > 1;  // tensor memory, several cells per block
   // TM: the CTA's tensor memory (warp 0 allocates it here and frees it after
   // the last read of the iterate)
   const int warp = threadIdx.x >> 5;
@@ -301,14 +306,14 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::TH
 #pragma unroll
           for (int v = 0; v < nV; v++)
             sF32[sa[d] + v] = (float)(Fl[d][v] - Fp[d][v]);
-      } else if (!done) {
+      } else if (kTMany || !done) {
 #pragma unroll
         for (int j = 0; j < TS; j++) {
           const int t = t0 + j;
           if (t < b && !(first && j > 0)) {
             double Q[nD];
-            q_ld(t, Q);
-            if (!nd_ok) continue;
+            q_ld(t, Q);  // kTMany: by every thread, the conditions are block-uniform
+            if (!nd_ok || done) continue;
             double Fl[DIM][nV];
             PDE::template flux<DIM>(Q, Fl);
 #pragma unroll
@@ -436,11 +441,12 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::TH
     }
     // residual, reduced per cell by one warp
     double part = 0.0;
-    if (!done) {
+    if (kTMany || !done) {
 #pragma unroll
       for (int l = 0; l < b; l++) {
         double qo[nD];
         if (!low) q_ld(l, qo);
+        if (kTMany && done) continue;
 #pragma unroll
         for (int v = 0; v < nV; v++) {
           const double dq = low ? qn[l][v] : qn[l][v] - qo[v];
@@ -450,7 +456,7 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::TH
       }
     }
     double sq_res;
-    if constexpr (TM) {
+    if constexpr (TM && C::CPB == 1) {
       // whole warps, one cell: each warp sums its lanes (the threads without
       // a node add zero), one barrier, every thread adds the warp sums in
       // the same order
@@ -483,7 +489,41 @@ __global__ void __launch_bounds__(LinesCfg<DIM, N, PDE, MINB, MIXED, TS, TM>::TH
       __syncthreads();
       sq_res = sR[P];
     }
-    if (!done) {
+    if constexpr (kTMany) {
+      // every thread: each slice's old iterate is read and the new one (a
+      // finished cell: the old one) written back; a cell that converges now
+      // takes the time average of its old fluxes
+      const bool conv = !done && (sq_res < 1e-7 * 1e-7 || iter + 1 == C::maxIter);
+      if (!done) it_done = iter + 1;
+      double fh[DIM][nV];
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int v = 0; v < nV; v++) fh[d][v] = 0.0;
+#pragma unroll
+      for (int t = 0; t < b; t++) {
+        double Q[nD], W[nD];
+        q_ld(t, Q);
+#pragma unroll
+        for (int v = 0; v < nD; v++) W[v] = done ? Q[v] : qn[t][v];
+        q_st(t, W);
+        if (conv && nd_ok) {
+          double Fl[DIM][nV];
+          PDE::template flux<DIM>(Q, Fl);
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int v = 0; v < nV; v++) fh[d][v] += Fl[d][v] * T.w[t];
+        }
+      }
+      if (conv && nd_ok)
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int v = 0; v < nV; v++) sF[sa[d] + v] = fh[d][v];
+      if (conv) done = true;
+      tmem::wait_st();
+    } else if (!done) {
       it_done = iter + 1;
       if (sq_res < 1e-7 * 1e-7 || iter + 1 == C::maxIter) {
         // time-averaged fluxes of this sweep = of the iterate before the

@@ -86,7 +86,7 @@ int exa_solver_sizes(const exa_solver* s, int* sizes4);
  * its own device buffers and synchronises the device. */
 #define EXA_PREDICTOR_VARIANTS 9  /* size of variant_ms; 4 and 5 (mixed) are not timed (-1) */
 /* Variant 8 keeps the Picard iterate of the line-form predictor in the SM's
- * tensor memory (3D solvers of order 5 with five state variables; other
+ * tensor memory (solvers of order up to 5 with five state variables; other
  * shapes run variant 6 under this number). */
 /* Variants beyond the autotuned ones (exa_solver_set_variant only): the
  * mixed-precision predictor. Its first Picard sweep is the FP64 sweep; every

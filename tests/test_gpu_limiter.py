@@ -44,7 +44,8 @@ def interior(lim, dim, order):
     return lim.reshape(n, E, E, E, 5)[:, 2:2 + B, 2:2 + B, 2:2 + B].reshape(n, -1, 5)
 
 
-def make_pair(eb, dim, order, cells, bc, helper, cure, seed, fv_ic=True, problem="explosion", radius=0.2):
+def make_pair(eb, dim, order, cells, bc, helper, cure, seed, fv_ic=True, problem="explosion", radius=0.2,
+              variant=None):
     from exahype_b200 import problems
     if problem == "explosion":
         luh, fv, _ = problems.explosion(dim, order, cells, seed=seed, radius=radius)
@@ -53,6 +54,8 @@ def make_pair(eb, dim, order, cells, bc, helper, cure, seed, fv_ic=True, problem
         fv = None
     size = [1.0] * dim
     s = eb.Solver(dim, order)
+    if variant is not None:
+        s.variant = variant
     g = eb.LimitingMesh(s, cells, [0.0] * dim, size, bc, helper_layers=helper, cure_steps=cure)
     o = pyoracle.LimitingMesh(dim, order, cells, size, bc, helper_layers=helper, cure_steps=cure, nthreads=8)
     for m in (g, o):
@@ -107,6 +110,23 @@ def test_limiting_mesh_2d_outflow(eb, dim, order, cells, steps, helper, cure):
         seen_irregular |= o.state()["irregular_steps"] > 0
     if helper == 1:  # with one helper layer the shock soon leaves the FV region
         assert seen_irregular
+
+
+@pytest.mark.parametrize("dim,order,cells,steps,helper,cure", [
+    (2, 3, (20, 20), 40, 1, 0),
+    (2, 5, (16, 16), 40, 1, 0),
+    (2, 4, (14, 14), 30, 1, 2),
+])
+def test_limiting_mesh_2d_tensor_memory_predictor(eb, dim, order, cells, steps, helper, cure):
+    """the same comparison with the line-form predictor that keeps the Picard
+    iterate in tensor memory (variant 8), run on the limiting mesh's
+    device-compacted cell lists with several cells per block"""
+    _, g, o = make_pair(eb, dim, order, cells, 0, helper, cure, seed=3, variant=8)
+    compare(g, o, dim, order, "init")
+    for k in range(steps):
+        g.step(1)
+        o.step(1)
+        compare(g, o, dim, order, "step %d" % (k + 1), check_lim=(k % 5 == 4))
 
 
 @pytest.mark.parametrize("order,cells,steps", [(3, (6, 6, 6), 10), (5, (5, 5, 5), 6)])
