@@ -312,10 +312,20 @@ __global__ void lim_merge_faces_kernel(const int* __restrict__ fl, const int* __
     double* mn2 = minB + ((size_t)c2 * D2 + f2) * 5;
     double* mx1 = maxB + ((size_t)c1 * D2 + f1) * 5;
     double* mx2 = maxB + ((size_t)c2 * D2 + f2) * 5;
+    // all twenty loads before the first store (the four blocks lie in one
+    // array each, so the compiler could not move a load above a store)
+    double a1[5], a2[5], b1[5], b2[5];
 #pragma unroll
     for (int i = 0; i < 5; i++) {
-      const double mn = (mn2[i] < mn1[i]) ? mn2[i] : mn1[i];
-      const double mx = (mx1[i] < mx2[i]) ? mx2[i] : mx1[i];
+      a1[i] = mn1[i];
+      a2[i] = mn2[i];
+      b1[i] = mx1[i];
+      b2[i] = mx2[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+      const double mn = (a2[i] < a1[i]) ? a2[i] : a1[i];
+      const double mx = (b1[i] < b2[i]) ? b2[i] : b1[i];
       mn1[i] = mn2[i] = mn;
       mx1[i] = mx2[i] = mx;
     }
@@ -953,17 +963,24 @@ __global__ void lim_spread_cells_kernel(int ncells, int* __restrict__ s, int* __
   if (c >= ncells || (gate && !*gate)) return;
   int alloc = 0;
   if (lane == 0) {
+    // every load first (one memory round trip), then the status machine
+    const int sc = s[c], hl = has_lim[c];
+    int fsc[D2];
+#pragma unroll
+    for (int i = 0; i < D2; i++) fsc[i] = fs[c * D2 + i];
     int ns;
-    if (s[c] < prm.T) {
+    if (sc < prm.T) {
       ns = 0;
-      for (int i = 0; i < D2; i++) ns = max(ns, fs[c * D2 + i]);
+#pragma unroll
+      for (int i = 0; i < D2; i++) ns = max(ns, fsc[i]);
     } else {
       ns = prm.T;
       cure[c] = prm.cure_steps + 1;
     }
     s[c] = ns;
+#pragma unroll
     for (int i = 0; i < D2; i++) fs[c * D2 + i] = 0;
-    alloc = ns > 0 && !has_lim[c];
+    alloc = ns > 0 && !hl;
     if (alloc) has_lim[c] = 1;
   }
   if (__shfl_sync(0xffffffffu, alloc, 0)) {
