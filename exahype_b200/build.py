@@ -14,7 +14,7 @@ REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "lib", "libexahype_b200.so")
 SOURCES = ["csrc/capi.cu"]
 HEADERS = ["csrc/common.cuh", "csrc/pde.cuh", "csrc/aderdg.cuh", "csrc/predictor_lines.cuh", "csrc/limiter.cuh", "csrc/batch.cuh",
-           "csrc/linear.cuh", "csrc/amr.cuh", "csrc/dg_tables.h"]
+           "csrc/linear.cuh", "csrc/amr.cuh", "csrc/dg_tables.h", "csrc/tmem.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
