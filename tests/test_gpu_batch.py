@@ -65,6 +65,20 @@ def test_batch_matches_single_meshes(eb, graph):
         check_same(eb, bt, iid, p, 8)
 
 
+def test_batch_tensor_memory_predictor(eb):
+    """every order forced to variant 8 (the tensor-memory predictor where the
+    shape allows it): each instance still equals its single-mesh run"""
+    probs = problems_mix()
+    bt = eb.Batch()
+    for p in probs:  # before the first instance of each order: its first predictor runs variant 8 too
+        bt.set_variant(p["dim"], p["order"], 8)
+    ids = [bt.add(p["dim"], p["order"], p["cells"], [1.0] * p["dim"], p["bc"], p["luh"]) for p in probs]
+    bt.step(6)
+    for iid, p in zip(ids, probs):
+        assert bt.variant(p["dim"], p["order"]) == 8
+        check_same(eb, bt, iid, p, 6)
+
+
 def test_batch_membership_changes(eb):
     probs = problems_mix()
     bt = eb.Batch()

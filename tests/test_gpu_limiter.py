@@ -129,9 +129,12 @@ def test_limiting_mesh_2d_tensor_memory_predictor(eb, dim, order, cells, steps, 
         compare(g, o, dim, order, "step %d" % (k + 1), check_lim=(k % 5 == 4))
 
 
-@pytest.mark.parametrize("order,cells,steps", [(3, (6, 6, 6), 10), (5, (5, 5, 5), 6)])
-def test_limiting_mesh_3d_outflow(eb, order, cells, steps):
-    _, g, o = make_pair(eb, 3, order, cells, 0, 1, 0, seed=1)
+@pytest.mark.parametrize("order,cells,steps,variant", [(3, (6, 6, 6), 10, None), (5, (5, 5, 5), 6, None),
+                                                     (3, (6, 6, 6), 10, 8), (5, (5, 5, 5), 6, 8)])
+def test_limiting_mesh_3d_outflow(eb, order, cells, steps, variant):
+    """variant 8: the tensor-memory predictor on the limiting mesh's cell lists
+    (3D N=5: one cell per block; N=3: four)"""
+    _, g, o = make_pair(eb, 3, order, cells, 0, 1, 0, seed=1, variant=variant)
     compare(g, o, 3, order, "init")
     for k in range(steps):
         g.step(1)
